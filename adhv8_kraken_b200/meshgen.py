@@ -1,0 +1,186 @@
+"""Seeded synthetic SW2 problems.
+
+The reference publishes no benchmark meshes, so every workload is generated here
+from a seed.  Two families:
+
+* :func:`channel` -- the rectangular channel: ``nx x ny`` squares, each split
+  into two triangles along the (i,j)-(i+1,j+1) diagonal, bed sloping along +x,
+  unit-discharge inflow (``NB VEL``) on the west edge and a tailwater level
+  (``NB OTW``) on the east edge.
+* :func:`bumpy_basin` -- Delaunay triangulation of seeded uniform points in a
+  square, bed = planar slope + Gaussian bumps, flat initial water surface (dry
+  bump tops give wet/dry fronts), per-element log-normal Manning n quantised into
+  ``nbins`` material classes, inflow hydrograph on the west edge and a tailwater
+  level on the east edge.
+
+Nodes are ordered along a Morton (Z-order) curve so that element gathers on the
+GPU and the block solver of the reference CPU path both see local data.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .model import (BCT_PRS_NEU, BCT_VEL_NEU, NORMAL, Material, Params, Series,
+                    StringSpec, SW2Model)
+
+
+def _morton_order(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """Permutation that sorts points along a 2D Z-order curve (16 bits per axis)."""
+    span = max(float(x.max() - x.min()), float(y.max() - y.min()), 1e-30)
+    ix = np.clip(((x - x.min()) / span * 65535.0).astype(np.uint64), 0, 65535)
+    iy = np.clip(((y - y.min()) / span * 65535.0).astype(np.uint64), 0, 65535)
+
+    def spread(v):
+        v = (v | (v << np.uint64(8))) & np.uint64(0x00FF00FF)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x0F0F0F0F)
+        v = (v | (v << np.uint64(2))) & np.uint64(0x33333333)
+        v = (v | (v << np.uint64(1))) & np.uint64(0x55555555)
+        return v
+
+    code = spread(ix) | (spread(iy) << np.uint64(1))
+    return np.argsort(code, kind="stable")
+
+
+def channel(nx: int = 100, ny: int = 20, length: float = 1000.0, width: float = 200.0,
+            slope: float = 1e-4, manning: float = 0.025, q_in: float = 0.5, h_out: float = 1.0,
+            h0: float = 1.0, dt: float = 10.0, nsteps: int = 20, tol_nonlin: float = 1e-8,
+            name: str = "channel") -> SW2Model:
+    """Rectangular channel (4,000 triangles and 2,121 nodes at the default 100 x 20).
+
+    Nodes are numbered column by column (y fastest), which keeps the reference's
+    profile LU bandwidth at ``3 (ny + 2)``.
+    """
+    ii, jj = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), indexing="ij")
+    x = (ii * (length / nx)).ravel().astype(np.float64)
+    y = (jj * (width / ny)).ravel().astype(np.float64)
+    z = -slope * x
+    nid = lambda i, j: i * (ny + 1) + j
+    tri = []
+    for i in range(nx):
+        for j in range(ny):
+            a, b, c, d = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
+            tri.append((a, b, c))
+            tri.append((a, c, d))
+    tri = np.array(tri, dtype=np.int32)
+    west = [(nid(0, j + 1), nid(0, j)) for j in range(ny)]
+    east = [(nid(nx, j), nid(nx, j + 1)) for j in range(ny)]
+    edges = np.array(west + east, dtype=np.int32)
+    strings = [StringSpec("mat", manning_n=manning),
+               StringSpec("edge", bc_flag=BCT_VEL_NEU, isigma=0),
+               StringSpec("edge", bc_flag=BCT_PRS_NEU, isigma=1)]
+    edge_string = np.array([1] * ny + [2] * ny, dtype=np.int32)
+    t_end = (nsteps + 10) * dt
+    series = [Series(np.array([0.0, t_end]), np.array([q_in, q_in])),
+              Series(np.array([0.0, t_end]), np.array([-slope * length + h_out] * 2))]
+    V = x.shape[0]
+    return SW2Model(x=x, y=y, z=z, tri=tri, tri_mat=np.zeros(tri.shape[0], np.int32),
+                    edges=edges, edge_string=edge_string,
+                    node_string=np.full(V, NORMAL, np.int32), strings=strings,
+                    materials=[Material(evs=(0.0, 0.0, 0.0))], series=series,
+                    params=Params(tol_nonlin=tol_nonlin), h0=np.full(V, h0), u0=np.zeros(V),
+                    v0=np.zeros(V), dt=dt, nsteps=nsteps, name=name)
+
+
+def bumpy_basin(npoints: int, seed: int, size: float = 20000.0, slope: float = 5e-4,
+                nbumps: int = 40, wse0: float = 2.0, n_median: float = 0.03, n_sigma: float = 0.3,
+                nbins: int = 32, q_start: float = 1.0, q_peak: float = 5.0, ramp_steps: int = 30,
+                dt: float = 5.0, nsteps: int = 100, drying_limit: float = 0.1,
+                tol_nonlin: float = 1e-6, name: str = "basin") -> SW2Model:
+    """Seeded Delaunay basin with bumps (triangle count is about ``2 * npoints``).
+
+    * bed: ``z = -slope * x + sum_k A_k exp(-|p - c_k|^2 / (2 s_k^2))`` with
+      ``A_k ~ U[0.5, 3]`` m, ``s_k ~ U[200, 1500]`` m (scaled with ``size``),
+      centres uniform;
+    * initial water surface flat at ``wse0``: depth ``h = wse0 - z`` (negative
+      where the bed is above the water, the reference's convention for dry land);
+    * Manning n ~ LogNormal(ln n_median, n_sigma) per element, quantised to
+      ``nbins`` geometric bins, one material (and one ``FR MNG`` string) per bin;
+    * west edge: unit-discharge inflow ramping linearly ``q_start -> q_peak`` over
+      ``ramp_steps`` steps, then held; east edge: tailwater level ``wse0``.
+    """
+    from scipy.spatial import Delaunay
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nb = max(8, int(round(math.sqrt(npoints) / 2)))        # points per side
+    s = np.linspace(0.0, size, nb + 1)[:-1]
+    bx = np.concatenate([s, np.full(nb, size), s[::-1] + size / nb, np.zeros(nb)])
+    by = np.concatenate([np.zeros(nb), s, np.full(nb, size), s[::-1] + size / nb])
+    nin = max(npoints - bx.shape[0], 16)
+    margin = size / nb * 0.25
+    ix = rng.uniform(margin, size - margin, nin)
+    iy = rng.uniform(margin, size - margin, nin)
+    x = np.concatenate([bx, ix])
+    y = np.concatenate([by, iy])
+    order = _morton_order(x, y)
+    x, y = x[order].copy(), y[order].copy()
+    tri = Delaunay(np.stack([x, y], axis=1)).simplices.astype(np.int32)
+    # counter-clockwise orientation and no slivers
+    x1, x2, x3 = x[tri[:, 0]], x[tri[:, 1]], x[tri[:, 2]]
+    y1, y2, y3 = y[tri[:, 0]], y[tri[:, 1]], y[tri[:, 2]]
+    cross = (x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1)
+    tri[cross < 0] = tri[cross < 0][:, [0, 2, 1]]
+    cross = np.abs(cross)
+    tri = tri[cross > 1e-6 * (size / math.sqrt(npoints)) ** 2]
+    # renumber elements by the Morton code of their centroid
+    cx = x[tri].mean(axis=1)
+    cy = y[tri].mean(axis=1)
+    tri = tri[_morton_order(cx, cy)]
+    scale = size / 20000.0
+    amp = rng.uniform(0.5, 3.0, nbumps)
+    wid = rng.uniform(200.0, 1500.0, nbumps) * scale
+    cxb = rng.uniform(0.0, size, nbumps)
+    cyb = rng.uniform(0.0, size, nbumps)
+    z = -slope * x
+    for a, w, u, v in zip(amp, wid, cxb, cyb):
+        z = z + a * np.exp(-((x - u) ** 2 + (y - v) ** 2) / (2.0 * w * w))
+    h0 = wse0 - z
+    # per-element roughness classes
+    n_elem = np.exp(rng.normal(math.log(n_median), n_sigma, tri.shape[0]))
+    lo, hi = n_median * math.exp(-3 * n_sigma), n_median * math.exp(3 * n_sigma)
+    edges_b = np.geomspace(lo, hi, nbins + 1)
+    tri_mat = np.clip(np.searchsorted(edges_b, n_elem) - 1, 0, nbins - 1).astype(np.int32)
+    bin_n = np.sqrt(edges_b[:-1] * edges_b[1:])
+    # boundary edges (west: inflow, east: tailwater), oriented as in the mesh
+    tol = 1e-9 * size
+    ekey = {}
+    for (a, b, c) in tri:
+        for p, q in ((a, b), (b, c), (c, a)):
+            k = (min(p, q), max(p, q))
+            ekey[k] = ekey.get(k, 0) + 1
+    bedges = [k for k, cnt in ekey.items() if cnt == 1]
+    west = sorted([k for k in bedges if x[k[0]] < tol and x[k[1]] < tol], key=lambda k: y[k[0]] + y[k[1]])
+    east = sorted([k for k in bedges if x[k[0]] > size - tol and x[k[1]] > size - tol],
+                  key=lambda k: y[k[0]] + y[k[1]])
+    edges = np.array(west + east, dtype=np.int32)
+    strings = [StringSpec("mat", manning_n=float(n)) for n in bin_n]
+    strings += [StringSpec("edge", bc_flag=BCT_VEL_NEU, isigma=0),
+                StringSpec("edge", bc_flag=BCT_PRS_NEU, isigma=1)]
+    edge_string = np.array([nbins] * len(west) + [nbins + 1] * len(east), dtype=np.int32)
+    t_end = (nsteps + 10) * dt
+    ramp = ramp_steps * dt
+    series = [Series(np.array([0.0, ramp, max(t_end, ramp + dt)]), np.array([q_start, q_peak, q_peak])),
+              Series(np.array([0.0, t_end]), np.array([wse0, wse0]))]
+    V = x.shape[0]
+    params = Params(tol_nonlin=tol_nonlin, drying_limit=drying_limit, nblock=max(1, V // 2000))
+    return SW2Model(x=x, y=y, z=z, tri=tri, tri_mat=tri_mat, edges=edges, edge_string=edge_string,
+                    node_string=np.full(V, NORMAL, np.int32), strings=strings,
+                    materials=[Material(evs=(0.0, 0.0, 0.0)) for _ in range(nbins)], series=series,
+                    params=params, h0=h0, u0=np.zeros(V), v0=np.zeros(V), dt=dt, nsteps=nsteps, name=name)
+
+
+def ensemble_member(seed: int, tri_lo: float = 5e3, tri_hi: float = 2e5, nsteps: int = 50,
+                    name: str = "member") -> SW2Model:
+    """One instance of the batched ensemble: triangle count log-uniform in
+    [tri_lo, tri_hi], Manning median U[0.015, 0.05], inflow peak U[1, 8] m^2/s,
+    dt U[2, 10] s, its own bathymetry seed."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    T = math.exp(rng.uniform(math.log(tri_lo), math.log(tri_hi)))
+    n_med = rng.uniform(0.015, 0.05)
+    q_peak = rng.uniform(1.0, 8.0)
+    dt = rng.uniform(2.0, 10.0)
+    sub = int(rng.integers(0, 2**31 - 1))
+    size = 20000.0 * math.sqrt(T / 1.0e6)
+    return bumpy_basin(int(T / 2), sub, size=size, n_median=n_med, q_peak=q_peak, dt=dt,
+                       nsteps=nsteps, name=f"{name}{seed}")

@@ -1,0 +1,151 @@
+/* sw2gpu.h -- C ABI of the B200 SW2 (2D shallow-water) Newton step.
+ *
+ * Drop-in for the AdH SW2 solve path:
+ *   fe_sw2_solve(SSUPER_MODEL*, int)            src/fe/sw2/fe_sw2_solve.c:30-57
+ *     -> fe_newton(..., fe_sw2_init, fe_sw2_update, fe_sw2_resid, fe_sw2_load, fe_sw2_inc)
+ *                                               src/fe/fe_newton.c:214-912
+ *        -> fe_sw2_resid / fe_sw2_body_resid / fe_sw2_boundary_resid
+ *                                               src/fe/sw2/fe_sw2_resid.c:29-216
+ *        -> fe_sw2_load (FD Jacobian)           src/fe/sw2/fe_sw2_load.c:34-269
+ *        -> solv_linear_sys_setup / _solve      src/solver/solv_linear_sys_setup.c:15,
+ *                                               src/solver/solv_linear_sys_solve.c:16
+ *
+ * Plain pointers and sizes only.  Every entry point returns 0 on success and a
+ * nonzero SW2GPU_E* code on failure; sw2gpu_last_error() gives the message.
+ * Node unknowns are ordered [u, v, h] per node, Jacobian blocks are 3x3
+ * row-major with rows (x-momentum, y-momentum, continuity) and columns (u, v, h)
+ * (src/fe/fe_assemble_matrix.c:200-208).
+ */
+#ifndef SW2GPU_H
+#define SW2GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SW2GPU_ABI_VERSION 1
+
+/* status codes */
+#define SW2GPU_OK            0
+#define SW2GPU_E_ARG         1   /* bad argument / unsupported input */
+#define SW2GPU_E_CUDA        2   /* CUDA runtime error */
+#define SW2GPU_E_NOMEM       3   /* device allocation failed / admission refused */
+#define SW2GPU_E_NEWTON      4   /* Newton did not converge: state reset, caller scales dt (tc_scale) */
+#define SW2GPU_E_LINEAR      5   /* Krylov hit max_lin_it (solv_bcgstab.c:280-292) */
+#define SW2GPU_E_NAN         6   /* NaN/Inf residual (fe_newton.c:119-124, 639-646) */
+#define SW2GPU_E_TIMEOUT     7   /* a bounded device wait ran out */
+
+/* boundary-condition flags (src/include/define.h) */
+#define SW2GPU_NORMAL        (-1)
+#define SW2GPU_BCT_OUTFLOW     4
+#define SW2GPU_BCT_PRS_DIR     7
+#define SW2GPU_BCT_VEL_DIR     8
+#define SW2GPU_BCT_PRS_NEU     9   /* NB OTW: tailwater elevation */
+#define SW2GPU_BCT_VEL_NEU    10   /* NB VEL: prescribed normal unit discharge */
+#define SW2GPU_BCT_WATER_SOURCE 12
+#define SW2GPU_BCT_VEL_PRS_DIR 16
+
+/* precision modes */
+#define SW2GPU_FP64          0   /* everything FP64 */
+#define SW2GPU_MIXED         1   /* FP32 Jacobian storage, SpMV and preconditioner; FP64 Newton */
+
+/* preconditioners of the device Krylov solve */
+#define SW2GPU_PREC_BJACOBI  0   /* 3x3 block Jacobi */
+#define SW2GPU_PREC_ILU0     1   /* block ILU(0) on the BCSR pattern, colour-ordered */
+
+/* Mesh and model data (what fe_sw2_* read from SGRID / SMODEL).  Host pointers;
+ * the library copies what it needs at create time. */
+typedef struct sw2gpu_mesh {
+    int32_t nnodes, nelems2d, nelems1d, nstrings, nmats, nseries;
+    const double  *x, *y, *z;          /* [nnodes] node coordinates and bed elevation */
+    const int32_t *node_string;        /* [nnodes] SW2GPU_NORMAL or string id (NDS) */
+    const int32_t *elem2d_nodes;       /* [3*nelems2d] counter-clockwise */
+    const int32_t *elem2d_mat;         /* [nelems2d] material id; its string id is the same */
+    const int32_t *elem1d_nodes;       /* [2*nelems1d] */
+    const int32_t *elem1d_string;      /* [nelems1d] edge string */
+    const int32_t *elem1d_parent;      /* [nelems1d] adjacent 2D element */
+    const int32_t *str_bc_flag;        /* [nstrings] ol_flow.bc_flag */
+    const int32_t *str_isigma;         /* [nstrings] series id or -1 */
+    const int32_t *str_ivx, *str_ivy, *str_iu0;   /* [nstrings] Dirichlet series ids or -1 */
+    const double  *str_rough_height;   /* [nstrings] fterms.eqrheight (UNSET_FLT = no drag) */
+    const int32_t *mat_eev_mode;       /* [nmats] 0: user eddy viscosity (EVS); 1..3: EEV mode */
+    const double  *mat_ev;             /* [3*nmats] EVS xx, yy, xy */
+    const double  *mat_eev_coef;       /* [nmats] */
+    const double  *mat_coriolis;       /* [nmats] latitude, degrees */
+} sw2gpu_mesh;
+
+typedef struct sw2gpu_params {
+    double  gravity, density, viscosity;
+    double  drying_lower_limit, drying_upper_limit;
+    double  tau_temporal, tau_pg;
+    double  tol_nonlin, inc_nonlin;    /* IP NTL / IP ITL (UNSET_FLT = unset) */
+    int32_t max_nonlin_it, max_lin_it, max_linesearch_cuts;
+    int32_t precision;                 /* SW2GPU_FP64 / SW2GPU_MIXED */
+    int32_t precond;                   /* SW2GPU_PREC_* */
+    int32_t reserved;
+    double  lin_rtol, lin_atol;        /* Krylov stop ||r||inf <= atol + rtol ||b||inf (ref: 1e-5, 1e-10) */
+} sw2gpu_params;
+
+typedef struct sw2gpu_stats {
+    int32_t status;                    /* SW2GPU_OK or error code */
+    int32_t newton_its;                /* nonlinear iterations of this call */
+    int32_t linear_its;                /* total Krylov iterations of this call */
+    int32_t linesearch_cuts;           /* total line-search halvings */
+    double  resid_max, resid_l2, inc_max;   /* final norms (get_residual_norms) */
+    double  device_ms;                 /* device time of the call (CUDA events) */
+    int32_t kernel_launches;           /* kernels launched by the call */
+    int32_t wd_elems;                  /* elements with wd_flag != 0 after the step */
+} sw2gpu_stats;
+
+typedef struct sw2gpu_ctx sw2gpu_ctx;
+
+/* Library / error info. */
+int         sw2gpu_abi_version(void);
+const char *sw2gpu_last_error(void);
+
+/* Builds the device mesh, element colouring and BCSR pattern (sw2gpu_prepare in the
+ * reference-side adapter; call again after every mesh adaption).  `stream` is a
+ * cudaStream_t (NULL = a stream owned by the context). */
+int sw2gpu_create(const sw2gpu_mesh *mesh, const sw2gpu_params *params, void *stream, sw2gpu_ctx **out);
+int sw2gpu_destroy(sw2gpu_ctx *ctx);
+
+/* State of time level `level` (0 = current t+dt iterate, 1 = old, 2 = older);
+ * SW2 state is (head, vel.x, vel.y) as in src/structs/ssw_2d.h:13-18. */
+int sw2gpu_set_state(sw2gpu_ctx *ctx, int level, const double *h, const double *u, const double *v);
+int sw2gpu_get_state(sw2gpu_ctx *ctx, int level, double *h, double *u, double *v);
+int sw2gpu_get_wd_flag(sw2gpu_ctx *ctx, int32_t *wd_flag);
+
+/* One implicit time step: time-level shift (fe_sw2, src/fe/sw2/fe_sw2.c:43-50) then the
+ * damped Newton loop (fe_newton).  `series` holds the step-averaged value of every BC
+ * series over [t, t+dt] (sseries_setall_ts_valuesAVG).  On SW2GPU_E_NEWTON the current
+ * state is reset to the old level (fe_sw2_init) and the caller retries with dt * 0.25. */
+int sw2gpu_step(sw2gpu_ctx *ctx, double dt, const double *series, sw2gpu_stats *stats);
+
+/* Hot-path pieces, for parity checks against the reference units:
+ *   sw2gpu_resid: fe_sw2_init-free residual at the current state (fe_sw2_resid);
+ *                 writes resid[3*nnodes] and applies the dry-node velocity zeroing.
+ *   sw2gpu_load:  FD Jacobian (fe_sw2_load incl. the tiny-diagonal fix) in BCSR form:
+ *                 row_ptr[nnodes+1], col[nnzb], val[9*nnzb] (sorted columns), and the
+ *                 residual after the fix in resid[3*nnodes].  Pass NULL to query nnzb. */
+int sw2gpu_set_dt(sw2gpu_ctx *ctx, double dt, const double *series);
+int sw2gpu_resid(sw2gpu_ctx *ctx, double *resid);
+int sw2gpu_load(sw2gpu_ctx *ctx, int32_t *nnzb, int32_t *row_ptr, int32_t *col, double *val, double *resid);
+
+/* Linear solve of a given BCSR system with the device Krylov solver (solv_linear_sys_setup
+ * + solv_linear_sys_solve): Jacobi scaling, preconditioned BiCGSTAB, unscaling.  The matrix
+ * uses the pattern of the context. */
+int sw2gpu_linear_solve(sw2gpu_ctx *ctx, const double *val, const double *rhs, double *x, int32_t *iterations);
+
+/* Batched ensemble: many independent contexts stepped by one persistent launch per
+ * phase over a concatenated BCSR with per-instance offsets. */
+typedef struct sw2gpu_batch sw2gpu_batch;
+int sw2gpu_batch_create(sw2gpu_ctx **ctxs, int32_t n, void *stream, sw2gpu_batch **out);
+int sw2gpu_batch_step(sw2gpu_batch *b, const double *dt, const double *const *series, sw2gpu_stats *stats);
+int sw2gpu_batch_destroy(sw2gpu_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SW2GPU_H */

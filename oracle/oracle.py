@@ -1,0 +1,161 @@
+"""ctypes front end of the CPU oracle (``oracle/sw2_oracle.c``).  TEST INFRASTRUCTURE ONLY.
+
+Used by ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` as the checker of the B200 library; never by the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from adhv8_kraken_b200.capi import MeshArrays, Stats, make_params, c_double_p, c_int32_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "sw2_oracle.c")
+LIB = os.path.join(HERE, "libsw2oracle.so")
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+        subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-std=c99", "-o", LIB, SRC, "-lm"], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        for name in ("orc_destroy", "orc_resid", "orc_load", "orc_wdflag"):
+            getattr(L, name).argtypes = [C.c_void_p] + ([c_double_p] if name == "orc_resid" else [])
+        L.orc_nnzb.restype = C.c_int
+        L.orc_bandwidth.restype = C.c_int
+        L.orc_step.restype = C.c_int
+        L.orc_step.argtypes = [C.c_void_p, C.c_double, c_double_p, C.c_void_p]
+        L.orc_linear_solve.restype = C.c_int
+        L.orc_linear_solve.argtypes = [C.c_void_p, c_double_p, c_double_p]
+        L.orc_set_dt.argtypes = [C.c_void_p, C.c_double, c_double_p]
+        L.orc_body_resid.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, c_double_p]
+        L.orc_nnzb.argtypes = [C.c_void_p]
+        L.orc_bandwidth.argtypes = [C.c_void_p]
+        L.orc_set_state.argtypes = [C.c_void_p, C.c_int, c_double_p, c_double_p, c_double_p]
+        L.orc_get_state.argtypes = [C.c_void_p, C.c_int, c_double_p, c_double_p, c_double_p]
+        L.orc_get_wd.argtypes = [C.c_void_p, c_int32_p]
+        L.orc_set_wd.argtypes = [C.c_void_p, c_int32_p]
+        L.orc_pattern.argtypes = [C.c_void_p, c_int32_p, c_int32_p]
+        L.orc_get_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
+        L.orc_set_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(c_double_p)
+
+
+def _ip(a):
+    return a.ctypes.data_as(c_int32_p)
+
+
+class Oracle:
+    """One SW2 model on the CPU, restating the reference step by step."""
+
+    def __init__(self, model, nblock: int = 1, lin_rtol: float = 1e-5, lin_atol: float = 1e-10):
+        self.model = model
+        self.arrays = MeshArrays(model)
+        self.params = make_params(model, lin_rtol=lin_rtol, lin_atol=lin_atol)
+        L = lib()
+        self.h = L.orc_create(C.byref(self.arrays.mesh), C.byref(self.params), nblock)
+        if not self.h:
+            raise ValueError("oracle rejected the model")
+        self.V, self.T = model.nnodes, model.nelems2d
+        self.nnzb = L.orc_nnzb(self.h)
+        self.t = model.t0
+        self.set_state(0, model.h0, model.u0, model.v0)
+        self.set_state(1, model.h0, model.u0, model.v0)
+        self.set_state(2, model.h0, model.u0, model.v0)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def set_state(self, level, h, u, v):
+        h, u, v = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, u, v))
+        lib().orc_set_state(C.c_void_p(self.h), level, _dp(h), _dp(u), _dp(v))
+
+    def get_state(self, level=0):
+        h, u, v = (np.zeros(self.V) for _ in range(3))
+        lib().orc_get_state(C.c_void_p(self.h), level, _dp(h), _dp(u), _dp(v))
+        return h, u, v
+
+    def set_dt(self, dt, series):
+        s = np.ascontiguousarray(series, dtype=np.float64)
+        lib().orc_set_dt(C.c_void_p(self.h), dt, _dp(s) if s.size else None)
+
+    def wdflag(self):
+        lib().orc_wdflag(self.h)
+        return self.get_wd()
+
+    def get_wd(self):
+        wd = np.zeros(self.T, np.int32)
+        lib().orc_get_wd(C.c_void_p(self.h), _ip(wd))
+        return wd
+
+    def set_wd(self, wd):
+        wd = np.ascontiguousarray(wd, dtype=np.int32)
+        lib().orc_set_wd(C.c_void_p(self.h), _ip(wd))
+
+    def pattern(self):
+        rp = np.zeros(self.V + 1, np.int32)
+        col = np.zeros(self.nnzb, np.int32)
+        lib().orc_pattern(C.c_void_p(self.h), _ip(rp), _ip(col))
+        return rp, col
+
+    def resid(self):
+        r = np.zeros(3 * self.V)
+        lib().orc_resid(self.h, _dp(r))
+        return r
+
+    def load(self):
+        """FD Jacobian (sorted BCSR values) and the residual after the tiny-diagonal fix."""
+        lib().orc_load(self.h)
+        val = np.zeros(9 * self.nnzb)
+        r = np.zeros(3 * self.V)
+        lib().orc_get_matrix(C.c_void_p(self.h), _dp(val), _dp(r))
+        return val.reshape(-1, 3, 3), r
+
+    def set_matrix(self, val, resid):
+        val = np.ascontiguousarray(val, dtype=np.float64).reshape(-1)
+        resid = np.ascontiguousarray(resid, dtype=np.float64)
+        lib().orc_set_matrix(C.c_void_p(self.h), _dp(val), _dp(resid))
+
+    def linear_solve(self, rhs):
+        b = np.array(rhs, dtype=np.float64)
+        x = np.zeros(3 * self.V)
+        its = lib().orc_linear_solve(self.h, _dp(b), _dp(x))
+        return x, its
+
+    def body_resid(self, ie, eps=0.0, pnode=0, pvar=-1, psign=0):
+        out = np.zeros(9)
+        lib().orc_body_resid(self.h, ie, eps, pnode, pvar, psign, _dp(out))
+        return out.reshape(3, 3)
+
+    def step(self, dt=None, t=None):
+        """One time step with the series averaged over [t, t + dt]; returns the stats dict."""
+        dt = self.model.dt if dt is None else dt
+        t = self.t if t is None else t
+        s = self.model.series_values(t, t + dt)
+        st = Stats()
+        rc = lib().orc_step(self.h, dt, _dp(s) if s.size else None, C.byref(st))
+        if rc == 0:
+            self.t = t + dt
+        return st.as_dict()

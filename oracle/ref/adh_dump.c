@@ -1,0 +1,136 @@
+/* Observation harness for the reference AdH executable (test infrastructure only).
+ *
+ * The reference's own objects are linked unmodified; the linker option
+ * ``--wrap=fe_main --wrap=fe_sw2_load`` routes the calls made by the time loop
+ * (src/main/adh_func.c:549) and by the Newton driver (src/fe/fe_newton.c:454)
+ * through the two functions below, which call the originals and then append
+ * full-precision records to the binary file named by the environment variable
+ * ADH_DUMP:
+ *
+ *   "step"   after every accepted time step: t_prev, dt, Newton iterations of
+ *            the step (including failed attempts), the number of attempts, and
+ *            the nodal head / vel.x / vel.y / wd_flag arrays;
+ *   "load"   for the first ADH_DUMP_LOADS calls of fe_sw2_load: the state the
+ *            Jacobian was built at (three time levels), the residual vector,
+ *            the 3x3 diagonal blocks and every off-diagonal SPARSE_VECT row.
+ *
+ * Record layout: char tag[8]; int32 kind (0 = f64, 1 = i32); int64 count; data.
+ */
+#include "global_header.h"
+
+int __real_fe_main(SSUPER_MODEL *sm);
+void __real_fe_sw2_load(SSUPER_MODEL *sm, int imod);
+
+static FILE *dump_fp = NULL;
+static int dump_loads_left = -1;
+static int attempts = 0;
+static int it_mark = 0;
+
+static void dump_open(void) {
+    if (dump_fp != NULL) return;
+    const char *path = getenv("ADH_DUMP");
+    if (path == NULL) return;
+    dump_fp = fopen(path, "wb");
+    const char *nl = getenv("ADH_DUMP_LOADS");
+    dump_loads_left = nl ? atoi(nl) : 0;
+}
+
+static void put_f64(const char *tag, const double *v, long n) {
+    char t[8] = {0};
+    int kind = 0;
+    long long cnt = n;
+    strncpy(t, tag, 8);
+    fwrite(t, 1, 8, dump_fp);
+    fwrite(&kind, sizeof(int), 1, dump_fp);
+    fwrite(&cnt, sizeof(long long), 1, dump_fp);
+    fwrite(v, sizeof(double), (size_t) n, dump_fp);
+}
+
+static void put_i32(const char *tag, const int *v, long n) {
+    char t[8] = {0};
+    int kind = 1;
+    long long cnt = n;
+    strncpy(t, tag, 8);
+    fwrite(t, 1, 8, dump_fp);
+    fwrite(&kind, sizeof(int), 1, dump_fp);
+    fwrite(&cnt, sizeof(long long), 1, dump_fp);
+    fwrite(v, sizeof(int), (size_t) n, dump_fp);
+}
+
+static void put_state(const char *th, const char *tu, const char *tv, double *h, SVECT2D *vel, int n) {
+    double *u = (double *) malloc(sizeof(double) * n);
+    double *v = (double *) malloc(sizeof(double) * n);
+    int i;
+    for (i = 0; i < n; i++) { u[i] = vel[i].x; v[i] = vel[i].y; }
+    put_f64(th, h, n);
+    put_f64(tu, u, n);
+    put_f64(tv, v, n);
+    free(u);
+    free(v);
+}
+
+int __wrap_fe_main(SSUPER_MODEL *sm) {
+    int r;
+    dump_open();
+    r = __real_fe_main(sm);
+    attempts++;
+    if (r == YES && dump_fp != NULL) {
+        SMODEL *mod = &(sm->submodel[0]);
+        int n = mod->grid->nnodes;
+        double hdr[2];
+        int ihdr[3];
+        hdr[0] = mod->t_prev;
+        hdr[1] = sm->dt;
+        ihdr[0] = sm->solver_info.it_count_nonlin - it_mark;
+        ihdr[1] = attempts;
+        ihdr[2] = n;
+        put_f64("step", hdr, 2);
+        put_i32("stepi", ihdr, 3);
+        put_state("h", "u", "v", mod->sw->d2->head, mod->sw->d2->vel, n);
+        put_i32("wd", mod->grid->wd_flag, mod->grid->nelems2d);
+        fflush(dump_fp);
+        attempts = 0;
+        it_mark = sm->solver_info.it_count_nonlin;
+    }
+    return r;
+}
+
+void __wrap_fe_sw2_load(SSUPER_MODEL *sm, int imod) {
+    dump_open();
+    if (dump_fp != NULL && dump_loads_left > 0) {
+        SMODEL *mod = &(sm->submodel[imod]);
+        int n = mod->grid->nnodes;
+        double hdr[2];
+        hdr[0] = mod->t_prev;
+        hdr[1] = mod->dt;
+        put_f64("load", hdr, 2);
+        put_state("h", "u", "v", mod->sw->d2->head, mod->sw->d2->vel, n);
+        put_state("h1", "u1", "v1", mod->sw->d2->old_head, mod->sw->d2->old_vel, n);
+        put_state("h2", "u2", "v2", mod->sw->d2->older_head, mod->sw->d2->older_vel, n);
+        put_i32("wd", mod->grid->wd_flag, mod->grid->nelems2d);
+    }
+    __real_fe_sw2_load(sm, imod);
+    if (dump_fp != NULL && dump_loads_left > 0) {
+        SMODEL *mod = &(sm->submodel[imod]);
+        int n = mod->grid->nnodes, i, nnz = 0, k = 0;
+        put_f64("resid", sm->residual, 3 * n);
+        put_f64("diag", sm->diagonal, 9 * n);
+        int *rowsz = (int *) malloc(sizeof(int) * n);
+        for (i = 0; i < n; i++) { rowsz[i] = sm->matrix[i].size; nnz += rowsz[i]; }
+        int *cols = (int *) malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+        double *vals = (double *) malloc(sizeof(double) * 9 * (nnz > 0 ? nnz : 1));
+        for (i = 0; i < n; i++) {
+            memcpy(cols + k, sm->matrix[i].index, sizeof(int) * rowsz[i]);
+            memcpy(vals + 9 * k, sm->matrix[i].value, sizeof(double) * 9 * rowsz[i]);
+            k += rowsz[i];
+        }
+        put_i32("rowsz", rowsz, n);
+        put_i32("cols", cols, nnz);
+        put_f64("vals", vals, 9L * nnz);
+        free(rowsz);
+        free(cols);
+        free(vals);
+        fflush(dump_fp);
+        dump_loads_left--;
+    }
+}
