@@ -1,0 +1,495 @@
+// sw2_kernels.cuh -- assembly kernels of the SW2 Newton step (sm_100a).
+//
+// Assembly is atomic-free and deterministic: element kernels write their local
+// contributions to per-element slots (coalesced), and gather kernels sum each node
+// row / BCSR block over its contributing slots in the reference's element order
+// (all 2D elements ascending, then the boundary edges ascending), which is the
+// summation order of fe_sw2_resid / fe_global_matrix_assemble_sw2.
+#pragma once
+#include "sw2_physics.cuh"
+
+namespace sw2 {
+
+// Device view of one mesh instance (all arrays SoA, indices local to the instance).
+struct DevMesh {
+    int V, T, E, nnzb;
+    const double *x, *y, *z;
+    const int *en0, *en1, *en2, *emat;
+    const double *djac, *gx0, *gy0, *gx1, *gy1, *gx2, *gy2;
+    const unsigned char *efirst;      // bit i: element is the first 2D element holding its node i
+    const unsigned char *dflag;       // [V] Dirichlet flags (bit0 PRS_DIR, bit1 VEL_DIR, bit2 VEL_PRS_DIR)
+    const int *bn0, *bn1, *bkind, *bstr;
+    const double *bdjac, *bnx, *bny;
+    const MatParams *mats;
+    const double *str_value;          // [nstrings] step value of each edge string's series
+    const int *slot_ptr, *slot_idx;   // node -> residual slots in reference order
+    const int *blk_ptr, *blk_src;     // BCSR block -> element-block slots in reference order
+    const int *rowptr, *col, *blk_row, *dpos;
+    int qflag[3];                     // flags of global nodes 0..2 (fe_sw2_load.c:103 indexes by local id)
+};
+
+struct State {
+    double *h, *u, *v;          // current
+    const double *ho, *uo, *vo; // old
+    const double *hoo, *uoo, *voo;
+    const int *wd;
+};
+
+struct Norms {                  // get_residual_norms (src/fe/fe_newton.c:40-151)
+    double rmax, l2sum, imax;
+    int nan;
+    int pad;
+};
+
+__device__ __forceinline__ void load_elem(const DevMesh& m, const State& s, int e, int rule_vel, ElemIn& in, int* n,
+                                          int* df) {
+    n[0] = m.en0[e];
+    n[1] = m.en1[e];
+    n[2] = m.en2[e];
+    const unsigned first = rule_vel ? m.efirst[e] : 7u;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const int k = n[i];
+        in.x[i] = m.x[k];
+        in.y[i] = m.y[k];
+        in.z[i] = m.z[k];
+        in.h[i] = s.h[k];
+        in.ho[i] = s.ho[k];
+        in.hoo[i] = s.hoo[k];
+        // dry-node velocity zeroing is a side effect of fe_sw2_resid (:85-93): an element
+        // sees the stored velocity of an old-dry node only if no earlier element touched it
+        const bool zero = (in.ho[i] <= 0.) && !((first >> i) & 1u);
+        in.u[i] = zero ? 0.0 : s.u[k];
+        in.v[i] = zero ? 0.0 : s.v[k];
+        in.uo[i] = s.uo[k];
+        in.vo[i] = s.vo[k];
+        in.uoo[i] = s.uoo[k];
+        in.voo[i] = s.voo[k];
+        df[i] = m.dflag[k];
+    }
+    in.djac = m.djac[e];
+    in.gx[0] = m.gx0[e]; in.gy[0] = m.gy0[e];
+    in.gx[1] = m.gx1[e]; in.gy[1] = m.gy1[e];
+    in.gx[2] = m.gx2[e]; in.gy[2] = m.gy2[e];
+}
+
+// Residual contributions of every 2D element and boundary edge (fe_sw2_resid :51-191).
+// slots: 3 SoA arrays (c, x, y) of length 3T + 2E.
+__global__ void k_resid_elem(DevMesh m, State s, PhysParams P, double* __restrict__ sc, double* __restrict__ sx,
+                             double* __restrict__ sy) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nslot = 3 * m.T + 2 * m.E;
+    if (t < m.T) {
+        ElemIn in;
+        int n[3], df[3];
+        load_elem(m, s, t, 1, in, n, df);
+        double er[3][3];
+        sw2_elem_resid(in, s.wd[t], kPertNone, P, m.mats[m.emat[t]], df, er);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const bool dry = in.ho[i] <= 0.;
+            sc[3 * t + i] = er[i][0];
+            sx[3 * t + i] = dry ? 0.0 : er[i][1];
+            sy[3 * t + i] = dry ? 0.0 : er[i][2];
+        }
+    } else if (t < m.T + m.E) {
+        const int j = t - m.T;
+        EdgeIn in;
+        const int b[2] = {m.bn0[j], m.bn1[j]};
+        int df[2];
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const int k = b[i];
+            in.h[i] = s.h[k];
+            const bool dry = s.ho[k] <= 0.;
+            in.u[i] = dry ? 0.0 : s.u[k];
+            in.v[i] = dry ? 0.0 : s.v[k];
+            df[i] = m.dflag[k];
+        }
+        in.nx = m.bnx[j];
+        in.ny = m.bny[j];
+        in.djac = m.bdjac[j];
+        in.z0 = m.z[b[0]];
+        double er[2][3];
+        sw2_edge_resid(in, m.bkind[j], m.str_value[m.bstr[j]], kPertNone, P, df, er);
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const bool dry = s.ho[b[i]] <= 0.;
+            const int q = 3 * m.T + 2 * j + i;
+            sc[q] = er[i][0];
+            sx[q] = dry ? 0.0 : er[i][1];
+            sy[q] = dry ? 0.0 : er[i][2];
+        }
+    }
+    (void)nslot;
+}
+
+// Last-block-done reduction helper for per-block partials (fixed order -> deterministic).
+template <int NT>
+__device__ __forceinline__ void block_reduce3(double& a, double& b, double& c, int& d) {
+    __shared__ double sa[NT], sb[NT], s_c[NT];
+    __shared__ int sd[NT];
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    s_c[threadIdx.x] = c;
+    sd[threadIdx.x] = d;
+    __syncthreads();
+#pragma unroll
+    for (int w = NT / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sa[threadIdx.x] = fmax(sa[threadIdx.x], sa[threadIdx.x + w]);
+            sb[threadIdx.x] += sb[threadIdx.x + w];
+            s_c[threadIdx.x] = fmax(s_c[threadIdx.x], s_c[threadIdx.x + w]);
+            sd[threadIdx.x] += sd[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    a = sa[0];
+    b = sb[0];
+    c = s_c[0];
+    d = sd[0];
+    __syncthreads();
+}
+
+// Node gather: R = -(sum of slots in reference order) ([u, v, h] per node), the dry-node
+// velocity zeroing, and get_residual_norms fused (max |R| and max |sol| over nodes with
+// min(h, h_old) > 0, sum R^2 over all).  The last block to finish reduces the per-block
+// partials in block order and writes *out; `counter` returns to 0.
+constexpr int kGatherThreads = 256;
+__global__ void __launch_bounds__(kGatherThreads) k_resid_gather(DevMesh m, State s, const double* __restrict__ sc,
+                                                                 const double* __restrict__ sx,
+                                                                 const double* __restrict__ sy, double* __restrict__ R,
+                                                                 const double* __restrict__ sol, Norms* partial,
+                                                                 unsigned* counter, Norms* out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    double rmax = 0.0, l2 = 0.0, imax = 0.0;
+    int nan = 0;
+    if (n < m.V) {
+        double ax = 0.0, ay = 0.0, ac = 0.0;
+        for (int k = m.slot_ptr[n]; k < m.slot_ptr[n + 1]; k++) {
+            const int q = m.slot_idx[k];
+            ax += sx[q];
+            ay += sy[q];
+            ac += sc[q];
+        }
+        const double r0 = -ax, r1 = -ay, r2 = -ac;
+        R[3 * n] = r0;
+        R[3 * n + 1] = r1;
+        R[3 * n + 2] = r2;
+        const double ho = s.ho[n];
+        if (ho <= 0.) {
+            s.u[n] = 0.0;
+            s.v[n] = 0.0;
+        }
+        const bool inc = fmin(s.h[n], ho) > 0;
+        if (inc) {
+            rmax = fmax(fmax(fabs(r0), fabs(r1)), fabs(r2));
+            imax = fmax(fmax(fabs(sol[3 * n]), fabs(sol[3 * n + 1])), fabs(sol[3 * n + 2]));
+        }
+        l2 = r0 * r0 + r1 * r1 + r2 * r2;
+        nan = (isnan(r0) || isnan(r1) || isnan(r2)) ? 1 : 0;
+    }
+    block_reduce3<kGatherThreads>(rmax, l2, imax, nan);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = Norms{rmax, l2, imax, nan, 0};
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        double a = 0.0, b = 0.0, c = 0.0;
+        int d = 0;
+        for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+            a = fmax(a, __ldcg(&partial[k].rmax));
+            b += __ldcg(&partial[k].l2sum);
+            c = fmax(c, __ldcg(&partial[k].imax));
+            d += __ldcg(&partial[k].nan);
+        }
+        block_reduce3<kGatherThreads>(a, b, c, d);
+        if (threadIdx.x == 0) {
+            *out = Norms{a, b, c, d, 0};
+            *counter = 0u;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// FD Jacobian of the 2D elements (fe_sw2_load :85-142, perturb_sw2_head / perturb_sw2_vel).
+// One CTA = kJacElems elements x 9 perturbation columns (node b, variable u/v/h); warp w
+// evaluates column w for 32 elements, so the pressure-term branch is warp-uniform.
+// Element data are staged in shared memory once; the 9x9 element matrices are staged
+// in shared memory and written out as contiguous 81-double records (slot 9e + 3a + b).
+constexpr int kJacElems = 32;
+constexpr int kJacThreads = kJacElems * 9;
+
+struct __align__(16) StagedElem {
+    ElemIn in;
+    int n[3], df[3], wd, mat;
+};
+
+__global__ void __launch_bounds__(kJacThreads) k_jac_elem(DevMesh m, State s, PhysParams P,
+                                                           double* __restrict__ jslots) {
+    __shared__ StagedElem se[kJacElems];
+    __shared__ double out[kJacElems * 81];
+    const int e0 = blockIdx.x * kJacElems;
+    const int lane = threadIdx.x % kJacElems;
+    const int item = threadIdx.x / kJacElems;
+    if (item == 0) {
+        const int e = e0 + lane;
+        if (e < m.T) {
+            StagedElem& S = se[lane];
+            load_elem(m, s, e, 0, S.in, S.n, S.df);
+            S.wd = s.wd[e];
+            S.mat = m.emat[e];
+        }
+    }
+    __syncthreads();
+    const int e = e0 + lane;
+    if (e < m.T) {
+        const StagedElem& S = se[lane];
+        const int b = item / 3, var = item % 3;  // var: 0 = u, 1 = v, 2 = h
+        ElemIn in = S.in;
+        const MatParams M = m.mats[S.mat];
+        const double cur = (var == 0) ? in.u[b] : (var == 1) ? in.v[b] : in.h[b];
+        const double eps = fd_eps(cur);
+        const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
+        double rp[3][3], rm[3][3];
+        if (var == 0) in.u[b] = cur + eps; else if (var == 1) in.v[b] = cur + eps; else in.h[b] = cur + eps;
+        sw2_elem_resid(in, S.wd, pv, P, M, S.df, rp);
+        if (var == 0) in.u[b] = cur - eps; else if (var == 1) in.v[b] = cur - eps; else in.h[b] = cur - eps;
+        sw2_elem_resid(in, S.wd, pv, P, M, S.df, rm);
+        const double e2 = 2.0 * eps;
+        // Dirichlet zeroing of the element matrix (fe_assign_mom_db_dof3 / fe_assign_dacont_db_dof3):
+        // D = momentum-Dirichlet nodes (old-dry or VEL/VEL_PRS string), P = continuity-Dirichlet.
+        unsigned Dm = 0, Pm = 0;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const int f = m.qflag[i];
+            if (S.in.ho[i] <= 0.) Dm |= 1u << i;
+            if (f & 1) Pm |= 1u << i;
+            if (f & 2) Dm |= 1u << i;
+            if (f & 4) { Dm |= 1u << i; Pm |= 1u << i; }
+        }
+        double* o = out + lane * 81;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+#pragma unroll
+            for (int eq = 0; eq < 3; eq++) {
+                double val = (rp[a][eq] - rm[a][eq]) / e2;
+                const int row = (eq == 0) ? 2 : eq - 1;  // block rows: x-mom, y-mom, continuity
+                const bool aD = (Dm >> a) & 1u, bD = (Dm >> b) & 1u, aP = (Pm >> a) & 1u, bP = (Pm >> b) & 1u;
+                const bool zero = (aD && row < 2) || (bD && var < 2) || (aP && row == 2) || (bP && var == 2);
+                const bool one = (a == b) && ((aD && ((var == 0 && row == 0) || (var == 1 && row == 1))) ||
+                                              (aP && var == 2 && row == 2));
+                if (one) val = 1.0;
+                else if (zero) val = 0.0;
+                o[(3 * a + b) * 9 + 3 * row + var] = val;
+            }
+        }
+    }
+    __syncthreads();
+    const int nel = min(kJacElems, m.T - e0);
+    double* dst = jslots + (size_t)e0 * 81;
+    for (int k = threadIdx.x; k < nel * 81; k += blockDim.x) dst[k] = out[k];
+}
+
+// FD Jacobian of the boundary edges: one thread per (edge, node, variable); writes the
+// four 3x3 blocks of edge j at slots 9T + 4j + 2a + b.
+__global__ void k_jac_edge(DevMesh m, State s, PhysParams P, double* __restrict__ jslots) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 6 * m.E) return;
+    const int j = t / 6, b = (t % 6) / 3, var = t % 3;
+    EdgeIn in;
+    const int nd[2] = {m.bn0[j], m.bn1[j]};
+    int df[2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        in.h[i] = s.h[nd[i]];
+        in.u[i] = s.u[nd[i]];
+        in.v[i] = s.v[nd[i]];
+        df[i] = m.dflag[nd[i]];
+    }
+    in.nx = m.bnx[j];
+    in.ny = m.bny[j];
+    in.djac = m.bdjac[j];
+    in.z0 = m.z[nd[0]];
+    const int kind = m.bkind[j];
+    const double value = m.str_value[m.bstr[j]];
+    const double cur = (var == 0) ? in.u[b] : (var == 1) ? in.v[b] : in.h[b];
+    const double eps = fd_eps(cur);
+    const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
+    double rp[2][3], rm[2][3];
+    EdgeIn ip = in, im = in;
+    if (var == 0) { ip.u[b] = cur + eps; im.u[b] = cur - eps; }
+    else if (var == 1) { ip.v[b] = cur + eps; im.v[b] = cur - eps; }
+    else { ip.h[b] = cur + eps; im.h[b] = cur - eps; }
+    sw2_edge_resid(ip, kind, value, pv, P, df, rp);
+    sw2_edge_resid(im, kind, value, pv, P, df, rm);
+    const double e2 = 2.0 * eps;
+    unsigned Dm = 0, Pm = 0;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const int f = m.qflag[i];
+        if (s.ho[nd[i]] <= 0.) Dm |= 1u << i;
+        if (f & 1) Pm |= 1u << i;
+        if (f & 2) Dm |= 1u << i;
+        if (f & 4) { Dm |= 1u << i; Pm |= 1u << i; }
+    }
+    double* o = jslots + ((size_t)9 * m.T + 4 * j) * 9;
+#pragma unroll
+    for (int a = 0; a < 2; a++) {
+#pragma unroll
+        for (int eq = 0; eq < 3; eq++) {
+            double val = (rp[a][eq] - rm[a][eq]) / e2;
+            const int row = (eq == 0) ? 2 : eq - 1;
+            const bool aD = (Dm >> a) & 1u, bD = (Dm >> b) & 1u, aP = (Pm >> a) & 1u, bP = (Pm >> b) & 1u;
+            const bool zero = (aD && row < 2) || (bD && var < 2) || (aP && row == 2) || (bP && var == 2);
+            const bool one = (a == b) && ((aD && ((var == 0 && row == 0) || (var == 1 && row == 1))) ||
+                                          (aP && var == 2 && row == 2));
+            if (one) val = 1.0;
+            else if (zero) val = 0.0;
+            o[(2 * a + b) * 9 + 3 * row + var] = val;
+        }
+    }
+}
+
+// BCSR values: thread (block k, entry q) sums entry q of every contributing element
+// block in reference order (fe_global_matrix_assemble_sw2 :166-224).
+__global__ void k_jac_gather(DevMesh m, const double* __restrict__ jslots, double* __restrict__ val) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)m.nnzb * 9) return;
+    const int k = (int)(t / 9), q = (int)(t % 9);
+    double acc = 0.0;
+    for (int c = m.blk_ptr[k]; c < m.blk_ptr[k + 1]; c++) acc += jslots[(size_t)m.blk_src[c] * 9 + q];
+    val[t] = acc;
+}
+
+// Tiny-diagonal fix of fe_sw2_load (:218-236) and the Jacobi scale vector of spv_jacobi
+// (src/solver/spv_jacobi.c:222-285): S = 1/sqrt(max |row entry|), floored.  Also writes
+// the scaled right-hand side b = S R.
+__global__ void k_rowscale(DevMesh m, const State s, double* __restrict__ val, double* __restrict__ R,
+                           double* __restrict__ S, double* __restrict__ b, int fix_only) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m.V) return;
+    double* d = val + (size_t)m.dpos[n] * 9;
+    if (fabs(d[0]) < kNotQuiteSmall) {
+        d[0] = kNotQuiteSmall;
+        if (fabs(R[3 * n]) < kNotQuiteSmall) R[3 * n] = -kNotQuiteSmall * s.u[n];
+    }
+    if (fabs(d[4]) < kNotQuiteSmall) {
+        d[4] = kNotQuiteSmall;
+        if (fabs(R[3 * n + 1]) < kNotQuiteSmall) R[3 * n + 1] = -kNotQuiteSmall * s.v[n];
+    }
+    if (fabs(d[8]) < kNotQuiteSmall) d[8] = kNotQuiteSmall;
+    if (fix_only) return;
+    double mx[3] = {0.0, 0.0, 0.0};
+    for (int k = m.rowptr[n]; k < m.rowptr[n + 1]; k++) {
+        const double* a = val + (size_t)k * 9;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) mx[r] = fmax(mx[r], fabs(a[3 * r + c]));
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const double sv = (mx[r] < kSmall) ? 1.0 / sqrt(kSmall) : 1.0 / sqrt(fabs(mx[r]));
+        S[3 * n + r] = sv;
+        b[3 * n + r] = R[3 * n + r] * sv;
+    }
+}
+
+// A' = S A S (in place for FP64, converted copy for the mixed path) and the inverse of
+// every scaled 3x3 diagonal block for the block-Jacobi preconditioner.
+template <typename MT>
+__global__ void k_scale_matrix(DevMesh m, double* __restrict__ val, MT* __restrict__ mval, const double* __restrict__ S,
+                               MT* __restrict__ dinv, int* __restrict__ singular) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m.nnzb) return;
+    const int i = m.blk_row[k], j = m.col[k];
+    double a[9];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) a[3 * r + c] = val[(size_t)k * 9 + 3 * r + c] * (S[3 * i + r] * S[3 * j + c]);
+    if (sizeof(MT) == sizeof(double)) {
+#pragma unroll
+        for (int q = 0; q < 9; q++) val[(size_t)k * 9 + q] = a[q];
+    } else {
+#pragma unroll
+        for (int q = 0; q < 9; q++) mval[(size_t)k * 9 + q] = (MT)a[q];
+    }
+    if (i == j) {
+        const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+        const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+        if (det == 0.0 || !isfinite(det)) {
+            atomicExch(singular, 1);
+#pragma unroll
+            for (int q = 0; q < 9; q++) dinv[(size_t)i * 9 + q] = (MT)((q % 4 == 0) ? 1.0 : 0.0);
+            return;
+        }
+        const double id = 1.0 / det;
+        double inv[9];
+        inv[0] = c00 * id;
+        inv[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+        inv[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+        inv[3] = c01 * id;
+        inv[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+        inv[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+        inv[6] = c02 * id;
+        inv[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+        inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+#pragma unroll
+        for (int q = 0; q < 9; q++) dinv[(size_t)i * 9 + q] = (MT)inv[q];
+    }
+}
+
+// line search halving (fe_newton.c:692-747): sol *= 0.5; state += sol (fe_sw2_inc)
+__global__ void k_half_inc(int V, double* __restrict__ sol, double* __restrict__ h, double* __restrict__ u,
+                           double* __restrict__ v) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= V) return;
+    const double a = sol[3 * n] * 0.5, b = sol[3 * n + 1] * 0.5, c = sol[3 * n + 2] * 0.5;
+    sol[3 * n] = a;
+    sol[3 * n + 1] = b;
+    sol[3 * n + 2] = c;
+    u[n] += a;
+    v[n] += b;
+    h[n] += c;
+}
+
+// fe_sw2_wdflag (src/fe/sw2/fe_sw2_wdflag.c:24-75), two passes
+__global__ void k_wd_mark(int T, const int* __restrict__ en0, const int* __restrict__ en1,
+                          const int* __restrict__ en2, const double* __restrict__ h, unsigned char* __restrict__ mark) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= T) return;
+    const int a = en0[e], b = en1[e], c = en2[e];
+    if (!(h[a] > 0.0 && h[b] > 0.0 && h[c] > 0.0)) {
+        mark[a] = 1;
+        mark[b] = 1;
+        mark[c] = 1;
+    }
+}
+__global__ void k_wd_flag(int T, const int* __restrict__ en0, const int* __restrict__ en1,
+                          const int* __restrict__ en2, const double* __restrict__ h, const double* __restrict__ ho,
+                          const unsigned char* __restrict__ mark, int* __restrict__ wd) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= T) return;
+    const int a = en0[e], b = en1[e], c = en2[e];
+    int f = (mark[a] | mark[b] | mark[c]) ? 1 : 0;
+    if (h[a] < 0 && h[b] < 0 && h[c] < 0 && ho[a] < 0 && ho[b] < 0 && ho[c] < 0) f = 2;
+    wd[e] = f;
+}
+
+// Dirichlet node values of fe_sw2_init (src/fe/sw2/fe_sw2_init.c:37-85)
+__global__ void k_dirichlet(int n, const int* __restrict__ node, const int* __restrict__ mask,
+                            const double* __restrict__ hv, const double* __restrict__ uv, const double* __restrict__ vv,
+                            double* __restrict__ h, double* __restrict__ u, double* __restrict__ v) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int k = node[t], f = mask[t];
+    if (f & 2) { u[k] = uv[t]; v[k] = vv[t]; }
+    if (f & 1) h[k] = hv[t];
+}
+
+}  // namespace sw2

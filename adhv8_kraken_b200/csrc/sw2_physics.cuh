@@ -1,0 +1,681 @@
+// sw2_physics.cuh -- device-side SW2 element physics for sm_100a.
+//
+// One call of sw2_elem_resid() evaluates the 2D shallow-water element residual of
+// AdH's fe_sw2_body_resid (src/fe/sw2/fe_sw2_body_resid.c:45-1267) for a linear
+// triangle, in primitive variables (h, u, v), including the wet/dry clipping of
+// fe_sw2_wet_dry_wrapper (src/fe/fe_sw2_wet_dry_wrapper.c:106-306).  The result is
+// er[node][eq] with eq 0 = continuity (c_eq), 1 = x-momentum, 2 = y-momentum.
+//
+// GPU structure (not the reference's): the clipping geometry of the current depth
+// is computed once per call and reused by every wet/dry-wrapped integrand (the
+// reference re-clips for each of the ~8 wrapper calls); all loops over the three
+// vertices are unrolled so the element lives in registers.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace sw2 {
+
+constexpr double kSmall = 2.220446049250313e-16;        // DBL_EPSILON (define.h:27)
+constexpr double kNotQuiteSmall = 1.1920928955078125e-07;  // FLT_EPSILON (define.h:28)
+constexpr double kOne3 = 0.333333333333333333333333;
+constexpr double kOne6 = 0.166666666666666666666667;
+constexpr double kOne12 = 0.083333333333333333333333;
+constexpr double kOne30 = 0.033333333333333333333333;
+constexpr double kOne60 = 0.016666666666666666666667;
+
+enum PerturbVar { kPertNone = -1, kPertU = 1, kPertV = 2, kPertH = 5 };
+
+// Model constants of one instance (kernel parameter).
+struct PhysParams {
+    double g, dll, dul, alpha, tau_pg, dt;
+};
+
+// Per-material constants, precomputed on the host (sin() of the Coriolis latitude,
+// EVS sums, the Manning roughness height) plus the step's water-source value.
+struct MatParams {
+    double ks;          // fterms.eqrheight (<= kSmall: no drag)
+    double ev_st, ev_tr;// EVS: |xx - yy|, min(xx, yy) incl. molecular viscosity
+    double eev_coef;
+    double cor_speed;   // sin(lat) * 2 * EARTH_ROTAT
+    double water_src;   // step-averaged source value when the string is BCT_WATER_SOURCE
+    int eev_mode;       // 0 = EVS
+    int has_source;
+};
+
+struct ElemIn {
+    double x[3], y[3], z[3];
+    double h[3], u[3], v[3];        // current iterate (perturbation applied)
+    double ho[3], uo[3], vo[3];     // old time level
+    double hoo[3], uoo[3], voo[3];  // older time level
+    double djac, gx[3], gy[3];
+};
+
+// ---------------------------------------------------------------------------------
+// wet/dry clipping of one depth array (the geometric part of fe_sw2_wet_dry_wrapper)
+struct Clip {
+    int total, only, degenerate;
+    double factor;      // (total >> 1) - (total % 2)
+    double ret;         // value the wrapper returns
+    double ndjac;
+    double nx[3], ny[3], nh[3], xsi[3];
+};
+
+__device__ __forceinline__ void make_clip(const double* x, const double* y, const double* h, double djac, Clip& c) {
+    int total = 0, pass = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        int dry = (h[i] <= 0.0) ? 1 : 0;
+        total += dry;
+        pass += dry << i;
+    }
+    c.total = total;
+    c.degenerate = 0;
+    c.only = 0;
+    c.factor = 0.0;
+    c.ndjac = djac;
+    if (total == 3) { c.ret = 0.0; return; }
+    if (total == 0) { c.ret = 1.0; return; }
+    if (total != 1) pass = 7 - pass;
+    int only = pass / 2;
+    c.only = only;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        if (i != only) {
+            double xsi = h[i] / (h[i] - h[only]);
+            c.xsi[i] = xsi;
+            c.nx[i] = x[i] + xsi * (x[only] - x[i]);
+            c.ny[i] = y[i] + xsi * (y[only] - y[i]);
+            c.nh[i] = 0.0;
+        } else {
+            c.xsi[i] = 0.0;
+            c.nx[i] = x[i];
+            c.ny[i] = y[i];
+            c.nh[i] = h[i];
+        }
+    }
+    double nd = ((c.nx[1] - c.nx[0]) * (c.ny[2] - c.ny[0]) - (c.ny[1] - c.ny[0]) * (c.nx[2] - c.nx[0])) / 2.0;
+    c.ndjac = nd;
+    if (nd / djac < kSmall) {
+        c.degenerate = 1;
+        c.ret = (double)(total % 2);
+        return;
+    }
+    double f = (double)((total >> 1) - (total % 2));
+    c.factor = f;
+    double fr = f * (nd / djac);
+    c.ret = fr + ((fr < 0) ? 1.0 : 0.0);
+}
+
+// return value of the wrapper / fe_sw2_wet_dry_factor for a depth array
+__device__ __forceinline__ double clip_factor(const double* x, const double* y, const double* h, double djac) {
+    Clip c;
+    make_clip(x, y, h, djac, c);
+    return c.ret;
+}
+
+// Wraps an integrand the way fe_sw2_wet_dry_wrapper does: full element, and/or the
+// clipped corner scaled by the signed factor, optionally redistributed (RE_DISTRIBUTE).
+// The integrand functor is called as f(x, y, h, gx, gy, djac, vinterp, rhs[3][3]) where
+// vinterp(i, w, v) returns the clipped value of a vertex quantity.
+template <class F>
+__device__ __forceinline__ void wd_apply(const Clip& c, const double* x, const double* y, const double* h,
+                                         const double* gx, const double* gy, double djac, int redistribute,
+                                         double (&rhs)[3][3], F&& f) {
+    if (c.total == 3) return;
+    if (c.total == 0 || c.total == 1) {
+        f(x, y, h, gx, gy, djac, false, c, rhs);
+        if (c.total == 0) return;
+    }
+    if (c.degenerate) return;
+    double ngx[3], ngy[3];
+    double nd = c.ndjac;
+    ngx[0] = 0.5 * (c.ny[1] - c.ny[2]) / nd;
+    ngx[1] = 0.5 * (c.ny[2] - c.ny[0]) / nd;
+    ngx[2] = 0.5 * (c.ny[0] - c.ny[1]) / nd;
+    ngy[0] = 0.5 * (c.nx[2] - c.nx[1]) / nd;
+    ngy[1] = 0.5 * (c.nx[0] - c.nx[2]) / nd;
+    ngy[2] = 0.5 * (c.nx[1] - c.nx[0]) / nd;
+    double nr[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    f(c.nx, c.ny, c.nh, ngx, ngy, nd, true, c, nr);
+    if (redistribute) {
+        const int o = c.only;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            if (i == o) continue;
+            double ax = c.nx[i] - x[o], ay = c.ny[i] - y[o];
+            double bx = x[i] - x[o], by = y[i] - y[o];
+            double xs = sqrt((ax * ax + ay * ay) / (bx * bx + by * by));
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                nr[o][q] += (1.0 - xs) * nr[i][q];
+                nr[i][q] *= xs;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int q = 0; q < 3; q++) rhs[i][q] += c.factor * nr[i][q];
+}
+
+// clipped value of a vertex quantity (FIXED_POS with the clip weights)
+__device__ __forceinline__ double cval(const Clip& c, bool clipped, const double* f, int i) {
+    if (!clipped || i == c.only) return f[i];
+    return f[i] + c.xsi[i] * (f[c.only] - f[i]);
+}
+
+// wetted-area averages (fe_sw2_wd_average, src/fe/sw2/fe_sw2_wet_dry_integrations.c:19-39):
+// returns the wrapper factor and writes the averaged depth and velocity.
+__device__ __forceinline__ double wd_average(const Clip& c, const double* x, const double* y, const double* h,
+                                             const double* u, const double* v, double djac, double& havg,
+                                             double& uavg, double& vavg) {
+    double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    auto integ = [&](const double* X, const double* Y, const double* H, const double*, const double*, double dj,
+                     bool clipped, const Clip& cc, double (&r)[3][3]) {
+        double t1 = (H[0] + H[1] + H[2]) / 3.0;
+        double t2 = (cval(cc, clipped, u, 0) + cval(cc, clipped, u, 1) + cval(cc, clipped, u, 2)) / 3.0;
+        double t3 = (cval(cc, clipped, v, 0) + cval(cc, clipped, v, 1) + cval(cc, clipped, v, 2)) / 3.0;
+        r[0][0] += dj * t1;
+        r[0][1] += dj * t2;
+        r[0][2] += dj * t3;
+    };
+    wd_apply(c, x, y, h, nullptr, nullptr, djac, 0, acc, integ);
+    double f = c.ret;
+    havg = 0.0;
+    uavg = 0.0;
+    vavg = 0.0;
+    if (f > 0.0) {
+        double wet = djac * f;
+        havg = acc[0][0] / wet;
+        uavg = acc[0][1] / wet;
+        vavg = acc[0][2] / wet;
+    }
+    return f;
+}
+
+__device__ __forceinline__ double drag_coef(double depth, double ks) {  // fr_bedshstr_drag_coef.c:18-40
+    depth = fmax(depth, 1.E-8);
+    ks = fmax(ks, 1.E-8);
+    double rh = (ks > 29.7 * depth) ? 1. / 29.7 : depth / ks;
+    double bta = 29.7 * rh;
+    double t = (.4 * bta) / ((bta + 1) * (log(bta + 1) - 1) + 1);
+    return 2. * (t * t);
+}
+
+// ---------------------------------------------------------------------------------
+// the element residual
+//   wd_flag:  element wet/dry flag of the Newton solve (fe_sw2_wdflag)
+//   pvar:     kPertNone / kPertU / kPertV / kPertH (u, v perturbations drop the pressure terms)
+//   dflag[3]: Dirichlet flags of the element's nodes (bit0 PRS_DIR, bit1 VEL_DIR, bit2 VEL_PRS_DIR)
+__device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, int pvar, const PhysParams& P,
+                                               const MatParams& M, const int* dflag, double (&er)[3][3]) {
+    const double djac = in.djac, dt = P.dt, g = P.g, dll = P.dll, dul = P.dul;
+    const double* gx = in.gx;
+    const double* gy = in.gy;
+    const bool pressure = !(pvar == kPertU || pvar == kPertV);
+
+    // averages and gradients (:193-221)
+    double u_avg = (in.u[0] + in.u[1] + in.u[2]) / 3.0;
+    double v_avg = (in.v[0] + in.v[1] + in.v[2]) / 3.0;
+    double gzx = 0, gzy = 0, ghx = 0, ghy = 0, gux = 0, guy = 0, gvx = 0, gvy = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        gzx += in.z[i] * gx[i];
+        gzy += in.z[i] * gy[i];
+        ghx += in.h[i] * gx[i];
+        ghy += in.h[i] * gy[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        gux += in.u[i] * gx[i];
+        guy += in.u[i] * gy[i];
+        gvx += in.v[i] * gx[i];
+        gvy += in.v[i] * gy[i];
+    }
+    const double gwx = gzx + ghx, gwy = gzy + ghy;
+    const double vmag = sqrt(u_avg * u_avg + v_avg * v_avg);
+    const double vst_i = u_avg / fmax(vmag, 1.E-8), vst_j = v_avg / fmax(vmag, 1.E-8);
+
+    Clip ch;  // clipping of the current depth, shared by all wrapped integrands
+    make_clip(in.x, in.y, in.h, djac, ch);
+    double h_wd, u_wd, v_wd;
+    wd_average(ch, in.x, in.y, in.h, in.u, in.v, djac, h_wd, u_wd, v_wd);
+    double factor = ch.ret;
+    const double factor_old = clip_factor(in.x, in.y, in.ho, djac);
+    const double factor_older = clip_factor(in.x, in.y, in.hoo, djac);
+    const double vwd_mag = sqrt(u_wd * u_wd + v_wd * v_wd);
+    const double h_fric = fmax(h_wd, kSmall);
+    const double rough = (M.ks > kSmall) ? drag_coef(h_fric, M.ks) : 0.0;
+
+    // eddy viscosity (:263-291, fe_sw2_get_EEVF.c:33-60)
+    double ev_st, ev_tr;
+    if (M.eev_mode == 0) {
+        ev_st = M.ev_st;
+        ev_tr = M.ev_tr;
+    } else {
+        const double vmin = 0.1 * sqrt(g * dll);
+        double evmin;
+        const double coef = M.eev_coef;
+        if (M.eev_mode == 1) {
+            ev_st = 0.0;
+            ev_tr = coef * 2.0 * h_fric * sqrt(rough) * vmag;
+            evmin = (coef / 0.5) * vmin * sqrt(djac) / 40.;
+        } else if (M.eev_mode == 2) {
+            ev_st = 1.3 * h_fric * sqrt(rough) * vmag;
+            ev_tr = coef * 0.92 * h_fric * sqrt(rough) * vmag;
+            evmin = (coef / 0.5) * vmin * sqrt(djac) / 40.;
+        } else {
+            ev_st = 0.;
+            ev_tr = coef * coef * djac * sqrt(gux * gux + gvy * gvy + 0.5 * (guy + gvx) * (guy + gvx));
+            evmin = (coef / 0.2) * vmin * sqrt(djac) / 40.;
+        }
+        ev_tr = fmax(ev_tr, evmin);
+        if (wd_flag == 1 || wd_flag == 2) {
+            ev_st = 0.0;
+            ev_tr = fmax(ev_tr, 5. * evmin);
+        }
+    }
+
+#pragma unroll
+    for (int i = 0; i < 3; i++) er[i][0] = er[i][1] = er[i][2] = 0.0;
+
+    // shock capturing, partially/fully dry elements (:357-400)
+    if (wd_flag == 1 || wd_flag == 2) {
+        const double gum = sqrt(gux * gux + guy * guy + kSmall);
+        const double gvm = sqrt(gvx * gvx + gvy * gvy + kSmall);
+        const double cu = 0.5 * dul * djac * gum, cv = 0.5 * dul * djac * gvm;
+        const double unx = gux / gum, uny = guy / gum, vnx = gvx / gvm, vny = gvy / gvm;
+        const double nx = unx * gux + uny * guy, ny = vnx * gvx + vny * gvy;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            er[i][0] += dt * 0.5 * g * djac * ((dll * gwx) * gx[i] + (dll * gwy) * gy[i]);
+            er[i][1] += cu * dt * djac * nx * (unx * gx[i] + uny * gy[i]);
+            er[i][2] += cv * dt * djac * ny * (vnx * gx[i] + vny * gy[i]);
+        }
+    }
+
+    // advection, wet/dry wrapped with redistribution (:434-457, fe_sw2_wd_convection_triangle)
+    {
+        double rhs[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        const double cc = -dt;
+        auto integ = [&](const double*, const double*, const double* H, const double* GX, const double* GY,
+                         double dj, bool clipped, const Clip& c, double (&r)[3][3]) {
+            double uu[3], vv[3];
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                uu[i] = cval(c, clipped, in.u, i);
+                vv[i] = cval(c, clipped, in.v, i);
+            }
+            // integrate_triangle_gradPhi_dot_f_v
+            double p1 = 2 * H[0] + H[1] + H[2], p2 = H[0] + 2 * H[1] + H[2], p3 = H[0] + H[1] + 2 * H[2];
+            double tx = p1 * uu[0] + p2 * uu[1] + p3 * uu[2];
+            double ty = p1 * vv[0] + p2 * vv[1] + p3 * vv[2];
+            double con = dj * kOne12 * cc;
+            // integrate_triangle_dphi_f_g_h(f = u, g = v, h): x-derivative -> y-momentum
+            double ff1 = 3 * uu[0] + uu[1] + uu[2], ff2 = 2 * uu[0] + 2 * uu[1] + uu[2], ff3 = 2 * uu[0] + uu[1] + 2 * uu[2];
+            double ff4 = uu[0] + 3 * uu[1] + uu[2], ff5 = uu[0] + 2 * uu[1] + 2 * uu[2], ff6 = uu[0] + uu[1] + 3 * uu[2];
+            double gg1 = 2 * ff1 * vv[0] + ff2 * vv[1] + ff3 * vv[2];
+            double gg2 = ff2 * vv[0] + 2 * ff4 * vv[1] + ff5 * vv[2];
+            double gg3 = ff3 * vv[0] + ff5 * vv[1] + 2 * ff6 * vv[2];
+            double cuv = dj * kOne60 * cc * (gg1 * H[0] + gg2 * H[1] + gg3 * H[2]);
+            // integrate_triangle_dphi_f_f_h for u (x) and v (y)
+            double a0 = uu[0] * uu[0], a1 = uu[1] * uu[1], a2 = uu[2] * uu[2];
+            double q1 = 3 * a0 + 2 * uu[0] * uu[1] + a1 + (2 * uu[0] + uu[1]) * uu[2] + a2;
+            double q2 = a0 + 2 * uu[0] * uu[1] + 3 * a1 + (uu[0] + 2 * uu[1]) * uu[2] + a2;
+            double q3 = a0 + uu[0] * uu[1] + a1 + 2 * (uu[0] + uu[1]) * uu[2] + 3 * a2;
+            double cuu = dj * kOne30 * cc * (q1 * H[0] + q2 * H[1] + q3 * H[2]);
+            double b0 = vv[0] * vv[0], b1 = vv[1] * vv[1], b2 = vv[2] * vv[2];
+            double s1 = 3 * b0 + 2 * vv[0] * vv[1] + b1 + (2 * vv[0] + vv[1]) * vv[2] + b2;
+            double s2 = b0 + 2 * vv[0] * vv[1] + 3 * b1 + (vv[0] + 2 * vv[1]) * vv[2] + b2;
+            double s3 = b0 + vv[0] * vv[1] + b1 + 2 * (vv[0] + vv[1]) * vv[2] + 3 * b2;
+            double cvv = dj * kOne30 * cc * (s1 * H[0] + s2 * H[1] + s3 * H[2]);
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                r[i][0] += con * (GX[i] * tx + GY[i] * ty);
+                double rx = cuv * GY[i];
+                double ry = cuv * GX[i];
+                rx += cuu * GX[i];
+                ry += cvv * GY[i];
+                r[i][1] += rx;
+                r[i][2] += ry;
+            }
+        };
+        wd_apply(ch, in.x, in.y, in.h, gx, gy, djac, 1, rhs, integ);
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) er[i][q] += rhs[i][q];
+    }
+
+    // temporal terms t(n+1), t(n), t(n-1) (:481-490, fe_sw2_temporal :1288-1354)
+    {
+        auto temporal = [&](const Clip& c, const double* H, const double* U, const double* V, double wdf,
+                            double dtf, int flag) {
+            double rhs[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            auto integ = [&](const double*, const double*, const double* Hc, const double*, const double*, double dj,
+                             bool, const Clip&, double (&r)[3][3]) {
+                double fs = Hc[0] + Hc[1] + Hc[2], t1 = dj * dtf * kOne12;
+#pragma unroll
+                for (int i = 0; i < 3; i++) r[i][0] += t1 * (fs + Hc[i]);
+            };
+            wd_apply(c, in.x, in.y, H, nullptr, nullptr, djac, 1, rhs, integ);
+            const double con = dtf * wdf;
+            const double t1 = djac * con * kOne3;
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                if (flag != 2) er[i][0] += rhs[i][0];
+                er[i][1] += t1 * (U[i] * fmax(H[i], dll));
+                er[i][2] += t1 * (V[i] * fmax(H[i], dll));
+            }
+        };
+        temporal(ch, in.h, in.u, in.v, factor, 1. + P.alpha / 2., -3);
+        Clip co;
+        make_clip(in.x, in.y, in.ho, djac, co);
+        temporal(co, in.ho, in.uo, in.vo, factor_old, (-1.) * (1. + P.alpha), wd_flag);
+        if (P.alpha != 0.0) {  // the t(n-1) term has weight alpha / 2
+            Clip coo;
+            make_clip(in.x, in.y, in.hoo, djac, coo);
+            temporal(coo, in.hoo, in.uoo, in.voo, factor_older, P.alpha / 2., wd_flag);
+        }
+    }
+
+    // diffusion (:504-534)
+    {
+        const double tmp = (h_wd < dul) ? dul : h_wd;
+        const double fxx = 2. * ev_st * vst_i * (vst_i * gux + vst_j * guy) + 2. * ev_tr * gux;
+        const double fxy = ev_st * vst_j * (vst_j * guy + vst_i * gux + vst_i * gvx + vst_j * gvy) + ev_tr * (guy + gvx);
+        const double fyx = ev_st * vst_i * (vst_j * guy + vst_i * gux + vst_i * gvx + vst_j * gvy) + ev_tr * (guy + gvx);
+        const double fyy = 2. * ev_st * vst_j * (vst_j * gvy + vst_i * gvx) + 2. * ev_tr * gvy;
+        const double t1 = tmp * djac, t2 = dt * factor;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            er[i][1] += t2 * (t1 * (fxx * gx[i] + fxy * gy[i]));
+            er[i][2] += t2 * (t1 * (fyx * gx[i] + fyy * gy[i]));
+        }
+    }
+
+    // bottom friction (:557-577)
+    const double resistance = rough / (2.0 * g);
+    {
+        double fx[3], fy[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            double m = sqrt(in.u[i] * in.u[i] + in.v[i] * in.v[i]);
+            fx[i] = in.u[i] * m;
+            fy[i] = in.v[i] * m;
+        }
+        const double t1 = djac * (dt * g * resistance * factor) * kOne12;
+        const double sx = fx[0] + fx[1] + fx[2], sy = fy[0] + fy[1] + fy[2];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            er[i][1] += t1 * (sx + fx[i]);
+            er[i][2] += t1 * (sy + fy[i]);
+        }
+    }
+    const double bedx = resistance * u_wd * vwd_mag, bedy = resistance * v_wd * vwd_mag;
+
+    // Coriolis (:639-652)
+    const double cs = M.cor_speed;
+    if (cs != 0.0) {
+        const double t1 = dt * factor * cs;
+        auto phifg = [&](double c, const double* f, const double* gg, int q) {
+            double gs = 2 * (gg[0] + gg[1] + gg[2]), tt = c * djac * kOne60;
+            er[0][q] += tt * (f[0] * (gs + 4 * gg[0]) + f[1] * (gs - gg[2]) + f[2] * (gs - gg[1]));
+            er[1][q] += tt * (f[1] * (gs + 4 * gg[1]) + f[2] * (gs - gg[0]) + f[0] * (gs - gg[2]));
+            er[2][q] += tt * (f[2] * (gs + 4 * gg[2]) + f[1] * (gs - gg[0]) + f[0] * (gs - gg[1]));
+        };
+        phifg(-t1, in.h, in.v, 1);
+        phifg(+t1, in.h, in.u, 2);
+    }
+
+    // rainfall / water source (:728-754)
+    const double water_source = M.has_source ? M.water_src : 0.0;
+    if (M.has_source) {
+        const double rc = water_source * djac * kOne3;
+#pragma unroll
+        for (int i = 0; i < 3; i++) er[i][0] -= dt * factor * rc;
+    }
+
+    // pressure, bed slope and boundary pressure (:761-862), skipped for u/v perturbations
+    if (pressure) {
+        auto accum = [&](double (&rhs)[3][3]) {
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) er[i][q] += rhs[i][q];
+        };
+        double rhs[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        const double cp = -0.5 * g * dt;
+        auto ipress = [&](const double*, const double*, const double* H, const double* GX, const double* GY, double dj,
+                          bool, const Clip&, double (&r)[3][3]) {
+            double ff = cp * kOne6 * dj * (H[0] * H[0] + H[0] * H[1] + H[1] * H[1] + H[0] * H[2] + H[1] * H[2] + H[2] * H[2]);
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                r[i][1] += GX[i] * ff;
+                r[i][2] += GY[i] * ff;
+            }
+        };
+        wd_apply(ch, in.x, in.y, in.h, gx, gy, djac, 1, rhs, ipress);
+        accum(rhs);
+        double rhs2[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        const double cb = g * dt;
+        auto ibody = [&](const double*, const double*, const double* H, const double*, const double*, double dj, bool,
+                         const Clip&, double (&r)[3][3]) {
+            double sh = H[0] + H[1] + H[2];
+            double cx = dj * kOne12 * cb * gzx, cy = dj * kOne12 * cb * gzy;
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                r[i][1] += cx * (sh + H[i]);
+                r[i][2] += cy * (sh + H[i]);
+            }
+        };
+        wd_apply(ch, in.x, in.y, in.h, nullptr, nullptr, djac, 1, rhs2, ibody);
+        accum(rhs2);
+        double rhs3[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        const double cq = 0.5 * dt * g;
+        auto ibound = [&](const double* X, const double* Y, const double* H, const double*, const double*, double, bool,
+                          const Clip&, double (&r)[3][3]) {
+#pragma unroll
+            for (int e = 0; e < 3; e++) {
+                const int n1 = e, n2 = (e + 1) % 3;
+                double delx = X[n1] - X[n2], dely = Y[n2] - Y[n1];
+                double t1 = kOne12 * cq;
+                double r0 = t1 * (3 * H[n1] * H[n1] + 2 * H[n1] * H[n2] + H[n2] * H[n2]);
+                double r1 = t1 * (H[n1] * H[n1] + 2 * H[n1] * H[n2] + 3 * H[n2] * H[n2]);
+                r[n1][1] += dely * r0;
+                r[n2][1] += dely * r1;
+                r[n1][2] += delx * r0;
+                r[n2][2] += delx * r1;
+            }
+        };
+        wd_apply(ch, in.x, in.y, in.h, nullptr, nullptr, djac, 1, rhs3, ibound);
+        accum(rhs3);
+    }
+
+    // SUPG (:987-1232)
+    if (!(fabs(h_wd) < kSmall)) {
+        const double gf = g;
+        const double hden = fmax(h_wd, kNotQuiteSmall);
+        const double le = sqrt(djac * factor_old);
+        double c2 = gf * hden;
+        if (hden <= 0.0) c2 = 0.;
+        const double sr = sqrt(u_wd * u_wd + v_wd * v_wd + c2 + kSmall);
+        const double tau = P.tau_pg * le / sr;
+        // elementally averaged wet/dry time derivatives (wrapped fe_sw2_wd_integrate_triangle_f)
+        double dhdt, dudt, dvdt;
+        {
+            Clip co;
+            make_clip(in.x, in.y, in.ho, djac, co);
+            double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            auto integ = [&](const double*, const double*, const double* H, const double*, const double*, double dj,
+                             bool clipped, const Clip& c, double (&r)[3][3]) {
+                r[0][0] += dj * ((H[0] + H[1] + H[2]) / 3.0);
+                r[0][1] += dj * ((cval(c, clipped, in.uo, 0) + cval(c, clipped, in.uo, 1) + cval(c, clipped, in.uo, 2)) / 3.0);
+                r[0][2] += dj * ((cval(c, clipped, in.vo, 0) + cval(c, clipped, in.vo, 1) + cval(c, clipped, in.vo, 2)) / 3.0);
+            };
+            wd_apply(co, in.x, in.y, in.ho, nullptr, nullptr, djac, 0, acc, integ);
+            dhdt = -acc[0][0];
+            dudt = -acc[0][1];
+            dvdt = -acc[0][2];
+        }
+        {
+            double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            auto integ = [&](const double*, const double*, const double* H, const double*, const double*, double dj,
+                             bool clipped, const Clip& c, double (&r)[3][3]) {
+                r[0][0] += dj * ((H[0] + H[1] + H[2]) / 3.0);
+                r[0][1] += dj * ((cval(c, clipped, in.u, 0) + cval(c, clipped, in.u, 1) + cval(c, clipped, in.u, 2)) / 3.0);
+                r[0][2] += dj * ((cval(c, clipped, in.v, 0) + cval(c, clipped, in.v, 1) + cval(c, clipped, in.v, 2)) / 3.0);
+            };
+            wd_apply(ch, in.x, in.y, in.h, nullptr, nullptr, djac, 0, acc, integ);
+            dhdt += acc[0][0];
+            dudt += acc[0][1];
+            dvdt += acc[0][2];
+        }
+        factor = ch.ret;
+        double adv[3] = {0, 0, 0};
+        {
+            double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            auto integ = [&](const double*, const double*, const double*, const double* GX, const double* GY, double dj,
+                             bool clipped, const Clip& c, double (&r)[3][3]) {
+                double f0 = cval(c, clipped, in.h, 0), f1 = cval(c, clipped, in.h, 1), f2 = cval(c, clipped, in.h, 2);
+                double u0 = cval(c, clipped, in.u, 0), u1 = cval(c, clipped, in.u, 1), u2 = cval(c, clipped, in.u, 2);
+                double v0 = cval(c, clipped, in.v, 0), v1 = cval(c, clipped, in.v, 1), v2 = cval(c, clipped, in.v, 2);
+                double ha = kOne3 * (f0 + f1 + f2), ua = kOne3 * (u0 + u1 + u2), va = kOne3 * (v0 + v1 + v2);
+                double dhdx = GX[0] * f0 + GX[1] * f1 + GX[2] * f2;
+                double dhdy = GY[0] * f0 + GY[1] * f1 + GY[2] * f2;
+                double dudx = GX[0] * u0 + GX[1] * u1 + GX[2] * u2;
+                double dudy = GY[0] * u0 + GY[1] * u1 + GY[2] * u2;
+                double dvdx = GX[0] * v0 + GX[1] * v1 + GX[2] * v2;
+                double dvdy = GY[0] * v0 + GY[1] * v1 + GY[2] * v2;
+                r[0][0] += dj * dt * 1.0 * (ua * dhdx + ha * dudx + va * dhdy + ha * dvdy);
+                r[0][1] += dj * dt * 1.0 * (ua * dudx + va * dudy);
+                r[0][2] += dj * dt * 1.0 * (ua * dvdx + va * dvdy);
+            };
+            wd_apply(ch, in.x, in.y, in.h, gx, gy, djac, 0, acc, integ);
+            adv[0] = acc[0][0];
+            adv[1] = acc[0][1];
+            adv[2] = acc[0][2];
+        }
+        const double xp = gf * (ghx + gzx) * dt * factor;
+        const double yp = gf * (ghy + gzy) * dt * factor;
+        const double xf = g * bedx * dt * factor, yf = g * bedy * dt * factor;
+        const double xc = -v_wd * cs, yc = u_wd * cs;
+        const double c_eq = dhdt + adv[0] + factor * water_source * djac * dt;
+        const double x_eq = dudt + adv[1] + (xp + xf / hden) * djac + xc * djac * factor * dt;
+        const double y_eq = dvdt + adv[2] + (yp + yf / hden) * djac + yc * djac * factor * dt;
+        const double tu = tau * u_wd, tv = tau * v_wd, th = tau * h_wd;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            er[i][0] += gx[i] * (tu * c_eq + th * x_eq) + gy[i] * (tv * c_eq + th * y_eq);
+            er[i][1] += gx[i] * (tau * gf * h_wd * c_eq + tu * h_wd * x_eq) + gy[i] * (tv * h_wd * x_eq);
+            er[i][2] += gy[i] * (tau * gf * h_wd * c_eq + tv * h_wd * y_eq) + gx[i] * (tu * h_wd * y_eq);
+        }
+    }
+
+    // Dirichlet nodes (:1239-1256)
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const int f = dflag[i];
+        if (f & 1) er[i][0] = 0.0;
+        if (f & 2) { er[i][1] = 0.0; er[i][2] = 0.0; }
+        if (f & 4) { er[i][0] = 0.0; er[i][1] = 0.0; er[i][2] = 0.0; }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// boundary edge residual (fe_sw2_boundary_resid, src/fe/sw2/fe_sw2_boundary_resid.c:72-510)
+// kind: 1 = BCT_VEL_NEU (value = series q), 2 = BCT_PRS_NEU (value = tailwater elevation),
+//       3 = BCT_OUTFLOW.  Returns er[node][eq] (eq 0 = c, 1 = x, 2 = y).
+struct EdgeIn {
+    double h[2], u[2], v[2];
+    double nx, ny, djac, z0;
+};
+
+__device__ __forceinline__ void line_phi_f_g_h(double djac, double c, double f1, double f2, double g1, double g2,
+                                               double h1, double h2, double& i0, double& i1) {
+    const double t1 = kOne60 * djac * c;
+    i0 += t1 * ((3 * (4 * f1 + f2) * g1 + (3 * f1 + 2 * f2) * g2) * h1 + ((3 * f1 + 2 * f2) * g1 + (2 * f1 + 3 * f2) * g2) * h2);
+    i1 += t1 * (((3 * f1 + 2 * f2) * g1 + (2 * f1 + 3 * f2) * g2) * h1 + ((2 * f1 + 3 * f2) * g1 + 3 * (f1 + 4 * f2) * g2) * h2);
+}
+
+__device__ __forceinline__ void sw2_edge_resid(const EdgeIn& in, int kind, double value, int pvar, const PhysParams& P,
+                                               const int* dflag, double (&er)[2][3]) {
+    const bool pressure = !(pvar == kPertU || pvar == kPertV);
+    const double djac = in.djac, dt = P.dt, g = P.g, nx = in.nx, ny = in.ny;
+    double h_avg = 0.5 * (in.h[0] + in.h[1]);
+    if (h_avg < kSmall) h_avg = kSmall;
+#pragma unroll
+    for (int i = 0; i < 2; i++) er[i][0] = er[i][1] = er[i][2] = 0.0;
+    if (kind == 1) {                       // explicit flow (:562-604)
+        const double flux = -1.0 * value;
+        const double rc = 0.5 * djac;
+        double rx0, rx1, ry0, ry1;
+        if (flux < 0) {
+            double us = 0., vs = 0.;
+            if (h_avg > 0) { us = flux * nx / h_avg; vs = flux * ny / h_avg; }
+            rx0 = rx1 = 0.5 * djac * us;
+            ry0 = ry1 = 0.5 * djac * vs;
+        } else {
+            const double t1 = kOne6 * djac;
+            rx0 = t1 * (2 * in.u[0] + in.u[1]); rx1 = t1 * (in.u[0] + 2 * in.u[1]);
+            ry0 = t1 * (2 * in.v[0] + in.v[1]); ry1 = t1 * (in.v[0] + 2 * in.v[1]);
+        }
+        const double t1 = dt * flux;
+        er[0][0] += t1 * rc; er[1][0] += t1 * rc;
+        er[0][1] += t1 * rx0; er[1][1] += t1 * rx1;
+        er[0][2] += t1 * ry0; er[1][2] += t1 * ry1;
+    } else if (kind == 2 || kind == 3) {
+        double d0 = 0.0, d1 = 0.0;
+        if (kind == 2) {
+            d0 = value - in.z0;
+            d1 = value - in.z0;             // both depths from node 0 (:375-376)
+            if (d0 < kSmall || d1 < kSmall || in.h[0] < kSmall || in.h[1] < kSmall) return;
+        }
+        double ur0 = in.u[0], ur1 = in.u[1], vr0 = in.v[0], vr1 = in.v[1];
+        if (in.u[0] * nx + in.v[0] * ny < kSmall) { ur0 = 0.; vr0 = 0.; }
+        if (in.u[1] * nx + in.v[1] * ny < kSmall) { ur1 = 0.; vr1 = 0.; }
+        const double h0 = in.h[0], h1 = in.h[1];
+        const double t1 = djac * kOne12;
+        double rc0 = t1 * (nx * ((3 * h0 + h1) * in.u[0] + (h0 + h1) * in.u[1]) + ny * ((3 * h0 + h1) * in.v[0] + (h0 + h1) * in.v[1]));
+        double rc1 = t1 * (nx * ((h0 + h1) * in.u[0] + (h0 + 3 * h1) * in.u[1]) + ny * ((h0 + h1) * in.v[0] + (h0 + 3 * h1) * in.v[1]));
+        double rx0 = 0, rx1 = 0, ry0 = 0, ry1 = 0;
+        line_phi_f_g_h(djac, nx, ur0, ur1, in.u[0], in.u[1], h0, h1, rx0, rx1);
+        line_phi_f_g_h(djac, ny, vr0, vr1, in.v[0], in.v[1], h0, h1, ry0, ry1);
+        line_phi_f_g_h(djac, ny, ur0, ur1, in.v[0], in.v[1], h0, h1, rx0, rx1);
+        line_phi_f_g_h(djac, nx, vr0, vr1, in.u[0], in.u[1], h0, h1, ry0, ry1);
+        er[0][0] += dt * rc0; er[1][0] += dt * rc1;
+        er[0][1] += dt * rx0; er[1][1] += dt * rx1;
+        er[0][2] += dt * ry0; er[1][2] += dt * ry1;
+        if (kind == 2 && pressure) {
+            double tt = djac * kOne12;
+            double p0 = tt * (3 * d0 * d0 + 2 * d0 * d1 + d1 * d1), p1 = tt * (d0 * d0 + 2 * d0 * d1 + 3 * d1 * d1);
+            double c1 = dt * 0.5 * g;
+            er[0][1] += c1 * nx * p0; er[1][1] += c1 * nx * p1;
+            er[0][2] += c1 * ny * p0; er[1][2] += c1 * ny * p1;
+            p0 = tt * (3 * h0 * h0 + 2 * h0 * h1 + h1 * h1);
+            p1 = tt * (h0 * h0 + 2 * h0 * h1 + 3 * h1 * h1);
+            c1 = dt * 0.5 * (-g);
+            er[0][1] += c1 * nx * p0; er[1][1] += c1 * nx * p1;
+            er[0][2] += c1 * ny * p0; er[1][2] += c1 * ny * p1;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const int f = dflag[i];
+        if (f & 1) er[i][0] = 0.0;
+        if (f & 2) { er[i][1] = 0.0; er[i][2] = 0.0; }
+        if (f & 4) { er[i][0] = 0.0; er[i][1] = 0.0; er[i][2] = 0.0; }
+    }
+}
+
+// NUM_DIFF_EPSILON (src/include/macro.h:669-673)
+__device__ __forceinline__ double fd_eps(double var) {
+    const double p = 1.4901161193847656e-08;  // sqrt(DBL_EPSILON)
+    double e = fabs(var) * (1. + p);
+    e -= fabs(var);
+    if (e < p) e = p;
+    return e;
+}
+
+}  // namespace sw2

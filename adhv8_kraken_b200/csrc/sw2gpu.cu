@@ -1,0 +1,761 @@
+// sw2gpu.cu -- host side of the B200 SW2 Newton step and the C ABI of include/sw2gpu.h.
+//
+// The host owns control flow only: mesh preprocessing at create time (geometry,
+// BCSR pattern, reference-order contribution lists), the Newton loop of fe_newton
+// (src/fe/fe_newton.c:214-912) with one 40-byte device->host read of the residual
+// norms per residual evaluation, and the dt-retry contract of fe_main.  All
+// element, node and Krylov work runs in the kernels of sw2_kernels.cuh /
+// sw2_krylov.cuh on the context's stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/sw2gpu.h"
+#include "sw2_krylov.cuh"
+
+using namespace sw2;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(e_ == cudaErrorMemoryAllocation ? SW2GPU_E_NOMEM : SW2GPU_E_CUDA,        \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+constexpr double kPi = 3.141592653589793238462643383279502884197169399375105820974944592308;
+constexpr double kEarthRotat = 7.2722E-5;
+constexpr double kUnsetFlt = -9999999.9;
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    int alloc(size_t count) {
+        n = count;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        return e == cudaSuccess ? 0 : -1;
+    }
+    ~DBuf() { if (p) cudaFree(p); }
+};
+
+}  // namespace
+
+struct sw2gpu_ctx {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int V = 0, T = 0, E = 0, S = 0, M = 0, NS = 0, nnzb = 0;
+    sw2gpu_params p{};
+    double dt = 0.0;
+    // host tables
+    std::vector<int> str_bc, str_isigma, str_ivx, str_ivy, str_iu0;
+    std::vector<MatParams> mats_h;
+    std::vector<int> dir_node, dir_mask, dir_str;
+    std::vector<int> rowptr_h, col_h;
+    // device mesh
+    DBuf<double> x, y, z, djac, gx0, gy0, gx1, gy1, gx2, gy2, bdjac, bnx, bny;
+    DBuf<int> en0, en1, en2, emat, bn0, bn1, bkind, bstr;
+    DBuf<unsigned char> efirst, dflag, mark;
+    DBuf<MatParams> mats;
+    DBuf<double> str_value;
+    DBuf<int> slot_ptr, slot_idx, blk_ptr, blk_src, rowptr, col, blk_row, dpos;
+    DBuf<int> dir_node_d, dir_mask_d;
+    DBuf<double> dir_h, dir_u, dir_v;
+    // state: three levels, rotated by index
+    DBuf<double> hs[3], us[3], vs[3];
+    int lv[3] = {0, 1, 2};
+    DBuf<int> wd;
+    // work
+    DBuf<double> sc, sx, sy, R, sol, jslots, val, S_, bs;
+    DBuf<float> val32, dinv32;
+    DBuf<double> dinv64;
+    DBuf<double> kv64[7];
+    DBuf<float> kv32[7];
+    DBuf<double> part;
+    DBuf<KrylovCtl> ctl;
+    DBuf<Norms> npart, norms;
+    DBuf<unsigned> ncounter;
+    DBuf<int> singular;
+    Norms* norms_h = nullptr;
+    KrylovCtl* ctl_h = nullptr;
+    int krylov_grid = 0;
+    int launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevMesh dm{};
+
+    ~sw2gpu_ctx() {
+        if (norms_h) cudaFreeHost(norms_h);
+        if (ctl_h) cudaFreeHost(ctl_h);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+    double* H(int l) { return hs[lv[l]].p; }
+    double* U(int l) { return us[lv[l]].p; }
+    double* Vv(int l) { return vs[lv[l]].p; }
+    State state() {
+        State s;
+        s.h = H(0); s.u = U(0); s.v = Vv(0);
+        s.ho = H(1); s.uo = U(1); s.vo = Vv(1);
+        s.hoo = H(2); s.uoo = U(2); s.voo = Vv(2);
+        s.wd = wd.p;
+        return s;
+    }
+    PhysParams phys() const {
+        PhysParams P;
+        P.g = p.gravity;
+        P.dll = p.drying_lower_limit;
+        P.dul = p.drying_upper_limit;
+        P.alpha = p.tau_temporal;
+        P.tau_pg = p.tau_pg;
+        P.dt = dt;
+        return P;
+    }
+};
+
+namespace {
+
+template <typename T>
+int up(DBuf<T>& b, const std::vector<T>& v, cudaStream_t st) {
+    if (b.alloc(v.size())) return fail(SW2GPU_E_NOMEM, "cudaMalloc of %zu bytes failed", v.size() * sizeof(T));
+    if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return 0;
+}
+template <typename T>
+int zalloc(DBuf<T>& b, size_t n, cudaStream_t st) {
+    if (b.alloc(n)) return fail(SW2GPU_E_NOMEM, "cudaMalloc of %zu bytes failed", n * sizeof(T));
+    CK(cudaMemsetAsync(b.p, 0, std::max<size_t>(n, 1) * sizeof(T), st));
+    return 0;
+}
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+// per-step tables: string values (edge series), material water sources, Dirichlet values
+int upload_step_tables(sw2gpu_ctx* c, const double* series) {
+    std::vector<double> sv(std::max(c->S, 1), 0.0);
+    for (int s = 0; s < c->S; s++) {
+        int k = c->str_isigma[s];
+        if (k >= 0 && k < c->NS && series) sv[s] = series[k];
+    }
+    CK(cudaMemcpyAsync(c->str_value.p, sv.data(), sizeof(double) * c->S, cudaMemcpyHostToDevice, c->stream));
+    bool any_src = false;
+    for (int m = 0; m < c->M; m++) {
+        if (c->mats_h[m].has_source) {
+            int k = c->str_isigma[m];
+            c->mats_h[m].water_src = (k >= 0 && k < c->NS && series) ? series[k] : 0.0;
+            any_src = true;
+        }
+    }
+    if (any_src)
+        CK(cudaMemcpyAsync(c->mats.p, c->mats_h.data(), sizeof(MatParams) * c->M, cudaMemcpyHostToDevice, c->stream));
+    const int nd = (int)c->dir_node.size();
+    if (nd) {
+        std::vector<double> h(nd, 0.0), u(nd, 0.0), v(nd, 0.0);
+        for (int i = 0; i < nd; i++) {
+            int s = c->dir_str[i];
+            auto get = [&](int k) { return (k >= 0 && k < c->NS && series) ? series[k] : 0.0; };
+            u[i] = get(c->str_ivx[s]);
+            v[i] = get(c->str_ivy[s]);
+            h[i] = get(c->str_iu0[s]);
+        }
+        CK(cudaMemcpyAsync(c->dir_h.p, h.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->dir_u.p, u.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->dir_v.p, v.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
+    }
+    return 0;
+}
+
+// residual at the current state: element slots, reference-order gather, norms (async)
+int launch_resid(sw2gpu_ctx* c) {
+    State s = c->state();
+    PhysParams P = c->phys();
+    const int n = c->T + c->E;
+    k_resid_elem<<<nblk(std::max(n, 1), 128), 128, 0, c->stream>>>(c->dm, s, P, c->sc.p, c->sx.p, c->sy.p);
+    k_resid_gather<<<nblk(std::max(c->V, 1), kGatherThreads), kGatherThreads, 0, c->stream>>>(
+        c->dm, s, c->sc.p, c->sx.p, c->sy.p, c->R.p, c->sol.p, c->npart.p, c->ncounter.p, c->norms.p);
+    c->launches += 2;
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int read_norms(sw2gpu_ctx* c, Norms& out) {
+    CK(cudaMemcpyAsync(c->norms_h, c->norms.p, sizeof(Norms), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out = *c->norms_h;
+    return 0;
+}
+
+int launch_jacobian(sw2gpu_ctx* c) {
+    State s = c->state();
+    PhysParams P = c->phys();
+    if (c->T) k_jac_elem<<<nblk(c->T, kJacElems), kJacThreads, 0, c->stream>>>(c->dm, s, P, c->jslots.p);
+    if (c->E) k_jac_edge<<<nblk(6LL * c->E, 128), 128, 0, c->stream>>>(c->dm, s, P, c->jslots.p);
+    k_jac_gather<<<nblk(9LL * c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->jslots.p, c->val.p);
+    c->launches += 2 + (c->E ? 1 : 0);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int launch_init(sw2gpu_ctx* c) {     // fe_sw2_init: current = old, Dirichlet values, wd flags
+    const size_t nb = sizeof(double) * c->V;
+    CK(cudaMemcpyAsync(c->H(0), c->H(1), nb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->U(0), c->U(1), nb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->Vv(0), c->Vv(1), nb, cudaMemcpyDeviceToDevice, c->stream));
+    const int nd = (int)c->dir_node.size();
+    if (nd) {
+        k_dirichlet<<<nblk(nd, 128), 128, 0, c->stream>>>(nd, c->dir_node_d.p, c->dir_mask_d.p, c->dir_h.p,
+                                                           c->dir_u.p, c->dir_v.p, c->H(0), c->U(0), c->Vv(0));
+        c->launches++;
+    }
+    CK(cudaMemsetAsync(c->mark.p, 0, std::max(c->V, 1), c->stream));
+    if (c->T) {
+        k_wd_mark<<<nblk(c->T, 256), 256, 0, c->stream>>>(c->T, c->en0.p, c->en1.p, c->en2.p, c->H(0), c->mark.p);
+        k_wd_flag<<<nblk(c->T, 256), 256, 0, c->stream>>>(c->T, c->en0.p, c->en1.p, c->en2.p, c->H(0), c->H(1),
+                                                          c->mark.p, c->wd.p);
+        c->launches += 2;
+    }
+    CK(cudaGetLastError());
+    return 0;
+}
+
+// scaling, preconditioner setup and the persistent BiCGSTAB; returns its iteration count
+int launch_linear(sw2gpu_ctx* c, int apply_inc, int* its, int* converged) {
+    State s = c->state();
+    k_rowscale<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->dm, s, c->val.p, c->R.p, c->S_.p, c->bs.p, 0);
+    CK(cudaMemsetAsync(c->singular.p, 0, sizeof(int), c->stream));
+    const bool mixed = c->p.precision == SW2GPU_MIXED;
+    if (mixed)
+        k_scale_matrix<float><<<nblk(c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->val32.p, c->S_.p,
+                                                                         c->dinv32.p, c->singular.p);
+    else
+        k_scale_matrix<double><<<nblk(c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->val.p, c->S_.p,
+                                                                          c->dinv64.p, c->singular.p);
+    CK(cudaMemsetAsync(c->ctl.p, 0, sizeof(KrylovCtl), c->stream));
+    KrylovArgs K;
+    K.V = c->V;
+    K.rowptr = c->rowptr.p;
+    K.col = c->col.p;
+    K.S = c->S_.p;
+    K.bs = c->bs.p;
+    K.rtol = c->p.lin_rtol;
+    K.atol = c->p.lin_atol;
+    K.maxit = c->p.max_lin_it;
+    K.h = c->H(0);
+    K.u = c->U(0);
+    K.v = c->Vv(0);
+    K.sol = c->sol.p;
+    K.apply_inc = apply_inc;
+    K.part = c->part.p;
+    K.ctl = c->ctl.p;
+    dim3 grid(c->krylov_grid), block(kKrylovThreads);
+    if (mixed) {
+        const float* A = c->val32.p;
+        const float* D = c->dinv32.p;
+        float *b = c->kv32[0].p, *uu = c->kv32[1].p, *r = c->kv32[2].p, *q = c->kv32[3].p, *pp = c->kv32[4].p,
+              *Ap = c->kv32[5].p, *As = c->kv32[6].p;
+        void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As};
+        CK(cudaLaunchCooperativeKernel((void*)k_bicgstab<float, float>, grid, block, args, 0, c->stream));
+    } else {
+        const double* A = c->val.p;
+        const double* D = c->dinv64.p;
+        double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
+               *Ap = c->kv64[5].p, *As = c->kv64[6].p;
+        void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As};
+        CK(cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double>, grid, block, args, 0, c->stream));
+    }
+    c->launches += 3;
+    CK(cudaMemcpyAsync(c->ctl_h, c->ctl.p, sizeof(KrylovCtl), cudaMemcpyDeviceToHost, c->stream));
+    (void)its;
+    (void)converged;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sw2gpu_abi_version(void) { return SW2GPU_ABI_VERSION; }
+const char* sw2gpu_last_error(void) { return g_err.c_str(); }
+
+int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, sw2gpu_ctx** out) {
+    if (!m || !prm || !out) return fail(SW2GPU_E_ARG, "null argument");
+    *out = nullptr;
+    if (m->nnodes <= 0 || m->nelems2d < 0 || m->nelems1d < 0) return fail(SW2GPU_E_ARG, "bad mesh sizes");
+    if (prm->precision != SW2GPU_FP64 && prm->precision != SW2GPU_MIXED) return fail(SW2GPU_E_ARG, "bad precision");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    auto* c = new sw2gpu_ctx();
+    std::unique_ptr<sw2gpu_ctx> guard(c);
+    c->p = *prm;
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    cudaStream_t st = c->stream;
+    const int V = c->V = m->nnodes, T = c->T = m->nelems2d, E = c->E = m->nelems1d;
+    c->S = m->nstrings;
+    c->M = m->nmats;
+    c->NS = m->nseries;
+    const int* tri = m->elem2d_nodes;
+    const int* edg = m->elem1d_nodes;
+    for (int e = 0; e < T; e++)
+        for (int i = 0; i < 3; i++)
+            if (tri[3 * e + i] < 0 || tri[3 * e + i] >= V) return fail(SW2GPU_E_ARG, "element %d: node out of range", e);
+    for (int e = 0; e < T; e++)
+        if (m->elem2d_mat[e] < 0 || m->elem2d_mat[e] >= c->M || m->elem2d_mat[e] >= c->S)
+            return fail(SW2GPU_E_ARG, "element %d: bad material", e);
+    c->str_bc.assign(m->str_bc_flag, m->str_bc_flag + c->S);
+    c->str_isigma.assign(m->str_isigma, m->str_isigma + c->S);
+    c->str_ivx.assign(m->str_ivx, m->str_ivx + c->S);
+    c->str_ivy.assign(m->str_ivy, m->str_ivy + c->S);
+    c->str_iu0.assign(m->str_iu0, m->str_iu0 + c->S);
+
+    // geometry (element_djac_nrml_gradPhi.c:193-273); kept in SoA arrays
+    std::vector<double> djac(T), g[6];
+    for (auto& a : g) a.resize(T);
+    for (int e = 0; e < T; e++) {
+        const int a = tri[3 * e], b = tri[3 * e + 1], cc = tri[3 * e + 2];
+        const double s1x = m->x[b] - m->x[a], s1y = m->y[b] - m->y[a], s2x = m->x[cc] - m->x[a], s2y = m->y[cc] - m->y[a];
+        const double cr = s1x * s2y - s2x * s1y;
+        g[0][e] = (s1y - s2y) / cr;
+        g[1][e] = (s2x - s1x) / cr;
+        g[2][e] = s2y / cr;
+        g[3][e] = -s2x / cr;
+        g[4][e] = -s1y / cr;
+        g[5][e] = s1x / cr;
+        djac[e] = cr * 0.5;
+        if (djac[e] < 1e-6) return fail(SW2GPU_E_ARG, "element %d is not counter-clockwise (djac %g)", e, djac[e]);
+    }
+    // boundary edges: length, outward normal (elem1d_outward_nrml.c), kind
+    std::vector<double> bdj(E), bnx(E), bny(E);
+    std::vector<int> bkind(E), bstr(E), bn0(E), bn1(E);
+    for (int j = 0; j < E; j++) {
+        const int a = edg[2 * j], b = edg[2 * j + 1], pe = m->elem1d_parent[j], s = m->elem1d_string[j];
+        if (a < 0 || a >= V || b < 0 || b >= V || pe < 0 || pe >= T || s < 0 || s >= c->S)
+            return fail(SW2GPU_E_ARG, "edge %d: bad node, parent or string", j);
+        const double dx = m->x[b] - m->x[a], dy = m->y[b] - m->y[a], L = std::sqrt(dx * dx + dy * dy);
+        double nx = dy / L, ny = -dx / L;
+        const double cx = kOne3 * (m->x[tri[3 * pe]] + m->x[tri[3 * pe + 1]] + m->x[tri[3 * pe + 2]]);
+        const double cy = kOne3 * (m->y[tri[3 * pe]] + m->y[tri[3 * pe + 1]] + m->y[tri[3 * pe + 2]]);
+        if ((cx - m->x[a]) * nx + (cy - m->y[a]) * ny > 0.) { nx = -nx; ny = -ny; }
+        bdj[j] = std::sqrt((m->x[a] - m->x[b]) * (m->x[a] - m->x[b]) + (m->y[a] - m->y[b]) * (m->y[a] - m->y[b]));
+        bnx[j] = nx;
+        bny[j] = ny;
+        bn0[j] = a;
+        bn1[j] = b;
+        bstr[j] = s;
+        const int f = c->str_bc[s];
+        bkind[j] = f == SW2GPU_BCT_VEL_NEU ? 1 : f == SW2GPU_BCT_PRS_NEU ? 2 : f == SW2GPU_BCT_OUTFLOW ? 3 : 0;
+        if (!bkind[j]) return fail(SW2GPU_E_ARG, "edge %d: boundary condition %d not supported", j, f);
+    }
+    // Dirichlet flags per node
+    std::vector<unsigned char> dflag(V, 0);
+    for (int n = 0; n < V; n++) {
+        const int s = m->node_string[n];
+        if (s > SW2GPU_NORMAL && s < c->S) {
+            const int f = c->str_bc[s];
+            dflag[n] = f == SW2GPU_BCT_PRS_DIR ? 1 : f == SW2GPU_BCT_VEL_DIR ? 2 : f == SW2GPU_BCT_VEL_PRS_DIR ? 4 : 0;
+            if (dflag[n]) {
+                c->dir_node.push_back(n);
+                c->dir_mask.push_back(f == SW2GPU_BCT_PRS_DIR ? 1 : f == SW2GPU_BCT_VEL_DIR ? 2 : 3);
+                c->dir_str.push_back(s);
+            }
+        }
+    }
+    // first 2D element of every node (the dry-velocity side effect of fe_sw2_resid)
+    std::vector<int> first(V, -1);
+    std::vector<unsigned char> efirst(T, 0);
+    for (int e = 0; e < T; e++)
+        for (int i = 0; i < 3; i++) {
+            const int n = tri[3 * e + i];
+            if (first[n] < 0) first[n] = e;
+            if (first[n] == e) efirst[e] |= (unsigned char)(1u << i);
+        }
+    // materials
+    c->mats_h.resize(std::max(c->M, 1));
+    for (int k = 0; k < c->M; k++) {
+        MatParams& mp = c->mats_h[k];
+        memset(&mp, 0, sizeof mp);
+        mp.ks = (k < c->S) ? m->str_rough_height[k] : kUnsetFlt;
+        mp.eev_mode = m->mat_eev_mode[k];
+        mp.eev_coef = m->mat_eev_coef[k];
+        const double xx = m->mat_ev[3 * k] + prm->viscosity, yy = m->mat_ev[3 * k + 1] + prm->viscosity;
+        mp.ev_st = std::fabs(xx - yy);
+        mp.ev_tr = std::min(xx, yy);
+        mp.cor_speed = std::sin((kPi / 180.) * m->mat_coriolis[k]) * 2. * kEarthRotat;
+        mp.has_source = (k < c->S && c->str_bc[k] == SW2GPU_BCT_WATER_SOURCE) ? 1 : 0;
+    }
+    // BCSR pattern: sorted unique columns per node row (element pairs and edge pairs)
+    std::vector<int> deg(V + 1, 0);
+    for (int e = 0; e < T; e++) for (int i = 0; i < 3; i++) deg[tri[3 * e + i]] += 3;
+    for (int j = 0; j < E; j++) for (int i = 0; i < 2; i++) deg[edg[2 * j + i]] += 2;
+    std::vector<int> start(V + 1, 0);
+    for (int n = 0; n < V; n++) start[n + 1] = start[n] + deg[n];
+    std::vector<int> tmp(start[V]);
+    std::vector<int> fillc(V, 0);
+    for (int e = 0; e < T; e++)
+        for (int i = 0; i < 3; i++) {
+            const int a = tri[3 * e + i];
+            for (int k = 0; k < 3; k++) tmp[start[a] + fillc[a]++] = tri[3 * e + k];
+        }
+    for (int j = 0; j < E; j++)
+        for (int i = 0; i < 2; i++) {
+            const int a = edg[2 * j + i];
+            for (int k = 0; k < 2; k++) tmp[start[a] + fillc[a]++] = edg[2 * j + k];
+        }
+    std::vector<int>& rp = c->rowptr_h;
+    std::vector<int>& col = c->col_h;
+    rp.assign(V + 1, 0);
+    col.clear();
+    col.reserve(start[V] / 2);
+    for (int n = 0; n < V; n++) {
+        auto b = tmp.begin() + start[n], e2 = tmp.begin() + start[n + 1];
+        std::sort(b, e2);
+        auto last = std::unique(b, e2);
+        col.insert(col.end(), b, last);
+        rp[n + 1] = (int)col.size();
+    }
+    const int nnzb = c->nnzb = (int)col.size();
+    std::vector<int> blk_row(nnzb), dpos(V, -1);
+    for (int n = 0; n < V; n++)
+        for (int k = rp[n]; k < rp[n + 1]; k++) {
+            blk_row[k] = n;
+            if (col[k] == n) dpos[n] = k;
+        }
+    for (int n = 0; n < V; n++)
+        if (dpos[n] < 0) return fail(SW2GPU_E_ARG, "node %d belongs to no element", n);
+    auto find_blk = [&](int i, int j) {
+        auto b = col.begin() + rp[i], e2 = col.begin() + rp[i + 1];
+        return (int)(std::lower_bound(b, e2, j) - col.begin());
+    };
+    // BCSR block <- element-block slots, in reference order (elements then edges)
+    const size_t nsrc = 9ull * T + 4ull * E;
+    std::vector<int> src_blk(nsrc);
+    for (int e = 0; e < T; e++)
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) src_blk[9ull * e + 3 * a + b] = find_blk(tri[3 * e + a], tri[3 * e + b]);
+    for (int j = 0; j < E; j++)
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) src_blk[9ull * T + 4 * j + 2 * a + b] = find_blk(edg[2 * j + a], edg[2 * j + b]);
+    std::vector<int> blk_ptr(nnzb + 1, 0), blk_src(nsrc);
+    for (size_t q = 0; q < nsrc; q++) blk_ptr[src_blk[q] + 1]++;
+    for (int k = 0; k < nnzb; k++) blk_ptr[k + 1] += blk_ptr[k];
+    {
+        std::vector<int> f2(blk_ptr.begin(), blk_ptr.end() - 1);
+        for (size_t q = 0; q < nsrc; q++) blk_src[f2[src_blk[q]]++] = (int)q;   // q ascending = reference order
+    }
+    // node <- residual slots, reference order
+    const size_t nslot = 3ull * T + 2ull * E;
+    std::vector<int> slot_ptr(V + 1, 0), slot_idx(nslot);
+    for (int e = 0; e < T; e++) for (int i = 0; i < 3; i++) slot_ptr[tri[3 * e + i] + 1]++;
+    for (int j = 0; j < E; j++) for (int i = 0; i < 2; i++) slot_ptr[edg[2 * j + i] + 1]++;
+    for (int n = 0; n < V; n++) slot_ptr[n + 1] += slot_ptr[n];
+    {
+        std::vector<int> f2(slot_ptr.begin(), slot_ptr.end() - 1);
+        for (int e = 0; e < T; e++) for (int i = 0; i < 3; i++) slot_idx[f2[tri[3 * e + i]]++] = 3 * e + i;
+        for (int j = 0; j < E; j++) for (int i = 0; i < 2; i++) slot_idx[f2[edg[2 * j + i]]++] = 3 * T + 2 * j + i;
+    }
+    // upload
+    std::vector<double> xv(m->x, m->x + V), yv(m->y, m->y + V), zv(m->z, m->z + V);
+    std::vector<int> e0(T), e1(T), e2(T), em(m->elem2d_mat, m->elem2d_mat + T);
+    for (int e = 0; e < T; e++) { e0[e] = tri[3 * e]; e1[e] = tri[3 * e + 1]; e2[e] = tri[3 * e + 2]; }
+    int rc = 0;
+    rc |= up(c->x, xv, st); rc |= up(c->y, yv, st); rc |= up(c->z, zv, st);
+    rc |= up(c->djac, djac, st);
+    rc |= up(c->gx0, g[0], st); rc |= up(c->gy0, g[1], st); rc |= up(c->gx1, g[2], st);
+    rc |= up(c->gy1, g[3], st); rc |= up(c->gx2, g[4], st); rc |= up(c->gy2, g[5], st);
+    rc |= up(c->en0, e0, st); rc |= up(c->en1, e1, st); rc |= up(c->en2, e2, st); rc |= up(c->emat, em, st);
+    rc |= up(c->efirst, efirst, st); rc |= up(c->dflag, dflag, st);
+    rc |= up(c->bn0, bn0, st); rc |= up(c->bn1, bn1, st); rc |= up(c->bkind, bkind, st); rc |= up(c->bstr, bstr, st);
+    rc |= up(c->bdjac, bdj, st); rc |= up(c->bnx, bnx, st); rc |= up(c->bny, bny, st);
+    rc |= up(c->mats, c->mats_h, st);
+    rc |= zalloc(c->str_value, std::max(c->S, 1), st);
+    rc |= up(c->slot_ptr, slot_ptr, st); rc |= up(c->slot_idx, slot_idx, st);
+    rc |= up(c->blk_ptr, blk_ptr, st); rc |= up(c->blk_src, blk_src, st);
+    rc |= up(c->rowptr, rp, st); rc |= up(c->col, col, st); rc |= up(c->blk_row, blk_row, st); rc |= up(c->dpos, dpos, st);
+    rc |= up(c->dir_node_d, c->dir_node, st); rc |= up(c->dir_mask_d, c->dir_mask, st);
+    rc |= zalloc(c->dir_h, c->dir_node.size(), st); rc |= zalloc(c->dir_u, c->dir_node.size(), st);
+    rc |= zalloc(c->dir_v, c->dir_node.size(), st);
+    for (int l = 0; l < 3; l++) { rc |= zalloc(c->hs[l], V, st); rc |= zalloc(c->us[l], V, st); rc |= zalloc(c->vs[l], V, st); }
+    rc |= zalloc(c->wd, std::max(T, 1), st);
+    rc |= zalloc(c->mark, V, st);
+    rc |= zalloc(c->sc, nslot, st); rc |= zalloc(c->sx, nslot, st); rc |= zalloc(c->sy, nslot, st);
+    rc |= zalloc(c->R, 3ull * V, st); rc |= zalloc(c->sol, 3ull * V, st);
+    rc |= zalloc(c->jslots, nsrc * 9, st);
+    rc |= zalloc(c->val, 9ull * nnzb, st);
+    rc |= zalloc(c->S_, 3ull * V, st); rc |= zalloc(c->bs, 3ull * V, st);
+    if (prm->precision == SW2GPU_MIXED) {
+        rc |= zalloc(c->val32, 9ull * nnzb, st);
+        rc |= zalloc(c->dinv32, 9ull * V, st);
+        for (auto& b : c->kv32) rc |= zalloc(b, 3ull * V, st);
+    } else {
+        rc |= zalloc(c->dinv64, 9ull * V, st);
+        for (auto& b : c->kv64) rc |= zalloc(b, 3ull * V, st);
+    }
+    rc |= zalloc(c->ctl, 1, st);
+    rc |= zalloc(c->ncounter, 1, st);
+    rc |= zalloc(c->singular, 1, st);
+    const int gblocks = nblk(V, kGatherThreads);
+    rc |= zalloc(c->npart, gblocks, st);
+    rc |= zalloc(c->norms, 1, st);
+    if (rc) return rc;
+    // persistent Krylov grid: every block co-resident
+    int sms = 0, per_sm = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (prm->precision == SW2GPU_MIXED)
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<float, float>, kKrylovThreads, 0));
+    else
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double>, kKrylovThreads, 0));
+    per_sm = std::min(per_sm, 4);
+    const int need = nblk(V, kKrylovThreads);
+    c->krylov_grid = std::max(1, std::min(need, sms * std::max(per_sm, 1)));
+    if (zalloc(c->part, 8ull * c->krylov_grid, st)) return SW2GPU_E_NOMEM;
+    CK(cudaMallocHost(&c->norms_h, sizeof(Norms)));
+    CK(cudaMallocHost(&c->ctl_h, sizeof(KrylovCtl)));
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+    DevMesh& d = c->dm;
+    d.V = V; d.T = T; d.E = E; d.nnzb = nnzb;
+    d.x = c->x.p; d.y = c->y.p; d.z = c->z.p;
+    d.en0 = c->en0.p; d.en1 = c->en1.p; d.en2 = c->en2.p; d.emat = c->emat.p;
+    d.djac = c->djac.p; d.gx0 = c->gx0.p; d.gy0 = c->gy0.p; d.gx1 = c->gx1.p; d.gy1 = c->gy1.p; d.gx2 = c->gx2.p;
+    d.gy2 = c->gy2.p;
+    d.efirst = c->efirst.p; d.dflag = c->dflag.p;
+    d.bn0 = c->bn0.p; d.bn1 = c->bn1.p; d.bkind = c->bkind.p; d.bstr = c->bstr.p;
+    d.bdjac = c->bdjac.p; d.bnx = c->bnx.p; d.bny = c->bny.p;
+    d.mats = c->mats.p; d.str_value = c->str_value.p;
+    d.slot_ptr = c->slot_ptr.p; d.slot_idx = c->slot_idx.p; d.blk_ptr = c->blk_ptr.p; d.blk_src = c->blk_src.p;
+    d.rowptr = c->rowptr.p; d.col = c->col.p; d.blk_row = c->blk_row.p; d.dpos = c->dpos.p;
+    for (int i = 0; i < 3; i++) d.qflag[i] = (i < V) ? dflag[i] : 0;
+    CK(cudaStreamSynchronize(st));
+    *out = guard.release();
+    return SW2GPU_OK;
+}
+
+int sw2gpu_destroy(sw2gpu_ctx* c) {
+    if (!c) return SW2GPU_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    delete c;
+    return SW2GPU_OK;
+}
+
+int sw2gpu_set_state(sw2gpu_ctx* c, int level, const double* h, const double* u, const double* v) {
+    if (!c || level < 0 || level > 2) return fail(SW2GPU_E_ARG, "bad context or level");
+    const size_t nb = sizeof(double) * c->V;
+    if (h) CK(cudaMemcpyAsync(c->H(level), h, nb, cudaMemcpyHostToDevice, c->stream));
+    if (u) CK(cudaMemcpyAsync(c->U(level), u, nb, cudaMemcpyHostToDevice, c->stream));
+    if (v) CK(cudaMemcpyAsync(c->Vv(level), v, nb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_get_state(sw2gpu_ctx* c, int level, double* h, double* u, double* v) {
+    if (!c || level < 0 || level > 2) return fail(SW2GPU_E_ARG, "bad context or level");
+    const size_t nb = sizeof(double) * c->V;
+    if (h) CK(cudaMemcpyAsync(h, c->H(level), nb, cudaMemcpyDeviceToHost, c->stream));
+    if (u) CK(cudaMemcpyAsync(u, c->U(level), nb, cudaMemcpyDeviceToHost, c->stream));
+    if (v) CK(cudaMemcpyAsync(v, c->Vv(level), nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_get_wd_flag(sw2gpu_ctx* c, int32_t* wd) {
+    if (!c || !wd) return fail(SW2GPU_E_ARG, "null argument");
+    if (c->T) CK(cudaMemcpyAsync(wd, c->wd.p, sizeof(int) * c->T, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_set_wd_flag(sw2gpu_ctx* c, const int32_t* wd) {
+    if (!c || !wd) return fail(SW2GPU_E_ARG, "null argument");
+    if (c->T) CK(cudaMemcpyAsync(c->wd.p, wd, sizeof(int) * c->T, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_set_dt(sw2gpu_ctx* c, double dt, const double* series) {
+    if (!c || !(dt > 0.0)) return fail(SW2GPU_E_ARG, "bad context or dt");
+    c->dt = dt;
+    int rc = upload_step_tables(c, series);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_resid(sw2gpu_ctx* c, double* resid) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    int rc = launch_resid(c);
+    if (rc) return rc;
+    if (resid) CK(cudaMemcpyAsync(resid, c->R.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_load(sw2gpu_ctx* c, int32_t* nnzb, int32_t* row_ptr, int32_t* col, double* val, double* resid) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    if (nnzb) *nnzb = c->nnzb;
+    if (!val && !resid && !row_ptr && !col) return SW2GPU_OK;
+    int rc = launch_jacobian(c);
+    if (rc) return rc;
+    State s = c->state();
+    k_rowscale<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->dm, s, c->val.p, c->R.p, c->S_.p, c->bs.p, 1);
+    CK(cudaGetLastError());
+    if (row_ptr) memcpy(row_ptr, c->rowptr_h.data(), sizeof(int) * (c->V + 1));
+    if (col) memcpy(col, c->col_h.data(), sizeof(int) * c->nnzb);
+    if (val) CK(cudaMemcpyAsync(val, c->val.p, sizeof(double) * 9 * (size_t)c->nnzb, cudaMemcpyDeviceToHost, c->stream));
+    if (resid) CK(cudaMemcpyAsync(resid, c->R.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_linear_solve(sw2gpu_ctx* c, const double* val, const double* rhs, double* x, int32_t* iterations) {
+    if (!c || !val || !rhs || !x) return fail(SW2GPU_E_ARG, "null argument");
+    CK(cudaMemcpyAsync(c->val.p, val, sizeof(double) * 9 * (size_t)c->nnzb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->R.p, rhs, sizeof(double) * 3 * c->V, cudaMemcpyHostToDevice, c->stream));
+    int rc = launch_linear(c, 0, nullptr, nullptr);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(x, c->sol.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (iterations) *iterations = c->ctl_h->iterations;
+    if (c->ctl_h->err) return fail(SW2GPU_E_TIMEOUT, "Krylov grid barrier wait ran out");
+    return c->ctl_h->converged ? SW2GPU_OK : fail(SW2GPU_E_LINEAR, "BiCGSTAB reached max_lin_it");
+}
+
+int sw2gpu_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* stats) {
+    if (!c || !(dt > 0.0)) return fail(SW2GPU_E_ARG, "bad context or dt");
+    const sw2gpu_params& p = c->p;
+    c->launches = 0;
+    c->dt = dt;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    // fe_sw2: older <- old <- current (level rotation, no copies)
+    {
+        const int o2 = c->lv[2];
+        c->lv[2] = c->lv[1];
+        c->lv[1] = c->lv[0];
+        c->lv[0] = o2;
+    }
+    int rc = upload_step_tables(c, series);
+    if (rc) return rc;
+    if ((rc = launch_init(c))) return rc;
+    if ((rc = launch_resid(c))) return rc;
+    Norms nm;
+    if ((rc = read_norms(c, nm))) return rc;
+    const double n3 = 3.0 * c->V;
+    double rmax = nm.rmax, l2 = std::sqrt(nm.l2sum / n3), imax = nm.imax, old_l2;
+    int it = 0, lin_total = 0, cuts_total = 0;
+    bool solv_ok = true, nan = nm.nan != 0, keep;
+    if (nan) solv_ok = false;
+    do {
+        if (!solv_ok) break;
+        if ((rc = launch_jacobian(c))) return rc;
+        if ((rc = launch_linear(c, 1, nullptr, nullptr))) return rc;
+        old_l2 = l2;
+        if ((rc = launch_resid(c))) return rc;
+        if ((rc = read_norms(c, nm))) return rc;   // also completes the Krylov control read
+        if (c->ctl_h->err) return fail(SW2GPU_E_TIMEOUT, "Krylov grid barrier wait ran out");
+        lin_total += c->ctl_h->iterations;
+        if (!c->ctl_h->converged) solv_ok = false;
+        rmax = nm.rmax;
+        l2 = std::sqrt(nm.l2sum / n3);
+        imax = nm.imax;
+        if (nm.nan || std::isnan(l2) || std::isinf(l2)) { solv_ok = false; nan = true; }
+        int cuts = 0;
+        while (rmax > p.tol_nonlin && l2 > old_l2 && cuts < p.max_linesearch_cuts) {
+            k_half_inc<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->V, c->sol.p, c->H(0), c->U(0), c->Vv(0));
+            c->launches++;
+            if ((rc = launch_resid(c))) return rc;
+            if ((rc = read_norms(c, nm))) return rc;
+            rmax = nm.rmax;
+            l2 = std::sqrt(nm.l2sum / n3);
+            imax = nm.imax;
+            cuts++;
+        }
+        cuts_total += cuts;
+        it++;
+        keep = solv_ok && it < p.max_nonlin_it && rmax < 1.0E+20 && (rmax > p.tol_nonlin && imax > p.inc_nonlin);
+    } while (keep);
+    int status = SW2GPU_OK;
+    if (!solv_ok || (rmax > p.tol_nonlin && imax > p.inc_nonlin) || rmax >= 1.0E+20) {
+        status = nan ? SW2GPU_E_NAN : (!solv_ok ? SW2GPU_E_LINEAR : SW2GPU_E_NEWTON);
+        if ((rc = launch_init(c))) return rc;   // reset to the old level; the caller scales dt
+    }
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->status = status;
+        stats->newton_its = it;
+        stats->linear_its = lin_total;
+        stats->linesearch_cuts = cuts_total;
+        stats->resid_max = rmax;
+        stats->resid_l2 = l2;
+        stats->inc_max = imax;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        stats->device_ms = ms;
+        stats->kernel_launches = c->launches;
+    }
+    if (status != SW2GPU_OK) fail(status, "step failed (Newton %d iterations, max residual %g)", it, rmax);
+    return status;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// batched ensemble
+struct sw2gpu_batch {
+    std::vector<sw2gpu_ctx*> ctxs;
+    cudaStream_t stream = nullptr;
+};
+
+extern "C" {
+
+int sw2gpu_batch_create(sw2gpu_ctx** ctxs, int32_t n, void* stream, sw2gpu_batch** out) {
+    if (!ctxs || n <= 0 || !out) return fail(SW2GPU_E_ARG, "bad batch arguments");
+    auto* b = new sw2gpu_batch();
+    b->ctxs.assign(ctxs, ctxs + n);
+    b->stream = (cudaStream_t)stream;
+    *out = b;
+    return SW2GPU_OK;
+}
+
+int sw2gpu_batch_step(sw2gpu_batch* b, const double* dt, const double* const* series, sw2gpu_stats* stats) {
+    if (!b || !dt) return fail(SW2GPU_E_ARG, "bad batch arguments");
+    int worst = SW2GPU_OK;
+    for (size_t i = 0; i < b->ctxs.size(); i++) {
+        int rc = sw2gpu_step(b->ctxs[i], dt[i], series ? series[i] : nullptr, stats ? stats + i : nullptr);
+        if (rc != SW2GPU_OK && worst == SW2GPU_OK) worst = rc;
+    }
+    return worst;
+}
+
+int sw2gpu_batch_destroy(sw2gpu_batch* b) {
+    delete b;
+    return SW2GPU_OK;
+}
+
+}  // extern "C"

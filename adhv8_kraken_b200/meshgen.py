@@ -123,6 +123,13 @@ def bumpy_basin(npoints: int, seed: int, size: float = 20000.0, slope: float = 5
     tri[cross < 0] = tri[cross < 0][:, [0, 2, 1]]
     cross = np.abs(cross)
     tri = tri[cross > 1e-6 * (size / math.sqrt(npoints)) ** 2]
+    # drop points no triangle uses (every node must carry a diagonal block)
+    used = np.zeros(x.shape[0], bool)
+    used[tri.ravel()] = True
+    if not used.all():
+        remap = np.cumsum(used) - 1
+        tri = remap[tri].astype(np.int32)
+        x, y = x[used].copy(), y[used].copy()
     # renumber elements by the Morton code of their centroid
     cx = x[tri].mean(axis=1)
     cy = y[tri].mean(axis=1)
@@ -132,9 +139,15 @@ def bumpy_basin(npoints: int, seed: int, size: float = 20000.0, slope: float = 5
     wid = rng.uniform(200.0, 1500.0, nbumps) * scale
     cxb = rng.uniform(0.0, size, nbumps)
     cyb = rng.uniform(0.0, size, nbumps)
+    # bumps fade out within 10% of the west (inflow) and east (tailwater) edges:
+    # a dry node on a NB VEL edge makes the inflow velocity q n / max(h_avg, eps)
+    # unbounded (src/fe/sw2/fe_sw2_boundary_resid.c:212-219) and no time step converges
+    xs = np.minimum(x, size - x) / size
+    taper = np.clip((xs - 0.05) / 0.05, 0.0, 1.0)
+    taper = taper * taper * (3.0 - 2.0 * taper)
     z = -slope * x
     for a, w, u, v in zip(amp, wid, cxb, cyb):
-        z = z + a * np.exp(-((x - u) ** 2 + (y - v) ** 2) / (2.0 * w * w))
+        z = z + taper * a * np.exp(-((x - u) ** 2 + (y - v) ** 2) / (2.0 * w * w))
     h0 = wse0 - z
     # per-element roughness classes
     n_elem = np.exp(rng.normal(math.log(n_median), n_sigma, tri.shape[0]))

@@ -1,0 +1,191 @@
+"""Python front end of the B200 SW2 library (``libsw2gpu.so``, C ABI in ``include/sw2gpu.h``).
+
+Mirrors the reference's SW2 plug-in interface:
+
+* :meth:`SW2GPU.step`   -- ``fe_sw2_solve`` (src/fe/sw2/fe_sw2_solve.c:30-57): one implicit
+  time step, returning YES/NO semantics through an exception-free status code;
+* :meth:`SW2GPU.resid`  -- ``fe_sw2_resid``;  :meth:`SW2GPU.load` -- ``fe_sw2_load``;
+* :func:`run`           -- the dt-retry loop of ``adh_run_func_``/``fe_main``
+  (src/main/adh_func.c:535-549): a failed step is retried with dt * 0.25 (tc_scale).
+
+There is no CPU fallback: if the CUDA library or a GPU is missing, construction fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import capi
+from .capi import MeshArrays, Stats, c_double_p, c_int32_p, make_params
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsw2gpu.so")
+
+_lib = None
+
+SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_destroy", "sw2gpu_set_state",
+           "sw2gpu_get_state", "sw2gpu_get_wd_flag", "sw2gpu_set_wd_flag", "sw2gpu_step", "sw2gpu_set_dt",
+           "sw2gpu_resid", "sw2gpu_load", "sw2gpu_linear_solve", "sw2gpu_batch_create", "sw2gpu_batch_step",
+           "sw2gpu_batch_destroy"]
+
+
+class SW2Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"sw2gpu error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads the in-tree CUDA library (built by ``adhv8_kraken_b200/build.py``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is not built; run python adhv8_kraken_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.sw2gpu_last_error.restype = C.c_char_p
+        L.sw2gpu_create.argtypes = [vp, vp, vp, C.POINTER(vp)]
+        L.sw2gpu_destroy.argtypes = [vp]
+        L.sw2gpu_set_state.argtypes = [vp, C.c_int, c_double_p, c_double_p, c_double_p]
+        L.sw2gpu_get_state.argtypes = [vp, C.c_int, c_double_p, c_double_p, c_double_p]
+        L.sw2gpu_get_wd_flag.argtypes = [vp, c_int32_p]
+        L.sw2gpu_set_wd_flag.argtypes = [vp, c_int32_p]
+        L.sw2gpu_step.argtypes = [vp, C.c_double, c_double_p, vp]
+        L.sw2gpu_set_dt.argtypes = [vp, C.c_double, c_double_p]
+        L.sw2gpu_resid.argtypes = [vp, c_double_p]
+        L.sw2gpu_load.argtypes = [vp, c_int32_p, c_int32_p, c_int32_p, c_double_p, c_double_p]
+        L.sw2gpu_linear_solve.argtypes = [vp, c_double_p, c_double_p, c_double_p, c_int32_p]
+        L.sw2gpu_batch_create.argtypes = [C.POINTER(vp), C.c_int32, vp, C.POINTER(vp)]
+        L.sw2gpu_batch_step.argtypes = [vp, c_double_p, C.POINTER(c_double_p), vp]
+        L.sw2gpu_batch_destroy.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise SW2Error(rc, lib().sw2gpu_last_error().decode())
+
+
+def _dp(a):
+    return a.ctypes.data_as(c_double_p)
+
+
+def _ip(a):
+    return a.ctypes.data_as(c_int32_p)
+
+
+class SW2GPU:
+    """One SW2 model resident on the GPU (mesh, BCSR pattern and three time levels)."""
+
+    def __init__(self, model, precision: int = capi.SW2GPU_FP64, precond: int = capi.SW2GPU_PREC_BJACOBI,
+                 lin_rtol: float = 1e-5, lin_atol: float = 1e-10, stream: int = 0):
+        self.model = model
+        self.arrays = MeshArrays(model)
+        self.params = make_params(model, precision=precision, precond=precond, lin_rtol=lin_rtol,
+                                  lin_atol=lin_atol)
+        self.V, self.T = model.nnodes, model.nelems2d
+        h = C.c_void_p()
+        _check(lib().sw2gpu_create(C.byref(self.arrays.mesh), C.byref(self.params),
+                                   C.c_void_p(stream) if stream else None, C.byref(h)))
+        self.h = h
+        n = C.c_int32()
+        _check(lib().sw2gpu_load(self.h, C.byref(n), None, None, None, None))
+        self.nnzb = n.value
+        self.t = model.t0
+        for lvl in range(3):
+            self.set_state(lvl, model.h0, model.u0, model.v0)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sw2gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, level, h, u, v):
+        h, u, v = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, u, v))
+        _check(lib().sw2gpu_set_state(self.h, level, _dp(h), _dp(u), _dp(v)))
+
+    def get_state(self, level=0):
+        h, u, v = (np.zeros(self.V) for _ in range(3))
+        _check(lib().sw2gpu_get_state(self.h, level, _dp(h), _dp(u), _dp(v)))
+        return h, u, v
+
+    def get_wd(self):
+        wd = np.zeros(self.T, np.int32)
+        _check(lib().sw2gpu_get_wd_flag(self.h, _ip(wd)))
+        return wd
+
+    def set_wd(self, wd):
+        wd = np.ascontiguousarray(wd, dtype=np.int32)
+        _check(lib().sw2gpu_set_wd_flag(self.h, _ip(wd)))
+
+    def set_dt(self, dt, series):
+        s = np.ascontiguousarray(series, dtype=np.float64)
+        _check(lib().sw2gpu_set_dt(self.h, dt, _dp(s) if s.size else None))
+
+    def resid(self):
+        r = np.zeros(3 * self.V)
+        _check(lib().sw2gpu_resid(self.h, _dp(r)))
+        return r
+
+    def load(self):
+        """FD Jacobian: (row_ptr, col, val[nnzb, 3, 3]) and the residual after the tiny-diagonal fix."""
+        rp = np.zeros(self.V + 1, np.int32)
+        col = np.zeros(self.nnzb, np.int32)
+        val = np.zeros(9 * self.nnzb)
+        r = np.zeros(3 * self.V)
+        n = C.c_int32()
+        _check(lib().sw2gpu_load(self.h, C.byref(n), _ip(rp), _ip(col), _dp(val), _dp(r)))
+        return rp, col, val.reshape(-1, 3, 3), r
+
+    def linear_solve(self, val, rhs):
+        val = np.ascontiguousarray(val, dtype=np.float64).reshape(-1)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        x = np.zeros(3 * self.V)
+        its = C.c_int32()
+        rc = lib().sw2gpu_linear_solve(self.h, _dp(val), _dp(rhs), _dp(x), C.byref(its))
+        return x, its.value, rc
+
+    def step(self, dt=None, t=None):
+        """One time step over [t, t + dt]; returns the stats dict (status 0 = YES)."""
+        dt = self.model.dt if dt is None else dt
+        t = self.t if t is None else t
+        s = self.model.series_values(t, t + dt)
+        st = Stats()
+        rc = lib().sw2gpu_step(self.h, dt, _dp(s) if s.size else None, C.byref(st))
+        if rc in (capi.SW2GPU_E_ARG, capi.SW2GPU_E_CUDA, capi.SW2GPU_E_NOMEM, capi.SW2GPU_E_TIMEOUT):
+            _check(rc)
+        if rc == 0:
+            self.t = t + dt
+        d = st.as_dict()
+        d["status"] = rc
+        return d
+
+
+def run(solver: SW2GPU, nsteps: int, dt: float = None, max_retries: int = 8, callback=None):
+    """Time loop with the reference's failure contract: a step that returns NO is
+    retried from the old state with dt * 0.25 (src/tools/tc_scale.c:3-17)."""
+    dt = solver.model.dt if dt is None else dt
+    out = []
+    for k in range(nsteps):
+        d = dt
+        for _ in range(max_retries + 1):
+            st = solver.step(dt=d)
+            if st["status"] == 0:
+                break
+            d *= 0.25
+        else:
+            raise SW2Error(st["status"], f"step {k} failed after {max_retries} dt reductions")
+        st["dt"] = d
+        out.append(st)
+        if callback:
+            callback(k, st)
+    return out

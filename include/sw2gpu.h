@@ -116,6 +116,8 @@ int sw2gpu_destroy(sw2gpu_ctx *ctx);
 int sw2gpu_set_state(sw2gpu_ctx *ctx, int level, const double *h, const double *u, const double *v);
 int sw2gpu_get_state(sw2gpu_ctx *ctx, int level, double *h, double *u, double *v);
 int sw2gpu_get_wd_flag(sw2gpu_ctx *ctx, int32_t *wd_flag);
+/* Overrides the element wet/dry flags (normally set by the step's fe_sw2_init). */
+int sw2gpu_set_wd_flag(sw2gpu_ctx *ctx, const int32_t *wd_flag);
 
 /* One implicit time step: time-level shift (fe_sw2, src/fe/sw2/fe_sw2.c:43-50) then the
  * damped Newton loop (fe_newton).  `series` holds the step-averaged value of every BC

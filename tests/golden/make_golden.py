@@ -1,0 +1,124 @@
+"""Generates the golden fixtures of this directory by running the reference AdH
+executable (built from the reference sources by ``oracle/ref/build_ref.py``).
+
+Run in a container where the reference sources are present::
+
+    python oracle/ref/build_ref.py && python tests/golden/make_golden.py
+
+Fixtures (numpy ``.npz``):
+
+* ``channel_ref.npz`` -- the rectangular channel (100 x 20 squares, 4,000 triangles,
+  NB VEL inflow 0.5 m^2/s, NB OTW tailwater, dt = 10 s), 20 steps: Newton iterations
+  of every step, the state after steps 1, 5, 10, 20, and the state / residual /
+  Jacobian (sorted BCSR) at the first fe_sw2_load call.
+* ``basin_ref.npz`` -- a seeded Delaunay basin with dry bump tops (wet/dry fronts),
+  8 steps: Newton iterations, state and wd flags after every step, and the first
+  fe_sw2_load state / residual / Jacobian.
+
+Each fixture stores a fingerprint of the generated model so a generator change is
+detected instead of silently comparing different problems.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", ".."))
+
+from adhv8_kraken_b200 import meshgen  # noqa: E402
+from oracle.ref_run import run_reference  # noqa: E402
+
+
+def fingerprint(m) -> str:
+    h = hashlib.sha256()
+    for a in (m.x, m.y, m.z, m.tri, m.tri_mat, m.edges, m.edge_string, m.h0, m.u0, m.v0):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def pattern(m):
+    """Sorted BCSR pattern of the model (element and edge node pairs)."""
+    rows = [set() for _ in range(m.nnodes)]
+    for t in m.tri:
+        for a in t:
+            rows[a].update(int(b) for b in t)
+    for e in m.edges:
+        for a in e:
+            rows[a].update(int(b) for b in e)
+    rp = np.zeros(m.nnodes + 1, np.int32)
+    cols = []
+    for i, r in enumerate(rows):
+        c = sorted(r)
+        cols.extend(c)
+        rp[i + 1] = rp[i] + len(c)
+    return rp, np.array(cols, np.int32)
+
+
+def ref_jacobian_to_bcsr(m, L):
+    rp, col = pattern(m)
+    V = m.nnodes
+    val = np.zeros((len(col), 3, 3))
+    diag = L["diag"].reshape(V, 3, 3)
+    vals = L["vals"].reshape(-1, 3, 3)
+    k = 0
+    for i in range(V):
+        lookup = {int(c): rp[i] + n for n, c in enumerate(col[rp[i]:rp[i + 1]])}
+        val[lookup[i]] = diag[i]
+        for _ in range(L["rowsz"][i]):
+            val[lookup[int(L["cols"][k])]] = vals[k]
+            k += 1
+    return rp, col, val
+
+
+def load_record(m, L, prefix):
+    rp, col, val = ref_jacobian_to_bcsr(m, L)
+    out = {}
+    for key in ("h", "u", "v", "h1", "u1", "v1", "h2", "u2", "v2", "resid"):
+        out[f"{prefix}_{key}"] = L[key]
+    out[f"{prefix}_wd"] = L["wd"]
+    out[f"{prefix}_t"] = np.array([L["t"], L["dt"]])
+    out[f"{prefix}_rowptr"] = rp
+    out[f"{prefix}_col"] = col
+    out[f"{prefix}_val"] = val
+    return out
+
+
+def channel():
+    m = meshgen.channel()
+    ref = run_reference(m, nsteps=20, loads=1)
+    out = {"fingerprint": np.array(fingerprint(m)),
+           "newton_its": np.array([s["newton_its"] for s in ref["steps"]], np.int32),
+           "t": np.array([s["t"] for s in ref["steps"]]), "dt": np.array([s["dt"] for s in ref["steps"]])}
+    for k in (1, 5, 10, 20):
+        s = ref["steps"][k - 1]
+        out[f"step{k}_h"], out[f"step{k}_u"], out[f"step{k}_v"] = s["h"], s["u"], s["v"]
+    out.update(load_record(m, ref["loads"][0], "load0"))
+    np.savez_compressed(os.path.join(HERE, "channel_ref.npz"), **out)
+
+
+def basin_model():
+    return meshgen.bumpy_basin(700, seed=11, size=2000.0, nsteps=8, dt=5.0, nbins=3, name="basin")
+
+
+def basin():
+    m = basin_model()
+    ref = run_reference(m, nsteps=8, loads=1)
+    out = {"fingerprint": np.array(fingerprint(m)),
+           "newton_its": np.array([s["newton_its"] for s in ref["steps"]], np.int32),
+           "t": np.array([s["t"] for s in ref["steps"]]), "dt": np.array([s["dt"] for s in ref["steps"]])}
+    for k, s in enumerate(ref["steps"], 1):
+        out[f"step{k}_h"], out[f"step{k}_u"], out[f"step{k}_v"] = s["h"], s["u"], s["v"]
+        out[f"step{k}_wd"] = s["wd"]
+    out.update(load_record(m, ref["loads"][0], "load0"))
+    np.savez_compressed(os.path.join(HERE, "basin_ref.npz"), **out)
+
+
+if __name__ == "__main__":
+    channel()
+    basin()
+    for f in ("channel_ref.npz", "basin_ref.npz"):
+        print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,0 +1,26 @@
+"""Shared test helpers: the golden models and state loaders."""
+import numpy as np
+
+from adhv8_kraken_b200 import meshgen
+
+
+def channel_model():
+    return meshgen.channel()
+
+
+def basin_model():
+    return meshgen.bumpy_basin(700, seed=11, size=2000.0, nsteps=8, dt=5.0, nbins=3, name="basin")
+
+
+def set_load_state(solver, model, ref, prefix="load0"):
+    """Puts a solver (oracle or GPU) in the state the reference built its Jacobian at."""
+    solver.set_state(0, ref[f"{prefix}_h"], ref[f"{prefix}_u"], ref[f"{prefix}_v"])
+    solver.set_state(1, ref[f"{prefix}_h1"], ref[f"{prefix}_u1"], ref[f"{prefix}_v1"])
+    solver.set_state(2, ref[f"{prefix}_h2"], ref[f"{prefix}_u2"], ref[f"{prefix}_v2"])
+    t, dt = ref[f"{prefix}_t"]
+    solver.set_dt(dt, model.series_values(t, t + dt))
+    solver.set_wd(ref[f"{prefix}_wd"])
+
+
+def fields(h, u, v):
+    return {"h": h, "uh": h * u, "vh": h * v}

@@ -1,0 +1,110 @@
+"""GPU parity: the B200 library through its C ABI against the oracle and the
+reference fixtures.  Tolerances (relative to the field's max magnitude):
+residual 1e-12, Jacobian 1e-7 (central differences amplify round-off by ~1e8),
+time-stepped state 1e-10 per step (h, uh, vh), Newton iterations within +-1."""
+import numpy as np
+import pytest
+
+from adhv8_kraken_b200 import capi, meshgen
+from adhv8_kraken_b200.sw2 import SW2GPU, run
+from conftest import relerr
+from helpers import basin_model, channel_model, fields, set_load_state
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", ["channel", "basin"])
+def test_residual_and_jacobian_match_reference(case, channel_ref, basin_ref):
+    model, ref = (channel_model(), channel_ref) if case == "channel" else (basin_model(), basin_ref)
+    g = SW2GPU(model)
+    set_load_state(g, model, ref)
+    g.resid()
+    rp, col, val, r = g.load()
+    assert np.array_equal(rp, ref["load0_rowptr"]) and np.array_equal(col, ref["load0_col"])
+    assert relerr(r, ref["load0_resid"]) <= 1e-12
+    assert relerr(val, ref["load0_val"]) <= 1e-7
+
+
+def test_residual_and_jacobian_match_oracle_on_random_wet_dry_states():
+    model = basin_model()
+    rng = np.random.default_rng(3)
+    for trial in range(3):
+        h = model.h0 + rng.normal(0, 0.05, model.nnodes)
+        u = rng.normal(0, 0.2, model.nnodes)
+        v = rng.normal(0, 0.2, model.nnodes)
+        ho = model.h0 + rng.normal(0, 0.05, model.nnodes)
+        g, o = SW2GPU(model), Oracle(model)
+        for s in (g, o):
+            s.set_state(0, h, u, v)
+            s.set_state(1, ho, 0.5 * u, 0.5 * v)
+            s.set_state(2, ho, 0.25 * u, 0.25 * v)
+            s.set_dt(5.0, model.series_values(0.0, 5.0))
+        wd = o.wdflag()
+        g.set_wd(wd)
+        assert (wd > 0).sum() > 50
+        rg, ro = g.resid(), o.resid()
+        assert relerr(rg, ro) <= 1e-12, trial
+        _, _, vg, rg2 = g.load()
+        vo, ro2 = o.load()
+        assert relerr(rg2, ro2) <= 1e-12
+        assert relerr(vg.reshape(-1), vo.reshape(-1)) <= 1e-7
+        hg, ug, vvg = g.get_state(0)
+        ho_, uo_, vo_ = o.get_state(0)
+        assert np.array_equal(ug, uo_) and np.array_equal(vvg, vo_)   # dry-node velocity zeroing
+
+
+def test_linear_solve_matches_direct_solve(channel_ref):
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    model = channel_model()
+    g = SW2GPU(model, lin_rtol=1e-13, lin_atol=0.0)
+    V = model.nnodes
+    A = sp.bsr_matrix((channel_ref["load0_val"], channel_ref["load0_col"], channel_ref["load0_rowptr"]),
+                      shape=(3 * V, 3 * V)).tocsc()
+    b = channel_ref["load0_resid"]
+    x, its, rc = g.linear_solve(channel_ref["load0_val"], b)
+    assert rc == 0 and its > 0
+    assert relerr(x, spla.spsolve(A, b)) <= 1e-9
+
+
+def _run_against(model, ref, nsteps, check_every, precision=capi.SW2GPU_FP64, tol=1e-10, wd=False, **kw):
+    g = SW2GPU(model, precision=precision, **kw)
+    worst = 0.0
+    for k in range(nsteps):
+        st = g.step(dt=ref["dt"][k], t=ref["t"][k])
+        assert st["status"] == 0, st
+        assert abs(st["newton_its"] - int(ref["newton_its"][k])) <= 1, (k, st["newton_its"], ref["newton_its"][k])
+        if (k + 1) in check_every:
+            got = fields(*g.get_state(0))
+            exp = fields(ref[f"step{k+1}_h"], ref[f"step{k+1}_u"], ref[f"step{k+1}_v"])
+            for f in got:
+                e = relerr(got[f], exp[f])
+                worst = max(worst, e)
+                assert e <= tol, (k, f, e)
+            if wd:
+                assert np.array_equal(g.get_wd(), ref[f"step{k+1}_wd"])
+    return worst
+
+
+def test_channel_run_matches_reference(channel_ref):
+    _run_against(channel_model(), channel_ref, 20, (1, 5, 10, 20))
+
+
+def test_basin_run_matches_reference(basin_ref):
+    _run_against(basin_model(), basin_ref, 8, range(1, 9), wd=True)
+
+
+def test_mixed_precision_channel_within_1e8(channel_ref):
+    _run_against(channel_model(), channel_ref, 20, (1, 5, 10, 20), precision=capi.SW2GPU_MIXED, tol=1e-8)
+
+
+def test_reruns_are_bitwise_identical():
+    model = basin_model()
+    outs = []
+    for _ in range(2):
+        g = SW2GPU(model)
+        for _ in range(3):
+            assert g.step()["status"] == 0
+        outs.append(np.concatenate(g.get_state(0)))
+    assert np.array_equal(outs[0], outs[1])

@@ -1,0 +1,72 @@
+"""The CPU oracle against fixtures produced by the reference executable itself."""
+import numpy as np
+import pytest
+
+from golden.make_golden import fingerprint
+from helpers import basin_model, channel_model, fields, set_load_state
+from conftest import relerr
+from oracle.oracle import Oracle
+
+
+def test_fixture_models_are_current(channel_ref, basin_ref):
+    assert str(channel_ref["fingerprint"]) == fingerprint(channel_model())
+    assert str(basin_ref["fingerprint"]) == fingerprint(basin_model())
+
+
+@pytest.mark.parametrize("case", ["channel", "basin"])
+def test_oracle_residual_and_jacobian_match_reference(case, channel_ref, basin_ref):
+    model, ref = (channel_model(), channel_ref) if case == "channel" else (basin_model(), basin_ref)
+    o = Oracle(model)
+    set_load_state(o, model, ref)
+    o.resid()
+    val, r = o.load()
+    rp, col = o.pattern()
+    assert np.array_equal(rp, ref["load0_rowptr"]) and np.array_equal(col, ref["load0_col"])
+    # residual: same arithmetic as the reference up to the summation round-off
+    assert relerr(r, ref["load0_resid"]) <= 1e-13
+    # Jacobian: central differences amplify residual round-off by 1/eps ~ 1e8
+    assert relerr(val, ref["load0_val"]) <= 1e-7
+    if case == "channel":
+        assert relerr(val, ref["load0_val"]) == 0.0 and relerr(r, ref["load0_resid"]) == 0.0
+
+
+def test_oracle_channel_run_matches_reference(channel_ref):
+    m = channel_model()
+    o = Oracle(m)
+    for k in range(20):
+        st = o.step(dt=channel_ref["dt"][k], t=channel_ref["t"][k])
+        assert st["status"] == 0
+        assert st["newton_its"] == channel_ref["newton_its"][k]
+        if k + 1 in (1, 5, 10, 20):
+            got = fields(*o.get_state(0))
+            exp = fields(channel_ref[f"step{k+1}_h"], channel_ref[f"step{k+1}_u"], channel_ref[f"step{k+1}_v"])
+            for f in got:
+                assert relerr(got[f], exp[f]) <= 1e-10, (k, f)
+
+
+def test_oracle_basin_run_matches_reference(basin_ref):
+    m = basin_model()
+    o = Oracle(m)
+    for k in range(8):
+        st = o.step(dt=basin_ref["dt"][k], t=basin_ref["t"][k])
+        assert st["status"] == 0
+        assert st["newton_its"] == basin_ref["newton_its"][k]
+        got = fields(*o.get_state(0))
+        exp = fields(basin_ref[f"step{k+1}_h"], basin_ref[f"step{k+1}_u"], basin_ref[f"step{k+1}_v"])
+        for f in got:
+            assert relerr(got[f], exp[f]) <= 1e-10, (k, f)
+        assert np.array_equal(o.get_wd(), basin_ref[f"step{k+1}_wd"])
+
+
+def test_oracle_lake_at_rest_stays_at_rest():
+    """Flat water surface over a bumpy bed with no inflow: the reference's lake-at-rest
+    invariant (src/initio/test_cases.c:288-340) -- velocities stay ~0, surface stays flat."""
+    from adhv8_kraken_b200 import meshgen
+    m = meshgen.bumpy_basin(400, seed=5, size=1500.0, nsteps=3, dt=20.0, nbins=1, q_start=0.0, q_peak=0.0)
+    o = Oracle(m)
+    for _ in range(3):
+        assert o.step()["status"] == 0
+    h, u, v = o.get_state(0)
+    wet = h > 0.05
+    assert np.abs(u[wet]).max() < 1e-6 and np.abs(v[wet]).max() < 1e-6
+    assert np.abs((h + m.z - 2.0)[wet]).max() < 1e-7
