@@ -59,7 +59,8 @@ class Stats(C.Structure):
         ("status", C.c_int32), ("newton_its", C.c_int32), ("linear_its", C.c_int32),
         ("linesearch_cuts", C.c_int32), ("resid_max", C.c_double), ("resid_l2", C.c_double),
         ("inc_max", C.c_double), ("device_ms", C.c_double), ("kernel_launches", C.c_int32),
-        ("wd_elems", C.c_int32),
+        ("wd_elems", C.c_int32), ("jac_ms", C.c_double), ("krylov_ms", C.c_double),
+        ("resid_ms", C.c_double), ("other_ms", C.c_double),
     ]
 
     def as_dict(self):

@@ -129,11 +129,12 @@ struct KrylovArgs {
     KrylovCtl* ctl;
 };
 
-// y = Dinv_i * sum_j A'_ij x_j for node row i, with x_j = xa_j - alpha * xb_j when xb != null
+// y = Dinv_i * sum_j A'_ij x_j for node row i, with x_j = xa_j - alpha * xb_j when xb != null.
+// Products and sums are formed in the matrix type MT (FP32 accumulation on the mixed path).
 template <typename MT, typename VT>
 __device__ __forceinline__ void row_apply(int i, const int* rowptr, const int* col, const MT* A, const MT* Dinv,
                                           const VT* xa, const VT* xb, VT alpha, VT y[3]) {
-    VT acc0 = 0, acc1 = 0, acc2 = 0;
+    MT acc0 = 0, acc1 = 0, acc2 = 0;
     const int k1 = rowptr[i + 1];
     for (int k = rowptr[i]; k < k1; k++) {
         const int j = col[k];
@@ -144,17 +145,20 @@ __device__ __forceinline__ void row_apply(int i, const int* rowptr, const int* c
             x1 -= alpha * ldv(xb + 3 * j + 1);
             x2 -= alpha * ldv(xb + 3 * j + 2);
         }
-        acc0 += (VT)__ldg(a + 0) * x0 + (VT)__ldg(a + 1) * x1 + (VT)__ldg(a + 2) * x2;
-        acc1 += (VT)__ldg(a + 3) * x0 + (VT)__ldg(a + 4) * x1 + (VT)__ldg(a + 5) * x2;
-        acc2 += (VT)__ldg(a + 6) * x0 + (VT)__ldg(a + 7) * x1 + (VT)__ldg(a + 8) * x2;
+        const MT m0 = (MT)x0, m1 = (MT)x1, m2 = (MT)x2;
+        acc0 += __ldg(a + 0) * m0 + __ldg(a + 1) * m1 + __ldg(a + 2) * m2;
+        acc1 += __ldg(a + 3) * m0 + __ldg(a + 4) * m1 + __ldg(a + 5) * m2;
+        acc2 += __ldg(a + 6) * m0 + __ldg(a + 7) * m1 + __ldg(a + 8) * m2;
     }
     const MT* d = Dinv + (size_t)i * 9;
-    y[0] = (VT)__ldg(d + 0) * acc0 + (VT)__ldg(d + 1) * acc1 + (VT)__ldg(d + 2) * acc2;
-    y[1] = (VT)__ldg(d + 3) * acc0 + (VT)__ldg(d + 4) * acc1 + (VT)__ldg(d + 5) * acc2;
-    y[2] = (VT)__ldg(d + 6) * acc0 + (VT)__ldg(d + 7) * acc1 + (VT)__ldg(d + 8) * acc2;
+    y[0] = (VT)(__ldg(d + 0) * acc0 + __ldg(d + 1) * acc1 + __ldg(d + 2) * acc2);
+    y[1] = (VT)(__ldg(d + 3) * acc0 + __ldg(d + 4) * acc1 + __ldg(d + 5) * acc2);
+    y[2] = (VT)(__ldg(d + 6) * acc0 + __ldg(d + 7) * acc1 + __ldg(d + 8) * acc2);
 }
 
-// MT: matrix / preconditioner storage and SpMV accumulation type; VT: Krylov vector type.
+// MT: matrix / preconditioner storage and SpMV accumulation type; VT: Krylov vector type
+// (FP64 on both paths: FP32 vectors let the recursively updated residual drift away from
+// the true one and the iteration stagnates).
 template <typename MT, typename VT>
 __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const MT* __restrict__ A,
                                                             const MT* __restrict__ Dinv, VT* __restrict__ b,

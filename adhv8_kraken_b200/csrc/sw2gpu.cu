@@ -92,7 +92,6 @@ struct sw2gpu_ctx {
     DBuf<float> val32, dinv32;
     DBuf<double> dinv64;
     DBuf<double> kv64[7];
-    DBuf<float> kv32[7];
     DBuf<double> part;
     DBuf<KrylovCtl> ctl;
     DBuf<Norms> npart, norms;
@@ -103,9 +102,15 @@ struct sw2gpu_ctx {
     int krylov_grid = 0;
     int launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // per-phase device timing: event pairs recorded around the main kernels of a step
+    static constexpr int kMaxPhases = 512;
+    std::vector<cudaEvent_t> pev;
+    std::vector<int> pkind;
+    int nphase = 0;
     DevMesh dm{};
 
     ~sw2gpu_ctx() {
+        for (auto e : pev) cudaEventDestroy(e);
         if (norms_h) cudaFreeHost(norms_h);
         if (ctl_h) cudaFreeHost(ctl_h);
         if (ev0) cudaEventDestroy(ev0);
@@ -136,6 +141,24 @@ struct sw2gpu_ctx {
 };
 
 namespace {
+
+enum PhaseKind { kPhJac = 0, kPhKrylov = 1, kPhResid = 2 };
+
+// phase timer: brackets launches with an event pair when the pool has room
+struct Phase {
+    sw2gpu_ctx* c;
+    int slot;
+    Phase(sw2gpu_ctx* ctx, int kind) : c(ctx), slot(-1) {
+        if (c->nphase < sw2gpu_ctx::kMaxPhases && !c->pev.empty()) {
+            slot = c->nphase++;
+            c->pkind[slot] = kind;
+            cudaEventRecord(c->pev[2 * slot], c->stream);
+        }
+    }
+    ~Phase() {
+        if (slot >= 0) cudaEventRecord(c->pev[2 * slot + 1], c->stream);
+    }
+};
 
 template <typename T>
 int up(DBuf<T>& b, const std::vector<T>& v, cudaStream_t st) {
@@ -192,6 +215,7 @@ int launch_resid(sw2gpu_ctx* c) {
     State s = c->state();
     PhysParams P = c->phys();
     const int n = c->T + c->E;
+    Phase ph(c, kPhResid);
     k_resid_elem<<<nblk(std::max(n, 1), 128), 128, 0, c->stream>>>(c->dm, s, P, c->sc.p, c->sx.p, c->sy.p);
     k_resid_gather<<<nblk(std::max(c->V, 1), kGatherThreads), kGatherThreads, 0, c->stream>>>(
         c->dm, s, c->sc.p, c->sx.p, c->sy.p, c->R.p, c->sol.p, c->npart.p, c->ncounter.p, c->norms.p);
@@ -210,7 +234,10 @@ int read_norms(sw2gpu_ctx* c, Norms& out) {
 int launch_jacobian(sw2gpu_ctx* c) {
     State s = c->state();
     PhysParams P = c->phys();
-    if (c->T) k_jac_elem<<<nblk(c->T, kJacElems), kJacThreads, 0, c->stream>>>(c->dm, s, P, c->jslots.p);
+    if (c->T) {
+        Phase ph(c, kPhJac);
+        k_jac_elem<<<nblk(c->T, kJacElems), kJacThreads, 0, c->stream>>>(c->dm, s, P, c->jslots.p);
+    }
     if (c->E) k_jac_edge<<<nblk(6LL * c->E, 128), 128, 0, c->stream>>>(c->dm, s, P, c->jslots.p);
     k_jac_gather<<<nblk(9LL * c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->jslots.p, c->val.p);
     c->launches += 2 + (c->E ? 1 : 0);
@@ -270,13 +297,14 @@ int launch_linear(sw2gpu_ctx* c, int apply_inc, int* its, int* converged) {
     K.part = c->part.p;
     K.ctl = c->ctl.p;
     dim3 grid(c->krylov_grid), block(kKrylovThreads);
+    Phase ph(c, kPhKrylov);
     if (mixed) {
         const float* A = c->val32.p;
         const float* D = c->dinv32.p;
-        float *b = c->kv32[0].p, *uu = c->kv32[1].p, *r = c->kv32[2].p, *q = c->kv32[3].p, *pp = c->kv32[4].p,
-              *Ap = c->kv32[5].p, *As = c->kv32[6].p;
+        double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
+               *Ap = c->kv64[5].p, *As = c->kv64[6].p;
         void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As};
-        CK(cudaLaunchCooperativeKernel((void*)k_bicgstab<float, float>, grid, block, args, 0, c->stream));
+        CK(cudaLaunchCooperativeKernel((void*)k_bicgstab<float, double>, grid, block, args, 0, c->stream));
     } else {
         const double* A = c->val.p;
         const double* D = c->dinv64.p;
@@ -511,11 +539,10 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     if (prm->precision == SW2GPU_MIXED) {
         rc |= zalloc(c->val32, 9ull * nnzb, st);
         rc |= zalloc(c->dinv32, 9ull * V, st);
-        for (auto& b : c->kv32) rc |= zalloc(b, 3ull * V, st);
     } else {
         rc |= zalloc(c->dinv64, 9ull * V, st);
-        for (auto& b : c->kv64) rc |= zalloc(b, 3ull * V, st);
     }
+    for (auto& b : c->kv64) rc |= zalloc(b, 3ull * V, st);
     rc |= zalloc(c->ctl, 1, st);
     rc |= zalloc(c->ncounter, 1, st);
     rc |= zalloc(c->singular, 1, st);
@@ -527,7 +554,7 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     int sms = 0, per_sm = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     if (prm->precision == SW2GPU_MIXED)
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<float, float>, kKrylovThreads, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<float, double>, kKrylovThreads, 0));
     else
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double>, kKrylovThreads, 0));
     per_sm = std::min(per_sm, 4);
@@ -538,6 +565,9 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     CK(cudaMallocHost(&c->ctl_h, sizeof(KrylovCtl)));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
+    c->pev.resize(2 * sw2gpu_ctx::kMaxPhases);
+    c->pkind.resize(sw2gpu_ctx::kMaxPhases);
+    for (auto& e : c->pev) CK(cudaEventCreate(&e));
     DevMesh& d = c->dm;
     d.V = V; d.T = T; d.E = E; d.nnzb = nnzb;
     d.x = c->x.p; d.y = c->y.p; d.z = c->z.p;
@@ -649,6 +679,7 @@ int sw2gpu_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* st
     if (!c || !(dt > 0.0)) return fail(SW2GPU_E_ARG, "bad context or dt");
     const sw2gpu_params& p = c->p;
     c->launches = 0;
+    c->nphase = 0;
     c->dt = dt;
     CK(cudaEventRecord(c->ev0, c->stream));
     // fe_sw2: older <- old <- current (level rotation, no copies)
@@ -678,7 +709,10 @@ int sw2gpu_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* st
         if ((rc = read_norms(c, nm))) return rc;   // also completes the Krylov control read
         if (c->ctl_h->err) return fail(SW2GPU_E_TIMEOUT, "Krylov grid barrier wait ran out");
         lin_total += c->ctl_h->iterations;
-        if (!c->ctl_h->converged) solv_ok = false;
+        // the plain path fails the step when BiCGSTAB hits max_lin_it (solv_bcgstab.c:280-292);
+        // on the mixed path the FP32 inner solve is a correction refined by the FP64 Newton
+        // loop, so its last iterate is accepted (the reference's force_lin_it behaviour)
+        if (!c->ctl_h->converged && p.precision != SW2GPU_MIXED) solv_ok = false;
         rmax = nm.rmax;
         l2 = std::sqrt(nm.l2sum / n3);
         imax = nm.imax;
@@ -718,6 +752,15 @@ int sw2gpu_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* st
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         stats->device_ms = ms;
         stats->kernel_launches = c->launches;
+        double ph[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < c->nphase; k++) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, c->pev[2 * k], c->pev[2 * k + 1]) == cudaSuccess) ph[c->pkind[k]] += t;
+        }
+        stats->jac_ms = ph[kPhJac];
+        stats->krylov_ms = ph[kPhKrylov];
+        stats->resid_ms = ph[kPhResid];
+        stats->other_ms = ms - ph[0] - ph[1] - ph[2];
     }
     if (status != SW2GPU_OK) fail(status, "step failed (Newton %d iterations, max residual %g)", it, rmax);
     return status;

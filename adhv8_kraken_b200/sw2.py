@@ -80,12 +80,25 @@ def _ip(a):
 class SW2GPU:
     """One SW2 model resident on the GPU (mesh, BCSR pattern and three time levels)."""
 
+    # Krylov stopping defaults.  The reference preconditions with an exact LU of the
+    # whole system, so its linear solves are exact to round-off; the plain FP64 path
+    # matches that with a tight tolerance.  The mixed path solves to 1e-6 in the
+    # FP32-preconditioned system and lets the FP64 Newton loop refine.
+    DEFAULT_TOL = {capi.SW2GPU_FP64: (1e-12, 1e-20), capi.SW2GPU_MIXED: (1e-6, 1e-20)}
+
     def __init__(self, model, precision: int = capi.SW2GPU_FP64, precond: int = capi.SW2GPU_PREC_BJACOBI,
-                 lin_rtol: float = 1e-5, lin_atol: float = 1e-10, stream: int = 0):
+                 lin_rtol: float = None, lin_atol: float = None, stream: int = 0, max_lin_it: int = None):
         self.model = model
+        rt, at = self.DEFAULT_TOL[precision]
+        lin_rtol = rt if lin_rtol is None else lin_rtol
+        lin_atol = at if lin_atol is None else lin_atol
         self.arrays = MeshArrays(model)
         self.params = make_params(model, precision=precision, precond=precond, lin_rtol=lin_rtol,
                                   lin_atol=lin_atol)
+        if max_lin_it is not None:
+            self.params.max_lin_it = max_lin_it
+        elif precision == capi.SW2GPU_MIXED:
+            self.params.max_lin_it = min(self.params.max_lin_it, 100)
         self.V, self.T = model.nnodes, model.nelems2d
         h = C.c_void_p()
         _check(lib().sw2gpu_create(C.byref(self.arrays.mesh), C.byref(self.params),

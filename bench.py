@@ -1,0 +1,344 @@
+"""Benchmark of the B200 SW2 Newton step (triangle-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--points P]
+
+Workload (one "step" = one implicit time step: FD Jacobian + block-Jacobi BiCGSTAB +
+damped Newton, to the reference's convergence test): the plain FP64 drop-in at scale --
+a seeded Delaunay basin of 500k points (~1M triangles) over 20 km x 20 km with 40
+Gaussian bumps (dry tops, wet/dry fronts), log-normal Manning n, an inflow hydrograph
+ramping 1 -> 5 m^2/s over 30 steps, dt = 5 s.  Data are synthetic (no dataset exists).
+
+* ``value``  -- triangle-steps/s with the state resident in HBM, timed with CUDA events on
+  the library's stream (max over ranks for N > 1; every rank runs its own replica).
+* ``e2e``    -- the same through the C ABI with host buffers: every step uploads the three
+  time levels from pinned host memory and reads the new state back, as a drop-in for the
+  reference's ``fe_sw2_solve`` would.
+* ``mixed``  -- the mixed-precision path on the same workload (FP32 Jacobian storage,
+  SpMV and preconditioner inside the FP64 Newton loop) with its error against the FP64 run.
+* ``roofline`` -- the dominant kernel (largest device time in the timed region).
+* ``cpu_baseline`` -- the reference AdH executable built from its own sources
+  (``oracle/_ref``), timed on this host's cores on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SW2 triangle-steps/s at <=1e-8 rel err vs FP64, plain vs batched; p50/p99 latency"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def config2_model(points: int, nsteps: int):
+    from adhv8_kraken_b200 import meshgen
+    size = 20000.0 * math.sqrt(points / 5e5)
+    return meshgen.bumpy_basin(points, seed=2024, size=size, nsteps=nsteps, dt=5.0, name="config2")
+
+
+def cpu_reference_sample(points: int = 10000, steps: int = 4, procs: int = 1, timeout: float = 600.0):
+    """Runs the reference executable on `procs` seeded instances concurrently (one per
+    core); returns aggregate triangle-steps/s over the time-loop seconds of each run."""
+    from adhv8_kraken_b200 import meshgen
+    from oracle.ref_run import EXE, parse, read_dump
+    if not os.path.exists(EXE):
+        return None
+    runs = []
+    for r in range(procs):
+        m = meshgen.bumpy_basin(points, seed=7000 + r, size=20000.0 * math.sqrt(points / 5e5), nsteps=steps,
+                                dt=5.0, name="refsample")
+        d = tempfile.mkdtemp(prefix="adhref_")
+        m.write_adh(d, "m", nsteps=steps)
+        env = dict(os.environ, ADH_DUMP=os.path.join(d, "dump.bin"), ADH_DUMP_LOADS="0")
+        runs.append((m, d, subprocess.Popen([EXE, "m"], cwd=d, env=env, stdout=subprocess.DEVNULL,
+                                            stderr=subprocess.DEVNULL)))
+    tri_steps, secs = 0.0, []
+    for m, d, p in runs:
+        p.wait(timeout=timeout)
+        out = parse(read_dump(os.path.join(d, "dump.bin")))
+        s = sum(st["seconds"] for st in out["steps"])
+        tri_steps += m.nelems2d * len(out["steps"])
+        secs.append(s)
+    elapsed = max(secs)
+    return {"value": tri_steps / elapsed, "tri_steps": tri_steps, "seconds": elapsed,
+            "triangles": runs[0][0].nelems2d, "steps": steps, "procs": procs}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    res = cpu_reference_sample(points=args.ref_points, steps=max(1, args.steps), procs=procs)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/adh_dump is not built"}))
+        return
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": "triangle-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["seconds"] / res["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"reference AdH executable (serial C, profile-LU block-Jacobi BiCGSTAB) on "
+                               f"{procs} concurrent seeded basins of {res['triangles']} triangles, "
+                               f"{res['steps']} steps each (bounded sample of the 1M-triangle workload)"},
+        "cpu_baseline": {"value": res["value"], "unit": "triangle-steps/s", "cores": procs, "kind": "reference",
+                         "sample": f"{procs} x {res['triangles']} triangles x {res['steps']} steps"},
+        "e2e": {"value": res["value"], "unit": "triangle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from adhv8_kraken_b200 import capi
+    from adhv8_kraken_b200.sw2 import SW2GPU
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    model = config2_model(args.points, args.warmup + args.steps + 8)
+    T, V = model.nelems2d, model.nnodes
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- plain FP64, state resident in HBM
+    g = SW2GPU(model, precision=capi.SW2GPU_FP64, stream=stream.cuda_stream)
+    for _ in range(args.warmup):
+        st = g.step()
+        assert st["status"] == 0, st
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            stats.append(g.step())
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    assert all(s["status"] == 0 for s in stats), [s["status"] for s in stats]
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    value = world * T * args.steps / (ms * 1e-3)
+    h64 = g.get_state(0)
+
+    # ---- dominant kernel and its roofline
+    jac = sum(s["jac_ms"] for s in stats)
+    kry = sum(s["krylov_ms"] for s in stats)
+    res = sum(s["resid_ms"] for s in stats)
+    newton = sum(s["newton_its"] for s in stats)
+    lin = sum(s["linear_its"] for s in stats)
+    nnzb = g.nnzb
+    hbm, src = peaks()
+    # algorithmic bytes per launch ("Roofline accounting")
+    jac_bytes = T * (3 * 4 + 7 * 8 + 4 + 4 + 1) + V * 12 * 8 + T * 81 * 8       # gather + element data + 81 outputs
+    kry_iter_bytes = 2 * (nnzb * (9 * 8 + 4) + (V + 1) * 4 + V * 9 * 8) + V * 3 * 8 * 14
+    kernels = {
+        "k_jac_elem": (jac, newton, jac_bytes),
+        "k_bicgstab": (kry, newton, kry_iter_bytes * (lin / max(newton, 1)) + V * 3 * 8 * 10),
+    }
+    name = max(kernels, key=lambda k: kernels[k][0])
+    tot_ms, launches, bytes_per_launch = kernels[name]
+    per_launch_ms = tot_ms / max(launches, 1)
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", f"{name}_traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            tr = json.load(f)
+        traffic = tr.get("bytes_per_triangle", 0) * T if name == "k_jac_elem" else tr.get("bytes_per_launch")
+    roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": per_launch_ms,
+                "share_of_step": tot_ms / ms}
+
+    # ---- e2e through the C ABI with host buffers (drop-in semantics)
+    g.close()
+    g = SW2GPU(model, precision=capi.SW2GPU_FP64, stream=stream.cuda_stream)
+    for _ in range(args.warmup):
+        g.step()
+    pinned = [torch.empty(V, dtype=torch.float64, pin_memory=True) for _ in range(9)]
+    host = [p.numpy() for p in pinned]
+    for lvl in range(3):
+        hh, uu, vv = g.get_state(lvl)
+        host[3 * lvl][:], host[3 * lvl + 1][:], host[3 * lvl + 2][:] = hh, uu, vv
+    out = [np.empty(V) for _ in range(3)]
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for lvl in range(3):
+            g.set_state(lvl, host[3 * lvl], host[3 * lvl + 1], host[3 * lvl + 2])
+        st = g.step()
+        assert st["status"] == 0
+        out = g.get_state(0)
+        # the caller's state advances: older <- old <- current
+        for k in range(3):
+            host[6 + k][:] = host[3 + k]
+            host[3 + k][:] = host[k]
+            host[k][:] = out[k]
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e = {"value": world * T * args.steps / float(e2e_t.item()), "unit": "triangle-steps/s",
+           "h2d_bytes_per_step": 9 * 8 * V, "d2h_bytes_per_step": 3 * 8 * V}
+    g.close()
+
+    # ---- mixed precision on the same workload and its error vs the FP64 run
+    gm = SW2GPU(model, precision=capi.SW2GPU_MIXED, stream=stream.cuda_stream)
+    for _ in range(args.warmup):
+        gm.step()
+    torch.cuda.synchronize()
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    mstats = [gm.step() for _ in range(args.steps)]
+    m1.record(stream)
+    torch.cuda.synchronize()
+    mms = m0.elapsed_time(m1)
+    hm = gm.get_state(0)
+    gm.close()
+    err = {}
+    for f, a, b in (("h", hm[0], h64[0]), ("uh", hm[0] * hm[1], h64[0] * h64[1]),
+                    ("vh", hm[0] * hm[2], h64[0] * h64[2])):
+        err[f] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    mixed = {"value": world * T * args.steps / (mms * 1e-3), "ms_per_step": mms / args.steps,
+             "max_rel_err_vs_fp64": err, "newton_its": sum(s["newton_its"] for s in mstats),
+             "linear_its": sum(s["linear_its"] for s in mstats)}
+
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        cpu_res = cpu_reference_sample(points=args.ref_points, steps=3, procs=1)
+        if cpu_res:
+            cpu = {"value": cpu_res["value"], "unit": "triangle-steps/s", "cores": 1, "kind": "reference",
+                   "sample": f"reference AdH executable, one seeded basin of {cpu_res['triangles']} triangles "
+                             f"from the same generator, 3 steps, time loop only ({cpu_res['seconds']:.1f} s)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "triangle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"plain FP64 SW2 drop-in at scale: seeded Delaunay basin, {T} triangles, "
+                               f"{V} nodes, 40 bumps with dry tops, inflow ramp 1->5 m^2/s, dt 5 s",
+                   "triangles": T, "nodes": V, "nnzb": nnzb, "precision": "fp64",
+                   "l2": "inputs larger than L2 (BCSR alone is %.0f MB)" % (nnzb * 72 / 1e6),
+                   "parallelism": f"replicas{world}"},
+        "newton_its_per_step": newton / args.steps, "krylov_its_per_step": lin / args.steps,
+        "phase_ms_per_step": {"jacobian": jac / args.steps, "krylov": kry / args.steps,
+                              "residual": res / args.steps,
+                              "other": (ms - jac - kry - res) / args.steps},
+        "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+        "clocks": clk.summary(),
+        "roofline": roofline,
+        "e2e": e2e,
+        "mixed": mixed,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--points", type=int, default=500000)
+    ap.add_argument("--ref-points", type=int, default=10000)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

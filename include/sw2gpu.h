@@ -97,6 +97,10 @@ typedef struct sw2gpu_stats {
     double  device_ms;                 /* device time of the call (CUDA events) */
     int32_t kernel_launches;           /* kernels launched by the call */
     int32_t wd_elems;                  /* elements with wd_flag != 0 after the step */
+    double  jac_ms;                    /* FD Jacobian element kernel (summed over Newton iterations) */
+    double  krylov_ms;                 /* persistent BiCGSTAB kernel */
+    double  resid_ms;                  /* residual element + gather kernels */
+    double  other_ms;                  /* block gather, scaling, line search, init */
 } sw2gpu_stats;
 
 typedef struct sw2gpu_ctx sw2gpu_ctx;

@@ -21,7 +21,8 @@ _lib = None
 
 
 def build(force: bool = False) -> str:
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+    hdr = os.path.join(HERE, "..", "include", "sw2gpu.h")
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(SRC), os.path.getmtime(hdr)):
         subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-std=c99", "-o", LIB, SRC, "-lm"], check=True)
     return LIB
 
@@ -29,8 +30,7 @@ def build(force: bool = False) -> str:
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
-            build()
+        build()
         L = C.CDLL(LIB)
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.c_void_p, C.c_void_p, C.c_int]

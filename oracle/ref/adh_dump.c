@@ -7,9 +7,10 @@
  * full-precision records to the binary file named by the environment variable
  * ADH_DUMP:
  *
- *   "step"   after every accepted time step: t_prev, dt, Newton iterations of
- *            the step (including failed attempts), the number of attempts, and
- *            the nodal head / vel.x / vel.y / wd_flag arrays;
+ *   "step"   after every accepted time step: t_prev, dt, the wall time of the
+ *            step's fe_main calls, Newton iterations of the step (including failed
+ *            attempts), the number of attempts, and the nodal head / vel.x / vel.y /
+ *            wd_flag arrays;
  *   "load"   for the first ADH_DUMP_LOADS calls of fe_sw2_load: the state the
  *            Jacobian was built at (three time levels), the residual vector,
  *            the 3x3 diagonal blocks and every off-diagonal SPARSE_VECT row.
@@ -17,6 +18,7 @@
  * Record layout: char tag[8]; int32 kind (0 = f64, 1 = i32); int64 count; data.
  */
 #include "global_header.h"
+#include <time.h>
 
 int __real_fe_main(SSUPER_MODEL *sm);
 void __real_fe_sw2_load(SSUPER_MODEL *sm, int imod);
@@ -25,6 +27,13 @@ static FILE *dump_fp = NULL;
 static int dump_loads_left = -1;
 static int attempts = 0;
 static int it_mark = 0;
+static double solve_seconds = 0.0;   /* fe_main wall time since the last accepted step */
+
+static double now_seconds(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double) ts.tv_sec + 1e-9 * (double) ts.tv_nsec;
+}
 
 static void dump_open(void) {
     if (dump_fp != NULL) return;
@@ -72,24 +81,28 @@ static void put_state(const char *th, const char *tu, const char *tv, double *h,
 int __wrap_fe_main(SSUPER_MODEL *sm) {
     int r;
     dump_open();
+    double t0 = now_seconds();
     r = __real_fe_main(sm);
+    solve_seconds += now_seconds() - t0;
     attempts++;
     if (r == YES && dump_fp != NULL) {
         SMODEL *mod = &(sm->submodel[0]);
         int n = mod->grid->nnodes;
-        double hdr[2];
+        double hdr[3];
         int ihdr[3];
         hdr[0] = mod->t_prev;
         hdr[1] = sm->dt;
+        hdr[2] = solve_seconds;
         ihdr[0] = sm->solver_info.it_count_nonlin - it_mark;
         ihdr[1] = attempts;
         ihdr[2] = n;
-        put_f64("step", hdr, 2);
+        put_f64("step", hdr, 3);
         put_i32("stepi", ihdr, 3);
         put_state("h", "u", "v", mod->sw->d2->head, mod->sw->d2->vel, n);
         put_i32("wd", mod->grid->wd_flag, mod->grid->nelems2d);
         fflush(dump_fp);
         attempts = 0;
+        solve_seconds = 0.0;
         it_mark = sm->solver_info.it_count_nonlin;
     }
     return r;

@@ -43,7 +43,8 @@ def parse(recs) -> Dict[str, list]:
         tag, arr = recs[i]
         if tag == "step":
             hi = recs[i + 1][1]
-            steps.append(dict(t=arr[0], dt=arr[1], newton_its=int(hi[0]), attempts=int(hi[1]),
+            steps.append(dict(t=arr[0], dt=arr[1], seconds=float(arr[2]) if arr.size > 2 else 0.0,
+                              newton_its=int(hi[0]), attempts=int(hi[1]),
                               h=recs[i + 2][1], u=recs[i + 3][1], v=recs[i + 4][1], wd=recs[i + 5][1]))
             i += 6
         elif tag == "load":
