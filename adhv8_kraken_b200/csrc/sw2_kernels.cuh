@@ -228,7 +228,7 @@ struct __align__(16) StagedElem {
     int n[3], df[3], wd, mat;
 };
 
-__global__ void __launch_bounds__(kJacThreads) k_jac_elem(DevMesh m, State s, PhysParams P,
+__global__ void __maxnreg__(224) k_jac_elem(DevMesh m, State s, PhysParams P,
                                                            double* __restrict__ jslots) {
     __shared__ StagedElem se[kJacElems];
     __shared__ double out[kJacElems * 81];
@@ -251,13 +251,28 @@ __global__ void __launch_bounds__(kJacThreads) k_jac_elem(DevMesh m, State s, Ph
         const int b = item / 3, var = item % 3;  // var: 0 = u, 1 = v, 2 = h
         ElemIn in = S.in;
         const MatParams M = m.mats[S.mat];
-        const double cur = (var == 0) ? in.u[b] : (var == 1) ? in.v[b] : in.h[b];
+        // perturbed value, selected without runtime array indexing (keeps `in` in registers)
+        double cur = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            if (i == b) cur = (var == 0) ? in.u[i] : (var == 1) ? in.v[i] : in.h[i];
+        }
         const double eps = fd_eps(cur);
         const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
         double rp[3][3], rm[3][3];
-        if (var == 0) in.u[b] = cur + eps; else if (var == 1) in.v[b] = cur + eps; else in.h[b] = cur + eps;
+        auto setp = [&](double val) {
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                if (i == b) {
+                    if (var == 0) in.u[i] = val;
+                    else if (var == 1) in.v[i] = val;
+                    else in.h[i] = val;
+                }
+            }
+        };
+        setp(cur + eps);
         sw2_elem_resid(in, S.wd, pv, P, M, S.df, rp);
-        if (var == 0) in.u[b] = cur - eps; else if (var == 1) in.v[b] = cur - eps; else in.h[b] = cur - eps;
+        setp(cur - eps);
         sw2_elem_resid(in, S.wd, pv, P, M, S.df, rm);
         const double e2 = 2.0 * eps;
         // Dirichlet zeroing of the element matrix (fe_assign_mom_db_dof3 / fe_assign_dacont_db_dof3):
@@ -316,14 +331,21 @@ __global__ void k_jac_edge(DevMesh m, State s, PhysParams P, double* __restrict_
     in.z0 = m.z[nd[0]];
     const int kind = m.bkind[j];
     const double value = m.str_value[m.bstr[j]];
-    const double cur = (var == 0) ? in.u[b] : (var == 1) ? in.v[b] : in.h[b];
+    double cur = 0.0;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+        if (i == b) cur = (var == 0) ? in.u[i] : (var == 1) ? in.v[i] : in.h[i];
     const double eps = fd_eps(cur);
     const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
     double rp[2][3], rm[2][3];
     EdgeIn ip = in, im = in;
-    if (var == 0) { ip.u[b] = cur + eps; im.u[b] = cur - eps; }
-    else if (var == 1) { ip.v[b] = cur + eps; im.v[b] = cur - eps; }
-    else { ip.h[b] = cur + eps; im.h[b] = cur - eps; }
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        if (i != b) continue;
+        if (var == 0) { ip.u[i] = cur + eps; im.u[i] = cur - eps; }
+        else if (var == 1) { ip.v[i] = cur + eps; im.v[i] = cur - eps; }
+        else { ip.h[i] = cur + eps; im.h[i] = cur - eps; }
+    }
     sw2_edge_resid(ip, kind, value, pv, P, df, rp);
     sw2_edge_resid(im, kind, value, pv, P, df, rm);
     const double e2 = 2.0 * eps;

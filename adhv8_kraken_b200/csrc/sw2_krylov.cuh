@@ -130,30 +130,44 @@ struct KrylovArgs {
 };
 
 // y = Dinv_i * sum_j A'_ij x_j for node row i, with x_j = xa_j - alpha * xb_j when xb != null.
-// Products and sums are formed in the matrix type MT (FP32 accumulation on the mixed path).
+// Eight lanes share a row: lane l takes the row's values l, l+8, ... (the row's blocks are
+// contiguous, so every load instruction of the 8 lanes reads 64 consecutive bytes), and the
+// three row sums are combined with xor shuffles in a fixed order.  Products and sums are
+// formed in the matrix type MT (FP32 accumulation on the mixed path).  The result is valid
+// on lane 0 of the group; `active` false contributes zeros so the whole warp can shuffle.
+constexpr int kRowLanes = 8;
 template <typename MT, typename VT>
-__device__ __forceinline__ void row_apply(int i, const int* rowptr, const int* col, const MT* A, const MT* Dinv,
-                                          const VT* xa, const VT* xb, VT alpha, VT y[3]) {
-    MT acc0 = 0, acc1 = 0, acc2 = 0;
-    const int k1 = rowptr[i + 1];
-    for (int k = rowptr[i]; k < k1; k++) {
-        const int j = col[k];
-        const MT* a = A + (size_t)k * 9;
-        VT x0 = ldv(xa + 3 * j), x1 = ldv(xa + 3 * j + 1), x2 = ldv(xa + 3 * j + 2);
-        if (xb) {
-            x0 -= alpha * ldv(xb + 3 * j);
-            x1 -= alpha * ldv(xb + 3 * j + 1);
-            x2 -= alpha * ldv(xb + 3 * j + 2);
+__device__ __forceinline__ void row_apply8(int i, bool active, int lane8, const int* rowptr, const int* col,
+                                           const MT* A, const MT* Dinv, const VT* xa, const VT* xb, VT alpha,
+                                           VT y[3]) {
+    MT a0 = 0, a1 = 0, a2 = 0;
+    if (active) {
+        const int v1 = __ldg(rowptr + i + 1) * 9;
+        for (int v = __ldg(rowptr + i) * 9 + lane8; v < v1; v += kRowLanes) {
+            const int kb = v / 9, q = v - 9 * kb, r = q / 3, c = q - 3 * r;
+            const int j = __ldg(col + kb);
+            VT x = ldv(xa + 3 * j + c);
+            if (xb) x -= alpha * ldv(xb + 3 * j + c);
+            const MT prod = __ldg(A + v) * (MT)x;
+            a0 += (r == 0) ? prod : (MT)0;
+            a1 += (r == 1) ? prod : (MT)0;
+            a2 += (r == 2) ? prod : (MT)0;
         }
-        const MT m0 = (MT)x0, m1 = (MT)x1, m2 = (MT)x2;
-        acc0 += __ldg(a + 0) * m0 + __ldg(a + 1) * m1 + __ldg(a + 2) * m2;
-        acc1 += __ldg(a + 3) * m0 + __ldg(a + 4) * m1 + __ldg(a + 5) * m2;
-        acc2 += __ldg(a + 6) * m0 + __ldg(a + 7) * m1 + __ldg(a + 8) * m2;
     }
-    const MT* d = Dinv + (size_t)i * 9;
-    y[0] = (VT)(__ldg(d + 0) * acc0 + __ldg(d + 1) * acc1 + __ldg(d + 2) * acc2);
-    y[1] = (VT)(__ldg(d + 3) * acc0 + __ldg(d + 4) * acc1 + __ldg(d + 5) * acc2);
-    y[2] = (VT)(__ldg(d + 6) * acc0 + __ldg(d + 7) * acc1 + __ldg(d + 8) * acc2);
+#pragma unroll
+    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o, kRowLanes);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o, kRowLanes);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o, kRowLanes);
+    }
+    if (active && lane8 == 0) {
+        const MT* d = Dinv + (size_t)i * 9;
+        y[0] = (VT)(__ldg(d + 0) * a0 + __ldg(d + 1) * a1 + __ldg(d + 2) * a2);
+        y[1] = (VT)(__ldg(d + 3) * a0 + __ldg(d + 4) * a1 + __ldg(d + 5) * a2);
+        y[2] = (VT)(__ldg(d + 6) * a0 + __ldg(d + 7) * a1 + __ldg(d + 8) * a2);
+    } else {
+        y[0] = y[1] = y[2] = (VT)0;
+    }
 }
 
 // MT: matrix / preconditioner storage and SpMV accumulation type; VT: Krylov vector type
@@ -168,6 +182,12 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
     const int V = K.V;
     const int stride = gridDim.x * blockDim.x;
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    // SpMV phases: groups of kRowLanes lanes per row; a warp covers 32 / kRowLanes rows
+    const int lane8 = threadIdx.x % kRowLanes;
+    const int warp_g = t0 / 32;
+    const int grp_off = (threadIdx.x % 32) / kRowLanes;
+    const int g0 = warp_g * (32 / kRowLanes);
+    const int gstride = (stride / 32) * (32 / kRowLanes);
     const int SUM = 0, MAX = 1;
     KrylovCtl* ctl = K.ctl;
     int nred = 0;   // reductions so far; selects the partial buffer
@@ -189,20 +209,24 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
     {
         double vals[4] = {0, 0, 0, 0};
         const int ism[4] = {MAX, MAX, SUM, SUM};
-        for (int i = t0; i < V; i += stride) {
+        for (int base = g0; base < V; base += gstride) {
+            const int i = base + grp_off;
+            const bool act = i < V;
             VT y[3];
-            row_apply<MT, VT>(i, K.rowptr, K.col, A, Dinv, uu, (const VT*)nullptr, (VT)0, y);
+            row_apply8<MT, VT>(i, act, lane8, K.rowptr, K.col, A, Dinv, uu, (const VT*)nullptr, (VT)0, y);
+            if (act && lane8 == 0) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const VT bb = ldv(b + 3 * i + c);
-                const VT rr = bb - y[c];
-                r[3 * i + c] = rr;
-                q[3 * i + c] = rr;
-                p[3 * i + c] = rr;
-                Ap[3 * i + c] = 0;
-                vals[0] = fmax(vals[0], fabs((double)rr));
-                vals[1] = fmax(vals[1], fabs((double)bb));
-                vals[2] += (double)rr * (double)rr;
+                for (int c = 0; c < 3; c++) {
+                    const VT bb = ldv(b + 3 * i + c);
+                    const VT rr = bb - y[c];
+                    r[3 * i + c] = rr;
+                    q[3 * i + c] = rr;
+                    p[3 * i + c] = rr;
+                    Ap[3 * i + c] = 0;
+                    vals[0] = fmax(vals[0], fabs((double)rr));
+                    vals[1] = fmax(vals[1], fabs((double)bb));
+                    vals[2] += (double)rr * (double)rr;
+                }
             }
         }
         block_partial<4>(vals, ism, pbuf());
@@ -221,13 +245,17 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
             {
                 double g[4] = {0, 0, 0, 0};
                 const int gm[4] = {SUM, SUM, SUM, SUM};
-                for (int i = t0; i < V; i += stride) {
+                for (int base = g0; base < V; base += gstride) {
+                    const int i = base + grp_off;
+                    const bool act = i < V;
                     VT y[3];
-                    row_apply<MT, VT>(i, K.rowptr, K.col, A, Dinv, p, (const VT*)nullptr, (VT)0, y);
+                    row_apply8<MT, VT>(i, act, lane8, K.rowptr, K.col, A, Dinv, p, (const VT*)nullptr, (VT)0, y);
+                    if (act && lane8 == 0) {
 #pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        Ap[3 * i + c] = y[c];
-                        g[0] += (double)ldv(q + 3 * i + c) * (double)y[c];
+                        for (int c = 0; c < 3; c++) {
+                            Ap[3 * i + c] = y[c];
+                            g[0] += (double)ldv(q + 3 * i + c) * (double)y[c];
+                        }
                     }
                 }
                 block_partial<1>(g, gm, pbuf());
@@ -241,16 +269,20 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
                 double w[4] = {0, 0, 0, 0};
                 const int wm[4] = {SUM, SUM, SUM, SUM};
                 const VT al = (VT)alpha;
-                for (int i = t0; i < V; i += stride) {
+                for (int base = g0; base < V; base += gstride) {
+                    const int i = base + grp_off;
+                    const bool act = i < V;
                     VT y[3];
-                    row_apply<MT, VT>(i, K.rowptr, K.col, A, Dinv, r, Ap, al, y);
+                    row_apply8<MT, VT>(i, act, lane8, K.rowptr, K.col, A, Dinv, r, Ap, al, y);
+                    if (act && lane8 == 0) {
 #pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        const VT s = ldv(r + 3 * i + c) - al * ldv(Ap + 3 * i + c);
-                        As[3 * i + c] = y[c];
-                        w[0] += (double)y[c] * (double)s;
-                        w[1] += (double)y[c] * (double)y[c];
-                        w[2] += (double)y[c] * (double)ldv(q + 3 * i + c);
+                        for (int c = 0; c < 3; c++) {
+                            const VT s = ldv(r + 3 * i + c) - al * ldv(Ap + 3 * i + c);
+                            As[3 * i + c] = y[c];
+                            w[0] += (double)y[c] * (double)s;
+                            w[1] += (double)y[c] * (double)y[c];
+                            w[2] += (double)y[c] * (double)ldv(q + 3 * i + c);
+                        }
                     }
                 }
                 block_partial<3>(w, wm, pbuf());

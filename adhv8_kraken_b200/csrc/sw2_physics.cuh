@@ -51,6 +51,9 @@ struct ElemIn {
     double djac, gx[3], gy[3];
 };
 
+// a[k] for a runtime k in 0..2 as selects, so register arrays stay in registers
+__device__ __forceinline__ double sel3(const double* a, int k) { return (k == 0) ? a[0] : ((k == 1) ? a[1] : a[2]); }
+
 // ---------------------------------------------------------------------------------
 // wet/dry clipping of one depth array (the geometric part of fe_sw2_wet_dry_wrapper)
 struct Clip {
@@ -79,13 +82,14 @@ __device__ __forceinline__ void make_clip(const double* x, const double* y, cons
     if (total != 1) pass = 7 - pass;
     int only = pass / 2;
     c.only = only;
+    const double ho = sel3(h, only), xo = sel3(x, only), yo = sel3(y, only);
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         if (i != only) {
-            double xsi = h[i] / (h[i] - h[only]);
+            double xsi = h[i] / (h[i] - ho);
             c.xsi[i] = xsi;
-            c.nx[i] = x[i] + xsi * (x[only] - x[i]);
-            c.ny[i] = y[i] + xsi * (y[only] - y[i]);
+            c.nx[i] = x[i] + xsi * (xo - x[i]);
+            c.ny[i] = y[i] + xsi * (yo - y[i]);
             c.nh[i] = 0.0;
         } else {
             c.xsi[i] = 0.0;
@@ -140,15 +144,19 @@ __device__ __forceinline__ void wd_apply(const Clip& c, const double* x, const d
     f(c.nx, c.ny, c.nh, ngx, ngy, nd, true, c, nr);
     if (redistribute) {
         const int o = c.only;
+        const double xo = sel3(x, o), yo = sel3(y, o);
 #pragma unroll
         for (int i = 0; i < 3; i++) {
             if (i == o) continue;
-            double ax = c.nx[i] - x[o], ay = c.ny[i] - y[o];
-            double bx = x[i] - x[o], by = y[i] - y[o];
+            double ax = c.nx[i] - xo, ay = c.ny[i] - yo;
+            double bx = x[i] - xo, by = y[i] - yo;
             double xs = sqrt((ax * ax + ay * ay) / (bx * bx + by * by));
 #pragma unroll
             for (int q = 0; q < 3; q++) {
-                nr[o][q] += (1.0 - xs) * nr[i][q];
+                const double add = (1.0 - xs) * nr[i][q];
+#pragma unroll
+                for (int t = 0; t < 3; t++)
+                    if (t == o) nr[t][q] += add;
                 nr[i][q] *= xs;
             }
         }
@@ -162,7 +170,7 @@ __device__ __forceinline__ void wd_apply(const Clip& c, const double* x, const d
 // clipped value of a vertex quantity (FIXED_POS with the clip weights)
 __device__ __forceinline__ double cval(const Clip& c, bool clipped, const double* f, int i) {
     if (!clipped || i == c.only) return f[i];
-    return f[i] + c.xsi[i] * (f[c.only] - f[i]);
+    return f[i] + c.xsi[i] * (sel3(f, c.only) - f[i]);
 }
 
 // wetted-area averages (fe_sw2_wd_average, src/fe/sw2/fe_sw2_wet_dry_integrations.c:19-39):
