@@ -84,7 +84,7 @@ __global__ void k_resid_elem(DevMesh m, State s, PhysParams P, double* __restric
         int n[3], df[3];
         load_elem(m, s, t, 1, in, n, df);
         double er[3][3];
-        sw2_elem_resid(in, s.wd[t], kPertNone, P, m.mats[m.emat[t]], df, er);
+        sw2_elem_resid(in, in.h, in.u, in.v, s.wd[t], kPertNone, P, m.mats[m.emat[t]], df, er);
 #pragma unroll
         for (int i = 0; i < 3; i++) {
             const bool dry = in.ho[i] <= 0.;
@@ -228,7 +228,7 @@ struct __align__(16) StagedElem {
     int n[3], df[3], wd, mat;
 };
 
-__global__ void __maxnreg__(224) k_jac_elem(DevMesh m, State s, PhysParams P,
+__global__ void __launch_bounds__(kJacThreads) k_jac_elem(DevMesh m, State s, PhysParams P,
                                                            double* __restrict__ jslots) {
     __shared__ StagedElem se[kJacElems];
     __shared__ double out[kJacElems * 81];
@@ -249,13 +249,21 @@ __global__ void __maxnreg__(224) k_jac_elem(DevMesh m, State s, PhysParams P,
     if (e < m.T) {
         const StagedElem& S = se[lane];
         const int b = item / 3, var = item % 3;  // var: 0 = u, 1 = v, 2 = h
-        ElemIn in = S.in;
+        // only the current iterate (9 values) is private; everything else is read from the
+        // staged element in shared memory
+        double hc[3], uc[3], vc[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            hc[i] = S.in.h[i];
+            uc[i] = S.in.u[i];
+            vc[i] = S.in.v[i];
+        }
         const MatParams M = m.mats[S.mat];
-        // perturbed value, selected without runtime array indexing (keeps `in` in registers)
+        // perturbed value, selected without runtime array indexing (keeps the arrays in registers)
         double cur = 0.0;
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            if (i == b) cur = (var == 0) ? in.u[i] : (var == 1) ? in.v[i] : in.h[i];
+            if (i == b) cur = (var == 0) ? uc[i] : (var == 1) ? vc[i] : hc[i];
         }
         const double eps = fd_eps(cur);
         const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
@@ -264,16 +272,16 @@ __global__ void __maxnreg__(224) k_jac_elem(DevMesh m, State s, PhysParams P,
 #pragma unroll
             for (int i = 0; i < 3; i++) {
                 if (i == b) {
-                    if (var == 0) in.u[i] = val;
-                    else if (var == 1) in.v[i] = val;
-                    else in.h[i] = val;
+                    if (var == 0) uc[i] = val;
+                    else if (var == 1) vc[i] = val;
+                    else hc[i] = val;
                 }
             }
         };
         setp(cur + eps);
-        sw2_elem_resid(in, S.wd, pv, P, M, S.df, rp);
+        sw2_elem_resid(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, rp);
         setp(cur - eps);
-        sw2_elem_resid(in, S.wd, pv, P, M, S.df, rm);
+        sw2_elem_resid(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, rm);
         const double e2 = 2.0 * eps;
         // Dirichlet zeroing of the element matrix (fe_assign_mom_db_dof3 / fe_assign_dacont_db_dof3):
         // D = momentum-Dirichlet nodes (old-dry or VEL/VEL_PRS string), P = continuity-Dirichlet.

@@ -122,10 +122,18 @@ __device__ __forceinline__ double clip_factor(const double* x, const double* y, 
 // clipped corner scaled by the signed factor, optionally redistributed (RE_DISTRIBUTE).
 // The integrand functor is called as f(x, y, h, gx, gy, djac, vinterp, rhs[3][3]) where
 // vinterp(i, w, v) returns the clipped value of a vertex quantity.
-template <class F>
-__device__ __forceinline__ void wd_apply(const Clip& c, const double* x, const double* y, const double* h,
+template <bool WET, class F>
+__device__ __forceinline__ void wd_apply(const double* x, const double* y, const double* h,
                                          const double* gx, const double* gy, double djac, int redistribute,
                                          double (&rhs)[3][3], F&& f) {
+    Clip c;
+    if (WET) {             // caller guarantees h > 0 at every vertex: the wrapper's full-element case
+        c.total = 0;
+        c.only = 0;
+        f(x, y, h, gx, gy, djac, false, c, rhs);
+        return;
+    }
+    make_clip(x, y, h, djac, c);
     if (c.total == 3) return;
     if (c.total == 0 || c.total == 1) {
         f(x, y, h, gx, gy, djac, false, c, rhs);
@@ -175,7 +183,8 @@ __device__ __forceinline__ double cval(const Clip& c, bool clipped, const double
 
 // wetted-area averages (fe_sw2_wd_average, src/fe/sw2/fe_sw2_wet_dry_integrations.c:19-39):
 // returns the wrapper factor and writes the averaged depth and velocity.
-__device__ __forceinline__ double wd_average(const Clip& c, const double* x, const double* y, const double* h,
+template <bool WET>
+__device__ __forceinline__ double wd_average(const double* x, const double* y, const double* h,
                                              const double* u, const double* v, double djac, double& havg,
                                              double& uavg, double& vavg) {
     double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -188,8 +197,8 @@ __device__ __forceinline__ double wd_average(const Clip& c, const double* x, con
         r[0][1] += dj * t2;
         r[0][2] += dj * t3;
     };
-    wd_apply(c, x, y, h, nullptr, nullptr, djac, 0, acc, integ);
-    double f = c.ret;
+    wd_apply<WET>(x, y, h, nullptr, nullptr, djac, 0, acc, integ);
+    const double f = WET ? 1.0 : clip_factor(x, y, h, djac);
     havg = 0.0;
     uavg = 0.0;
     vavg = 0.0;
@@ -213,45 +222,46 @@ __device__ __forceinline__ double drag_coef(double depth, double ks) {  // fr_be
 
 // ---------------------------------------------------------------------------------
 // the element residual
+//   in:       the element's static data and old / older levels (may live in shared memory)
+//   hc,uc,vc: the current iterate at the three vertices, perturbation applied (registers)
 //   wd_flag:  element wet/dry flag of the Newton solve (fe_sw2_wdflag)
 //   pvar:     kPertNone / kPertU / kPertV / kPertH (u, v perturbations drop the pressure terms)
 //   dflag[3]: Dirichlet flags of the element's nodes (bit0 PRS_DIR, bit1 VEL_DIR, bit2 VEL_PRS_DIR)
-__device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, int pvar, const PhysParams& P,
-                                               const MatParams& M, const int* dflag, double (&er)[3][3]) {
+template <bool WET>
+__device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* hc, const double* uc, const double* vc,
+                                                int wd_flag, int pvar, const PhysParams& P, const MatParams& M,
+                                                const int* dflag, double (&er)[3][3]) {
     const double djac = in.djac, dt = P.dt, g = P.g, dll = P.dll, dul = P.dul;
     const double* gx = in.gx;
     const double* gy = in.gy;
     const bool pressure = !(pvar == kPertU || pvar == kPertV);
 
     // averages and gradients (:193-221)
-    double u_avg = (in.u[0] + in.u[1] + in.u[2]) / 3.0;
-    double v_avg = (in.v[0] + in.v[1] + in.v[2]) / 3.0;
+    double u_avg = (uc[0] + uc[1] + uc[2]) / 3.0;
+    double v_avg = (vc[0] + vc[1] + vc[2]) / 3.0;
     double gzx = 0, gzy = 0, ghx = 0, ghy = 0, gux = 0, guy = 0, gvx = 0, gvy = 0;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         gzx += in.z[i] * gx[i];
         gzy += in.z[i] * gy[i];
-        ghx += in.h[i] * gx[i];
-        ghy += in.h[i] * gy[i];
+        ghx += hc[i] * gx[i];
+        ghy += hc[i] * gy[i];
     }
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-        gux += in.u[i] * gx[i];
-        guy += in.u[i] * gy[i];
-        gvx += in.v[i] * gx[i];
-        gvy += in.v[i] * gy[i];
+        gux += uc[i] * gx[i];
+        guy += uc[i] * gy[i];
+        gvx += vc[i] * gx[i];
+        gvy += vc[i] * gy[i];
     }
     const double gwx = gzx + ghx, gwy = gzy + ghy;
     const double vmag = sqrt(u_avg * u_avg + v_avg * v_avg);
     const double vst_i = u_avg / fmax(vmag, 1.E-8), vst_j = v_avg / fmax(vmag, 1.E-8);
 
-    Clip ch;  // clipping of the current depth, shared by all wrapped integrands
-    make_clip(in.x, in.y, in.h, djac, ch);
     double h_wd, u_wd, v_wd;
-    wd_average(ch, in.x, in.y, in.h, in.u, in.v, djac, h_wd, u_wd, v_wd);
-    double factor = ch.ret;
-    const double factor_old = clip_factor(in.x, in.y, in.ho, djac);
-    const double factor_older = clip_factor(in.x, in.y, in.hoo, djac);
+    double factor = wd_average<WET>(in.x, in.y, hc, uc, vc, djac, h_wd, u_wd, v_wd);
+    const double factor_old = WET ? 1.0 : clip_factor(in.x, in.y, in.ho, djac);
+    const double factor_older = WET ? 1.0 : clip_factor(in.x, in.y, in.hoo, djac);
     const double vwd_mag = sqrt(u_wd * u_wd + v_wd * v_wd);
     const double h_fric = fmax(h_wd, kSmall);
     const double rough = (M.ks > kSmall) ? drag_coef(h_fric, M.ks) : 0.0;
@@ -289,7 +299,7 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
     for (int i = 0; i < 3; i++) er[i][0] = er[i][1] = er[i][2] = 0.0;
 
     // shock capturing, partially/fully dry elements (:357-400)
-    if (wd_flag == 1 || wd_flag == 2) {
+    if (!WET && (wd_flag == 1 || wd_flag == 2)) {
         const double gum = sqrt(gux * gux + guy * guy + kSmall);
         const double gvm = sqrt(gvx * gvx + gvy * gvy + kSmall);
         const double cu = 0.5 * dul * djac * gum, cv = 0.5 * dul * djac * gvm;
@@ -312,8 +322,8 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
             double uu[3], vv[3];
 #pragma unroll
             for (int i = 0; i < 3; i++) {
-                uu[i] = cval(c, clipped, in.u, i);
-                vv[i] = cval(c, clipped, in.v, i);
+                uu[i] = cval(c, clipped, uc, i);
+                vv[i] = cval(c, clipped, vc, i);
             }
             // integrate_triangle_gradPhi_dot_f_v
             double p1 = 2 * H[0] + H[1] + H[2], p2 = H[0] + 2 * H[1] + H[2], p3 = H[0] + H[1] + 2 * H[2];
@@ -349,7 +359,7 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
                 r[i][2] += ry;
             }
         };
-        wd_apply(ch, in.x, in.y, in.h, gx, gy, djac, 1, rhs, integ);
+        wd_apply<WET>(in.x, in.y, hc, gx, gy, djac, 1, rhs, integ);
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -358,8 +368,7 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
 
     // temporal terms t(n+1), t(n), t(n-1) (:481-490, fe_sw2_temporal :1288-1354)
     {
-        auto temporal = [&](const Clip& c, const double* H, const double* U, const double* V, double wdf,
-                            double dtf, int flag) {
+        auto temporal = [&](const double* H, const double* U, const double* V, double wdf, double dtf, int flag) {
             double rhs[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
             auto integ = [&](const double*, const double*, const double* Hc, const double*, const double*, double dj,
                              bool, const Clip&, double (&r)[3][3]) {
@@ -367,7 +376,7 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
 #pragma unroll
                 for (int i = 0; i < 3; i++) r[i][0] += t1 * (fs + Hc[i]);
             };
-            wd_apply(c, in.x, in.y, H, nullptr, nullptr, djac, 1, rhs, integ);
+            wd_apply<WET>(in.x, in.y, H, nullptr, nullptr, djac, 1, rhs, integ);
             const double con = dtf * wdf;
             const double t1 = djac * con * kOne3;
 #pragma unroll
@@ -377,15 +386,10 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
                 er[i][2] += t1 * (V[i] * fmax(H[i], dll));
             }
         };
-        temporal(ch, in.h, in.u, in.v, factor, 1. + P.alpha / 2., -3);
-        Clip co;
-        make_clip(in.x, in.y, in.ho, djac, co);
-        temporal(co, in.ho, in.uo, in.vo, factor_old, (-1.) * (1. + P.alpha), wd_flag);
-        if (P.alpha != 0.0) {  // the t(n-1) term has weight alpha / 2
-            Clip coo;
-            make_clip(in.x, in.y, in.hoo, djac, coo);
-            temporal(coo, in.hoo, in.uoo, in.voo, factor_older, P.alpha / 2., wd_flag);
-        }
+        temporal(hc, uc, vc, factor, 1. + P.alpha / 2., -3);
+        temporal(in.ho, in.uo, in.vo, factor_old, (-1.) * (1. + P.alpha), wd_flag);
+        if (P.alpha != 0.0)  // the t(n-1) term has weight alpha / 2
+            temporal(in.hoo, in.uoo, in.voo, factor_older, P.alpha / 2., wd_flag);
     }
 
     // diffusion (:504-534)
@@ -409,9 +413,9 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
         double fx[3], fy[3];
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            double m = sqrt(in.u[i] * in.u[i] + in.v[i] * in.v[i]);
-            fx[i] = in.u[i] * m;
-            fy[i] = in.v[i] * m;
+            double m = sqrt(uc[i] * uc[i] + vc[i] * vc[i]);
+            fx[i] = uc[i] * m;
+            fy[i] = vc[i] * m;
         }
         const double t1 = djac * (dt * g * resistance * factor) * kOne12;
         const double sx = fx[0] + fx[1] + fx[2], sy = fy[0] + fy[1] + fy[2];
@@ -433,8 +437,8 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
             er[1][q] += tt * (f[1] * (gs + 4 * gg[1]) + f[2] * (gs - gg[0]) + f[0] * (gs - gg[2]));
             er[2][q] += tt * (f[2] * (gs + 4 * gg[2]) + f[1] * (gs - gg[0]) + f[0] * (gs - gg[1]));
         };
-        phifg(-t1, in.h, in.v, 1);
-        phifg(+t1, in.h, in.u, 2);
+        phifg(-t1, hc, vc, 1);
+        phifg(+t1, hc, uc, 2);
     }
 
     // rainfall / water source (:728-754)
@@ -464,7 +468,7 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
                 r[i][2] += GY[i] * ff;
             }
         };
-        wd_apply(ch, in.x, in.y, in.h, gx, gy, djac, 1, rhs, ipress);
+        wd_apply<WET>(in.x, in.y, hc, gx, gy, djac, 1, rhs, ipress);
         accum(rhs);
         double rhs2[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         const double cb = g * dt;
@@ -478,7 +482,7 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
                 r[i][2] += cy * (sh + H[i]);
             }
         };
-        wd_apply(ch, in.x, in.y, in.h, nullptr, nullptr, djac, 1, rhs2, ibody);
+        wd_apply<WET>(in.x, in.y, hc, nullptr, nullptr, djac, 1, rhs2, ibody);
         accum(rhs2);
         double rhs3[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         const double cq = 0.5 * dt * g;
@@ -497,7 +501,7 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
                 r[n2][2] += delx * r1;
             }
         };
-        wd_apply(ch, in.x, in.y, in.h, nullptr, nullptr, djac, 1, rhs3, ibound);
+        wd_apply<WET>(in.x, in.y, hc, nullptr, nullptr, djac, 1, rhs3, ibound);
         accum(rhs3);
     }
 
@@ -513,8 +517,6 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
         // elementally averaged wet/dry time derivatives (wrapped fe_sw2_wd_integrate_triangle_f)
         double dhdt, dudt, dvdt;
         {
-            Clip co;
-            make_clip(in.x, in.y, in.ho, djac, co);
             double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
             auto integ = [&](const double*, const double*, const double* H, const double*, const double*, double dj,
                              bool clipped, const Clip& c, double (&r)[3][3]) {
@@ -522,7 +524,7 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
                 r[0][1] += dj * ((cval(c, clipped, in.uo, 0) + cval(c, clipped, in.uo, 1) + cval(c, clipped, in.uo, 2)) / 3.0);
                 r[0][2] += dj * ((cval(c, clipped, in.vo, 0) + cval(c, clipped, in.vo, 1) + cval(c, clipped, in.vo, 2)) / 3.0);
             };
-            wd_apply(co, in.x, in.y, in.ho, nullptr, nullptr, djac, 0, acc, integ);
+            wd_apply<WET>(in.x, in.y, in.ho, nullptr, nullptr, djac, 0, acc, integ);
             dhdt = -acc[0][0];
             dudt = -acc[0][1];
             dvdt = -acc[0][2];
@@ -532,23 +534,23 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
             auto integ = [&](const double*, const double*, const double* H, const double*, const double*, double dj,
                              bool clipped, const Clip& c, double (&r)[3][3]) {
                 r[0][0] += dj * ((H[0] + H[1] + H[2]) / 3.0);
-                r[0][1] += dj * ((cval(c, clipped, in.u, 0) + cval(c, clipped, in.u, 1) + cval(c, clipped, in.u, 2)) / 3.0);
-                r[0][2] += dj * ((cval(c, clipped, in.v, 0) + cval(c, clipped, in.v, 1) + cval(c, clipped, in.v, 2)) / 3.0);
+                r[0][1] += dj * ((cval(c, clipped, uc, 0) + cval(c, clipped, uc, 1) + cval(c, clipped, uc, 2)) / 3.0);
+                r[0][2] += dj * ((cval(c, clipped, vc, 0) + cval(c, clipped, vc, 1) + cval(c, clipped, vc, 2)) / 3.0);
             };
-            wd_apply(ch, in.x, in.y, in.h, nullptr, nullptr, djac, 0, acc, integ);
+            wd_apply<WET>(in.x, in.y, hc, nullptr, nullptr, djac, 0, acc, integ);
             dhdt += acc[0][0];
             dudt += acc[0][1];
             dvdt += acc[0][2];
         }
-        factor = ch.ret;
+        factor = WET ? 1.0 : clip_factor(in.x, in.y, hc, djac);
         double adv[3] = {0, 0, 0};
         {
             double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
             auto integ = [&](const double*, const double*, const double*, const double* GX, const double* GY, double dj,
                              bool clipped, const Clip& c, double (&r)[3][3]) {
-                double f0 = cval(c, clipped, in.h, 0), f1 = cval(c, clipped, in.h, 1), f2 = cval(c, clipped, in.h, 2);
-                double u0 = cval(c, clipped, in.u, 0), u1 = cval(c, clipped, in.u, 1), u2 = cval(c, clipped, in.u, 2);
-                double v0 = cval(c, clipped, in.v, 0), v1 = cval(c, clipped, in.v, 1), v2 = cval(c, clipped, in.v, 2);
+                double f0 = cval(c, clipped, hc, 0), f1 = cval(c, clipped, hc, 1), f2 = cval(c, clipped, hc, 2);
+                double u0 = cval(c, clipped, uc, 0), u1 = cval(c, clipped, uc, 1), u2 = cval(c, clipped, uc, 2);
+                double v0 = cval(c, clipped, vc, 0), v1 = cval(c, clipped, vc, 1), v2 = cval(c, clipped, vc, 2);
                 double ha = kOne3 * (f0 + f1 + f2), ua = kOne3 * (u0 + u1 + u2), va = kOne3 * (v0 + v1 + v2);
                 double dhdx = GX[0] * f0 + GX[1] * f1 + GX[2] * f2;
                 double dhdy = GY[0] * f0 + GY[1] * f1 + GY[2] * f2;
@@ -560,7 +562,7 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
                 r[0][1] += dj * dt * 1.0 * (ua * dudx + va * dudy);
                 r[0][2] += dj * dt * 1.0 * (ua * dvdx + va * dvdy);
             };
-            wd_apply(ch, in.x, in.y, in.h, gx, gy, djac, 0, acc, integ);
+            wd_apply<WET>(in.x, in.y, hc, gx, gy, djac, 0, acc, integ);
             adv[0] = acc[0][0];
             adv[1] = acc[0][1];
             adv[2] = acc[0][2];
@@ -589,6 +591,25 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, int wd_flag, in
         if (f & 2) { er[i][1] = 0.0; er[i][2] = 0.0; }
         if (f & 4) { er[i][0] = 0.0; er[i][1] = 0.0; er[i][2] = 0.0; }
     }
+}
+
+// general path (some vertex dry at some level, or a wet/dry-flagged element): out of line,
+// so the fully wet path below is not charged the clipping code's registers
+__device__ __noinline__ void elem_resid_general(const ElemIn& in, const double* hc, const double* uc, const double* vc,
+                                                int wd_flag, int pvar, const PhysParams& P, const MatParams& M,
+                                                const int* dflag, double (&er)[3][3]) {
+    elem_resid_impl<false>(in, hc, uc, vc, wd_flag, pvar, P, M, dflag, er);
+}
+
+__device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, const double* hc, const double* uc, const double* vc,
+                                               int wd_flag, int pvar, const PhysParams& P, const MatParams& M,
+                                               const int* dflag, double (&er)[3][3]) {
+    const bool wet = wd_flag == 0 && hc[0] > 0.0 && hc[1] > 0.0 && hc[2] > 0.0 && in.ho[0] > 0.0 &&
+                     in.ho[1] > 0.0 && in.ho[2] > 0.0 && in.hoo[0] > 0.0 && in.hoo[1] > 0.0 && in.hoo[2] > 0.0;
+    if (wet)
+        elem_resid_impl<true>(in, hc, uc, vc, wd_flag, pvar, P, M, dflag, er);
+    else
+        elem_resid_general(in, hc, uc, vc, wd_flag, pvar, P, M, dflag, er);
 }
 
 // ---------------------------------------------------------------------------------

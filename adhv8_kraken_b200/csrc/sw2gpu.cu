@@ -268,7 +268,7 @@ int launch_init(sw2gpu_ctx* c) {     // fe_sw2_init: current = old, Dirichlet va
 }
 
 // scaling, preconditioner setup and the persistent BiCGSTAB; returns its iteration count
-int launch_linear(sw2gpu_ctx* c, int apply_inc, double atol_floor) {
+int launch_linear(sw2gpu_ctx* c, int apply_inc, double rtol) {
     State s = c->state();
     k_rowscale<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->dm, s, c->val.p, c->R.p, c->S_.p, c->bs.p, 0);
     CK(cudaMemsetAsync(c->singular.p, 0, sizeof(int), c->stream));
@@ -286,8 +286,8 @@ int launch_linear(sw2gpu_ctx* c, int apply_inc, double atol_floor) {
     K.col = c->col.p;
     K.S = c->S_.p;
     K.bs = c->bs.p;
-    K.rtol = c->p.lin_rtol;
-    K.atol = std::max(c->p.lin_atol, atol_floor);
+    K.rtol = rtol;
+    K.atol = c->p.lin_atol;
     K.maxit = c->p.max_lin_it;
     K.h = c->H(0);
     K.u = c->U(0);
@@ -664,7 +664,7 @@ int sw2gpu_linear_solve(sw2gpu_ctx* c, const double* val, const double* rhs, dou
     if (!c || !val || !rhs || !x) return fail(SW2GPU_E_ARG, "null argument");
     CK(cudaMemcpyAsync(c->val.p, val, sizeof(double) * 9 * (size_t)c->nnzb, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->R.p, rhs, sizeof(double) * 3 * c->V, cudaMemcpyHostToDevice, c->stream));
-    int rc = launch_linear(c, 0, 0.0);
+    int rc = launch_linear(c, 0, c->p.lin_rtol);
     if (rc) return rc;
     CK(cudaMemcpyAsync(x, c->sol.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -697,25 +697,32 @@ int sw2gpu_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* st
     double rmax = nm.rmax, l2 = std::sqrt(nm.l2sum / n3), imax = nm.imax, old_l2;
     int it = 0, lin_total = 0, cuts_total = 0;
     bool solv_ok = true, nan = nm.nan != 0, keep;
-    // Krylov accuracy is measured against the first Newton system of the step: later
-    // systems have tiny right-hand sides, where a purely relative test would ask for
-    // accuracy below the FP64 round-off of the operator itself
-    double atol_floor = 0.0;
+    // Inexact Newton: the linear residual of iteration k only needs to be small next to
+    // the Newton tolerance, so the Krylov test is relative with
+    //   eta_k = max(lin_rtol, kEtaNtl * tol_nonlin / max|R_k|)      (capped at 1e-5).
+    // Early iterations (large R) solve to near round-off like the reference's exact LU;
+    // late ones (R close to tol_nonlin) stop early.  A solve that reaches max_lin_it
+    // but reduced its residual by kAcceptRel is accepted: its error is already far below
+    // what the next residual evaluation can see.
+    constexpr double kEtaNtl = 1e-4, kAcceptRel = 1e-8;
     if (nan) solv_ok = false;
     do {
         if (!solv_ok) break;
         if ((rc = launch_jacobian(c))) return rc;
-        if ((rc = launch_linear(c, 1, atol_floor))) return rc;
+        const double eta = std::min(1e-5, std::max(p.lin_rtol, kEtaNtl * p.tol_nonlin / std::max(rmax, 1e-300)));
+        if ((rc = launch_linear(c, 1, eta))) return rc;
         old_l2 = l2;
         if ((rc = launch_resid(c))) return rc;
         if ((rc = read_norms(c, nm))) return rc;   // also completes the Krylov control read
         if (c->ctl_h->err) return fail(SW2GPU_E_TIMEOUT, "Krylov grid barrier wait ran out");
         lin_total += c->ctl_h->iterations;
-        if (it == 0) atol_floor = p.lin_rtol * c->ctl_h->bnorm;
-        // the plain path fails the step when BiCGSTAB hits max_lin_it (solv_bcgstab.c:280-292);
-        // on the mixed path the FP32 inner solve is a correction refined by the FP64 Newton
-        // loop, so its last iterate is accepted (the reference's force_lin_it behaviour)
-        if (!c->ctl_h->converged && p.precision != SW2GPU_MIXED) solv_ok = false;
+        // the plain path fails the step when BiCGSTAB hits max_lin_it without a useful
+        // reduction (solv_bcgstab.c:280-292); on the mixed path the FP32 inner solve is a
+        // correction refined by the FP64 Newton loop, so its last iterate is accepted (the
+        // reference's force_lin_it behaviour)
+        if (!c->ctl_h->converged && p.precision != SW2GPU_MIXED &&
+            !(c->ctl_h->rnorm <= kAcceptRel * c->ctl_h->bnorm))
+            solv_ok = false;
         rmax = nm.rmax;
         l2 = std::sqrt(nm.l2sum / n3);
         imax = nm.imax;

@@ -23,4 +23,16 @@ def set_load_state(solver, model, ref, prefix="load0"):
 
 
 def fields(h, u, v):
+    """Depth and unit discharge q = (uh, vh); used with field_errors()."""
     return {"h": h, "uh": h * u, "vh": h * v}
+
+
+def field_errors(got, exp):
+    """Relative errors per field: depth against max|h|; the unit-discharge field as a vector,
+    max |q_got - q_exp| / max |q_exp| (its components alone can be round-off noise, e.g. vh
+    in a straight channel)."""
+    import numpy as np
+    eh = float(np.abs(got["h"] - exp["h"]).max() / np.abs(exp["h"]).max())
+    dq = np.hypot(got["uh"] - exp["uh"], got["vh"] - exp["vh"])
+    qm = float(np.hypot(exp["uh"], exp["vh"]).max())
+    return {"h": eh, "q": float(dq.max() / max(qm, 1e-300))}

@@ -8,7 +8,7 @@ import pytest
 from adhv8_kraken_b200 import capi, meshgen
 from adhv8_kraken_b200.sw2 import SW2GPU, run
 from conftest import relerr
-from helpers import basin_model, channel_model, fields, set_load_state
+from helpers import basin_model, channel_model, field_errors, fields, set_load_state
 from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -78,8 +78,7 @@ def _run_against(model, ref, nsteps, check_every, precision=capi.SW2GPU_FP64, to
         if (k + 1) in check_every:
             got = fields(*g.get_state(0))
             exp = fields(ref[f"step{k+1}_h"], ref[f"step{k+1}_u"], ref[f"step{k+1}_v"])
-            for f in got:
-                e = relerr(got[f], exp[f])
+            for f, e in field_errors(got, exp).items():
                 worst = max(worst, e)
                 assert e <= tol, (k, f, e)
             if wd:
