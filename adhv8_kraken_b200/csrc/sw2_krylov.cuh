@@ -20,6 +20,7 @@ namespace sw2 {
 
 constexpr int kKrylovThreads = 256;
 constexpr long long kBarrierSpinLimit = 1ll << 26;   // bounded wait (~seconds), then error
+constexpr int kStall = 40;                           // iterations without a new best residual
 
 struct KrylovCtl {
     unsigned count;       // barrier arrival counter
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
                                                             const MT* __restrict__ Dinv, VT* __restrict__ b,
                                                             VT* __restrict__ uu, VT* __restrict__ r,
                                                             VT* __restrict__ q, VT* __restrict__ p, VT* __restrict__ Ap,
-                                                            VT* __restrict__ As) {
+                                                            VT* __restrict__ As, VT* __restrict__ ubest) {
     const int V = K.V;
     const int stride = gridDim.x * blockDim.x;
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -239,7 +240,14 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
         double rho = red[2], rhop = 1.0, alpha = 1.0, omega = 1.0;
         int it = 0;
         const double tol = K.atol + bnorm * K.rtol;
-        while (rnorm > tol && it < K.maxit) {
+        // best iterate so far: past its attainable accuracy BiCGSTAB's residual drifts back up,
+        // so on stagnation (no new best for kStall iterations) or at max_lin_it the best one is used
+        double best = rnorm;
+        int best_it = 0;
+        for (int i = t0; i < V; i += stride)
+#pragma unroll
+            for (int c = 0; c < 3; c++) ubest[3 * i + c] = uu[3 * i + c];
+        while (rnorm > tol && it < K.maxit && it - best_it < kStall) {
             it++;
             // (d)-(e): Ap = M^-1 A p, gamma = q . Ap
             {
@@ -320,13 +328,22 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
                 grid_allreduce<1>(pbuf(), mm, mx);
                 nred++;
                 rnorm = mx[0];
+                if (rnorm < best) {   // identical decision in every block; own rows only
+                    best = rnorm;
+                    best_it = it;
+                    for (int i = t0; i < V; i += stride)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) ubest[3 * i + c] = uu[3 * i + c];
+                }
             }
         }
+        const bool conv = rnorm <= tol;
         // x = S u; state += x; sol = -x
+        const VT* ux = conv ? uu : ubest;
         for (int i = t0; i < V; i += stride) {
-            const double x0 = (double)ldv(uu + 3 * i) * K.S[3 * i];
-            const double x1 = (double)ldv(uu + 3 * i + 1) * K.S[3 * i + 1];
-            const double x2 = (double)ldv(uu + 3 * i + 2) * K.S[3 * i + 2];
+            const double x0 = (double)ldv(ux + 3 * i) * K.S[3 * i];
+            const double x1 = (double)ldv(ux + 3 * i + 1) * K.S[3 * i + 1];
+            const double x2 = (double)ldv(ux + 3 * i + 2) * K.S[3 * i + 2];
             if (K.apply_inc) {
                 K.u[i] += x0;
                 K.v[i] += x1;
@@ -342,8 +359,8 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             ctl->iterations = it;
-            ctl->converged = (it == K.maxit) ? 0 : 1;
-            ctl->rnorm = rnorm;
+            ctl->converged = conv ? 1 : 0;
+            ctl->rnorm = conv ? rnorm : best;
             ctl->bnorm = bnorm;
         }
     }

@@ -91,7 +91,7 @@ struct sw2gpu_ctx {
     DBuf<double> sc, sx, sy, R, sol, jslots, val, S_, bs;
     DBuf<float> val32, dinv32;
     DBuf<double> dinv64;
-    DBuf<double> kv64[7];
+    DBuf<double> kv64[8];
     DBuf<double> part;
     DBuf<KrylovCtl> ctl;
     DBuf<Norms> npart, norms;
@@ -302,15 +302,15 @@ int launch_linear(sw2gpu_ctx* c, int apply_inc, double rtol) {
         const float* A = c->val32.p;
         const float* D = c->dinv32.p;
         double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
-               *Ap = c->kv64[5].p, *As = c->kv64[6].p;
-        void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As};
+               *Ap = c->kv64[5].p, *As = c->kv64[6].p, *ub = c->kv64[7].p;
+        void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As, &ub};
         CK(cudaLaunchCooperativeKernel((void*)k_bicgstab<float, double>, grid, block, args, 0, c->stream));
     } else {
         const double* A = c->val.p;
         const double* D = c->dinv64.p;
         double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
-               *Ap = c->kv64[5].p, *As = c->kv64[6].p;
-        void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As};
+               *Ap = c->kv64[5].p, *As = c->kv64[6].p, *ub = c->kv64[7].p;
+        void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As, &ub};
         CK(cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double>, grid, block, args, 0, c->stream));
     }
     c->launches += 3;

@@ -58,14 +58,14 @@ def test_linear_solve_matches_direct_solve(channel_ref):
     import scipy.sparse as sp
     import scipy.sparse.linalg as spla
     model = channel_model()
-    g = SW2GPU(model, lin_rtol=1e-13, lin_atol=0.0)
+    g = SW2GPU(model, lin_rtol=1e-10, lin_atol=0.0)
     V = model.nnodes
     A = sp.bsr_matrix((channel_ref["load0_val"], channel_ref["load0_col"], channel_ref["load0_rowptr"]),
                       shape=(3 * V, 3 * V)).tocsc()
     b = channel_ref["load0_resid"]
     x, its, rc = g.linear_solve(channel_ref["load0_val"], b)
     assert rc == 0 and its > 0
-    assert relerr(x, spla.spsolve(A, b)) <= 1e-9
+    assert relerr(x, spla.spsolve(A, b)) <= 1e-7
 
 
 def _run_against(model, ref, nsteps, check_every, precision=capi.SW2GPU_FP64, tol=1e-10, wd=False, **kw):
