@@ -201,7 +201,9 @@ def run_ours(args, rank, world, local_rank):
     lin = sum(s["linear_its"] for s in stats)
     nnzb = g.nnzb
     hbm, src = peaks()
-    # algorithmic bytes per launch ("Roofline accounting")
+    # algorithmic bytes per launch: FD Jacobian = element inputs + node state + 81 outputs per
+    # triangle; BiCGSTAB iteration = two SpMV passes over the BCSR values, column indices,
+    # row pointers and block-Jacobi inverses plus 14 vector streams of 3 doubles per node
     jac_bytes = T * (3 * 4 + 7 * 8 + 4 + 4 + 1) + V * 12 * 8 + T * 81 * 8       # gather + element data + 81 outputs
     kry_iter_bytes = 2 * (nnzb * (9 * 8 + 4) + (V + 1) * 4 + V * 9 * 8) + V * 3 * 8 * 14
     kernels = {

@@ -93,7 +93,14 @@ def _sources(src: str):
     return sorted(set(srcs))
 
 
-def build(src: str = "/root/reference/src", jobs: int = os.cpu_count() or 4) -> str:
+REFERENCE_SRC = "/root/reference/src"
+
+
+def sources_present(src: str = REFERENCE_SRC) -> bool:
+    return os.path.isdir(src)
+
+
+def build(src: str = REFERENCE_SRC, jobs: int = os.cpu_count() or 4) -> str:
     exe = os.path.join(OUT, "adh_dump")
     if not os.path.isdir(src):
         if os.path.exists(exe):
@@ -127,4 +134,4 @@ def build(src: str = "/root/reference/src", jobs: int = os.cpu_count() or 4) -> 
 
 
 if __name__ == "__main__":
-    print(build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"))
+    print(build(sys.argv[1] if len(sys.argv) > 1 else REFERENCE_SRC))
