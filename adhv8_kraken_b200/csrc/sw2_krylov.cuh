@@ -14,7 +14,7 @@
 // On exit the kernel applies the Newton increment: x = S u, state += x (fe_sw2_inc),
 // sol = -x (fe_newton.c:561-585).
 #pragma once
-#include "sw2_kernels.cuh"
+#include <cuda_runtime.h>
 
 namespace sw2 {
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/sw2gpu.h"
+#include "sw2_kernels.cuh"
 #include "sw2_krylov.cuh"
 
 using namespace sw2;
@@ -62,6 +63,9 @@ struct DBuf {
 };
 
 }  // namespace
+
+// lets other translation units of this library report through sw2gpu_last_error()
+__attribute__((visibility("hidden"))) void sw2gpu_internal_set_error(const char* msg) { g_err = msg; }
 
 struct sw2gpu_ctx {
     cudaStream_t stream = nullptr;

@@ -1,0 +1,214 @@
+// sw2gpu_noalloc.cu -- the allocation-free variant of the device linear solve.
+//
+// Some callers cannot let a library allocate GPU memory during a solve: applications
+// that own all device memory themselves (a fixed arena sized once at start-up, as a
+// coupled model's time loop or a long-running serving process does) and must not have
+// a call inside their step run cudaMalloc, which can synchronize the device, can fail
+// half-way through a run, and is invisible to their memory accounting.  For them,
+// sw2gpu_bcsr_solve_noalloc() solves a 3x3-block CSR system that lives entirely in the
+// caller's device buffers, using as its only work memory the file-scope array below.
+//
+// The array is a static __device__ allocation of kScratchDoubles doubles (14.6 MB): every
+// GPU that loads this library holds it until the process exits.  Its size bounds the
+// problem: at most SW2GPU_NOALLOC_MAX_NODES node rows and SW2GPU_NOALLOC_MAX_BLOCKS
+// blocks; larger systems are rejected.  All calls share the one array and it keeps the
+// previous call's contents, so the barrier/control words are cleared on every call, and
+// two calls that overlap on the GPU (different streams, or different host threads at
+// once) race on it and corrupt each other's results.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+
+#include "../../include/sw2gpu.h"
+#include "sw2_krylov.cuh"
+
+using namespace sw2;
+
+namespace {
+
+constexpr double kSmall = 2.220446049250313e-16;   // DBL_EPSILON, the spv_jacobi floor
+constexpr int kMaxNodes = SW2GPU_NOALLOC_MAX_NODES;
+constexpr int kMaxBlocks = SW2GPU_NOALLOC_MAX_BLOCKS;
+constexpr int kMaxGrid = (kMaxNodes + kKrylovThreads - 1) / kKrylovThreads;   // persistent-kernel blocks
+constexpr size_t kAlign = 32;                                                 // doubles = 256 bytes
+constexpr size_t al(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
+// layout (in doubles): control word, partials, S, b', Dinv, scaled matrix, 8 Krylov vectors
+constexpr size_t kOffCtl = 0;
+constexpr size_t kOffPart = kOffCtl + al((sizeof(KrylovCtl) + 7) / 8);
+constexpr size_t kOffS = kOffPart + al(2ull * kMaxGrid * 4);
+constexpr size_t kOffB = kOffS + al(3ull * kMaxNodes);
+constexpr size_t kOffDinv = kOffB + al(3ull * kMaxNodes);
+constexpr size_t kOffA = kOffDinv + al(9ull * kMaxNodes);
+constexpr size_t kOffVec = kOffA + al(9ull * kMaxBlocks);
+constexpr size_t kScratchDoubles = kOffVec + 8 * al(3ull * kMaxNodes);
+
+static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
+
+std::mutex g_setup_mutex;
+double* g_scratch_dev[128] = {nullptr};   // device address of the array, per device ordinal
+
+}  // namespace
+
+// error text shared with sw2gpu_last_error() (defined in sw2gpu.cu, not exported)
+void sw2gpu_internal_set_error(const char* msg);
+
+namespace {
+
+int na_fail(int code, const char* msg) {
+    sw2gpu_internal_set_error(msg);
+    return code;
+}
+
+// S = 1/sqrt(max |row entry|) (spv_jacobi) and b' = S rhs, one thread per node row
+__global__ void k_na_rowscale(int V, const int* __restrict__ rowptr, const double* __restrict__ val,
+                              const double* __restrict__ rhs, double* __restrict__ S, double* __restrict__ bs) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= V) return;
+    double mx[3] = {0.0, 0.0, 0.0};
+    for (int k = rowptr[n]; k < rowptr[n + 1]; k++)
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) mx[r] = fmax(mx[r], fabs(val[(size_t)k * 9 + 3 * r + c]));
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const double sv = (mx[r] < kSmall) ? 1.0 / sqrt(kSmall) : 1.0 / sqrt(fabs(mx[r]));
+        S[3 * n + r] = sv;
+        bs[3 * n + r] = rhs[3 * n + r] * sv;
+    }
+}
+
+// A' = S A S into the scratch copy and the inverse of each scaled diagonal block,
+// one thread per node row (the caller's matrix is not modified)
+__global__ void k_na_scale(int V, const int* __restrict__ rowptr, const int* __restrict__ col,
+                           const double* __restrict__ val, const double* __restrict__ S, double* __restrict__ Aout,
+                           double* __restrict__ dinv, int* __restrict__ singular) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    bool have_diag = false;
+    for (int k = rowptr[i]; k < rowptr[i + 1]; k++) {
+        const int j = col[k];
+        double a[9];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) a[3 * r + c] = val[(size_t)k * 9 + 3 * r + c] * (S[3 * i + r] * S[3 * j + c]);
+#pragma unroll
+        for (int q = 0; q < 9; q++) Aout[(size_t)k * 9 + q] = a[q];
+        if (j != i) continue;
+        have_diag = true;
+        const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+        const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+        double inv[9];
+        if (det == 0.0 || !isfinite(det)) {
+            *singular = 1;
+#pragma unroll
+            for (int q = 0; q < 9; q++) inv[q] = (q % 4 == 0) ? 1.0 : 0.0;
+        } else {
+            const double id = 1.0 / det;
+            inv[0] = c00 * id;
+            inv[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+            inv[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+            inv[3] = c01 * id;
+            inv[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+            inv[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+            inv[6] = c02 * id;
+            inv[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+            inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+        }
+#pragma unroll
+        for (int q = 0; q < 9; q++) dinv[(size_t)i * 9 + q] = inv[q];
+    }
+    if (!have_diag) {
+        *singular = 1;
+#pragma unroll
+        for (int q = 0; q < 9; q++) dinv[(size_t)i * 9 + q] = (q % 4 == 0) ? 1.0 : 0.0;
+    }
+}
+
+// device address of the scratch array for the current device (looked up once per device)
+int scratch_for_current_device(double** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return na_fail(SW2GPU_E_CUDA, "no current CUDA device");
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_dev[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return na_fail(SW2GPU_E_CUDA, cudaGetErrorString(e));
+        g_scratch_dev[dev] = (double*)p;
+    }
+    *out = g_scratch_dev[dev];
+    return SW2GPU_OK;
+}
+
+}  // namespace
+
+extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int32_t* row_ptr, const int32_t* col,
+                                         const double* val, const double* rhs, double* x, double rtol, double atol,
+                                         int32_t max_it, void* stream, int32_t* iterations) {
+    if (nnodes <= 0 || nnzb <= 0 || !row_ptr || !col || !val || !rhs || !x || max_it <= 0)
+        return na_fail(SW2GPU_E_ARG, "sw2gpu_bcsr_solve_noalloc: bad argument");
+    if (nnodes > kMaxNodes || nnzb > kMaxBlocks) {
+        char buf[200];
+        snprintf(buf, sizeof buf,
+                 "sw2gpu_bcsr_solve_noalloc: system of %d nodes / %d blocks exceeds the fixed scratch limit "
+                 "of %d nodes / %d blocks",
+                 nnodes, nnzb, kMaxNodes, kMaxBlocks);
+        return na_fail(SW2GPU_E_ARG, buf);
+    }
+    double* sc = nullptr;
+    int rc = scratch_for_current_device(&sc);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    KrylovCtl* ctl = reinterpret_cast<KrylovCtl*>(sc + kOffCtl);
+    double* part = sc + kOffPart;
+    double* S = sc + kOffS;
+    double* bs = sc + kOffB;
+    double* dinv = sc + kOffDinv;
+    double* A = sc + kOffA;
+    double* v[8];
+    for (int k = 0; k < 8; k++) v[k] = sc + kOffVec + k * al(3ull * kMaxNodes);
+    // the control words (barrier counter and generation, error and result fields) must
+    // start at zero; everything else is written before it is read
+    if (cudaMemsetAsync(ctl, 0, sizeof(KrylovCtl), st) != cudaSuccess)
+        return na_fail(SW2GPU_E_CUDA, "cudaMemsetAsync of the control words failed");
+    int* singular = reinterpret_cast<int*>(&ctl->pad);
+    const int nb = (nnodes + 255) / 256;
+    k_na_rowscale<<<nb, 256, 0, st>>>(nnodes, row_ptr, val, rhs, S, bs);
+    k_na_scale<<<nb, 256, 0, st>>>(nnodes, row_ptr, col, val, S, A, dinv, singular);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double>, kKrylovThreads, 0);
+    const int grid = std::max(1, std::min({kMaxGrid, (nnodes + kKrylovThreads - 1) / kKrylovThreads,
+                                           sms * std::max(per_sm, 1)}));
+    KrylovArgs K;
+    K.V = nnodes;
+    K.rowptr = row_ptr;
+    K.col = col;
+    K.S = S;
+    K.bs = bs;
+    K.rtol = rtol;
+    K.atol = atol;
+    K.maxit = max_it;
+    K.h = K.u = K.v = nullptr;
+    K.sol = x;
+    K.apply_inc = 0;
+    K.part = part;
+    K.ctl = ctl;
+    const double* Ac = A;
+    const double* Dc = dinv;
+    void* args[] = {&K, &Ac, &Dc, &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7]};
+    cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double>, dim3(grid), dim3(kKrylovThreads),
+                                                args, 0, st);
+    if (e != cudaSuccess) return na_fail(SW2GPU_E_CUDA, cudaGetErrorString(e));
+    KrylovCtl h;
+    e = cudaMemcpyAsync(&h, ctl, sizeof(KrylovCtl), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return na_fail(SW2GPU_E_CUDA, cudaGetErrorString(e));
+    if (iterations) *iterations = h.iterations;
+    if (h.err) return na_fail(SW2GPU_E_TIMEOUT, "Krylov grid barrier wait ran out");
+    return h.converged ? SW2GPU_OK : na_fail(SW2GPU_E_LINEAR, "BiCGSTAB did not reach the tolerance");
+}

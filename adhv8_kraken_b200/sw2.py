@@ -28,7 +28,7 @@ _lib = None
 SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_destroy", "sw2gpu_set_state",
            "sw2gpu_get_state", "sw2gpu_get_wd_flag", "sw2gpu_set_wd_flag", "sw2gpu_step", "sw2gpu_set_dt",
            "sw2gpu_resid", "sw2gpu_load", "sw2gpu_linear_solve", "sw2gpu_batch_create", "sw2gpu_batch_step",
-           "sw2gpu_batch_destroy"]
+           "sw2gpu_batch_destroy", "sw2gpu_bcsr_solve_noalloc"]
 
 
 class SW2Error(RuntimeError):
@@ -60,6 +60,8 @@ def lib():
         L.sw2gpu_batch_create.argtypes = [C.POINTER(vp), C.c_int32, vp, C.POINTER(vp)]
         L.sw2gpu_batch_step.argtypes = [vp, c_double_p, C.POINTER(c_double_p), vp]
         L.sw2gpu_batch_destroy.argtypes = [vp]
+        L.sw2gpu_bcsr_solve_noalloc.argtypes = [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
+                                                C.c_int32, vp, c_int32_p]
         _lib = L
     return _lib
 

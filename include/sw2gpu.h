@@ -144,6 +144,25 @@ int sw2gpu_load(sw2gpu_ctx *ctx, int32_t *nnzb, int32_t *row_ptr, int32_t *col, 
  * uses the pattern of the context. */
 int sw2gpu_linear_solve(sw2gpu_ctx *ctx, const double *val, const double *rhs, double *x, int32_t *iterations);
 
+/* Allocation-free linear solve.  No counterpart in the reference: it exists for callers
+ * that own all of their GPU memory (a fixed arena sized at start-up, as a coupled model's
+ * time loop or a serving process has) and cannot let a library call cudaMalloc during a
+ * step, since that can synchronize the device, fail mid-run and escape their accounting.
+ * Solves the 3x3-block CSR system (row_ptr[nnodes+1], col[nnzb], val[9*nnzb], rhs[3*nnodes]
+ * -> x[3*nnodes], all DEVICE pointers owned by the caller) with the same Jacobi scaling and
+ * block-Jacobi BiCGSTAB as sw2gpu_linear_solve; the stopping test is
+ * ||r||inf <= atol + rtol ||M^-1 S rhs||inf.  Its only work memory is one file-scope device
+ * array of about 14.6 MB that every GPU loading the library keeps until exit, so systems
+ * above SW2GPU_NOALLOC_MAX_NODES rows or SW2GPU_NOALLOC_MAX_BLOCKS blocks are rejected with
+ * SW2GPU_E_ARG.  The first call on a device looks up that array's device address (make it
+ * before any stream capture).  All calls share the array: calls that overlap on the GPU
+ * race and corrupt each other.  Returns SW2GPU_E_LINEAR if max_it is reached. */
+#define SW2GPU_NOALLOC_MAX_NODES  16384
+#define SW2GPU_NOALLOC_MAX_BLOCKS 131072
+int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int32_t *row_ptr, const int32_t *col,
+                              const double *val, const double *rhs, double *x, double rtol, double atol,
+                              int32_t max_it, void *stream, int32_t *iterations);
+
 /* Batched ensemble: many independent contexts stepped by one persistent launch per
  * phase over a concatenated BCSR with per-instance offsets. */
 typedef struct sw2gpu_batch sw2gpu_batch;
