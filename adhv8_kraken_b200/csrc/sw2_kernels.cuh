@@ -38,8 +38,13 @@ struct State {
 struct Norms {                  // get_residual_norms (src/fe/fe_newton.c:40-151)
     double rmax, l2sum, imax;
     int nan;
-    int pad;
+    int ngeneral;               // elements on the wet/dry (general) Jacobian list
 };
+
+// An element takes the fully wet Jacobian path when its flag is 0 and every vertex depth
+// at all three levels is positive with a margin no finite-difference perturbation of h
+// (|eps| <= max(1.5e-8, 1.5e-8 |h|)) can cross; every other element goes on the list.
+constexpr double kWetMargin = 1e-6;
 
 __device__ __forceinline__ void load_elem(const DevMesh& m, const State& s, int e, int rule_vel, ElemIn& in, int* n,
                                           int* df) {
@@ -75,16 +80,46 @@ __device__ __forceinline__ void load_elem(const DevMesh& m, const State& s, int 
 
 // Residual contributions of every 2D element and boundary edge (fe_sw2_resid :51-191).
 // slots: 3 SoA arrays (c, x, y) of length 3T + 2E.
+__device__ __forceinline__ bool wet_depths(const double* h, const double* ho, const double* hoo) {
+    bool wet = true;
+#pragma unroll
+    for (int i = 0; i < 3; i++) wet = wet && h[i] > kWetMargin && ho[i] > 0.0 && hoo[i] > 0.0;
+    return wet;
+}
+__device__ __forceinline__ void classify_elem(int t, bool wet, unsigned char* ewet, int* glist, int* gcount) {
+    ewet[t] = wet ? 1 : 0;
+    if (!wet) glist[atomicAdd(gcount, 1)] = t;   // list order is free: each element is independent
+}
+
+// the same classification without a residual (sw2gpu_load called on its own)
+__global__ void k_classify(DevMesh m, State s, unsigned char* __restrict__ ewet, int* __restrict__ glist,
+                           int* __restrict__ gcount) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.T) return;
+    double h[3], ho[3], hoo[3];
+    const int n[3] = {m.en0[t], m.en1[t], m.en2[t]};
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        h[i] = s.h[n[i]];
+        ho[i] = s.ho[n[i]];
+        hoo[i] = s.hoo[n[i]];
+    }
+    classify_elem(t, s.wd[t] == 0 && wet_depths(h, ho, hoo), ewet, glist, gcount);
+}
+
 __global__ void k_resid_elem(DevMesh m, State s, PhysParams P, double* __restrict__ sc, double* __restrict__ sx,
-                             double* __restrict__ sy) {
+                             double* __restrict__ sy, unsigned char* __restrict__ ewet, int* __restrict__ glist,
+                             int* __restrict__ gcount) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int nslot = 3 * m.T + 2 * m.E;
     if (t < m.T) {
         ElemIn in;
         int n[3], df[3];
         load_elem(m, s, t, 1, in, n, df);
+        const int wd = s.wd[t];
+        classify_elem(t, wd == 0 && wet_depths(in.h, in.ho, in.hoo), ewet, glist, gcount);
         double er[3][3];
-        sw2_elem_resid(in, in.h, in.u, in.v, s.wd[t], kPertNone, P, m.mats[m.emat[t]], df, er);
+        sw2_elem_resid(in, in.h, in.u, in.v, wd, kPertNone, P, m.mats[m.emat[t]], df, er);
 #pragma unroll
         for (int i = 0; i < 3; i++) {
             const bool dry = in.ho[i] <= 0.;
@@ -160,7 +195,8 @@ __global__ void __launch_bounds__(kGatherThreads) k_resid_gather(DevMesh m, Stat
                                                                  const double* __restrict__ sx,
                                                                  const double* __restrict__ sy, double* __restrict__ R,
                                                                  const double* __restrict__ sol, Norms* partial,
-                                                                 unsigned* counter, Norms* out) {
+                                                                 unsigned* counter, Norms* out,
+                                                                 const int* __restrict__ gcount) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     double rmax = 0.0, l2 = 0.0, imax = 0.0;
     int nan = 0;
@@ -208,7 +244,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_resid_gather(DevMesh m, Stat
         }
         block_reduce3<kGatherThreads>(a, b, c, d);
         if (threadIdx.x == 0) {
-            *out = Norms{a, b, c, d, 0};
+            *out = Norms{a, b, c, d, *gcount};
             *counter = 0u;
         }
     }
@@ -228,16 +264,28 @@ struct __align__(16) StagedElem {
     int n[3], df[3], wd, mat;
 };
 
-__global__ void __launch_bounds__(kJacThreads) k_jac_elem(DevMesh m, State s, PhysParams P,
-                                                           double* __restrict__ jslots) {
+// GENERAL = false: every element, fully wet physics inlined (register-lean), elements not
+// eligible for it are skipped (their records are rewritten by the general launch, which runs
+// after it on the same stream).  GENERAL = true: the elements of `list`, full wet/dry physics.
+template <bool GENERAL>
+__device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, const PhysParams& P,
+                                              double* __restrict__ jslots, const unsigned char* __restrict__ ewet,
+                                              const int* __restrict__ list, int count) {
     __shared__ StagedElem se[kJacElems];
     __shared__ double out[kJacElems * 81];
+    __shared__ int eid[kJacElems];
     const int e0 = blockIdx.x * kJacElems;
     const int lane = threadIdx.x % kJacElems;
     const int item = threadIdx.x / kJacElems;
+    const int nel = min(kJacElems, count - e0);
     if (item == 0) {
-        const int e = e0 + lane;
-        if (e < m.T) {
+        int e = -1;
+        if (lane < nel) {
+            e = GENERAL ? list[e0 + lane] : e0 + lane;
+            if (!GENERAL && !ewet[e]) e = -1;
+        }
+        eid[lane] = e;
+        if (e >= 0) {
             StagedElem& S = se[lane];
             load_elem(m, s, e, 0, S.in, S.n, S.df);
             S.wd = s.wd[e];
@@ -245,8 +293,7 @@ __global__ void __launch_bounds__(kJacThreads) k_jac_elem(DevMesh m, State s, Ph
         }
     }
     __syncthreads();
-    const int e = e0 + lane;
-    if (e < m.T) {
+    if (eid[lane] >= 0) {
         const StagedElem& S = se[lane];
         const int b = item / 3, var = item % 3;  // var: 0 = u, 1 = v, 2 = h
         // only the current iterate (9 values) is private; everything else is read from the
@@ -267,22 +314,6 @@ __global__ void __launch_bounds__(kJacThreads) k_jac_elem(DevMesh m, State s, Ph
         }
         const double eps = fd_eps(cur);
         const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
-        double rp[3][3], rm[3][3];
-        auto setp = [&](double val) {
-#pragma unroll
-            for (int i = 0; i < 3; i++) {
-                if (i == b) {
-                    if (var == 0) uc[i] = val;
-                    else if (var == 1) vc[i] = val;
-                    else hc[i] = val;
-                }
-            }
-        };
-        setp(cur + eps);
-        sw2_elem_resid(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, rp);
-        setp(cur - eps);
-        sw2_elem_resid(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, rm);
-        const double e2 = 2.0 * eps;
         // Dirichlet zeroing of the element matrix (fe_assign_mom_db_dof3 / fe_assign_dacont_db_dof3):
         // D = momentum-Dirichlet nodes (old-dry or VEL/VEL_PRS string), P = continuity-Dirichlet.
         unsigned Dm = 0, Pm = 0;
@@ -295,26 +326,73 @@ __global__ void __launch_bounds__(kJacThreads) k_jac_elem(DevMesh m, State s, Ph
             if (f & 4) { Dm |= 1u << i; Pm |= 1u << i; }
         }
         double* o = out + lane * 81;
+        const double e2 = 2.0 * eps;
+        // pass 0 stores R(x + eps e_j) in this thread's 9 output entries, pass 1 turns them
+        // into the central difference; one residual body is instantiated, not two
+#pragma unroll 1
+        for (int pass = 0; pass < 2; pass++) {
+            const double xv = pass == 0 ? cur + eps : cur - eps;
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
+            for (int i = 0; i < 3; i++) {
+                if (i == b) {
+                    if (var == 0) uc[i] = xv;
+                    else if (var == 1) vc[i] = xv;
+                    else hc[i] = xv;
+                }
+            }
+            double r[3][3];
+            if (GENERAL) sw2_elem_resid(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, r);
+            else elem_resid_impl<true>(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, r);
 #pragma unroll
-            for (int eq = 0; eq < 3; eq++) {
-                double val = (rp[a][eq] - rm[a][eq]) / e2;
-                const int row = (eq == 0) ? 2 : eq - 1;  // block rows: x-mom, y-mom, continuity
-                const bool aD = (Dm >> a) & 1u, bD = (Dm >> b) & 1u, aP = (Pm >> a) & 1u, bP = (Pm >> b) & 1u;
-                const bool zero = (aD && row < 2) || (bD && var < 2) || (aP && row == 2) || (bP && var == 2);
-                const bool one = (a == b) && ((aD && ((var == 0 && row == 0) || (var == 1 && row == 1))) ||
-                                              (aP && var == 2 && row == 2));
-                if (one) val = 1.0;
-                else if (zero) val = 0.0;
-                o[(3 * a + b) * 9 + 3 * row + var] = val;
+            for (int a = 0; a < 3; a++) {
+#pragma unroll
+                for (int eq = 0; eq < 3; eq++) {
+                    const int row = (eq == 0) ? 2 : eq - 1;  // block rows: x-mom, y-mom, continuity
+                    double& slot = o[(3 * a + b) * 9 + 3 * row + var];
+                    if (pass == 0) {
+                        slot = r[a][eq];
+                        continue;
+                    }
+                    double val = (slot - r[a][eq]) / e2;
+                    const bool aD = (Dm >> a) & 1u, bD = (Dm >> b) & 1u, aP = (Pm >> a) & 1u, bP = (Pm >> b) & 1u;
+                    const bool zero = (aD && row < 2) || (bD && var < 2) || (aP && row == 2) || (bP && var == 2);
+                    const bool one = (a == b) && ((aD && ((var == 0 && row == 0) || (var == 1 && row == 1))) ||
+                                                  (aP && var == 2 && row == 2));
+                    if (one) val = 1.0;
+                    else if (zero) val = 0.0;
+                    slot = val;
+                }
             }
         }
     }
     __syncthreads();
-    const int nel = min(kJacElems, m.T - e0);
-    double* dst = jslots + (size_t)e0 * 81;
-    for (int k = threadIdx.x; k < nel * 81; k += blockDim.x) dst[k] = out[k];
+    if (!GENERAL) {
+        double* dst = jslots + (size_t)e0 * 81;
+        for (int k = threadIdx.x; k < nel * 81; k += blockDim.x)
+            if (eid[k / 81] >= 0) dst[k] = out[k];
+    } else {
+        for (int k = threadIdx.x; k < nel * 81; k += blockDim.x)
+            jslots[(size_t)eid[k / 81] * 81 + k % 81] = out[k];
+    }
+}
+
+// FD Jacobian of the 2D elements (fe_sw2_load :85-142, perturb_sw2_head / perturb_sw2_vel).
+// One CTA = kJacElems elements x 9 perturbation columns (node b, variable u/v/h); warp w
+// evaluates column w for 32 elements, so the pressure-term branch is warp-uniform.
+// Element data are staged in shared memory once; the 9x9 element matrices are staged
+// in shared memory and written out as contiguous 81-double records (slot 9e + 3a + b).
+#ifndef SW2_JAC_MIN_BLOCKS
+#define SW2_JAC_MIN_BLOCKS 2   // resident CTAs per SM the wet kernel's register budget is cut for
+#endif
+__global__ void __launch_bounds__(kJacThreads, SW2_JAC_MIN_BLOCKS) k_jac_elem_wet(DevMesh m, State s, PhysParams P,
+                                                               double* __restrict__ jslots,
+                                                               const unsigned char* __restrict__ ewet) {
+    jac_elem_body<false>(m, s, P, jslots, ewet, nullptr, m.T);
+}
+__global__ void __launch_bounds__(kJacThreads) k_jac_elem_general(DevMesh m, State s, PhysParams P,
+                                                                   double* __restrict__ jslots,
+                                                                   const int* __restrict__ list, int count) {
+    jac_elem_body<true>(m, s, P, jslots, nullptr, list, count);
 }
 
 // FD Jacobian of the boundary edges: one thread per (edge, node, variable); writes the

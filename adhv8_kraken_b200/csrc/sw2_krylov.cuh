@@ -20,12 +20,16 @@ namespace sw2 {
 
 constexpr int kKrylovThreads = 256;
 constexpr long long kBarrierSpinLimit = 1ll << 26;   // bounded wait (~seconds), then error
+constexpr long long kMbarSpinLimit = 1ll << 20;      // polls of one tile copy's mbarrier, then error
 constexpr int kStall = 40;                           // iterations without a new best residual
+constexpr int kRowLanes = 8;                         // lanes per node row in the SpMV sweeps
+constexpr int kTileRows = kKrylovThreads / kRowLanes;   // node rows per CTA tile (32)
+constexpr int kStages = 3;                           // shared-memory tile ring of the staged sweeps
 
 struct KrylovCtl {
     unsigned count;       // barrier arrival counter
     unsigned gen;         // barrier generation
-    int err;              // 1 = a barrier wait ran out
+    int err;              // 1 = a barrier or tile-copy wait ran out
     int iterations;
     int converged;        // 1 = stopping test met, 0 = hit max_lin_it
     int pad;
@@ -61,11 +65,23 @@ __device__ __forceinline__ bool grid_sync(KrylovCtl* ctl) {
     return *(volatile int*)&ctl->err == 0;
 }
 
-// deterministic all-reduce of up to 4 per-block partials: every block sums the partials
-// of all blocks in block order (sum or max per slot)
+constexpr int kKrylovWarps = kKrylovThreads / 32;
+
+// fixed-order warp tree (xor shuffles): every lane ends with the same value
+__device__ __forceinline__ double warp_combine(double a, bool is_max) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, a, o);
+        a = is_max ? fmax(a, t) : a + t;
+    }
+    return a;
+}
+
+// deterministic all-reduce of up to 4 per-block partials: every block combines the partials
+// of all blocks in the same fixed order (sum or max per slot); red = shared [4][kKrylovWarps]
 template <int NV>
-__device__ __forceinline__ void grid_allreduce(const double* part, const int* is_max, double* out) {
-    __shared__ double red[NV][kKrylovThreads];
+__device__ __forceinline__ void grid_allreduce(const double* part, const int* is_max, double* out, double* red) {
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 #pragma unroll
     for (int q = 0; q < NV; q++) {
         double a = 0.0;
@@ -73,42 +89,39 @@ __device__ __forceinline__ void grid_allreduce(const double* part, const int* is
             const double p = __ldcg(part + (size_t)k * 4 + q);
             a = is_max[q] ? fmax(a, p) : a + p;
         }
-        red[q][threadIdx.x] = a;
+        a = warp_combine(a, is_max[q]);
+        if (lane == 0) red[q * kKrylovWarps + warp] = a;
     }
     __syncthreads();
-    for (int w = kKrylovThreads / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
 #pragma unroll
-            for (int q = 0; q < NV; q++)
-                red[q][threadIdx.x] = is_max[q] ? fmax(red[q][threadIdx.x], red[q][threadIdx.x + w])
-                                                : red[q][threadIdx.x] + red[q][threadIdx.x + w];
-        }
-        __syncthreads();
+    for (int q = 0; q < NV; q++) {
+        double a = red[q * kKrylovWarps];
+#pragma unroll
+        for (int w = 1; w < kKrylovWarps; w++) a = is_max[q] ? fmax(a, red[q * kKrylovWarps + w]) : a + red[q * kKrylovWarps + w];
+        out[q] = a;
     }
-#pragma unroll
-    for (int q = 0; q < NV; q++) out[q] = red[q][0];
     __syncthreads();
 }
 
-// block partials: thread values reduced in a fixed tree, written by thread 0
+// block partials: thread values combined in a fixed order, written by thread 0
 template <int NV>
-__device__ __forceinline__ void block_partial(double* vals, const int* is_max, double* part) {
-    __shared__ double red[NV][kKrylovThreads];
+__device__ __forceinline__ void block_partial(double* vals, const int* is_max, double* part, double* red) {
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 #pragma unroll
-    for (int q = 0; q < NV; q++) red[q][threadIdx.x] = vals[q];
-    __syncthreads();
-    for (int w = kKrylovThreads / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-#pragma unroll
-            for (int q = 0; q < NV; q++)
-                red[q][threadIdx.x] = is_max[q] ? fmax(red[q][threadIdx.x], red[q][threadIdx.x + w])
-                                                : red[q][threadIdx.x] + red[q][threadIdx.x + w];
-        }
-        __syncthreads();
+    for (int q = 0; q < NV; q++) {
+        const double a = warp_combine(vals[q], is_max[q]);
+        if (lane == 0) red[q * kKrylovWarps + warp] = a;
     }
+    __syncthreads();
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int q = 0; q < NV; q++) part[(size_t)blockIdx.x * 4 + q] = red[q][0];
+        for (int q = 0; q < NV; q++) {
+            double a = red[q * kKrylovWarps];
+#pragma unroll
+            for (int w = 1; w < kKrylovWarps; w++)
+                a = is_max[q] ? fmax(a, red[q * kKrylovWarps + w]) : a + red[q * kKrylovWarps + w];
+            part[(size_t)blockIdx.x * 4 + q] = a;
+        }
     }
     __syncthreads();
 }
@@ -128,31 +141,129 @@ struct KrylovArgs {
     int apply_inc;            // 1: Newton increment of the state; 0: plain solve
     double* part;             // [2][grid][4] partials (ping-pong: a slot is rewritten only two reductions later)
     KrylovCtl* ctl;
+    // staged sweeps: byte offsets inside one stage of the tile's column indices, row pointers,
+    // block-Jacobi inverses and epilogue vectors (the blocks start at 0); stage stride
+    unsigned c_off, r_off, d_off, v_off, stage_bytes;
 };
 
-// y = Dinv_i * sum_j A'_ij x_j for node row i, with x_j = xa_j - alpha * xb_j when xb != null.
-// Eight lanes share a row: lane l takes the row's values l, l+8, ... (the row's blocks are
-// contiguous, so every load instruction of the 8 lanes reads 64 consecutive bytes), and the
-// three row sums are combined with xor shuffles in a fixed order.  Products and sums are
-// formed in the matrix type MT (FP32 accumulation on the mixed path).  The result is valid
-// on lane 0 of the group; `active` false contributes zeros so the whole warp can shuffle.
-constexpr int kRowLanes = 8;
+// bytes of one epilogue vector's slice for a full tile (3 components per row)
+template <typename VT>
+__host__ __device__ constexpr unsigned tile_vec_bytes() { return kTileRows * 3 * sizeof(VT); }
+
+// ---- tile staging: one bulk copy per tile, completion on an mbarrier -------------------------
+// Tile m = node rows [m kTileRows, (m+1) kTileRows); its blocks and column indices are contiguous.
+// The copied ranges are rounded out to 16 bytes (the bulk-copy rule); the arrays are allocated
+// with 16 spare bytes and start on 256-byte boundaries, so the rounded ranges stay inside them.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// the same with an L2 eviction policy (evict_first for data streamed once per sweep)
+__device__ __forceinline__ void bulk_load_hint(void* dst, const void* src, unsigned bytes, unsigned long long* bar,
+                                               unsigned long long policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+        : "memory");
+}
+__device__ __forceinline__ unsigned long long policy_evict_first() {
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// orders this thread's view of global data written through the generic proxy (other CTAs'
+// stores before the last grid barrier) before its following bulk copies (async proxy)
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+// bounded wait for the completion of the phase with the given parity
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    const unsigned a = smem_addr(bar);
+    for (long long k = 0; k < kMbarSpinLimit; k++) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ unsigned long long lo16(const void* p) { return (unsigned long long)p & ~15ull; }
+__device__ __forceinline__ unsigned long long hi16(const void* p) { return ((unsigned long long)p + 15ull) & ~15ull; }
+
+// One bulk copy group per tile m: its blocks and column indices (16-byte-rounded ranges),
+// its kTileRows + 1 row pointers, block-Jacobi inverses and the slices of up to three
+// epilogue vectors (these start on 16-byte boundaries: tile offsets are multiples of 128,
+// 1152 and 768 bytes).  All completions land on one mbarrier.
 template <typename MT, typename VT>
-__device__ __forceinline__ void row_apply8(int i, bool active, int lane8, const int* rowptr, const int* col,
-                                           const MT* A, const MT* Dinv, const VT* xa, const VT* xb, VT alpha,
-                                           VT y[3]) {
+__device__ __forceinline__ void issue_tile(int m, int V, const int* rowptr, const int* col, const MT* A,
+                                           const MT* Dinv, int nvec, const VT* const* vecs, unsigned char* stage,
+                                           const KrylovArgs& K, unsigned long long* bar, unsigned long long pol) {
+    const int r0 = m * kTileRows, nr = min(kTileRows, V - r0);
+    const int k0 = __ldg(rowptr + r0), k1 = __ldg(rowptr + r0 + nr);
+    const unsigned long long alo = lo16(A + (size_t)k0 * 9), ahi = hi16(A + (size_t)k1 * 9);
+    const unsigned long long clo = lo16(col + k0), chi = hi16(col + k1);
+    const unsigned ab = (unsigned)(ahi - alo), cb = (unsigned)(chi - clo);
+    const unsigned rb = ((unsigned)(nr + 1) * 4u + 15u) & ~15u;
+    const unsigned db = ((unsigned)nr * 9u * (unsigned)sizeof(MT) + 15u) & ~15u;
+    const unsigned vb = ((unsigned)nr * 3u * (unsigned)sizeof(VT) + 15u) & ~15u;
+    mbar_arrive_expect_tx(bar, ab + cb + rb + db + (unsigned)nvec * vb);
+    bulk_load_hint(stage, (const void*)alo, ab, bar, pol);
+    bulk_load_hint(stage + K.c_off, (const void*)clo, cb, bar, pol);
+    bulk_load_hint(stage + K.r_off, rowptr + r0, rb, bar, pol);
+    bulk_load_hint(stage + K.d_off, Dinv + (size_t)r0 * 9, db, bar, pol);
+    for (int v = 0; v < nvec; v++)
+        bulk_load(stage + K.v_off + v * tile_vec_bytes<VT>(), vecs[v] + (size_t)r0 * 3, vb, bar);
+}
+
+template <int N>
+struct IntC {
+    static constexpr int value = N;
+};
+
+// y = Dinv_i * sum_j A'_ij x_j for node row i (blocks kb..ke-1), with x_j = xa_j - alpha * xb_j
+// when xb != null.  Eight lanes share a row and each lane takes whole 3x3 blocks (lane l: the
+// row's blocks l, l+8, ...); the column index and the three x components are loaded once per
+// block.  blk(k) / cix(k) / dinv(q) give block k's values, its column index and entry q of the
+// row's block-Jacobi inverse (from the staged tile in shared memory, or from global memory).
+// The three row sums are combined with xor shuffles in a fixed order, so staged and direct
+// sweeps give bitwise identical results.  Products and sums are formed in the matrix type MT
+// (FP32 accumulation on the mixed path).  The result is valid on lane 0 of the group;
+// `active` false contributes zeros so the whole warp can shuffle.
+template <typename MT, typename VT, class BLK, class CIX, class DIN>
+__device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke, BLK blk, CIX cix, DIN dinv,
+                                          const VT* xa, const VT* xb, VT alpha, VT y[3]) {
     MT a0 = 0, a1 = 0, a2 = 0;
     if (active) {
-        const int v1 = __ldg(rowptr + i + 1) * 9;
-        for (int v = __ldg(rowptr + i) * 9 + lane8; v < v1; v += kRowLanes) {
-            const int kb = v / 9, q = v - 9 * kb, r = q / 3, c = q - 3 * r;
-            const int j = __ldg(col + kb);
-            VT x = ldv(xa + 3 * j + c);
-            if (xb) x -= alpha * ldv(xb + 3 * j + c);
-            const MT prod = __ldg(A + v) * (MT)x;
-            a0 += (r == 0) ? prod : (MT)0;
-            a1 += (r == 1) ? prod : (MT)0;
-            a2 += (r == 2) ? prod : (MT)0;
+        for (int k = kb + lane8; k < ke; k += kRowLanes) {
+            const MT* bk = blk(k);
+            MT m[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++) m[q] = bk[q];
+            const int j = cix(k);
+            VT x0 = ldv(xa + 3 * j), x1 = ldv(xa + 3 * j + 1), x2 = ldv(xa + 3 * j + 2);
+            if (xb) {
+                x0 -= alpha * ldv(xb + 3 * j);
+                x1 -= alpha * ldv(xb + 3 * j + 1);
+                x2 -= alpha * ldv(xb + 3 * j + 2);
+            }
+            const MT c0 = (MT)x0, c1 = (MT)x1, c2 = (MT)x2;
+            a0 += m[0] * c0 + m[1] * c1 + m[2] * c2;
+            a1 += m[3] * c0 + m[4] * c1 + m[5] * c2;
+            a2 += m[6] * c0 + m[7] * c1 + m[8] * c2;
         }
     }
 #pragma unroll
@@ -162,10 +273,9 @@ __device__ __forceinline__ void row_apply8(int i, bool active, int lane8, const 
         a2 += __shfl_xor_sync(0xffffffffu, a2, o, kRowLanes);
     }
     if (active && lane8 == 0) {
-        const MT* d = Dinv + (size_t)i * 9;
-        y[0] = (VT)(__ldg(d + 0) * a0 + __ldg(d + 1) * a1 + __ldg(d + 2) * a2);
-        y[1] = (VT)(__ldg(d + 3) * a0 + __ldg(d + 4) * a1 + __ldg(d + 5) * a2);
-        y[2] = (VT)(__ldg(d + 6) * a0 + __ldg(d + 7) * a1 + __ldg(d + 8) * a2);
+        y[0] = (VT)(dinv(0) * a0 + dinv(1) * a1 + dinv(2) * a2);
+        y[1] = (VT)(dinv(3) * a0 + dinv(4) * a1 + dinv(5) * a2);
+        y[2] = (VT)(dinv(6) * a0 + dinv(7) * a1 + dinv(8) * a2);
     } else {
         y[0] = y[1] = y[2] = (VT)0;
     }
@@ -173,26 +283,119 @@ __device__ __forceinline__ void row_apply8(int i, bool active, int lane8, const 
 
 // MT: matrix / preconditioner storage and SpMV accumulation type; VT: Krylov vector type
 // (FP64 on both paths: FP32 vectors let the recursively updated residual drift away from
-// the true one and the iteration stagnates).
-template <typename MT, typename VT>
-__global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const MT* __restrict__ A,
+// the true one and the iteration stagnates).  STAGED: the SpMV sweeps read each tile's
+// blocks, column indices, row pointers, block-Jacobi inverses and epilogue vectors from a
+// kStages-deep shared-memory ring filled by bulk copies (one thread issues, completion on an
+// mbarrier) kStages - 1 tiles ahead of the rows being computed, so a row's only global loads
+// are its x gathers; the streamed matrix data carry an L2 evict-first hint, which keeps the
+// Krylov vectors in L2.  The dynamic shared memory is kStages * K.stage_bytes.  Otherwise the
+// lanes load everything from global memory.
+template <typename MT, typename VT, bool STAGED>
+__global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, const MT* __restrict__ A,
                                                             const MT* __restrict__ Dinv, VT* __restrict__ b,
                                                             VT* __restrict__ uu, VT* __restrict__ r,
                                                             VT* __restrict__ q, VT* __restrict__ p, VT* __restrict__ Ap,
                                                             VT* __restrict__ As, VT* __restrict__ ubest) {
+    __shared__ double red[4 * kKrylovWarps];
+    __shared__ unsigned long long bar[kStages];
+    extern __shared__ __align__(128) unsigned char stage_mem[];
     const int V = K.V;
     const int stride = gridDim.x * blockDim.x;
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
-    // SpMV phases: groups of kRowLanes lanes per row; a warp covers 32 / kRowLanes rows
     const int lane8 = threadIdx.x % kRowLanes;
-    const int warp_g = t0 / 32;
-    const int grp_off = (threadIdx.x % 32) / kRowLanes;
-    const int g0 = warp_g * (32 / kRowLanes);
-    const int gstride = (stride / 32) * (32 / kRowLanes);
+    const int li = threadIdx.x / kRowLanes;   // row of the tile this lane group works on
+    const int ntiles = (V + kTileRows - 1) / kTileRows;
     const int SUM = 0, MAX = 1;
     KrylovCtl* ctl = K.ctl;
-    int nred = 0;   // reductions so far; selects the partial buffer
+    int nred = 0;      // reductions so far; selects the partial buffer
+    unsigned tc = 0;   // tiles consumed by this CTA: stage tc % kStages, mbarrier parity (tc / kStages) & 1
+    bool wait_failed = false;
+    unsigned long long pol = 0;
     auto pbuf = [&]() { return K.part + (size_t)(nred & 1) * gridDim.x * 4; };
+    auto stage = [&](unsigned c) { return stage_mem + (c % kStages) * K.stage_bytes; };
+
+    if (STAGED) {
+        if (threadIdx.x == 0) {
+            for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
+            mbar_init_fence();
+            pol = policy_evict_first();
+        }
+        __syncthreads();
+    }
+
+    // One SpMV sweep over this CTA's tiles (m = blockIdx.x, blockIdx.x + gridDim.x, ...):
+    // y = M^-1 A' (xa - alpha xb) per row; lane 0 of each row group calls epi(i, y, ev) with
+    // ev[v][c] = component c of epilogue vector v at row i (NV vectors: v0, v1, v2).
+    auto sweep = [&](auto nvc, const VT* xa, const VT* xb, VT alpha, const VT* v0, const VT* v1, const VT* v2,
+                     auto&& epi) {
+        constexpr int NV = decltype(nvc)::value;
+        const VT* vecs[3] = {v0, v1, v2};
+        if (STAGED && threadIdx.x == 0) {
+            fence_proxy_async_global();
+            for (int d = 0; d < kStages - 1; d++) {
+                const int m = blockIdx.x + d * gridDim.x;
+                if (m < ntiles)
+                    issue_tile<MT, VT>(m, V, K.rowptr, K.col, A, Dinv, NV, vecs, stage(tc + d), K,
+                                       &bar[(tc + d) % kStages], pol);
+            }
+        }
+        for (int m = blockIdx.x; m < ntiles; m += gridDim.x) {
+            const int i = m * kTileRows + li;
+            const bool act = i < V;
+            VT y[3];
+            VT ev[NV > 0 ? NV : 1][3];
+            if (STAGED) {
+                if (threadIdx.x == 0) {
+                    // into the stage of tile tc - 1, released by the __syncthreads that ended it
+                    const int mn = m + (kStages - 1) * gridDim.x;
+                    if (mn < ntiles)
+                        issue_tile<MT, VT>(mn, V, K.rowptr, K.col, A, Dinv, NV, vecs, stage(tc + kStages - 1), K,
+                                           &bar[(tc + kStages - 1) % kStages], pol);
+                }
+                // a wait that runs out flags the error once; this thread then stops waiting, the
+                // sweep finishes on stale data and the next grid barrier returns
+                if (!wait_failed && !mbar_wait(&bar[tc % kStages], (tc / kStages) & 1u)) {
+                    wait_failed = true;
+                    atomicExch(&ctl->err, 1);
+                }
+                const unsigned char* st = stage(tc);
+                const int* sR = (const int*)(st + K.r_off);
+                const int k0 = sR[0];
+                const MT* sA = (const MT*)(st + ((unsigned long long)(A + (size_t)k0 * 9) & 15ull));
+                const int* sC = (const int*)(st + K.c_off + ((unsigned long long)(K.col + k0) & 15ull));
+                const MT* sD = (const MT*)(st + K.d_off) + li * 9;
+                const VT* sV = (const VT*)(st + K.v_off);
+                const int kb = act ? sR[li] : 0, ke = act ? sR[li + 1] : 0;
+                row_apply<MT, VT>(
+                    act, lane8, kb, ke, [&](int k) { return sA + (size_t)(k - k0) * 9; },
+                    [&](int k) { return sC[k - k0]; }, [&](int qq) { return sD[qq]; }, xa, xb, alpha, y);
+                if (act && lane8 == 0) {
+#pragma unroll
+                    for (int v = 0; v < NV; v++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) ev[v][c] = sV[v * (tile_vec_bytes<VT>() / sizeof(VT)) + 3 * li + c];
+                }
+            } else {
+                if (act && lane8 == 0) {   // issued ahead of the row's gathers
+#pragma unroll
+                    for (int v = 0; v < NV; v++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) ev[v][c] = ldv(vecs[v] + 3 * i + c);
+                }
+                const int kb = act ? __ldg(K.rowptr + i) : 0, ke = act ? __ldg(K.rowptr + i + 1) : 0;
+                const MT* gD = Dinv + (size_t)i * 9;
+                row_apply<MT, VT>(
+                    act, lane8, kb, ke, [&](int k) { return A + (size_t)k * 9; },
+                    [&](int k) { return __ldg(K.col + k); }, [&](int qq) { return __ldg(gD + qq); }, xa, xb, alpha,
+                    y);
+            }
+            if (act && lane8 == 0) epi(i, y, ev);
+            if (STAGED) {
+                __syncthreads();
+                tc++;
+            }
+        }
+    };
 
     // b <- M^-1 b'
     for (int i = t0; i < V; i += stride) {
@@ -210,65 +413,54 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
     {
         double vals[4] = {0, 0, 0, 0};
         const int ism[4] = {MAX, MAX, SUM, SUM};
-        for (int base = g0; base < V; base += gstride) {
-            const int i = base + grp_off;
-            const bool act = i < V;
-            VT y[3];
-            row_apply8<MT, VT>(i, act, lane8, K.rowptr, K.col, A, Dinv, uu, (const VT*)nullptr, (VT)0, y);
-            if (act && lane8 == 0) {
+        sweep(IntC<1>{}, uu, (const VT*)nullptr, (VT)0, b, nullptr, nullptr, [&](int i, const VT* y, const VT (*ev)[3]) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const VT bb = ldv(b + 3 * i + c);
-                    const VT rr = bb - y[c];
-                    r[3 * i + c] = rr;
-                    q[3 * i + c] = rr;
-                    p[3 * i + c] = rr;
-                    Ap[3 * i + c] = 0;
-                    vals[0] = fmax(vals[0], fabs((double)rr));
-                    vals[1] = fmax(vals[1], fabs((double)bb));
-                    vals[2] += (double)rr * (double)rr;
-                }
+            for (int c = 0; c < 3; c++) {
+                const VT bb = ev[0][c];
+                const VT rr = bb - y[c];
+                r[3 * i + c] = rr;
+                q[3 * i + c] = rr;
+                p[3 * i + c] = rr;
+                Ap[3 * i + c] = 0;
+                vals[0] = fmax(vals[0], fabs((double)rr));
+                vals[1] = fmax(vals[1], fabs((double)bb));
+                vals[2] += (double)rr * (double)rr;
             }
-        }
-        block_partial<4>(vals, ism, pbuf());
+        });
+        block_partial<4>(vals, ism, pbuf(), red);
         if (!grid_sync(ctl)) return;
-        double red[4];
-        grid_allreduce<4>(pbuf(), ism, red);
+        double rd[4];
+        grid_allreduce<4>(pbuf(), ism, rd, red);
         nred++;
-        double rnorm = red[0];
-        const double bnorm = red[1];
-        double rho = red[2], rhop = 1.0, alpha = 1.0, omega = 1.0;
+        double rnorm = rd[0];
+        const double bnorm = rd[1];
+        double rho = rd[2], rhop = 1.0, alpha = 1.0, omega = 1.0;
         int it = 0;
         const double tol = K.atol + bnorm * K.rtol;
         // best iterate so far: past its attainable accuracy BiCGSTAB's residual drifts back up,
-        // so on stagnation (no new best for kStall iterations) or at max_lin_it the best one is used
+        // so on stagnation (no new best for kStall iterations) or at max_lin_it the best one is
+        // used.  It is saved lazily: when an iteration sets a new best (`pending`), the next
+        // update pass, which reads u anyway, writes that u to ubest before overwriting it.
         double best = rnorm;
         int best_it = 0;
-        for (int i = t0; i < V; i += stride)
-#pragma unroll
-            for (int c = 0; c < 3; c++) ubest[3 * i + c] = uu[3 * i + c];
+        bool pending = true;
         while (rnorm > tol && it < K.maxit && it - best_it < kStall) {
             it++;
             // (d)-(e): Ap = M^-1 A p, gamma = q . Ap
             {
                 double g[4] = {0, 0, 0, 0};
                 const int gm[4] = {SUM, SUM, SUM, SUM};
-                for (int base = g0; base < V; base += gstride) {
-                    const int i = base + grp_off;
-                    const bool act = i < V;
-                    VT y[3];
-                    row_apply8<MT, VT>(i, act, lane8, K.rowptr, K.col, A, Dinv, p, (const VT*)nullptr, (VT)0, y);
-                    if (act && lane8 == 0) {
+                sweep(IntC<1>{}, p, (const VT*)nullptr, (VT)0, q, nullptr, nullptr,
+                      [&](int i, const VT* y, const VT (*ev)[3]) {
 #pragma unroll
-                        for (int c = 0; c < 3; c++) {
-                            Ap[3 * i + c] = y[c];
-                            g[0] += (double)ldv(q + 3 * i + c) * (double)y[c];
-                        }
-                    }
-                }
-                block_partial<1>(g, gm, pbuf());
+                          for (int c = 0; c < 3; c++) {
+                              Ap[3 * i + c] = y[c];
+                              g[0] += (double)ev[0][c] * (double)y[c];
+                          }
+                      });
+                block_partial<1>(g, gm, pbuf(), red);
                 if (!grid_sync(ctl)) return;
-                grid_allreduce<1>(pbuf(), gm, g);
+                grid_allreduce<1>(pbuf(), gm, g, red);
                 nred++;
                 alpha = rho / g[0];
             }
@@ -277,25 +469,19 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
                 double w[4] = {0, 0, 0, 0};
                 const int wm[4] = {SUM, SUM, SUM, SUM};
                 const VT al = (VT)alpha;
-                for (int base = g0; base < V; base += gstride) {
-                    const int i = base + grp_off;
-                    const bool act = i < V;
-                    VT y[3];
-                    row_apply8<MT, VT>(i, act, lane8, K.rowptr, K.col, A, Dinv, r, Ap, al, y);
-                    if (act && lane8 == 0) {
+                sweep(IntC<3>{}, r, Ap, al, r, Ap, q, [&](int i, const VT* y, const VT (*ev)[3]) {
 #pragma unroll
-                        for (int c = 0; c < 3; c++) {
-                            const VT s = ldv(r + 3 * i + c) - al * ldv(Ap + 3 * i + c);
-                            As[3 * i + c] = y[c];
-                            w[0] += (double)y[c] * (double)s;
-                            w[1] += (double)y[c] * (double)y[c];
-                            w[2] += (double)y[c] * (double)ldv(q + 3 * i + c);
-                        }
+                    for (int c = 0; c < 3; c++) {
+                        const VT s = ev[0][c] - al * ev[1][c];
+                        As[3 * i + c] = y[c];
+                        w[0] += (double)y[c] * (double)s;
+                        w[1] += (double)y[c] * (double)y[c];
+                        w[2] += (double)y[c] * (double)ev[2][c];
                     }
-                }
-                block_partial<3>(w, wm, pbuf());
+                });
+                block_partial<3>(w, wm, pbuf(), red);
                 if (!grid_sync(ctl)) return;
-                grid_allreduce<3>(pbuf(), wm, w);
+                grid_allreduce<3>(pbuf(), wm, w, red);
                 nred++;
                 omega = w[0] / w[1];
                 rhop = rho;
@@ -314,6 +500,7 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
                         const int k = 3 * i + c;
                         const VT s = ldv(r + k) - al * ldv(Ap + k);
                         VT uk = ldv(uu + k);
+                        if (pending) ubest[k] = uk;
                         uk += al * ldv(p + k);
                         uk += om * s;
                         uu[k] = uk;
@@ -323,23 +510,22 @@ __global__ void __launch_bounds__(kKrylovThreads) k_bicgstab(KrylovArgs K, const
                         mx[0] = fmax(mx[0], fabs((double)rk));
                     }
                 }
-                block_partial<1>(mx, mm, pbuf());
+                block_partial<1>(mx, mm, pbuf(), red);
                 if (!grid_sync(ctl)) return;
-                grid_allreduce<1>(pbuf(), mm, mx);
+                grid_allreduce<1>(pbuf(), mm, mx, red);
                 nred++;
                 rnorm = mx[0];
-                if (rnorm < best) {   // identical decision in every block; own rows only
+                pending = rnorm < best;   // identical decision in every block
+                if (pending) {
                     best = rnorm;
                     best_it = it;
-                    for (int i = t0; i < V; i += stride)
-#pragma unroll
-                        for (int c = 0; c < 3; c++) ubest[3 * i + c] = uu[3 * i + c];
                 }
             }
         }
         const bool conv = rnorm <= tol;
-        // x = S u; state += x; sol = -x
-        const VT* ux = conv ? uu : ubest;
+        // x = S u; state += x; sol = -x.  Without convergence the best iterate is u itself when
+        // the last iteration set it (not saved yet), else ubest.
+        const VT* ux = (conv || pending) ? uu : ubest;
         for (int i = t0; i < V; i += stride) {
             const double x0 = (double)ldv(ux + 3 * i) * K.S[3 * i];
             const double x1 = (double)ldv(ux + 3 * i + 1) * K.S[3 * i + 1];

@@ -56,7 +56,8 @@ struct DBuf {
     int alloc(size_t count) {
         n = count;
         if (count == 0) count = 1;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        // 16 spare bytes: bulk copies of a 16-byte-rounded range may reach past the last element
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 16);
         return e == cudaSuccess ? 0 : -1;
     }
     ~DBuf() { if (p) cudaFree(p); }
@@ -91,6 +92,9 @@ struct sw2gpu_ctx {
     DBuf<double> hs[3], us[3], vs[3];
     int lv[3] = {0, 1, 2};
     DBuf<int> wd;
+    DBuf<unsigned char> ewet;    // element takes the fully wet Jacobian path
+    DBuf<int> glist, gcount;     // elements on the general (wet/dry) Jacobian path
+    int ngeneral = 0;
     // work
     DBuf<double> sc, sx, sy, R, sol, jslots, val, S_, bs;
     DBuf<float> val32, dinv32;
@@ -104,6 +108,9 @@ struct sw2gpu_ctx {
     Norms* norms_h = nullptr;
     KrylovCtl* ctl_h = nullptr;
     int krylov_grid = 0;
+    bool staged = false;            // Krylov sweeps read matrix tiles through the shared-memory ring
+    unsigned c_off = 0, r_off = 0, d_off = 0, v_off = 0, stage_bytes = 0;
+    size_t krylov_smem = 0;         // dynamic shared memory of the Krylov launch
     int launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // per-phase device timing: event pairs recorded around the main kernels of a step
@@ -220,9 +227,11 @@ int launch_resid(sw2gpu_ctx* c) {
     PhysParams P = c->phys();
     const int n = c->T + c->E;
     Phase ph(c, kPhResid);
-    k_resid_elem<<<nblk(std::max(n, 1), 128), 128, 0, c->stream>>>(c->dm, s, P, c->sc.p, c->sx.p, c->sy.p);
+    CK(cudaMemsetAsync(c->gcount.p, 0, sizeof(int), c->stream));
+    k_resid_elem<<<nblk(std::max(n, 1), 128), 128, 0, c->stream>>>(c->dm, s, P, c->sc.p, c->sx.p, c->sy.p,
+                                                                   c->ewet.p, c->glist.p, c->gcount.p);
     k_resid_gather<<<nblk(std::max(c->V, 1), kGatherThreads), kGatherThreads, 0, c->stream>>>(
-        c->dm, s, c->sc.p, c->sx.p, c->sy.p, c->R.p, c->sol.p, c->npart.p, c->ncounter.p, c->norms.p);
+        c->dm, s, c->sc.p, c->sx.p, c->sy.p, c->R.p, c->sol.p, c->npart.p, c->ncounter.p, c->norms.p, c->gcount.p);
     c->launches += 2;
     CK(cudaGetLastError());
     return 0;
@@ -232,6 +241,7 @@ int read_norms(sw2gpu_ctx* c, Norms& out) {
     CK(cudaMemcpyAsync(c->norms_h, c->norms.p, sizeof(Norms), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     out = *c->norms_h;
+    c->ngeneral = out.ngeneral;
     return 0;
 }
 
@@ -239,8 +249,14 @@ int launch_jacobian(sw2gpu_ctx* c) {
     State s = c->state();
     PhysParams P = c->phys();
     if (c->T) {
+        // the list and the wet flags come from the residual evaluated at this same state
         Phase ph(c, kPhJac);
-        k_jac_elem<<<nblk(c->T, kJacElems), kJacThreads, 0, c->stream>>>(c->dm, s, P, c->jslots.p);
+        k_jac_elem_wet<<<nblk(c->T, kJacElems), kJacThreads, 0, c->stream>>>(c->dm, s, P, c->jslots.p, c->ewet.p);
+        if (c->ngeneral > 0) {
+            k_jac_elem_general<<<nblk(c->ngeneral, kJacElems), kJacThreads, 0, c->stream>>>(
+                c->dm, s, P, c->jslots.p, c->glist.p, c->ngeneral);
+            c->launches++;
+        }
     }
     if (c->E) k_jac_edge<<<nblk(6LL * c->E, 128), 128, 0, c->stream>>>(c->dm, s, P, c->jslots.p);
     k_jac_gather<<<nblk(9LL * c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->jslots.p, c->val.p);
@@ -269,6 +285,29 @@ int launch_init(sw2gpu_ctx* c) {     // fe_sw2_init: current = old, Dirichlet va
     }
     CK(cudaGetLastError());
     return 0;
+}
+
+// bytes per stage of the staged Krylov sweeps: the largest 16-byte-rounded block range and
+// column-index range of any tile of kTileRows rows, for matrix elements of esz bytes
+void stage_caps(const std::vector<int>& rp, int V, size_t esz, unsigned& a_cap, unsigned& c_cap) {
+    size_t am = 16, cm = 16;
+    for (int r0 = 0; r0 < V; r0 += kTileRows) {
+        const size_t k0 = (size_t)rp[r0], k1 = (size_t)rp[std::min(r0 + kTileRows, V)];
+        am = std::max(am, ((k1 * 9 * esz + 15) & ~size_t(15)) - ((k0 * 9 * esz) & ~size_t(15)));
+        cm = std::max(cm, ((k1 * 4 + 15) & ~size_t(15)) - ((k0 * 4) & ~size_t(15)));
+    }
+    a_cap = (unsigned)am;
+    c_cap = (unsigned)cm;
+}
+
+#ifndef SW2_MAX_STAGED_SMEM
+#define SW2_MAX_STAGED_SMEM (96 * 1024)   // dynamic shared memory allowed for the tile ring
+#endif
+constexpr size_t kMaxStagedSmem = SW2_MAX_STAGED_SMEM;
+
+template <typename MT>
+void* krylov_kernel(bool staged) {
+    return staged ? (void*)k_bicgstab<MT, double, true> : (void*)k_bicgstab<MT, double, false>;
 }
 
 // scaling, preconditioner setup and the persistent BiCGSTAB; returns its iteration count
@@ -300,6 +339,11 @@ int launch_linear(sw2gpu_ctx* c, int apply_inc, double rtol) {
     K.apply_inc = apply_inc;
     K.part = c->part.p;
     K.ctl = c->ctl.p;
+    K.c_off = c->c_off;
+    K.r_off = c->r_off;
+    K.d_off = c->d_off;
+    K.v_off = c->v_off;
+    K.stage_bytes = c->stage_bytes;
     dim3 grid(c->krylov_grid), block(kKrylovThreads);
     Phase ph(c, kPhKrylov);
     if (mixed) {
@@ -308,14 +352,14 @@ int launch_linear(sw2gpu_ctx* c, int apply_inc, double rtol) {
         double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
                *Ap = c->kv64[5].p, *As = c->kv64[6].p, *ub = c->kv64[7].p;
         void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As, &ub};
-        CK(cudaLaunchCooperativeKernel((void*)k_bicgstab<float, double>, grid, block, args, 0, c->stream));
+        CK(cudaLaunchCooperativeKernel(krylov_kernel<float>(c->staged), grid, block, args, c->krylov_smem, c->stream));
     } else {
         const double* A = c->val.p;
         const double* D = c->dinv64.p;
         double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
                *Ap = c->kv64[5].p, *As = c->kv64[6].p, *ub = c->kv64[7].p;
         void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As, &ub};
-        CK(cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double>, grid, block, args, 0, c->stream));
+        CK(cudaLaunchCooperativeKernel(krylov_kernel<double>(c->staged), grid, block, args, c->krylov_smem, c->stream));
     }
     c->launches += 3;
     CK(cudaMemcpyAsync(c->ctl_h, c->ctl.p, sizeof(KrylovCtl), cudaMemcpyDeviceToHost, c->stream));
@@ -532,6 +576,9 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     rc |= zalloc(c->dir_v, c->dir_node.size(), st);
     for (int l = 0; l < 3; l++) { rc |= zalloc(c->hs[l], V, st); rc |= zalloc(c->us[l], V, st); rc |= zalloc(c->vs[l], V, st); }
     rc |= zalloc(c->wd, std::max(T, 1), st);
+    rc |= zalloc(c->ewet, std::max(T, 1), st);
+    rc |= zalloc(c->glist, std::max(T, 1), st);
+    rc |= zalloc(c->gcount, 1, st);
     rc |= zalloc(c->mark, V, st);
     rc |= zalloc(c->sc, nslot, st); rc |= zalloc(c->sx, nslot, st); rc |= zalloc(c->sy, nslot, st);
     rc |= zalloc(c->R, 3ull * V, st); rc |= zalloc(c->sol, 3ull * V, st);
@@ -552,13 +599,34 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     rc |= zalloc(c->npart, gblocks, st);
     rc |= zalloc(c->norms, 1, st);
     if (rc) return rc;
-    // persistent Krylov grid: every block co-resident
+    // persistent Krylov grid: every block co-resident.  The sweeps stage matrix tiles in
+    // shared memory when kStages tiles fit in kMaxStagedSmem (true for triangle meshes,
+    // ~7 blocks per row); a mesh with much denser rows falls back to direct loads.
     int sms = 0, per_sm = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    if (prm->precision == SW2GPU_MIXED)
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<float, double>, kKrylovThreads, 0));
-    else
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double>, kKrylovThreads, 0));
+    {
+        const bool mixed = prm->precision == SW2GPU_MIXED;
+        const unsigned esz = mixed ? sizeof(float) : sizeof(double);
+        unsigned a_cap = 0, c_cap = 0;
+        stage_caps(rp, V, esz, a_cap, c_cap);
+        // stage layout: blocks | column indices | kTileRows + 1 row pointers | inverses | 3 vectors
+        const unsigned c_off = a_cap, r_off = c_off + c_cap;
+        const unsigned d_off = r_off + ((unsigned)(kTileRows + 1) * 4u + 15u) / 16u * 16u;
+        const unsigned v_off = d_off + (unsigned)kTileRows * 9u * esz;
+        const unsigned stage = (v_off + 3u * tile_vec_bytes<double>() + 127u) & ~127u;
+        c->staged = (size_t)kStages * stage <= kMaxStagedSmem;
+        if (c->staged) {
+            c->c_off = c_off;
+            c->r_off = r_off;
+            c->d_off = d_off;
+            c->v_off = v_off;
+            c->stage_bytes = stage;
+        }
+        c->krylov_smem = (size_t)kStages * c->stage_bytes;
+        void* kern = mixed ? krylov_kernel<float>(c->staged) : krylov_kernel<double>(c->staged);
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->krylov_smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kKrylovThreads, c->krylov_smem));
+    }
     per_sm = std::min(per_sm, 4);
     const int need = nblk(V, kKrylovThreads);
     c->krylov_grid = std::max(1, std::min(need, sms * std::max(per_sm, 1)));
@@ -651,6 +719,17 @@ int sw2gpu_load(sw2gpu_ctx* c, int32_t* nnzb, int32_t* row_ptr, int32_t* col, do
     if (!c) return fail(SW2GPU_E_ARG, "null context");
     if (nnzb) *nnzb = c->nnzb;
     if (!val && !resid && !row_ptr && !col) return SW2GPU_OK;
+    // element classification for the two Jacobian kernels (sw2gpu_step takes it from the
+    // residual pass at the same state); R is the last sw2gpu_resid's, as in fe_newton
+    {
+        State s = c->state();
+        CK(cudaMemsetAsync(c->gcount.p, 0, sizeof(int), c->stream));
+        if (c->T) k_classify<<<nblk(c->T, 256), 256, 0, c->stream>>>(c->dm, s, c->ewet.p, c->glist.p, c->gcount.p);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(&c->norms_h->ngeneral, c->gcount.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->ngeneral = c->norms_h->ngeneral;
+    }
     int rc = launch_jacobian(c);
     if (rc) return rc;
     State s = c->state();

@@ -181,7 +181,7 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double>, kKrylovThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double, false>, kKrylovThreads, 0);
     const int grid = std::max(1, std::min({kMaxGrid, (nnodes + kKrylovThreads - 1) / kKrylovThreads,
                                            sms * std::max(per_sm, 1)}));
     KrylovArgs K;
@@ -198,10 +198,11 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     K.apply_inc = 0;
     K.part = part;
     K.ctl = ctl;
+    K.c_off = K.r_off = K.d_off = K.v_off = K.stage_bytes = 0;   // direct sweeps
     const double* Ac = A;
     const double* Dc = dinv;
     void* args[] = {&K, &Ac, &Dc, &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7]};
-    cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double>, dim3(grid), dim3(kKrylovThreads),
+    cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double, false>, dim3(grid), dim3(kKrylovThreads),
                                                 args, 0, st);
     if (e != cudaSuccess) return na_fail(SW2GPU_E_CUDA, cudaGetErrorString(e));
     KrylovCtl h;

@@ -21,7 +21,7 @@ from . import capi
 from .capi import MeshArrays, Stats, c_double_p, c_int32_p, make_params
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsw2gpu.so")
+LIB_PATH = os.environ.get("SW2GPU_LIB") or os.path.join(HERE, "libsw2gpu.so")
 
 _lib = None
 
