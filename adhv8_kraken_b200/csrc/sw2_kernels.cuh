@@ -6,6 +6,7 @@
 // (all 2D elements ascending, then the boundary edges ascending), which is the
 // summation order of fe_sw2_resid / fe_global_matrix_assemble_sw2.
 #pragma once
+#include "sw2_krylov.cuh"   // inv3, fold_block
 #include "sw2_physics.cuh"
 
 namespace sw2 {
@@ -507,49 +508,42 @@ __global__ void k_rowscale(DevMesh m, const State s, double* __restrict__ val, d
     }
 }
 
-// A' = S A S (in place for FP64, converted copy for the mixed path) and the inverse of
-// every scaled 3x3 diagonal block for the block-Jacobi preconditioner.
-template <typename MT>
-__global__ void k_scale_matrix(DevMesh m, double* __restrict__ val, MT* __restrict__ mval, const double* __restrict__ S,
-                               MT* __restrict__ dinv, int* __restrict__ singular) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= m.nnzb) return;
-    const int i = m.blk_row[k], j = m.col[k];
+// Block-Jacobi preconditioner folded into the matrix.  With A' = S A S (spv_jacobi scaling)
+// and D_i the scaled diagonal block of row i, the Krylov operator M^-1 A' has identity
+// diagonal blocks and off-diagonal blocks D_i^-1 A'_ij, so the sweeps stream only those
+// (nnzb - V blocks, no inverses).  k_fold_diag: D_i^-1 per node row (FP64).
+__global__ void k_fold_diag(DevMesh m, const double* __restrict__ val, const double* __restrict__ S,
+                            double* __restrict__ dinv, int* __restrict__ singular) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.V) return;
+    const double* v = val + (size_t)m.dpos[i] * 9;
     double a[9];
 #pragma unroll
     for (int r = 0; r < 3; r++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) a[3 * r + c] = val[(size_t)k * 9 + 3 * r + c] * (S[3 * i + r] * S[3 * j + c]);
-    if (sizeof(MT) == sizeof(double)) {
+        for (int c = 0; c < 3; c++) a[3 * r + c] = v[3 * r + c] * (S[3 * i + r] * S[3 * i + c]);
+    if (!inv3(a, dinv + (size_t)i * 9)) atomicExch(singular, 1);
+}
+
+// off-diagonal block k of row i -> position k - i - (k > dpos_i) of the folded matrix,
+// D_i^-1 (S_i A_ij S_j) formed in FP64 and stored as MT
+template <typename MT>
+__global__ void k_fold_offdiag(DevMesh m, const double* __restrict__ val, const double* __restrict__ S,
+                               const double* __restrict__ dinv, MT* __restrict__ aoff) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m.nnzb) return;
+    const int i = m.blk_row[k], j = m.col[k];
+    const int dp = m.dpos[i];
+    if (k == dp) return;
+    double bq[9], d[9];
 #pragma unroll
-        for (int q = 0; q < 9; q++) val[(size_t)k * 9 + q] = a[q];
-    } else {
+    for (int r = 0; r < 3; r++)
 #pragma unroll
-        for (int q = 0; q < 9; q++) mval[(size_t)k * 9 + q] = (MT)a[q];
-    }
-    if (i == j) {
-        const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
-        const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
-        if (det == 0.0 || !isfinite(det)) {
-            atomicExch(singular, 1);
+        for (int c = 0; c < 3; c++) bq[3 * r + c] = val[(size_t)k * 9 + 3 * r + c] * (S[3 * i + r] * S[3 * j + c]);
 #pragma unroll
-            for (int q = 0; q < 9; q++) dinv[(size_t)i * 9 + q] = (MT)((q % 4 == 0) ? 1.0 : 0.0);
-            return;
-        }
-        const double id = 1.0 / det;
-        double inv[9];
-        inv[0] = c00 * id;
-        inv[1] = (a[2] * a[7] - a[1] * a[8]) * id;
-        inv[2] = (a[1] * a[5] - a[2] * a[4]) * id;
-        inv[3] = c01 * id;
-        inv[4] = (a[0] * a[8] - a[2] * a[6]) * id;
-        inv[5] = (a[2] * a[3] - a[0] * a[5]) * id;
-        inv[6] = c02 * id;
-        inv[7] = (a[1] * a[6] - a[0] * a[7]) * id;
-        inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
-#pragma unroll
-        for (int q = 0; q < 9; q++) dinv[(size_t)i * 9 + q] = (MT)inv[q];
-    }
+    for (int q = 0; q < 9; q++) d[q] = dinv[(size_t)i * 9 + q];
+    MT* o = aoff + (size_t)(k - i - (k > dp ? 1 : 0)) * 9;
+    fold_block(d, bq, o);
 }
 
 // line search halving (fe_newton.c:692-747): sol *= 0.5; state += sol (fe_sw2_inc)

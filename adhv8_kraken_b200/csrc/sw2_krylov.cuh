@@ -129,9 +129,42 @@ __device__ __forceinline__ void block_partial(double* vals, const int* is_max, d
 template <typename T>
 __device__ __forceinline__ T ldv(const T* p) { return __ldcg(p); }
 
+// inverse of a 3x3 block (cofactors over the determinant); false (and the identity) when
+// the block is singular or not finite
+__device__ __forceinline__ bool inv3(const double* a, double* out) {
+    const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    if (det == 0.0 || !isfinite(det)) {
+#pragma unroll
+        for (int q = 0; q < 9; q++) out[q] = (q % 4 == 0) ? 1.0 : 0.0;
+        return false;
+    }
+    const double id = 1.0 / det;
+    out[0] = c00 * id;
+    out[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    out[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    out[3] = c01 * id;
+    out[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    out[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    out[6] = c02 * id;
+    out[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    out[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    return true;
+}
+
+// o = d * b for 3x3 blocks (row-major), formed in FP64 and stored as MT
+template <typename MT>
+__device__ __forceinline__ void fold_block(const double* d, const double* b, MT* o) {
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            o[3 * r + c] = (MT)(d[3 * r] * b[c] + d[3 * r + 1] * b[3 + c] + d[3 * r + 2] * b[6 + c]);
+}
+
 struct KrylovArgs {
     int V;
-    const int *rowptr, *col;
+    const int *rowptr, *col;  // off-diagonal block structure of the folded operator M^-1 A'
     const double* S;          // scale vector [3V]
     const double* bs;         // scaled rhs S R [3V]
     double rtol, atol;
@@ -141,9 +174,9 @@ struct KrylovArgs {
     int apply_inc;            // 1: Newton increment of the state; 0: plain solve
     double* part;             // [2][grid][4] partials (ping-pong: a slot is rewritten only two reductions later)
     KrylovCtl* ctl;
-    // staged sweeps: byte offsets inside one stage of the tile's column indices, row pointers,
-    // block-Jacobi inverses and epilogue vectors (the blocks start at 0); stage stride
-    unsigned c_off, r_off, d_off, v_off, stage_bytes;
+    // staged sweeps: byte offsets inside one stage of the tile's column indices, row pointers
+    // and epilogue vectors (the blocks start at 0); stage stride
+    unsigned c_off, r_off, v_off, stage_bytes;
 };
 
 // bytes of one epilogue vector's slice for a full tile (3 components per row)
@@ -204,27 +237,25 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 __device__ __forceinline__ unsigned long long lo16(const void* p) { return (unsigned long long)p & ~15ull; }
 __device__ __forceinline__ unsigned long long hi16(const void* p) { return ((unsigned long long)p + 15ull) & ~15ull; }
 
-// One bulk copy group per tile m: its blocks and column indices (16-byte-rounded ranges),
-// its kTileRows + 1 row pointers, block-Jacobi inverses and the slices of up to three
-// epilogue vectors (these start on 16-byte boundaries: tile offsets are multiples of 128,
-// 1152 and 768 bytes).  All completions land on one mbarrier.
+// One bulk copy group per tile m: its off-diagonal blocks and column indices (16-byte-rounded
+// ranges), its kTileRows + 1 row pointers and the slices of up to three epilogue vectors (these
+// start on 16-byte boundaries: tile offsets are multiples of 128 and 768 bytes).  All
+// completions land on one mbarrier.
 template <typename MT, typename VT>
-__device__ __forceinline__ void issue_tile(int m, int V, const int* rowptr, const int* col, const MT* A,
-                                           const MT* Dinv, int nvec, const VT* const* vecs, unsigned char* stage,
-                                           const KrylovArgs& K, unsigned long long* bar, unsigned long long pol) {
+__device__ __forceinline__ void issue_tile(int m, int V, const int* rowptr, const int* col, const MT* A, int nvec,
+                                           const VT* const* vecs, unsigned char* stage, const KrylovArgs& K,
+                                           unsigned long long* bar, unsigned long long pol) {
     const int r0 = m * kTileRows, nr = min(kTileRows, V - r0);
     const int k0 = __ldg(rowptr + r0), k1 = __ldg(rowptr + r0 + nr);
     const unsigned long long alo = lo16(A + (size_t)k0 * 9), ahi = hi16(A + (size_t)k1 * 9);
     const unsigned long long clo = lo16(col + k0), chi = hi16(col + k1);
     const unsigned ab = (unsigned)(ahi - alo), cb = (unsigned)(chi - clo);
     const unsigned rb = ((unsigned)(nr + 1) * 4u + 15u) & ~15u;
-    const unsigned db = ((unsigned)nr * 9u * (unsigned)sizeof(MT) + 15u) & ~15u;
     const unsigned vb = ((unsigned)nr * 3u * (unsigned)sizeof(VT) + 15u) & ~15u;
-    mbar_arrive_expect_tx(bar, ab + cb + rb + db + (unsigned)nvec * vb);
-    bulk_load_hint(stage, (const void*)alo, ab, bar, pol);
-    bulk_load_hint(stage + K.c_off, (const void*)clo, cb, bar, pol);
+    mbar_arrive_expect_tx(bar, ab + cb + rb + (unsigned)nvec * vb);
+    if (ab) bulk_load_hint(stage, (const void*)alo, ab, bar, pol);
+    if (cb) bulk_load_hint(stage + K.c_off, (const void*)clo, cb, bar, pol);
     bulk_load_hint(stage + K.r_off, rowptr + r0, rb, bar, pol);
-    bulk_load_hint(stage + K.d_off, Dinv + (size_t)r0 * 9, db, bar, pol);
     for (int v = 0; v < nvec; v++)
         bulk_load(stage + K.v_off + v * tile_vec_bytes<VT>(), vecs[v] + (size_t)r0 * 3, vb, bar);
 }
@@ -234,18 +265,18 @@ struct IntC {
     static constexpr int value = N;
 };
 
-// y = Dinv_i * sum_j A'_ij x_j for node row i (blocks kb..ke-1), with x_j = xa_j - alpha * xb_j
-// when xb != null.  Eight lanes share a row and each lane takes whole 3x3 blocks (lane l: the
-// row's blocks l, l+8, ...); the column index and the three x components are loaded once per
-// block.  blk(k) / cix(k) / dinv(q) give block k's values, its column index and entry q of the
-// row's block-Jacobi inverse (from the staged tile in shared memory, or from global memory).
-// The three row sums are combined with xor shuffles in a fixed order, so staged and direct
-// sweeps give bitwise identical results.  Products and sums are formed in the matrix type MT
-// (FP32 accumulation on the mixed path).  The result is valid on lane 0 of the group;
-// `active` false contributes zeros so the whole warp can shuffle.
-template <typename MT, typename VT, class BLK, class CIX, class DIN>
-__device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke, BLK blk, CIX cix, DIN dinv,
-                                          const VT* xa, const VT* xb, VT alpha, VT y[3]) {
+// Off-diagonal row sum y = sum_j B_ij x_j of the folded operator (B_ij = D_i^-1 A'_ij, blocks
+// kb..ke-1) for node row i, with x_j = xa_j - alpha * xb_j when xb != null; the caller adds the
+// identity diagonal block's x_i.  Eight lanes share a row and each lane takes whole 3x3 blocks
+// (lane l: the row's blocks l, l+8, ...); the column index and the three x components are loaded
+// once per block.  blk(k) / cix(k) give block k's values and column index (from the staged tile
+// in shared memory, or from global memory).  The three sums are combined with xor shuffles in a
+// fixed order, so staged and direct sweeps give bitwise identical results.  Products and sums
+// are formed in the matrix type MT (FP32 accumulation on the mixed path).  The result is valid
+// on lane 0 of the group; `active` false contributes zeros so the whole warp can shuffle.
+template <typename MT, typename VT, class BLK, class CIX>
+__device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke, BLK blk, CIX cix, const VT* xa,
+                                          const VT* xb, VT alpha, VT y[3]) {
     MT a0 = 0, a1 = 0, a2 = 0;
     if (active) {
         for (int k = kb + lane8; k < ke; k += kRowLanes) {
@@ -272,30 +303,28 @@ __device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke
         a1 += __shfl_xor_sync(0xffffffffu, a1, o, kRowLanes);
         a2 += __shfl_xor_sync(0xffffffffu, a2, o, kRowLanes);
     }
-    if (active && lane8 == 0) {
-        y[0] = (VT)(dinv(0) * a0 + dinv(1) * a1 + dinv(2) * a2);
-        y[1] = (VT)(dinv(3) * a0 + dinv(4) * a1 + dinv(5) * a2);
-        y[2] = (VT)(dinv(6) * a0 + dinv(7) * a1 + dinv(8) * a2);
-    } else {
-        y[0] = y[1] = y[2] = (VT)0;
-    }
+    y[0] = (VT)a0;
+    y[1] = (VT)a1;
+    y[2] = (VT)a2;
 }
 
-// MT: matrix / preconditioner storage and SpMV accumulation type; VT: Krylov vector type
-// (FP64 on both paths: FP32 vectors let the recursively updated residual drift away from
-// the true one and the iteration stagnates).  STAGED: the SpMV sweeps read each tile's
-// blocks, column indices, row pointers, block-Jacobi inverses and epilogue vectors from a
-// kStages-deep shared-memory ring filled by bulk copies (one thread issues, completion on an
-// mbarrier) kStages - 1 tiles ahead of the rows being computed, so a row's only global loads
-// are its x gathers; the streamed matrix data carry an L2 evict-first hint, which keeps the
-// Krylov vectors in L2.  The dynamic shared memory is kStages * K.stage_bytes.  Otherwise the
-// lanes load everything from global memory.
+// MT: matrix storage and SpMV accumulation type; VT: Krylov vector type (FP64 on both paths:
+// FP32 vectors let the recursively updated residual drift away from the true one and the
+// iteration stagnates).  A holds the folded off-diagonal blocks D_i^-1 A'_ij (rowptr / col of
+// K), Dinv the FP64 inverses (used once, for b = M^-1 b').  STAGED: the SpMV sweeps read each
+// tile's blocks, column indices, row pointers and epilogue vectors from a kStages-deep
+// shared-memory ring filled by bulk copies (one thread issues, completion on an mbarrier)
+// kStages - 1 tiles ahead of the rows being computed, so a row's only global loads are its x
+// gathers; the streamed matrix data carry an L2 evict-first hint, which keeps the Krylov
+// vectors in L2.  The dynamic shared memory is kStages * K.stage_bytes.  Otherwise the lanes
+// load everything from global memory.
 template <typename MT, typename VT, bool STAGED>
 __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, const MT* __restrict__ A,
-                                                            const MT* __restrict__ Dinv, VT* __restrict__ b,
-                                                            VT* __restrict__ uu, VT* __restrict__ r,
-                                                            VT* __restrict__ q, VT* __restrict__ p, VT* __restrict__ Ap,
-                                                            VT* __restrict__ As, VT* __restrict__ ubest) {
+                                                               const double* __restrict__ Dinv, VT* __restrict__ b,
+                                                               VT* __restrict__ uu, VT* __restrict__ r,
+                                                               VT* __restrict__ q, VT* __restrict__ p,
+                                                               VT* __restrict__ Ap, VT* __restrict__ As,
+                                                               VT* __restrict__ ubest) {
     __shared__ double red[4 * kKrylovWarps];
     __shared__ unsigned long long bar[kStages];
     extern __shared__ __align__(128) unsigned char stage_mem[];
@@ -324,8 +353,9 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
     }
 
     // One SpMV sweep over this CTA's tiles (m = blockIdx.x, blockIdx.x + gridDim.x, ...):
-    // y = M^-1 A' (xa - alpha xb) per row; lane 0 of each row group calls epi(i, y, ev) with
-    // ev[v][c] = component c of epilogue vector v at row i (NV vectors: v0, v1, v2).
+    // y = sum_j B_ij (xa_j - alpha xb_j) over the off-diagonal blocks of each row; lane 0 of each
+    // row group calls epi(i, y, ev) with ev[v][c] = component c of epilogue vector v at row i
+    // (NV vectors: v0, v1, v2), from which the epilogue forms the diagonal term.
     auto sweep = [&](auto nvc, const VT* xa, const VT* xb, VT alpha, const VT* v0, const VT* v1, const VT* v2,
                      auto&& epi) {
         constexpr int NV = decltype(nvc)::value;
@@ -335,7 +365,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
             for (int d = 0; d < kStages - 1; d++) {
                 const int m = blockIdx.x + d * gridDim.x;
                 if (m < ntiles)
-                    issue_tile<MT, VT>(m, V, K.rowptr, K.col, A, Dinv, NV, vecs, stage(tc + d), K,
+                    issue_tile<MT, VT>(m, V, K.rowptr, K.col, A, NV, vecs, stage(tc + d), K,
                                        &bar[(tc + d) % kStages], pol);
             }
         }
@@ -343,13 +373,13 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
             const int i = m * kTileRows + li;
             const bool act = i < V;
             VT y[3];
-            VT ev[NV > 0 ? NV : 1][3];
+            VT ev[NV][3];
             if (STAGED) {
                 if (threadIdx.x == 0) {
                     // into the stage of tile tc - 1, released by the __syncthreads that ended it
                     const int mn = m + (kStages - 1) * gridDim.x;
                     if (mn < ntiles)
-                        issue_tile<MT, VT>(mn, V, K.rowptr, K.col, A, Dinv, NV, vecs, stage(tc + kStages - 1), K,
+                        issue_tile<MT, VT>(mn, V, K.rowptr, K.col, A, NV, vecs, stage(tc + kStages - 1), K,
                                            &bar[(tc + kStages - 1) % kStages], pol);
                 }
                 // a wait that runs out flags the error once; this thread then stops waiting, the
@@ -363,12 +393,11 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
                 const int k0 = sR[0];
                 const MT* sA = (const MT*)(st + ((unsigned long long)(A + (size_t)k0 * 9) & 15ull));
                 const int* sC = (const int*)(st + K.c_off + ((unsigned long long)(K.col + k0) & 15ull));
-                const MT* sD = (const MT*)(st + K.d_off) + li * 9;
                 const VT* sV = (const VT*)(st + K.v_off);
                 const int kb = act ? sR[li] : 0, ke = act ? sR[li + 1] : 0;
                 row_apply<MT, VT>(
                     act, lane8, kb, ke, [&](int k) { return sA + (size_t)(k - k0) * 9; },
-                    [&](int k) { return sC[k - k0]; }, [&](int qq) { return sD[qq]; }, xa, xb, alpha, y);
+                    [&](int k) { return sC[k - k0]; }, xa, xb, alpha, y);
                 if (act && lane8 == 0) {
 #pragma unroll
                     for (int v = 0; v < NV; v++)
@@ -383,11 +412,9 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
                         for (int c = 0; c < 3; c++) ev[v][c] = ldv(vecs[v] + 3 * i + c);
                 }
                 const int kb = act ? __ldg(K.rowptr + i) : 0, ke = act ? __ldg(K.rowptr + i + 1) : 0;
-                const MT* gD = Dinv + (size_t)i * 9;
                 row_apply<MT, VT>(
                     act, lane8, kb, ke, [&](int k) { return A + (size_t)k * 9; },
-                    [&](int k) { return __ldg(K.col + k); }, [&](int qq) { return __ldg(gD + qq); }, xa, xb, alpha,
-                    y);
+                    [&](int k) { return __ldg(K.col + k); }, xa, xb, alpha, y);
             }
             if (act && lane8 == 0) epi(i, y, ev);
             if (STAGED) {
@@ -399,11 +426,11 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
 
     // b <- M^-1 b'
     for (int i = t0; i < V; i += stride) {
-        const MT* d = Dinv + (size_t)i * 9;
+        const double* d = Dinv + (size_t)i * 9;
         const double b0 = K.bs[3 * i], b1 = K.bs[3 * i + 1], b2 = K.bs[3 * i + 2];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            const VT y = (VT)((double)d[3 * c] * b0 + (double)d[3 * c + 1] * b1 + (double)d[3 * c + 2] * b2);
+            const VT y = (VT)(d[3 * c] * b0 + d[3 * c + 1] * b1 + d[3 * c + 2] * b2);
             b[3 * i + c] = y;
             uu[3 * i + c] = y;
         }
@@ -413,11 +440,11 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
     {
         double vals[4] = {0, 0, 0, 0};
         const int ism[4] = {MAX, MAX, SUM, SUM};
-        sweep(IntC<1>{}, uu, (const VT*)nullptr, (VT)0, b, nullptr, nullptr, [&](int i, const VT* y, const VT (*ev)[3]) {
+        sweep(IntC<2>{}, uu, (const VT*)nullptr, (VT)0, b, uu, nullptr, [&](int i, const VT* y, const VT (*ev)[3]) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const VT bb = ev[0][c];
-                const VT rr = bb - y[c];
+                const VT rr = bb - (ev[1][c] + y[c]);
                 r[3 * i + c] = rr;
                 q[3 * i + c] = rr;
                 p[3 * i + c] = rr;
@@ -450,12 +477,13 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
             {
                 double g[4] = {0, 0, 0, 0};
                 const int gm[4] = {SUM, SUM, SUM, SUM};
-                sweep(IntC<1>{}, p, (const VT*)nullptr, (VT)0, q, nullptr, nullptr,
+                sweep(IntC<2>{}, p, (const VT*)nullptr, (VT)0, q, p, nullptr,
                       [&](int i, const VT* y, const VT (*ev)[3]) {
 #pragma unroll
                           for (int c = 0; c < 3; c++) {
-                              Ap[3 * i + c] = y[c];
-                              g[0] += (double)ev[0][c] * (double)y[c];
+                              const VT apc = ev[1][c] + y[c];
+                              Ap[3 * i + c] = apc;
+                              g[0] += (double)ev[0][c] * (double)apc;
                           }
                       });
                 block_partial<1>(g, gm, pbuf(), red);
@@ -473,10 +501,11 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
                         const VT s = ev[0][c] - al * ev[1][c];
-                        As[3 * i + c] = y[c];
-                        w[0] += (double)y[c] * (double)s;
-                        w[1] += (double)y[c] * (double)y[c];
-                        w[2] += (double)y[c] * (double)ev[2][c];
+                        const VT asc = s + y[c];
+                        As[3 * i + c] = asc;
+                        w[0] += (double)asc * (double)s;
+                        w[1] += (double)asc * (double)asc;
+                        w[2] += (double)asc * (double)ev[2][c];
                     }
                 });
                 block_partial<3>(w, wm, pbuf(), red);
@@ -487,28 +516,25 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
                 rhop = rho;
                 rho = -1.0 * omega * w[2];
             }
-            // (h)-(i) and the next search direction (c): u += alpha p + omega s; r = s - omega As;
+    // (h)-(i) and the next search direction (c): u += alpha p + omega s; r = s - omega As;
             // p = beta (p - omega Ap) + r with beta = (rho alpha) / (rhop omega)
             {
                 double mx[4] = {0, 0, 0, 0};
                 const int mm[4] = {MAX, MAX, MAX, MAX};
                 const double beta = (rho * alpha) / (rhop * omega);
                 const VT al = (VT)alpha, om = (VT)omega, be = (VT)beta;
-                for (int i = t0; i < V; i += stride) {
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        const int k = 3 * i + c;
-                        const VT s = ldv(r + k) - al * ldv(Ap + k);
-                        VT uk = ldv(uu + k);
-                        if (pending) ubest[k] = uk;
-                        uk += al * ldv(p + k);
-                        uk += om * s;
-                        uu[k] = uk;
-                        const VT rk = s - om * ldv(As + k);
-                        r[k] = rk;
-                        p[k] = (ldv(p + k) - om * ldv(Ap + k)) * be + rk;
-                        mx[0] = fmax(mx[0], fabs((double)rk));
-                    }
+                for (int k = t0; k < 3 * V; k += stride) {   // element-wise: every load coalesced
+                    const VT apk = ldv(Ap + k), pk = ldv(p + k);
+                    const VT s = ldv(r + k) - al * apk;
+                    VT uk = ldv(uu + k);
+                    if (pending) ubest[k] = uk;
+                    uk += al * pk;
+                    uk += om * s;
+                    uu[k] = uk;
+                    const VT rk = s - om * ldv(As + k);
+                    r[k] = rk;
+                    p[k] = (pk - om * apk) * be + rk;
+                    mx[0] = fmax(mx[0], fabs((double)rk));
                 }
                 block_partial<1>(mx, mm, pbuf(), red);
                 if (!grid_sync(ctl)) return;

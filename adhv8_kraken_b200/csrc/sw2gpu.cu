@@ -97,8 +97,12 @@ struct sw2gpu_ctx {
     int ngeneral = 0;
     // work
     DBuf<double> sc, sx, sy, R, sol, jslots, val, S_, bs;
-    DBuf<float> val32, dinv32;
-    DBuf<double> dinv64;
+    // Krylov operator: block-Jacobi inverse folded into the off-diagonal blocks
+    // (orowptr / ocol: the BCSR pattern without its diagonal); FP64 or FP32 storage
+    std::vector<int> orowptr_h;
+    DBuf<int> orowptr, ocol;
+    DBuf<double> aoff64, dinv64;
+    DBuf<float> aoff32;
     DBuf<double> kv64[8];
     DBuf<double> part;
     DBuf<KrylovCtl> ctl;
@@ -109,7 +113,7 @@ struct sw2gpu_ctx {
     KrylovCtl* ctl_h = nullptr;
     int krylov_grid = 0;
     bool staged = false;            // Krylov sweeps read matrix tiles through the shared-memory ring
-    unsigned c_off = 0, r_off = 0, d_off = 0, v_off = 0, stage_bytes = 0;
+    unsigned c_off = 0, r_off = 0, v_off = 0, stage_bytes = 0;
     size_t krylov_smem = 0;         // dynamic shared memory of the Krylov launch
     int launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -316,17 +320,18 @@ int launch_linear(sw2gpu_ctx* c, int apply_inc, double rtol) {
     k_rowscale<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->dm, s, c->val.p, c->R.p, c->S_.p, c->bs.p, 0);
     CK(cudaMemsetAsync(c->singular.p, 0, sizeof(int), c->stream));
     const bool mixed = c->p.precision == SW2GPU_MIXED;
+    k_fold_diag<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->S_.p, c->dinv64.p, c->singular.p);
     if (mixed)
-        k_scale_matrix<float><<<nblk(c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->val32.p, c->S_.p,
-                                                                         c->dinv32.p, c->singular.p);
+        k_fold_offdiag<float><<<nblk(c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->S_.p, c->dinv64.p,
+                                                                         c->aoff32.p);
     else
-        k_scale_matrix<double><<<nblk(c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->val.p, c->S_.p,
-                                                                          c->dinv64.p, c->singular.p);
+        k_fold_offdiag<double><<<nblk(c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->S_.p, c->dinv64.p,
+                                                                          c->aoff64.p);
     CK(cudaMemsetAsync(c->ctl.p, 0, sizeof(KrylovCtl), c->stream));
     KrylovArgs K;
     K.V = c->V;
-    K.rowptr = c->rowptr.p;
-    K.col = c->col.p;
+    K.rowptr = c->orowptr.p;
+    K.col = c->ocol.p;
     K.S = c->S_.p;
     K.bs = c->bs.p;
     K.rtol = rtol;
@@ -341,20 +346,19 @@ int launch_linear(sw2gpu_ctx* c, int apply_inc, double rtol) {
     K.ctl = c->ctl.p;
     K.c_off = c->c_off;
     K.r_off = c->r_off;
-    K.d_off = c->d_off;
     K.v_off = c->v_off;
     K.stage_bytes = c->stage_bytes;
     dim3 grid(c->krylov_grid), block(kKrylovThreads);
     Phase ph(c, kPhKrylov);
     if (mixed) {
-        const float* A = c->val32.p;
-        const float* D = c->dinv32.p;
+        const float* A = c->aoff32.p;
+        const double* D = c->dinv64.p;
         double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
                *Ap = c->kv64[5].p, *As = c->kv64[6].p, *ub = c->kv64[7].p;
         void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As, &ub};
         CK(cudaLaunchCooperativeKernel(krylov_kernel<float>(c->staged), grid, block, args, c->krylov_smem, c->stream));
     } else {
-        const double* A = c->val.p;
+        const double* A = c->aoff64.p;
         const double* D = c->dinv64.p;
         double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
                *Ap = c->kv64[5].p, *As = c->kv64[6].p, *ub = c->kv64[7].p;
@@ -585,11 +589,24 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     rc |= zalloc(c->jslots, nsrc * 9, st);
     rc |= zalloc(c->val, 9ull * nnzb, st);
     rc |= zalloc(c->S_, 3ull * V, st); rc |= zalloc(c->bs, 3ull * V, st);
-    if (prm->precision == SW2GPU_MIXED) {
-        rc |= zalloc(c->val32, 9ull * nnzb, st);
-        rc |= zalloc(c->dinv32, 9ull * V, st);
-    } else {
-        rc |= zalloc(c->dinv64, 9ull * V, st);
+    rc |= zalloc(c->dinv64, 9ull * V, st);
+    if (prm->precision == SW2GPU_MIXED)
+        rc |= zalloc(c->aoff32, 9ull * (nnzb - V), st);
+    else
+        rc |= zalloc(c->aoff64, 9ull * (nnzb - V), st);
+    {
+        // the pattern without its diagonal (one diagonal block per row, checked above)
+        std::vector<int>& orp = c->orowptr_h;
+        orp.assign(V + 1, 0);
+        std::vector<int> ocol;
+        ocol.reserve(nnzb - V);
+        for (int n = 0; n < V; n++) {
+            for (int k = rp[n]; k < rp[n + 1]; k++)
+                if (col[k] != n) ocol.push_back(col[k]);
+            orp[n + 1] = (int)ocol.size();
+        }
+        rc |= up(c->orowptr, orp, st);
+        rc |= up(c->ocol, ocol, st);
     }
     for (auto& b : c->kv64) rc |= zalloc(b, 3ull * V, st);
     rc |= zalloc(c->ctl, 1, st);
@@ -608,17 +625,15 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
         const bool mixed = prm->precision == SW2GPU_MIXED;
         const unsigned esz = mixed ? sizeof(float) : sizeof(double);
         unsigned a_cap = 0, c_cap = 0;
-        stage_caps(rp, V, esz, a_cap, c_cap);
-        // stage layout: blocks | column indices | kTileRows + 1 row pointers | inverses | 3 vectors
+        stage_caps(c->orowptr_h, V, esz, a_cap, c_cap);
+        // stage layout: blocks | column indices | kTileRows + 1 row pointers | 3 vectors
         const unsigned c_off = a_cap, r_off = c_off + c_cap;
-        const unsigned d_off = r_off + ((unsigned)(kTileRows + 1) * 4u + 15u) / 16u * 16u;
-        const unsigned v_off = d_off + (unsigned)kTileRows * 9u * esz;
+        const unsigned v_off = r_off + ((unsigned)(kTileRows + 1) * 4u + 15u) / 16u * 16u;
         const unsigned stage = (v_off + 3u * tile_vec_bytes<double>() + 127u) & ~127u;
         c->staged = (size_t)kStages * stage <= kMaxStagedSmem;
         if (c->staged) {
             c->c_off = c_off;
             c->r_off = r_off;
-            c->d_off = d_off;
             c->v_off = v_off;
             c->stage_bytes = stage;
         }

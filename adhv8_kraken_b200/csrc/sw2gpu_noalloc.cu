@@ -34,14 +34,17 @@ constexpr int kMaxBlocks = SW2GPU_NOALLOC_MAX_BLOCKS;
 constexpr int kMaxGrid = (kMaxNodes + kKrylovThreads - 1) / kKrylovThreads;   // persistent-kernel blocks
 constexpr size_t kAlign = 32;                                                 // doubles = 256 bytes
 constexpr size_t al(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
-// layout (in doubles): control word, partials, S, b', Dinv, scaled matrix, 8 Krylov vectors
+// layout (in doubles): control word, partials, S, b', Dinv, folded off-diagonal blocks, their
+// row pointers and column indices (int32, two per double), 8 Krylov vectors
 constexpr size_t kOffCtl = 0;
 constexpr size_t kOffPart = kOffCtl + al((sizeof(KrylovCtl) + 7) / 8);
 constexpr size_t kOffS = kOffPart + al(2ull * kMaxGrid * 4);
 constexpr size_t kOffB = kOffS + al(3ull * kMaxNodes);
 constexpr size_t kOffDinv = kOffB + al(3ull * kMaxNodes);
 constexpr size_t kOffA = kOffDinv + al(9ull * kMaxNodes);
-constexpr size_t kOffVec = kOffA + al(9ull * kMaxBlocks);
+constexpr size_t kOffRp = kOffA + al(9ull * kMaxBlocks);
+constexpr size_t kOffCol = kOffRp + al((kMaxNodes + 2) / 2);
+constexpr size_t kOffVec = kOffCol + al((kMaxBlocks + 1) / 2);
 constexpr size_t kScratchDoubles = kOffVec + 8 * al(3ull * kMaxNodes);
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
@@ -80,51 +83,49 @@ __global__ void k_na_rowscale(int V, const int* __restrict__ rowptr, const doubl
     }
 }
 
-// A' = S A S into the scratch copy and the inverse of each scaled diagonal block,
-// one thread per node row (the caller's matrix is not modified)
-__global__ void k_na_scale(int V, const int* __restrict__ rowptr, const int* __restrict__ col,
-                           const double* __restrict__ val, const double* __restrict__ S, double* __restrict__ Aout,
-                           double* __restrict__ dinv, int* __restrict__ singular) {
+// The Krylov operator with the block-Jacobi inverse folded in, one thread per node row: the
+// inverse D_i^-1 of the scaled diagonal block S_i A_ii S_i, and the row's off-diagonal blocks
+// D_i^-1 S_i A_ij S_j with their column indices, packed without the diagonal (position k - i
+// for blocks before it, k - i - 1 after it).  A row without a diagonal block sets `singular`;
+// positions stay below nnzb, so nothing is written outside the scratch regions.
+__global__ void k_na_fold(int V, const int* __restrict__ rowptr, const int* __restrict__ col,
+                          const double* __restrict__ val, const double* __restrict__ S, double* __restrict__ dinv,
+                          double* __restrict__ aoff, int* __restrict__ orp, int* __restrict__ ocol,
+                          int* __restrict__ singular) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V) return;
-    bool have_diag = false;
-    for (int k = rowptr[i]; k < rowptr[i + 1]; k++) {
-        const int j = col[k];
+    const int kb = rowptr[i], ke = rowptr[i + 1];
+    int dp = -1;
+    for (int k = kb; k < ke; k++)
+        if (col[k] == i) dp = k;
+    double d[9];
+    if (dp < 0) {
+        *singular = 1;
+#pragma unroll
+        for (int q = 0; q < 9; q++) d[q] = (q % 4 == 0) ? 1.0 : 0.0;
+    } else {
         double a[9];
 #pragma unroll
         for (int r = 0; r < 3; r++)
 #pragma unroll
-            for (int c = 0; c < 3; c++) a[3 * r + c] = val[(size_t)k * 9 + 3 * r + c] * (S[3 * i + r] * S[3 * j + c]);
-#pragma unroll
-        for (int q = 0; q < 9; q++) Aout[(size_t)k * 9 + q] = a[q];
-        if (j != i) continue;
-        have_diag = true;
-        const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
-        const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
-        double inv[9];
-        if (det == 0.0 || !isfinite(det)) {
-            *singular = 1;
-#pragma unroll
-            for (int q = 0; q < 9; q++) inv[q] = (q % 4 == 0) ? 1.0 : 0.0;
-        } else {
-            const double id = 1.0 / det;
-            inv[0] = c00 * id;
-            inv[1] = (a[2] * a[7] - a[1] * a[8]) * id;
-            inv[2] = (a[1] * a[5] - a[2] * a[4]) * id;
-            inv[3] = c01 * id;
-            inv[4] = (a[0] * a[8] - a[2] * a[6]) * id;
-            inv[5] = (a[2] * a[3] - a[0] * a[5]) * id;
-            inv[6] = c02 * id;
-            inv[7] = (a[1] * a[6] - a[0] * a[7]) * id;
-            inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
-        }
-#pragma unroll
-        for (int q = 0; q < 9; q++) dinv[(size_t)i * 9 + q] = inv[q];
+            for (int c = 0; c < 3; c++) a[3 * r + c] = val[(size_t)dp * 9 + 3 * r + c] * (S[3 * i + r] * S[3 * i + c]);
+        if (!inv3(a, d)) *singular = 1;
     }
-    if (!have_diag) {
-        *singular = 1;
 #pragma unroll
-        for (int q = 0; q < 9; q++) dinv[(size_t)i * 9 + q] = (q % 4 == 0) ? 1.0 : 0.0;
+    for (int q = 0; q < 9; q++) dinv[(size_t)i * 9 + q] = d[q];
+    orp[i] = kb - i;
+    if (i == V - 1) orp[V] = ke - V;
+    for (int k = kb; k < ke; k++) {
+        if (k == dp) continue;
+        const int j = col[k];
+        double bq[9];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) bq[3 * r + c] = val[(size_t)k * 9 + 3 * r + c] * (S[3 * i + r] * S[3 * j + c]);
+        const int ko = k - i - ((dp >= 0 && k > dp) ? 1 : 0);
+        ocol[ko] = j;
+        fold_block(d, bq, aoff + (size_t)ko * 9);
     }
 }
 
@@ -168,6 +169,8 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     double* bs = sc + kOffB;
     double* dinv = sc + kOffDinv;
     double* A = sc + kOffA;
+    int* orp = reinterpret_cast<int*>(sc + kOffRp);
+    int* ocol = reinterpret_cast<int*>(sc + kOffCol);
     double* v[8];
     for (int k = 0; k < 8; k++) v[k] = sc + kOffVec + k * al(3ull * kMaxNodes);
     // the control words (barrier counter and generation, error and result fields) must
@@ -177,7 +180,7 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     int* singular = reinterpret_cast<int*>(&ctl->pad);
     const int nb = (nnodes + 255) / 256;
     k_na_rowscale<<<nb, 256, 0, st>>>(nnodes, row_ptr, val, rhs, S, bs);
-    k_na_scale<<<nb, 256, 0, st>>>(nnodes, row_ptr, col, val, S, A, dinv, singular);
+    k_na_fold<<<nb, 256, 0, st>>>(nnodes, row_ptr, col, val, S, dinv, A, orp, ocol, singular);
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -186,8 +189,8 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
                                            sms * std::max(per_sm, 1)}));
     KrylovArgs K;
     K.V = nnodes;
-    K.rowptr = row_ptr;
-    K.col = col;
+    K.rowptr = orp;
+    K.col = ocol;
     K.S = S;
     K.bs = bs;
     K.rtol = rtol;
@@ -198,7 +201,7 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     K.apply_inc = 0;
     K.part = part;
     K.ctl = ctl;
-    K.c_off = K.r_off = K.d_off = K.v_off = K.stage_bytes = 0;   // direct sweeps
+    K.c_off = K.r_off = K.v_off = K.stage_bytes = 0;   // direct sweeps
     const double* Ac = A;
     const double* Dc = dinv;
     void* args[] = {&K, &Ac, &Dc, &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7]};
@@ -211,5 +214,6 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     if (e != cudaSuccess) return na_fail(SW2GPU_E_CUDA, cudaGetErrorString(e));
     if (iterations) *iterations = h.iterations;
     if (h.err) return na_fail(SW2GPU_E_TIMEOUT, "Krylov grid barrier wait ran out");
+    if (h.pad) return na_fail(SW2GPU_E_LINEAR, "a node row has no diagonal block or a singular one");
     return h.converged ? SW2GPU_OK : na_fail(SW2GPU_E_LINEAR, "BiCGSTAB did not reach the tolerance");
 }
