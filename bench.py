@@ -201,14 +201,21 @@ def run_ours(args, rank, world, local_rank):
     lin = sum(s["linear_its"] for s in stats)
     nnzb = g.nnzb
     hbm, src = peaks()
-    # algorithmic bytes per launch: FD Jacobian = element inputs + node state + 81 outputs per
-    # triangle; BiCGSTAB iteration = two SpMV passes over the BCSR values, column indices,
-    # row pointers and block-Jacobi inverses plus 14 vector streams of 3 doubles per node
-    jac_bytes = T * (3 * 4 + 7 * 8 + 4 + 4 + 1) + V * 12 * 8 + T * 81 * 8       # gather + element data + 81 outputs
-    kry_iter_bytes = 2 * (nnzb * (9 * 8 + 4) + (V + 1) * 4 + V * 9 * 8) + V * 3 * 8 * 14
+    # algorithmic bytes per launch.  FD Jacobian: element inputs + node state + 81 outputs per
+    # triangle.  BiCGSTAB on the folded operator (block-Jacobi inverse multiplied into the
+    # off-diagonal blocks, identity diagonal): per iteration two sweeps over the nnzb - V
+    # off-diagonal blocks (72 B values + 4 B column) and the row pointers, plus 16 vector
+    # streams of 3 doubles per node (sweep 1: q, p in, Ap out; sweep 2: r, Ap, q in, As out;
+    # update: r, Ap, u, p, As in, u, r, p, best-u out).  Per launch once: b' and the inverses
+    # in, b and u out (prologue), one more sweep with b, u in and r, q, p, Ap out, and the
+    # exit pass (u and S in, state in and out, solution out).
+    jac_bytes = T * (3 * 4 + 7 * 8 + 4 + 4 + 1) + V * 12 * 8 + T * 81 * 8
+    sweep_bytes = (nnzb - V) * (9 * 8 + 4) + (V + 1) * 4
+    kry_iter_bytes = 2 * sweep_bytes + V * 24 * 16
+    kry_launch_bytes = V * (24 + 72 + 48) + sweep_bytes + V * 24 * 6 + V * (48 + 48 + 24)
     kernels = {
         "k_jac_elem": (jac, newton, jac_bytes),
-        "k_bicgstab": (kry, newton, kry_iter_bytes * (lin / max(newton, 1)) + V * 3 * 8 * 10),
+        "k_bicgstab": (kry, newton, kry_iter_bytes * (lin / max(newton, 1)) + kry_launch_bytes),
     }
     name = max(kernels, key=lambda k: kernels[k][0])
     tot_ms, launches, bytes_per_launch = kernels[name]
