@@ -42,6 +42,29 @@ struct Norms {                  // get_residual_norms (src/fe/fe_newton.c:40-151
     int ngeneral;               // elements on the wet/dry (general) Jacobian list
 };
 
+// Everything the assembly kernels need about one instance (one mesh and its state).  A launch
+// covers a list of instances -- a batch of independent solves of uneven size -- through a
+// device table of these and a LaunchMap (instance ids[j] owns blocks boff[j]..boff[j+1]-1);
+// a single solve is a batch of one.  Work indices inside a block are local to its instance,
+// so every instance computes exactly what it computes alone.
+struct Inst {
+    DevMesh m;
+    State s;
+    PhysParams P;
+    double *sc, *sx, *sy;       // residual slots (3T + 2E each)
+    double *R, *sol, *jslots, *val, *S, *bs, *dinv;
+    void* aoff;                 // folded off-diagonal blocks (MT of the Krylov launch)
+    unsigned char *ewet, *mark;
+    int *glist, *gcount;
+    Norms* npart;               // per-gather-block partials
+    Norms* norms;               // result of the last residual evaluation
+    unsigned* ncounter;
+    int* singular;
+    int ndir;                   // Dirichlet nodes and their step values
+    const int *dir_node, *dir_mask;
+    const double *dir_h, *dir_u, *dir_v;
+};
+
 // An element takes the fully wet Jacobian path when its flag is 0 and every vertex depth
 // at all three levels is positive with a margin no finite-difference perturbation of h
 // (|eps| <= max(1.5e-8, 1.5e-8 |h|)) can cross; every other element goes on the list.
@@ -93,9 +116,15 @@ __device__ __forceinline__ void classify_elem(int t, bool wet, unsigned char* ew
 }
 
 // the same classification without a residual (sw2gpu_load called on its own)
-__global__ void k_classify(DevMesh m, State s, unsigned char* __restrict__ ewet, int* __restrict__ glist,
-                           int* __restrict__ gcount) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_classify(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const State s = I.s;
+    unsigned char* ewet = I.ewet;
+    int* glist = I.glist;
+    int* gcount = I.gcount;
+    const int t = lb * blockDim.x + threadIdx.x;
     if (t >= m.T) return;
     double h[3], ho[3], hoo[3];
     const int n[3] = {m.en0[t], m.en1[t], m.en2[t]};
@@ -108,10 +137,19 @@ __global__ void k_classify(DevMesh m, State s, unsigned char* __restrict__ ewet,
     classify_elem(t, s.wd[t] == 0 && wet_depths(h, ho, hoo), ewet, glist, gcount);
 }
 
-__global__ void k_resid_elem(DevMesh m, State s, PhysParams P, double* __restrict__ sc, double* __restrict__ sx,
-                             double* __restrict__ sy, unsigned char* __restrict__ ewet, int* __restrict__ glist,
-                             int* __restrict__ gcount) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_resid_elem(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const State s = I.s;
+    const PhysParams P = I.P;
+    double* __restrict__ sc = I.sc;
+    double* __restrict__ sx = I.sx;
+    double* __restrict__ sy = I.sy;
+    unsigned char* ewet = I.ewet;
+    int* glist = I.glist;
+    int* gcount = I.gcount;
+    const int t = lb * blockDim.x + threadIdx.x;
     const int nslot = 3 * m.T + 2 * m.E;
     if (t < m.T) {
         ElemIn in;
@@ -190,15 +228,24 @@ __device__ __forceinline__ void block_reduce3(double& a, double& b, double& c, i
 // Node gather: R = -(sum of slots in reference order) ([u, v, h] per node), the dry-node
 // velocity zeroing, and get_residual_norms fused (max |R| and max |sol| over nodes with
 // min(h, h_old) > 0, sum R^2 over all).  The last block to finish reduces the per-block
-// partials in block order and writes *out; `counter` returns to 0.
+// partials in block order and writes *out (with the general-list length, after which the
+// list counter returns to 0 for the next evaluation); `counter` returns to 0.
 constexpr int kGatherThreads = 256;
-__global__ void __launch_bounds__(kGatherThreads) k_resid_gather(DevMesh m, State s, const double* __restrict__ sc,
-                                                                 const double* __restrict__ sx,
-                                                                 const double* __restrict__ sy, double* __restrict__ R,
-                                                                 const double* __restrict__ sol, Norms* partial,
-                                                                 unsigned* counter, Norms* out,
-                                                                 const int* __restrict__ gcount) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kGatherThreads) k_resid_gather(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const State s = I.s;
+    const double* __restrict__ sc = I.sc;
+    const double* __restrict__ sx = I.sx;
+    const double* __restrict__ sy = I.sy;
+    double* __restrict__ R = I.R;
+    const double* __restrict__ sol = I.sol;
+    Norms* partial = I.npart;
+    unsigned* counter = I.ncounter;
+    Norms* out = I.norms;
+    int* gcount = I.gcount;
+    const int n = lb * blockDim.x + threadIdx.x;
     double rmax = 0.0, l2 = 0.0, imax = 0.0;
     int nan = 0;
     if (n < m.V) {
@@ -229,15 +276,16 @@ __global__ void __launch_bounds__(kGatherThreads) k_resid_gather(DevMesh m, Stat
     block_reduce3<kGatherThreads>(rmax, l2, imax, nan);
     __shared__ bool last;
     if (threadIdx.x == 0) {
-        partial[blockIdx.x] = Norms{rmax, l2, imax, nan, 0};
+        partial[lb] = Norms{rmax, l2, imax, nan, 0};
         __threadfence();
-        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+        last = (atomicAdd(counter, 1u) == (unsigned)nb - 1u);
     }
     __syncthreads();
     if (last) {
+        __threadfence();
         double a = 0.0, b = 0.0, c = 0.0;
         int d = 0;
-        for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+        for (int k = threadIdx.x; k < nb; k += blockDim.x) {
             a = fmax(a, __ldcg(&partial[k].rmax));
             b += __ldcg(&partial[k].l2sum);
             c = fmax(c, __ldcg(&partial[k].imax));
@@ -245,7 +293,8 @@ __global__ void __launch_bounds__(kGatherThreads) k_resid_gather(DevMesh m, Stat
         }
         block_reduce3<kGatherThreads>(a, b, c, d);
         if (threadIdx.x == 0) {
-            *out = Norms{a, b, c, d, *gcount};
+            *out = Norms{a, b, c, d, *(volatile int*)gcount};
+            *gcount = 0;
             *counter = 0u;
         }
     }
@@ -271,11 +320,11 @@ struct __align__(16) StagedElem {
 template <bool GENERAL>
 __device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, const PhysParams& P,
                                               double* __restrict__ jslots, const unsigned char* __restrict__ ewet,
-                                              const int* __restrict__ list, int count) {
+                                              const int* __restrict__ list, int count, int lb) {
     __shared__ StagedElem se[kJacElems];
     __shared__ double out[kJacElems * 81];
     __shared__ int eid[kJacElems];
-    const int e0 = blockIdx.x * kJacElems;
+    const int e0 = lb * kJacElems;
     const int lane = threadIdx.x % kJacElems;
     const int item = threadIdx.x / kJacElems;
     const int nel = min(kJacElems, count - e0);
@@ -385,21 +434,35 @@ __device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, 
 #ifndef SW2_JAC_MIN_BLOCKS
 #define SW2_JAC_MIN_BLOCKS 2   // resident CTAs per SM the wet kernel's register budget is cut for
 #endif
-__global__ void __launch_bounds__(kJacThreads, SW2_JAC_MIN_BLOCKS) k_jac_elem_wet(DevMesh m, State s, PhysParams P,
-                                                               double* __restrict__ jslots,
-                                                               const unsigned char* __restrict__ ewet) {
-    jac_elem_body<false>(m, s, P, jslots, ewet, nullptr, m.T);
+__global__ void __launch_bounds__(kJacThreads, SW2_JAC_MIN_BLOCKS) k_jac_elem_wet(const Inst* __restrict__ tab,
+                                                                                  const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const State s = I.s;
+    const PhysParams P = I.P;
+    jac_elem_body<false>(m, s, P, I.jslots, I.ewet, nullptr, m.T, lb);
 }
-__global__ void __launch_bounds__(kJacThreads) k_jac_elem_general(DevMesh m, State s, PhysParams P,
-                                                                   double* __restrict__ jslots,
-                                                                   const int* __restrict__ list, int count) {
-    jac_elem_body<true>(m, s, P, jslots, nullptr, list, count);
+// the list length is the one the last residual evaluation recorded
+__global__ void __launch_bounds__(kJacThreads) k_jac_elem_general(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const State s = I.s;
+    const PhysParams P = I.P;
+    jac_elem_body<true>(m, s, P, I.jslots, nullptr, I.glist, I.norms->ngeneral, lb);
 }
 
 // FD Jacobian of the boundary edges: one thread per (edge, node, variable); writes the
 // four 3x3 blocks of edge j at slots 9T + 4j + 2a + b.
-__global__ void k_jac_edge(DevMesh m, State s, PhysParams P, double* __restrict__ jslots) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_jac_edge(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const State s = I.s;
+    const PhysParams P = I.P;
+    double* __restrict__ jslots = I.jslots;
+    const int t = lb * blockDim.x + threadIdx.x;
     if (t >= 6 * m.E) return;
     const int j = t / 6, b = (t % 6) / 3, var = t % 3;
     EdgeIn in;
@@ -465,8 +528,13 @@ __global__ void k_jac_edge(DevMesh m, State s, PhysParams P, double* __restrict_
 
 // BCSR values: thread (block k, entry q) sums entry q of every contributing element
 // block in reference order (fe_global_matrix_assemble_sw2 :166-224).
-__global__ void k_jac_gather(DevMesh m, const double* __restrict__ jslots, double* __restrict__ val) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_jac_gather(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const double* __restrict__ jslots = I.jslots;
+    double* __restrict__ val = I.val;
+    const long long t = (long long)lb * blockDim.x + threadIdx.x;
     if (t >= (long long)m.nnzb * 9) return;
     const int k = (int)(t / 9), q = (int)(t % 9);
     double acc = 0.0;
@@ -477,9 +545,16 @@ __global__ void k_jac_gather(DevMesh m, const double* __restrict__ jslots, doubl
 // Tiny-diagonal fix of fe_sw2_load (:218-236) and the Jacobi scale vector of spv_jacobi
 // (src/solver/spv_jacobi.c:222-285): S = 1/sqrt(max |row entry|), floored.  Also writes
 // the scaled right-hand side b = S R.
-__global__ void k_rowscale(DevMesh m, const State s, double* __restrict__ val, double* __restrict__ R,
-                           double* __restrict__ S, double* __restrict__ b, int fix_only) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_rowscale(const Inst* __restrict__ tab, const LaunchMap mp, int fix_only) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const State s = I.s;
+    double* __restrict__ val = I.val;
+    double* __restrict__ R = I.R;
+    double* __restrict__ S = I.S;
+    double* __restrict__ b = I.bs;
+    const int n = lb * blockDim.x + threadIdx.x;
     if (n >= m.V) return;
     double* d = val + (size_t)m.dpos[n] * 9;
     if (fabs(d[0]) < kNotQuiteSmall) {
@@ -512,9 +587,15 @@ __global__ void k_rowscale(DevMesh m, const State s, double* __restrict__ val, d
 // and D_i the scaled diagonal block of row i, the Krylov operator M^-1 A' has identity
 // diagonal blocks and off-diagonal blocks D_i^-1 A'_ij, so the sweeps stream only those
 // (nnzb - V blocks, no inverses).  k_fold_diag: D_i^-1 per node row (FP64).
-__global__ void k_fold_diag(DevMesh m, const double* __restrict__ val, const double* __restrict__ S,
-                            double* __restrict__ dinv, int* __restrict__ singular) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_fold_diag(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const double* __restrict__ val = I.val;
+    const double* __restrict__ S = I.S;
+    double* __restrict__ dinv = I.dinv;
+    int* singular = I.singular;
+    const int i = lb * blockDim.x + threadIdx.x;
     if (i >= m.V) return;
     const double* v = val + (size_t)m.dpos[i] * 9;
     double a[9];
@@ -528,9 +609,15 @@ __global__ void k_fold_diag(DevMesh m, const double* __restrict__ val, const dou
 // off-diagonal block k of row i -> position k - i - (k > dpos_i) of the folded matrix,
 // D_i^-1 (S_i A_ij S_j) formed in FP64 and stored as MT
 template <typename MT>
-__global__ void k_fold_offdiag(DevMesh m, const double* __restrict__ val, const double* __restrict__ S,
-                               const double* __restrict__ dinv, MT* __restrict__ aoff) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_fold_offdiag(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const double* __restrict__ val = I.val;
+    const double* __restrict__ S = I.S;
+    const double* __restrict__ dinv = I.dinv;
+    MT* __restrict__ aoff = (MT*)I.aoff;
+    const int k = lb * blockDim.x + threadIdx.x;
     if (k >= m.nnzb) return;
     const int i = m.blk_row[k], j = m.col[k];
     const int dp = m.dpos[i];
@@ -547,10 +634,15 @@ __global__ void k_fold_offdiag(DevMesh m, const double* __restrict__ val, const 
 }
 
 // line search halving (fe_newton.c:692-747): sol *= 0.5; state += sol (fe_sw2_inc)
-__global__ void k_half_inc(int V, double* __restrict__ sol, double* __restrict__ h, double* __restrict__ u,
-                           double* __restrict__ v) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= V) return;
+__global__ void k_half_inc(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    double* __restrict__ sol = I.sol;
+    double* __restrict__ h = I.s.h;
+    double* __restrict__ u = I.s.u;
+    double* __restrict__ v = I.s.v;
+    const int n = lb * blockDim.x + threadIdx.x;
+    if (n >= I.m.V) return;
     const double a = sol[3 * n] * 0.5, b = sol[3 * n + 1] * 0.5, c = sol[3 * n + 2] * 0.5;
     sol[3 * n] = a;
     sol[3 * n + 1] = b;
@@ -560,38 +652,64 @@ __global__ void k_half_inc(int V, double* __restrict__ sol, double* __restrict__
     h[n] += c;
 }
 
+// fe_sw2_init (src/fe/sw2/fe_sw2_init.c:24-92), first part: current level <- old level,
+// and the node marks of the wet/dry flag pass cleared
+__global__ void k_init_level(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const State s = I.s;
+    const int n = lb * blockDim.x + threadIdx.x;
+    if (n >= I.m.V) return;
+    s.h[n] = s.ho[n];
+    s.u[n] = s.uo[n];
+    s.v[n] = s.vo[n];
+    I.mark[n] = 0;
+}
+
 // fe_sw2_wdflag (src/fe/sw2/fe_sw2_wdflag.c:24-75), two passes
-__global__ void k_wd_mark(int T, const int* __restrict__ en0, const int* __restrict__ en1,
-                          const int* __restrict__ en2, const double* __restrict__ h, unsigned char* __restrict__ mark) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= T) return;
-    const int a = en0[e], b = en1[e], c = en2[e];
+__global__ void k_wd_mark(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const double* __restrict__ h = I.s.h;
+    unsigned char* __restrict__ mark = I.mark;
+    const int e = lb * blockDim.x + threadIdx.x;
+    if (e >= m.T) return;
+    const int a = m.en0[e], b = m.en1[e], c = m.en2[e];
     if (!(h[a] > 0.0 && h[b] > 0.0 && h[c] > 0.0)) {
         mark[a] = 1;
         mark[b] = 1;
         mark[c] = 1;
     }
 }
-__global__ void k_wd_flag(int T, const int* __restrict__ en0, const int* __restrict__ en1,
-                          const int* __restrict__ en2, const double* __restrict__ h, const double* __restrict__ ho,
-                          const unsigned char* __restrict__ mark, int* __restrict__ wd) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= T) return;
-    const int a = en0[e], b = en1[e], c = en2[e];
+__global__ void k_wd_flag(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const DevMesh m = I.m;
+    const double* __restrict__ h = I.s.h;
+    const double* __restrict__ ho = I.s.ho;
+    const unsigned char* __restrict__ mark = I.mark;
+    int* __restrict__ wd = const_cast<int*>(I.s.wd);
+    const int e = lb * blockDim.x + threadIdx.x;
+    if (e >= m.T) return;
+    const int a = m.en0[e], b = m.en1[e], c = m.en2[e];
     int f = (mark[a] | mark[b] | mark[c]) ? 1 : 0;
     if (h[a] < 0 && h[b] < 0 && h[c] < 0 && ho[a] < 0 && ho[b] < 0 && ho[c] < 0) f = 2;
     wd[e] = f;
 }
 
 // Dirichlet node values of fe_sw2_init (src/fe/sw2/fe_sw2_init.c:37-85)
-__global__ void k_dirichlet(int n, const int* __restrict__ node, const int* __restrict__ mask,
-                            const double* __restrict__ hv, const double* __restrict__ uv, const double* __restrict__ vv,
-                            double* __restrict__ h, double* __restrict__ u, double* __restrict__ v) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int k = node[t], f = mask[t];
-    if (f & 2) { u[k] = uv[t]; v[k] = vv[t]; }
-    if (f & 1) h[k] = hv[t];
+__global__ void k_dirichlet(const Inst* __restrict__ tab, const LaunchMap mp) {
+    int lb, nb;
+    const Inst& I = tab[map_block(mp, lb, nb)];
+    const int t = lb * blockDim.x + threadIdx.x;
+    if (t >= I.ndir) return;
+    const int k = I.dir_node[t], f = I.dir_mask[t];
+    if (f & 2) {
+        I.s.u[k] = I.dir_u[t];
+        I.s.v[k] = I.dir_v[t];
+    }
+    if (f & 1) I.s.h[k] = I.dir_h[t];
 }
 
 }  // namespace sw2

@@ -6,11 +6,14 @@
 // guess u = M^-1 b'.  M is the 3x3 block-Jacobi inverse (the reference factors
 // OP BLK node blocks exactly; any M that converges gives the same Newton result).
 //
-// One cooperative launch runs the whole iteration: phases are grid-stride loops over
-// node rows separated by a bounded grid barrier; every dot product / norm is a
-// per-block partial reduced by every block in the same fixed order, so all blocks
-// take identical control decisions and reruns are bitwise identical.  s = r - alpha Ap
-// is never stored: the second SpMV forms it on the fly from r and Ap.
+// One cooperative launch runs the whole iteration for every instance of a batch: each
+// instance owns a contiguous range of CTAs with its own bounded barrier.  Its work is cut
+// into a fixed number of virtual CTAs (the grid the instance would get alone); a physical
+// CTA runs virtual CTAs pl, pl + np, ... in turn.  Every dot product / norm is a per-virtual-
+// CTA partial reduced in the same fixed order by every CTA, so all CTAs of an instance take
+// identical control decisions, and an instance's results are bitwise the same alone, in any
+// batch and on reruns.  s = r - alpha Ap is never stored: the second SpMV forms it on the
+// fly from r and Ap.
 // On exit the kernel applies the Newton increment: x = S u, state += x (fe_sw2_inc),
 // sol = -x (fe_newton.c:561-585).
 #pragma once
@@ -26,6 +29,28 @@ constexpr int kRowLanes = 8;                         // lanes per node row in th
 constexpr int kTileRows = kKrylovThreads / kRowLanes;   // node rows per CTA tile (32)
 constexpr int kStages = 3;                           // shared-memory tile ring of the staged sweeps
 
+// Blocks of one launch over a batch: instance ids[j] owns blocks boff[j] .. boff[j+1]-1.
+// Passed by value (kernel parameter space), so lookups are uniform constant-bank reads.
+constexpr int kMaxBatch = 256;
+struct LaunchMap {
+    int n;
+    int boff[kMaxBatch + 1];
+    int ids[kMaxBatch];
+};
+// instance id of this block; lb = block index inside the instance, nb = its block count
+__device__ __forceinline__ int map_block(const LaunchMap& mp, int& lb, int& nb) {
+    const int b = blockIdx.x;
+    int lo = 0, hi = mp.n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (mp.boff[mid] <= b) lo = mid;
+        else hi = mid;
+    }
+    lb = b - mp.boff[lo];
+    nb = mp.boff[lo + 1] - mp.boff[lo];
+    return mp.ids[lo];
+}
+
 struct KrylovCtl {
     unsigned count;       // barrier arrival counter
     unsigned gen;         // barrier generation
@@ -38,14 +63,14 @@ struct KrylovCtl {
 
 // Grid barrier with a bounded spin.  Returns false (and sets ctl->err) if any block
 // gave up; the caller then returns, so the kernel always terminates.
-__device__ __forceinline__ bool grid_sync(KrylovCtl* ctl) {
+__device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned* vgen = &ctl->gen;
         const unsigned g = *vgen;
         __threadfence();
         const unsigned arrived = atomicAdd(&ctl->count, 1u) + 1u;
-        if (arrived == gridDim.x) {
+        if (arrived == nblocks) {
             ctl->count = 0u;
             __threadfence();
             atomicAdd(&ctl->gen, 1u);
@@ -80,12 +105,13 @@ __device__ __forceinline__ double warp_combine(double a, bool is_max) {
 // deterministic all-reduce of up to 4 per-block partials: every block combines the partials
 // of all blocks in the same fixed order (sum or max per slot); red = shared [4][kKrylovWarps]
 template <int NV>
-__device__ __forceinline__ void grid_allreduce(const double* part, const int* is_max, double* out, double* red) {
+__device__ __forceinline__ void grid_allreduce(const double* part, int nparts, const int* is_max, double* out,
+                                               double* red) {
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 #pragma unroll
     for (int q = 0; q < NV; q++) {
         double a = 0.0;
-        for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+        for (int k = threadIdx.x; k < nparts; k += blockDim.x) {
             const double p = __ldcg(part + (size_t)k * 4 + q);
             a = is_max[q] ? fmax(a, p) : a + p;
         }
@@ -103,9 +129,9 @@ __device__ __forceinline__ void grid_allreduce(const double* part, const int* is
     __syncthreads();
 }
 
-// block partials: thread values combined in a fixed order, written by thread 0
+// block partials: thread values combined in a fixed order, written by thread 0 to slot `slot`
 template <int NV>
-__device__ __forceinline__ void block_partial(double* vals, const int* is_max, double* part, double* red) {
+__device__ __forceinline__ void block_partial(double* vals, const int* is_max, double* part, int slot, double* red) {
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
 #pragma unroll
     for (int q = 0; q < NV; q++) {
@@ -120,7 +146,7 @@ __device__ __forceinline__ void block_partial(double* vals, const int* is_max, d
 #pragma unroll
             for (int w = 1; w < kKrylovWarps; w++)
                 a = is_max[q] ? fmax(a, red[q * kKrylovWarps + w]) : a + red[q * kKrylovWarps + w];
-            part[(size_t)blockIdx.x * 4 + q] = a;
+            part[(size_t)slot * 4 + q] = a;
         }
     }
     __syncthreads();
@@ -167,15 +193,30 @@ struct KrylovArgs {
     const int *rowptr, *col;  // off-diagonal block structure of the folded operator M^-1 A'
     const double* S;          // scale vector [3V]
     const double* bs;         // scaled rhs S R [3V]
-    double rtol, atol;
+    double atol;              // absolute Krylov tolerance (the relative one is per launch)
     int maxit;
     double *h, *u, *v;        // state, incremented on exit
     double* sol;              // -x on exit (x itself when apply_inc == 0)
     int apply_inc;            // 1: Newton increment of the state; 0: plain solve
-    double* part;             // [2][grid][4] partials (ping-pong: a slot is rewritten only two reductions later)
+    double* part;             // [2][vgrid][4] partials (ping-pong: a slot is rewritten only two reductions later)
     KrylovCtl* ctl;
-    // staged sweeps: byte offsets inside one stage of the tile's column indices, row pointers
-    // and epilogue vectors (the blocks start at 0); stage stride
+    int vgrid;                // virtual CTAs: the partial structure, fixed per instance
+};
+
+// one instance of a Krylov launch
+struct KrylovInst {
+    KrylovArgs K;
+    const void* A;            // folded off-diagonal blocks, MT
+    const double* Dinv;       // FP64 block-Jacobi inverses (b = M^-1 b' only)
+    double* vec[8];           // b, u, r, q, p, Ap, As, best u
+};
+
+// launch-wide parameters: the map, each mapped instance's relative tolerance and the stage
+// layout of the staged sweeps (byte offsets inside one stage of the tile's column indices,
+// row pointers and epilogue vectors -- the blocks start at 0 -- and the stage stride)
+struct KrylovLaunch {
+    LaunchMap mp;
+    double rtol[kMaxBatch];
     unsigned c_off, r_off, v_off, stage_bytes;
 };
 
@@ -243,7 +284,7 @@ __device__ __forceinline__ unsigned long long hi16(const void* p) { return ((uns
 // completions land on one mbarrier.
 template <typename MT, typename VT>
 __device__ __forceinline__ void issue_tile(int m, int V, const int* rowptr, const int* col, const MT* A, int nvec,
-                                           const VT* const* vecs, unsigned char* stage, const KrylovArgs& K,
+                                           const VT* const* vecs, unsigned char* stage, const KrylovLaunch& K,
                                            unsigned long long* bar, unsigned long long pol) {
     const int r0 = m * kTileRows, nr = min(kTileRows, V - r0);
     const int k0 = __ldg(rowptr + r0), k1 = __ldg(rowptr + r0 + nr);
@@ -310,38 +351,62 @@ __device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke
 
 // MT: matrix storage and SpMV accumulation type; VT: Krylov vector type (FP64 on both paths:
 // FP32 vectors let the recursively updated residual drift away from the true one and the
-// iteration stagnates).  A holds the folded off-diagonal blocks D_i^-1 A'_ij (rowptr / col of
-// K), Dinv the FP64 inverses (used once, for b = M^-1 b').  STAGED: the SpMV sweeps read each
-// tile's blocks, column indices, row pointers and epilogue vectors from a kStages-deep
-// shared-memory ring filled by bulk copies (one thread issues, completion on an mbarrier)
-// kStages - 1 tiles ahead of the rows being computed, so a row's only global loads are its x
-// gathers; the streamed matrix data carry an L2 evict-first hint, which keeps the Krylov
-// vectors in L2.  The dynamic shared memory is kStages * K.stage_bytes.  Otherwise the lanes
-// load everything from global memory.
+// iteration stagnates).  Per instance, A holds the folded off-diagonal blocks D_i^-1 A'_ij
+// (rowptr / col of K) and Dinv the FP64 inverses (used once, for b = M^-1 b').  STAGED: the
+// SpMV sweeps read each tile's blocks, column indices, row pointers and epilogue vectors from
+// a kStages-deep shared-memory ring filled by bulk copies (one thread issues, completion on
+// an mbarrier) kStages - 1 tiles ahead of the rows being computed, so a row's only global
+// loads are its x gathers; the streamed matrix data carry an L2 evict-first hint, which keeps
+// the Krylov vectors in L2.  The dynamic shared memory is kStages * L.stage_bytes.  Otherwise
+// the lanes load everything from global memory.
 template <typename MT, typename VT, bool STAGED>
-__global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, const MT* __restrict__ A,
-                                                               const double* __restrict__ Dinv, VT* __restrict__ b,
-                                                               VT* __restrict__ uu, VT* __restrict__ r,
-                                                               VT* __restrict__ q, VT* __restrict__ p,
-                                                               VT* __restrict__ Ap, VT* __restrict__ As,
-                                                               VT* __restrict__ ubest) {
+__global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const KrylovInst* __restrict__ tab,
+                                                               const __grid_constant__ KrylovLaunch L) {
     __shared__ double red[4 * kKrylovWarps];
     __shared__ unsigned long long bar[kStages];
     extern __shared__ __align__(128) unsigned char stage_mem[];
+    int pl, np;   // this CTA's index among the instance's np CTAs
+    int slot;     // position of the instance in the launch map
+    {
+        const int b = blockIdx.x;
+        int lo = 0, hi = L.mp.n;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (L.mp.boff[mid] <= b) lo = mid;
+            else hi = mid;
+        }
+        slot = lo;
+        pl = b - L.mp.boff[lo];
+        np = L.mp.boff[lo + 1] - L.mp.boff[lo];
+    }
+    const KrylovInst& KI = tab[L.mp.ids[slot]];
+    const KrylovArgs K = KI.K;
+    const MT* __restrict__ A = (const MT*)KI.A;
+    const double* __restrict__ Dinv = KI.Dinv;
+    VT* __restrict__ b = KI.vec[0];
+    VT* __restrict__ uu = KI.vec[1];
+    VT* __restrict__ r = KI.vec[2];
+    VT* __restrict__ q = KI.vec[3];
+    VT* __restrict__ p = KI.vec[4];
+    VT* __restrict__ Ap = KI.vec[5];
+    VT* __restrict__ As = KI.vec[6];
+    VT* __restrict__ ubest = KI.vec[7];
+    const double rtol = L.rtol[slot];
     const int V = K.V;
-    const int stride = gridDim.x * blockDim.x;
-    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int VG = K.vgrid;
+    const int pstride = np * blockDim.x;                  // reduction-free loops: physical CTAs
+    const int pt0 = pl * blockDim.x + threadIdx.x;
     const int lane8 = threadIdx.x % kRowLanes;
     const int li = threadIdx.x / kRowLanes;   // row of the tile this lane group works on
-    const int ntiles = (V + kTileRows - 1) / kTileRows;
+    const int ntiles = (V + kTileRows - 1) / kTileRows;   // >= VG: every virtual CTA has a tile
     const int SUM = 0, MAX = 1;
     KrylovCtl* ctl = K.ctl;
     int nred = 0;      // reductions so far; selects the partial buffer
     unsigned tc = 0;   // tiles consumed by this CTA: stage tc % kStages, mbarrier parity (tc / kStages) & 1
     bool wait_failed = false;
     unsigned long long pol = 0;
-    auto pbuf = [&]() { return K.part + (size_t)(nred & 1) * gridDim.x * 4; };
-    auto stage = [&](unsigned c) { return stage_mem + (c % kStages) * K.stage_bytes; };
+    auto pbuf = [&]() { return K.part + (size_t)(nred & 1) * VG * 4; };
+    auto stage = [&](unsigned c) { return stage_mem + (c % kStages) * L.stage_bytes; };
 
     if (STAGED) {
         if (threadIdx.x == 0) {
@@ -352,80 +417,86 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
         __syncthreads();
     }
 
-    // One SpMV sweep over this CTA's tiles (m = blockIdx.x, blockIdx.x + gridDim.x, ...):
-    // y = sum_j B_ij (xa_j - alpha xb_j) over the off-diagonal blocks of each row; lane 0 of each
-    // row group calls epi(i, y, ev) with ev[v][c] = component c of epilogue vector v at row i
-    // (NV vectors: v0, v1, v2), from which the epilogue forms the diagonal term.
+    // One SpMV sweep: this CTA runs virtual CTAs v = pl, pl + np, ... < VG, each over tiles
+    // m = v, v + VG, ... < ntiles.  y = sum_j B_ij (xa_j - alpha xb_j) over the off-diagonal
+    // blocks of each row; lane 0 of each row group calls epi(i, y, ev) with ev[v][c] =
+    // component c of epilogue vector v at row i (NV vectors: v0, v1, v2), from which the
+    // epilogue forms the diagonal term; fin(v) closes virtual CTA v (its partial).  The
+    // producer cursor (pv, pm) runs kStages - 1 items ahead along the same sequence.
     auto sweep = [&](auto nvc, const VT* xa, const VT* xb, VT alpha, const VT* v0, const VT* v1, const VT* v2,
-                     auto&& epi) {
+                     auto&& epi, auto&& fin) {
         constexpr int NV = decltype(nvc)::value;
         const VT* vecs[3] = {v0, v1, v2};
+        int pv = pl, pm = pl;
+        auto produce = [&](unsigned item) {
+            if (pv >= VG) return;
+            issue_tile<MT, VT>(pm, V, K.rowptr, K.col, A, NV, vecs, stage(item), L, &bar[item % kStages], pol);
+            pm += VG;
+            if (pm >= ntiles) {
+                pv += np;
+                pm = pv;
+            }
+        };
         if (STAGED && threadIdx.x == 0) {
             fence_proxy_async_global();
-            for (int d = 0; d < kStages - 1; d++) {
-                const int m = blockIdx.x + d * gridDim.x;
-                if (m < ntiles)
-                    issue_tile<MT, VT>(m, V, K.rowptr, K.col, A, NV, vecs, stage(tc + d), K,
-                                       &bar[(tc + d) % kStages], pol);
-            }
+            for (int d = 0; d < kStages - 1; d++) produce(tc + d);
         }
-        for (int m = blockIdx.x; m < ntiles; m += gridDim.x) {
-            const int i = m * kTileRows + li;
-            const bool act = i < V;
-            VT y[3];
-            VT ev[NV][3];
-            if (STAGED) {
-                if (threadIdx.x == 0) {
-                    // into the stage of tile tc - 1, released by the __syncthreads that ended it
-                    const int mn = m + (kStages - 1) * gridDim.x;
-                    if (mn < ntiles)
-                        issue_tile<MT, VT>(mn, V, K.rowptr, K.col, A, NV, vecs, stage(tc + kStages - 1), K,
-                                           &bar[(tc + kStages - 1) % kStages], pol);
-                }
-                // a wait that runs out flags the error once; this thread then stops waiting, the
-                // sweep finishes on stale data and the next grid barrier returns
-                if (!wait_failed && !mbar_wait(&bar[tc % kStages], (tc / kStages) & 1u)) {
-                    wait_failed = true;
-                    atomicExch(&ctl->err, 1);
-                }
-                const unsigned char* st = stage(tc);
-                const int* sR = (const int*)(st + K.r_off);
-                const int k0 = sR[0];
-                const MT* sA = (const MT*)(st + ((unsigned long long)(A + (size_t)k0 * 9) & 15ull));
-                const int* sC = (const int*)(st + K.c_off + ((unsigned long long)(K.col + k0) & 15ull));
-                const VT* sV = (const VT*)(st + K.v_off);
-                const int kb = act ? sR[li] : 0, ke = act ? sR[li + 1] : 0;
-                row_apply<MT, VT>(
-                    act, lane8, kb, ke, [&](int k) { return sA + (size_t)(k - k0) * 9; },
-                    [&](int k) { return sC[k - k0]; }, xa, xb, alpha, y);
-                if (act && lane8 == 0) {
+        for (int v = pl; v < VG; v += np) {
+            for (int m = v; m < ntiles; m += VG) {
+                const int i = m * kTileRows + li;
+                const bool act = i < V;
+                VT y[3];
+                VT ev[NV][3];
+                if (STAGED) {
+                    // into the stage of item tc - 1, released by the __syncthreads that ended it
+                    if (threadIdx.x == 0) produce(tc + kStages - 1);
+                    // a wait that runs out flags the error once; this thread then stops waiting,
+                    // the sweep finishes on stale data and the next barrier returns
+                    if (!wait_failed && !mbar_wait(&bar[tc % kStages], (tc / kStages) & 1u)) {
+                        wait_failed = true;
+                        atomicExch(&ctl->err, 1);
+                    }
+                    const unsigned char* st = stage(tc);
+                    const int* sR = (const int*)(st + L.r_off);
+                    const int k0 = sR[0];
+                    const MT* sA = (const MT*)(st + ((unsigned long long)(A + (size_t)k0 * 9) & 15ull));
+                    const int* sC = (const int*)(st + L.c_off + ((unsigned long long)(K.col + k0) & 15ull));
+                    const VT* sV = (const VT*)(st + L.v_off);
+                    const int kb = act ? sR[li] : 0, ke = act ? sR[li + 1] : 0;
+                    row_apply<MT, VT>(
+                        act, lane8, kb, ke, [&](int k) { return sA + (size_t)(k - k0) * 9; },
+                        [&](int k) { return sC[k - k0]; }, xa, xb, alpha, y);
+                    if (act && lane8 == 0) {
 #pragma unroll
-                    for (int v = 0; v < NV; v++)
+                        for (int w = 0; w < NV; w++)
 #pragma unroll
-                        for (int c = 0; c < 3; c++) ev[v][c] = sV[v * (tile_vec_bytes<VT>() / sizeof(VT)) + 3 * li + c];
+                            for (int c = 0; c < 3; c++)
+                                ev[w][c] = sV[w * (tile_vec_bytes<VT>() / sizeof(VT)) + 3 * li + c];
+                    }
+                } else {
+                    if (act && lane8 == 0) {   // issued ahead of the row's gathers
+#pragma unroll
+                        for (int w = 0; w < NV; w++)
+#pragma unroll
+                            for (int c = 0; c < 3; c++) ev[w][c] = ldv(vecs[w] + 3 * i + c);
+                    }
+                    const int kb = act ? __ldg(K.rowptr + i) : 0, ke = act ? __ldg(K.rowptr + i + 1) : 0;
+                    row_apply<MT, VT>(
+                        act, lane8, kb, ke, [&](int k) { return A + (size_t)k * 9; },
+                        [&](int k) { return __ldg(K.col + k); }, xa, xb, alpha, y);
                 }
-            } else {
-                if (act && lane8 == 0) {   // issued ahead of the row's gathers
-#pragma unroll
-                    for (int v = 0; v < NV; v++)
-#pragma unroll
-                        for (int c = 0; c < 3; c++) ev[v][c] = ldv(vecs[v] + 3 * i + c);
+                if (act && lane8 == 0) epi(i, y, ev);
+                if (STAGED) {
+                    __syncthreads();
+                    tc++;
                 }
-                const int kb = act ? __ldg(K.rowptr + i) : 0, ke = act ? __ldg(K.rowptr + i + 1) : 0;
-                row_apply<MT, VT>(
-                    act, lane8, kb, ke, [&](int k) { return A + (size_t)k * 9; },
-                    [&](int k) { return __ldg(K.col + k); }, xa, xb, alpha, y);
             }
-            if (act && lane8 == 0) epi(i, y, ev);
-            if (STAGED) {
-                __syncthreads();
-                tc++;
-            }
+            fin(v);
         }
     };
 
     // b <- M^-1 b'
-    for (int i = t0; i < V; i += stride) {
+    for (int i = pt0; i < V; i += pstride) {
         const double* d = Dinv + (size_t)i * 9;
         const double b0 = K.bs[3 * i], b1 = K.bs[3 * i + 1], b2 = K.bs[3 * i + 2];
 #pragma unroll
@@ -435,35 +506,40 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
             uu[3 * i + c] = y;
         }
     }
-    if (!grid_sync(ctl)) return;
+    if (!grid_sync(ctl, np)) return;
     // r = b - M^-1 A u, q = r, p = r; norms and rho
     {
         double vals[4] = {0, 0, 0, 0};
         const int ism[4] = {MAX, MAX, SUM, SUM};
-        sweep(IntC<2>{}, uu, (const VT*)nullptr, (VT)0, b, uu, nullptr, [&](int i, const VT* y, const VT (*ev)[3]) {
+        sweep(
+            IntC<2>{}, uu, (const VT*)nullptr, (VT)0, b, uu, nullptr,
+            [&](int i, const VT* y, const VT(*ev)[3]) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const VT bb = ev[0][c];
-                const VT rr = bb - (ev[1][c] + y[c]);
-                r[3 * i + c] = rr;
-                q[3 * i + c] = rr;
-                p[3 * i + c] = rr;
-                Ap[3 * i + c] = 0;
-                vals[0] = fmax(vals[0], fabs((double)rr));
-                vals[1] = fmax(vals[1], fabs((double)bb));
-                vals[2] += (double)rr * (double)rr;
-            }
-        });
-        block_partial<4>(vals, ism, pbuf(), red);
-        if (!grid_sync(ctl)) return;
+                for (int c = 0; c < 3; c++) {
+                    const VT bb = ev[0][c];
+                    const VT rr = bb - (ev[1][c] + y[c]);
+                    r[3 * i + c] = rr;
+                    q[3 * i + c] = rr;
+                    p[3 * i + c] = rr;
+                    Ap[3 * i + c] = 0;
+                    vals[0] = fmax(vals[0], fabs((double)rr));
+                    vals[1] = fmax(vals[1], fabs((double)bb));
+                    vals[2] += (double)rr * (double)rr;
+                }
+            },
+            [&](int v) {
+                block_partial<4>(vals, ism, pbuf(), v, red);
+                vals[0] = vals[1] = vals[2] = vals[3] = 0.0;
+            });
+        if (!grid_sync(ctl, np)) return;
         double rd[4];
-        grid_allreduce<4>(pbuf(), ism, rd, red);
+        grid_allreduce<4>(pbuf(), VG, ism, rd, red);
         nred++;
         double rnorm = rd[0];
         const double bnorm = rd[1];
         double rho = rd[2], rhop = 1.0, alpha = 1.0, omega = 1.0;
         int it = 0;
-        const double tol = K.atol + bnorm * K.rtol;
+        const double tol = K.atol + bnorm * rtol;
         // best iterate so far: past its attainable accuracy BiCGSTAB's residual drifts back up,
         // so on stagnation (no new best for kStall iterations) or at max_lin_it the best one is
         // used.  It is saved lazily: when an iteration sets a new best (`pending`), the next
@@ -477,18 +553,22 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
             {
                 double g[4] = {0, 0, 0, 0};
                 const int gm[4] = {SUM, SUM, SUM, SUM};
-                sweep(IntC<2>{}, p, (const VT*)nullptr, (VT)0, q, p, nullptr,
-                      [&](int i, const VT* y, const VT (*ev)[3]) {
+                sweep(
+                    IntC<2>{}, p, (const VT*)nullptr, (VT)0, q, p, nullptr,
+                    [&](int i, const VT* y, const VT(*ev)[3]) {
 #pragma unroll
-                          for (int c = 0; c < 3; c++) {
-                              const VT apc = ev[1][c] + y[c];
-                              Ap[3 * i + c] = apc;
-                              g[0] += (double)ev[0][c] * (double)apc;
-                          }
-                      });
-                block_partial<1>(g, gm, pbuf(), red);
-                if (!grid_sync(ctl)) return;
-                grid_allreduce<1>(pbuf(), gm, g, red);
+                        for (int c = 0; c < 3; c++) {
+                            const VT apc = ev[1][c] + y[c];
+                            Ap[3 * i + c] = apc;
+                            g[0] += (double)ev[0][c] * (double)apc;
+                        }
+                    },
+                    [&](int v) {
+                        block_partial<1>(g, gm, pbuf(), v, red);
+                        g[0] = 0.0;
+                    });
+                if (!grid_sync(ctl, np)) return;
+                grid_allreduce<1>(pbuf(), VG, gm, g, red);
                 nred++;
                 alpha = rho / g[0];
             }
@@ -497,51 +577,60 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
                 double w[4] = {0, 0, 0, 0};
                 const int wm[4] = {SUM, SUM, SUM, SUM};
                 const VT al = (VT)alpha;
-                sweep(IntC<3>{}, r, Ap, al, r, Ap, q, [&](int i, const VT* y, const VT (*ev)[3]) {
+                sweep(
+                    IntC<3>{}, r, Ap, al, r, Ap, q,
+                    [&](int i, const VT* y, const VT(*ev)[3]) {
 #pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        const VT s = ev[0][c] - al * ev[1][c];
-                        const VT asc = s + y[c];
-                        As[3 * i + c] = asc;
-                        w[0] += (double)asc * (double)s;
-                        w[1] += (double)asc * (double)asc;
-                        w[2] += (double)asc * (double)ev[2][c];
-                    }
-                });
-                block_partial<3>(w, wm, pbuf(), red);
-                if (!grid_sync(ctl)) return;
-                grid_allreduce<3>(pbuf(), wm, w, red);
+                        for (int c = 0; c < 3; c++) {
+                            const VT s = ev[0][c] - al * ev[1][c];
+                            const VT asc = s + y[c];
+                            As[3 * i + c] = asc;
+                            w[0] += (double)asc * (double)s;
+                            w[1] += (double)asc * (double)asc;
+                            w[2] += (double)asc * (double)ev[2][c];
+                        }
+                    },
+                    [&](int v) {
+                        block_partial<3>(w, wm, pbuf(), v, red);
+                        w[0] = w[1] = w[2] = 0.0;
+                    });
+                if (!grid_sync(ctl, np)) return;
+                grid_allreduce<3>(pbuf(), VG, wm, w, red);
                 nred++;
                 omega = w[0] / w[1];
                 rhop = rho;
                 rho = -1.0 * omega * w[2];
             }
-    // (h)-(i) and the next search direction (c): u += alpha p + omega s; r = s - omega As;
+            // (h)-(i) and the next search direction (c): u += alpha p + omega s; r = s - omega As;
             // p = beta (p - omega Ap) + r with beta = (rho alpha) / (rhop omega)
             {
                 double mx[4] = {0, 0, 0, 0};
                 const int mm[4] = {MAX, MAX, MAX, MAX};
                 const double beta = (rho * alpha) / (rhop * omega);
                 const VT al = (VT)alpha, om = (VT)omega, be = (VT)beta;
-                for (int k = t0; k < 3 * V; k += stride) {   // element-wise: every load coalesced
-                    const VT apk = ldv(Ap + k), pk = ldv(p + k);
-                    const VT s = ldv(r + k) - al * apk;
-                    VT uk = ldv(uu + k);
-                    if (pending) ubest[k] = uk;
-                    uk += al * pk;
-                    uk += om * s;
-                    uu[k] = uk;
-                    const VT rk = s - om * ldv(As + k);
-                    r[k] = rk;
-                    p[k] = (pk - om * apk) * be + rk;
-                    mx[0] = fmax(mx[0], fabs((double)rk));
+                for (int v = pl; v < VG; v += np) {
+                    // element-wise (every load coalesced), virtual CTA v's share
+                    for (int k = v * blockDim.x + threadIdx.x; k < 3 * V; k += VG * blockDim.x) {
+                        const VT apk = ldv(Ap + k), pk = ldv(p + k);
+                        const VT s = ldv(r + k) - al * apk;
+                        VT uk = ldv(uu + k);
+                        if (pending) ubest[k] = uk;
+                        uk += al * pk;
+                        uk += om * s;
+                        uu[k] = uk;
+                        const VT rk = s - om * ldv(As + k);
+                        r[k] = rk;
+                        p[k] = (pk - om * apk) * be + rk;
+                        mx[0] = fmax(mx[0], fabs((double)rk));
+                    }
+                    block_partial<1>(mx, mm, pbuf(), v, red);
+                    mx[0] = 0.0;
                 }
-                block_partial<1>(mx, mm, pbuf(), red);
-                if (!grid_sync(ctl)) return;
-                grid_allreduce<1>(pbuf(), mm, mx, red);
+                if (!grid_sync(ctl, np)) return;
+                grid_allreduce<1>(pbuf(), VG, mm, mx, red);
                 nred++;
                 rnorm = mx[0];
-                pending = rnorm < best;   // identical decision in every block
+                pending = rnorm < best;   // identical decision in every CTA of the instance
                 if (pending) {
                     best = rnorm;
                     best_it = it;
@@ -552,7 +641,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
         // x = S u; state += x; sol = -x.  Without convergence the best iterate is u itself when
         // the last iteration set it (not saved yet), else ubest.
         const VT* ux = (conv || pending) ? uu : ubest;
-        for (int i = t0; i < V; i += stride) {
+        for (int i = pt0; i < V; i += pstride) {
             const double x0 = (double)ldv(ux + 3 * i) * K.S[3 * i];
             const double x1 = (double)ldv(ux + 3 * i + 1) * K.S[3 * i + 1];
             const double x2 = (double)ldv(ux + 3 * i + 2) * K.S[3 * i + 2];
@@ -569,7 +658,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(KrylovArgs K, co
                 K.sol[3 * i + 2] = x2;
             }
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (pl == 0 && threadIdx.x == 0) {
             ctl->iterations = it;
             ctl->converged = conv ? 1 : 0;
             ctl->rnorm = conv ? rnorm : best;

@@ -68,6 +68,8 @@ struct DBuf {
 // lets other translation units of this library report through sw2gpu_last_error()
 __attribute__((visibility("hidden"))) void sw2gpu_internal_set_error(const char* msg) { g_err = msg; }
 
+struct Runner;
+
 struct sw2gpu_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -94,7 +96,7 @@ struct sw2gpu_ctx {
     DBuf<int> wd;
     DBuf<unsigned char> ewet;    // element takes the fully wet Jacobian path
     DBuf<int> glist, gcount;     // elements on the general (wet/dry) Jacobian path
-    int ngeneral = 0;
+    int ngeneral = 0;            // its length at the last residual evaluation
     // work
     DBuf<double> sc, sx, sy, R, sol, jslots, val, S_, bs;
     // Krylov operator: block-Jacobi inverse folded into the off-diagonal blocks
@@ -105,33 +107,14 @@ struct sw2gpu_ctx {
     DBuf<float> aoff32;
     DBuf<double> kv64[8];
     DBuf<double> part;
-    DBuf<KrylovCtl> ctl;
-    DBuf<Norms> npart, norms;
+    DBuf<Norms> npart;
     DBuf<unsigned> ncounter;
-    DBuf<int> singular;
-    Norms* norms_h = nullptr;
-    KrylovCtl* ctl_h = nullptr;
-    int krylov_grid = 0;
-    bool staged = false;            // Krylov sweeps read matrix tiles through the shared-memory ring
-    unsigned c_off = 0, r_off = 0, v_off = 0, stage_bytes = 0;
-    size_t krylov_smem = 0;         // dynamic shared memory of the Krylov launch
-    int launches = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // per-phase device timing: event pairs recorded around the main kernels of a step
-    static constexpr int kMaxPhases = 512;
-    std::vector<cudaEvent_t> pev;
-    std::vector<int> pkind;
-    int nphase = 0;
+    int krylov_grid = 0;            // virtual CTAs of the Krylov solve (its partial structure)
+    unsigned a_cap = 0, c_cap = 0;  // largest tile block / column-index ranges (staged sweeps)
     DevMesh dm{};
+    std::unique_ptr<Runner> self;   // runs this instance alone
 
-    ~sw2gpu_ctx() {
-        for (auto e : pev) cudaEventDestroy(e);
-        if (norms_h) cudaFreeHost(norms_h);
-        if (ctl_h) cudaFreeHost(ctl_h);
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        if (own_stream && stream) cudaStreamDestroy(stream);
-    }
+    ~sw2gpu_ctx();
     double* H(int l) { return hs[lv[l]].p; }
     double* U(int l) { return us[lv[l]].p; }
     double* Vv(int l) { return vs[lv[l]].p; }
@@ -159,19 +142,91 @@ namespace {
 
 enum PhaseKind { kPhJac = 0, kPhKrylov = 1, kPhResid = 2 };
 
+#ifndef SW2_MAX_STAGED_SMEM
+#define SW2_MAX_STAGED_SMEM (96 * 1024)   // dynamic shared memory allowed for the tile ring
+#endif
+constexpr size_t kMaxStagedSmem = SW2_MAX_STAGED_SMEM;
+
+// bytes per stage of the staged Krylov sweeps: the largest 16-byte-rounded block range and
+// column-index range of any tile of kTileRows rows, for matrix elements of esz bytes
+void stage_caps(const std::vector<int>& rp, int V, size_t esz, unsigned& a_cap, unsigned& c_cap) {
+    size_t am = 16, cm = 16;
+    for (int r0 = 0; r0 < V; r0 += kTileRows) {
+        const size_t k0 = (size_t)rp[r0], k1 = (size_t)rp[std::min(r0 + kTileRows, V)];
+        am = std::max(am, ((k1 * 9 * esz + 15) & ~size_t(15)) - ((k0 * 9 * esz) & ~size_t(15)));
+        cm = std::max(cm, ((k1 * 4 + 15) & ~size_t(15)) - ((k0 * 4) & ~size_t(15)));
+    }
+    a_cap = (unsigned)am;
+    c_cap = (unsigned)cm;
+}
+
+template <typename MT>
+void* krylov_kernel(bool staged) {
+    return staged ? (void*)k_bicgstab<MT, double, true> : (void*)k_bicgstab<MT, double, false>;
+}
+
+}  // namespace
+
+// A batch of instances stepped together: device tables of the instances, per-instance
+// results (norms, Krylov control words), the Krylov launch configuration and the phase
+// timers.  Every kernel launch covers a subset of the instances through a LaunchMap.
+struct Runner {
+    cudaStream_t stream = nullptr;
+    std::vector<sw2gpu_ctx*> ctx;
+    bool mixed = false;
+    DBuf<Inst> tab;
+    DBuf<KrylovInst> ktab;
+    std::vector<Inst> tab_h;
+    std::vector<KrylovInst> ktab_h;
+    DBuf<Norms> norms;
+    DBuf<KrylovCtl> ctl;
+    DBuf<int> singular;
+    Norms* norms_h = nullptr;     // pinned mirrors, one entry per instance
+    KrylovCtl* ctl_h = nullptr;
+    bool staged = false;
+    unsigned c_off = 0, r_off = 0, v_off = 0, stage_bytes = 0;
+    size_t smem = 0;
+    int capacity = 0;             // co-resident Krylov CTAs
+    int launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    static constexpr int kMaxPhases = 512;
+    std::vector<cudaEvent_t> pev;
+    std::vector<int> pkind;
+    int nphase = 0;
+    ~Runner() {
+        for (auto e : pev) cudaEventDestroy(e);
+        if (norms_h) cudaFreeHost(norms_h);
+        if (ctl_h) cudaFreeHost(ctl_h);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+sw2gpu_ctx::~sw2gpu_ctx() {
+    self.reset();
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+struct sw2gpu_batch {
+    std::unique_ptr<Runner> run;
+    bool own_stream = false;
+};
+
+namespace {
+
 // phase timer: brackets launches with an event pair when the pool has room
 struct Phase {
-    sw2gpu_ctx* c;
+    Runner* r;
     int slot;
-    Phase(sw2gpu_ctx* ctx, int kind) : c(ctx), slot(-1) {
-        if (c->nphase < sw2gpu_ctx::kMaxPhases && !c->pev.empty()) {
-            slot = c->nphase++;
-            c->pkind[slot] = kind;
-            cudaEventRecord(c->pev[2 * slot], c->stream);
+    Phase(Runner* rr, int kind) : r(rr), slot(-1) {
+        if (r->nphase < Runner::kMaxPhases && !r->pev.empty()) {
+            slot = r->nphase++;
+            r->pkind[slot] = kind;
+            cudaEventRecord(r->pev[2 * slot], r->stream);
         }
     }
     ~Phase() {
-        if (slot >= 0) cudaEventRecord(c->pev[2 * slot + 1], c->stream);
+        if (slot >= 0) cudaEventRecord(r->pev[2 * slot + 1], r->stream);
     }
 };
 
@@ -191,13 +246,13 @@ int zalloc(DBuf<T>& b, size_t n, cudaStream_t st) {
 inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
 // per-step tables: string values (edge series), material water sources, Dirichlet values
-int upload_step_tables(sw2gpu_ctx* c, const double* series) {
+int upload_step_tables(sw2gpu_ctx* c, const double* series, cudaStream_t st) {
     std::vector<double> sv(std::max(c->S, 1), 0.0);
     for (int s = 0; s < c->S; s++) {
         int k = c->str_isigma[s];
         if (k >= 0 && k < c->NS && series) sv[s] = series[k];
     }
-    CK(cudaMemcpyAsync(c->str_value.p, sv.data(), sizeof(double) * c->S, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->str_value.p, sv.data(), sizeof(double) * c->S, cudaMemcpyHostToDevice, st));
     bool any_src = false;
     for (int m = 0; m < c->M; m++) {
         if (c->mats_h[m].has_source) {
@@ -207,7 +262,7 @@ int upload_step_tables(sw2gpu_ctx* c, const double* series) {
         }
     }
     if (any_src)
-        CK(cudaMemcpyAsync(c->mats.p, c->mats_h.data(), sizeof(MatParams) * c->M, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->mats.p, c->mats_h.data(), sizeof(MatParams) * c->M, cudaMemcpyHostToDevice, st));
     const int nd = (int)c->dir_node.size();
     if (nd) {
         std::vector<double> h(nd, 0.0), u(nd, 0.0), v(nd, 0.0);
@@ -218,155 +273,404 @@ int upload_step_tables(sw2gpu_ctx* c, const double* series) {
             v[i] = get(c->str_ivy[s]);
             h[i] = get(c->str_iu0[s]);
         }
-        CK(cudaMemcpyAsync(c->dir_h.p, h.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->dir_u.p, u.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->dir_v.p, v.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->dir_h.p, h.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->dir_u.p, u.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->dir_v.p, v.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, st));
     }
+    // the host copy of the step tables is pageable: finish before it changes
+    CK(cudaStreamSynchronize(st));
     return 0;
+}
+
+// ---- runner ------------------------------------------------------------------------
+
+int runner_init(Runner& R, const std::vector<sw2gpu_ctx*>& ctx, cudaStream_t stream) {
+    if (ctx.empty() || (int)ctx.size() > kMaxBatch) return fail(SW2GPU_E_ARG, "batch of %zu instances (1..%d)", ctx.size(), kMaxBatch);
+    R.ctx = ctx;
+    R.stream = stream;
+    R.mixed = ctx[0]->p.precision == SW2GPU_MIXED;
+    for (auto* c : ctx)
+        if ((c->p.precision == SW2GPU_MIXED) != R.mixed) return fail(SW2GPU_E_ARG, "a batch has one precision");
+    const int K = (int)ctx.size();
+    if (R.tab.alloc(K) || R.ktab.alloc(K) || R.norms.alloc(K) || R.ctl.alloc(K) || R.singular.alloc(K))
+        return fail(SW2GPU_E_NOMEM, "batch tables");
+    CK(cudaMemsetAsync(R.norms.p, 0, sizeof(Norms) * K, stream));
+    CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * K, stream));
+    CK(cudaMallocHost(&R.norms_h, sizeof(Norms) * K));
+    CK(cudaMallocHost(&R.ctl_h, sizeof(KrylovCtl) * K));
+    R.tab_h.resize(K);
+    R.ktab_h.resize(K);
+    // Krylov launch: stage layout for the largest tile of any instance
+    unsigned a_cap = 16, c_cap = 16;
+    for (auto* c : ctx) {
+        a_cap = std::max(a_cap, c->a_cap);
+        c_cap = std::max(c_cap, c->c_cap);
+    }
+    const unsigned c_off = a_cap, r_off = c_off + c_cap;
+    const unsigned v_off = r_off + ((unsigned)(kTileRows + 1) * 4u + 15u) / 16u * 16u;
+    const unsigned stage = (v_off + 3u * tile_vec_bytes<double>() + 127u) & ~127u;
+    R.staged = (size_t)kStages * stage <= kMaxStagedSmem;
+    if (R.staged) {
+        R.c_off = c_off;
+        R.r_off = r_off;
+        R.v_off = v_off;
+        R.stage_bytes = stage;
+    }
+    R.smem = (size_t)kStages * R.stage_bytes;
+    int dev = 0, sms = 0, per_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    void* kern = R.mixed ? krylov_kernel<float>(R.staged) : krylov_kernel<double>(R.staged);
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R.smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kKrylovThreads, R.smem));
+    R.capacity = sms * std::max(1, std::min(per_sm, 4));
+    CK(cudaEventCreate(&R.ev0));
+    CK(cudaEventCreate(&R.ev1));
+    R.pev.resize(2 * Runner::kMaxPhases);
+    R.pkind.resize(Runner::kMaxPhases);
+    for (auto& e : R.pev) CK(cudaEventCreate(&e));
+    return 0;
+}
+
+// device tables from the instances' current buffers and state levels
+int runner_tables(Runner& R, int apply_inc) {
+    const int K = (int)R.ctx.size();
+    for (int k = 0; k < K; k++) {
+        sw2gpu_ctx* c = R.ctx[k];
+        Inst& I = R.tab_h[k];
+        I.m = c->dm;
+        I.s = c->state();
+        I.P = c->phys();
+        I.sc = c->sc.p; I.sx = c->sx.p; I.sy = c->sy.p;
+        I.R = c->R.p; I.sol = c->sol.p; I.jslots = c->jslots.p; I.val = c->val.p;
+        I.S = c->S_.p; I.bs = c->bs.p; I.dinv = c->dinv64.p;
+        I.aoff = R.mixed ? (void*)c->aoff32.p : (void*)c->aoff64.p;
+        I.ewet = c->ewet.p; I.mark = c->mark.p; I.glist = c->glist.p; I.gcount = c->gcount.p;
+        I.npart = c->npart.p; I.norms = R.norms.p + k; I.ncounter = c->ncounter.p; I.singular = R.singular.p + k;
+        I.ndir = (int)c->dir_node.size();
+        I.dir_node = c->dir_node_d.p; I.dir_mask = c->dir_mask_d.p;
+        I.dir_h = c->dir_h.p; I.dir_u = c->dir_u.p; I.dir_v = c->dir_v.p;
+        KrylovInst& Q = R.ktab_h[k];
+        KrylovArgs& A = Q.K;
+        A.V = c->V;
+        A.rowptr = c->orowptr.p;
+        A.col = c->ocol.p;
+        A.S = c->S_.p;
+        A.bs = c->bs.p;
+        A.atol = c->p.lin_atol;
+        A.maxit = c->p.max_lin_it;
+        A.h = c->H(0); A.u = c->U(0); A.v = c->Vv(0);
+        A.sol = c->sol.p;
+        A.apply_inc = apply_inc;
+        A.part = c->part.p;
+        A.ctl = R.ctl.p + k;
+        A.vgrid = c->krylov_grid;
+        Q.A = I.aoff;
+        Q.Dinv = c->dinv64.p;
+        for (int v = 0; v < 8; v++) Q.vec[v] = c->kv64[v].p;
+    }
+    CK(cudaMemcpyAsync(R.tab.p, R.tab_h.data(), sizeof(Inst) * K, cudaMemcpyHostToDevice, R.stream));
+    CK(cudaMemcpyAsync(R.ktab.p, R.ktab_h.data(), sizeof(KrylovInst) * K, cudaMemcpyHostToDevice, R.stream));
+    // pageable source: complete before the host tables change again
+    CK(cudaStreamSynchronize(R.stream));
+    return 0;
+}
+
+// map of a subset: instance k gets blocks(k) blocks (none: left out); returns the block total
+template <class F>
+int make_map(LaunchMap& mp, const std::vector<int>& subset, F blocks) {
+    int off = 0;
+    mp.n = 0;
+    for (int k : subset) {
+        const int nb = blocks(k);
+        if (nb <= 0) continue;
+        mp.boff[mp.n] = off;
+        mp.ids[mp.n] = k;
+        off += nb;
+        mp.n++;
+    }
+    mp.boff[mp.n] = off;
+    return off;
+}
+
+// one launch of kernel `kern` (tab, map) over the subset, `threads` per block
+template <class F, class... Args>
+int launch_map(Runner& R, const std::vector<int>& subset, int threads, F blocks,
+               void (*kern)(const Inst*, const LaunchMap, Args...), Args... args) {
+    LaunchMap mp;
+    const int nb = make_map(mp, subset, blocks);
+    if (nb == 0) return 0;
+    kern<<<nb, threads, 0, R.stream>>>(R.tab.p, mp, args...);
+    R.launches++;
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int launch_init(Runner& R, const std::vector<int>& sub) {     // fe_sw2_init
+    int rc = 0;
+    auto C = [&](int k) { return R.ctx[k]; };
+    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, k_init_level))) return rc;
+    if ((rc = launch_map(R, sub, 128, [&](int k) { return nblk((int)C(k)->dir_node.size(), 128); }, k_dirichlet)))
+        return rc;
+    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->T, 256); }, k_wd_mark))) return rc;
+    return launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->T, 256); }, k_wd_flag);
 }
 
 // residual at the current state: element slots, reference-order gather, norms (async)
-int launch_resid(sw2gpu_ctx* c) {
-    State s = c->state();
-    PhysParams P = c->phys();
-    const int n = c->T + c->E;
-    Phase ph(c, kPhResid);
-    CK(cudaMemsetAsync(c->gcount.p, 0, sizeof(int), c->stream));
-    k_resid_elem<<<nblk(std::max(n, 1), 128), 128, 0, c->stream>>>(c->dm, s, P, c->sc.p, c->sx.p, c->sy.p,
-                                                                   c->ewet.p, c->glist.p, c->gcount.p);
-    k_resid_gather<<<nblk(std::max(c->V, 1), kGatherThreads), kGatherThreads, 0, c->stream>>>(
-        c->dm, s, c->sc.p, c->sx.p, c->sy.p, c->R.p, c->sol.p, c->npart.p, c->ncounter.p, c->norms.p, c->gcount.p);
-    c->launches += 2;
-    CK(cudaGetLastError());
+int launch_resid(Runner& R, const std::vector<int>& sub) {
+    Phase ph(&R, kPhResid);
+    int rc = launch_map(R, sub, 128, [&](int k) { return nblk(R.ctx[k]->T + R.ctx[k]->E, 128); }, k_resid_elem);
+    if (rc) return rc;
+    return launch_map(R, sub, kGatherThreads, [&](int k) { return nblk(R.ctx[k]->V, kGatherThreads); },
+                      k_resid_gather);
+}
+
+// norms (and Krylov control words) of every instance; the one host sync of an evaluation
+int read_results(Runner& R) {
+    const int K = (int)R.ctx.size();
+    CK(cudaMemcpyAsync(R.norms_h, R.norms.p, sizeof(Norms) * K, cudaMemcpyDeviceToHost, R.stream));
+    CK(cudaMemcpyAsync(R.ctl_h, R.ctl.p, sizeof(KrylovCtl) * K, cudaMemcpyDeviceToHost, R.stream));
+    CK(cudaStreamSynchronize(R.stream));
+    for (int k = 0; k < K; k++) R.ctx[k]->ngeneral = R.norms_h[k].ngeneral;
     return 0;
 }
 
-int read_norms(sw2gpu_ctx* c, Norms& out) {
-    CK(cudaMemcpyAsync(c->norms_h, c->norms.p, sizeof(Norms), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    out = *c->norms_h;
-    c->ngeneral = out.ngeneral;
+int launch_jacobian(Runner& R, const std::vector<int>& sub) {
+    Phase ph(&R, kPhJac);
+    auto C = [&](int k) { return R.ctx[k]; };
+    // the general list and the wet flags come from the residual evaluated at this same state
+    int rc = launch_map(R, sub, kJacThreads, [&](int k) { return nblk(C(k)->T, kJacElems); }, k_jac_elem_wet);
+    if (rc) return rc;
+    if ((rc = launch_map(R, sub, kJacThreads, [&](int k) { return nblk(C(k)->ngeneral, kJacElems); },
+                         k_jac_elem_general)))
+        return rc;
+    if ((rc = launch_map(R, sub, 128, [&](int k) { return nblk(6LL * C(k)->E, 128); }, k_jac_edge))) return rc;
+    return launch_map(R, sub, 256, [&](int k) { return nblk(9LL * C(k)->nnzb, 256); }, k_jac_gather);
+}
+
+// Krylov CTAs per instance: shares of the co-resident capacity by block count, at least one,
+// at most the instance's virtual CTAs
+std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub) {
+    double wsum = 0.0;
+    for (int k : sub) wsum += (double)R.ctx[k]->nnzb;
+    std::vector<int> P(sub.size());
+    long long tot = 0;
+    for (size_t j = 0; j < sub.size(); j++) {
+        const sw2gpu_ctx* c = R.ctx[sub[j]];
+        const int want = (int)std::floor(R.capacity * (double)c->nnzb / std::max(wsum, 1.0));
+        P[j] = std::max(1, std::min(c->krylov_grid, want));
+        tot += P[j];
+    }
+    while (tot > R.capacity) {   // trim the largest shares
+        size_t jm = 0;
+        for (size_t j = 1; j < P.size(); j++)
+            if (P[j] > P[jm]) jm = j;
+        if (P[jm] <= 1) break;
+        P[jm]--;
+        tot--;
+    }
+    return P;
+}
+
+// scaling, preconditioner folding and the persistent BiCGSTAB of the subset, each instance
+// with its own relative tolerance eta[k]
+int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<double>& eta, int fix_only_unused = 0) {
+    (void)fix_only_unused;
+    auto C = [&](int k) { return R.ctx[k]; };
+    int rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, k_rowscale, 0);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(R.singular.p, 0, sizeof(int) * R.ctx.size(), R.stream));
+    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, k_fold_diag))) return rc;
+    if (R.mixed)
+        rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->nnzb, 256); }, k_fold_offdiag<float>);
+    else
+        rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->nnzb, 256); }, k_fold_offdiag<double>);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * R.ctx.size(), R.stream));
+    Phase ph(&R, kPhKrylov);
+    // instances that cannot all be co-resident go in successive launches
+    size_t j0 = 0;
+    while (j0 < sub.size()) {
+        std::vector<int> grp;
+        for (size_t j = j0; j < sub.size() && (int)grp.size() < R.capacity; j++) grp.push_back(sub[j]);
+        j0 += grp.size();
+        const std::vector<int> P = krylov_shares(R, grp);
+        static thread_local KrylovLaunch L;   // ~4 KB: not on the stack of every caller
+        int off = 0;
+        L.mp.n = (int)grp.size();
+        for (size_t j = 0; j < grp.size(); j++) {
+            L.mp.boff[j] = off;
+            L.mp.ids[j] = grp[j];
+            L.rtol[j] = eta[grp[j]];
+            off += P[j];
+        }
+        L.mp.boff[grp.size()] = off;
+        L.c_off = R.c_off;
+        L.r_off = R.r_off;
+        L.v_off = R.v_off;
+        L.stage_bytes = R.stage_bytes;
+        const KrylovInst* tab = R.ktab.p;
+        void* args[] = {(void*)&tab, (void*)&L};
+        void* kern = R.mixed ? krylov_kernel<float>(R.staged) : krylov_kernel<double>(R.staged);
+        CK(cudaLaunchCooperativeKernel(kern, dim3(off), dim3(kKrylovThreads), args, R.smem, R.stream));
+        R.launches++;
+    }
     return 0;
 }
 
-int launch_jacobian(sw2gpu_ctx* c) {
-    State s = c->state();
-    PhysParams P = c->phys();
-    if (c->T) {
-        // the list and the wet flags come from the residual evaluated at this same state
-        Phase ph(c, kPhJac);
-        k_jac_elem_wet<<<nblk(c->T, kJacElems), kJacThreads, 0, c->stream>>>(c->dm, s, P, c->jslots.p, c->ewet.p);
-        if (c->ngeneral > 0) {
-            k_jac_elem_general<<<nblk(c->ngeneral, kJacElems), kJacThreads, 0, c->stream>>>(
-                c->dm, s, P, c->jslots.p, c->glist.p, c->ngeneral);
-            c->launches++;
+int launch_half_inc(Runner& R, const std::vector<int>& sub) {
+    return launch_map(R, sub, 256, [&](int k) { return nblk(R.ctx[k]->V, 256); }, k_half_inc);
+}
+
+// One time step of every instance (fe_sw2 level shift + fe_newton), the instances in
+// lockstep: each Newton phase is one launch over the instances still iterating, and each
+// instance follows exactly the decisions it takes alone.
+int runner_step(Runner& R, const double* dt, const double* const* series, sw2gpu_stats* stats, int* status) {
+    const int K = (int)R.ctx.size();
+    for (int k = 0; k < K; k++)
+        if (!(dt[k] > 0.0)) return fail(SW2GPU_E_ARG, "instance %d: bad dt", k);
+    R.launches = 0;
+    R.nphase = 0;
+    CK(cudaEventRecord(R.ev0, R.stream));
+    int rc = 0;
+    for (int k = 0; k < K; k++) {
+        sw2gpu_ctx* c = R.ctx[k];
+        c->dt = dt[k];
+        const int o2 = c->lv[2];   // fe_sw2: older <- old <- current (level rotation, no copies)
+        c->lv[2] = c->lv[1];
+        c->lv[1] = c->lv[0];
+        c->lv[0] = o2;
+        if ((rc = upload_step_tables(c, series ? series[k] : nullptr, R.stream))) return rc;
+    }
+    if ((rc = runner_tables(R, 1))) return rc;
+    std::vector<int> all(K);
+    for (int k = 0; k < K; k++) all[k] = k;
+    if ((rc = launch_init(R, all))) return rc;
+    if ((rc = launch_resid(R, all))) return rc;
+    if ((rc = read_results(R))) return rc;
+    // Inexact Newton: the linear residual of iteration k only needs to be small next to
+    // the Newton tolerance, so the Krylov test is relative with
+    //   eta_k = max(lin_rtol, kEtaNtl * tol_nonlin / max|R_k|)      (capped at 1e-5).
+    // Early iterations (large R) solve to near round-off like the reference's exact LU;
+    // late ones (R close to tol_nonlin) stop early.  A solve that reaches max_lin_it
+    // but reduced its residual by kAcceptRel is accepted: its error is already far below
+    // what the next residual evaluation can see.
+    constexpr double kEtaNtl = 1e-4, kAcceptRel = 1e-8;
+    std::vector<double> rmax(K), l2(K), imax(K), old_l2(K, 0.0), eta(K, 0.0);
+    std::vector<int> it(K, 0), lin(K, 0), cuts(K, 0), cuts_total(K, 0);
+    std::vector<char> ok(K, 1), nan(K, 0), done(K, 0);
+    for (int k = 0; k < K; k++) {
+        const Norms& nm = R.norms_h[k];
+        const double n3 = 3.0 * R.ctx[k]->V;
+        rmax[k] = nm.rmax;
+        l2[k] = std::sqrt(nm.l2sum / n3);
+        imax[k] = nm.imax;
+        if (nm.nan) {
+            nan[k] = 1;
+            ok[k] = 0;
+            done[k] = 1;
         }
     }
-    if (c->E) k_jac_edge<<<nblk(6LL * c->E, 128), 128, 0, c->stream>>>(c->dm, s, P, c->jslots.p);
-    k_jac_gather<<<nblk(9LL * c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->jslots.p, c->val.p);
-    c->launches += 2 + (c->E ? 1 : 0);
-    CK(cudaGetLastError());
-    return 0;
-}
-
-int launch_init(sw2gpu_ctx* c) {     // fe_sw2_init: current = old, Dirichlet values, wd flags
-    const size_t nb = sizeof(double) * c->V;
-    CK(cudaMemcpyAsync(c->H(0), c->H(1), nb, cudaMemcpyDeviceToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->U(0), c->U(1), nb, cudaMemcpyDeviceToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->Vv(0), c->Vv(1), nb, cudaMemcpyDeviceToDevice, c->stream));
-    const int nd = (int)c->dir_node.size();
-    if (nd) {
-        k_dirichlet<<<nblk(nd, 128), 128, 0, c->stream>>>(nd, c->dir_node_d.p, c->dir_mask_d.p, c->dir_h.p,
-                                                           c->dir_u.p, c->dir_v.p, c->H(0), c->U(0), c->Vv(0));
-        c->launches++;
+    for (;;) {
+        std::vector<int> act;
+        for (int k = 0; k < K; k++)
+            if (!done[k]) act.push_back(k);
+        if (act.empty()) break;
+        if ((rc = launch_jacobian(R, act))) return rc;
+        for (int k : act) {
+            const sw2gpu_params& p = R.ctx[k]->p;
+            eta[k] = std::min(1e-5, std::max(p.lin_rtol, kEtaNtl * p.tol_nonlin / std::max(rmax[k], 1e-300)));
+        }
+        if ((rc = launch_linear(R, act, eta))) return rc;
+        for (int k : act) old_l2[k] = l2[k];
+        if ((rc = launch_resid(R, act))) return rc;
+        if ((rc = read_results(R))) return rc;
+        std::vector<int> ls;
+        for (int k : act) {
+            const sw2gpu_params& p = R.ctx[k]->p;
+            const KrylovCtl& q = R.ctl_h[k];
+            if (q.err) return fail(SW2GPU_E_TIMEOUT, "instance %d: Krylov barrier or tile-copy wait ran out", k);
+            lin[k] += q.iterations;
+            // the plain path fails the step when BiCGSTAB hits max_lin_it without a useful
+            // reduction (solv_bcgstab.c:280-292); on the mixed path the FP32 inner solve is a
+            // correction refined by the FP64 Newton loop, so its last iterate is accepted (the
+            // reference's force_lin_it behaviour)
+            if (!q.converged && p.precision != SW2GPU_MIXED && !(q.rnorm <= kAcceptRel * q.bnorm)) ok[k] = 0;
+            const Norms& nm = R.norms_h[k];
+            rmax[k] = nm.rmax;
+            l2[k] = std::sqrt(nm.l2sum / (3.0 * R.ctx[k]->V));
+            imax[k] = nm.imax;
+            if (nm.nan || std::isnan(l2[k]) || std::isinf(l2[k])) {
+                ok[k] = 0;
+                nan[k] = 1;
+            }
+            cuts[k] = 0;
+            if (rmax[k] > p.tol_nonlin && l2[k] > old_l2[k] && cuts[k] < p.max_linesearch_cuts) ls.push_back(k);
+        }
+        // line search (fe_newton.c:692-747): halve the increment while the l2 norm grew
+        while (!ls.empty()) {
+            if ((rc = launch_half_inc(R, ls))) return rc;
+            if ((rc = launch_resid(R, ls))) return rc;
+            if ((rc = read_results(R))) return rc;
+            std::vector<int> next;
+            for (int k : ls) {
+                const sw2gpu_params& p = R.ctx[k]->p;
+                const Norms& nm = R.norms_h[k];
+                rmax[k] = nm.rmax;
+                l2[k] = std::sqrt(nm.l2sum / (3.0 * R.ctx[k]->V));
+                imax[k] = nm.imax;
+                cuts[k]++;
+                if (rmax[k] > p.tol_nonlin && l2[k] > old_l2[k] && cuts[k] < p.max_linesearch_cuts) next.push_back(k);
+            }
+            ls.swap(next);
+        }
+        for (int k : act) {
+            const sw2gpu_params& p = R.ctx[k]->p;
+            cuts_total[k] += cuts[k];
+            it[k]++;
+            const bool keep = ok[k] && it[k] < p.max_nonlin_it && rmax[k] < 1.0E+20 &&
+                              (rmax[k] > p.tol_nonlin && imax[k] > p.inc_nonlin);
+            if (!keep) done[k] = 1;
+        }
     }
-    CK(cudaMemsetAsync(c->mark.p, 0, std::max(c->V, 1), c->stream));
-    if (c->T) {
-        k_wd_mark<<<nblk(c->T, 256), 256, 0, c->stream>>>(c->T, c->en0.p, c->en1.p, c->en2.p, c->H(0), c->mark.p);
-        k_wd_flag<<<nblk(c->T, 256), 256, 0, c->stream>>>(c->T, c->en0.p, c->en1.p, c->en2.p, c->H(0), c->H(1),
-                                                          c->mark.p, c->wd.p);
-        c->launches += 2;
+    std::vector<int> failed;
+    for (int k = 0; k < K; k++) {
+        const sw2gpu_params& p = R.ctx[k]->p;
+        status[k] = SW2GPU_OK;
+        if (!ok[k] || (rmax[k] > p.tol_nonlin && imax[k] > p.inc_nonlin) || rmax[k] >= 1.0E+20) {
+            status[k] = nan[k] ? SW2GPU_E_NAN : (!ok[k] ? SW2GPU_E_LINEAR : SW2GPU_E_NEWTON);
+            failed.push_back(k);
+        }
     }
-    CK(cudaGetLastError());
-    return 0;
-}
-
-// bytes per stage of the staged Krylov sweeps: the largest 16-byte-rounded block range and
-// column-index range of any tile of kTileRows rows, for matrix elements of esz bytes
-void stage_caps(const std::vector<int>& rp, int V, size_t esz, unsigned& a_cap, unsigned& c_cap) {
-    size_t am = 16, cm = 16;
-    for (int r0 = 0; r0 < V; r0 += kTileRows) {
-        const size_t k0 = (size_t)rp[r0], k1 = (size_t)rp[std::min(r0 + kTileRows, V)];
-        am = std::max(am, ((k1 * 9 * esz + 15) & ~size_t(15)) - ((k0 * 9 * esz) & ~size_t(15)));
-        cm = std::max(cm, ((k1 * 4 + 15) & ~size_t(15)) - ((k0 * 4) & ~size_t(15)));
+    if (!failed.empty() && (rc = launch_init(R, failed))) return rc;   // reset to the old level
+    CK(cudaEventRecord(R.ev1, R.stream));
+    CK(cudaEventSynchronize(R.ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, R.ev0, R.ev1);
+    double ph[3] = {0.0, 0.0, 0.0};
+    for (int q = 0; q < R.nphase; q++) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, R.pev[2 * q], R.pev[2 * q + 1]) == cudaSuccess) ph[R.pkind[q]] += t;
     }
-    a_cap = (unsigned)am;
-    c_cap = (unsigned)cm;
-}
-
-#ifndef SW2_MAX_STAGED_SMEM
-#define SW2_MAX_STAGED_SMEM (96 * 1024)   // dynamic shared memory allowed for the tile ring
-#endif
-constexpr size_t kMaxStagedSmem = SW2_MAX_STAGED_SMEM;
-
-template <typename MT>
-void* krylov_kernel(bool staged) {
-    return staged ? (void*)k_bicgstab<MT, double, true> : (void*)k_bicgstab<MT, double, false>;
-}
-
-// scaling, preconditioner setup and the persistent BiCGSTAB; returns its iteration count
-int launch_linear(sw2gpu_ctx* c, int apply_inc, double rtol) {
-    State s = c->state();
-    k_rowscale<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->dm, s, c->val.p, c->R.p, c->S_.p, c->bs.p, 0);
-    CK(cudaMemsetAsync(c->singular.p, 0, sizeof(int), c->stream));
-    const bool mixed = c->p.precision == SW2GPU_MIXED;
-    k_fold_diag<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->S_.p, c->dinv64.p, c->singular.p);
-    if (mixed)
-        k_fold_offdiag<float><<<nblk(c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->S_.p, c->dinv64.p,
-                                                                         c->aoff32.p);
-    else
-        k_fold_offdiag<double><<<nblk(c->nnzb, 256), 256, 0, c->stream>>>(c->dm, c->val.p, c->S_.p, c->dinv64.p,
-                                                                          c->aoff64.p);
-    CK(cudaMemsetAsync(c->ctl.p, 0, sizeof(KrylovCtl), c->stream));
-    KrylovArgs K;
-    K.V = c->V;
-    K.rowptr = c->orowptr.p;
-    K.col = c->ocol.p;
-    K.S = c->S_.p;
-    K.bs = c->bs.p;
-    K.rtol = rtol;
-    K.atol = c->p.lin_atol;
-    K.maxit = c->p.max_lin_it;
-    K.h = c->H(0);
-    K.u = c->U(0);
-    K.v = c->Vv(0);
-    K.sol = c->sol.p;
-    K.apply_inc = apply_inc;
-    K.part = c->part.p;
-    K.ctl = c->ctl.p;
-    K.c_off = c->c_off;
-    K.r_off = c->r_off;
-    K.v_off = c->v_off;
-    K.stage_bytes = c->stage_bytes;
-    dim3 grid(c->krylov_grid), block(kKrylovThreads);
-    Phase ph(c, kPhKrylov);
-    if (mixed) {
-        const float* A = c->aoff32.p;
-        const double* D = c->dinv64.p;
-        double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
-               *Ap = c->kv64[5].p, *As = c->kv64[6].p, *ub = c->kv64[7].p;
-        void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As, &ub};
-        CK(cudaLaunchCooperativeKernel(krylov_kernel<float>(c->staged), grid, block, args, c->krylov_smem, c->stream));
-    } else {
-        const double* A = c->aoff64.p;
-        const double* D = c->dinv64.p;
-        double *b = c->kv64[0].p, *uu = c->kv64[1].p, *r = c->kv64[2].p, *q = c->kv64[3].p, *pp = c->kv64[4].p,
-               *Ap = c->kv64[5].p, *As = c->kv64[6].p, *ub = c->kv64[7].p;
-        void* args[] = {&K, &A, &D, &b, &uu, &r, &q, &pp, &Ap, &As, &ub};
-        CK(cudaLaunchCooperativeKernel(krylov_kernel<double>(c->staged), grid, block, args, c->krylov_smem, c->stream));
+    if (stats) {
+        for (int k = 0; k < K; k++) {
+            sw2gpu_stats& st = stats[k];
+            memset(&st, 0, sizeof(st));
+            st.status = status[k];
+            st.newton_its = it[k];
+            st.linear_its = lin[k];
+            st.linesearch_cuts = cuts_total[k];
+            st.resid_max = rmax[k];
+            st.resid_l2 = l2[k];
+            st.inc_max = imax[k];
+            st.device_ms = ms;
+            st.kernel_launches = R.launches;
+            st.jac_ms = ph[kPhJac];
+            st.krylov_ms = ph[kPhKrylov];
+            st.resid_ms = ph[kPhResid];
+            st.other_ms = ms - ph[0] - ph[1] - ph[2];
+        }
     }
-    c->launches += 3;
-    CK(cudaMemcpyAsync(c->ctl_h, c->ctl.p, sizeof(KrylovCtl), cudaMemcpyDeviceToHost, c->stream));
     return 0;
 }
 
@@ -609,50 +913,24 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
         rc |= up(c->ocol, ocol, st);
     }
     for (auto& b : c->kv64) rc |= zalloc(b, 3ull * V, st);
-    rc |= zalloc(c->ctl, 1, st);
     rc |= zalloc(c->ncounter, 1, st);
-    rc |= zalloc(c->singular, 1, st);
     const int gblocks = nblk(V, kGatherThreads);
     rc |= zalloc(c->npart, gblocks, st);
-    rc |= zalloc(c->norms, 1, st);
     if (rc) return rc;
-    // persistent Krylov grid: every block co-resident.  The sweeps stage matrix tiles in
-    // shared memory when kStages tiles fit in kMaxStagedSmem (true for triangle meshes,
-    // ~7 blocks per row); a mesh with much denser rows falls back to direct loads.
-    int sms = 0, per_sm = 0;
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // Krylov: the largest tile ranges (for the staged sweeps' stage layout) and the virtual
+    // grid, which is the co-resident grid this instance gets alone (it fixes the order of
+    // every Krylov reduction, so the instance's results do not depend on its batch)
     {
         const bool mixed = prm->precision == SW2GPU_MIXED;
         const unsigned esz = mixed ? sizeof(float) : sizeof(double);
-        unsigned a_cap = 0, c_cap = 0;
-        stage_caps(c->orowptr_h, V, esz, a_cap, c_cap);
-        // stage layout: blocks | column indices | kTileRows + 1 row pointers | 3 vectors
-        const unsigned c_off = a_cap, r_off = c_off + c_cap;
-        const unsigned v_off = r_off + ((unsigned)(kTileRows + 1) * 4u + 15u) / 16u * 16u;
-        const unsigned stage = (v_off + 3u * tile_vec_bytes<double>() + 127u) & ~127u;
-        c->staged = (size_t)kStages * stage <= kMaxStagedSmem;
-        if (c->staged) {
-            c->c_off = c_off;
-            c->r_off = r_off;
-            c->v_off = v_off;
-            c->stage_bytes = stage;
-        }
-        c->krylov_smem = (size_t)kStages * c->stage_bytes;
-        void* kern = mixed ? krylov_kernel<float>(c->staged) : krylov_kernel<double>(c->staged);
-        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->krylov_smem));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kKrylovThreads, c->krylov_smem));
+        stage_caps(c->orowptr_h, V, esz, c->a_cap, c->c_cap);
     }
-    per_sm = std::min(per_sm, 4);
+    std::vector<sw2gpu_ctx*> me(1, c);
+    c->self.reset(new Runner());
+    if ((rc = runner_init(*c->self, me, st))) return rc;
     const int need = nblk(V, kKrylovThreads);
-    c->krylov_grid = std::max(1, std::min(need, sms * std::max(per_sm, 1)));
+    c->krylov_grid = std::max(1, std::min(need, c->self->capacity));
     if (zalloc(c->part, 8ull * c->krylov_grid, st)) return SW2GPU_E_NOMEM;
-    CK(cudaMallocHost(&c->norms_h, sizeof(Norms)));
-    CK(cudaMallocHost(&c->ctl_h, sizeof(KrylovCtl)));
-    CK(cudaEventCreate(&c->ev0));
-    CK(cudaEventCreate(&c->ev1));
-    c->pev.resize(2 * sw2gpu_ctx::kMaxPhases);
-    c->pkind.resize(sw2gpu_ctx::kMaxPhases);
-    for (auto& e : c->pev) CK(cudaEventCreate(&e));
     DevMesh& d = c->dm;
     d.V = V; d.T = T; d.E = E; d.nnzb = nnzb;
     d.x = c->x.p; d.y = c->y.p; d.z = c->z.p;
@@ -715,15 +993,16 @@ int sw2gpu_set_wd_flag(sw2gpu_ctx* c, const int32_t* wd) {
 int sw2gpu_set_dt(sw2gpu_ctx* c, double dt, const double* series) {
     if (!c || !(dt > 0.0)) return fail(SW2GPU_E_ARG, "bad context or dt");
     c->dt = dt;
-    int rc = upload_step_tables(c, series);
-    if (rc) return rc;
-    CK(cudaStreamSynchronize(c->stream));
-    return SW2GPU_OK;
+    return upload_step_tables(c, series, c->stream);
 }
 
 int sw2gpu_resid(sw2gpu_ctx* c, double* resid) {
     if (!c) return fail(SW2GPU_E_ARG, "null context");
-    int rc = launch_resid(c);
+    Runner& R = *c->self;
+    const std::vector<int> one(1, 0);
+    int rc = runner_tables(R, 1);
+    if (!rc) rc = launch_resid(R, one);
+    if (!rc) rc = read_results(R);
     if (rc) return rc;
     if (resid) CK(cudaMemcpyAsync(resid, c->R.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -734,22 +1013,18 @@ int sw2gpu_load(sw2gpu_ctx* c, int32_t* nnzb, int32_t* row_ptr, int32_t* col, do
     if (!c) return fail(SW2GPU_E_ARG, "null context");
     if (nnzb) *nnzb = c->nnzb;
     if (!val && !resid && !row_ptr && !col) return SW2GPU_OK;
+    Runner& R = *c->self;
+    const std::vector<int> one(1, 0);
+    int rc = runner_tables(R, 1);
+    if (rc) return rc;
     // element classification for the two Jacobian kernels (sw2gpu_step takes it from the
     // residual pass at the same state); R is the last sw2gpu_resid's, as in fe_newton
-    {
-        State s = c->state();
-        CK(cudaMemsetAsync(c->gcount.p, 0, sizeof(int), c->stream));
-        if (c->T) k_classify<<<nblk(c->T, 256), 256, 0, c->stream>>>(c->dm, s, c->ewet.p, c->glist.p, c->gcount.p);
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(&c->norms_h->ngeneral, c->gcount.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        c->ngeneral = c->norms_h->ngeneral;
-    }
-    int rc = launch_jacobian(c);
-    if (rc) return rc;
-    State s = c->state();
-    k_rowscale<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->dm, s, c->val.p, c->R.p, c->S_.p, c->bs.p, 1);
-    CK(cudaGetLastError());
+    if ((rc = launch_map(R, one, 256, [&](int) { return nblk(c->T, 256); }, k_classify))) return rc;
+    CK(cudaMemcpyAsync(&R.norms.p[0].ngeneral, c->gcount.p, sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemsetAsync(c->gcount.p, 0, sizeof(int), c->stream));
+    if ((rc = read_results(R))) return rc;
+    if ((rc = launch_jacobian(R, one))) return rc;
+    if ((rc = launch_map(R, one, 256, [&](int) { return nblk(c->V, 256); }, k_rowscale, 1))) return rc;
     if (row_ptr) memcpy(row_ptr, c->rowptr_h.data(), sizeof(int) * (c->V + 1));
     if (col) memcpy(col, c->col_h.data(), sizeof(int) * c->nnzb);
     if (val) CK(cudaMemcpyAsync(val, c->val.p, sizeof(double) * 9 * (size_t)c->nnzb, cudaMemcpyDeviceToHost, c->stream));
@@ -760,151 +1035,79 @@ int sw2gpu_load(sw2gpu_ctx* c, int32_t* nnzb, int32_t* row_ptr, int32_t* col, do
 
 int sw2gpu_linear_solve(sw2gpu_ctx* c, const double* val, const double* rhs, double* x, int32_t* iterations) {
     if (!c || !val || !rhs || !x) return fail(SW2GPU_E_ARG, "null argument");
+    Runner& R = *c->self;
+    const std::vector<int> one(1, 0);
     CK(cudaMemcpyAsync(c->val.p, val, sizeof(double) * 9 * (size_t)c->nnzb, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->R.p, rhs, sizeof(double) * 3 * c->V, cudaMemcpyHostToDevice, c->stream));
-    int rc = launch_linear(c, 0, c->p.lin_rtol);
+    int rc = runner_tables(R, 0);
+    if (!rc) rc = launch_linear(R, one, std::vector<double>(1, c->p.lin_rtol));
     if (rc) return rc;
     CK(cudaMemcpyAsync(x, c->sol.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    if (iterations) *iterations = c->ctl_h->iterations;
-    if (c->ctl_h->err) return fail(SW2GPU_E_TIMEOUT, "Krylov grid barrier wait ran out");
-    return c->ctl_h->converged ? SW2GPU_OK : fail(SW2GPU_E_LINEAR, "BiCGSTAB reached max_lin_it");
+    if ((rc = read_results(R))) return rc;
+    const KrylovCtl& q = R.ctl_h[0];
+    if (iterations) *iterations = q.iterations;
+    if (q.err) return fail(SW2GPU_E_TIMEOUT, "Krylov barrier or tile-copy wait ran out");
+    return q.converged ? SW2GPU_OK : fail(SW2GPU_E_LINEAR, "BiCGSTAB reached max_lin_it");
 }
 
 int sw2gpu_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* stats) {
     if (!c || !(dt > 0.0)) return fail(SW2GPU_E_ARG, "bad context or dt");
-    const sw2gpu_params& p = c->p;
-    c->launches = 0;
-    c->nphase = 0;
-    c->dt = dt;
-    CK(cudaEventRecord(c->ev0, c->stream));
-    // fe_sw2: older <- old <- current (level rotation, no copies)
-    {
-        const int o2 = c->lv[2];
-        c->lv[2] = c->lv[1];
-        c->lv[1] = c->lv[0];
-        c->lv[0] = o2;
-    }
-    int rc = upload_step_tables(c, series);
+    const double* ser[1] = {series};
+    int status = 0;
+    int rc = runner_step(*c->self, &dt, ser, stats, &status);
     if (rc) return rc;
-    if ((rc = launch_init(c))) return rc;
-    if ((rc = launch_resid(c))) return rc;
-    Norms nm;
-    if ((rc = read_norms(c, nm))) return rc;
-    const double n3 = 3.0 * c->V;
-    double rmax = nm.rmax, l2 = std::sqrt(nm.l2sum / n3), imax = nm.imax, old_l2;
-    int it = 0, lin_total = 0, cuts_total = 0;
-    bool solv_ok = true, nan = nm.nan != 0, keep;
-    // Inexact Newton: the linear residual of iteration k only needs to be small next to
-    // the Newton tolerance, so the Krylov test is relative with
-    //   eta_k = max(lin_rtol, kEtaNtl * tol_nonlin / max|R_k|)      (capped at 1e-5).
-    // Early iterations (large R) solve to near round-off like the reference's exact LU;
-    // late ones (R close to tol_nonlin) stop early.  A solve that reaches max_lin_it
-    // but reduced its residual by kAcceptRel is accepted: its error is already far below
-    // what the next residual evaluation can see.
-    constexpr double kEtaNtl = 1e-4, kAcceptRel = 1e-8;
-    if (nan) solv_ok = false;
-    do {
-        if (!solv_ok) break;
-        if ((rc = launch_jacobian(c))) return rc;
-        const double eta = std::min(1e-5, std::max(p.lin_rtol, kEtaNtl * p.tol_nonlin / std::max(rmax, 1e-300)));
-        if ((rc = launch_linear(c, 1, eta))) return rc;
-        old_l2 = l2;
-        if ((rc = launch_resid(c))) return rc;
-        if ((rc = read_norms(c, nm))) return rc;   // also completes the Krylov control read
-        if (c->ctl_h->err) return fail(SW2GPU_E_TIMEOUT, "Krylov grid barrier wait ran out");
-        lin_total += c->ctl_h->iterations;
-        // the plain path fails the step when BiCGSTAB hits max_lin_it without a useful
-        // reduction (solv_bcgstab.c:280-292); on the mixed path the FP32 inner solve is a
-        // correction refined by the FP64 Newton loop, so its last iterate is accepted (the
-        // reference's force_lin_it behaviour)
-        if (!c->ctl_h->converged && p.precision != SW2GPU_MIXED &&
-            !(c->ctl_h->rnorm <= kAcceptRel * c->ctl_h->bnorm))
-            solv_ok = false;
-        rmax = nm.rmax;
-        l2 = std::sqrt(nm.l2sum / n3);
-        imax = nm.imax;
-        if (nm.nan || std::isnan(l2) || std::isinf(l2)) { solv_ok = false; nan = true; }
-        int cuts = 0;
-        while (rmax > p.tol_nonlin && l2 > old_l2 && cuts < p.max_linesearch_cuts) {
-            k_half_inc<<<nblk(c->V, 256), 256, 0, c->stream>>>(c->V, c->sol.p, c->H(0), c->U(0), c->Vv(0));
-            c->launches++;
-            if ((rc = launch_resid(c))) return rc;
-            if ((rc = read_norms(c, nm))) return rc;
-            rmax = nm.rmax;
-            l2 = std::sqrt(nm.l2sum / n3);
-            imax = nm.imax;
-            cuts++;
-        }
-        cuts_total += cuts;
-        it++;
-        keep = solv_ok && it < p.max_nonlin_it && rmax < 1.0E+20 && (rmax > p.tol_nonlin && imax > p.inc_nonlin);
-    } while (keep);
-    int status = SW2GPU_OK;
-    if (!solv_ok || (rmax > p.tol_nonlin && imax > p.inc_nonlin) || rmax >= 1.0E+20) {
-        status = nan ? SW2GPU_E_NAN : (!solv_ok ? SW2GPU_E_LINEAR : SW2GPU_E_NEWTON);
-        if ((rc = launch_init(c))) return rc;   // reset to the old level; the caller scales dt
-    }
-    CK(cudaEventRecord(c->ev1, c->stream));
-    CK(cudaEventSynchronize(c->ev1));
-    if (stats) {
-        memset(stats, 0, sizeof(*stats));
-        stats->status = status;
-        stats->newton_its = it;
-        stats->linear_its = lin_total;
-        stats->linesearch_cuts = cuts_total;
-        stats->resid_max = rmax;
-        stats->resid_l2 = l2;
-        stats->inc_max = imax;
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-        stats->device_ms = ms;
-        stats->kernel_launches = c->launches;
-        double ph[3] = {0.0, 0.0, 0.0};
-        for (int k = 0; k < c->nphase; k++) {
-            float t = 0.f;
-            if (cudaEventElapsedTime(&t, c->pev[2 * k], c->pev[2 * k + 1]) == cudaSuccess) ph[c->pkind[k]] += t;
-        }
-        stats->jac_ms = ph[kPhJac];
-        stats->krylov_ms = ph[kPhKrylov];
-        stats->resid_ms = ph[kPhResid];
-        stats->other_ms = ms - ph[0] - ph[1] - ph[2];
-    }
-    if (status != SW2GPU_OK) fail(status, "step failed (Newton %d iterations, max residual %g)", it, rmax);
+    if (status != SW2GPU_OK)
+        fail(status, "step failed (Newton %d iterations, max residual %g)", stats ? stats->newton_its : -1,
+             stats ? stats->resid_max : 0.0);
     return status;
 }
 
-}  // extern "C"
-
-// ---------------------------------------------------------------------------------
-// batched ensemble
-struct sw2gpu_batch {
-    std::vector<sw2gpu_ctx*> ctxs;
-    cudaStream_t stream = nullptr;
-};
-
-extern "C" {
-
 int sw2gpu_batch_create(sw2gpu_ctx** ctxs, int32_t n, void* stream, sw2gpu_batch** out) {
     if (!ctxs || n <= 0 || !out) return fail(SW2GPU_E_ARG, "bad batch arguments");
+    if (n > kMaxBatch) return fail(SW2GPU_E_ARG, "batch of %d instances exceeds %d", n, kMaxBatch);
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < i; j++)
+            if (ctxs[i] == ctxs[j] || !ctxs[i]) return fail(SW2GPU_E_ARG, "batch instance %d repeated or null", i);
+    *out = nullptr;
     auto* b = new sw2gpu_batch();
-    b->ctxs.assign(ctxs, ctxs + n);
-    b->stream = (cudaStream_t)stream;
-    *out = b;
+    std::unique_ptr<sw2gpu_batch> guard(b);
+    b->run.reset(new Runner());
+    cudaStream_t st = (cudaStream_t)stream;
+    bool own = false;
+    if (!st) {
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        own = true;
+    }
+    b->own_stream = own;
+    int rc = runner_init(*b->run, std::vector<sw2gpu_ctx*>(ctxs, ctxs + n), st);
+    if (rc) {
+        if (own) cudaStreamDestroy(st);
+        return rc;
+    }
+    *out = guard.release();
     return SW2GPU_OK;
 }
 
 int sw2gpu_batch_step(sw2gpu_batch* b, const double* dt, const double* const* series, sw2gpu_stats* stats) {
     if (!b || !dt) return fail(SW2GPU_E_ARG, "bad batch arguments");
-    int worst = SW2GPU_OK;
-    for (size_t i = 0; i < b->ctxs.size(); i++) {
-        int rc = sw2gpu_step(b->ctxs[i], dt[i], series ? series[i] : nullptr, stats ? stats + i : nullptr);
-        if (rc != SW2GPU_OK && worst == SW2GPU_OK) worst = rc;
-    }
-    return worst;
+    const int K = (int)b->run->ctx.size();
+    std::vector<int> status(K, 0);
+    std::vector<sw2gpu_stats> st(K);
+    // instances' own streams may still hold work (state uploads): order it before the batch
+    for (auto* c : b->run->ctx) CK(cudaStreamSynchronize(c->stream));
+    int rc = runner_step(*b->run, dt, series, stats ? stats : st.data(), status.data());
+    if (rc) return rc;
+    for (int k = 0; k < K; k++)
+        if (status[k] != SW2GPU_OK) return fail(status[k], "instance %d: step failed", k);
+    return SW2GPU_OK;
 }
 
 int sw2gpu_batch_destroy(sw2gpu_batch* b) {
+    if (!b) return SW2GPU_OK;
+    cudaStream_t st = b->run->stream;
+    cudaStreamSynchronize(st);
+    b->run.reset();
+    if (b->own_stream) cudaStreamDestroy(st);
     delete b;
     return SW2GPU_OK;
 }

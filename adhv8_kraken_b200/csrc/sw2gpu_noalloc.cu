@@ -45,7 +45,8 @@ constexpr size_t kOffA = kOffDinv + al(9ull * kMaxNodes);
 constexpr size_t kOffRp = kOffA + al(9ull * kMaxBlocks);
 constexpr size_t kOffCol = kOffRp + al((kMaxNodes + 2) / 2);
 constexpr size_t kOffVec = kOffCol + al((kMaxBlocks + 1) / 2);
-constexpr size_t kScratchDoubles = kOffVec + 8 * al(3ull * kMaxNodes);
+constexpr size_t kOffInst = kOffVec + 8 * al(3ull * kMaxNodes);   // the Krylov launch's instance record
+constexpr size_t kScratchDoubles = kOffInst + al((sizeof(KrylovInst) + 7) / 8);
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
@@ -129,6 +130,10 @@ __global__ void k_na_fold(int V, const int* __restrict__ rowptr, const int* __re
     }
 }
 
+// writes the instance record of the Krylov launch into the scratch array (a kernel argument
+// copied on the device: no host staging buffer)
+__global__ void k_na_put(KrylovInst q, KrylovInst* dst) { *dst = q; }
+
 // device address of the scratch array for the current device (looked up once per device)
 int scratch_for_current_device(double** out) {
     int dev = 0;
@@ -187,13 +192,13 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double, false>, kKrylovThreads, 0);
     const int grid = std::max(1, std::min({kMaxGrid, (nnodes + kKrylovThreads - 1) / kKrylovThreads,
                                            sms * std::max(per_sm, 1)}));
-    KrylovArgs K;
+    KrylovInst Q;
+    KrylovArgs& K = Q.K;
     K.V = nnodes;
     K.rowptr = orp;
     K.col = ocol;
     K.S = S;
     K.bs = bs;
-    K.rtol = rtol;
     K.atol = atol;
     K.maxit = max_it;
     K.h = K.u = K.v = nullptr;
@@ -201,12 +206,24 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     K.apply_inc = 0;
     K.part = part;
     K.ctl = ctl;
-    K.c_off = K.r_off = K.v_off = K.stage_bytes = 0;   // direct sweeps
-    const double* Ac = A;
-    const double* Dc = dinv;
-    void* args[] = {&K, &Ac, &Dc, &v[0], &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7]};
-    cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double, false>, dim3(grid), dim3(kKrylovThreads),
-                                                args, 0, st);
+    K.vgrid = grid;
+    Q.A = A;
+    Q.Dinv = dinv;
+    for (int k = 0; k < 8; k++) Q.vec[k] = v[k];
+    KrylovInst* qdev = reinterpret_cast<KrylovInst*>(sc + kOffInst);
+    k_na_put<<<1, 1, 0, st>>>(Q, qdev);
+    // one instance, direct sweeps (no tile ring)
+    static thread_local KrylovLaunch L;
+    L.mp.n = 1;
+    L.mp.boff[0] = 0;
+    L.mp.boff[1] = grid;
+    L.mp.ids[0] = 0;
+    L.rtol[0] = rtol;
+    L.c_off = L.r_off = L.v_off = L.stage_bytes = 0;
+    const KrylovInst* tabp = qdev;
+    void* args[] = {(void*)&tabp, (void*)&L};
+    cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double, false>, dim3(grid),
+                                                dim3(kKrylovThreads), args, 0, st);
     if (e != cudaSuccess) return na_fail(SW2GPU_E_CUDA, cudaGetErrorString(e));
     KrylovCtl h;
     e = cudaMemcpyAsync(&h, ctl, sizeof(KrylovCtl), cudaMemcpyDeviceToHost, st);

@@ -187,6 +187,53 @@ class SW2GPU:
         return d
 
 
+class SW2Batch:
+    """Independent SW2GPU instances of uneven size stepped together (``sw2gpu_batch_*``): each
+    Newton phase is one launch over the instances still iterating, and every instance's
+    results are bitwise those it computes alone.  All instances share one precision."""
+
+    _FATAL = (capi.SW2GPU_E_ARG, capi.SW2GPU_E_CUDA, capi.SW2GPU_E_NOMEM, capi.SW2GPU_E_TIMEOUT)
+
+    def __init__(self, solvers, stream: int = 0):
+        self.solvers = list(solvers)
+        n = len(self.solvers)
+        arr = (C.c_void_p * n)(*[s.h.value for s in self.solvers])
+        h = C.c_void_p()
+        _check(lib().sw2gpu_batch_create(arr, n, C.c_void_p(stream) if stream else None, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sw2gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, dts=None):
+        """One time step of every instance (dts[k] or its model's dt); list of stats dicts."""
+        n = len(self.solvers)
+        dts = np.array([s.model.dt if dts is None or dts[k] is None else dts[k] for k, s in enumerate(self.solvers)],
+                       dtype=np.float64)
+        series = [np.ascontiguousarray(s.model.series_values(s.t, s.t + dts[k]), dtype=np.float64)
+                  for k, s in enumerate(self.solvers)]
+        ptrs = (c_double_p * n)(*[_dp(a) if a.size else c_double_p() for a in series])
+        stats = (Stats * n)()
+        rc = lib().sw2gpu_batch_step(self.h, _dp(dts), ptrs, stats)
+        if rc in self._FATAL:
+            _check(rc)
+        out = []
+        for k, s in enumerate(self.solvers):
+            d = stats[k].as_dict()
+            if d["status"] == 0:
+                s.t = s.t + dts[k]
+            out.append(d)
+        return out
+
+
 def run(solver: SW2GPU, nsteps: int, dt: float = None, max_retries: int = 8, callback=None):
     """Time loop with the reference's failure contract: a step that returns NO is
     retried from the old state with dt * 0.25 (src/tools/tc_scale.c:3-17)."""
