@@ -47,7 +47,7 @@ struct Norms {                  // get_residual_norms (src/fe/fe_newton.c:40-151
 // device table of these and a LaunchMap (instance ids[j] owns blocks boff[j]..boff[j+1]-1);
 // a single solve is a batch of one.  Work indices inside a block are local to its instance,
 // so every instance computes exactly what it computes alone.
-struct Inst {
+struct __align__(16) Inst {
     DevMesh m;
     State s;
     PhysParams P;
@@ -63,6 +63,23 @@ struct Inst {
     int ndir;                   // Dirichlet nodes and their step values
     const int *dir_node, *dir_mask;
     const double *dir_h, *dir_u, *dir_v;
+};
+
+// Where a launch finds its instances.  SrcOne: a single instance, its descriptor a kernel
+// parameter (fields read from the constant bank, the physics constants as direct operands);
+// SrcTab: a batch, descriptors in a device table and a LaunchMap of blocks to instances.
+struct SrcOne {
+    Inst I;
+    __device__ __forceinline__ const Inst& get(int& lb, int& nb) const {
+        lb = blockIdx.x;
+        nb = gridDim.x;
+        return I;
+    }
+};
+struct SrcTab {
+    const Inst* tab;
+    LaunchMap mp;
+    __device__ __forceinline__ const Inst& get(int& lb, int& nb) const { return tab[map_block(mp, lb, nb)]; }
 };
 
 // An element takes the fully wet Jacobian path when its flag is 0 and every vertex depth
@@ -116,9 +133,10 @@ __device__ __forceinline__ void classify_elem(int t, bool wet, unsigned char* ew
 }
 
 // the same classification without a residual (sw2gpu_load called on its own)
-__global__ void k_classify(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_classify(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const State s = I.s;
     unsigned char* ewet = I.ewet;
@@ -137,9 +155,10 @@ __global__ void k_classify(const Inst* __restrict__ tab, const LaunchMap mp) {
     classify_elem(t, s.wd[t] == 0 && wet_depths(h, ho, hoo), ewet, glist, gcount);
 }
 
-__global__ void k_resid_elem(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_resid_elem(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const State s = I.s;
     const PhysParams P = I.P;
@@ -231,9 +250,10 @@ __device__ __forceinline__ void block_reduce3(double& a, double& b, double& c, i
 // partials in block order and writes *out (with the general-list length, after which the
 // list counter returns to 0 for the next evaluation); `counter` returns to 0.
 constexpr int kGatherThreads = 256;
-__global__ void __launch_bounds__(kGatherThreads) k_resid_gather(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void __launch_bounds__(kGatherThreads) k_resid_gather(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const State s = I.s;
     const double* __restrict__ sc = I.sc;
@@ -434,19 +454,20 @@ __device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, 
 #ifndef SW2_JAC_MIN_BLOCKS
 #define SW2_JAC_MIN_BLOCKS 2   // resident CTAs per SM the wet kernel's register budget is cut for
 #endif
-__global__ void __launch_bounds__(kJacThreads, SW2_JAC_MIN_BLOCKS) k_jac_elem_wet(const Inst* __restrict__ tab,
-                                                                                  const LaunchMap mp) {
+template <class Src>
+__global__ void __launch_bounds__(kJacThreads, SW2_JAC_MIN_BLOCKS) k_jac_elem_wet(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const State s = I.s;
     const PhysParams P = I.P;
     jac_elem_body<false>(m, s, P, I.jslots, I.ewet, nullptr, m.T, lb);
 }
 // the list length is the one the last residual evaluation recorded
-__global__ void __launch_bounds__(kJacThreads) k_jac_elem_general(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void __launch_bounds__(kJacThreads) k_jac_elem_general(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const State s = I.s;
     const PhysParams P = I.P;
@@ -455,9 +476,10 @@ __global__ void __launch_bounds__(kJacThreads) k_jac_elem_general(const Inst* __
 
 // FD Jacobian of the boundary edges: one thread per (edge, node, variable); writes the
 // four 3x3 blocks of edge j at slots 9T + 4j + 2a + b.
-__global__ void k_jac_edge(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_jac_edge(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const State s = I.s;
     const PhysParams P = I.P;
@@ -528,9 +550,10 @@ __global__ void k_jac_edge(const Inst* __restrict__ tab, const LaunchMap mp) {
 
 // BCSR values: thread (block k, entry q) sums entry q of every contributing element
 // block in reference order (fe_global_matrix_assemble_sw2 :166-224).
-__global__ void k_jac_gather(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_jac_gather(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const double* __restrict__ jslots = I.jslots;
     double* __restrict__ val = I.val;
@@ -545,9 +568,10 @@ __global__ void k_jac_gather(const Inst* __restrict__ tab, const LaunchMap mp) {
 // Tiny-diagonal fix of fe_sw2_load (:218-236) and the Jacobi scale vector of spv_jacobi
 // (src/solver/spv_jacobi.c:222-285): S = 1/sqrt(max |row entry|), floored.  Also writes
 // the scaled right-hand side b = S R.
-__global__ void k_rowscale(const Inst* __restrict__ tab, const LaunchMap mp, int fix_only) {
+template <class Src>
+__global__ void k_rowscale(const __grid_constant__ Src src, int fix_only) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const State s = I.s;
     double* __restrict__ val = I.val;
@@ -587,9 +611,10 @@ __global__ void k_rowscale(const Inst* __restrict__ tab, const LaunchMap mp, int
 // and D_i the scaled diagonal block of row i, the Krylov operator M^-1 A' has identity
 // diagonal blocks and off-diagonal blocks D_i^-1 A'_ij, so the sweeps stream only those
 // (nnzb - V blocks, no inverses).  k_fold_diag: D_i^-1 per node row (FP64).
-__global__ void k_fold_diag(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_fold_diag(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const double* __restrict__ val = I.val;
     const double* __restrict__ S = I.S;
@@ -608,10 +633,10 @@ __global__ void k_fold_diag(const Inst* __restrict__ tab, const LaunchMap mp) {
 
 // off-diagonal block k of row i -> position k - i - (k > dpos_i) of the folded matrix,
 // D_i^-1 (S_i A_ij S_j) formed in FP64 and stored as MT
-template <typename MT>
-__global__ void k_fold_offdiag(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src, typename MT>
+__global__ void k_fold_offdiag(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const double* __restrict__ val = I.val;
     const double* __restrict__ S = I.S;
@@ -634,9 +659,10 @@ __global__ void k_fold_offdiag(const Inst* __restrict__ tab, const LaunchMap mp)
 }
 
 // line search halving (fe_newton.c:692-747): sol *= 0.5; state += sol (fe_sw2_inc)
-__global__ void k_half_inc(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_half_inc(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     double* __restrict__ sol = I.sol;
     double* __restrict__ h = I.s.h;
     double* __restrict__ u = I.s.u;
@@ -654,9 +680,10 @@ __global__ void k_half_inc(const Inst* __restrict__ tab, const LaunchMap mp) {
 
 // fe_sw2_init (src/fe/sw2/fe_sw2_init.c:24-92), first part: current level <- old level,
 // and the node marks of the wet/dry flag pass cleared
-__global__ void k_init_level(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_init_level(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const State s = I.s;
     const int n = lb * blockDim.x + threadIdx.x;
     if (n >= I.m.V) return;
@@ -667,9 +694,10 @@ __global__ void k_init_level(const Inst* __restrict__ tab, const LaunchMap mp) {
 }
 
 // fe_sw2_wdflag (src/fe/sw2/fe_sw2_wdflag.c:24-75), two passes
-__global__ void k_wd_mark(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_wd_mark(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const double* __restrict__ h = I.s.h;
     unsigned char* __restrict__ mark = I.mark;
@@ -682,9 +710,10 @@ __global__ void k_wd_mark(const Inst* __restrict__ tab, const LaunchMap mp) {
         mark[c] = 1;
     }
 }
-__global__ void k_wd_flag(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_wd_flag(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const double* __restrict__ h = I.s.h;
     const double* __restrict__ ho = I.s.ho;
@@ -699,9 +728,10 @@ __global__ void k_wd_flag(const Inst* __restrict__ tab, const LaunchMap mp) {
 }
 
 // Dirichlet node values of fe_sw2_init (src/fe/sw2/fe_sw2_init.c:37-85)
-__global__ void k_dirichlet(const Inst* __restrict__ tab, const LaunchMap mp) {
+template <class Src>
+__global__ void k_dirichlet(const __grid_constant__ Src src) {
     int lb, nb;
-    const Inst& I = tab[map_block(mp, lb, nb)];
+    const Inst& I = src.get(lb, nb);
     const int t = lb * blockDim.x + threadIdx.x;
     if (t >= I.ndir) return;
     const int k = I.dir_node[t], f = I.dir_mask[t];

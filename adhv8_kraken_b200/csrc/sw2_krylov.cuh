@@ -211,13 +211,46 @@ struct KrylovInst {
     double* vec[8];           // b, u, r, q, p, Ap, As, best u
 };
 
-// launch-wide parameters: the map, each mapped instance's relative tolerance and the stage
-// layout of the staged sweeps (byte offsets inside one stage of the tile's column indices,
-// row pointers and epilogue vectors -- the blocks start at 0 -- and the stage stride)
-struct KrylovLaunch {
+// Stage layout of the staged sweeps: byte offsets inside one stage of the tile's column
+// indices, row pointers and epilogue vectors (the blocks start at 0), and the stage stride.
+struct StageLayout {
+    unsigned c_off, r_off, v_off, stage_bytes;
+};
+
+// Where a Krylov launch finds its instances.  KrylovOne: one instance, its record and
+// tolerance kernel parameters; KrylovTab: a batch, records in a device table, the map and
+// each mapped instance's relative tolerance in the parameters.
+struct KrylovOne {
+    KrylovInst Q;
+    double rtol;
+    StageLayout lay;
+    __device__ __forceinline__ const KrylovInst& get(int& pl, int& np, double& rt) const {
+        pl = blockIdx.x;
+        np = gridDim.x;
+        rt = rtol;
+        return Q;
+    }
+};
+struct KrylovTab {
+    const KrylovInst* tab;
     LaunchMap mp;
     double rtol[kMaxBatch];
-    unsigned c_off, r_off, v_off, stage_bytes;
+    StageLayout lay;
+    __device__ __forceinline__ const KrylovInst& get(int& pl, int& np, double& rt) const {
+        int nb;
+        const int b = blockIdx.x;
+        int lo = 0, hi = mp.n;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (mp.boff[mid] <= b) lo = mid;
+            else hi = mid;
+        }
+        pl = b - mp.boff[lo];
+        nb = mp.boff[lo + 1] - mp.boff[lo];
+        np = nb;
+        rt = rtol[lo];
+        return tab[mp.ids[lo]];
+    }
 };
 
 // bytes of one epilogue vector's slice for a full tile (3 components per row)
@@ -284,7 +317,7 @@ __device__ __forceinline__ unsigned long long hi16(const void* p) { return ((uns
 // completions land on one mbarrier.
 template <typename MT, typename VT>
 __device__ __forceinline__ void issue_tile(int m, int V, const int* rowptr, const int* col, const MT* A, int nvec,
-                                           const VT* const* vecs, unsigned char* stage, const KrylovLaunch& K,
+                                           const VT* const* vecs, unsigned char* stage, const StageLayout& K,
                                            unsigned long long* bar, unsigned long long pol) {
     const int r0 = m * kTileRows, nr = min(kTileRows, V - r0);
     const int k0 = __ldg(rowptr + r0), k1 = __ldg(rowptr + r0 + nr);
@@ -300,6 +333,11 @@ __device__ __forceinline__ void issue_tile(int m, int V, const int* rowptr, cons
     for (int v = 0; v < nvec; v++)
         bulk_load(stage + K.v_off + v * tile_vec_bytes<VT>(), vecs[v] + (size_t)r0 * 3, vb, bar);
 }
+
+// explicit fused multiply-add, a * b + c rounded once (the library is built without implicit
+// contraction so that every kernel instantiation rounds alike; hot loops state their FMAs)
+__device__ __forceinline__ double fmadd(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fmadd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
 template <int N>
 struct IntC {
@@ -328,14 +366,14 @@ __device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke
             const int j = cix(k);
             VT x0 = ldv(xa + 3 * j), x1 = ldv(xa + 3 * j + 1), x2 = ldv(xa + 3 * j + 2);
             if (xb) {
-                x0 -= alpha * ldv(xb + 3 * j);
-                x1 -= alpha * ldv(xb + 3 * j + 1);
-                x2 -= alpha * ldv(xb + 3 * j + 2);
+                x0 = fmadd(-alpha, ldv(xb + 3 * j), x0);
+                x1 = fmadd(-alpha, ldv(xb + 3 * j + 1), x1);
+                x2 = fmadd(-alpha, ldv(xb + 3 * j + 2), x2);
             }
             const MT c0 = (MT)x0, c1 = (MT)x1, c2 = (MT)x2;
-            a0 += m[0] * c0 + m[1] * c1 + m[2] * c2;
-            a1 += m[3] * c0 + m[4] * c1 + m[5] * c2;
-            a2 += m[6] * c0 + m[7] * c1 + m[8] * c2;
+            a0 = fmadd(m[2], c2, fmadd(m[1], c1, fmadd(m[0], c0, a0)));
+            a1 = fmadd(m[5], c2, fmadd(m[4], c1, fmadd(m[3], c0, a1)));
+            a2 = fmadd(m[8], c2, fmadd(m[7], c1, fmadd(m[6], c0, a2)));
         }
     }
 #pragma unroll
@@ -359,27 +397,15 @@ __device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke
 // loads are its x gathers; the streamed matrix data carry an L2 evict-first hint, which keeps
 // the Krylov vectors in L2.  The dynamic shared memory is kStages * L.stage_bytes.  Otherwise
 // the lanes load everything from global memory.
-template <typename MT, typename VT, bool STAGED>
-__global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const KrylovInst* __restrict__ tab,
-                                                               const __grid_constant__ KrylovLaunch L) {
+template <typename MT, typename VT, bool STAGED, class KS>
+__global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_constant__ KS src) {
     __shared__ double red[4 * kKrylovWarps];
     __shared__ unsigned long long bar[kStages];
     extern __shared__ __align__(128) unsigned char stage_mem[];
     int pl, np;   // this CTA's index among the instance's np CTAs
-    int slot;     // position of the instance in the launch map
-    {
-        const int b = blockIdx.x;
-        int lo = 0, hi = L.mp.n;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (L.mp.boff[mid] <= b) lo = mid;
-            else hi = mid;
-        }
-        slot = lo;
-        pl = b - L.mp.boff[lo];
-        np = L.mp.boff[lo + 1] - L.mp.boff[lo];
-    }
-    const KrylovInst& KI = tab[L.mp.ids[slot]];
+    double rtol;
+    const KrylovInst& KI = src.get(pl, np, rtol);
+    const StageLayout& L = src.lay;
     const KrylovArgs K = KI.K;
     const MT* __restrict__ A = (const MT*)KI.A;
     const double* __restrict__ Dinv = KI.Dinv;
@@ -391,7 +417,6 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const KrylovInst
     VT* __restrict__ Ap = KI.vec[5];
     VT* __restrict__ As = KI.vec[6];
     VT* __restrict__ ubest = KI.vec[7];
-    const double rtol = L.rtol[slot];
     const int V = K.V;
     const int VG = K.vgrid;
     const int pstride = np * blockDim.x;                  // reduction-free loops: physical CTAs
@@ -582,7 +607,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const KrylovInst
                     [&](int i, const VT* y, const VT(*ev)[3]) {
 #pragma unroll
                         for (int c = 0; c < 3; c++) {
-                            const VT s = ev[0][c] - al * ev[1][c];
+                            const VT s = fmadd(-al, ev[1][c], ev[0][c]);   // the s the gathers form
                             const VT asc = s + y[c];
                             As[3 * i + c] = asc;
                             w[0] += (double)asc * (double)s;
@@ -612,15 +637,15 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const KrylovInst
                     // element-wise (every load coalesced), virtual CTA v's share
                     for (int k = v * blockDim.x + threadIdx.x; k < 3 * V; k += VG * blockDim.x) {
                         const VT apk = ldv(Ap + k), pk = ldv(p + k);
-                        const VT s = ldv(r + k) - al * apk;
+                        const VT s = fmadd(-al, apk, ldv(r + k));
                         VT uk = ldv(uu + k);
                         if (pending) ubest[k] = uk;
-                        uk += al * pk;
-                        uk += om * s;
+                        uk = fmadd(al, pk, uk);
+                        uk = fmadd(om, s, uk);
                         uu[k] = uk;
-                        const VT rk = s - om * ldv(As + k);
+                        const VT rk = fmadd(-om, ldv(As + k), s);
                         r[k] = rk;
-                        p[k] = (pk - om * apk) * be + rk;
+                        p[k] = fmadd(fmadd(-om, apk, pk), be, rk);
                         mx[0] = fmax(mx[0], fabs((double)rk));
                     }
                     block_partial<1>(mx, mm, pbuf(), v, red);

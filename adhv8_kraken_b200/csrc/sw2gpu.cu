@@ -15,6 +15,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/sw2gpu.h"
@@ -160,9 +161,9 @@ void stage_caps(const std::vector<int>& rp, int V, size_t esz, unsigned& a_cap, 
     c_cap = (unsigned)cm;
 }
 
-template <typename MT>
+template <typename MT, class KS>
 void* krylov_kernel(bool staged) {
-    return staged ? (void*)k_bicgstab<MT, double, true> : (void*)k_bicgstab<MT, double, false>;
+    return staged ? (void*)k_bicgstab<MT, double, true, KS> : (void*)k_bicgstab<MT, double, false, KS>;
 }
 
 }  // namespace
@@ -320,9 +321,18 @@ int runner_init(Runner& R, const std::vector<sw2gpu_ctx*>& ctx, cudaStream_t str
     int dev = 0, sms = 0, per_sm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    void* kern = R.mixed ? krylov_kernel<float>(R.staged) : krylov_kernel<double>(R.staged);
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R.smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kKrylovThreads, R.smem));
+    // the dynamic shared-memory cap is an attribute of the kernel, shared by every runner:
+    // set to the largest tile ring any runner may use
+    void* kone = R.mixed ? krylov_kernel<float, KrylovOne>(R.staged) : krylov_kernel<double, KrylovOne>(R.staged);
+    void* ktab = R.mixed ? krylov_kernel<float, KrylovTab>(R.staged) : krylov_kernel<double, KrylovTab>(R.staged);
+    if (R.staged) {
+        CK(cudaFuncSetAttribute(kone, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStagedSmem));
+        CK(cudaFuncSetAttribute(ktab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStagedSmem));
+    }
+    int per_sm_tab = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kone, kKrylovThreads, R.smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tab, ktab, kKrylovThreads, R.smem));
+    per_sm = std::min(per_sm, per_sm_tab);
     R.capacity = sms * std::max(1, std::min(per_sm, 4));
     CK(cudaEventCreate(&R.ev0));
     CK(cudaEventCreate(&R.ev1));
@@ -393,36 +403,47 @@ int make_map(LaunchMap& mp, const std::vector<int>& subset, F blocks) {
     return off;
 }
 
-// one launch of kernel `kern` (tab, map) over the subset, `threads` per block
-template <class F, class... Args>
-int launch_map(Runner& R, const std::vector<int>& subset, int threads, F blocks,
-               void (*kern)(const Inst*, const LaunchMap, Args...), Args... args) {
-    LaunchMap mp;
-    const int nb = make_map(mp, subset, blocks);
+// one launch over the subset: instance k gets blocks(k) blocks of `threads` threads, and
+// go(src, blocks, threads) launches the kernel with its instance source -- the descriptor
+// itself when one instance is mapped, else the device table and the map
+template <class F, class G>
+int launch_map(Runner& R, const std::vector<int>& subset, int threads, F blocks, G go) {
+    static thread_local SrcTab t;   // ~2 KB map: not on every caller's stack
+    const int nb = make_map(t.mp, subset, blocks);
     if (nb == 0) return 0;
-    kern<<<nb, threads, 0, R.stream>>>(R.tab.p, mp, args...);
+    if (t.mp.n == 1) {
+        SrcOne one;
+        one.I = R.tab_h[t.mp.ids[0]];
+        go(one, nb, threads);
+    } else {
+        t.tab = R.tab.p;
+        go(t, nb, threads);
+    }
     R.launches++;
     CK(cudaGetLastError());
     return 0;
 }
+#define SW2_GO(kernel, ...) [&](const auto& src, int nb_, int th_) { kernel<<<nb_, th_, 0, R.stream>>>(src, ##__VA_ARGS__); }
+#define SW2_GO_T(kernel, T, ...) \
+    [&](const auto& src, int nb_, int th_) { kernel<std::decay_t<decltype(src)>, T><<<nb_, th_, 0, R.stream>>>(src, ##__VA_ARGS__); }
 
 int launch_init(Runner& R, const std::vector<int>& sub) {     // fe_sw2_init
     int rc = 0;
     auto C = [&](int k) { return R.ctx[k]; };
-    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, k_init_level))) return rc;
-    if ((rc = launch_map(R, sub, 128, [&](int k) { return nblk((int)C(k)->dir_node.size(), 128); }, k_dirichlet)))
+    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, SW2_GO(k_init_level<std::decay_t<decltype(src)>>)))) return rc;
+    if ((rc = launch_map(R, sub, 128, [&](int k) { return nblk((int)C(k)->dir_node.size(), 128); }, SW2_GO(k_dirichlet<std::decay_t<decltype(src)>>))))
         return rc;
-    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->T, 256); }, k_wd_mark))) return rc;
-    return launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->T, 256); }, k_wd_flag);
+    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->T, 256); }, SW2_GO(k_wd_mark<std::decay_t<decltype(src)>>)))) return rc;
+    return launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->T, 256); }, SW2_GO(k_wd_flag<std::decay_t<decltype(src)>>));
 }
 
 // residual at the current state: element slots, reference-order gather, norms (async)
 int launch_resid(Runner& R, const std::vector<int>& sub) {
     Phase ph(&R, kPhResid);
-    int rc = launch_map(R, sub, 128, [&](int k) { return nblk(R.ctx[k]->T + R.ctx[k]->E, 128); }, k_resid_elem);
+    int rc = launch_map(R, sub, 128, [&](int k) { return nblk(R.ctx[k]->T + R.ctx[k]->E, 128); }, SW2_GO(k_resid_elem<std::decay_t<decltype(src)>>));
     if (rc) return rc;
     return launch_map(R, sub, kGatherThreads, [&](int k) { return nblk(R.ctx[k]->V, kGatherThreads); },
-                      k_resid_gather);
+                      SW2_GO(k_resid_gather<std::decay_t<decltype(src)>>));
 }
 
 // norms (and Krylov control words) of every instance; the one host sync of an evaluation
@@ -439,13 +460,13 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
     Phase ph(&R, kPhJac);
     auto C = [&](int k) { return R.ctx[k]; };
     // the general list and the wet flags come from the residual evaluated at this same state
-    int rc = launch_map(R, sub, kJacThreads, [&](int k) { return nblk(C(k)->T, kJacElems); }, k_jac_elem_wet);
+    int rc = launch_map(R, sub, kJacThreads, [&](int k) { return nblk(C(k)->T, kJacElems); }, SW2_GO(k_jac_elem_wet<std::decay_t<decltype(src)>>));
     if (rc) return rc;
     if ((rc = launch_map(R, sub, kJacThreads, [&](int k) { return nblk(C(k)->ngeneral, kJacElems); },
-                         k_jac_elem_general)))
+                         SW2_GO(k_jac_elem_general<std::decay_t<decltype(src)>>))))
         return rc;
-    if ((rc = launch_map(R, sub, 128, [&](int k) { return nblk(6LL * C(k)->E, 128); }, k_jac_edge))) return rc;
-    return launch_map(R, sub, 256, [&](int k) { return nblk(9LL * C(k)->nnzb, 256); }, k_jac_gather);
+    if ((rc = launch_map(R, sub, 128, [&](int k) { return nblk(6LL * C(k)->E, 128); }, SW2_GO(k_jac_edge<std::decay_t<decltype(src)>>)))) return rc;
+    return launch_map(R, sub, 256, [&](int k) { return nblk(9LL * C(k)->nnzb, 256); }, SW2_GO(k_jac_gather<std::decay_t<decltype(src)>>));
 }
 
 // Krylov CTAs per instance: shares of the co-resident capacity by block count, at least one,
@@ -477,14 +498,14 @@ std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub) {
 int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<double>& eta, int fix_only_unused = 0) {
     (void)fix_only_unused;
     auto C = [&](int k) { return R.ctx[k]; };
-    int rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, k_rowscale, 0);
+    int rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, SW2_GO(k_rowscale<std::decay_t<decltype(src)>>, 0));
     if (rc) return rc;
     CK(cudaMemsetAsync(R.singular.p, 0, sizeof(int) * R.ctx.size(), R.stream));
-    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, k_fold_diag))) return rc;
+    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, SW2_GO(k_fold_diag<std::decay_t<decltype(src)>>)))) return rc;
     if (R.mixed)
-        rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->nnzb, 256); }, k_fold_offdiag<float>);
+        rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->nnzb, 256); }, SW2_GO_T(k_fold_offdiag, float));
     else
-        rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->nnzb, 256); }, k_fold_offdiag<double>);
+        rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->nnzb, 256); }, SW2_GO_T(k_fold_offdiag, double));
     if (rc) return rc;
     CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * R.ctx.size(), R.stream));
     Phase ph(&R, kPhKrylov);
@@ -495,31 +516,41 @@ int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<doub
         for (size_t j = j0; j < sub.size() && (int)grp.size() < R.capacity; j++) grp.push_back(sub[j]);
         j0 += grp.size();
         const std::vector<int> P = krylov_shares(R, grp);
-        static thread_local KrylovLaunch L;   // ~4 KB: not on the stack of every caller
-        int off = 0;
-        L.mp.n = (int)grp.size();
-        for (size_t j = 0; j < grp.size(); j++) {
-            L.mp.boff[j] = off;
-            L.mp.ids[j] = grp[j];
-            L.rtol[j] = eta[grp[j]];
-            off += P[j];
+        const StageLayout lay{R.c_off, R.r_off, R.v_off, R.stage_bytes};
+        int total = 0;
+        for (int q : P) total += q;
+        if (grp.size() == 1) {
+            KrylovOne one;
+            one.Q = R.ktab_h[grp[0]];
+            one.rtol = eta[grp[0]];
+            one.lay = lay;
+            void* args[] = {(void*)&one};
+            void* kern = R.mixed ? krylov_kernel<float, KrylovOne>(R.staged) : krylov_kernel<double, KrylovOne>(R.staged);
+            CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kKrylovThreads), args, R.smem, R.stream));
+        } else {
+            static thread_local KrylovTab t;   // ~4 KB: not on the stack of every caller
+            int off = 0;
+            t.tab = R.ktab.p;
+            t.mp.n = (int)grp.size();
+            for (size_t j = 0; j < grp.size(); j++) {
+                t.mp.boff[j] = off;
+                t.mp.ids[j] = grp[j];
+                t.rtol[j] = eta[grp[j]];
+                off += P[j];
+            }
+            t.mp.boff[grp.size()] = off;
+            t.lay = lay;
+            void* args[] = {(void*)&t};
+            void* kern = R.mixed ? krylov_kernel<float, KrylovTab>(R.staged) : krylov_kernel<double, KrylovTab>(R.staged);
+            CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kKrylovThreads), args, R.smem, R.stream));
         }
-        L.mp.boff[grp.size()] = off;
-        L.c_off = R.c_off;
-        L.r_off = R.r_off;
-        L.v_off = R.v_off;
-        L.stage_bytes = R.stage_bytes;
-        const KrylovInst* tab = R.ktab.p;
-        void* args[] = {(void*)&tab, (void*)&L};
-        void* kern = R.mixed ? krylov_kernel<float>(R.staged) : krylov_kernel<double>(R.staged);
-        CK(cudaLaunchCooperativeKernel(kern, dim3(off), dim3(kKrylovThreads), args, R.smem, R.stream));
         R.launches++;
     }
     return 0;
 }
 
 int launch_half_inc(Runner& R, const std::vector<int>& sub) {
-    return launch_map(R, sub, 256, [&](int k) { return nblk(R.ctx[k]->V, 256); }, k_half_inc);
+    return launch_map(R, sub, 256, [&](int k) { return nblk(R.ctx[k]->V, 256); }, SW2_GO(k_half_inc<std::decay_t<decltype(src)>>));
 }
 
 // One time step of every instance (fe_sw2 level shift + fe_newton), the instances in
@@ -1019,12 +1050,12 @@ int sw2gpu_load(sw2gpu_ctx* c, int32_t* nnzb, int32_t* row_ptr, int32_t* col, do
     if (rc) return rc;
     // element classification for the two Jacobian kernels (sw2gpu_step takes it from the
     // residual pass at the same state); R is the last sw2gpu_resid's, as in fe_newton
-    if ((rc = launch_map(R, one, 256, [&](int) { return nblk(c->T, 256); }, k_classify))) return rc;
+    if ((rc = launch_map(R, one, 256, [&](int) { return nblk(c->T, 256); }, SW2_GO(k_classify<std::decay_t<decltype(src)>>)))) return rc;
     CK(cudaMemcpyAsync(&R.norms.p[0].ngeneral, c->gcount.p, sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemsetAsync(c->gcount.p, 0, sizeof(int), c->stream));
     if ((rc = read_results(R))) return rc;
     if ((rc = launch_jacobian(R, one))) return rc;
-    if ((rc = launch_map(R, one, 256, [&](int) { return nblk(c->V, 256); }, k_rowscale, 1))) return rc;
+    if ((rc = launch_map(R, one, 256, [&](int) { return nblk(c->V, 256); }, SW2_GO(k_rowscale<std::decay_t<decltype(src)>>, 1)))) return rc;
     if (row_ptr) memcpy(row_ptr, c->rowptr_h.data(), sizeof(int) * (c->V + 1));
     if (col) memcpy(col, c->col_h.data(), sizeof(int) * c->nnzb);
     if (val) CK(cudaMemcpyAsync(val, c->val.p, sizeof(double) * 9 * (size_t)c->nnzb, cudaMemcpyDeviceToHost, c->stream));

@@ -45,8 +45,7 @@ constexpr size_t kOffA = kOffDinv + al(9ull * kMaxNodes);
 constexpr size_t kOffRp = kOffA + al(9ull * kMaxBlocks);
 constexpr size_t kOffCol = kOffRp + al((kMaxNodes + 2) / 2);
 constexpr size_t kOffVec = kOffCol + al((kMaxBlocks + 1) / 2);
-constexpr size_t kOffInst = kOffVec + 8 * al(3ull * kMaxNodes);   // the Krylov launch's instance record
-constexpr size_t kScratchDoubles = kOffInst + al((sizeof(KrylovInst) + 7) / 8);
+constexpr size_t kScratchDoubles = kOffVec + 8 * al(3ull * kMaxNodes);
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
@@ -130,10 +129,6 @@ __global__ void k_na_fold(int V, const int* __restrict__ rowptr, const int* __re
     }
 }
 
-// writes the instance record of the Krylov launch into the scratch array (a kernel argument
-// copied on the device: no host staging buffer)
-__global__ void k_na_put(KrylovInst q, KrylovInst* dst) { *dst = q; }
-
 // device address of the scratch array for the current device (looked up once per device)
 int scratch_for_current_device(double** out) {
     int dev = 0;
@@ -189,11 +184,12 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double, false>, kKrylovThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double, false, KrylovOne>, kKrylovThreads, 0);
     const int grid = std::max(1, std::min({kMaxGrid, (nnodes + kKrylovThreads - 1) / kKrylovThreads,
                                            sms * std::max(per_sm, 1)}));
-    KrylovInst Q;
-    KrylovArgs& K = Q.K;
+    // one instance, direct sweeps (no tile ring); the record is a kernel parameter
+    static thread_local KrylovOne one;
+    KrylovArgs& K = one.Q.K;
     K.V = nnodes;
     K.rowptr = orp;
     K.col = ocol;
@@ -207,22 +203,13 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     K.part = part;
     K.ctl = ctl;
     K.vgrid = grid;
-    Q.A = A;
-    Q.Dinv = dinv;
-    for (int k = 0; k < 8; k++) Q.vec[k] = v[k];
-    KrylovInst* qdev = reinterpret_cast<KrylovInst*>(sc + kOffInst);
-    k_na_put<<<1, 1, 0, st>>>(Q, qdev);
-    // one instance, direct sweeps (no tile ring)
-    static thread_local KrylovLaunch L;
-    L.mp.n = 1;
-    L.mp.boff[0] = 0;
-    L.mp.boff[1] = grid;
-    L.mp.ids[0] = 0;
-    L.rtol[0] = rtol;
-    L.c_off = L.r_off = L.v_off = L.stage_bytes = 0;
-    const KrylovInst* tabp = qdev;
-    void* args[] = {(void*)&tabp, (void*)&L};
-    cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double, false>, dim3(grid),
+    one.Q.A = A;
+    one.Q.Dinv = dinv;
+    for (int k = 0; k < 8; k++) one.Q.vec[k] = v[k];
+    one.rtol = rtol;
+    one.lay = StageLayout{0, 0, 0, 0};
+    void* args[] = {(void*)&one};
+    cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double, false, KrylovOne>, dim3(grid),
                                                 dim3(kKrylovThreads), args, 0, st);
     if (e != cudaSuccess) return na_fail(SW2GPU_E_CUDA, cudaGetErrorString(e));
     KrylovCtl h;

@@ -50,33 +50,64 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clocks, power and clock-event (throttle) reasons sampled during the timed region:
+    NVML every 20 ms (read-only queries), else nvidia-smi every 200 ms."""
 
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.rows = []
+        self.rows = []          # (sm_mhz, max_mhz, set of active reasons)
         self._stop = threading.Event()
         self._t = None
 
-    def _run(self):
+    def _run_nvml(self, nv):
+        h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            try:
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            self.rows.append((float(sm), float(mx), {k for k, b in self.REASONS.items() if bits & b}))
+            self._stop.wait(0.02)
+
+    def _run_smi(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
                                       "--format=csv,noheader,nounits"], capture_output=True, text=True,
                                      timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([c.strip() for c in out.split(",")])
+                r = [c.strip() for c in out.split(",")]
+                if len(r) >= 9 and r[1].replace(".", "").isdigit():
+                    self.rows.append((float(r[1]), float(r[2]), {names[i] for i in range(4) if r[5 + i] == "Active"}))
             except Exception:
                 pass
             self._stop.wait(0.2)
 
+    def _run(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+        except Exception:
+            nv = None
+        if nv is None:
+            self._run_smi()
+            return
+        try:
+            self._run_nvml(nv)
+        except Exception:
+            self._run_smi()
+
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        time.sleep(0.05)
         return self
 
     def __exit__(self, *a):
@@ -86,18 +117,132 @@ class ClockSampler:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted(set().union(*[r[2] for r in self.rows])), "samples": len(self.rows)}
 
 
 def config2_model(points: int, nsteps: int):
     from adhv8_kraken_b200 import meshgen
     size = 20000.0 * math.sqrt(points / 5e5)
     return meshgen.bumpy_basin(points, seed=2024, size=size, nsteps=nsteps, dt=5.0, name="config2")
+
+
+def _ensemble_member(args):
+    seed, nsteps = args
+    from adhv8_kraken_b200 import meshgen
+    return meshgen.ensemble_member(seed, nsteps=nsteps)
+
+
+def ensemble_models(n: int, nsteps: int, seed0: int = 7000, procs: int = 0):
+    """The batched-ensemble instances (triangle count log-uniform 5k-200k, own bathymetry
+    seed, Manning median U[0.015, 0.05], inflow peak U[1, 8], dt U[2, 10]), generated in a
+    spawn-started process pool (before any CUDA work in this process)."""
+    from multiprocessing import get_context
+    procs = procs or max(1, min(32, (os.cpu_count() or 2) - 1))
+    with get_context("spawn").Pool(procs) as pool:
+        return pool.map(_ensemble_member, [(seed0 + i, nsteps) for i in range(n)])
+
+
+def run_ensemble(models, stream, rounds: int):
+    """Config-4 legs on the same instances and rounds (one step attempt per instance per
+    round; a failed step is retried next round with dt / 4, as the reference's time loop
+    does, and counts as wasted time):
+
+    * plain FP64 -- each instance stepped alone, one after the other (the drop-in path);
+    * batched FP64 and batched mixed -- all instances in one batch (sw2gpu_batch_step).
+
+    Throughput = sum over instances of triangles x completed steps / device time."""
+    import torch
+    from adhv8_kraken_b200 import capi
+    from adhv8_kraken_b200.sw2 import SW2Batch, SW2GPU
+
+    tri = np.array([m.nelems2d for m in models], dtype=np.float64)
+
+    def reset(gs):
+        for g in gs:
+            for lvl in range(3):
+                g.set_state(lvl, g.model.h0, g.model.u0, g.model.v0)
+            g.t = g.model.t0
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def rounds_alone(gs):
+        dts = [g.model.dt for g in gs]
+        done = np.zeros(len(gs))
+        for _ in range(rounds):
+            for k, g in enumerate(gs):
+                st = g.step(dt=dts[k])
+                if st["status"] == 0:
+                    done[k] += 1
+                else:
+                    dts[k] *= 0.25
+        return done
+
+    def rounds_batch(b, gs):
+        dts = [g.model.dt for g in gs]
+        done = np.zeros(len(gs))
+        for _ in range(rounds):
+            sts = b.step(dts)
+            for k, st in enumerate(sts):
+                if st["status"] == 0:
+                    done[k] += 1
+                else:
+                    dts[k] *= 0.25
+        return done
+
+    out = {}
+    g64 = [SW2GPU(m, precision=capi.SW2GPU_FP64, stream=stream.cuda_stream) for m in models]
+    for g in g64:            # warm-up: one step each, then back to the initial state
+        g.step()
+    reset(g64)
+    ms, done = timed(lambda: rounds_alone(g64))
+    out["plain_fp64"] = {"value": float((tri * done).sum() / (ms * 1e-3)), "ms_per_round": ms / rounds,
+                         "failed_steps": int(rounds * len(models) - done.sum())}
+    plain_state = [g.get_state(0) for g in g64]
+    reset(g64)
+    b64 = SW2Batch(g64, stream=stream.cuda_stream)
+    b64.step()
+    reset(g64)
+    ms, done = timed(lambda: rounds_batch(b64, g64))
+    out["batched_fp64"] = {"value": float((tri * done).sum() / (ms * 1e-3)), "ms_per_round": ms / rounds,
+                           "failed_steps": int(rounds * len(models) - done.sum())}
+    b64_state = [g.get_state(0) for g in g64]
+    out["batched_fp64"]["bitwise_equal_to_plain"] = bool(all(
+        all(np.array_equal(x, y) for x, y in zip(a, c)) for a, c in zip(plain_state, b64_state)))
+    b64.close()
+    for g in g64:
+        g.close()
+    gm = [SW2GPU(m, precision=capi.SW2GPU_MIXED, stream=stream.cuda_stream) for m in models]
+    bm = SW2Batch(gm, stream=stream.cuda_stream)
+    bm.step()
+    reset(gm)
+    ms, done = timed(lambda: rounds_batch(bm, gm))
+    eh = eq = 0.0
+    for g, ref in zip(gm, b64_state):
+        h, u, v = g.get_state(0)
+        eh = max(eh, float(np.abs(h - ref[0]).max() / max(np.abs(ref[0]).max(), 1e-300)))
+        dq = np.hypot(h * u - ref[0] * ref[1], h * v - ref[0] * ref[2])
+        eq = max(eq, float(dq.max() / max(np.hypot(ref[0] * ref[1], ref[0] * ref[2]).max(), 1e-300)))
+    out["batched_mixed"] = {"value": float((tri * done).sum() / (ms * 1e-3)), "ms_per_round": ms / rounds,
+                            "failed_steps": int(rounds * len(models) - done.sum()),
+                            "max_rel_err_vs_fp64": {"h": eh, "q": eq}}
+    bm.close()
+    for g in gm:
+        g.close()
+    out["workload"] = (f"batched ensemble: {len(models)} seeded basins, triangles log-uniform 5k-200k "
+                       f"(total {int(tri.sum())}), own bathymetry, Manning median U[0.015,0.05], inflow peak "
+                       f"U[1,8] m^2/s, dt U[2,10] s; {rounds} rounds of one step per instance")
+    out["instances"] = len(models)
+    out["triangles"] = int(tri.sum())
+    out["rounds"] = rounds
+    return out
 
 
 def cpu_reference_sample(points: int = 10000, steps: int = 4, procs: int = 1, timeout: float = 600.0):
@@ -152,7 +297,7 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
-def run_ours(args, rank, world, local_rank):
+def run_ours(args, rank, world, local_rank, ens_models=None):
     import torch
     import torch.distributed as dist
     from adhv8_kraken_b200 import capi
@@ -287,6 +432,11 @@ def run_ours(args, rank, world, local_rank):
              "max_rel_err_vs_fp64": err, "newton_its": sum(s["newton_its"] for s in mstats),
              "linear_its": sum(s["linear_its"] for s in mstats)}
 
+    # ---- batched ensemble (plain FP64 alone vs batched FP64 vs batched mixed)
+    batched = None
+    if ens_models:
+        batched = run_ensemble(ens_models, stream, args.ens_steps)
+
     if rank != 0:
         return
     cpu = None
@@ -314,6 +464,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline,
         "e2e": e2e,
         "mixed": mixed,
+        "batched": batched,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
@@ -328,6 +479,8 @@ def main():
     ap.add_argument("--points", type=int, default=500000)
     ap.add_argument("--ref-points", type=int, default=10000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ens", type=int, default=256, help="batched-ensemble instances (0: skip the leg)")
+    ap.add_argument("--ens-steps", type=int, default=20, help="rounds of the ensemble legs")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -341,8 +494,12 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if world > 1:
+        args.ens = 0   # the ensemble legs are a single-GPU measurement
+    ens = ensemble_models(args.ens, nsteps=args.ens_steps,
+                          procs=max(1, ((os.cpu_count() or 2) - 1) // world)) if args.ens > 0 else None
     try:
-        run_ours(args, rank, world, local_rank)
+        run_ours(args, rank, world, local_rank, ens)
     finally:
         if world > 1:
             import torch.distributed as dist
