@@ -75,6 +75,18 @@ def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
 
 
+class RunStats(C.Structure):
+    """sw2gpu_run_stats: one instance that left a continuous-batching engine."""
+    _fields_ = [
+        ("id", C.c_int64), ("status", C.c_int32), ("steps", C.c_int32), ("failures", C.c_int32),
+        ("newton_its", C.c_int32), ("linear_its", C.c_int32), ("ticks", C.c_int32), ("t", C.c_double),
+        ("dt", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class MeshArrays:
     """Owns the numpy buffers behind a :class:`Mesh` struct."""
 

@@ -56,6 +56,8 @@ struct __align__(16) Inst {
     void* aoff;                 // folded off-diagonal blocks (MT of the Krylov launch)
     unsigned char *ewet, *mark;
     int *glist, *gcount;
+    int* ngen;                  // general-list length of the last residual evaluation (the
+                                // instance's own word: it outlives the batch slot of `norms`)
     Norms* npart;               // per-gather-block partials
     Norms* norms;               // result of the last residual evaluation
     unsigned* ncounter;
@@ -313,7 +315,9 @@ __global__ void __launch_bounds__(kGatherThreads) k_resid_gather(const __grid_co
         }
         block_reduce3<kGatherThreads>(a, b, c, d);
         if (threadIdx.x == 0) {
-            *out = Norms{a, b, c, d, *(volatile int*)gcount};
+            const int ng = *(volatile int*)gcount;
+            *out = Norms{a, b, c, d, ng};
+            *I.ngen = ng;
             *gcount = 0;
             *counter = 0u;
         }
@@ -471,7 +475,7 @@ __global__ void __launch_bounds__(kJacThreads) k_jac_elem_general(const __grid_c
     const DevMesh m = I.m;
     const State s = I.s;
     const PhysParams P = I.P;
-    jac_elem_body<true>(m, s, P, I.jslots, nullptr, I.glist, I.norms->ngeneral, lb);
+    jac_elem_body<true>(m, s, P, I.jslots, nullptr, I.glist, *I.ngen, lb);
 }
 
 // FD Jacobian of the boundary edges: one thread per (edge, node, variable); writes the

@@ -97,6 +97,7 @@ struct sw2gpu_ctx {
     DBuf<int> wd;
     DBuf<unsigned char> ewet;    // element takes the fully wet Jacobian path
     DBuf<int> glist, gcount;     // elements on the general (wet/dry) Jacobian path
+    DBuf<int> ngen;              // its length at the last residual evaluation (device copy)
     int ngeneral = 0;            // its length at the last residual evaluation
     // work
     DBuf<double> sc, sx, sy, R, sol, jslots, val, S_, bs;
@@ -188,6 +189,7 @@ struct Runner {
     unsigned c_off = 0, r_off = 0, v_off = 0, stage_bytes = 0;
     size_t smem = 0;
     int capacity = 0;             // co-resident Krylov CTAs
+    int cap = 0;                  // instances the tables hold
     int launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     static constexpr int kMaxPhases = 512;
@@ -285,23 +287,34 @@ int upload_step_tables(sw2gpu_ctx* c, const double* series, cudaStream_t st) {
 
 // ---- runner ------------------------------------------------------------------------
 
-int runner_init(Runner& R, const std::vector<sw2gpu_ctx*>& ctx, cudaStream_t stream) {
-    if (ctx.empty() || (int)ctx.size() > kMaxBatch) return fail(SW2GPU_E_ARG, "batch of %zu instances (1..%d)", ctx.size(), kMaxBatch);
-    R.ctx = ctx;
+// per-instance device arrays and pinned mirrors for up to `cap` instances, timing events
+int runner_alloc(Runner& R, cudaStream_t stream, bool mixed, int cap) {
     R.stream = stream;
-    R.mixed = ctx[0]->p.precision == SW2GPU_MIXED;
+    R.mixed = mixed;
+    R.cap = cap;
+    if (R.tab.alloc(cap) || R.ktab.alloc(cap) || R.norms.alloc(cap) || R.ctl.alloc(cap) || R.singular.alloc(cap))
+        return fail(SW2GPU_E_NOMEM, "batch tables");
+    CK(cudaMemsetAsync(R.norms.p, 0, sizeof(Norms) * cap, stream));
+    CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * cap, stream));
+    CK(cudaMallocHost(&R.norms_h, sizeof(Norms) * cap));
+    CK(cudaMallocHost(&R.ctl_h, sizeof(KrylovCtl) * cap));
+    R.tab_h.resize(cap);
+    R.ktab_h.resize(cap);
+    CK(cudaEventCreate(&R.ev0));
+    CK(cudaEventCreate(&R.ev1));
+    R.pev.resize(2 * Runner::kMaxPhases);
+    R.pkind.resize(Runner::kMaxPhases);
+    for (auto& e : R.pev) CK(cudaEventCreate(&e));
+    return 0;
+}
+
+// the instances of the runner (at most its capacity, one precision) and the Krylov launch
+// configuration for them: stage layout for the largest tile of any instance, co-resident CTAs
+int runner_set(Runner& R, const std::vector<sw2gpu_ctx*>& ctx) {
+    if ((int)ctx.size() > R.cap) return fail(SW2GPU_E_ARG, "batch of %zu instances (at most %d)", ctx.size(), R.cap);
     for (auto* c : ctx)
         if ((c->p.precision == SW2GPU_MIXED) != R.mixed) return fail(SW2GPU_E_ARG, "a batch has one precision");
-    const int K = (int)ctx.size();
-    if (R.tab.alloc(K) || R.ktab.alloc(K) || R.norms.alloc(K) || R.ctl.alloc(K) || R.singular.alloc(K))
-        return fail(SW2GPU_E_NOMEM, "batch tables");
-    CK(cudaMemsetAsync(R.norms.p, 0, sizeof(Norms) * K, stream));
-    CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * K, stream));
-    CK(cudaMallocHost(&R.norms_h, sizeof(Norms) * K));
-    CK(cudaMallocHost(&R.ctl_h, sizeof(KrylovCtl) * K));
-    R.tab_h.resize(K);
-    R.ktab_h.resize(K);
-    // Krylov launch: stage layout for the largest tile of any instance
+    R.ctx = ctx;
     unsigned a_cap = 16, c_cap = 16;
     for (auto* c : ctx) {
         a_cap = std::max(a_cap, c->a_cap);
@@ -310,7 +323,12 @@ int runner_init(Runner& R, const std::vector<sw2gpu_ctx*>& ctx, cudaStream_t str
     const unsigned c_off = a_cap, r_off = c_off + c_cap;
     const unsigned v_off = r_off + ((unsigned)(kTileRows + 1) * 4u + 15u) / 16u * 16u;
     const unsigned stage = (v_off + 3u * tile_vec_bytes<double>() + 127u) & ~127u;
-    R.staged = (size_t)kStages * stage <= kMaxStagedSmem;
+    const bool staged = (size_t)kStages * stage <= kMaxStagedSmem;
+    if (R.capacity > 0 && staged == R.staged &&
+        (!staged || (a_cap <= R.c_off && c_cap <= R.r_off - R.c_off)))
+        return 0;   // the current layout still holds every tile
+    R.staged = staged;
+    R.c_off = R.r_off = R.v_off = R.stage_bytes = 0;
     if (R.staged) {
         R.c_off = c_off;
         R.r_off = r_off;
@@ -334,12 +352,13 @@ int runner_init(Runner& R, const std::vector<sw2gpu_ctx*>& ctx, cudaStream_t str
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tab, ktab, kKrylovThreads, R.smem));
     per_sm = std::min(per_sm, per_sm_tab);
     R.capacity = sms * std::max(1, std::min(per_sm, 4));
-    CK(cudaEventCreate(&R.ev0));
-    CK(cudaEventCreate(&R.ev1));
-    R.pev.resize(2 * Runner::kMaxPhases);
-    R.pkind.resize(Runner::kMaxPhases);
-    for (auto& e : R.pev) CK(cudaEventCreate(&e));
     return 0;
+}
+
+int runner_init(Runner& R, const std::vector<sw2gpu_ctx*>& ctx, cudaStream_t stream) {
+    if (ctx.empty() || (int)ctx.size() > kMaxBatch) return fail(SW2GPU_E_ARG, "batch of %zu instances (1..%d)", ctx.size(), kMaxBatch);
+    int rc = runner_alloc(R, stream, ctx[0]->p.precision == SW2GPU_MIXED, (int)ctx.size());
+    return rc ? rc : runner_set(R, ctx);
 }
 
 // device tables from the instances' current buffers and state levels
@@ -355,7 +374,7 @@ int runner_tables(Runner& R, int apply_inc) {
         I.R = c->R.p; I.sol = c->sol.p; I.jslots = c->jslots.p; I.val = c->val.p;
         I.S = c->S_.p; I.bs = c->bs.p; I.dinv = c->dinv64.p;
         I.aoff = R.mixed ? (void*)c->aoff32.p : (void*)c->aoff64.p;
-        I.ewet = c->ewet.p; I.mark = c->mark.p; I.glist = c->glist.p; I.gcount = c->gcount.p;
+        I.ewet = c->ewet.p; I.mark = c->mark.p; I.glist = c->glist.p; I.gcount = c->gcount.p; I.ngen = c->ngen.p;
         I.npart = c->npart.p; I.norms = R.norms.p + k; I.ncounter = c->ncounter.p; I.singular = R.singular.p + k;
         I.ndir = (int)c->dir_node.size();
         I.dir_node = c->dir_node_d.p; I.dir_mask = c->dir_mask_d.p;
@@ -553,6 +572,129 @@ int launch_half_inc(Runner& R, const std::vector<int>& sub) {
     return launch_map(R, sub, 256, [&](int k) { return nblk(R.ctx[k]->V, 256); }, SW2_GO(k_half_inc<std::decay_t<decltype(src)>>));
 }
 
+// Newton state of one instance inside a time step (fe_newton.c:214-912)
+struct NState {
+    double rmax = 0, l2 = 0, imax = 0, old_l2 = 0, eta = 0;
+    int it = 0, lin = 0, cuts = 0, cuts_total = 0;
+    bool ok = true, nan = false, done = false;
+};
+
+// Inexact Newton: the linear residual of iteration k only needs to be small next to the
+// Newton tolerance, so the Krylov test is relative with
+//   eta_k = max(lin_rtol, kEtaNtl * tol_nonlin / max|R_k|)      (capped at 1e-5).
+// Early iterations (large R) solve to near round-off like the reference's exact LU; late
+// ones (R close to tol_nonlin) stop early.  A solve that reaches max_lin_it but reduced its
+// residual by kAcceptRel is accepted: its error is already far below what the next residual
+// evaluation can see.
+constexpr double kEtaNtl = 1e-4, kAcceptRel = 1e-8;
+
+// the state after the residual at the start of a step (norms read)
+void newton_begin(Runner& R, int k, NState& ns) {
+    const Norms& nm = R.norms_h[k];
+    ns = NState();
+    ns.rmax = nm.rmax;
+    ns.l2 = std::sqrt(nm.l2sum / (3.0 * R.ctx[k]->V));
+    ns.imax = nm.imax;
+    if (nm.nan) {
+        ns.nan = true;
+        ns.ok = false;
+        ns.done = true;
+    }
+}
+
+// one Newton iteration (Jacobian, Krylov, update, residual, line search, convergence test) of
+// every instance of `act`, each in one launch per phase; sets ns[k].done when k's step ends
+int newton_iteration(Runner& R, const std::vector<int>& act, std::vector<NState>& ns) {
+    int rc = launch_jacobian(R, act);
+    if (rc) return rc;
+    std::vector<double> eta(R.ctx.size(), 0.0);
+    for (int k : act) {
+        const sw2gpu_params& p = R.ctx[k]->p;
+        eta[k] = std::min(1e-5, std::max(p.lin_rtol, kEtaNtl * p.tol_nonlin / std::max(ns[k].rmax, 1e-300)));
+    }
+    if ((rc = launch_linear(R, act, eta))) return rc;
+    for (int k : act) ns[k].old_l2 = ns[k].l2;
+    if ((rc = launch_resid(R, act))) return rc;
+    if ((rc = read_results(R))) return rc;
+    std::vector<int> ls;
+    for (int k : act) {
+        NState& n = ns[k];
+        const sw2gpu_params& p = R.ctx[k]->p;
+        const KrylovCtl& q = R.ctl_h[k];
+        if (q.err) return fail(SW2GPU_E_TIMEOUT, "instance %d: Krylov barrier or tile-copy wait ran out", k);
+        n.lin += q.iterations;
+        // the plain path fails the step when BiCGSTAB hits max_lin_it without a useful
+        // reduction (solv_bcgstab.c:280-292); on the mixed path the FP32 inner solve is a
+        // correction refined by the FP64 Newton loop, so its last iterate is accepted (the
+        // reference's force_lin_it behaviour)
+        if (!q.converged && p.precision != SW2GPU_MIXED && !(q.rnorm <= kAcceptRel * q.bnorm)) n.ok = false;
+        const Norms& nm = R.norms_h[k];
+        n.rmax = nm.rmax;
+        n.l2 = std::sqrt(nm.l2sum / (3.0 * R.ctx[k]->V));
+        n.imax = nm.imax;
+        if (nm.nan || std::isnan(n.l2) || std::isinf(n.l2)) {
+            n.ok = false;
+            n.nan = true;
+        }
+        n.cuts = 0;
+        if (n.rmax > p.tol_nonlin && n.l2 > n.old_l2 && n.cuts < p.max_linesearch_cuts) ls.push_back(k);
+    }
+    // line search (fe_newton.c:692-747): halve the increment while the l2 norm grew
+    while (!ls.empty()) {
+        if ((rc = launch_half_inc(R, ls))) return rc;
+        if ((rc = launch_resid(R, ls))) return rc;
+        if ((rc = read_results(R))) return rc;
+        std::vector<int> next;
+        for (int k : ls) {
+            NState& n = ns[k];
+            const sw2gpu_params& p = R.ctx[k]->p;
+            const Norms& nm = R.norms_h[k];
+            n.rmax = nm.rmax;
+            n.l2 = std::sqrt(nm.l2sum / (3.0 * R.ctx[k]->V));
+            n.imax = nm.imax;
+            n.cuts++;
+            if (n.rmax > p.tol_nonlin && n.l2 > n.old_l2 && n.cuts < p.max_linesearch_cuts) next.push_back(k);
+        }
+        ls.swap(next);
+    }
+    for (int k : act) {
+        NState& n = ns[k];
+        const sw2gpu_params& p = R.ctx[k]->p;
+        n.cuts_total += n.cuts;
+        n.it++;
+        const bool keep = n.ok && n.it < p.max_nonlin_it && n.rmax < 1.0E+20 && (n.rmax > p.tol_nonlin && n.imax > p.inc_nonlin);
+        if (!keep) n.done = true;
+    }
+    return 0;
+}
+
+// status of a finished step (0 = YES)
+int newton_status(const NState& n, const sw2gpu_params& p) {
+    if (!n.ok || (n.rmax > p.tol_nonlin && n.imax > p.inc_nonlin) || n.rmax >= 1.0E+20)
+        return n.nan ? SW2GPU_E_NAN : (!n.ok ? SW2GPU_E_LINEAR : SW2GPU_E_NEWTON);
+    return SW2GPU_OK;
+}
+
+// start of a step for instance k: dt, level rotation (fe_sw2: older <- old <- current, no
+// copies) and the step tables
+int step_begin(Runner& R, int k, double dt, const double* series) {
+    sw2gpu_ctx* c = R.ctx[k];
+    c->dt = dt;
+    const int o2 = c->lv[2];
+    c->lv[2] = c->lv[1];
+    c->lv[1] = c->lv[0];
+    c->lv[0] = o2;
+    return upload_step_tables(c, series, R.stream);
+}
+
+void phase_times(Runner& R, double ph[3]) {
+    ph[0] = ph[1] = ph[2] = 0.0;
+    for (int q = 0; q < R.nphase; q++) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, R.pev[2 * q], R.pev[2 * q + 1]) == cudaSuccess) ph[R.pkind[q]] += t;
+    }
+}
+
 // One time step of every instance (fe_sw2 level shift + fe_newton), the instances in
 // lockstep: each Newton phase is one launch over the instances still iterating, and each
 // instance follows exactly the decisions it takes alone.
@@ -564,136 +706,47 @@ int runner_step(Runner& R, const double* dt, const double* const* series, sw2gpu
     R.nphase = 0;
     CK(cudaEventRecord(R.ev0, R.stream));
     int rc = 0;
-    for (int k = 0; k < K; k++) {
-        sw2gpu_ctx* c = R.ctx[k];
-        c->dt = dt[k];
-        const int o2 = c->lv[2];   // fe_sw2: older <- old <- current (level rotation, no copies)
-        c->lv[2] = c->lv[1];
-        c->lv[1] = c->lv[0];
-        c->lv[0] = o2;
-        if ((rc = upload_step_tables(c, series ? series[k] : nullptr, R.stream))) return rc;
-    }
+    for (int k = 0; k < K; k++)
+        if ((rc = step_begin(R, k, dt[k], series ? series[k] : nullptr))) return rc;
     if ((rc = runner_tables(R, 1))) return rc;
     std::vector<int> all(K);
     for (int k = 0; k < K; k++) all[k] = k;
     if ((rc = launch_init(R, all))) return rc;
     if ((rc = launch_resid(R, all))) return rc;
     if ((rc = read_results(R))) return rc;
-    // Inexact Newton: the linear residual of iteration k only needs to be small next to
-    // the Newton tolerance, so the Krylov test is relative with
-    //   eta_k = max(lin_rtol, kEtaNtl * tol_nonlin / max|R_k|)      (capped at 1e-5).
-    // Early iterations (large R) solve to near round-off like the reference's exact LU;
-    // late ones (R close to tol_nonlin) stop early.  A solve that reaches max_lin_it
-    // but reduced its residual by kAcceptRel is accepted: its error is already far below
-    // what the next residual evaluation can see.
-    constexpr double kEtaNtl = 1e-4, kAcceptRel = 1e-8;
-    std::vector<double> rmax(K), l2(K), imax(K), old_l2(K, 0.0), eta(K, 0.0);
-    std::vector<int> it(K, 0), lin(K, 0), cuts(K, 0), cuts_total(K, 0);
-    std::vector<char> ok(K, 1), nan(K, 0), done(K, 0);
-    for (int k = 0; k < K; k++) {
-        const Norms& nm = R.norms_h[k];
-        const double n3 = 3.0 * R.ctx[k]->V;
-        rmax[k] = nm.rmax;
-        l2[k] = std::sqrt(nm.l2sum / n3);
-        imax[k] = nm.imax;
-        if (nm.nan) {
-            nan[k] = 1;
-            ok[k] = 0;
-            done[k] = 1;
-        }
-    }
+    std::vector<NState> ns(K);
+    for (int k = 0; k < K; k++) newton_begin(R, k, ns[k]);
     for (;;) {
         std::vector<int> act;
         for (int k = 0; k < K; k++)
-            if (!done[k]) act.push_back(k);
+            if (!ns[k].done) act.push_back(k);
         if (act.empty()) break;
-        if ((rc = launch_jacobian(R, act))) return rc;
-        for (int k : act) {
-            const sw2gpu_params& p = R.ctx[k]->p;
-            eta[k] = std::min(1e-5, std::max(p.lin_rtol, kEtaNtl * p.tol_nonlin / std::max(rmax[k], 1e-300)));
-        }
-        if ((rc = launch_linear(R, act, eta))) return rc;
-        for (int k : act) old_l2[k] = l2[k];
-        if ((rc = launch_resid(R, act))) return rc;
-        if ((rc = read_results(R))) return rc;
-        std::vector<int> ls;
-        for (int k : act) {
-            const sw2gpu_params& p = R.ctx[k]->p;
-            const KrylovCtl& q = R.ctl_h[k];
-            if (q.err) return fail(SW2GPU_E_TIMEOUT, "instance %d: Krylov barrier or tile-copy wait ran out", k);
-            lin[k] += q.iterations;
-            // the plain path fails the step when BiCGSTAB hits max_lin_it without a useful
-            // reduction (solv_bcgstab.c:280-292); on the mixed path the FP32 inner solve is a
-            // correction refined by the FP64 Newton loop, so its last iterate is accepted (the
-            // reference's force_lin_it behaviour)
-            if (!q.converged && p.precision != SW2GPU_MIXED && !(q.rnorm <= kAcceptRel * q.bnorm)) ok[k] = 0;
-            const Norms& nm = R.norms_h[k];
-            rmax[k] = nm.rmax;
-            l2[k] = std::sqrt(nm.l2sum / (3.0 * R.ctx[k]->V));
-            imax[k] = nm.imax;
-            if (nm.nan || std::isnan(l2[k]) || std::isinf(l2[k])) {
-                ok[k] = 0;
-                nan[k] = 1;
-            }
-            cuts[k] = 0;
-            if (rmax[k] > p.tol_nonlin && l2[k] > old_l2[k] && cuts[k] < p.max_linesearch_cuts) ls.push_back(k);
-        }
-        // line search (fe_newton.c:692-747): halve the increment while the l2 norm grew
-        while (!ls.empty()) {
-            if ((rc = launch_half_inc(R, ls))) return rc;
-            if ((rc = launch_resid(R, ls))) return rc;
-            if ((rc = read_results(R))) return rc;
-            std::vector<int> next;
-            for (int k : ls) {
-                const sw2gpu_params& p = R.ctx[k]->p;
-                const Norms& nm = R.norms_h[k];
-                rmax[k] = nm.rmax;
-                l2[k] = std::sqrt(nm.l2sum / (3.0 * R.ctx[k]->V));
-                imax[k] = nm.imax;
-                cuts[k]++;
-                if (rmax[k] > p.tol_nonlin && l2[k] > old_l2[k] && cuts[k] < p.max_linesearch_cuts) next.push_back(k);
-            }
-            ls.swap(next);
-        }
-        for (int k : act) {
-            const sw2gpu_params& p = R.ctx[k]->p;
-            cuts_total[k] += cuts[k];
-            it[k]++;
-            const bool keep = ok[k] && it[k] < p.max_nonlin_it && rmax[k] < 1.0E+20 &&
-                              (rmax[k] > p.tol_nonlin && imax[k] > p.inc_nonlin);
-            if (!keep) done[k] = 1;
-        }
+        if ((rc = newton_iteration(R, act, ns))) return rc;
     }
     std::vector<int> failed;
     for (int k = 0; k < K; k++) {
-        const sw2gpu_params& p = R.ctx[k]->p;
-        status[k] = SW2GPU_OK;
-        if (!ok[k] || (rmax[k] > p.tol_nonlin && imax[k] > p.inc_nonlin) || rmax[k] >= 1.0E+20) {
-            status[k] = nan[k] ? SW2GPU_E_NAN : (!ok[k] ? SW2GPU_E_LINEAR : SW2GPU_E_NEWTON);
-            failed.push_back(k);
-        }
+        status[k] = newton_status(ns[k], R.ctx[k]->p);
+        if (status[k] != SW2GPU_OK) failed.push_back(k);
     }
     if (!failed.empty() && (rc = launch_init(R, failed))) return rc;   // reset to the old level
     CK(cudaEventRecord(R.ev1, R.stream));
     CK(cudaEventSynchronize(R.ev1));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, R.ev0, R.ev1);
-    double ph[3] = {0.0, 0.0, 0.0};
-    for (int q = 0; q < R.nphase; q++) {
-        float t = 0.f;
-        if (cudaEventElapsedTime(&t, R.pev[2 * q], R.pev[2 * q + 1]) == cudaSuccess) ph[R.pkind[q]] += t;
-    }
+    double ph[3];
+    phase_times(R, ph);
     if (stats) {
         for (int k = 0; k < K; k++) {
             sw2gpu_stats& st = stats[k];
+            const NState& n = ns[k];
             memset(&st, 0, sizeof(st));
             st.status = status[k];
-            st.newton_its = it[k];
-            st.linear_its = lin[k];
-            st.linesearch_cuts = cuts_total[k];
-            st.resid_max = rmax[k];
-            st.resid_l2 = l2[k];
-            st.inc_max = imax[k];
+            st.newton_its = n.it;
+            st.linear_its = n.lin;
+            st.linesearch_cuts = n.cuts_total;
+            st.resid_max = n.rmax;
+            st.resid_l2 = n.l2;
+            st.inc_max = n.imax;
             st.device_ms = ms;
             st.kernel_launches = R.launches;
             st.jac_ms = ph[kPhJac];
@@ -918,6 +971,7 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     rc |= zalloc(c->ewet, std::max(T, 1), st);
     rc |= zalloc(c->glist, std::max(T, 1), st);
     rc |= zalloc(c->gcount, 1, st);
+    rc |= zalloc(c->ngen, 1, st);
     rc |= zalloc(c->mark, V, st);
     rc |= zalloc(c->sc, nslot, st); rc |= zalloc(c->sx, nslot, st); rc |= zalloc(c->sy, nslot, st);
     rc |= zalloc(c->R, 3ull * V, st); rc |= zalloc(c->sol, 3ull * V, st);
@@ -1052,6 +1106,7 @@ int sw2gpu_load(sw2gpu_ctx* c, int32_t* nnzb, int32_t* row_ptr, int32_t* col, do
     // residual pass at the same state); R is the last sw2gpu_resid's, as in fe_newton
     if ((rc = launch_map(R, one, 256, [&](int) { return nblk(c->T, 256); }, SW2_GO(k_classify<std::decay_t<decltype(src)>>)))) return rc;
     CK(cudaMemcpyAsync(&R.norms.p[0].ngeneral, c->gcount.p, sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->ngen.p, c->gcount.p, sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemsetAsync(c->gcount.p, 0, sizeof(int), c->stream));
     if ((rc = read_results(R))) return rc;
     if ((rc = launch_jacobian(R, one))) return rc;
@@ -1140,6 +1195,227 @@ int sw2gpu_batch_destroy(sw2gpu_batch* b) {
     b->run.reset();
     if (b->own_stream) cudaStreamDestroy(st);
     delete b;
+    return SW2GPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// continuous batching engine
+
+namespace {
+
+// piecewise-linear series and its average over a step (sseries_set_values_average,
+// src/structs/sseries.c:566-613): exact trapezoid integral over the breakpoints inside the
+// step, end segments extrapolated linearly
+struct PwlSeries {
+    std::vector<double> t, v;
+    double at(double tt) const {
+        const size_t n = t.size();
+        if (n == 1) return v[0];
+        long i = (long)(std::upper_bound(t.begin(), t.end(), tt) - t.begin()) - 1;
+        i = std::min(std::max(i, 0L), (long)n - 2);
+        const double w = (tt - t[i]) / (t[i + 1] - t[i]);
+        return v[i] + w * (v[i + 1] - v[i]);
+    }
+    double avg(double t1, double t2) const {
+        if (t2 <= t1) return at(t1);
+        double area = 0.0, a = t1;
+        for (double x : t) {
+            if (!(t1 < x && x < t2)) continue;
+            area += 0.5 * (at(a) + at(x)) * (x - a);
+            a = x;
+        }
+        area += 0.5 * (at(a) + at(t2)) * (t2 - a);
+        return area / (t2 - t1);
+    }
+};
+
+struct EngInst {
+    sw2gpu_ctx* c = nullptr;
+    int64_t id = 0;
+    double t = 0.0, dt = 0.0, dt0 = 0.0;   // current and base time step
+    int nsteps = 0, steps = 0, failures = 0, consecutive = 0, max_retries = 0, ticks = 0, last_status = 0;
+    long newton = 0, linear = 0;
+    std::vector<PwlSeries> ser;
+    bool in_step = false;
+    NState ns;
+};
+
+}  // namespace
+
+struct sw2gpu_engine {
+    std::unique_ptr<Runner> R;
+    std::vector<EngInst> inst;     // slot k of the runner = inst[k]
+    bool dirty = true;             // membership changed since the runner last saw it
+    bool own_stream = false;
+    int precision = SW2GPU_FP64;
+};
+
+extern "C" {
+
+int sw2gpu_engine_create(int32_t precision, void* stream, sw2gpu_engine** out) {
+    if (!out || (precision != SW2GPU_FP64 && precision != SW2GPU_MIXED)) return fail(SW2GPU_E_ARG, "bad engine arguments");
+    *out = nullptr;
+    auto* e = new sw2gpu_engine();
+    std::unique_ptr<sw2gpu_engine> guard(e);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!st) {
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        e->own_stream = true;
+    }
+    e->precision = precision;
+    e->R.reset(new Runner());
+    int rc = runner_alloc(*e->R, st, precision == SW2GPU_MIXED, kMaxBatch);
+    if (rc) {
+        if (e->own_stream) cudaStreamDestroy(st);
+        return rc;
+    }
+    *out = guard.release();
+    return SW2GPU_OK;
+}
+
+int sw2gpu_engine_add(sw2gpu_engine* e, sw2gpu_ctx* ctx, int64_t id, double t0, double dt, int32_t nsteps,
+                      int32_t max_retries, int32_t nseries, const int32_t* series_len, const double* series_t,
+                      const double* series_v) {
+    if (!e || !ctx || !(dt > 0.0) || nsteps <= 0 || max_retries < 0 || nseries < 0)
+        return fail(SW2GPU_E_ARG, "bad engine_add arguments");
+    if ((int)e->inst.size() >= kMaxBatch) return fail(SW2GPU_E_ARG, "engine holds %d instances already", kMaxBatch);
+    if (ctx->p.precision != e->precision) return fail(SW2GPU_E_ARG, "instance precision differs from the engine's");
+    for (auto& x : e->inst)
+        if (x.c == ctx || x.id == id) return fail(SW2GPU_E_ARG, "instance or id already in the engine");
+    if (nseries < ctx->NS) return fail(SW2GPU_E_ARG, "instance reads %d series, %d given", ctx->NS, nseries);
+    EngInst x;
+    x.c = ctx;
+    x.id = id;
+    x.t = t0;
+    x.dt = x.dt0 = dt;
+    x.nsteps = nsteps;
+    x.max_retries = max_retries;
+    size_t off = 0;
+    for (int s = 0; s < nseries; s++) {
+        const int n = series_len[s];
+        if (n <= 0) return fail(SW2GPU_E_ARG, "series %d is empty", s);
+        PwlSeries ps;
+        ps.t.assign(series_t + off, series_t + off + n);
+        ps.v.assign(series_v + off, series_v + off + n);
+        for (int i = 1; i < n; i++)
+            if (!(ps.t[i] > ps.t[i - 1])) return fail(SW2GPU_E_ARG, "series %d: times not increasing", s);
+        off += n;
+        x.ser.push_back(std::move(ps));
+    }
+    // the instance's own stream may still hold its state uploads: order them first
+    CK(cudaStreamSynchronize(ctx->stream));
+    e->inst.push_back(std::move(x));
+    e->dirty = true;
+    return SW2GPU_OK;
+}
+
+int32_t sw2gpu_engine_active(const sw2gpu_engine* e) { return e ? (int32_t)e->inst.size() : 0; }
+
+int sw2gpu_engine_tick(sw2gpu_engine* e, sw2gpu_run_stats* finished, int32_t max_finished, int32_t* nfinished) {
+    if (!e || !nfinished || (max_finished > 0 && !finished)) return fail(SW2GPU_E_ARG, "bad engine_tick arguments");
+    *nfinished = 0;
+    const int K = (int)e->inst.size();
+    if (K == 0) return SW2GPU_OK;
+    if (max_finished < K) return fail(SW2GPU_E_ARG, "room for %d finished instances needed", K);
+    Runner& R = *e->R;
+    int rc = 0;
+    if (e->dirty) {
+        std::vector<sw2gpu_ctx*> cs;
+        for (auto& x : e->inst) cs.push_back(x.c);
+        if ((rc = runner_set(R, cs))) return rc;
+        e->dirty = false;
+    }
+    R.launches = 0;
+    R.nphase = 0;
+    // instances between steps start one: dt, step-averaged series, level rotation
+    std::vector<int> S;
+    for (int k = 0; k < K; k++) {
+        EngInst& x = e->inst[k];
+        if (x.in_step) continue;
+        std::vector<double> sv(x.ser.size());
+        for (size_t q = 0; q < x.ser.size(); q++) sv[q] = x.ser[q].avg(x.t, x.t + x.dt);
+        if ((rc = step_begin(R, k, x.dt, sv.empty() ? nullptr : sv.data()))) return rc;
+        S.push_back(k);
+    }
+    if ((rc = runner_tables(R, 1))) return rc;
+    if (!S.empty()) {
+        if ((rc = launch_init(R, S))) return rc;
+        if ((rc = launch_resid(R, S))) return rc;
+        if ((rc = read_results(R))) return rc;
+        for (int k : S) {
+            newton_begin(R, k, e->inst[k].ns);
+            e->inst[k].in_step = true;
+        }
+    }
+    // one Newton iteration of every instance inside a step
+    std::vector<int> N;
+    for (int k = 0; k < K; k++)
+        if (e->inst[k].in_step && !e->inst[k].ns.done) N.push_back(k);
+    if (!N.empty()) {
+        std::vector<NState> ns(K);
+        for (int k = 0; k < K; k++) ns[k] = e->inst[k].ns;
+        if ((rc = newton_iteration(R, N, ns))) return rc;
+        for (int k : N) e->inst[k].ns = ns[k];
+    }
+    // steps that ended: advance, or reset to the old level and retry with dt / 4
+    std::vector<int> failed;
+    for (int k = 0; k < K; k++) {
+        EngInst& x = e->inst[k];
+        x.ticks++;
+        if (!x.in_step || !x.ns.done) continue;
+        const int st = newton_status(x.ns, x.c->p);
+        x.newton += x.ns.it;
+        x.linear += x.ns.lin;
+        x.in_step = false;
+        if (st == SW2GPU_OK) {   // the next step runs with the base dt again (as sw2.run does)
+            x.steps++;
+            x.t += x.dt;
+            x.dt = x.dt0;
+            x.consecutive = 0;
+        } else {
+            x.failures++;
+            x.consecutive++;
+            x.last_status = st;
+            x.dt *= 0.25;
+            failed.push_back(k);
+        }
+    }
+    if (!failed.empty() && (rc = launch_init(R, failed))) return rc;
+    CK(cudaStreamSynchronize(R.stream));
+    // instances done with their steps (or out of retries) leave the engine
+    std::vector<EngInst> keep;
+    for (auto& x : e->inst) {
+        const bool gave_up = x.consecutive > x.max_retries;
+        if (x.steps >= x.nsteps || gave_up) {
+            sw2gpu_run_stats& o = finished[(*nfinished)++];
+            memset(&o, 0, sizeof(o));
+            o.id = x.id;
+            o.status = gave_up ? x.last_status : SW2GPU_OK;
+            o.steps = x.steps;
+            o.failures = x.failures;
+            o.newton_its = (int32_t)x.newton;
+            o.linear_its = (int32_t)x.linear;
+            o.ticks = x.ticks;
+            o.t = x.t;
+            o.dt = x.dt;
+            e->dirty = true;
+        } else {
+            keep.push_back(std::move(x));
+        }
+    }
+    e->inst.swap(keep);
+    return SW2GPU_OK;
+}
+
+int sw2gpu_engine_destroy(sw2gpu_engine* e) {
+    if (!e) return SW2GPU_OK;
+    cudaStream_t st = e->R->stream;
+    cudaStreamSynchronize(st);
+    e->R.reset();
+    if (e->own_stream) cudaStreamDestroy(st);
+    delete e;
     return SW2GPU_OK;
 }
 

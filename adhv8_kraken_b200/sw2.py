@@ -28,7 +28,8 @@ _lib = None
 SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_destroy", "sw2gpu_set_state",
            "sw2gpu_get_state", "sw2gpu_get_wd_flag", "sw2gpu_set_wd_flag", "sw2gpu_step", "sw2gpu_set_dt",
            "sw2gpu_resid", "sw2gpu_load", "sw2gpu_linear_solve", "sw2gpu_batch_create", "sw2gpu_batch_step",
-           "sw2gpu_batch_destroy", "sw2gpu_bcsr_solve_noalloc"]
+           "sw2gpu_batch_destroy", "sw2gpu_bcsr_solve_noalloc", "sw2gpu_engine_create", "sw2gpu_engine_add",
+           "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_destroy"]
 
 
 class SW2Error(RuntimeError):
@@ -62,6 +63,13 @@ def lib():
         L.sw2gpu_batch_destroy.argtypes = [vp]
         L.sw2gpu_bcsr_solve_noalloc.argtypes = [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
                                                 C.c_int32, vp, c_int32_p]
+        L.sw2gpu_engine_create.argtypes = [C.c_int32, vp, C.POINTER(vp)]
+        L.sw2gpu_engine_add.argtypes = [vp, vp, C.c_int64, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int32,
+                                        c_int32_p, c_double_p, c_double_p]
+        L.sw2gpu_engine_tick.argtypes = [vp, vp, C.c_int32, c_int32_p]
+        L.sw2gpu_engine_active.argtypes = [vp]
+        L.sw2gpu_engine_active.restype = C.c_int32
+        L.sw2gpu_engine_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -232,6 +240,69 @@ class SW2Batch:
                 s.t = s.t + dts[k]
             out.append(d)
         return out
+
+
+class SW2Engine:
+    """Continuous batching (``sw2gpu_engine_*``): SW2GPU instances of one precision join with
+    a number of steps to run; every tick starts the steps of the instances between steps and
+    runs one Newton iteration of the others, each phase one launch over all of them.  A failed
+    step is retried with dt / 4.  Each instance computes exactly what it computes alone."""
+
+    def __init__(self, precision: int = capi.SW2GPU_FP64, stream: int = 0):
+        h = C.c_void_p()
+        _check(lib().sw2gpu_engine_create(precision, C.c_void_p(stream) if stream else None, C.byref(h)))
+        self.h = h
+        self.members = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sw2gpu_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, solver: "SW2GPU", nsteps: int, dt: float = None, max_retries: int = 8, key=None) -> int:
+        """Queue ``nsteps`` steps of ``solver`` from its current time; returns the instance id."""
+        key = id(solver) if key is None else key
+        ser = solver.model.series
+        lens = np.array([len(sr.times) for sr in ser], dtype=np.int32)
+        ts = np.ascontiguousarray(np.concatenate([np.asarray(sr.times, np.float64) for sr in ser]) if ser else np.zeros(1))
+        vs = np.ascontiguousarray(np.concatenate([np.asarray(sr.values, np.float64) for sr in ser]) if ser else np.zeros(1))
+        dt = solver.model.dt if dt is None else dt
+        _check(lib().sw2gpu_engine_add(self.h, solver.h, key, solver.t, dt, nsteps, max_retries, len(ser),
+                                       _ip(lens) if len(ser) else None, _dp(ts), _dp(vs)))
+        self.members[key] = solver
+        return key
+
+    @property
+    def active(self) -> int:
+        return lib().sw2gpu_engine_active(self.h)
+
+    def tick(self):
+        """One tick; returns the run stats of the instances that finished in it."""
+        n = max(self.active, 1)
+        out = (capi.RunStats * n)()
+        nf = C.c_int32()
+        _check(lib().sw2gpu_engine_tick(self.h, out, n, C.byref(nf)))
+        done = []
+        for k in range(nf.value):
+            d = out[k].as_dict()
+            s = self.members.pop(d["id"], None)
+            if s is not None:
+                s.t = d["t"]
+            done.append(d)
+        return done
+
+    def run(self):
+        """Ticks until every instance finished; returns all their run stats."""
+        done = []
+        while self.active:
+            done += self.tick()
+        return done
 
 
 def run(solver: SW2GPU, nsteps: int, dt: float = None, max_retries: int = 8, callback=None):

@@ -181,6 +181,7 @@ def run_ensemble(models, stream, rounds: int):
                 st = g.step(dt=dts[k])
                 if st["status"] == 0:
                     done[k] += 1
+                    dts[k] = g.model.dt
                 else:
                     dts[k] *= 0.25
         return done
@@ -193,6 +194,7 @@ def run_ensemble(models, stream, rounds: int):
             for k, st in enumerate(sts):
                 if st["status"] == 0:
                     done[k] += 1
+                    dts[k] = gs[k].model.dt
                 else:
                     dts[k] *= 0.25
         return done

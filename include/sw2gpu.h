@@ -170,6 +170,39 @@ int sw2gpu_batch_create(sw2gpu_ctx **ctxs, int32_t n, void *stream, sw2gpu_batch
 int sw2gpu_batch_step(sw2gpu_batch *b, const double *dt, const double *const *series, sw2gpu_stats *stats);
 int sw2gpu_batch_destroy(sw2gpu_batch *b);
 
+/* Continuous batching (no counterpart in the reference, whose time loop runs one model).
+ * Instances of uneven size join and leave an engine between ticks.  A tick starts a time
+ * step for every instance between steps (step-averaged series, level shift, fe_sw2_init,
+ * residual) and runs one Newton iteration for every instance inside a step, each phase as
+ * one launch over all of them.  A failed step is retried with dt / 4, as the reference's
+ * time loop does, and the step after a successful retry starts again from the base dt; an
+ * instance computes exactly what sw2gpu_step computes for it alone.
+ * The engine does not own the contexts; an instance that finished leaves the engine and is
+ * reported by the tick. */
+typedef struct sw2gpu_engine sw2gpu_engine;
+typedef struct {
+    int64_t id;
+    int32_t status;      /* 0: nsteps completed; else the failure code of the last attempt (gave up) */
+    int32_t steps;       /* completed time steps */
+    int32_t failures;    /* failed step attempts (each retried with dt / 4) */
+    int32_t newton_its;
+    int32_t linear_its;
+    int32_t ticks;       /* ticks the instance was in the engine */
+    double t;            /* model time reached */
+    double dt;           /* time step at the end */
+} sw2gpu_run_stats;
+int sw2gpu_engine_create(int32_t precision, void *stream, sw2gpu_engine **out);
+/* nseries piecewise-linear series (the instance's BC series, ids as in the mesh): series_len[s]
+ * points each, times and values concatenated in series order; averaged over every step.
+ * max_retries: consecutive failed attempts allowed before the instance gives up. */
+int sw2gpu_engine_add(sw2gpu_engine *e, sw2gpu_ctx *ctx, int64_t id, double t0, double dt, int32_t nsteps,
+                      int32_t max_retries, int32_t nseries, const int32_t *series_len, const double *series_t,
+                      const double *series_v);
+/* finished: room for at least sw2gpu_engine_active(e) records */
+int sw2gpu_engine_tick(sw2gpu_engine *e, sw2gpu_run_stats *finished, int32_t max_finished, int32_t *nfinished);
+int32_t sw2gpu_engine_active(const sw2gpu_engine *e);
+int sw2gpu_engine_destroy(sw2gpu_engine *e);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,3 +64,43 @@ def test_batch_order_does_not_matter():
             assert np.array_equal(x, y)
     ba.close()
     bb.close()
+
+
+def _run_alone(solver, nsteps, max_retries=8):
+    """sw2.run's contract: a failed step is retried with dt / 4, the next step uses dt again."""
+    from adhv8_kraken_b200.sw2 import run
+    return run(solver, nsteps, max_retries=max_retries)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [capi.SW2GPU_FP64, capi.SW2GPU_MIXED])
+def test_engine_equals_alone(precision):
+    """Continuous batching: instances with different step counts join one engine (one of
+    them later, while the others are mid-run) and each ends bitwise where it ends alone."""
+    from adhv8_kraken_b200.sw2 import SW2Engine
+    models = uneven_models()
+    nsteps = [3, 2, 4, 1]
+    alone = []
+    for m, n in zip(models, nsteps):
+        g = SW2GPU(m, precision=precision)
+        _run_alone(g, n)
+        alone.append((g.get_state(0), g.get_state(1), g.t))
+        g.close()
+    solvers = [SW2GPU(m, precision=precision) for m in models]
+    eng = SW2Engine(precision)
+    for g, n in list(zip(solvers, nsteps))[:3]:
+        eng.add(g, n)
+    done = eng.tick() + eng.tick()
+    eng.add(solvers[3], nsteps[3])   # joins while the others are inside their steps
+    done += eng.run()
+    assert len(done) == len(models) and all(d["status"] == 0 for d in done)
+    for k, g in enumerate(solvers):
+        (h0, u0, v0), (h1, u1, v1), t = alone[k]
+        h, u, v = g.get_state(0)
+        assert np.array_equal(h, h0) and np.array_equal(u, u0) and np.array_equal(v, v0), models[k].name
+        hh, uu, vv = g.get_state(1)
+        assert np.array_equal(hh, h1) and np.array_equal(uu, u1), models[k].name
+        assert g.t == t
+    eng.close()
+    for g in solvers:
+        g.close()
