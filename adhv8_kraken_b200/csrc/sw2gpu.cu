@@ -112,6 +112,11 @@ struct sw2gpu_ctx {
     DBuf<Norms> npart;
     DBuf<unsigned> ncounter;
     int krylov_grid = 0;            // virtual CTAs of the Krylov solve (its partial structure)
+    // Krylov iterations expected of the next solve, and those seen at each Newton iteration
+    // of the last step (the first Newton iteration of a step needs the tightest solve): they
+    // weight the instance's CTA share in a batch
+    int pred_its = 20;
+    int its_at[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     unsigned a_cap = 0, c_cap = 0;  // largest tile block / column-index ranges (staged sweeps)
     DevMesh dm{};
     std::unique_ptr<Runner> self;   // runs this instance alone
@@ -465,13 +470,15 @@ int launch_resid(Runner& R, const std::vector<int>& sub) {
                       SW2_GO(k_resid_gather<std::decay_t<decltype(src)>>));
 }
 
-// norms (and Krylov control words) of every instance; the one host sync of an evaluation
-int read_results(Runner& R) {
+// norms (and Krylov control words) of every instance; the one host sync of an evaluation.
+// `evaluated`: the instances whose residual was just computed (their slots hold fresh norms;
+// the others' slots may hold an earlier occupant's)
+int read_results(Runner& R, const std::vector<int>& evaluated) {
     const int K = (int)R.ctx.size();
     CK(cudaMemcpyAsync(R.norms_h, R.norms.p, sizeof(Norms) * K, cudaMemcpyDeviceToHost, R.stream));
     CK(cudaMemcpyAsync(R.ctl_h, R.ctl.p, sizeof(KrylovCtl) * K, cudaMemcpyDeviceToHost, R.stream));
     CK(cudaStreamSynchronize(R.stream));
-    for (int k = 0; k < K; k++) R.ctx[k]->ngeneral = R.norms_h[k].ngeneral;
+    for (int k : evaluated) R.ctx[k]->ngeneral = R.norms_h[k].ngeneral;
     return 0;
 }
 
@@ -488,16 +495,18 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
     return launch_map(R, sub, 256, [&](int k) { return nblk(9LL * C(k)->nnzb, 256); }, SW2_GO(k_jac_gather<std::decay_t<decltype(src)>>));
 }
 
-// Krylov CTAs per instance: shares of the co-resident capacity by block count, at least one,
-// at most the instance's virtual CTAs
+// Krylov CTAs per instance: shares of the co-resident capacity by expected work (blocks x
+// iterations of the instance's last solve), at least one, at most its virtual CTAs, so that
+// the instances of a launch finish together
 std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub) {
+    auto work = [&](const sw2gpu_ctx* c) { return (double)c->nnzb * (double)std::max(c->pred_its, 1); };
     double wsum = 0.0;
-    for (int k : sub) wsum += (double)R.ctx[k]->nnzb;
+    for (int k : sub) wsum += work(R.ctx[k]);
     std::vector<int> P(sub.size());
     long long tot = 0;
     for (size_t j = 0; j < sub.size(); j++) {
         const sw2gpu_ctx* c = R.ctx[sub[j]];
-        const int want = (int)std::floor(R.capacity * (double)c->nnzb / std::max(wsum, 1.0));
+        const int want = (int)std::floor(R.capacity * work(c) / std::max(wsum, 1.0));
         P[j] = std::max(1, std::min(c->krylov_grid, want));
         tot += P[j];
     }
@@ -609,13 +618,16 @@ int newton_iteration(Runner& R, const std::vector<int>& act, std::vector<NState>
     if (rc) return rc;
     std::vector<double> eta(R.ctx.size(), 0.0);
     for (int k : act) {
-        const sw2gpu_params& p = R.ctx[k]->p;
+        sw2gpu_ctx* c = R.ctx[k];
+        const sw2gpu_params& p = c->p;
         eta[k] = std::min(1e-5, std::max(p.lin_rtol, kEtaNtl * p.tol_nonlin / std::max(ns[k].rmax, 1e-300)));
+        const int seen = c->its_at[std::min(ns[k].it, 7)];
+        if (seen > 0) c->pred_its = seen;
     }
     if ((rc = launch_linear(R, act, eta))) return rc;
     for (int k : act) ns[k].old_l2 = ns[k].l2;
     if ((rc = launch_resid(R, act))) return rc;
-    if ((rc = read_results(R))) return rc;
+    if ((rc = read_results(R, act))) return rc;
     std::vector<int> ls;
     for (int k : act) {
         NState& n = ns[k];
@@ -623,6 +635,8 @@ int newton_iteration(Runner& R, const std::vector<int>& act, std::vector<NState>
         const KrylovCtl& q = R.ctl_h[k];
         if (q.err) return fail(SW2GPU_E_TIMEOUT, "instance %d: Krylov barrier or tile-copy wait ran out", k);
         n.lin += q.iterations;
+        R.ctx[k]->its_at[std::min(n.it, 7)] = std::max(q.iterations, 1);
+        R.ctx[k]->pred_its = std::max(q.iterations, 1);
         // the plain path fails the step when BiCGSTAB hits max_lin_it without a useful
         // reduction (solv_bcgstab.c:280-292); on the mixed path the FP32 inner solve is a
         // correction refined by the FP64 Newton loop, so its last iterate is accepted (the
@@ -643,7 +657,7 @@ int newton_iteration(Runner& R, const std::vector<int>& act, std::vector<NState>
     while (!ls.empty()) {
         if ((rc = launch_half_inc(R, ls))) return rc;
         if ((rc = launch_resid(R, ls))) return rc;
-        if ((rc = read_results(R))) return rc;
+        if ((rc = read_results(R, ls))) return rc;
         std::vector<int> next;
         for (int k : ls) {
             NState& n = ns[k];
@@ -713,7 +727,7 @@ int runner_step(Runner& R, const double* dt, const double* const* series, sw2gpu
     for (int k = 0; k < K; k++) all[k] = k;
     if ((rc = launch_init(R, all))) return rc;
     if ((rc = launch_resid(R, all))) return rc;
-    if ((rc = read_results(R))) return rc;
+    if ((rc = read_results(R, all))) return rc;
     std::vector<NState> ns(K);
     for (int k = 0; k < K; k++) newton_begin(R, k, ns[k]);
     for (;;) {
@@ -1013,8 +1027,10 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     std::vector<sw2gpu_ctx*> me(1, c);
     c->self.reset(new Runner());
     if ((rc = runner_init(*c->self, me, st))) return rc;
-    const int need = nblk(V, kKrylovThreads);
-    c->krylov_grid = std::max(1, std::min(need, c->self->capacity));
+    // one virtual CTA per tile of kTileRows rows, at most the co-resident grid: small meshes get
+    // many CTAs when batched (a Krylov launch lasts as long as its slowest instance)
+    const int ntiles = nblk(V, kTileRows);
+    c->krylov_grid = std::max(1, std::min(ntiles, c->self->capacity));
     if (zalloc(c->part, 8ull * c->krylov_grid, st)) return SW2GPU_E_NOMEM;
     DevMesh& d = c->dm;
     d.V = V; d.T = T; d.E = E; d.nnzb = nnzb;
@@ -1087,7 +1103,7 @@ int sw2gpu_resid(sw2gpu_ctx* c, double* resid) {
     const std::vector<int> one(1, 0);
     int rc = runner_tables(R, 1);
     if (!rc) rc = launch_resid(R, one);
-    if (!rc) rc = read_results(R);
+    if (!rc) rc = read_results(R, one);
     if (rc) return rc;
     if (resid) CK(cudaMemcpyAsync(resid, c->R.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -1108,7 +1124,7 @@ int sw2gpu_load(sw2gpu_ctx* c, int32_t* nnzb, int32_t* row_ptr, int32_t* col, do
     CK(cudaMemcpyAsync(&R.norms.p[0].ngeneral, c->gcount.p, sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->ngen.p, c->gcount.p, sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemsetAsync(c->gcount.p, 0, sizeof(int), c->stream));
-    if ((rc = read_results(R))) return rc;
+    if ((rc = read_results(R, one))) return rc;
     if ((rc = launch_jacobian(R, one))) return rc;
     if ((rc = launch_map(R, one, 256, [&](int) { return nblk(c->V, 256); }, SW2_GO(k_rowscale<std::decay_t<decltype(src)>>, 1)))) return rc;
     if (row_ptr) memcpy(row_ptr, c->rowptr_h.data(), sizeof(int) * (c->V + 1));
@@ -1129,7 +1145,7 @@ int sw2gpu_linear_solve(sw2gpu_ctx* c, const double* val, const double* rhs, dou
     if (!rc) rc = launch_linear(R, one, std::vector<double>(1, c->p.lin_rtol));
     if (rc) return rc;
     CK(cudaMemcpyAsync(x, c->sol.p, sizeof(double) * 3 * c->V, cudaMemcpyDeviceToHost, c->stream));
-    if ((rc = read_results(R))) return rc;
+    if ((rc = read_results(R, {}))) return rc;
     const KrylovCtl& q = R.ctl_h[0];
     if (iterations) *iterations = q.iterations;
     if (q.err) return fail(SW2GPU_E_TIMEOUT, "Krylov barrier or tile-copy wait ran out");
@@ -1250,6 +1266,7 @@ struct sw2gpu_engine {
     bool dirty = true;             // membership changed since the runner last saw it
     bool own_stream = false;
     int precision = SW2GPU_FP64;
+    sw2gpu_stats last{};           // the last tick (see sw2gpu_engine_last_tick)
 };
 
 extern "C" {
@@ -1313,6 +1330,12 @@ int sw2gpu_engine_add(sw2gpu_engine* e, sw2gpu_ctx* ctx, int64_t id, double t0, 
 
 int32_t sw2gpu_engine_active(const sw2gpu_engine* e) { return e ? (int32_t)e->inst.size() : 0; }
 
+int sw2gpu_engine_last_tick(const sw2gpu_engine* e, sw2gpu_stats* out) {
+    if (!e || !out) return fail(SW2GPU_E_ARG, "null argument");
+    *out = e->last;
+    return SW2GPU_OK;
+}
+
 int sw2gpu_engine_tick(sw2gpu_engine* e, sw2gpu_run_stats* finished, int32_t max_finished, int32_t* nfinished) {
     if (!e || !nfinished || (max_finished > 0 && !finished)) return fail(SW2GPU_E_ARG, "bad engine_tick arguments");
     *nfinished = 0;
@@ -1329,6 +1352,7 @@ int sw2gpu_engine_tick(sw2gpu_engine* e, sw2gpu_run_stats* finished, int32_t max
     }
     R.launches = 0;
     R.nphase = 0;
+    CK(cudaEventRecord(R.ev0, R.stream));
     // instances between steps start one: dt, step-averaged series, level rotation
     std::vector<int> S;
     for (int k = 0; k < K; k++) {
@@ -1343,7 +1367,7 @@ int sw2gpu_engine_tick(sw2gpu_engine* e, sw2gpu_run_stats* finished, int32_t max
     if (!S.empty()) {
         if ((rc = launch_init(R, S))) return rc;
         if ((rc = launch_resid(R, S))) return rc;
-        if ((rc = read_results(R))) return rc;
+        if ((rc = read_results(R, S))) return rc;
         for (int k : S) {
             newton_begin(R, k, e->inst[k].ns);
             e->inst[k].in_step = true;
@@ -1383,7 +1407,26 @@ int sw2gpu_engine_tick(sw2gpu_engine* e, sw2gpu_run_stats* finished, int32_t max
         }
     }
     if (!failed.empty() && (rc = launch_init(R, failed))) return rc;
-    CK(cudaStreamSynchronize(R.stream));
+    CK(cudaEventRecord(R.ev1, R.stream));
+    CK(cudaEventSynchronize(R.ev1));
+    {
+        sw2gpu_stats& L = e->last;
+        memset(&L, 0, sizeof(L));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, R.ev0, R.ev1);
+        double ph[3];
+        phase_times(R, ph);
+        L.newton_its = (int32_t)N.size();
+        L.linesearch_cuts = (int32_t)S.size();
+        L.wd_elems = K;
+        for (int k : N) L.linear_its = std::max<int32_t>(L.linear_its, R.ctl_h[k].iterations);
+        L.device_ms = ms;
+        L.kernel_launches = R.launches;
+        L.jac_ms = ph[kPhJac];
+        L.krylov_ms = ph[kPhKrylov];
+        L.resid_ms = ph[kPhResid];
+        L.other_ms = ms - ph[0] - ph[1] - ph[2];
+    }
     // instances done with their steps (or out of retries) leave the engine
     std::vector<EngInst> keep;
     for (auto& x : e->inst) {

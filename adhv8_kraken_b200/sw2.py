@@ -29,7 +29,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_get_state", "sw2gpu_get_wd_flag", "sw2gpu_set_wd_flag", "sw2gpu_step", "sw2gpu_set_dt",
            "sw2gpu_resid", "sw2gpu_load", "sw2gpu_linear_solve", "sw2gpu_batch_create", "sw2gpu_batch_step",
            "sw2gpu_batch_destroy", "sw2gpu_bcsr_solve_noalloc", "sw2gpu_engine_create", "sw2gpu_engine_add",
-           "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_destroy"]
+           "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_last_tick", "sw2gpu_engine_destroy"]
 
 
 class SW2Error(RuntimeError):
@@ -70,6 +70,7 @@ def lib():
         L.sw2gpu_engine_active.argtypes = [vp]
         L.sw2gpu_engine_active.restype = C.c_int32
         L.sw2gpu_engine_destroy.argtypes = [vp]
+        L.sw2gpu_engine_last_tick.argtypes = [vp, vp]
         _lib = L
     return _lib
 
@@ -296,6 +297,16 @@ class SW2Engine:
                 s.t = d["t"]
             done.append(d)
         return done
+
+    def last_tick(self):
+        """Device time and phases of the last tick (see sw2gpu_engine_last_tick)."""
+        st = Stats()
+        _check(lib().sw2gpu_engine_last_tick(self.h, C.byref(st)))
+        d = st.as_dict()
+        return {"device_ms": d["device_ms"], "jac_ms": d["jac_ms"], "krylov_ms": d["krylov_ms"],
+                "resid_ms": d["resid_ms"], "other_ms": d["other_ms"], "launches": d["kernel_launches"],
+                "iterating": d["newton_its"], "max_krylov_its": d["linear_its"], "starting": d["linesearch_cuts"],
+                "instances": d["wd_elems"]}
 
     def run(self):
         """Ticks until every instance finished; returns all their run stats."""

@@ -143,18 +143,19 @@ def ensemble_models(n: int, nsteps: int, seed0: int = 7000, procs: int = 0):
         return pool.map(_ensemble_member, [(seed0 + i, nsteps) for i in range(n)])
 
 
-def run_ensemble(models, stream, rounds: int):
-    """Config-4 legs on the same instances and rounds (one step attempt per instance per
-    round; a failed step is retried next round with dt / 4, as the reference's time loop
-    does, and counts as wasted time):
+def run_ensemble(models, stream, steps: int):
+    """Config-4 legs on the same instances, every instance running `steps` time steps (a failed
+    step is retried with dt / 4 and counts as wasted time, the next step returns to dt):
 
     * plain FP64 -- each instance stepped alone, one after the other (the drop-in path);
-    * batched FP64 and batched mixed -- all instances in one batch (sw2gpu_batch_step).
+    * batched FP64 and batched mixed -- all instances in one continuous-batching engine
+      (sw2gpu_engine_*): each tick is one launch per Newton phase over every instance, an
+      instance that finished a step starts its next one in the following tick.
 
     Throughput = sum over instances of triangles x completed steps / device time."""
     import torch
     from adhv8_kraken_b200 import capi
-    from adhv8_kraken_b200.sw2 import SW2Batch, SW2GPU
+    from adhv8_kraken_b200.sw2 import SW2Engine, SW2GPU, run
 
     tri = np.array([m.nelems2d for m in models], dtype=np.float64)
 
@@ -173,77 +174,71 @@ def run_ensemble(models, stream, rounds: int):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), out
 
-    def rounds_alone(gs):
-        dts = [g.model.dt for g in gs]
-        done = np.zeros(len(gs))
-        for _ in range(rounds):
-            for k, g in enumerate(gs):
-                st = g.step(dt=dts[k])
-                if st["status"] == 0:
-                    done[k] += 1
-                    dts[k] = g.model.dt
-                else:
-                    dts[k] *= 0.25
+    def alone(gs):
+        done = 0.0
+        for k, g in enumerate(gs):
+            done += tri[k] * len(run(g, steps))
         return done
 
-    def rounds_batch(b, gs):
-        dts = [g.model.dt for g in gs]
-        done = np.zeros(len(gs))
-        for _ in range(rounds):
-            sts = b.step(dts)
-            for k, st in enumerate(sts):
-                if st["status"] == 0:
-                    done[k] += 1
-                    dts[k] = gs[k].model.dt
-                else:
-                    dts[k] *= 0.25
-        return done
+    def engine(gs, precision):
+        eng = SW2Engine(precision, stream=stream.cuda_stream)
+        for g in gs:
+            eng.add(g, steps)
+        res, ph = [], {"jac_ms": 0.0, "krylov_ms": 0.0, "resid_ms": 0.0, "other_ms": 0.0}
+        ticks = 0
+        while eng.active:
+            res += eng.tick()
+            lt = eng.last_tick()
+            for key in ph:
+                ph[key] += lt[key]
+            ticks += 1
+        eng.close()
+        by_id = {id(g): k for k, g in enumerate(gs)}
+        done = sum(tri[by_id[d["id"]]] * d["steps"] for d in res)
+        return done, sum(d["failures"] for d in res), ticks, ph
+
+    def warm(gs, precision):
+        eng = SW2Engine(precision, stream=stream.cuda_stream)
+        for g in gs:
+            eng.add(g, 1)
+        eng.run()
+        eng.close()
+        reset(gs)
 
     out = {}
     g64 = [SW2GPU(m, precision=capi.SW2GPU_FP64, stream=stream.cuda_stream) for m in models]
-    for g in g64:            # warm-up: one step each, then back to the initial state
-        g.step()
-    reset(g64)
-    ms, done = timed(lambda: rounds_alone(g64))
-    out["plain_fp64"] = {"value": float((tri * done).sum() / (ms * 1e-3)), "ms_per_round": ms / rounds,
-                         "failed_steps": int(rounds * len(models) - done.sum())}
+    warm(g64, capi.SW2GPU_FP64)
+    ms, done = timed(lambda: alone(g64))
+    out["plain_fp64"] = {"value": float(done / (ms * 1e-3)), "ms": ms}
     plain_state = [g.get_state(0) for g in g64]
     reset(g64)
-    b64 = SW2Batch(g64, stream=stream.cuda_stream)
-    b64.step()
-    reset(g64)
-    ms, done = timed(lambda: rounds_batch(b64, g64))
-    out["batched_fp64"] = {"value": float((tri * done).sum() / (ms * 1e-3)), "ms_per_round": ms / rounds,
-                           "failed_steps": int(rounds * len(models) - done.sum())}
+    ms, (done, fails, ticks, ph) = timed(lambda: engine(g64, capi.SW2GPU_FP64))
+    out["batched_fp64"] = {"value": float(done / (ms * 1e-3)), "ms": ms, "failed_steps": int(fails), "ticks": ticks,
+                           "phase_ms": ph}
     b64_state = [g.get_state(0) for g in g64]
     out["batched_fp64"]["bitwise_equal_to_plain"] = bool(all(
         all(np.array_equal(x, y) for x, y in zip(a, c)) for a, c in zip(plain_state, b64_state)))
-    b64.close()
     for g in g64:
         g.close()
     gm = [SW2GPU(m, precision=capi.SW2GPU_MIXED, stream=stream.cuda_stream) for m in models]
-    bm = SW2Batch(gm, stream=stream.cuda_stream)
-    bm.step()
-    reset(gm)
-    ms, done = timed(lambda: rounds_batch(bm, gm))
+    warm(gm, capi.SW2GPU_MIXED)
+    ms, (done, fails, ticks, ph) = timed(lambda: engine(gm, capi.SW2GPU_MIXED))
     eh = eq = 0.0
     for g, ref in zip(gm, b64_state):
         h, u, v = g.get_state(0)
         eh = max(eh, float(np.abs(h - ref[0]).max() / max(np.abs(ref[0]).max(), 1e-300)))
         dq = np.hypot(h * u - ref[0] * ref[1], h * v - ref[0] * ref[2])
         eq = max(eq, float(dq.max() / max(np.hypot(ref[0] * ref[1], ref[0] * ref[2]).max(), 1e-300)))
-    out["batched_mixed"] = {"value": float((tri * done).sum() / (ms * 1e-3)), "ms_per_round": ms / rounds,
-                            "failed_steps": int(rounds * len(models) - done.sum()),
-                            "max_rel_err_vs_fp64": {"h": eh, "q": eq}}
-    bm.close()
+    out["batched_mixed"] = {"value": float(done / (ms * 1e-3)), "ms": ms, "failed_steps": int(fails), "ticks": ticks,
+                            "phase_ms": ph, "max_rel_err_vs_fp64": {"h": eh, "q": eq}}
     for g in gm:
         g.close()
     out["workload"] = (f"batched ensemble: {len(models)} seeded basins, triangles log-uniform 5k-200k "
                        f"(total {int(tri.sum())}), own bathymetry, Manning median U[0.015,0.05], inflow peak "
-                       f"U[1,8] m^2/s, dt U[2,10] s; {rounds} rounds of one step per instance")
+                       f"U[1,8] m^2/s, dt U[2,10] s; {steps} steps per instance")
     out["instances"] = len(models)
     out["triangles"] = int(tri.sum())
-    out["rounds"] = rounds
+    out["steps"] = steps
     return out
 
 
@@ -482,7 +477,7 @@ def main():
     ap.add_argument("--ref-points", type=int, default=10000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ens", type=int, default=256, help="batched-ensemble instances (0: skip the leg)")
-    ap.add_argument("--ens-steps", type=int, default=20, help="rounds of the ensemble legs")
+    ap.add_argument("--ens-steps", type=int, default=10, help="time steps per ensemble instance")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -201,6 +201,11 @@ int sw2gpu_engine_add(sw2gpu_engine *e, sw2gpu_ctx *ctx, int64_t id, double t0, 
 /* finished: room for at least sw2gpu_engine_active(e) records */
 int sw2gpu_engine_tick(sw2gpu_engine *e, sw2gpu_run_stats *finished, int32_t max_finished, int32_t *nfinished);
 int32_t sw2gpu_engine_active(const sw2gpu_engine *e);
+/* the last tick: device_ms and the phase times of sw2gpu_stats, kernel_launches, and in
+ * newton_its the instances that ran a Newton iteration, in linear_its the largest Krylov
+ * iteration count among them, in linesearch_cuts the instances that started a time step,
+ * in wd_elems the instances in the engine */
+int sw2gpu_engine_last_tick(const sw2gpu_engine *e, sw2gpu_stats *out);
 int sw2gpu_engine_destroy(sw2gpu_engine *e);
 
 #ifdef __cplusplus
