@@ -87,6 +87,21 @@ class RunStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class RequestStats(C.Structure):
+    """sw2gpu_request_stats: one finished request of a sw2gpu_server."""
+    _fields_ = [
+        ("id", C.c_int64), ("status", C.c_int32), ("steps", C.c_int32), ("failures", C.c_int32),
+        ("newton_its", C.c_int32), ("linear_its", C.c_int32), ("reserved", C.c_int32), ("t", C.c_double),
+        ("queue_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double), ("device_bytes", C.c_int64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+SW2GPU_PENDING = 100
+
+
 class MeshArrays:
     """Owns the numpy buffers behind a :class:`Mesh` struct."""
 

@@ -9,7 +9,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -50,6 +56,10 @@ constexpr double kPi = 3.1415926535897932384626433832795028841971693993751058209
 constexpr double kEarthRotat = 7.2722E-5;
 constexpr double kUnsetFlt = -9999999.9;
 
+// device bytes allocated by this thread go to *g_alloc_bytes while it is set (sw2gpu_create
+// sets it to the context's total)
+thread_local size_t* g_alloc_bytes = nullptr;
+
 template <typename T>
 struct DBuf {
     T* p = nullptr;
@@ -59,6 +69,7 @@ struct DBuf {
         if (count == 0) count = 1;
         // 16 spare bytes: bulk copies of a 16-byte-rounded range may reach past the last element
         cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 16);
+        if (e == cudaSuccess && g_alloc_bytes) *g_alloc_bytes += count * sizeof(T) + 16;
         return e == cudaSuccess ? 0 : -1;
     }
     ~DBuf() { if (p) cudaFree(p); }
@@ -116,6 +127,7 @@ struct sw2gpu_ctx {
     // of the last step (the first Newton iteration of a step needs the tightest solve): they
     // weight the instance's CTA share in a batch
     int pred_its = 20;
+    size_t bytes = 0;               // device memory of the context
     int its_at[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     unsigned a_cap = 0, c_cap = 0;  // largest tile block / column-index ranges (staged sweeps)
     DevMesh dm{};
@@ -788,6 +800,10 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     CK(cudaGetDevice(&dev));
     auto* c = new sw2gpu_ctx();
     std::unique_ptr<sw2gpu_ctx> guard(c);
+    struct Count {   // counts this context's device allocations
+        explicit Count(size_t* b) { g_alloc_bytes = b; }
+        ~Count() { g_alloc_bytes = nullptr; }
+    } count(&c->bytes);
     c->p = *prm;
     if (stream) {
         c->stream = (cudaStream_t)stream;
@@ -1049,6 +1065,8 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     *out = guard.release();
     return SW2GPU_OK;
 }
+
+int64_t sw2gpu_device_bytes(const sw2gpu_ctx* c) { return c ? (int64_t)c->bytes : 0; }
 
 int sw2gpu_destroy(sw2gpu_ctx* c) {
     if (!c) return SW2GPU_OK;
@@ -1459,6 +1477,337 @@ int sw2gpu_engine_destroy(sw2gpu_engine* e) {
     e->R.reset();
     if (e->own_stream) cudaStreamDestroy(st);
     delete e;
+    return SW2GPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// request server: admission by free device memory, continuous batching, latencies
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+// a request's own copy of everything it was submitted with
+struct Request {
+    int64_t id = 0;
+    // mesh arrays
+    int32_t nnodes = 0, nelems2d = 0, nelems1d = 0, nstrings = 0, nmats = 0, nseries = 0;
+    std::vector<double> x, y, z, rough, ev, eevc, cor;
+    std::vector<int32_t> node_string, e2n, e2m, e1n, e1s, e1p, bc, isg, ivx, ivy, iu0, eevm;
+    sw2gpu_params prm{};
+    std::vector<double> h0, u0, v0;
+    double t0 = 0, dt = 0;
+    int32_t nsteps = 0;
+    std::vector<int32_t> slen;
+    std::vector<double> st, sv;
+    size_t est_bytes = 0;
+    sw2gpu_ctx* ctx = nullptr;
+    Clock::time_point submitted, admitted, finished;
+    // result
+    sw2gpu_request_stats stats{};
+    std::vector<double> h, u, v;
+    std::string error;
+    bool done = false;
+    sw2gpu_mesh mesh() const {
+        sw2gpu_mesh m;
+        m.nnodes = nnodes; m.nelems2d = nelems2d; m.nelems1d = nelems1d; m.nstrings = nstrings;
+        m.nmats = nmats; m.nseries = nseries;
+        m.x = x.data(); m.y = y.data(); m.z = z.data(); m.node_string = node_string.data();
+        m.elem2d_nodes = e2n.data(); m.elem2d_mat = e2m.data();
+        m.elem1d_nodes = e1n.data(); m.elem1d_string = e1s.data(); m.elem1d_parent = e1p.data();
+        m.str_bc_flag = bc.data(); m.str_isigma = isg.data(); m.str_ivx = ivx.data(); m.str_ivy = ivy.data();
+        m.str_iu0 = iu0.data(); m.str_rough_height = rough.data();
+        m.mat_eev_mode = eevm.data(); m.mat_ev = ev.data(); m.mat_eev_coef = eevc.data(); m.mat_coriolis = cor.data();
+        return m;
+    }
+};
+
+template <typename T>
+std::vector<T> vcopy(const T* p, size_t n) {
+    return p && n ? std::vector<T>(p, p + n) : std::vector<T>(std::max<size_t>(n, 0));
+}
+
+// device bytes of a request before its context exists: per triangle the element arrays, the
+// 81-value FD Jacobian records and ~3.5 BCSR blocks; per node the three state levels, the
+// Krylov vectors and the row data (measured contexts hold ~1.6 KB per triangle)
+size_t estimate_bytes(const Request& q) {
+    return (size_t)q.nelems2d * 1800 + (size_t)q.nnodes * 640 + (size_t)q.nelems1d * 400 + (1u << 20);
+}
+
+}  // namespace
+
+struct sw2gpu_server {
+    int precision = SW2GPU_FP64;
+    size_t budget = 0;                 // device bytes the admitted requests may hold
+    int max_active = kMaxBatch;
+    std::mutex mu;
+    std::condition_variable cv;        // new work, admission room, results
+    std::deque<std::shared_ptr<Request>> queue;     // submitted, not yet admitted
+    std::deque<std::shared_ptr<Request>> ready;     // context built, not yet in the engine
+    std::map<int64_t, std::shared_ptr<Request>> live;   // admitted, not yet collected
+    size_t in_use = 0;                 // device bytes of admitted requests
+    int admitted_active = 0;           // admitted and not finished
+    int64_t next_id = 1;
+    bool stop = false;
+    std::string fatal;                 // error that stopped the worker
+    sw2gpu_engine* eng = nullptr;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    std::thread loader, worker;
+
+    void load_loop();
+    void work_loop();
+};
+
+void sw2gpu_server::load_loop() {
+    cudaSetDevice(device);
+    for (;;) {
+        std::shared_ptr<Request> q;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            // FIFO admission: the head request waits until its bytes fit the budget
+            cv.wait(lk, [&] {
+                if (stop) return true;
+                if (queue.empty()) return false;
+                const auto& h = queue.front();
+                return admitted_active < max_active && (in_use + h->est_bytes <= budget || admitted_active == 0);
+            });
+            if (stop) return;
+            q = queue.front();
+            queue.pop_front();
+            in_use += q->est_bytes;
+            admitted_active++;
+        }
+        q->admitted = Clock::now();
+        const sw2gpu_mesh m = q->mesh();
+        sw2gpu_ctx* c = nullptr;
+        int rc = sw2gpu_create(&m, &q->prm, nullptr, &c);
+        if (!rc) rc = sw2gpu_set_state(c, 0, q->h0.data(), q->u0.data(), q->v0.data());
+        if (!rc) rc = sw2gpu_set_state(c, 1, q->h0.data(), q->u0.data(), q->v0.data());
+        if (!rc) rc = sw2gpu_set_state(c, 2, q->h0.data(), q->u0.data(), q->v0.data());
+        std::lock_guard<std::mutex> lk(mu);
+        if (rc) {   // the request fails on its own; the server goes on
+            q->error = g_err;
+            q->stats.status = rc;
+            q->done = true;
+            q->finished = Clock::now();
+            if (c) sw2gpu_destroy(c);
+            in_use -= q->est_bytes;
+            admitted_active--;
+        } else {
+            q->ctx = c;
+            in_use = in_use - q->est_bytes + c->bytes;   // the context's measured size
+            q->est_bytes = c->bytes;
+            ready.push_back(q);
+        }
+        cv.notify_all();
+    }
+}
+
+void sw2gpu_server::work_loop() {
+    cudaSetDevice(device);
+    std::map<int64_t, std::shared_ptr<Request>> running;
+    std::vector<sw2gpu_run_stats> fin(kMaxBatch);
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] { return stop || !ready.empty() || !running.empty(); });
+            if (stop) break;
+            // requests that arrived while others run join the engine between ticks
+            while (!ready.empty() && sw2gpu_engine_active(eng) < kMaxBatch) {
+                auto q = ready.front();
+                ready.pop_front();
+                std::vector<int32_t> len = q->slen;
+                const int rc = sw2gpu_engine_add(eng, q->ctx, q->id, q->t0, q->dt, q->nsteps, 8, (int32_t)len.size(),
+                                                 len.empty() ? nullptr : len.data(), q->st.data(), q->sv.data());
+                if (rc) {
+                    q->error = g_err;
+                    q->stats.status = rc;
+                    q->done = true;
+                    q->finished = Clock::now();
+                    sw2gpu_destroy(q->ctx);
+                    q->ctx = nullptr;
+                    in_use -= q->est_bytes;
+                    admitted_active--;
+                    cv.notify_all();
+                    continue;
+                }
+                running[q->id] = q;
+            }
+        }
+        if (running.empty()) continue;
+        int32_t nf = 0;
+        const int rc = sw2gpu_engine_tick(eng, fin.data(), (int32_t)fin.size(), &nf);
+        if (rc) {   // a device-level failure: fail every running request and stop
+            std::lock_guard<std::mutex> lk(mu);
+            fatal = g_err;
+            for (auto& kv : running) {
+                kv.second->error = fatal;
+                kv.second->stats.status = rc;
+                kv.second->done = true;
+                kv.second->finished = Clock::now();
+            }
+            stop = true;
+            cv.notify_all();
+            break;
+        }
+        for (int i = 0; i < nf; i++) {
+            auto it = running.find(fin[i].id);
+            if (it == running.end()) continue;
+            auto q = it->second;
+            running.erase(it);
+            q->h.resize(q->nnodes);
+            q->u.resize(q->nnodes);
+            q->v.resize(q->nnodes);
+            sw2gpu_get_state(q->ctx, 0, q->h.data(), q->u.data(), q->v.data());
+            sw2gpu_destroy(q->ctx);
+            q->ctx = nullptr;
+            q->finished = Clock::now();
+            sw2gpu_request_stats& st = q->stats;
+            st.id = q->id;
+            st.status = fin[i].status;
+            st.steps = fin[i].steps;
+            st.failures = fin[i].failures;
+            st.newton_its = fin[i].newton_its;
+            st.linear_its = fin[i].linear_its;
+            st.t = fin[i].t;
+            st.queue_ms = ms_between(q->submitted, q->admitted);
+            st.run_ms = ms_between(q->admitted, q->finished);
+            st.latency_ms = ms_between(q->submitted, q->finished);
+            st.device_bytes = (int64_t)q->est_bytes;
+            std::lock_guard<std::mutex> lk(mu);
+            q->done = true;
+            in_use -= q->est_bytes;
+            admitted_active--;
+            cv.notify_all();
+        }
+    }
+    // stopping: contexts of requests still in the engine are released here
+    for (auto& kv : running)
+        if (kv.second->ctx) {
+            sw2gpu_destroy(kv.second->ctx);
+            kv.second->ctx = nullptr;
+        }
+}
+
+extern "C" {
+
+int sw2gpu_server_create(int32_t precision, double hbm_fraction, int32_t max_active, sw2gpu_server** out) {
+    if (!out || !(hbm_fraction > 0.0 && hbm_fraction <= 1.0) || max_active <= 0 ||
+        (precision != SW2GPU_FP64 && precision != SW2GPU_MIXED))
+        return fail(SW2GPU_E_ARG, "bad server arguments");
+    *out = nullptr;
+    auto* S = new sw2gpu_server();
+    std::unique_ptr<sw2gpu_server> guard(S);
+    CK(cudaGetDevice(&S->device));
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    S->budget = (size_t)(hbm_fraction * (double)fr);
+    S->precision = precision;
+    S->max_active = std::min<int>(max_active, kMaxBatch);
+    CK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    int rc = sw2gpu_engine_create(precision, S->stream, &S->eng);
+    if (rc) {
+        cudaStreamDestroy(S->stream);
+        return rc;
+    }
+    S->loader = std::thread([S] { S->load_loop(); });
+    S->worker = std::thread([S] { S->work_loop(); });
+    *out = guard.release();
+    return SW2GPU_OK;
+}
+
+int sw2gpu_server_submit(sw2gpu_server* S, const sw2gpu_mesh* m, const sw2gpu_params* prm, const double* h0,
+                         const double* u0, const double* v0, double t0, double dt, int32_t nsteps, int32_t nseries,
+                         const int32_t* series_len, const double* series_t, const double* series_v, int64_t* id) {
+    if (!S || !m || !prm || !h0 || !u0 || !v0 || !id || !(dt > 0.0) || nsteps <= 0 || nseries < 0)
+        return fail(SW2GPU_E_ARG, "bad submit arguments");
+    auto q = std::make_shared<Request>();
+    q->nnodes = m->nnodes; q->nelems2d = m->nelems2d; q->nelems1d = m->nelems1d;
+    q->nstrings = m->nstrings; q->nmats = m->nmats; q->nseries = m->nseries;
+    const size_t V = m->nnodes, T = m->nelems2d, E = m->nelems1d, NS = m->nstrings, NM = m->nmats;
+    q->x = vcopy(m->x, V); q->y = vcopy(m->y, V); q->z = vcopy(m->z, V); q->node_string = vcopy(m->node_string, V);
+    q->e2n = vcopy(m->elem2d_nodes, 3 * T); q->e2m = vcopy(m->elem2d_mat, T);
+    q->e1n = vcopy(m->elem1d_nodes, 2 * E); q->e1s = vcopy(m->elem1d_string, E); q->e1p = vcopy(m->elem1d_parent, E);
+    q->bc = vcopy(m->str_bc_flag, NS); q->isg = vcopy(m->str_isigma, NS); q->ivx = vcopy(m->str_ivx, NS);
+    q->ivy = vcopy(m->str_ivy, NS); q->iu0 = vcopy(m->str_iu0, NS); q->rough = vcopy(m->str_rough_height, NS);
+    q->eevm = vcopy(m->mat_eev_mode, NM); q->ev = vcopy(m->mat_ev, 3 * NM); q->eevc = vcopy(m->mat_eev_coef, NM);
+    q->cor = vcopy(m->mat_coriolis, NM);
+    q->prm = *prm;
+    q->prm.precision = S->precision;
+    q->h0 = vcopy(h0, V); q->u0 = vcopy(u0, V); q->v0 = vcopy(v0, V);
+    q->t0 = t0; q->dt = dt; q->nsteps = nsteps;
+    size_t npts = 0;
+    for (int i = 0; i < nseries; i++) npts += (size_t)series_len[i];
+    q->slen = vcopy(series_len, (size_t)nseries);
+    q->st = vcopy(series_t, npts);
+    q->sv = vcopy(series_v, npts);
+    if (q->st.empty()) { q->st.push_back(0.0); q->sv.push_back(0.0); }
+    q->est_bytes = estimate_bytes(*q);
+    q->submitted = Clock::now();
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) return fail(SW2GPU_E_CUDA, "server stopped: %s", S->fatal.c_str());
+    q->id = S->next_id++;
+    *id = q->id;
+    S->live[q->id] = q;
+    S->queue.push_back(q);
+    S->cv.notify_all();
+    return SW2GPU_OK;
+}
+
+int sw2gpu_server_wait(sw2gpu_server* S, int64_t id, double timeout_s, sw2gpu_request_stats* st, double* h,
+                       double* u, double* v) {
+    if (!S) return fail(SW2GPU_E_ARG, "null server");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->live.find(id);
+    if (it == S->live.end()) return fail(SW2GPU_E_ARG, "unknown or collected request %lld", (long long)id);
+    auto q = it->second;
+    const auto deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(
+                                              std::chrono::duration<double>(std::max(timeout_s, 0.0)));
+    if (!S->cv.wait_until(lk, deadline, [&] { return q->done; })) return SW2GPU_PENDING;
+    if (st) *st = q->stats;
+    if (!q->h.empty()) {
+        const size_t nb = sizeof(double) * q->nnodes;
+        if (h) memcpy(h, q->h.data(), nb);
+        if (u) memcpy(u, q->u.data(), nb);
+        if (v) memcpy(v, q->v.data(), nb);
+    }
+    S->live.erase(it);
+    if (!q->error.empty()) return fail(q->stats.status ? q->stats.status : SW2GPU_E_CUDA, "%s", q->error.c_str());
+    return SW2GPU_OK;
+}
+
+int sw2gpu_server_status(sw2gpu_server* S, int32_t* queued, int32_t* active, int64_t* bytes_in_use,
+                         int64_t* budget) {
+    if (!S) return fail(SW2GPU_E_ARG, "null server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (queued) *queued = (int32_t)S->queue.size();
+    if (active) *active = S->admitted_active;
+    if (bytes_in_use) *bytes_in_use = (int64_t)S->in_use;
+    if (budget) *budget = (int64_t)S->budget;
+    return S->fatal.empty() ? SW2GPU_OK : fail(SW2GPU_E_CUDA, "server stopped: %s", S->fatal.c_str());
+}
+
+int sw2gpu_server_destroy(sw2gpu_server* S) {
+    if (!S) return SW2GPU_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->cv.notify_all();
+    }
+    if (S->loader.joinable()) S->loader.join();
+    if (S->worker.joinable()) S->worker.join();
+    for (auto& q : S->ready)
+        if (q->ctx) sw2gpu_destroy(q->ctx);
+    sw2gpu_engine_destroy(S->eng);
+    cudaStreamDestroy(S->stream);
+    delete S;
     return SW2GPU_OK;
 }
 

@@ -29,7 +29,9 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_get_state", "sw2gpu_get_wd_flag", "sw2gpu_set_wd_flag", "sw2gpu_step", "sw2gpu_set_dt",
            "sw2gpu_resid", "sw2gpu_load", "sw2gpu_linear_solve", "sw2gpu_batch_create", "sw2gpu_batch_step",
            "sw2gpu_batch_destroy", "sw2gpu_bcsr_solve_noalloc", "sw2gpu_engine_create", "sw2gpu_engine_add",
-           "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_last_tick", "sw2gpu_engine_destroy"]
+           "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_last_tick", "sw2gpu_engine_destroy",
+           "sw2gpu_device_bytes", "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait",
+           "sw2gpu_server_status", "sw2gpu_server_destroy"]
 
 
 class SW2Error(RuntimeError):
@@ -71,6 +73,15 @@ def lib():
         L.sw2gpu_engine_active.restype = C.c_int32
         L.sw2gpu_engine_destroy.argtypes = [vp]
         L.sw2gpu_engine_last_tick.argtypes = [vp, vp]
+        L.sw2gpu_device_bytes.argtypes = [vp]
+        L.sw2gpu_device_bytes.restype = C.c_int64
+        L.sw2gpu_server_create.argtypes = [C.c_int32, C.c_double, C.c_int32, C.POINTER(vp)]
+        L.sw2gpu_server_submit.argtypes = [vp, vp, vp, c_double_p, c_double_p, c_double_p, C.c_double, C.c_double,
+                                           C.c_int32, C.c_int32, c_int32_p, c_double_p, c_double_p,
+                                           C.POINTER(C.c_int64)]
+        L.sw2gpu_server_wait.argtypes = [vp, C.c_int64, C.c_double, vp, c_double_p, c_double_p, c_double_p]
+        L.sw2gpu_server_status.argtypes = [vp, c_int32_p, c_int32_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.sw2gpu_server_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -88,30 +99,45 @@ def _ip(a):
     return a.ctypes.data_as(c_int32_p)
 
 
+# Krylov stopping floors.  The reference preconditions with an exact LU of the whole system,
+# so its linear solves are exact to round-off; the plain FP64 path reaches toward that
+# (relative floor 1e-10, about where block-Jacobi BiCGSTAB on these systems stops improving;
+# the library tightens each Newton iteration's test against tol_nonlin).  The mixed path's
+# FP32 inner solves stop at 1e-6 (at most 100 iterations) and the FP64 Newton loop refines.
+DEFAULT_TOL = {capi.SW2GPU_FP64: (1e-10, 1e-30), capi.SW2GPU_MIXED: (1e-6, 1e-30)}
+
+
+def solver_params(model, precision=capi.SW2GPU_FP64, precond=capi.SW2GPU_PREC_BJACOBI, lin_rtol=None,
+                  lin_atol=None, max_lin_it=None):
+    """sw2gpu_params of a model with this library's Krylov defaults for the precision."""
+    rt, at = DEFAULT_TOL[precision]
+    p = make_params(model, precision=precision, precond=precond, lin_rtol=rt if lin_rtol is None else lin_rtol,
+                    lin_atol=at if lin_atol is None else lin_atol)
+    if max_lin_it is not None:
+        p.max_lin_it = max_lin_it
+    elif precision == capi.SW2GPU_MIXED:
+        p.max_lin_it = min(p.max_lin_it, 100)
+    return p
+
+
+def _series_arrays(model):
+    ser = model.series
+    lens = np.array([len(sr.times) for sr in ser] or [0], dtype=np.int32)
+    ts = np.ascontiguousarray(np.concatenate([np.asarray(sr.times, np.float64) for sr in ser]) if ser else np.zeros(1))
+    vs = np.ascontiguousarray(np.concatenate([np.asarray(sr.values, np.float64) for sr in ser]) if ser else np.zeros(1))
+    return len(ser), lens, ts, vs
+
+
 class SW2GPU:
     """One SW2 model resident on the GPU (mesh, BCSR pattern and three time levels)."""
 
-    # Krylov stopping floors.  The reference preconditions with an exact LU of the whole
-    # system, so its linear solves are exact to round-off; the plain FP64 path reaches
-    # toward that (relative floor 1e-10, about where block-Jacobi BiCGSTAB on these systems
-    # stops improving; the library tightens each Newton iteration's test against
-    # tol_nonlin).  The mixed path's FP32 inner solves stop at 1e-6 and the FP64 Newton
-    # loop refines.
-    DEFAULT_TOL = {capi.SW2GPU_FP64: (1e-10, 1e-30), capi.SW2GPU_MIXED: (1e-6, 1e-30)}
+    DEFAULT_TOL = DEFAULT_TOL
 
     def __init__(self, model, precision: int = capi.SW2GPU_FP64, precond: int = capi.SW2GPU_PREC_BJACOBI,
                  lin_rtol: float = None, lin_atol: float = None, stream: int = 0, max_lin_it: int = None):
         self.model = model
-        rt, at = self.DEFAULT_TOL[precision]
-        lin_rtol = rt if lin_rtol is None else lin_rtol
-        lin_atol = at if lin_atol is None else lin_atol
         self.arrays = MeshArrays(model)
-        self.params = make_params(model, precision=precision, precond=precond, lin_rtol=lin_rtol,
-                                  lin_atol=lin_atol)
-        if max_lin_it is not None:
-            self.params.max_lin_it = max_lin_it
-        elif precision == capi.SW2GPU_MIXED:
-            self.params.max_lin_it = min(self.params.max_lin_it, 100)
+        self.params = solver_params(model, precision, precond, lin_rtol, lin_atol, max_lin_it)
         self.V, self.T = model.nnodes, model.nelems2d
         h = C.c_void_p()
         _check(lib().sw2gpu_create(C.byref(self.arrays.mesh), C.byref(self.params),
@@ -269,13 +295,10 @@ class SW2Engine:
     def add(self, solver: "SW2GPU", nsteps: int, dt: float = None, max_retries: int = 8, key=None) -> int:
         """Queue ``nsteps`` steps of ``solver`` from its current time; returns the instance id."""
         key = id(solver) if key is None else key
-        ser = solver.model.series
-        lens = np.array([len(sr.times) for sr in ser], dtype=np.int32)
-        ts = np.ascontiguousarray(np.concatenate([np.asarray(sr.times, np.float64) for sr in ser]) if ser else np.zeros(1))
-        vs = np.ascontiguousarray(np.concatenate([np.asarray(sr.values, np.float64) for sr in ser]) if ser else np.zeros(1))
+        ns, lens, ts, vs = _series_arrays(solver.model)
         dt = solver.model.dt if dt is None else dt
-        _check(lib().sw2gpu_engine_add(self.h, solver.h, key, solver.t, dt, nsteps, max_retries, len(ser),
-                                       _ip(lens) if len(ser) else None, _dp(ts), _dp(vs)))
+        _check(lib().sw2gpu_engine_add(self.h, solver.h, key, solver.t, dt, nsteps, max_retries, ns,
+                                       _ip(lens) if ns else None, _dp(ts), _dp(vs)))
         self.members[key] = solver
         return key
 
@@ -314,6 +337,61 @@ class SW2Engine:
         while self.active:
             done += self.tick()
         return done
+
+
+class SW2Server:
+    """The library's request loop (``sw2gpu_server_*``): solves are submitted with their mesh,
+    initial state and number of steps, admitted in order while their device memory fits the
+    budget, and stepped together by continuous batching; ``wait`` returns a finished solve's
+    final state and its queue / run / total latency."""
+
+    def __init__(self, precision: int = capi.SW2GPU_FP64, hbm_fraction: float = 0.8, max_active: int = 256):
+        h = C.c_void_p()
+        _check(lib().sw2gpu_server_create(precision, hbm_fraction, max_active, C.byref(h)))
+        self.h = h
+        self.precision = precision
+        self.nnodes = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sw2gpu_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, model, nsteps: int, dt: float = None) -> int:
+        arrays = MeshArrays(model)
+        params = solver_params(model, self.precision)
+        ns, lens, ts, vs = _series_arrays(model)
+        h0, u0, v0 = (np.ascontiguousarray(a, dtype=np.float64) for a in (model.h0, model.u0, model.v0))
+        rid = C.c_int64()
+        _check(lib().sw2gpu_server_submit(self.h, C.byref(arrays.mesh), C.byref(params), _dp(h0), _dp(u0), _dp(v0),
+                                          model.t0, model.dt if dt is None else dt, nsteps, ns,
+                                          _ip(lens) if ns else None, _dp(ts), _dp(vs), C.byref(rid)))
+        self.nnodes[rid.value] = model.nnodes
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = 3600.0):
+        """(stats, (h, u, v)) of a finished request, None while it runs past the timeout."""
+        n = self.nnodes[rid]
+        st = capi.RequestStats()
+        h, u, v = np.zeros(n), np.zeros(n), np.zeros(n)
+        rc = lib().sw2gpu_server_wait(self.h, rid, timeout, C.byref(st), _dp(h), _dp(u), _dp(v))
+        if rc == capi.SW2GPU_PENDING:
+            return None
+        self.nnodes.pop(rid, None)
+        _check(rc)
+        return st.as_dict(), (h, u, v)
+
+    def status(self):
+        q, a = C.c_int32(), C.c_int32()
+        b, tot = C.c_int64(), C.c_int64()
+        _check(lib().sw2gpu_server_status(self.h, C.byref(q), C.byref(a), C.byref(b), C.byref(tot)))
+        return {"queued": q.value, "active": a.value, "bytes_in_use": b.value, "budget": tot.value}
 
 
 def run(solver: SW2GPU, nsteps: int, dt: float = None, max_retries: int = 8, callback=None):

@@ -114,6 +114,8 @@ const char *sw2gpu_last_error(void);
  * cudaStream_t (NULL = a stream owned by the context). */
 int sw2gpu_create(const sw2gpu_mesh *mesh, const sw2gpu_params *params, void *stream, sw2gpu_ctx **out);
 int sw2gpu_destroy(sw2gpu_ctx *ctx);
+/* device memory the context holds (bytes); no counterpart in the reference */
+int64_t sw2gpu_device_bytes(const sw2gpu_ctx *ctx);
 
 /* State of time level `level` (0 = current t+dt iterate, 1 = old, 2 = older);
  * SW2 state is (head, vel.x, vel.y) as in src/structs/ssw_2d.h:13-18. */
@@ -207,6 +209,42 @@ int32_t sw2gpu_engine_active(const sw2gpu_engine *e);
  * in wd_elems the instances in the engine */
 int sw2gpu_engine_last_tick(const sw2gpu_engine *e, sw2gpu_stats *out);
 int sw2gpu_engine_destroy(sw2gpu_engine *e);
+
+/* Request server (no counterpart in the reference): a request loop in the library.  Each
+ * submitted solve -- mesh, parameters, initial state, series, number of steps -- is copied,
+ * queued and admitted in arrival order when its device bytes fit the budget (a fraction of
+ * the device memory free at creation; a request that fits no budget is admitted alone).  A
+ * loader thread builds admitted requests' contexts while a worker thread ticks a
+ * continuous-batching engine, so requests that arrive while others run share their launches
+ * and every solve keeps its state on the device between steps.  Results and per-request
+ * times are collected with sw2gpu_server_wait.  One precision per server. */
+typedef struct sw2gpu_server sw2gpu_server;
+#define SW2GPU_PENDING 100   /* sw2gpu_server_wait: not finished within the timeout */
+typedef struct {
+    int64_t id;
+    int32_t status;       /* 0: all steps done */
+    int32_t steps, failures, newton_its, linear_its;
+    int32_t reserved;
+    double t;             /* model time reached */
+    double queue_ms;      /* submit -> admitted */
+    double run_ms;        /* admitted -> finished (context build, steps, result copy) */
+    double latency_ms;    /* submit -> finished */
+    int64_t device_bytes; /* device memory the request held */
+} sw2gpu_request_stats;
+int sw2gpu_server_create(int32_t precision, double hbm_fraction, int32_t max_active, sw2gpu_server **out);
+/* series as for sw2gpu_engine_add; *id receives the request id */
+int sw2gpu_server_submit(sw2gpu_server *s, const sw2gpu_mesh *mesh, const sw2gpu_params *params,
+                         const double *h0, const double *u0, const double *v0, double t0, double dt,
+                         int32_t nsteps, int32_t nseries, const int32_t *series_len, const double *series_t,
+                         const double *series_v, int64_t *id);
+/* waits up to timeout_s; on completion fills st and the final state (nnodes each, may be NULL)
+ * and forgets the request; SW2GPU_PENDING if still running */
+int sw2gpu_server_wait(sw2gpu_server *s, int64_t id, double timeout_s, sw2gpu_request_stats *st, double *h,
+                       double *u, double *v);
+int sw2gpu_server_status(sw2gpu_server *s, int32_t *queued, int32_t *active, int64_t *bytes_in_use,
+                         int64_t *budget);
+/* stops both threads; requests not finished are dropped */
+int sw2gpu_server_destroy(sw2gpu_server *s);
 
 #ifdef __cplusplus
 }
