@@ -143,6 +143,60 @@ def ensemble_models(n: int, nsteps: int, seed0: int = 7000, procs: int = 0):
         return pool.map(_ensemble_member, [(seed0 + i, nsteps) for i in range(n)])
 
 
+def _serve_member(args):
+    seed, nsteps = args
+    from adhv8_kraken_b200 import meshgen
+    return meshgen.ensemble_member(seed, tri_lo=1e4, tri_hi=2e6, nsteps=nsteps, name="req")
+
+
+def serve_requests(n: int, horizon_scale: float, seed0: int = 9000, procs: int = 0):
+    """Serving-loop requests: meshes with triangle count log-uniform 10k-2M and their own
+    bathymetry / roughness / inflow / dt draws, horizons uniform 10..500 steps times
+    `horizon_scale` (at least one step); generated in a spawn-started process pool."""
+    from multiprocessing import get_context
+    rng = np.random.Generator(np.random.PCG64(seed0))
+    horizons = [max(1, int(round(int(rng.integers(10, 501)) * horizon_scale))) for _ in range(n)]
+    procs = procs or max(1, min(32, (os.cpu_count() or 2) - 1))
+    with get_context("spawn").Pool(procs) as pool:
+        models = pool.map(_serve_member, [(seed0 + 1 + i, h) for i, h in enumerate(horizons)])
+    return models, horizons
+
+
+def run_serving(models, horizons, lam: float, seed: int = 1):
+    """Config-5 legs: Poisson arrivals at rate lam (req/s) into the library's request server,
+    FP64 and mixed on the same requests; per request the latency from submission to result,
+    and the aggregate triangle-steps/s from the first submission to the last result."""
+    from adhv8_kraken_b200 import capi
+    from adhv8_kraken_b200.sw2 import SW2Server
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gaps = rng.exponential(1.0 / lam, len(models))
+    out = {}
+    for name, prec in (("fp64", capi.SW2GPU_FP64), ("mixed", capi.SW2GPU_MIXED)):
+        srv = SW2Server(prec, hbm_fraction=0.8)
+        t0 = time.perf_counter()
+        due = t0
+        ids = []
+        for m, h, gap in zip(models, horizons, gaps):
+            due += gap
+            time.sleep(max(0.0, due - time.perf_counter()))
+            ids.append(srv.submit(m, h))
+        res = [srv.wait(i) for i in ids]
+        wall = time.perf_counter() - t0
+        srv.close()
+        st = [r[0] for r in res]
+        lat = np.array([x["latency_ms"] for x in st])
+        work = sum(m.nelems2d * x["steps"] for m, x in zip(models, st))
+        out[name] = {"value": work / wall, "p50_ms": float(np.percentile(lat, 50)),
+                     "p99_ms": float(np.percentile(lat, 99)), "mean_queue_ms": float(np.mean([x["queue_ms"] for x in st])),
+                     "failed": int(sum(1 for x in st if x["status"] != 0)), "wall_s": wall}
+    out["workload"] = (f"serving loop: {len(models)} requests, Poisson arrivals at {lam} req/s, triangles "
+                       f"log-uniform 10k-2M (total {sum(m.nelems2d for m in models)}), horizons "
+                       f"{min(horizons)}-{max(horizons)} steps (sum {sum(horizons)})")
+    out["requests"] = len(models)
+    out["rate_per_s"] = lam
+    return out
+
+
 def run_ensemble(models, stream, steps: int):
     """Config-4 legs on the same instances, every instance running `steps` time steps (a failed
     step is retried with dt / 4 and counts as wasted time, the next step returns to dt):
@@ -294,7 +348,7 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
-def run_ours(args, rank, world, local_rank, ens_models=None):
+def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
     import torch
     import torch.distributed as dist
     from adhv8_kraken_b200 import capi
@@ -363,12 +417,16 @@ def run_ours(args, rank, world, local_rank, ens_models=None):
     tot_ms, launches, bytes_per_launch = kernels[name]
     per_launch_ms = tot_ms / max(launches, 1)
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    # measured DRAM traffic of the Krylov kernel: bytes per BiCGSTAB iteration from one ncu
+    # capture of the same workload (profiles/traffic_basin_1M_tri.md), times this run's mean
+    # iterations per launch (traffic grows with the iterations)
     traffic = None
-    tf = os.path.join(ROOT, "profiles", f"{name}_traffic.json")
-    if os.path.exists(tf):
+    tf = os.path.join(ROOT, "profiles", "traffic_basin_1M_tri.md")
+    if name == "k_bicgstab" and os.path.exists(tf) and T == 998582:
         with open(tf) as f:
-            tr = json.load(f)
-        traffic = tr.get("bytes_per_triangle", 0) * T if name == "k_jac_elem" else tr.get("bytes_per_launch")
+            for ln in f:
+                if ln.startswith("k_bicgstab_bytes_per_iteration:"):
+                    traffic = float(ln.split(":")[1]) * (lin / max(newton, 1))
     roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": per_launch_ms,
@@ -433,6 +491,9 @@ def run_ours(args, rank, world, local_rank, ens_models=None):
     batched = None
     if ens_models:
         batched = run_ensemble(ens_models, stream, args.ens_steps)
+    serving = None
+    if serve:
+        serving = run_serving(serve[0], serve[1], args.serve_rate)
 
     if rank != 0:
         return
@@ -462,6 +523,7 @@ def run_ours(args, rank, world, local_rank, ens_models=None):
         "e2e": e2e,
         "mixed": mixed,
         "batched": batched,
+        "serving": serving,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
@@ -478,6 +540,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ens", type=int, default=256, help="batched-ensemble instances (0: skip the leg)")
     ap.add_argument("--ens-steps", type=int, default=10, help="time steps per ensemble instance")
+    ap.add_argument("--serve", type=int, default=24, help="serving-loop requests (0: skip the leg)")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-horizon-scale", type=float, default=0.1,
+                    help="horizons U{10..500} steps times this factor (1.0: the full horizons)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -495,8 +561,11 @@ def main():
         args.ens = 0   # the ensemble legs are a single-GPU measurement
     ens = ensemble_models(args.ens, nsteps=args.ens_steps,
                           procs=max(1, ((os.cpu_count() or 2) - 1) // world)) if args.ens > 0 else None
+    serve = None
+    if world == 1 and args.serve > 0:
+        serve = serve_requests(args.serve, args.serve_horizon_scale)
     try:
-        run_ours(args, rank, world, local_rank, ens)
+        run_ours(args, rank, world, local_rank, ens, serve)
     finally:
         if world > 1:
             import torch.distributed as dist
