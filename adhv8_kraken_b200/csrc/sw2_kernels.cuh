@@ -455,11 +455,10 @@ __device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, 
 // evaluates column w for 32 elements, so the pressure-term branch is warp-uniform.
 // Element data are staged in shared memory once; the 9x9 element matrices are staged
 // in shared memory and written out as contiguous 81-double records (slot 9e + 3a + b).
-#ifndef SW2_JAC_MIN_BLOCKS
-#define SW2_JAC_MIN_BLOCKS 2   // resident CTAs per SM the wet kernel's register budget is cut for
-#endif
-template <class Src>
-__global__ void __launch_bounds__(kJacThreads, SW2_JAC_MIN_BLOCKS) k_jac_elem_wet(const __grid_constant__ Src src) {
+// MINB: resident CTAs per SM the register budget is cut for (1: 168 registers, 2: 96 with more
+// spills); the autotuner picks per mesh, the arithmetic is the same
+template <class Src, int MINB>
+__global__ void __launch_bounds__(kJacThreads, MINB) k_jac_elem_wet(const __grid_constant__ Src src) {
     int lb, nb;
     const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;

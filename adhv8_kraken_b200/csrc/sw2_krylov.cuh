@@ -27,7 +27,9 @@ constexpr long long kMbarSpinLimit = 1ll << 20;      // polls of one tile copy's
 constexpr int kStall = 40;                           // iterations without a new best residual
 constexpr int kRowLanes = 8;                         // lanes per node row in the SpMV sweeps
 constexpr int kTileRows = kKrylovThreads / kRowLanes;   // node rows per CTA tile (32)
-constexpr int kStages = 3;                           // shared-memory tile ring of the staged sweeps
+constexpr int kMaxStages = 3;                        // deepest shared-memory tile ring of the staged sweeps
+constexpr int kVirtualPerSM = 3;                     // virtual CTAs per SM of a large instance (fixed:
+                                                     // it sets the reduction order, so no tuning knob may)
 
 // Blocks of one launch over a batch: instance ids[j] owns blocks boff[j] .. boff[j+1]-1.
 // Passed by value (kernel parameter space), so lookups are uniform constant-bank reads.
@@ -392,15 +394,17 @@ __device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke
 // iteration stagnates).  Per instance, A holds the folded off-diagonal blocks D_i^-1 A'_ij
 // (rowptr / col of K) and Dinv the FP64 inverses (used once, for b = M^-1 b').  STAGED: the
 // SpMV sweeps read each tile's blocks, column indices, row pointers and epilogue vectors from
-// a kStages-deep shared-memory ring filled by bulk copies (one thread issues, completion on
-// an mbarrier) kStages - 1 tiles ahead of the rows being computed, so a row's only global
+// a STAGES-deep shared-memory ring filled by bulk copies (one thread issues, completion on
+// an mbarrier) STAGES - 1 tiles ahead of the rows being computed, so a row's only global
 // loads are its x gathers; the streamed matrix data carry an L2 evict-first hint, which keeps
-// the Krylov vectors in L2.  The dynamic shared memory is kStages * L.stage_bytes.  Otherwise
-// the lanes load everything from global memory.
-template <typename MT, typename VT, bool STAGED, class KS>
+// the Krylov vectors in L2.  The dynamic shared memory is STAGES * L.stage_bytes.  STAGES = 0:
+// the lanes load everything from global memory.  Every variant computes the same bits.
+template <typename MT, typename VT, int STAGES, class KS>
 __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_constant__ KS src) {
     __shared__ double red[4 * kKrylovWarps];
-    __shared__ unsigned long long bar[kStages];
+    constexpr bool STAGED = STAGES > 0;
+    constexpr int NST = STAGES > 0 ? STAGES : 1;
+    __shared__ unsigned long long bar[NST];
     extern __shared__ __align__(128) unsigned char stage_mem[];
     int pl, np;   // this CTA's index among the instance's np CTAs
     double rtol;
@@ -427,15 +431,15 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     const int SUM = 0, MAX = 1;
     KrylovCtl* ctl = K.ctl;
     int nred = 0;      // reductions so far; selects the partial buffer
-    unsigned tc = 0;   // tiles consumed by this CTA: stage tc % kStages, mbarrier parity (tc / kStages) & 1
+    unsigned tc = 0;   // tiles consumed by this CTA: stage tc % NST, mbarrier parity (tc / NST) & 1
     bool wait_failed = false;
     unsigned long long pol = 0;
     auto pbuf = [&]() { return K.part + (size_t)(nred & 1) * VG * 4; };
-    auto stage = [&](unsigned c) { return stage_mem + (c % kStages) * L.stage_bytes; };
+    auto stage = [&](unsigned c) { return stage_mem + (c % NST) * L.stage_bytes; };
 
     if (STAGED) {
         if (threadIdx.x == 0) {
-            for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
+            for (int s = 0; s < NST; s++) mbar_init(&bar[s], 1);
             mbar_init_fence();
             pol = policy_evict_first();
         }
@@ -447,7 +451,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     // blocks of each row; lane 0 of each row group calls epi(i, y, ev) with ev[v][c] =
     // component c of epilogue vector v at row i (NV vectors: v0, v1, v2), from which the
     // epilogue forms the diagonal term; fin(v) closes virtual CTA v (its partial).  The
-    // producer cursor (pv, pm) runs kStages - 1 items ahead along the same sequence.
+    // producer cursor (pv, pm) runs NST - 1 items ahead along the same sequence.
     auto sweep = [&](auto nvc, const VT* xa, const VT* xb, VT alpha, const VT* v0, const VT* v1, const VT* v2,
                      auto&& epi, auto&& fin) {
         constexpr int NV = decltype(nvc)::value;
@@ -455,7 +459,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         int pv = pl, pm = pl;
         auto produce = [&](unsigned item) {
             if (pv >= VG) return;
-            issue_tile<MT, VT>(pm, V, K.rowptr, K.col, A, NV, vecs, stage(item), L, &bar[item % kStages], pol);
+            issue_tile<MT, VT>(pm, V, K.rowptr, K.col, A, NV, vecs, stage(item), L, &bar[item % NST], pol);
             pm += VG;
             if (pm >= ntiles) {
                 pv += np;
@@ -464,7 +468,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         };
         if (STAGED && threadIdx.x == 0) {
             fence_proxy_async_global();
-            for (int d = 0; d < kStages - 1; d++) produce(tc + d);
+            for (int d = 0; d < NST - 1; d++) produce(tc + d);
         }
         for (int v = pl; v < VG; v += np) {
             for (int m = v; m < ntiles; m += VG) {
@@ -474,10 +478,10 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                 VT ev[NV][3];
                 if (STAGED) {
                     // into the stage of item tc - 1, released by the __syncthreads that ended it
-                    if (threadIdx.x == 0) produce(tc + kStages - 1);
+                    if (threadIdx.x == 0) produce(tc + NST - 1);
                     // a wait that runs out flags the error once; this thread then stops waiting,
                     // the sweep finishes on stale data and the next barrier returns
-                    if (!wait_failed && !mbar_wait(&bar[tc % kStages], (tc / kStages) & 1u)) {
+                    if (!wait_failed && !mbar_wait(&bar[tc % NST], (tc / NST) & 1u)) {
                         wait_failed = true;
                         atomicExch(&ctl->err, 1);
                     }

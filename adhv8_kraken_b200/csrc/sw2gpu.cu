@@ -130,6 +130,9 @@ struct sw2gpu_ctx {
     size_t bytes = 0;               // device memory of the context
     int its_at[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     unsigned a_cap = 0, c_cap = 0;  // largest tile block / column-index ranges (staged sweeps)
+    // autotuned launch variants (sw2gpu_autotune): they change speed, never results
+    int tune_jac_minb = 2;          // wet-Jacobian CTAs per SM the register budget is cut for
+    int tune_stages = 3;            // Krylov tile-ring depth (0: sweeps from global memory)
     DevMesh dm{};
     std::unique_ptr<Runner> self;   // runs this instance alone
 
@@ -179,9 +182,14 @@ void stage_caps(const std::vector<int>& rp, int V, size_t esz, unsigned& a_cap, 
     c_cap = (unsigned)cm;
 }
 
+// Krylov kernel with a tile ring of `stages` stages (0: sweeps read global memory)
 template <typename MT, class KS>
-void* krylov_kernel(bool staged) {
-    return staged ? (void*)k_bicgstab<MT, double, true, KS> : (void*)k_bicgstab<MT, double, false, KS>;
+void* krylov_kernel(int stages) {
+    switch (stages) {
+        case 2: return (void*)k_bicgstab<MT, double, 2, KS>;
+        case 3: return (void*)k_bicgstab<MT, double, 3, KS>;
+        default: return (void*)k_bicgstab<MT, double, 0, KS>;
+    }
 }
 
 }  // namespace
@@ -202,7 +210,8 @@ struct Runner {
     DBuf<int> singular;
     Norms* norms_h = nullptr;     // pinned mirrors, one entry per instance
     KrylovCtl* ctl_h = nullptr;
-    bool staged = false;
+    int stages = 0;               // Krylov tile-ring depth in use (0: sweeps from global memory)
+    int jac_minb = 2;             // wet-Jacobian variant in use
     unsigned c_off = 0, r_off = 0, v_off = 0, stage_bytes = 0;
     size_t smem = 0;
     int capacity = 0;             // co-resident Krylov CTAs
@@ -325,42 +334,47 @@ int runner_alloc(Runner& R, cudaStream_t stream, bool mixed, int cap) {
     return 0;
 }
 
-// the instances of the runner (at most its capacity, one precision) and the Krylov launch
-// configuration for them: stage layout for the largest tile of any instance, co-resident CTAs
+// the instances of the runner (at most its capacity, one precision) and the launch variants
+// for them: those tuned for the instance with the most blocks, the stage layout for the
+// largest tile of any instance, the co-resident Krylov CTAs
 int runner_set(Runner& R, const std::vector<sw2gpu_ctx*>& ctx) {
     if ((int)ctx.size() > R.cap) return fail(SW2GPU_E_ARG, "batch of %zu instances (at most %d)", ctx.size(), R.cap);
     for (auto* c : ctx)
         if ((c->p.precision == SW2GPU_MIXED) != R.mixed) return fail(SW2GPU_E_ARG, "a batch has one precision");
     R.ctx = ctx;
     unsigned a_cap = 16, c_cap = 16;
+    const sw2gpu_ctx* big = nullptr;
     for (auto* c : ctx) {
         a_cap = std::max(a_cap, c->a_cap);
         c_cap = std::max(c_cap, c->c_cap);
+        if (!big || c->nnzb > big->nnzb) big = c;
     }
+    int want = big ? big->tune_stages : 3;
+    R.jac_minb = big ? big->tune_jac_minb : 2;
     const unsigned c_off = a_cap, r_off = c_off + c_cap;
     const unsigned v_off = r_off + ((unsigned)(kTileRows + 1) * 4u + 15u) / 16u * 16u;
     const unsigned stage = (v_off + 3u * tile_vec_bytes<double>() + 127u) & ~127u;
-    const bool staged = (size_t)kStages * stage <= kMaxStagedSmem;
-    if (R.capacity > 0 && staged == R.staged &&
-        (!staged || (a_cap <= R.c_off && c_cap <= R.r_off - R.c_off)))
+    if (want > 0 && (size_t)want * stage > kMaxStagedSmem) want = (size_t)2 * stage <= kMaxStagedSmem ? 2 : 0;
+    if (R.capacity > 0 && want == R.stages &&
+        (!want || (a_cap <= R.c_off && c_cap <= R.r_off - R.c_off)))
         return 0;   // the current layout still holds every tile
-    R.staged = staged;
+    R.stages = want;
     R.c_off = R.r_off = R.v_off = R.stage_bytes = 0;
-    if (R.staged) {
+    if (R.stages) {
         R.c_off = c_off;
         R.r_off = r_off;
         R.v_off = v_off;
         R.stage_bytes = stage;
     }
-    R.smem = (size_t)kStages * R.stage_bytes;
+    R.smem = (size_t)R.stages * R.stage_bytes;
     int dev = 0, sms = 0, per_sm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // the dynamic shared-memory cap is an attribute of the kernel, shared by every runner:
     // set to the largest tile ring any runner may use
-    void* kone = R.mixed ? krylov_kernel<float, KrylovOne>(R.staged) : krylov_kernel<double, KrylovOne>(R.staged);
-    void* ktab = R.mixed ? krylov_kernel<float, KrylovTab>(R.staged) : krylov_kernel<double, KrylovTab>(R.staged);
-    if (R.staged) {
+    void* kone = R.mixed ? krylov_kernel<float, KrylovOne>(R.stages) : krylov_kernel<double, KrylovOne>(R.stages);
+    void* ktab = R.mixed ? krylov_kernel<float, KrylovTab>(R.stages) : krylov_kernel<double, KrylovTab>(R.stages);
+    if (R.stages) {
         CK(cudaFuncSetAttribute(kone, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStagedSmem));
         CK(cudaFuncSetAttribute(ktab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxStagedSmem));
     }
@@ -498,7 +512,10 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
     Phase ph(&R, kPhJac);
     auto C = [&](int k) { return R.ctx[k]; };
     // the general list and the wet flags come from the residual evaluated at this same state
-    int rc = launch_map(R, sub, kJacThreads, [&](int k) { return nblk(C(k)->T, kJacElems); }, SW2_GO(k_jac_elem_wet<std::decay_t<decltype(src)>>));
+    auto wet_blocks = [&](int k) { return nblk(C(k)->T, kJacElems); };
+    int rc = R.jac_minb == 1
+                 ? launch_map(R, sub, kJacThreads, wet_blocks, SW2_GO_T(k_jac_elem_wet, 1))
+                 : launch_map(R, sub, kJacThreads, wet_blocks, SW2_GO_T(k_jac_elem_wet, 2));
     if (rc) return rc;
     if ((rc = launch_map(R, sub, kJacThreads, [&](int k) { return nblk(C(k)->ngeneral, kJacElems); },
                          SW2_GO(k_jac_elem_general<std::decay_t<decltype(src)>>))))
@@ -565,7 +582,7 @@ int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<doub
             one.rtol = eta[grp[0]];
             one.lay = lay;
             void* args[] = {(void*)&one};
-            void* kern = R.mixed ? krylov_kernel<float, KrylovOne>(R.staged) : krylov_kernel<double, KrylovOne>(R.staged);
+            void* kern = R.mixed ? krylov_kernel<float, KrylovOne>(R.stages) : krylov_kernel<double, KrylovOne>(R.stages);
             CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kKrylovThreads), args, R.smem, R.stream));
         } else {
             static thread_local KrylovTab t;   // ~4 KB: not on the stack of every caller
@@ -581,7 +598,7 @@ int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<doub
             t.mp.boff[grp.size()] = off;
             t.lay = lay;
             void* args[] = {(void*)&t};
-            void* kern = R.mixed ? krylov_kernel<float, KrylovTab>(R.staged) : krylov_kernel<double, KrylovTab>(R.staged);
+            void* kern = R.mixed ? krylov_kernel<float, KrylovTab>(R.stages) : krylov_kernel<double, KrylovTab>(R.stages);
             CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kKrylovThreads), args, R.smem, R.stream));
         }
         R.launches++;
@@ -1043,10 +1060,13 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     std::vector<sw2gpu_ctx*> me(1, c);
     c->self.reset(new Runner());
     if ((rc = runner_init(*c->self, me, st))) return rc;
-    // one virtual CTA per tile of kTileRows rows, at most the co-resident grid: small meshes get
-    // many CTAs when batched (a Krylov launch lasts as long as its slowest instance)
+    // one virtual CTA per tile of kTileRows rows, at most kVirtualPerSM per SM: small meshes get
+    // many CTAs when batched (a Krylov launch lasts as long as its slowest instance).  Fixed by
+    // the device, not by the tuned occupancy: it sets the order of every Krylov reduction
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int ntiles = nblk(V, kTileRows);
-    c->krylov_grid = std::max(1, std::min(ntiles, c->self->capacity));
+    c->krylov_grid = std::max(1, std::min(ntiles, kVirtualPerSM * sms));
     if (zalloc(c->part, 8ull * c->krylov_grid, st)) return SW2GPU_E_NOMEM;
     DevMesh& d = c->dm;
     d.V = V; d.T = T; d.E = E; d.nnzb = nnzb;
@@ -1168,6 +1188,89 @@ int sw2gpu_linear_solve(sw2gpu_ctx* c, const double* val, const double* rhs, dou
     if (iterations) *iterations = q.iterations;
     if (q.err) return fail(SW2GPU_E_TIMEOUT, "Krylov barrier or tile-copy wait ran out");
     return q.converged ? SW2GPU_OK : fail(SW2GPU_E_LINEAR, "BiCGSTAB reached max_lin_it");
+}
+
+int sw2gpu_set_variant(sw2gpu_ctx* c, int32_t jac_minb, int32_t stages) {
+    if (!c || (jac_minb != 1 && jac_minb != 2) || (stages != 0 && stages != 2 && stages != 3))
+        return fail(SW2GPU_E_ARG, "variant: jac_minb 1|2, stages 0|2|3");
+    c->tune_jac_minb = jac_minb;
+    c->tune_stages = stages;
+    return runner_set(*c->self, c->self->ctx);
+}
+
+int sw2gpu_get_variant(const sw2gpu_ctx* c, int32_t* jac_minb, int32_t* stages) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    if (jac_minb) *jac_minb = c->self->jac_minb;
+    if (stages) *stages = c->self->stages;
+    return SW2GPU_OK;
+}
+
+// Times every launch variant on the context's own mesh and current state and keeps the
+// fastest: the wet-Jacobian register budget (1 or 2 CTAs per SM) and the Krylov tile-ring
+// depth (0, 2 or 3 stages).  The variants compute the same bits; the state is left as found.
+int sw2gpu_autotune(sw2gpu_ctx* c, int32_t* jac_minb, int32_t* stages) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    Runner& R = *c->self;
+    const std::vector<int> one(1, 0);
+    const size_t nb = sizeof(double) * c->V;
+    cudaStream_t st = R.stream;
+    // the residual zeroes old-dry nodes' velocities of the current level: keep a copy
+    double* keep = c->kv64[7].p;
+    CK(cudaMemcpyAsync(keep, c->U(0), nb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(keep + c->V, c->Vv(0), nb, cudaMemcpyDeviceToDevice, st));
+    int rc = runner_tables(R, 0);
+    if (!rc) rc = launch_resid(R, one);
+    if (!rc) rc = read_results(R, one);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto timed = [&](auto&& fn, float& best) -> int {
+        int r = fn();   // warm
+        if (r) return r;
+        for (int rep = 0; rep < 2; rep++) {
+            CK(cudaEventRecord(e0, st));
+            if ((r = fn())) return r;
+            CK(cudaEventRecord(e1, st));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            best = std::min(best, ms);
+        }
+        return 0;
+    };
+    int best_j = c->tune_jac_minb;
+    float tb = 1e30f;
+    for (int m : {1, 2}) {
+        R.jac_minb = m;
+        float t = 1e30f;
+        if ((rc = timed([&] { return launch_jacobian(R, one); }, t))) break;
+        if (t < tb) { tb = t; best_j = m; }
+    }
+    c->tune_jac_minb = best_j;
+    int best_s = c->tune_stages;
+    tb = 1e30f;
+    const std::vector<double> eta(1, c->p.lin_rtol);
+    for (int sg : {0, 2, 3}) {
+        if (rc) break;
+        c->tune_stages = sg;
+        if ((rc = runner_set(R, R.ctx))) break;
+        if (R.stages != sg) continue;   // this mesh's tiles do not fit that ring
+        float t = 1e30f;
+        if ((rc = timed([&] { return launch_linear(R, one, eta); }, t))) break;
+        if (t < tb) { tb = t; best_s = sg; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->tune_stages = best_s;
+    if (!rc) rc = runner_set(R, R.ctx);
+    CK(cudaMemcpyAsync(c->U(0), keep, nb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(c->Vv(0), keep + c->V, nb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    if (rc) return rc;
+    if (jac_minb) *jac_minb = R.jac_minb;
+    if (stages) *stages = R.stages;
+    return SW2GPU_OK;
 }
 
 int sw2gpu_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* stats) {

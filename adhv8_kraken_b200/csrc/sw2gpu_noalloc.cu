@@ -184,7 +184,7 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double, false, KrylovOne>, kKrylovThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bicgstab<double, double, 0, KrylovOne>, kKrylovThreads, 0);
     const int grid = std::max(1, std::min({kMaxGrid, (nnodes + kKrylovThreads - 1) / kKrylovThreads,
                                            sms * std::max(per_sm, 1)}));
     // one instance, direct sweeps (no tile ring); the record is a kernel parameter
@@ -209,7 +209,7 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     one.rtol = rtol;
     one.lay = StageLayout{0, 0, 0, 0};
     void* args[] = {(void*)&one};
-    cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double, false, KrylovOne>, dim3(grid),
+    cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double, 0, KrylovOne>, dim3(grid),
                                                 dim3(kKrylovThreads), args, 0, st);
     if (e != cudaSuccess) return na_fail(SW2GPU_E_CUDA, cudaGetErrorString(e));
     KrylovCtl h;

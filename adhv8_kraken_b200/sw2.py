@@ -30,7 +30,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_resid", "sw2gpu_load", "sw2gpu_linear_solve", "sw2gpu_batch_create", "sw2gpu_batch_step",
            "sw2gpu_batch_destroy", "sw2gpu_bcsr_solve_noalloc", "sw2gpu_engine_create", "sw2gpu_engine_add",
            "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_last_tick", "sw2gpu_engine_destroy",
-           "sw2gpu_device_bytes", "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait",
+           "sw2gpu_device_bytes", "sw2gpu_autotune", "sw2gpu_set_variant", "sw2gpu_get_variant", "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait",
            "sw2gpu_server_status", "sw2gpu_server_destroy"]
 
 
@@ -74,6 +74,9 @@ def lib():
         L.sw2gpu_engine_destroy.argtypes = [vp]
         L.sw2gpu_engine_last_tick.argtypes = [vp, vp]
         L.sw2gpu_device_bytes.argtypes = [vp]
+        L.sw2gpu_autotune.argtypes = [vp, c_int32_p, c_int32_p]
+        L.sw2gpu_set_variant.argtypes = [vp, C.c_int32, C.c_int32]
+        L.sw2gpu_get_variant.argtypes = [vp, c_int32_p, c_int32_p]
         L.sw2gpu_device_bytes.restype = C.c_int64
         L.sw2gpu_server_create.argtypes = [C.c_int32, C.c_double, C.c_int32, C.POINTER(vp)]
         L.sw2gpu_server_submit.argtypes = [vp, vp, vp, c_double_p, c_double_p, c_double_p, C.c_double, C.c_double,
@@ -134,10 +137,13 @@ class SW2GPU:
     DEFAULT_TOL = DEFAULT_TOL
 
     def __init__(self, model, precision: int = capi.SW2GPU_FP64, precond: int = capi.SW2GPU_PREC_BJACOBI,
-                 lin_rtol: float = None, lin_atol: float = None, stream: int = 0, max_lin_it: int = None):
+                 lin_rtol: float = None, lin_atol: float = None, stream: int = 0, max_lin_it: int = None,
+                 overrides: dict = None):
         self.model = model
         self.arrays = MeshArrays(model)
         self.params = solver_params(model, precision, precond, lin_rtol, lin_atol, max_lin_it)
+        for k, v in (overrides or {}).items():   # sw2gpu_params fields, e.g. max_nonlin_it
+            setattr(self.params, k, v)
         self.V, self.T = model.nnodes, model.nelems2d
         h = C.c_void_p()
         _check(lib().sw2gpu_create(C.byref(self.arrays.mesh), C.byref(self.params),
@@ -149,6 +155,20 @@ class SW2GPU:
         self.t = model.t0
         for lvl in range(3):
             self.set_state(lvl, model.h0, model.u0, model.v0)
+
+    def autotune(self):
+        """Times the launch variants on this mesh and keeps the fastest; (jac_minb, stages)."""
+        j, s = C.c_int32(), C.c_int32()
+        _check(lib().sw2gpu_autotune(self.h, C.byref(j), C.byref(s)))
+        return j.value, s.value
+
+    def set_variant(self, jac_minb: int, stages: int):
+        _check(lib().sw2gpu_set_variant(self.h, jac_minb, stages))
+
+    def variant(self):
+        j, s = C.c_int32(), C.c_int32()
+        _check(lib().sw2gpu_get_variant(self.h, C.byref(j), C.byref(s)))
+        return j.value, s.value
 
     def close(self):
         if getattr(self, "h", None):
@@ -363,8 +383,8 @@ class SW2Server:
         except Exception:
             pass
 
-    def submit(self, model, nsteps: int, dt: float = None) -> int:
-        arrays = MeshArrays(model)
+    def submit(self, model, nsteps: int, dt: float = None, arrays: MeshArrays = None) -> int:
+        arrays = MeshArrays(model) if arrays is None else arrays
         params = solver_params(model, self.precision)
         ns, lens, ts, vs = _series_arrays(model)
         h0, u0, v0 = (np.ascontiguousarray(a, dtype=np.float64) for a in (model.h0, model.u0, model.v0))

@@ -127,6 +127,23 @@ def config2_model(points: int, nsteps: int):
     return meshgen.bumpy_basin(points, seed=2024, size=size, nsteps=nsteps, dt=5.0, name="config2")
 
 
+def max_over_ranks(x: float, world: int, device="cpu") -> float:
+    """Largest value of x over the ranks (the timed region of the slowest replica)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, triangles: int, steps: int, ms_max: float) -> float:
+    """Whole-job triangle-steps/s of `world` replicas, each `steps` steps of `triangles`,
+    timed by the slowest rank."""
+    return world * triangles * steps / (ms_max * 1e-3)
+
+
 def _ensemble_member(args):
     seed, nsteps = args
     from adhv8_kraken_b200 import meshgen
@@ -382,11 +399,8 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
     barrier()
     ms = e0.elapsed_time(e1)
     assert all(s["status"] == 0 for s in stats), [s["status"] for s in stats]
-    ms_t = torch.tensor([ms], device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
-    value = world * T * args.steps / (ms * 1e-3)
+    ms = max_over_ranks(ms, world, dev)
+    value = replica_throughput(world, T, args.steps, ms)
     h64 = g.get_state(0)
 
     # ---- dominant kernel and its roofline
@@ -459,10 +473,8 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
             host[k][:] = out[k]
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e = {"value": world * T * args.steps / float(e2e_t.item()), "unit": "triangle-steps/s",
+    e2e_s = max_over_ranks(e2e_s, world, dev)
+    e2e = {"value": replica_throughput(world, T, args.steps, e2e_s * 1e3), "unit": "triangle-steps/s",
            "h2d_bytes_per_step": 9 * 8 * V, "d2h_bytes_per_step": 3 * 8 * V}
     g.close()
 

@@ -1,0 +1,101 @@
+"""Failure paths, made on the host (no GPU fault is provoked): the step contract of fe_newton /
+fe_main -- a failed step returns NO with the state reset to the old level, the caller retries
+with dt / 4 -- and the library's own reporting (NaN residuals, capped linear solves, solves that
+give up in a batch, requests with bad input in the server)."""
+import numpy as np
+import pytest
+
+from adhv8_kraken_b200 import capi, meshgen
+from adhv8_kraken_b200.capi import MeshArrays
+from adhv8_kraken_b200.sw2 import SW2Engine, SW2Error, SW2GPU, SW2Server, run
+
+
+def _basin(n=700, seed=11, nsteps=4):
+    return meshgen.bumpy_basin(n, seed=seed, size=2000.0, nsteps=nsteps, dt=5.0, nbins=3, name=f"b{n}")
+
+
+@pytest.mark.gpu
+def test_newton_failure_resets_to_old_level():
+    m = _basin()
+    # one Newton iteration against an unreachable tolerance: the step must fail
+    g = SW2GPU(m, overrides={"max_nonlin_it": 1, "tol_nonlin": 1e-30, "inc_nonlin": 1e-30})
+    old = g.get_state(0)
+    st = g.step()
+    assert st["status"] == capi.SW2GPU_E_NEWTON and st["newton_its"] == 1
+    # fe_sw2_init: the current level is the old one again (the level shift already happened)
+    h, u, v = g.get_state(0)
+    h1, u1, v1 = g.get_state(1)
+    assert np.array_equal(h, h1) and np.array_equal(h1, old[0])
+    assert g.t == m.t0
+    # the retry loop gives up after its retries and says so
+    with pytest.raises(SW2Error):
+        run(g, 1, max_retries=2)
+    g.close()
+
+
+@pytest.mark.gpu
+def test_linear_failure_is_reported():
+    m = _basin()
+    g = SW2GPU(m, max_lin_it=1)      # one BiCGSTAB iteration cannot reach 1e-8 of the residual
+    st = g.step()
+    assert st["status"] == capi.SW2GPU_E_LINEAR
+    h, _, _ = g.get_state(0)
+    assert np.array_equal(h, g.get_state(1)[0])
+    g.close()
+
+
+@pytest.mark.gpu
+def test_nan_state_returns_error_instead_of_exiting():
+    m = _basin()
+    g = SW2GPU(m)
+    h, u, v = g.get_state(0)
+    h = h.copy()
+    h[len(h) // 2] = np.nan
+    g.set_state(0, h, u, v)          # becomes the old level at the next step's shift
+    st = g.step()
+    assert st["status"] == capi.SW2GPU_E_NAN
+    g.close()
+
+
+@pytest.mark.gpu
+def test_engine_instance_gives_up_alone():
+    good = [_basin(700, 11), _basin(1500, 7)]
+    alone = []
+    for m in good:
+        g = SW2GPU(m)
+        run(g, 2)
+        alone.append(g.get_state(0))
+        g.close()
+    bad = SW2GPU(_basin(900, 3), overrides={"max_nonlin_it": 1, "tol_nonlin": 1e-30, "inc_nonlin": 1e-30})
+    gs = [SW2GPU(m) for m in good]
+    eng = SW2Engine()
+    for g in gs:
+        eng.add(g, 2)
+    eng.add(bad, 2, max_retries=1)
+    done = {d["id"]: d for d in eng.run()}
+    assert done[id(bad)]["status"] == capi.SW2GPU_E_NEWTON and done[id(bad)]["steps"] == 0
+    assert done[id(bad)]["failures"] == 2
+    for g, ref in zip(gs, alone):
+        assert done[id(g)]["status"] == 0
+        for x, y in zip(g.get_state(0), ref):
+            assert np.array_equal(x, y)
+    eng.close()
+    for g in gs + [bad]:
+        g.close()
+
+
+@pytest.mark.gpu
+def test_server_request_with_bad_mesh_fails_alone():
+    srv = SW2Server()
+    good = _basin()
+    bad = _basin(900, 3)
+    arrays = MeshArrays(bad)
+    arrays.mesh.elem2d_nodes[0] = 10 ** 8          # a node index out of range
+    rid_bad = srv.submit(bad, 2, arrays=arrays)
+    rid_good = srv.submit(good, 2)
+    with pytest.raises(SW2Error) as err:
+        srv.wait(rid_bad)
+    assert err.value.code == capi.SW2GPU_E_ARG and "out of range" in str(err.value)
+    st, _ = srv.wait(rid_good)
+    assert st["status"] == 0 and st["steps"] == 2
+    srv.close()
