@@ -19,10 +19,12 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 namespace sw2 {
 
 constexpr int kKrylovThreads = 256;
-constexpr long long kBarrierSpinLimit = 1ll << 26;   // bounded wait (~seconds), then error
+constexpr long long kBarrierSpinLimit = 1ll << 28;   // bounded wait (~seconds of polls), then error
 constexpr long long kMbarSpinLimit = 1ll << 20;      // polls of one tile copy's mbarrier, then error
 constexpr int kStall = 40;                           // iterations without a new best residual
 constexpr int kRowLanes = 8;                         // lanes per node row in the SpMV sweeps
@@ -77,13 +79,17 @@ __device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks) {
             __threadfence();
             atomicAdd(&ctl->gen, 1u);
         } else {
+            // tight bounded poll of the generation word (acquire loads, no sleep: a wake-up
+            // later than the release would be paid at every barrier)
             long long spins = 0;
-            while (*vgen == g) {
+            for (;;) {
+                unsigned cur;
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&ctl->gen) : "memory");
+                if (cur != g) break;
                 if (++spins > kBarrierSpinLimit || *(volatile int*)&ctl->err) {
                     atomicExch(&ctl->err, 1);
                     break;
                 }
-                __nanosleep(64);
             }
         }
         __threadfence();
@@ -637,21 +643,60 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                 const int mm[4] = {MAX, MAX, MAX, MAX};
                 const double beta = (rho * alpha) / (rhop * omega);
                 const VT al = (VT)alpha, om = (VT)omega, be = (VT)beta;
-                for (int v = pl; v < VG; v += np) {
-                    // element-wise (every load coalesced), virtual CTA v's share
-                    for (int k = v * blockDim.x + threadIdx.x; k < 3 * V; k += VG * blockDim.x) {
-                        const VT apk = ldv(Ap + k), pk = ldv(p + k);
-                        const VT s = fmadd(-al, apk, ldv(r + k));
-                        VT uk = ldv(uu + k);
-                        if (pending) ubest[k] = uk;
-                        uk = fmadd(al, pk, uk);
+                auto upd = [&](int k) {
+                    const VT apk = ldv(Ap + k), pk = ldv(p + k);
+                    const VT s = fmadd(-al, apk, ldv(r + k));
+                    VT uk = ldv(uu + k);
+                    if (pending) ubest[k] = uk;
+                    uk = fmadd(al, pk, uk);
+                    uk = fmadd(om, s, uk);
+                    uu[k] = uk;
+                    const VT rk = fmadd(-om, ldv(As + k), s);
+                    r[k] = rk;
+                    p[k] = fmadd(fmadd(-om, apk, pk), be, rk);
+                    mx[0] = fmax(mx[0], fabs((double)rk));
+                };
+                // two elements per thread with 16-byte accesses (the vectors start on 256-byte
+                // boundaries); the arithmetic is that of upd, element by element
+                auto upd2 = [&](int k2) {
+                    using V2 = typename std::conditional<sizeof(VT) == 8, double2, float2>::type;
+                    const V2 a2 = __ldcg(reinterpret_cast<const V2*>(Ap) + k2);
+                    const V2 p2 = __ldcg(reinterpret_cast<const V2*>(p) + k2);
+                    const V2 r2 = __ldcg(reinterpret_cast<const V2*>(r) + k2);
+                    const V2 u2 = __ldcg(reinterpret_cast<const V2*>(uu) + k2);
+                    const V2 s2 = __ldcg(reinterpret_cast<const V2*>(As) + k2);
+                    if (pending) reinterpret_cast<V2*>(ubest)[k2] = u2;
+                    V2 un, rn, pn;
+                    {
+                        const VT s = fmadd(-al, (VT)a2.x, (VT)r2.x);
+                        VT uk = fmadd(al, (VT)p2.x, (VT)u2.x);
                         uk = fmadd(om, s, uk);
-                        uu[k] = uk;
-                        const VT rk = fmadd(-om, ldv(As + k), s);
-                        r[k] = rk;
-                        p[k] = fmadd(fmadd(-om, apk, pk), be, rk);
+                        const VT rk = fmadd(-om, (VT)s2.x, s);
+                        un.x = uk;
+                        rn.x = rk;
+                        pn.x = fmadd(fmadd(-om, (VT)a2.x, (VT)p2.x), be, rk);
                         mx[0] = fmax(mx[0], fabs((double)rk));
                     }
+                    {
+                        const VT s = fmadd(-al, (VT)a2.y, (VT)r2.y);
+                        VT uk = fmadd(al, (VT)p2.y, (VT)u2.y);
+                        uk = fmadd(om, s, uk);
+                        const VT rk = fmadd(-om, (VT)s2.y, s);
+                        un.y = uk;
+                        rn.y = rk;
+                        pn.y = fmadd(fmadd(-om, (VT)a2.y, (VT)p2.y), be, rk);
+                        mx[0] = fmax(mx[0], fabs((double)rk));
+                    }
+                    reinterpret_cast<V2*>(uu)[k2] = un;
+                    reinterpret_cast<V2*>(r)[k2] = rn;
+                    reinterpret_cast<V2*>(p)[k2] = pn;
+                };
+                for (int v = pl; v < VG; v += np) {
+                    // element pairs (16-byte accesses), virtual CTA v's share; each element is
+                    // updated on its own, the pairing only widens the loads
+                    const int n2 = (3 * V) / 2;
+                    for (int k2 = v * blockDim.x + threadIdx.x; k2 < n2; k2 += VG * blockDim.x) upd2(k2);
+                    if ((3 * V) % 2 && v == 0 && threadIdx.x == 0) upd(3 * V - 1);
                     block_partial<1>(mx, mm, pbuf(), v, red);
                     mx[0] = 0.0;
                 }
