@@ -83,6 +83,27 @@ struct SrcTab {
     LaunchMap mp;
     __device__ __forceinline__ const Inst& get(int& lb, int& nb) const { return tab[map_block(mp, lb, nb)]; }
 };
+// SrcPar: a group of up to kParInst instances whose descriptors are themselves kernel
+// parameters (~22 KB; fields come from the constant cache like SrcOne's instead of a global
+// table load in front of every gather); a batch is launched as ceil(n / kParInst) groups
+constexpr int kParInst = 30;
+struct SrcPar {
+    int n;
+    int boff[kParInst + 1];
+    Inst I[kParInst];
+    __device__ __forceinline__ const Inst& get(int& lb, int& nb) const {
+        const int b = blockIdx.x;
+        int lo = 0, hi = n;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (boff[mid] <= b) lo = mid;
+            else hi = mid;
+        }
+        lb = b - boff[lo];
+        nb = boff[lo + 1] - boff[lo];
+        return I[lo];
+    }
+};
 
 // An element takes the fully wet Jacobian path when its flag is 0 and every vertex depth
 // at all three levels is positive with a margin no finite-difference perturbation of h

@@ -459,17 +459,28 @@ int make_map(LaunchMap& mp, const std::vector<int>& subset, F blocks) {
 template <class F, class G>
 int launch_map(Runner& R, const std::vector<int>& subset, int threads, F blocks, G go) {
     static thread_local SrcTab t;   // ~2 KB map: not on every caller's stack
+    static thread_local SrcPar par; // ~22 KB
     const int nb = make_map(t.mp, subset, blocks);
     if (nb == 0) return 0;
     if (t.mp.n == 1) {
         SrcOne one;
         one.I = R.tab_h[t.mp.ids[0]];
         go(one, nb, threads);
+        R.launches++;
     } else {
-        t.tab = R.tab.p;
-        go(t, nb, threads);
+        // groups of kParInst instances, descriptors as kernel parameters
+        for (int j0 = 0; j0 < t.mp.n; j0 += kParInst) {
+            const int j1 = std::min(t.mp.n, j0 + kParInst);
+            par.n = j1 - j0;
+            for (int j = j0; j < j1; j++) {
+                par.boff[j - j0] = t.mp.boff[j] - t.mp.boff[j0];
+                par.I[j - j0] = R.tab_h[t.mp.ids[j]];
+            }
+            par.boff[j1 - j0] = t.mp.boff[j1] - t.mp.boff[j0];
+            go(par, par.boff[j1 - j0], threads);
+            R.launches++;
+        }
     }
-    R.launches++;
     CK(cudaGetLastError());
     return 0;
 }
@@ -1214,10 +1225,12 @@ int sw2gpu_autotune(sw2gpu_ctx* c, int32_t* jac_minb, int32_t* stages) {
     const std::vector<int> one(1, 0);
     const size_t nb = sizeof(double) * c->V;
     cudaStream_t st = R.stream;
-    // the residual zeroes old-dry nodes' velocities of the current level: keep a copy
-    double* keep = c->kv64[7].p;
-    CK(cudaMemcpyAsync(keep, c->U(0), nb, cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(keep + c->V, c->Vv(0), nb, cudaMemcpyDeviceToDevice, st));
+    // the residual zeroes old-dry nodes' velocities of the current level: keep a copy (on the
+    // host -- every device work array is written by the kernels being timed)
+    std::vector<double> keep(2 * (size_t)c->V);
+    CK(cudaMemcpyAsync(keep.data(), c->U(0), nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(keep.data() + c->V, c->Vv(0), nb, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     int rc = runner_tables(R, 0);
     if (!rc) rc = launch_resid(R, one);
     if (!rc) rc = read_results(R, one);
@@ -1264,8 +1277,8 @@ int sw2gpu_autotune(sw2gpu_ctx* c, int32_t* jac_minb, int32_t* stages) {
     cudaEventDestroy(e1);
     c->tune_stages = best_s;
     if (!rc) rc = runner_set(R, R.ctx);
-    CK(cudaMemcpyAsync(c->U(0), keep, nb, cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(c->Vv(0), keep + c->V, nb, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(c->U(0), keep.data(), nb, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->Vv(0), keep.data() + c->V, nb, cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
     if (rc) return rc;
     if (jac_minb) *jac_minb = R.jac_minb;

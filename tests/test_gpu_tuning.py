@@ -39,13 +39,18 @@ def test_variants_give_identical_steps(precision):
 
 
 @pytest.mark.gpu
-def test_autotune_keeps_state_and_results():
+@pytest.mark.parametrize("warm_steps", [0, 2])
+def test_autotune_keeps_state_and_results(warm_steps):
+    """Tuning at the start and in mid-run (three distinct time levels, an increment in
+    flight) leaves every level as it was and the following steps unchanged."""
     m = _model()
     g0 = SW2GPU(m)
-    run(g0, 3)
+    run(g0, warm_steps + 3)
     ref = _states(g0)
     g0.close()
     g = SW2GPU(m)
+    if warm_steps:
+        run(g, warm_steps)
     before = _states(g)
     jac, stages = g.autotune()
     assert jac in (1, 2) and stages in (0, 2, 3) and g.variant() == (jac, stages)
