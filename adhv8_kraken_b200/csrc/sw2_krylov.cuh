@@ -231,11 +231,13 @@ struct StageLayout {
 struct KrylovOne {
     KrylovInst Q;
     double rtol;
+    const double* rtol_dev;   // when set, the tolerance is read here (a launch replayed from a
+                              // CUDA graph takes each Newton iteration's tolerance from memory)
     StageLayout lay;
     __device__ __forceinline__ const KrylovInst& get(int& pl, int& np, double& rt) const {
         pl = blockIdx.x;
         np = gridDim.x;
-        rt = rtol;
+        rt = rtol_dev ? __ldcg(rtol_dev) : rtol;
         return Q;
     }
 };

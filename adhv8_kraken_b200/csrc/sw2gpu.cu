@@ -135,6 +135,23 @@ struct sw2gpu_ctx {
     int tune_stages = 3;            // Krylov tile-ring depth (0: sweeps from global memory)
     DevMesh dm{};
     std::unique_ptr<Runner> self;   // runs this instance alone
+    // CUDA graphs of a step's launch sequences (sw2gpu_set_graphs), one set per arrangement of
+    // the three rotating state levels (index lv[0]); recaptured when dt or a variant changes
+    struct StepGraph {
+        cudaGraphExec_t start = nullptr, newton = nullptr;
+        int kernels_start = 0, kernels_newton = 0;
+        double dt = -1.0;
+        int jac_minb = -1, stages = -1;
+    };
+    bool use_graphs = false;
+    StepGraph graphs[3];
+    void drop_graphs() {
+        for (auto& g : graphs) {
+            if (g.start) cudaGraphExecDestroy(g.start);
+            if (g.newton) cudaGraphExecDestroy(g.newton);
+            g = StepGraph();
+        }
+    }
 
     ~sw2gpu_ctx();
     double* H(int l) { return hs[lv[l]].p; }
@@ -199,6 +216,9 @@ void* krylov_kernel(int stages) {
 // timers.  Every kernel launch covers a subset of the instances through a LaunchMap.
 struct Runner {
     cudaStream_t stream = nullptr;
+    bool capturing = false;       // launches are being captured into a CUDA graph
+    DBuf<double> eta_dev;         // Krylov tolerance of a graph-replayed Newton iteration
+    double* eta_h = nullptr;      // its pinned host copy
     std::vector<sw2gpu_ctx*> ctx;
     bool mixed = false;
     DBuf<Inst> tab;
@@ -223,6 +243,7 @@ struct Runner {
     std::vector<int> pkind;
     int nphase = 0;
     ~Runner() {
+        if (eta_h) cudaFreeHost(eta_h);
         for (auto e : pev) cudaEventDestroy(e);
         if (norms_h) cudaFreeHost(norms_h);
         if (ctl_h) cudaFreeHost(ctl_h);
@@ -232,6 +253,7 @@ struct Runner {
 };
 
 sw2gpu_ctx::~sw2gpu_ctx() {
+    drop_graphs();
     self.reset();
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -248,7 +270,7 @@ struct Phase {
     Runner* r;
     int slot;
     Phase(Runner* rr, int kind) : r(rr), slot(-1) {
-        if (r->nphase < Runner::kMaxPhases && !r->pev.empty()) {
+        if (!r->capturing && r->nphase < Runner::kMaxPhases && !r->pev.empty()) {
             slot = r->nphase++;
             r->pkind[slot] = kind;
             cudaEventRecord(r->pev[2 * slot], r->stream);
@@ -323,6 +345,8 @@ int runner_alloc(Runner& R, cudaStream_t stream, bool mixed, int cap) {
     CK(cudaMemsetAsync(R.norms.p, 0, sizeof(Norms) * cap, stream));
     CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * cap, stream));
     CK(cudaMallocHost(&R.norms_h, sizeof(Norms) * cap));
+    CK(cudaMallocHost(&R.eta_h, sizeof(double)));
+    if (R.eta_dev.alloc(1)) return fail(SW2GPU_E_NOMEM, "tolerance word");
     CK(cudaMallocHost(&R.ctl_h, sizeof(KrylovCtl) * cap));
     R.tab_h.resize(cap);
     R.ktab_h.resize(cap);
@@ -510,13 +534,20 @@ int launch_resid(Runner& R, const std::vector<int>& sub) {
 // norms (and Krylov control words) of every instance; the one host sync of an evaluation.
 // `evaluated`: the instances whose residual was just computed (their slots hold fresh norms;
 // the others' slots may hold an earlier occupant's)
-int read_results(Runner& R, const std::vector<int>& evaluated) {
+int enqueue_results(Runner& R) {
     const int K = (int)R.ctx.size();
     CK(cudaMemcpyAsync(R.norms_h, R.norms.p, sizeof(Norms) * K, cudaMemcpyDeviceToHost, R.stream));
     CK(cudaMemcpyAsync(R.ctl_h, R.ctl.p, sizeof(KrylovCtl) * K, cudaMemcpyDeviceToHost, R.stream));
+    return 0;
+}
+int finish_results(Runner& R, const std::vector<int>& evaluated) {
     CK(cudaStreamSynchronize(R.stream));
     for (int k : evaluated) R.ctx[k]->ngeneral = R.norms_h[k].ngeneral;
     return 0;
+}
+int read_results(Runner& R, const std::vector<int>& evaluated) {
+    int rc = enqueue_results(R);
+    return rc ? rc : finish_results(R, evaluated);
 }
 
 int launch_jacobian(Runner& R, const std::vector<int>& sub) {
@@ -528,7 +559,9 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
                  ? launch_map(R, sub, kJacThreads, wet_blocks, SW2_GO_T(k_jac_elem_wet, 1))
                  : launch_map(R, sub, kJacThreads, wet_blocks, SW2_GO_T(k_jac_elem_wet, 2));
     if (rc) return rc;
-    if ((rc = launch_map(R, sub, kJacThreads, [&](int k) { return nblk(C(k)->ngeneral, kJacElems); },
+    // a captured launch covers the largest list (the kernel reads the list's length itself)
+    if ((rc = launch_map(R, sub, kJacThreads,
+                         [&](int k) { return nblk(R.capturing ? C(k)->T : C(k)->ngeneral, kJacElems); },
                          SW2_GO(k_jac_elem_general<std::decay_t<decltype(src)>>))))
         return rc;
     if ((rc = launch_map(R, sub, 128, [&](int k) { return nblk(6LL * C(k)->E, 128); }, SW2_GO(k_jac_edge<std::decay_t<decltype(src)>>)))) return rc;
@@ -591,6 +624,7 @@ int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<doub
             KrylovOne one;
             one.Q = R.ktab_h[grp[0]];
             one.rtol = eta[grp[0]];
+            one.rtol_dev = R.capturing ? R.eta_dev.p : nullptr;
             one.lay = lay;
             void* args[] = {(void*)&one};
             void* kern = R.mixed ? krylov_kernel<float, KrylovOne>(R.stages) : krylov_kernel<double, KrylovOne>(R.stages);
@@ -653,9 +687,8 @@ void newton_begin(Runner& R, int k, NState& ns) {
 
 // one Newton iteration (Jacobian, Krylov, update, residual, line search, convergence test) of
 // every instance of `act`, each in one launch per phase; sets ns[k].done when k's step ends
-int newton_iteration(Runner& R, const std::vector<int>& act, std::vector<NState>& ns) {
-    int rc = launch_jacobian(R, act);
-    if (rc) return rc;
+// Krylov tolerances of the instances' next solves (and their predicted iteration counts)
+std::vector<double> newton_eta(Runner& R, const std::vector<int>& act, const std::vector<NState>& ns) {
     std::vector<double> eta(R.ctx.size(), 0.0);
     for (int k : act) {
         sw2gpu_ctx* c = R.ctx[k];
@@ -664,10 +697,31 @@ int newton_iteration(Runner& R, const std::vector<int>& act, std::vector<NState>
         const int seen = c->its_at[std::min(ns[k].it, 7)];
         if (seen > 0) c->pred_its = seen;
     }
-    if ((rc = launch_linear(R, act, eta))) return rc;
+    return eta;
+}
+
+// the launches of one Newton iteration (Jacobian, Krylov with its update, residual, result copies)
+int newton_launch(Runner& R, const std::vector<int>& act, const std::vector<double>& eta) {
+    int rc = launch_jacobian(R, act);
+    if (!rc) rc = launch_linear(R, act, eta);
+    if (!rc) rc = launch_resid(R, act);
+    if (!rc) rc = enqueue_results(R);
+    return rc;
+}
+
+int newton_finish(Runner& R, const std::vector<int>& act, std::vector<NState>& ns);
+
+int newton_iteration(Runner& R, const std::vector<int>& act, std::vector<NState>& ns) {
+    const std::vector<double> eta = newton_eta(R, act, ns);
     for (int k : act) ns[k].old_l2 = ns[k].l2;
-    if ((rc = launch_resid(R, act))) return rc;
-    if ((rc = read_results(R, act))) return rc;
+    int rc = newton_launch(R, act, eta);
+    return rc ? rc : newton_finish(R, act, ns);
+}
+
+// results of a Newton iteration: line search, convergence test
+int newton_finish(Runner& R, const std::vector<int>& act, std::vector<NState>& ns) {
+    int rc = finish_results(R, act);
+    if (rc) return rc;
     std::vector<int> ls;
     for (int k : act) {
         NState& n = ns[k];
@@ -808,6 +862,112 @@ int runner_step(Runner& R, const double* dt, const double* const* series, sw2gpu
             st.resid_ms = ph[kPhResid];
             st.other_ms = ms - ph[0] - ph[1] - ph[2];
         }
+    }
+    return 0;
+}
+
+
+// captures body()'s launches on R.stream into an executable graph; `kernels` = launches made
+template <class F>
+int capture_graph(Runner& R, cudaGraphExec_t* out, int* kernels, F body) {
+    cudaGraph_t g = nullptr;
+    const int l0 = R.launches;
+    CK(cudaStreamBeginCapture(R.stream, cudaStreamCaptureModeThreadLocal));
+    R.capturing = true;
+    const int rc = body();
+    R.capturing = false;
+    const cudaError_t e = cudaStreamEndCapture(R.stream, &g);
+    *kernels = R.launches - l0;
+    R.launches = l0;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(SW2GPU_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return fail(SW2GPU_E_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ei));
+    return 0;
+}
+
+// the graphs of the current level arrangement, (re)captured if dt or a variant changed since;
+// the descriptors (state pointers of this arrangement, dt) are baked into their launches
+int ensure_graphs(sw2gpu_ctx* c) {
+    Runner& R = *c->self;
+    sw2gpu_ctx::StepGraph& G = c->graphs[c->lv[0]];
+    if (G.start && G.newton && G.dt == c->dt && G.jac_minb == R.jac_minb && G.stages == R.stages) return 0;
+    if (G.start) cudaGraphExecDestroy(G.start);
+    if (G.newton) cudaGraphExecDestroy(G.newton);
+    G = sw2gpu_ctx::StepGraph();
+    const std::vector<int> one(1, 0);
+    int rc = capture_graph(R, &G.start, &G.kernels_start, [&] {
+        int r = launch_init(R, one);
+        if (!r) r = launch_resid(R, one);
+        if (!r) r = enqueue_results(R);
+        return r;
+    });
+    if (!rc) rc = capture_graph(R, &G.newton, &G.kernels_newton, [&] {
+        return newton_launch(R, one, std::vector<double>(1, c->p.lin_rtol));   // tolerance read from eta_dev
+    });
+    if (rc) {
+        if (G.start) cudaGraphExecDestroy(G.start);
+        G = sw2gpu_ctx::StepGraph();
+        return rc;
+    }
+    G.dt = c->dt;
+    G.jac_minb = R.jac_minb;
+    G.stages = R.stages;
+    return 0;
+}
+
+// One time step of a single instance replayed from CUDA graphs: the step start and each
+// Newton iteration are one graph launch each (the iteration's Krylov tolerance goes to the
+// device first); line-search halvings and the failure reset are direct launches.  Same
+// kernels, same arithmetic as runner_step.
+int graph_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* stats, int* status) {
+    Runner& R = *c->self;
+    const std::vector<int> one(1, 0);
+    R.launches = 0;
+    R.nphase = 0;
+    CK(cudaEventRecord(R.ev0, R.stream));
+    int rc = step_begin(R, 0, dt, series);
+    if (!rc) rc = runner_tables(R, 1);
+    if (!rc) rc = ensure_graphs(c);
+    if (rc) return rc;
+    const sw2gpu_ctx::StepGraph& G = c->graphs[c->lv[0]];
+    CK(cudaGraphLaunch(G.start, R.stream));
+    R.launches += G.kernels_start;
+    if ((rc = finish_results(R, one))) return rc;
+    std::vector<NState> ns(1);
+    newton_begin(R, 0, ns[0]);
+    while (!ns[0].done) {
+        const std::vector<double> eta = newton_eta(R, one, ns);
+        *R.eta_h = eta[0];
+        CK(cudaMemcpyAsync(R.eta_dev.p, R.eta_h, sizeof(double), cudaMemcpyHostToDevice, R.stream));
+        ns[0].old_l2 = ns[0].l2;
+        CK(cudaGraphLaunch(G.newton, R.stream));
+        R.launches += G.kernels_newton;
+        if ((rc = newton_finish(R, one, ns))) return rc;
+    }
+    status[0] = newton_status(ns[0], c->p);
+    if (status[0] != SW2GPU_OK && (rc = launch_init(R, one))) return rc;   // reset to the old level
+    CK(cudaEventRecord(R.ev1, R.stream));
+    CK(cudaEventSynchronize(R.ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, R.ev0, R.ev1);
+    if (stats) {
+        const NState& n = ns[0];
+        memset(stats, 0, sizeof(*stats));
+        stats->status = status[0];
+        stats->newton_its = n.it;
+        stats->linear_its = n.lin;
+        stats->linesearch_cuts = n.cuts_total;
+        stats->resid_max = n.rmax;
+        stats->resid_l2 = n.l2;
+        stats->inc_max = n.imax;
+        stats->device_ms = ms;
+        stats->kernel_launches = R.launches;
+        stats->other_ms = ms;   // phases are not timed inside graphs
     }
     return 0;
 }
@@ -1206,6 +1366,7 @@ int sw2gpu_set_variant(sw2gpu_ctx* c, int32_t jac_minb, int32_t stages) {
         return fail(SW2GPU_E_ARG, "variant: jac_minb 1|2, stages 0|2|3");
     c->tune_jac_minb = jac_minb;
     c->tune_stages = stages;
+    c->drop_graphs();
     return runner_set(*c->self, c->self->ctx);
 }
 
@@ -1276,6 +1437,7 @@ int sw2gpu_autotune(sw2gpu_ctx* c, int32_t* jac_minb, int32_t* stages) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->tune_stages = best_s;
+    c->drop_graphs();
     if (!rc) rc = runner_set(R, R.ctx);
     CK(cudaMemcpyAsync(c->U(0), keep.data(), nb, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c->Vv(0), keep.data() + c->V, nb, cudaMemcpyHostToDevice, st));
@@ -1286,11 +1448,18 @@ int sw2gpu_autotune(sw2gpu_ctx* c, int32_t* jac_minb, int32_t* stages) {
     return SW2GPU_OK;
 }
 
+int sw2gpu_set_graphs(sw2gpu_ctx* c, int32_t enable) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    c->drop_graphs();
+    c->use_graphs = enable != 0;
+    return SW2GPU_OK;
+}
+
 int sw2gpu_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* stats) {
     if (!c || !(dt > 0.0)) return fail(SW2GPU_E_ARG, "bad context or dt");
     const double* ser[1] = {series};
     int status = 0;
-    int rc = runner_step(*c->self, &dt, ser, stats, &status);
+    int rc = c->use_graphs ? graph_step(c, dt, ser[0], stats, &status) : runner_step(*c->self, &dt, ser, stats, &status);
     if (rc) return rc;
     if (status != SW2GPU_OK)
         fail(status, "step failed (Newton %d iterations, max residual %g)", stats ? stats->newton_its : -1,
@@ -1675,7 +1844,8 @@ struct sw2gpu_server {
     sw2gpu_engine* eng = nullptr;
     cudaStream_t stream = nullptr;
     int device = 0;
-    std::thread loader, worker;
+    std::vector<std::thread> loaders;   // build admitted requests' contexts in parallel
+    std::thread worker;
 
     void load_loop();
     void work_loop();
@@ -1833,7 +2003,8 @@ int sw2gpu_server_create(int32_t precision, double hbm_fraction, int32_t max_act
         cudaStreamDestroy(S->stream);
         return rc;
     }
-    S->loader = std::thread([S] { S->load_loop(); });
+    const int nload = std::max(1, std::min(4, (int)std::thread::hardware_concurrency() / 2));
+    for (int i = 0; i < nload; i++) S->loaders.emplace_back([S] { S->load_loop(); });
     S->worker = std::thread([S] { S->work_loop(); });
     *out = guard.release();
     return SW2GPU_OK;
@@ -1917,7 +2088,8 @@ int sw2gpu_server_destroy(sw2gpu_server* S) {
         S->stop = true;
         S->cv.notify_all();
     }
-    if (S->loader.joinable()) S->loader.join();
+    for (auto& t : S->loaders)
+        if (t.joinable()) t.join();
     if (S->worker.joinable()) S->worker.join();
     for (auto& q : S->ready)
         if (q->ctx) sw2gpu_destroy(q->ctx);

@@ -207,6 +207,7 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     one.Q.Dinv = dinv;
     for (int k = 0; k < 8; k++) one.Q.vec[k] = v[k];
     one.rtol = rtol;
+    one.rtol_dev = nullptr;
     one.lay = StageLayout{0, 0, 0, 0};
     void* args[] = {(void*)&one};
     cudaError_t e = cudaLaunchCooperativeKernel((void*)k_bicgstab<double, double, 0, KrylovOne>, dim3(grid),

@@ -30,7 +30,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_resid", "sw2gpu_load", "sw2gpu_linear_solve", "sw2gpu_batch_create", "sw2gpu_batch_step",
            "sw2gpu_batch_destroy", "sw2gpu_bcsr_solve_noalloc", "sw2gpu_engine_create", "sw2gpu_engine_add",
            "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_last_tick", "sw2gpu_engine_destroy",
-           "sw2gpu_device_bytes", "sw2gpu_autotune", "sw2gpu_set_variant", "sw2gpu_get_variant", "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait",
+           "sw2gpu_device_bytes", "sw2gpu_autotune", "sw2gpu_set_graphs", "sw2gpu_set_variant", "sw2gpu_get_variant", "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait",
            "sw2gpu_server_status", "sw2gpu_server_destroy"]
 
 
@@ -75,6 +75,7 @@ def lib():
         L.sw2gpu_engine_last_tick.argtypes = [vp, vp]
         L.sw2gpu_device_bytes.argtypes = [vp]
         L.sw2gpu_autotune.argtypes = [vp, c_int32_p, c_int32_p]
+        L.sw2gpu_set_graphs.argtypes = [vp, C.c_int32]
         L.sw2gpu_set_variant.argtypes = [vp, C.c_int32, C.c_int32]
         L.sw2gpu_get_variant.argtypes = [vp, c_int32_p, c_int32_p]
         L.sw2gpu_device_bytes.restype = C.c_int64
@@ -161,6 +162,10 @@ class SW2GPU:
         j, s = C.c_int32(), C.c_int32()
         _check(lib().sw2gpu_autotune(self.h, C.byref(j), C.byref(s)))
         return j.value, s.value
+
+    def set_graphs(self, enable: bool = True):
+        """Replay each step's launch sequences from CUDA graphs (small meshes)."""
+        _check(lib().sw2gpu_set_graphs(self.h, 1 if enable else 0))
 
     def set_variant(self, jac_minb: int, stages: int):
         _check(lib().sw2gpu_set_variant(self.h, jac_minb, stages))

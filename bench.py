@@ -160,6 +160,31 @@ def ensemble_models(n: int, nsteps: int, seed0: int = 7000, procs: int = 0):
         return pool.map(_ensemble_member, [(seed0 + i, nsteps) for i in range(n)])
 
 
+def run_small(stream, steps: int = 20, warmup: int = 3):
+    """Config-1 channel (4,000 triangles), where launches and host round trips are a large
+    part of a step: direct launches vs the step replayed from CUDA graphs."""
+    import torch
+    from adhv8_kraken_b200 import meshgen
+    from adhv8_kraken_b200.sw2 import SW2GPU
+    m = meshgen.channel(nsteps=warmup + steps)
+    out = {"workload": f"config 1 channel: {m.nelems2d} triangles, dt {m.dt} s, {steps} steps after {warmup}"}
+    for name, graphs in (("direct", False), ("graphs", True)):
+        g = SW2GPU(m, stream=stream.cuda_stream)
+        g.set_graphs(graphs)
+        for _ in range(warmup):
+            g.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            st = g.step()
+            assert st["status"] == 0
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / steps
+        g.close()
+        out[name] = {"value": m.nelems2d / (ms * 1e-3), "ms_per_step": ms}
+    return out
+
+
 def _serve_member(args):
     seed, nsteps = args
     from adhv8_kraken_b200 import meshgen
@@ -507,6 +532,7 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
     batched = None
     if ens_models:
         batched = run_ensemble(ens_models, stream, args.ens_steps)
+    small = run_small(stream) if world == 1 else None
     serving = None
     if serve:
         serving = run_serving(serve[0], serve[1], args.serve_rate)
@@ -539,6 +565,7 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
         "roofline": roofline,
         "e2e": e2e,
         "mixed": mixed,
+        "small": small,
         "batched": batched,
         "serving": serving,
         "cpu_baseline": cpu,

@@ -123,6 +123,12 @@ int sw2gpu_destroy(sw2gpu_ctx *ctx);
 int sw2gpu_autotune(sw2gpu_ctx *ctx, int32_t *jac_minb, int32_t *stages);
 int sw2gpu_set_variant(sw2gpu_ctx *ctx, int32_t jac_minb, int32_t stages);
 int sw2gpu_get_variant(const sw2gpu_ctx *ctx, int32_t *jac_minb, int32_t *stages);
+/* CUDA graphs for small meshes, where launches and host round trips are a large part of a
+ * step (no counterpart in the reference): when enabled, sw2gpu_step replays the step start and
+ * each Newton iteration as one graph launch each (captured at first use for each arrangement
+ * of the rotating state levels, recaptured after a dt or variant change).  Same kernels and
+ * results as direct launches; phase times are not reported in graph mode. */
+int sw2gpu_set_graphs(sw2gpu_ctx *ctx, int32_t enable);
 /* device memory the context holds (bytes); no counterpart in the reference */
 int64_t sw2gpu_device_bytes(const sw2gpu_ctx *ctx);
 
@@ -222,8 +228,8 @@ int sw2gpu_engine_destroy(sw2gpu_engine *e);
 /* Request server (no counterpart in the reference): a request loop in the library.  Each
  * submitted solve -- mesh, parameters, initial state, series, number of steps -- is copied,
  * queued and admitted in arrival order when its device bytes fit the budget (a fraction of
- * the device memory free at creation; a request that fits no budget is admitted alone).  A
- * loader thread builds admitted requests' contexts while a worker thread ticks a
+ * the device memory free at creation; a request that fits no budget is admitted alone).
+ * Loader threads build admitted requests' contexts while a worker thread ticks a
  * continuous-batching engine, so requests that arrive while others run share their launches
  * and every solve keeps its state on the device between steps.  Results and per-request
  * times are collected with sw2gpu_server_wait.  One precision per server. */
