@@ -145,6 +145,10 @@ struct sw2gpu_ctx {
     };
     bool use_graphs = false;
     StepGraph graphs[3];
+    // pinned staging of the per-step tables; the event marks the end of their last upload
+    double* stage_h = nullptr;
+    cudaEvent_t stage_ev = nullptr;
+    bool stage_pending = false;
     void drop_graphs() {
         for (auto& g : graphs) {
             if (g.start) cudaGraphExecDestroy(g.start);
@@ -221,10 +225,11 @@ struct Runner {
     double* eta_h = nullptr;      // its pinned host copy
     std::vector<sw2gpu_ctx*> ctx;
     bool mixed = false;
-    DBuf<Inst> tab;
     DBuf<KrylovInst> ktab;
-    std::vector<Inst> tab_h;
-    std::vector<KrylovInst> ktab_h;
+    std::vector<Inst> tab_h;       // descriptors (kernel parameters of every launch)
+    KrylovInst* ktab_h = nullptr;  // pinned; uploaded to ktab for batch Krylov launches
+    cudaEvent_t tab_ev = nullptr;  // end of the last ktab upload
+    bool tab_pending = false;
     DBuf<Norms> norms;
     DBuf<KrylovCtl> ctl;
     DBuf<int> singular;
@@ -243,6 +248,11 @@ struct Runner {
     std::vector<int> pkind;
     int nphase = 0;
     ~Runner() {
+        if (tab_ev) {
+            cudaEventSynchronize(tab_ev);
+            cudaEventDestroy(tab_ev);
+        }
+        if (ktab_h) cudaFreeHost(ktab_h);
         if (eta_h) cudaFreeHost(eta_h);
         for (auto e : pev) cudaEventDestroy(e);
         if (norms_h) cudaFreeHost(norms_h);
@@ -254,6 +264,11 @@ struct Runner {
 
 sw2gpu_ctx::~sw2gpu_ctx() {
     drop_graphs();
+    if (stage_ev) {
+        cudaEventSynchronize(stage_ev);
+        cudaEventDestroy(stage_ev);
+    }
+    if (stage_h) cudaFreeHost(stage_h);
     self.reset();
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -297,13 +312,26 @@ int zalloc(DBuf<T>& b, size_t n, cudaStream_t st) {
 inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
 // per-step tables: string values (edge series), material water sources, Dirichlet values
+// Staging layout (doubles): S string values | M MatParams | 3 x ndir Dirichlet values.
+size_t stage_doubles(const sw2gpu_ctx* c) {
+    return (size_t)std::max(c->S, 1) + (sizeof(MatParams) * std::max(c->M, 1) + 7) / 8 + 3 * c->dir_node.size() + 1;
+}
+
+// per-step tables through the context's pinned staging buffer (no host sync; the buffer is
+// rewritten only after its last upload completed)
 int upload_step_tables(sw2gpu_ctx* c, const double* series, cudaStream_t st) {
-    std::vector<double> sv(std::max(c->S, 1), 0.0);
+    if (c->stage_pending) {
+        CK(cudaEventSynchronize(c->stage_ev));
+        c->stage_pending = false;
+    }
+    double* sv = c->stage_h;
+    MatParams* mp = reinterpret_cast<MatParams*>(sv + std::max(c->S, 1));
+    double* dv = sv + std::max(c->S, 1) + (sizeof(MatParams) * std::max(c->M, 1) + 7) / 8;
     for (int s = 0; s < c->S; s++) {
         int k = c->str_isigma[s];
-        if (k >= 0 && k < c->NS && series) sv[s] = series[k];
+        sv[s] = (k >= 0 && k < c->NS && series) ? series[k] : 0.0;
     }
-    CK(cudaMemcpyAsync(c->str_value.p, sv.data(), sizeof(double) * c->S, cudaMemcpyHostToDevice, st));
+    if (c->S) CK(cudaMemcpyAsync(c->str_value.p, sv, sizeof(double) * c->S, cudaMemcpyHostToDevice, st));
     bool any_src = false;
     for (int m = 0; m < c->M; m++) {
         if (c->mats_h[m].has_source) {
@@ -312,11 +340,13 @@ int upload_step_tables(sw2gpu_ctx* c, const double* series, cudaStream_t st) {
             any_src = true;
         }
     }
-    if (any_src)
-        CK(cudaMemcpyAsync(c->mats.p, c->mats_h.data(), sizeof(MatParams) * c->M, cudaMemcpyHostToDevice, st));
+    if (any_src) {
+        memcpy(mp, c->mats_h.data(), sizeof(MatParams) * c->M);
+        CK(cudaMemcpyAsync(c->mats.p, mp, sizeof(MatParams) * c->M, cudaMemcpyHostToDevice, st));
+    }
     const int nd = (int)c->dir_node.size();
     if (nd) {
-        std::vector<double> h(nd, 0.0), u(nd, 0.0), v(nd, 0.0);
+        double *h = dv, *u = dv + nd, *v = dv + 2 * nd;
         for (int i = 0; i < nd; i++) {
             int s = c->dir_str[i];
             auto get = [&](int k) { return (k >= 0 && k < c->NS && series) ? series[k] : 0.0; };
@@ -324,12 +354,12 @@ int upload_step_tables(sw2gpu_ctx* c, const double* series, cudaStream_t st) {
             v[i] = get(c->str_ivy[s]);
             h[i] = get(c->str_iu0[s]);
         }
-        CK(cudaMemcpyAsync(c->dir_h.p, h.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(c->dir_u.p, u.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(c->dir_v.p, v.data(), sizeof(double) * nd, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->dir_h.p, h, sizeof(double) * nd, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->dir_u.p, u, sizeof(double) * nd, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->dir_v.p, v, sizeof(double) * nd, cudaMemcpyHostToDevice, st));
     }
-    // the host copy of the step tables is pageable: finish before it changes
-    CK(cudaStreamSynchronize(st));
+    CK(cudaEventRecord(c->stage_ev, st));
+    c->stage_pending = true;
     return 0;
 }
 
@@ -340,7 +370,7 @@ int runner_alloc(Runner& R, cudaStream_t stream, bool mixed, int cap) {
     R.stream = stream;
     R.mixed = mixed;
     R.cap = cap;
-    if (R.tab.alloc(cap) || R.ktab.alloc(cap) || R.norms.alloc(cap) || R.ctl.alloc(cap) || R.singular.alloc(cap))
+    if (R.ktab.alloc(cap) || R.norms.alloc(cap) || R.ctl.alloc(cap) || R.singular.alloc(cap))
         return fail(SW2GPU_E_NOMEM, "batch tables");
     CK(cudaMemsetAsync(R.norms.p, 0, sizeof(Norms) * cap, stream));
     CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * cap, stream));
@@ -349,7 +379,8 @@ int runner_alloc(Runner& R, cudaStream_t stream, bool mixed, int cap) {
     if (R.eta_dev.alloc(1)) return fail(SW2GPU_E_NOMEM, "tolerance word");
     CK(cudaMallocHost(&R.ctl_h, sizeof(KrylovCtl) * cap));
     R.tab_h.resize(cap);
-    R.ktab_h.resize(cap);
+    CK(cudaMallocHost(&R.ktab_h, sizeof(KrylovInst) * cap));
+    CK(cudaEventCreateWithFlags(&R.tab_ev, cudaEventDisableTiming));
     CK(cudaEventCreate(&R.ev0));
     CK(cudaEventCreate(&R.ev1));
     R.pev.resize(2 * Runner::kMaxPhases);
@@ -419,6 +450,10 @@ int runner_init(Runner& R, const std::vector<sw2gpu_ctx*>& ctx, cudaStream_t str
 // device tables from the instances' current buffers and state levels
 int runner_tables(Runner& R, int apply_inc) {
     const int K = (int)R.ctx.size();
+    if (R.tab_pending) {   // the pinned Krylov table is rewritten only after its last upload
+        CK(cudaEventSynchronize(R.tab_ev));
+        R.tab_pending = false;
+    }
     for (int k = 0; k < K; k++) {
         sw2gpu_ctx* c = R.ctx[k];
         Inst& I = R.tab_h[k];
@@ -453,10 +488,12 @@ int runner_tables(Runner& R, int apply_inc) {
         Q.Dinv = c->dinv64.p;
         for (int v = 0; v < 8; v++) Q.vec[v] = c->kv64[v].p;
     }
-    CK(cudaMemcpyAsync(R.tab.p, R.tab_h.data(), sizeof(Inst) * K, cudaMemcpyHostToDevice, R.stream));
-    CK(cudaMemcpyAsync(R.ktab.p, R.ktab_h.data(), sizeof(KrylovInst) * K, cudaMemcpyHostToDevice, R.stream));
-    // pageable source: complete before the host tables change again
-    CK(cudaStreamSynchronize(R.stream));
+    // the descriptors travel as kernel parameters; only batch Krylov launches read a table
+    if (K > 1) {
+        CK(cudaMemcpyAsync(R.ktab.p, R.ktab_h, sizeof(KrylovInst) * K, cudaMemcpyHostToDevice, R.stream));
+        CK(cudaEventRecord(R.tab_ev, R.stream));
+        R.tab_pending = true;
+    }
     return 0;
 }
 
@@ -1228,6 +1265,8 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
         const unsigned esz = mixed ? sizeof(float) : sizeof(double);
         stage_caps(c->orowptr_h, V, esz, c->a_cap, c->c_cap);
     }
+    CK(cudaMallocHost(&c->stage_h, sizeof(double) * stage_doubles(c)));
+    CK(cudaEventCreateWithFlags(&c->stage_ev, cudaEventDisableTiming));
     std::vector<sw2gpu_ctx*> me(1, c);
     c->self.reset(new Runner());
     if ((rc = runner_init(*c->self, me, st))) return rc;
