@@ -584,12 +584,27 @@ __global__ void k_jac_gather(const __grid_constant__ Src src) {
     const long long t = (long long)lb * blockDim.x + threadIdx.x;
     if (t >= (long long)m.nnzb * 9) return;
     const int k = (int)(t / 9), q = (int)(t % 9);
+    const int c0 = m.blk_ptr[k], c1 = m.blk_ptr[k + 1];
+    // up to eight contributions' slot indices, then their values, are in flight together; the
+    // sum runs in contribution (reference) order
     double acc = 0.0;
-    for (int c = m.blk_ptr[k]; c < m.blk_ptr[k + 1]; c++) acc += jslots[(size_t)m.blk_src[c] * 9 + q];
+    for (int c = c0; c < c1; c += 8) {
+        int src[8];
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) src[u] = (c + u < c1) ? m.blk_src[c + u] : -1;
+#pragma unroll
+        for (int u = 0; u < 8; u++) v[u] = src[u] >= 0 ? jslots[(size_t)src[u] * 9 + q] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (c + u < c1) acc += v[u];
+    }
     val[t] = acc;
 }
 
-// Tiny-diagonal fix of fe_sw2_load (:218-236) and the Jacobi scale vector of spv_jacobi
+// Tiny-diagonal fix of fe_sw2_load (:218-236), the Jacobi scale vector of spv_jacobi and the
+// inverse of the scaled diagonal block (the block-Jacobi preconditioner, folded into the
+// off-diagonal blocks by k_fold_offdiag) in one pass per node row
 // (src/solver/spv_jacobi.c:222-285): S = 1/sqrt(max |row entry|), floored.  Also writes
 // the scaled right-hand side b = S R.
 template <class Src>
@@ -623,39 +638,28 @@ __global__ void k_rowscale(const __grid_constant__ Src src, int fix_only) {
 #pragma unroll
             for (int c = 0; c < 3; c++) mx[r] = fmax(mx[r], fabs(a[3 * r + c]));
     }
+    double sr[3];
 #pragma unroll
     for (int r = 0; r < 3; r++) {
         const double sv = (mx[r] < kSmall) ? 1.0 / sqrt(kSmall) : 1.0 / sqrt(fabs(mx[r]));
+        sr[r] = sv;
         S[3 * n + r] = sv;
         b[3 * n + r] = R[3 * n + r] * sv;
     }
+    // D_n^-1 of the scaled diagonal block S_n A_nn S_n
+    double a[9];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) a[3 * r + c] = d[3 * r + c] * (sr[r] * sr[c]);
+    if (!inv3(a, I.dinv + (size_t)n * 9)) atomicExch(I.singular, 1);
 }
 
 // Block-Jacobi preconditioner folded into the matrix.  With A' = S A S (spv_jacobi scaling)
 // and D_i the scaled diagonal block of row i, the Krylov operator M^-1 A' has identity
 // diagonal blocks and off-diagonal blocks D_i^-1 A'_ij, so the sweeps stream only those
-// (nnzb - V blocks, no inverses).  k_fold_diag: D_i^-1 per node row (FP64).
-template <class Src>
-__global__ void k_fold_diag(const __grid_constant__ Src src) {
-    int lb, nb;
-    const Inst& I = src.get(lb, nb);
-    const DevMesh m = I.m;
-    const double* __restrict__ val = I.val;
-    const double* __restrict__ S = I.S;
-    double* __restrict__ dinv = I.dinv;
-    int* singular = I.singular;
-    const int i = lb * blockDim.x + threadIdx.x;
-    if (i >= m.V) return;
-    const double* v = val + (size_t)m.dpos[i] * 9;
-    double a[9];
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) a[3 * r + c] = v[3 * r + c] * (S[3 * i + r] * S[3 * i + c]);
-    if (!inv3(a, dinv + (size_t)i * 9)) atomicExch(singular, 1);
-}
-
-// off-diagonal block k of row i -> position k - i - (k > dpos_i) of the folded matrix,
+// (nnzb - V blocks, no inverses).  D_i^-1 comes from k_rowscale; the off-diagonal block k of
+// row i goes to position k - i - (k > dpos_i) of the folded matrix,
 // D_i^-1 (S_i A_ij S_j) formed in FP64 and stored as MT
 template <class Src, typename MT>
 __global__ void k_fold_offdiag(const __grid_constant__ Src src) {

@@ -636,10 +636,9 @@ std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub) {
 int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<double>& eta, int fix_only_unused = 0) {
     (void)fix_only_unused;
     auto C = [&](int k) { return R.ctx[k]; };
+    CK(cudaMemsetAsync(R.singular.p, 0, sizeof(int) * R.ctx.size(), R.stream));
     int rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, SW2_GO(k_rowscale<std::decay_t<decltype(src)>>, 0));
     if (rc) return rc;
-    CK(cudaMemsetAsync(R.singular.p, 0, sizeof(int) * R.ctx.size(), R.stream));
-    if ((rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, SW2_GO(k_fold_diag<std::decay_t<decltype(src)>>)))) return rc;
     if (R.mixed)
         rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->nnzb, 256); }, SW2_GO_T(k_fold_offdiag, float));
     else
