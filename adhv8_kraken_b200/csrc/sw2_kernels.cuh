@@ -354,10 +354,15 @@ __global__ void __launch_bounds__(kGatherThreads) k_resid_gather(const __grid_co
 constexpr int kJacElems = 32;
 constexpr int kJacThreads = kJacElems * 9;
 
-struct __align__(16) StagedElem {
+// Lane l of a warp reads element l's record: an odd record stride in 8-byte words puts the
+// 32 lanes' doubles in distinct bank pairs (an even stride such as 48 words would make every
+// lane's read hit the same banks).
+struct StagedElem {
     ElemIn in;
     int n[3], df[3], wd, mat;
 };
+static_assert(sizeof(StagedElem) % 8 == 0 && (sizeof(StagedElem) / 8) % 2 == 1, "odd record stride");
+static_assert(sizeof(WetPre) % 8 == 0 && (sizeof(WetPre) / 8) % 2 == 1, "odd record stride");
 
 // GENERAL = false: every element, fully wet physics inlined (register-lean), elements not
 // eligible for it are skipped (their records are rewritten by the general launch, which runs
@@ -367,6 +372,7 @@ __device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, 
                                               double* __restrict__ jslots, const unsigned char* __restrict__ ewet,
                                               const int* __restrict__ list, int count, int lb) {
     __shared__ StagedElem se[kJacElems];
+    __shared__ WetPre pre[GENERAL ? 1 : kJacElems];
     __shared__ double out[kJacElems * 81];
     __shared__ int eid[kJacElems];
     const int e0 = lb * kJacElems;
@@ -388,6 +394,17 @@ __device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, 
         }
     }
     __syncthreads();
+    if (!GENERAL) {
+        // the parts of the wet residual that depend on the old levels, the depth or the
+        // velocity alone, at the unperturbed iterate, once per element (warps 0, 1, 2)
+        if (item < 3 && eid[lane] >= 0) {
+            const StagedElem& S = se[lane];
+            if (item == 0) wet_levels(S.in, P, pre[lane].L);
+            else if (item == 1) wet_depth(S.in, S.in.h, P, m.mats[S.mat], pre[lane].D);
+            else wet_pre_velocity(S.in, pre[lane]);
+        }
+        __syncthreads();
+    }
     if (eid[lane] >= 0) {
         const StagedElem& S = se[lane];
         const int b = item / 3, var = item % 3;  // var: 0 = u, 1 = v, 2 = h
@@ -409,6 +426,10 @@ __device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, 
         }
         const double eps = fd_eps(cur);
         const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
+        // what this column leaves unperturbed (GENERAL = false reads those parts from `pre`)
+        const unsigned fix = (var == 0)   ? (kFixH | kFixV | ((7u & ~(1u << b)) << kFixNode))
+                             : (var == 1) ? (kFixH | kFixU | ((7u & ~(1u << b)) << kFixNode))
+                                          : (kFixU | kFixV | (7u << kFixNode));
         // Dirichlet zeroing of the element matrix (fe_assign_mom_db_dof3 / fe_assign_dacont_db_dof3):
         // D = momentum-Dirichlet nodes (old-dry or VEL/VEL_PRS string), P = continuity-Dirichlet.
         unsigned Dm = 0, Pm = 0;
@@ -437,7 +458,7 @@ __device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, 
             }
             double r[3][3];
             if (GENERAL) sw2_elem_resid(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, r);
-            else elem_resid_impl<true>(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, r);
+            else elem_resid_impl<true, true>(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, r, &pre[lane], fix);
 #pragma unroll
             for (int a = 0; a < 3; a++) {
 #pragma unroll

@@ -221,50 +221,178 @@ __device__ __forceinline__ double drag_coef(double depth, double ks) {  // fr_be
 }
 
 // ---------------------------------------------------------------------------------
+// Parts of the fully wet residual that depend on one part of the iterate only.  An FD
+// Jacobian column perturbs one variable at one vertex, so what depends only on the old
+// levels, only on the depth or only on the velocity is shared by many of an element's 18
+// perturbed evaluations: the Jacobian kernel forms those parts once per element (wet_levels,
+// wet_depth, wet_pre_velocity) and the evaluations read them back.  Each part is formed by
+// the same function either way, so the residual has the same bits however a part was obtained.
+__device__ __forceinline__ double dot3(const double* f, const double* g) {
+    double s = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) s += f[i] * g[i];
+    return s;
+}
+__device__ __forceinline__ double avg3(const double* f) { return (f[0] + f[1] + f[2]) / 3.0; }
+// integral of a vertex quantity over the (fully wet) element, as the wrapped integrands form it
+__device__ __forceinline__ double wet_integral(const double* f, double djac) { return 0.0 + djac * avg3(f); }
+// temporal term of one level (fe_sw2_temporal :1288-1354) with the wet/dry factor 1
+__device__ __forceinline__ void wet_temporal(const double* H, const double* U, const double* V, double djac, double dtf,
+                                             double dll, bool cont, double (&c)[3][3]) {
+    const double fs = H[0] + H[1] + H[2], t1 = djac * dtf * kOne12;
+    const double con = dtf * 1.0;
+    const double t2 = djac * con * kOne3;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        if (cont) c[i][0] = 0.0 + t1 * (fs + H[i]);
+        c[i][1] = t2 * (U[i] * fmax(H[i], dll));
+        c[i][2] = t2 * (V[i] * fmax(H[i], dll));
+    }
+}
+
+struct WetLevels {              // old and older levels
+    double gzx, gzy, le, d0[3]; // d0: minus the old-level integrals of h, u, v (SUPG)
+    double to[3][3], too[3][3]; // t(n) and t(n-1) temporal contributions [vertex][eq]
+};
+struct WetDepth {               // current depth
+    double ghx, ghy, hint, h_wd, rough, resistance, tnc[3];
+};
+struct WetVel {                 // one current velocity component
+    double avg, gx, gy, vint, wd;
+};
+struct WetPre {
+    WetLevels L;
+    WetDepth D;
+    WetVel U, V;
+    double vmag, vst_i, vst_j, vwd_mag;     // both velocity components
+    double fx[3], fy[3];                    // per-vertex friction fluxes
+};
+// which parts an evaluation leaves unchanged: kFixH / kFixU / kFixV, and vertex i's velocity
+// unchanged at bit kFixNode + i
+enum WetFix : unsigned { kFixH = 1u, kFixU = 2u, kFixV = 4u, kFixNode = 3 };
+
+__device__ __forceinline__ void wet_levels(const ElemIn& in, const PhysParams& P, WetLevels& L) {
+    L.gzx = dot3(in.z, in.gx);
+    L.gzy = dot3(in.z, in.gy);
+    L.le = sqrt(in.djac * 1.0);
+    L.d0[0] = -wet_integral(in.ho, in.djac);
+    L.d0[1] = -wet_integral(in.uo, in.djac);
+    L.d0[2] = -wet_integral(in.vo, in.djac);
+    wet_temporal(in.ho, in.uo, in.vo, in.djac, (-1.) * (1. + P.alpha), P.dll, true, L.to);
+    if (P.alpha != 0.0) wet_temporal(in.hoo, in.uoo, in.voo, in.djac, P.alpha / 2., P.dll, true, L.too);
+}
+__device__ __forceinline__ void wet_depth(const ElemIn& in, const double* hc, const PhysParams& P, const MatParams& M,
+                                          WetDepth& D) {
+    D.ghx = dot3(hc, in.gx);
+    D.ghy = dot3(hc, in.gy);
+    D.hint = wet_integral(hc, in.djac);
+    D.h_wd = D.hint / in.djac;
+    const double h_fric = fmax(D.h_wd, kSmall);
+    D.rough = (M.ks > kSmall) ? drag_coef(h_fric, M.ks) : 0.0;
+    D.resistance = D.rough / (2.0 * P.g);
+    double c[3][3];
+    wet_temporal(hc, hc, hc, in.djac, 1. + P.alpha / 2., P.dll, true, c);
+#pragma unroll
+    for (int i = 0; i < 3; i++) D.tnc[i] = c[i][0];
+}
+__device__ __forceinline__ void wet_vel(const ElemIn& in, const double* f, WetVel& W) {
+    W.avg = avg3(f);
+    W.gx = dot3(f, in.gx);
+    W.gy = dot3(f, in.gy);
+    W.vint = wet_integral(f, in.djac);
+    W.wd = W.vint / in.djac;
+}
+__device__ __forceinline__ void flow_dir(double ua, double va, double& vmag, double& vi, double& vj) {
+    vmag = sqrt(ua * ua + va * va);
+    vi = ua / fmax(vmag, 1.E-8);
+    vj = va / fmax(vmag, 1.E-8);
+}
+__device__ __forceinline__ void friction_flux(double u, double v, double& fx, double& fy) {
+    const double m = sqrt(u * u + v * v);
+    fx = u * m;
+    fy = v * m;
+}
+__device__ __forceinline__ void wet_pre_velocity(const ElemIn& in, WetPre& p) {
+    wet_vel(in, in.u, p.U);
+    wet_vel(in, in.v, p.V);
+    flow_dir(p.U.avg, p.V.avg, p.vmag, p.vst_i, p.vst_j);
+    p.vwd_mag = sqrt(p.U.wd * p.U.wd + p.V.wd * p.V.wd);
+#pragma unroll
+    for (int i = 0; i < 3; i++) friction_flux(in.u[i], in.v[i], p.fx[i], p.fy[i]);
+}
+
+// ---------------------------------------------------------------------------------
 // the element residual
 //   in:       the element's static data and old / older levels (may live in shared memory)
 //   hc,uc,vc: the current iterate at the three vertices, perturbation applied (registers)
 //   wd_flag:  element wet/dry flag of the Newton solve (fe_sw2_wdflag)
 //   pvar:     kPertNone / kPertU / kPertV / kPertH (u, v perturbations drop the pressure terms)
 //   dflag[3]: Dirichlet flags of the element's nodes (bit0 PRS_DIR, bit1 VEL_DIR, bit2 VEL_PRS_DIR)
-template <bool WET>
+//   PRE:      (fully wet only) the parts named by `fix` are read from `pre` (see WetPre)
+template <bool WET, bool PRE = false>
 __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* hc, const double* uc, const double* vc,
                                                 int wd_flag, int pvar, const PhysParams& P, const MatParams& M,
-                                                const int* dflag, double (&er)[3][3]) {
+                                                const int* dflag, double (&er)[3][3], const WetPre* pre = nullptr,
+                                                unsigned fix = 0u) {
+    static_assert(WET || !PRE, "precomputed parts exist for fully wet elements only");
     const double djac = in.djac, dt = P.dt, g = P.g, dll = P.dll, dul = P.dul;
     const double* gx = in.gx;
     const double* gy = in.gy;
     const bool pressure = !(pvar == kPertU || pvar == kPertV);
+    const bool fh = PRE && (fix & kFixH), fu = PRE && (fix & kFixU), fv = PRE && (fix & kFixV);
 
     // averages and gradients (:193-221)
-    double u_avg = (uc[0] + uc[1] + uc[2]) / 3.0;
-    double v_avg = (vc[0] + vc[1] + vc[2]) / 3.0;
-    double gzx = 0, gzy = 0, ghx = 0, ghy = 0, gux = 0, guy = 0, gvx = 0, gvy = 0;
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-        gzx += in.z[i] * gx[i];
-        gzy += in.z[i] * gy[i];
-        ghx += hc[i] * gx[i];
-        ghy += hc[i] * gy[i];
+    WetDepth D;
+    WetVel Uw, Vw;
+    if (fu) Uw = pre->U;
+    else wet_vel(in, uc, Uw);
+    if (fv) Vw = pre->V;
+    else wet_vel(in, vc, Vw);
+    const double u_avg = Uw.avg, v_avg = Vw.avg;
+    const double gux = Uw.gx, guy = Uw.gy, gvx = Vw.gx, gvy = Vw.gy;
+    double gzx, gzy, ghx, ghy;
+    if (PRE) {
+        gzx = pre->L.gzx;
+        gzy = pre->L.gzy;
+    } else {
+        gzx = dot3(in.z, gx);
+        gzy = dot3(in.z, gy);
     }
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-        gux += uc[i] * gx[i];
-        guy += uc[i] * gy[i];
-        gvx += vc[i] * gx[i];
-        gvy += vc[i] * gy[i];
+    if (WET) {
+        if (fh) D = pre->D;
+        else wet_depth(in, hc, P, M, D);
+        ghx = D.ghx;
+        ghy = D.ghy;
+    } else {
+        ghx = dot3(hc, gx);
+        ghy = dot3(hc, gy);
     }
     const double gwx = gzx + ghx, gwy = gzy + ghy;
-    const double vmag = sqrt(u_avg * u_avg + v_avg * v_avg);
-    const double vst_i = u_avg / fmax(vmag, 1.E-8), vst_j = v_avg / fmax(vmag, 1.E-8);
+    double vmag, vst_i, vst_j;
+    if (fu && fv) {
+        vmag = pre->vmag;
+        vst_i = pre->vst_i;
+        vst_j = pre->vst_j;
+    } else {
+        flow_dir(u_avg, v_avg, vmag, vst_i, vst_j);
+    }
 
-    double h_wd, u_wd, v_wd;
-    double factor = wd_average<WET>(in.x, in.y, hc, uc, vc, djac, h_wd, u_wd, v_wd);
-    const double factor_old = WET ? 1.0 : clip_factor(in.x, in.y, in.ho, djac);
-    const double factor_older = WET ? 1.0 : clip_factor(in.x, in.y, in.hoo, djac);
-    const double vwd_mag = sqrt(u_wd * u_wd + v_wd * v_wd);
+    double h_wd, u_wd, v_wd, factor, factor_old, factor_older, vwd_mag, rough;
+    if (WET) {      // the wrapper's full-element case: factors 1, wetted-area averages
+        h_wd = D.h_wd;
+        u_wd = Uw.wd;
+        v_wd = Vw.wd;
+        factor = factor_old = factor_older = 1.0;
+        vwd_mag = (fu && fv) ? pre->vwd_mag : sqrt(u_wd * u_wd + v_wd * v_wd);
+        rough = D.rough;
+    } else {
+        factor = wd_average<WET>(in.x, in.y, hc, uc, vc, djac, h_wd, u_wd, v_wd);
+        factor_old = clip_factor(in.x, in.y, in.ho, djac);
+        factor_older = clip_factor(in.x, in.y, in.hoo, djac);
+        vwd_mag = sqrt(u_wd * u_wd + v_wd * v_wd);
+        rough = (M.ks > kSmall) ? drag_coef(fmax(h_wd, kSmall), M.ks) : 0.0;
+    }
     const double h_fric = fmax(h_wd, kSmall);
-    const double rough = (M.ks > kSmall) ? drag_coef(h_fric, M.ks) : 0.0;
 
     // eddy viscosity (:263-291, fe_sw2_get_EEVF.c:33-60)
     double ev_st, ev_tr;
@@ -367,7 +495,30 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
     }
 
     // temporal terms t(n+1), t(n), t(n-1) (:481-490, fe_sw2_temporal :1288-1354)
-    {
+    if (WET) {
+        auto add = [&](const double (&c)[3][3], bool cont) {
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+                    if (q > 0 || cont) er[i][q] += c[i][q];
+        };
+        double c[3][3];
+        wet_temporal(hc, uc, vc, djac, 1. + P.alpha / 2., dll, false, c);
+#pragma unroll
+        for (int i = 0; i < 3; i++) c[i][0] = D.tnc[i];
+        add(c, true);
+        // the old levels' continuity part is dropped for wet/dry flag 2, as in the wrapped form
+        if (PRE) {
+            add(pre->L.to, wd_flag != 2);
+            if (P.alpha != 0.0) add(pre->L.too, wd_flag != 2);
+        } else {
+            WetLevels L;
+            wet_levels(in, P, L);
+            add(L.to, wd_flag != 2);
+            if (P.alpha != 0.0) add(L.too, wd_flag != 2);
+        }
+    } else {
         auto temporal = [&](const double* H, const double* U, const double* V, double wdf, double dtf, int flag) {
             double rhs[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
             auto integ = [&](const double*, const double*, const double* Hc, const double*, const double*, double dj,
@@ -408,14 +559,17 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
     }
 
     // bottom friction (:557-577)
-    const double resistance = rough / (2.0 * g);
+    const double resistance = WET ? D.resistance : rough / (2.0 * g);
     {
         double fx[3], fy[3];
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            double m = sqrt(uc[i] * uc[i] + vc[i] * vc[i]);
-            fx[i] = uc[i] * m;
-            fy[i] = vc[i] * m;
+            if (PRE && ((fix >> (kFixNode + i)) & 1u)) {
+                fx[i] = pre->fx[i];
+                fy[i] = pre->fy[i];
+            } else {
+                friction_flux(uc[i], vc[i], fx[i], fy[i]);
+            }
         }
         const double t1 = djac * (dt * g * resistance * factor) * kOne12;
         const double sx = fx[0] + fx[1] + fx[2], sy = fy[0] + fy[1] + fy[2];
@@ -509,38 +663,54 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
     if (!(fabs(h_wd) < kSmall)) {
         const double gf = g;
         const double hden = fmax(h_wd, kNotQuiteSmall);
-        const double le = sqrt(djac * factor_old);
+        const double le = PRE ? pre->L.le : sqrt(djac * factor_old);
         double c2 = gf * hden;
         if (hden <= 0.0) c2 = 0.;
         const double sr = sqrt(u_wd * u_wd + v_wd * v_wd + c2 + kSmall);
         const double tau = P.tau_pg * le / sr;
         // elementally averaged wet/dry time derivatives (wrapped fe_sw2_wd_integrate_triangle_f)
         double dhdt, dudt, dvdt;
-        {
-            double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-            auto integ = [&](const double*, const double*, const double* H, const double*, const double*, double dj,
-                             bool clipped, const Clip& c, double (&r)[3][3]) {
-                r[0][0] += dj * ((H[0] + H[1] + H[2]) / 3.0);
-                r[0][1] += dj * ((cval(c, clipped, in.uo, 0) + cval(c, clipped, in.uo, 1) + cval(c, clipped, in.uo, 2)) / 3.0);
-                r[0][2] += dj * ((cval(c, clipped, in.vo, 0) + cval(c, clipped, in.vo, 1) + cval(c, clipped, in.vo, 2)) / 3.0);
-            };
-            wd_apply<WET>(in.x, in.y, in.ho, nullptr, nullptr, djac, 0, acc, integ);
-            dhdt = -acc[0][0];
-            dudt = -acc[0][1];
-            dvdt = -acc[0][2];
-        }
-        {
-            double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-            auto integ = [&](const double*, const double*, const double* H, const double*, const double*, double dj,
-                             bool clipped, const Clip& c, double (&r)[3][3]) {
-                r[0][0] += dj * ((H[0] + H[1] + H[2]) / 3.0);
-                r[0][1] += dj * ((cval(c, clipped, uc, 0) + cval(c, clipped, uc, 1) + cval(c, clipped, uc, 2)) / 3.0);
-                r[0][2] += dj * ((cval(c, clipped, vc, 0) + cval(c, clipped, vc, 1) + cval(c, clipped, vc, 2)) / 3.0);
-            };
-            wd_apply<WET>(in.x, in.y, hc, nullptr, nullptr, djac, 0, acc, integ);
-            dhdt += acc[0][0];
-            dudt += acc[0][1];
-            dvdt += acc[0][2];
+        if (WET) {
+            double d0[3];
+            if (PRE) {
+                d0[0] = pre->L.d0[0];
+                d0[1] = pre->L.d0[1];
+                d0[2] = pre->L.d0[2];
+            } else {
+                d0[0] = -wet_integral(in.ho, djac);
+                d0[1] = -wet_integral(in.uo, djac);
+                d0[2] = -wet_integral(in.vo, djac);
+            }
+            dhdt = d0[0] + D.hint;
+            dudt = d0[1] + Uw.vint;
+            dvdt = d0[2] + Vw.vint;
+        } else {
+            {
+                double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+                auto integ = [&](const double*, const double*, const double* H, const double*, const double*, double dj,
+                                 bool clipped, const Clip& c, double (&r)[3][3]) {
+                    r[0][0] += dj * ((H[0] + H[1] + H[2]) / 3.0);
+                    r[0][1] += dj * ((cval(c, clipped, in.uo, 0) + cval(c, clipped, in.uo, 1) + cval(c, clipped, in.uo, 2)) / 3.0);
+                    r[0][2] += dj * ((cval(c, clipped, in.vo, 0) + cval(c, clipped, in.vo, 1) + cval(c, clipped, in.vo, 2)) / 3.0);
+                };
+                wd_apply<WET>(in.x, in.y, in.ho, nullptr, nullptr, djac, 0, acc, integ);
+                dhdt = -acc[0][0];
+                dudt = -acc[0][1];
+                dvdt = -acc[0][2];
+            }
+            {
+                double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+                auto integ = [&](const double*, const double*, const double* H, const double*, const double*, double dj,
+                                 bool clipped, const Clip& c, double (&r)[3][3]) {
+                    r[0][0] += dj * ((H[0] + H[1] + H[2]) / 3.0);
+                    r[0][1] += dj * ((cval(c, clipped, uc, 0) + cval(c, clipped, uc, 1) + cval(c, clipped, uc, 2)) / 3.0);
+                    r[0][2] += dj * ((cval(c, clipped, vc, 0) + cval(c, clipped, vc, 1) + cval(c, clipped, vc, 2)) / 3.0);
+                };
+                wd_apply<WET>(in.x, in.y, hc, nullptr, nullptr, djac, 0, acc, integ);
+                dhdt += acc[0][0];
+                dudt += acc[0][1];
+                dvdt += acc[0][2];
+            }
         }
         factor = WET ? 1.0 : clip_factor(in.x, in.y, hc, djac);
         double adv[3] = {0, 0, 0};
