@@ -77,6 +77,12 @@ struct SrcOne {
         nb = gridDim.x;
         return I;
     }
+    // block v of a persistent launch that walks nvirt blocks
+    __device__ __forceinline__ const Inst& get_at(int v, int nvirt, int& lb, int& nb) const {
+        lb = v;
+        nb = nvirt;
+        return I;
+    }
 };
 struct SrcTab {
     const Inst* tab;
@@ -91,8 +97,9 @@ struct SrcPar {
     int n;
     int boff[kParInst + 1];
     Inst I[kParInst];
-    __device__ __forceinline__ const Inst& get(int& lb, int& nb) const {
-        const int b = blockIdx.x;
+    __device__ __forceinline__ const Inst& get(int& lb, int& nb) const { return get_at(blockIdx.x, 0, lb, nb); }
+    // block b of the group's block ranges (a persistent launch walks b = blockIdx.x, + gridDim.x, ...)
+    __device__ __forceinline__ const Inst& get_at(int b, int, int& lb, int& nb) const {
         int lo = 0, hi = n;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -347,10 +354,10 @@ __global__ void __launch_bounds__(kGatherThreads) k_resid_gather(const __grid_co
 
 // ---------------------------------------------------------------------------------
 // FD Jacobian of the 2D elements (fe_sw2_load :85-142, perturb_sw2_head / perturb_sw2_vel).
-// One CTA = kJacElems elements x 9 perturbation columns (node b, variable u/v/h); warp w
-// evaluates column w for 32 elements, so the pressure-term branch is warp-uniform.
-// Element data are staged in shared memory once; the 9x9 element matrices are staged
-// in shared memory and written out as contiguous 81-double records (slot 9e + 3a + b).
+// 32 elements x 9 perturbation columns (node b, variable u/v/h) at a time: warp w evaluates
+// column w for the 32 elements (lane = element), so the pressure-term branch is warp-uniform.
+// Element data are staged in shared memory once; the 9x9 element matrices are staged in
+// shared memory and written out as contiguous 81-double records (slot 9e + 3a + b).
 constexpr int kJacElems = 32;
 constexpr int kJacThreads = kJacElems * 9;
 
@@ -364,159 +371,195 @@ struct StagedElem {
 static_assert(sizeof(StagedElem) % 8 == 0 && (sizeof(StagedElem) / 8) % 2 == 1, "odd record stride");
 static_assert(sizeof(WetPre) % 8 == 0 && (sizeof(WetPre) / 8) % 2 == 1, "odd record stride");
 
-// GENERAL = false: every element, fully wet physics inlined (register-lean), elements not
-// eligible for it are skipped (their records are rewritten by the general launch, which runs
-// after it on the same stream).  GENERAL = true: the elements of `list`, full wet/dry physics.
+__device__ __forceinline__ void stage_elem(const DevMesh& m, const State& s, int e, StagedElem& S) {
+    load_elem(m, s, e, 0, S.in, S.n, S.df);
+    S.wd = s.wd[e];
+    S.mat = m.emat[e];
+}
+
+// One column (item = 3 b + var) of one element's 9x9 matrix into o[81]: R(x + eps e_j) and
+// R(x - eps e_j), the central difference, and the Dirichlet zeroing of the element matrix.
+// GENERAL = false: fully wet physics, with the parts the column leaves unperturbed read from
+// `pre`; GENERAL = true: full wet/dry physics.
 template <bool GENERAL>
-__device__ __forceinline__ void jac_elem_body(const DevMesh& m, const State& s, const PhysParams& P,
-                                              double* __restrict__ jslots, const unsigned char* __restrict__ ewet,
-                                              const int* __restrict__ list, int count, int lb) {
-    __shared__ StagedElem se[kJacElems];
-    __shared__ WetPre pre[GENERAL ? 1 : kJacElems];
-    __shared__ double out[kJacElems * 81];
-    __shared__ int eid[kJacElems];
-    const int e0 = lb * kJacElems;
-    const int lane = threadIdx.x % kJacElems;
-    const int item = threadIdx.x / kJacElems;
-    const int nel = min(kJacElems, count - e0);
-    if (item == 0) {
-        int e = -1;
-        if (lane < nel) {
-            e = GENERAL ? list[e0 + lane] : e0 + lane;
-            if (!GENERAL && !ewet[e]) e = -1;
-        }
-        eid[lane] = e;
-        if (e >= 0) {
-            StagedElem& S = se[lane];
-            load_elem(m, s, e, 0, S.in, S.n, S.df);
-            S.wd = s.wd[e];
-            S.mat = m.emat[e];
-        }
+__device__ __forceinline__ void jac_column(const DevMesh& m, const PhysParams& P, const StagedElem& S,
+                                           const WetPre* pre, int item, double* o) {
+    const int b = item / 3, var = item % 3;  // var: 0 = u, 1 = v, 2 = h
+    // only the current iterate (9 values) is private; everything else is read from the
+    // staged element in shared memory
+    double hc[3], uc[3], vc[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        hc[i] = S.in.h[i];
+        uc[i] = S.in.u[i];
+        vc[i] = S.in.v[i];
     }
-    __syncthreads();
-    if (!GENERAL) {
-        // the parts of the wet residual that depend on the old levels, the depth or the
-        // velocity alone, at the unperturbed iterate, once per element (warps 0, 1, 2)
-        if (item < 3 && eid[lane] >= 0) {
-            const StagedElem& S = se[lane];
-            if (item == 0) wet_levels(S.in, P, pre[lane].L);
-            else if (item == 1) wet_depth(S.in, S.in.h, P, m.mats[S.mat], pre[lane].D);
-            else wet_pre_velocity(S.in, pre[lane]);
-        }
-        __syncthreads();
+    const MatParams M = m.mats[S.mat];
+    // perturbed value, selected without runtime array indexing (keeps the arrays in registers)
+    double cur = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        if (i == b) cur = (var == 0) ? uc[i] : (var == 1) ? vc[i] : hc[i];
     }
-    if (eid[lane] >= 0) {
-        const StagedElem& S = se[lane];
-        const int b = item / 3, var = item % 3;  // var: 0 = u, 1 = v, 2 = h
-        // only the current iterate (9 values) is private; everything else is read from the
-        // staged element in shared memory
-        double hc[3], uc[3], vc[3];
+    const double eps = fd_eps(cur);
+    const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
+    // what this column leaves unperturbed
+    const unsigned fix = (var == 0)   ? (kFixH | kFixV | ((7u & ~(1u << b)) << kFixNode))
+                         : (var == 1) ? (kFixH | kFixU | ((7u & ~(1u << b)) << kFixNode))
+                                      : (kFixU | kFixV | (7u << kFixNode));
+    // Dirichlet zeroing of the element matrix (fe_assign_mom_db_dof3 / fe_assign_dacont_db_dof3):
+    // D = momentum-Dirichlet nodes (old-dry or VEL/VEL_PRS string), P = continuity-Dirichlet.
+    unsigned Dm = 0, Pm = 0;
 #pragma unroll
-        for (int i = 0; i < 3; i++) {
-            hc[i] = S.in.h[i];
-            uc[i] = S.in.u[i];
-            vc[i] = S.in.v[i];
-        }
-        const MatParams M = m.mats[S.mat];
-        // perturbed value, selected without runtime array indexing (keeps the arrays in registers)
-        double cur = 0.0;
-#pragma unroll
-        for (int i = 0; i < 3; i++) {
-            if (i == b) cur = (var == 0) ? uc[i] : (var == 1) ? vc[i] : hc[i];
-        }
-        const double eps = fd_eps(cur);
-        const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
-        // what this column leaves unperturbed (GENERAL = false reads those parts from `pre`)
-        const unsigned fix = (var == 0)   ? (kFixH | kFixV | ((7u & ~(1u << b)) << kFixNode))
-                             : (var == 1) ? (kFixH | kFixU | ((7u & ~(1u << b)) << kFixNode))
-                                          : (kFixU | kFixV | (7u << kFixNode));
-        // Dirichlet zeroing of the element matrix (fe_assign_mom_db_dof3 / fe_assign_dacont_db_dof3):
-        // D = momentum-Dirichlet nodes (old-dry or VEL/VEL_PRS string), P = continuity-Dirichlet.
-        unsigned Dm = 0, Pm = 0;
-#pragma unroll
-        for (int i = 0; i < 3; i++) {
-            const int f = m.qflag[i];
-            if (S.in.ho[i] <= 0.) Dm |= 1u << i;
-            if (f & 1) Pm |= 1u << i;
-            if (f & 2) Dm |= 1u << i;
-            if (f & 4) { Dm |= 1u << i; Pm |= 1u << i; }
-        }
-        double* o = out + lane * 81;
-        const double e2 = 2.0 * eps;
-        // pass 0 stores R(x + eps e_j) in this thread's 9 output entries, pass 1 turns them
-        // into the central difference; one residual body is instantiated, not two
+    for (int i = 0; i < 3; i++) {
+        const int f = m.qflag[i];
+        if (S.in.ho[i] <= 0.) Dm |= 1u << i;
+        if (f & 1) Pm |= 1u << i;
+        if (f & 2) Dm |= 1u << i;
+        if (f & 4) { Dm |= 1u << i; Pm |= 1u << i; }
+    }
+    const double e2 = 2.0 * eps;
+    // pass 0 stores R(x + eps e_j) in this thread's 9 output entries, pass 1 turns them
+    // into the central difference; one residual body is instantiated, not two
 #pragma unroll 1
-        for (int pass = 0; pass < 2; pass++) {
-            const double xv = pass == 0 ? cur + eps : cur - eps;
+    for (int pass = 0; pass < 2; pass++) {
+        const double xv = pass == 0 ? cur + eps : cur - eps;
 #pragma unroll
-            for (int i = 0; i < 3; i++) {
-                if (i == b) {
-                    if (var == 0) uc[i] = xv;
-                    else if (var == 1) vc[i] = xv;
-                    else hc[i] = xv;
-                }
-            }
-            double r[3][3];
-            if (GENERAL) sw2_elem_resid(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, r);
-            else elem_resid_impl<true, true>(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, r, &pre[lane], fix);
-#pragma unroll
-            for (int a = 0; a < 3; a++) {
-#pragma unroll
-                for (int eq = 0; eq < 3; eq++) {
-                    const int row = (eq == 0) ? 2 : eq - 1;  // block rows: x-mom, y-mom, continuity
-                    double& slot = o[(3 * a + b) * 9 + 3 * row + var];
-                    if (pass == 0) {
-                        slot = r[a][eq];
-                        continue;
-                    }
-                    double val = (slot - r[a][eq]) / e2;
-                    const bool aD = (Dm >> a) & 1u, bD = (Dm >> b) & 1u, aP = (Pm >> a) & 1u, bP = (Pm >> b) & 1u;
-                    const bool zero = (aD && row < 2) || (bD && var < 2) || (aP && row == 2) || (bP && var == 2);
-                    const bool one = (a == b) && ((aD && ((var == 0 && row == 0) || (var == 1 && row == 1))) ||
-                                                  (aP && var == 2 && row == 2));
-                    if (one) val = 1.0;
-                    else if (zero) val = 0.0;
-                    slot = val;
-                }
+        for (int i = 0; i < 3; i++) {
+            if (i == b) {
+                if (var == 0) uc[i] = xv;
+                else if (var == 1) vc[i] = xv;
+                else hc[i] = xv;
             }
         }
-    }
-    __syncthreads();
-    if (!GENERAL) {
-        double* dst = jslots + (size_t)e0 * 81;
-        for (int k = threadIdx.x; k < nel * 81; k += blockDim.x)
-            if (eid[k / 81] >= 0) dst[k] = out[k];
-    } else {
-        for (int k = threadIdx.x; k < nel * 81; k += blockDim.x)
-            jslots[(size_t)eid[k / 81] * 81 + k % 81] = out[k];
+        double r[3][3];
+        if (GENERAL) sw2_elem_resid(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, r);
+        else elem_resid_impl<true, true>(S.in, hc, uc, vc, S.wd, pv, P, M, S.df, r, pre, fix);
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+#pragma unroll
+            for (int eq = 0; eq < 3; eq++) {
+                const int row = (eq == 0) ? 2 : eq - 1;  // block rows: x-mom, y-mom, continuity
+                double& slot = o[(3 * a + b) * 9 + 3 * row + var];
+                if (pass == 0) {
+                    slot = r[a][eq];
+                    continue;
+                }
+                double val = (slot - r[a][eq]) / e2;
+                const bool aD = (Dm >> a) & 1u, bD = (Dm >> b) & 1u, aP = (Pm >> a) & 1u, bP = (Pm >> b) & 1u;
+                const bool zero = (aD && row < 2) || (bD && var < 2) || (aP && row == 2) || (bP && var == 2);
+                const bool one = (a == b) && ((aD && ((var == 0 && row == 0) || (var == 1 && row == 1))) ||
+                                              (aP && var == 2 && row == 2));
+                if (one) val = 1.0;
+                else if (zero) val = 0.0;
+                slot = val;
+            }
+        }
     }
 }
 
-// FD Jacobian of the 2D elements (fe_sw2_load :85-142, perturb_sw2_head / perturb_sw2_vel).
-// One CTA = kJacElems elements x 9 perturbation columns (node b, variable u/v/h); warp w
-// evaluates column w for 32 elements, so the pressure-term branch is warp-uniform.
-// Element data are staged in shared memory once; the 9x9 element matrices are staged
-// in shared memory and written out as contiguous 81-double records (slot 9e + 3a + b).
-// MINB: resident CTAs per SM the register budget is cut for (1: 168 registers, 2: 96 with more
+// named barriers of the wet-Jacobian CTA (0 is __syncthreads')
+__device__ __forceinline__ void bar_sync(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(int id, int count) {
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Fully wet elements: a persistent CTA of 9 column warps and one staging warp walks the
+// launch's 32-element groups (virtual blocks v = blockIdx.x, + gridDim.x, ...).  The staging
+// warp loads group i into buffer i & 1 and forms its shared parts (WetPre) while the column
+// warps evaluate group i - 1, so no column warp waits on element loads; buffers are handed
+// over with named barriers (FULL: staged, EMPTY: read).  Elements not eligible for the wet
+// physics are skipped; the general launch, which runs after this one on the same stream,
+// writes their records.
+constexpr int kJacWetThreads = kJacThreads + 32;
+enum : int { kBarFull = 1, kBarEmpty = 3, kBarCols = 5 };
+struct JacWetSmem {
+    StagedElem se[2][kJacElems];
+    WetPre pre[2][kJacElems];
+    double out[kJacElems * 81];
+    int eid[2][kJacElems];
+};
+constexpr size_t kJacWetSmem = sizeof(JacWetSmem);
+
+// MINB: resident CTAs per SM the register budget is cut for (1: 168 registers, 2: 96 with
 // spills); the autotuner picks per mesh, the arithmetic is the same
 template <class Src, int MINB>
-__global__ void __launch_bounds__(kJacThreads, MINB) k_jac_elem_wet(const __grid_constant__ Src src) {
-    int lb, nb;
-    const Inst& I = src.get(lb, nb);
-    const DevMesh m = I.m;
-    const State s = I.s;
-    const PhysParams P = I.P;
-    jac_elem_body<false>(m, s, P, I.jslots, I.ewet, nullptr, m.T, lb);
+__global__ void __launch_bounds__(kJacWetThreads, MINB) k_jac_elem_wet(const __grid_constant__ Src src, int nvirt) {
+    extern __shared__ __align__(16) unsigned char jac_smem[];
+    JacWetSmem& sm = *reinterpret_cast<JacWetSmem*>(jac_smem);
+    const int lane = threadIdx.x % kJacElems;
+    const int item = threadIdx.x / kJacElems;
+    const int stride = gridDim.x;
+    if (item == 9) {
+        for (int i = 0, v = blockIdx.x; v < nvirt; i++, v += stride) {
+            const int j = i & 1;
+            if (i >= 2) bar_sync(kBarEmpty + j, kJacWetThreads);
+            int lb, nb;
+            const Inst& I = src.get_at(v, nvirt, lb, nb);
+            const DevMesh m = I.m;
+            const int e0 = lb * kJacElems;
+            int e = -1;
+            if (e0 + lane < m.T && I.ewet[e0 + lane]) e = e0 + lane;
+            sm.eid[j][lane] = e;
+            if (e >= 0) {
+                StagedElem& S = sm.se[j][lane];
+                stage_elem(m, I.s, e, S);
+                WetPre& p = sm.pre[j][lane];
+                wet_levels(S.in, I.P, p.L);
+                wet_depth(S.in, S.in.h, I.P, m.mats[S.mat], p.D);
+                wet_pre_velocity(S.in, p);
+            }
+            __syncwarp();
+            bar_arrive(kBarFull + j, kJacWetThreads);
+        }
+        return;
+    }
+    for (int i = 0, v = blockIdx.x; v < nvirt; i++, v += stride) {
+        const int j = i & 1;
+        bar_sync(kBarFull + j, kJacWetThreads);
+        int lb, nb;
+        const Inst& I = src.get_at(v, nvirt, lb, nb);
+        const int e0 = lb * kJacElems;
+        const int nel = min(kJacElems, I.m.T - e0);
+        if (sm.eid[j][lane] >= 0) jac_column<false>(I.m, I.P, sm.se[j][lane], &sm.pre[j][lane], item, sm.out + lane * 81);
+        __syncwarp();
+        bar_sync(kBarCols, kJacThreads);
+        double* dst = I.jslots + (size_t)e0 * 81;
+        for (int k = threadIdx.x; k < nel * 81; k += kJacThreads)
+            if (sm.eid[j][k / 81] >= 0) dst[k] = sm.out[k];
+        __syncwarp();
+        bar_sync(kBarCols, kJacThreads);   // `out` and buffer j are free again
+        if (v + 2 * stride < nvirt) bar_arrive(kBarEmpty + j, kJacWetThreads);
+    }
 }
-// the list length is the one the last residual evaluation recorded
+
+// Elements of the general list (some vertex dry at some level, or a wet/dry-flagged
+// element), full wet/dry physics; the list length is the one the last residual evaluation
+// recorded.  One CTA per 32 listed elements.
 template <class Src>
 __global__ void __launch_bounds__(kJacThreads) k_jac_elem_general(const __grid_constant__ Src src) {
     int lb, nb;
     const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
-    const State s = I.s;
-    const PhysParams P = I.P;
-    jac_elem_body<true>(m, s, P, I.jslots, nullptr, I.glist, *I.ngen, lb);
+    __shared__ StagedElem se[kJacElems];
+    __shared__ double out[kJacElems * 81];
+    __shared__ int eid[kJacElems];
+    const int count = *I.ngen;
+    const int e0 = lb * kJacElems;
+    const int lane = threadIdx.x % kJacElems;
+    const int item = threadIdx.x / kJacElems;
+    const int nel = min(kJacElems, count - e0);
+    if (item == 0) {
+        const int e = lane < nel ? I.glist[e0 + lane] : -1;
+        eid[lane] = e;
+        if (e >= 0) stage_elem(m, I.s, e, se[lane]);
+    }
+    __syncthreads();
+    if (eid[lane] >= 0) jac_column<true>(m, I.P, se[lane], nullptr, item, out + lane * 81);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nel * 81; k += blockDim.x) I.jslots[(size_t)eid[k / 81] * 81 + k % 81] = out[k];
 }
 
 // FD Jacobian of the boundary edges: one thread per (edge, node, variable); writes the

@@ -237,6 +237,7 @@ struct Runner {
     KrylovCtl* ctl_h = nullptr;
     int stages = 0;               // Krylov tile-ring depth in use (0: sweeps from global memory)
     int jac_minb = 2;             // wet-Jacobian variant in use
+    int jac_ctas[2] = {0, 0};     // persistent wet-Jacobian grid per variant (co-resident CTAs)
     unsigned c_off = 0, r_off = 0, v_off = 0, stage_bytes = 0;
     size_t smem = 0;
     int capacity = 0;             // co-resident Krylov CTAs
@@ -438,6 +439,22 @@ int runner_set(Runner& R, const std::vector<sw2gpu_ctx*>& ctx) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tab, ktab, kKrylovThreads, R.smem));
     per_sm = std::min(per_sm, per_sm_tab);
     R.capacity = sms * std::max(1, std::min(per_sm, 4));
+    if (!R.jac_ctas[0]) {
+        // wet-Jacobian kernels: double-buffered records above the 48 KB static limit, and a
+        // persistent grid of the CTAs that fit at once
+        const void* wet[2][2] = {{(const void*)k_jac_elem_wet<SrcOne, 1>, (const void*)k_jac_elem_wet<SrcPar, 1>},
+                                 {(const void*)k_jac_elem_wet<SrcOne, 2>, (const void*)k_jac_elem_wet<SrcPar, 2>}};
+        for (int v = 0; v < 2; v++) {
+            int fit = 1 << 30;
+            for (int k = 0; k < 2; k++) {
+                int n = 0;
+                CK(cudaFuncSetAttribute(wet[v][k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacWetSmem));
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wet[v][k], kJacWetThreads, kJacWetSmem));
+                fit = std::min(fit, n);
+            }
+            R.jac_ctas[v] = sms * std::max(1, fit);
+        }
+    }
     return 0;
 }
 
@@ -592,9 +609,14 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
     auto C = [&](int k) { return R.ctx[k]; };
     // the general list and the wet flags come from the residual evaluated at this same state
     auto wet_blocks = [&](int k) { return nblk(C(k)->T, kJacElems); };
-    int rc = R.jac_minb == 1
-                 ? launch_map(R, sub, kJacThreads, wet_blocks, SW2_GO_T(k_jac_elem_wet, 1))
-                 : launch_map(R, sub, kJacThreads, wet_blocks, SW2_GO_T(k_jac_elem_wet, 2));
+    auto wet = [&](auto minb) {   // persistent: the grid walks the launch's nb_ element groups
+        constexpr int MB = decltype(minb)::value;
+        return launch_map(R, sub, kJacWetThreads, wet_blocks, [&](const auto& src, int nb_, int th_) {
+            k_jac_elem_wet<std::decay_t<decltype(src)>, MB>
+                <<<std::min(nb_, R.jac_ctas[MB - 1]), th_, kJacWetSmem, R.stream>>>(src, nb_);
+        });
+    };
+    int rc = R.jac_minb == 1 ? wet(std::integral_constant<int, 1>{}) : wet(std::integral_constant<int, 2>{});
     if (rc) return rc;
     // a captured launch covers the largest list (the kernel reads the list's length itself)
     if ((rc = launch_map(R, sub, kJacThreads,
