@@ -458,14 +458,6 @@ __device__ __forceinline__ void jac_column(const DevMesh& m, const PhysParams& P
     }
 }
 
-// named barriers of the wet-Jacobian CTA (0 is __syncthreads')
-__device__ __forceinline__ void bar_sync(int id, int count) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
-}
-__device__ __forceinline__ void bar_arrive(int id, int count) {
-    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
-}
-
 // Fully wet elements: a persistent CTA of 9 column warps and one staging warp walks the
 // launch's 32-element groups (virtual blocks v = blockIdx.x, + gridDim.x, ...).  The staging
 // warp loads group i into buffer i & 1 and forms its shared parts (WetPre) while the column
@@ -474,7 +466,8 @@ __device__ __forceinline__ void bar_arrive(int id, int count) {
 // physics are skipped; the general launch, which runs after this one on the same stream,
 // writes their records.
 constexpr int kJacWetThreads = kJacThreads + 32;
-enum : int { kBarFull = 1, kBarEmpty = 3, kBarCols = 5 };
+// named barriers of the wet-Jacobian CTA (0 is __syncthreads')
+constexpr int kJacBarFull = 1, kJacBarEmpty = 3, kJacBarCols = 5;
 struct JacWetSmem {
     StagedElem se[2][kJacElems];
     WetPre pre[2][kJacElems];
@@ -495,7 +488,7 @@ __global__ void __launch_bounds__(kJacWetThreads, MINB) k_jac_elem_wet(const __g
     if (item == 9) {
         for (int i = 0, v = blockIdx.x; v < nvirt; i++, v += stride) {
             const int j = i & 1;
-            if (i >= 2) bar_sync(kBarEmpty + j, kJacWetThreads);
+            if (i >= 2) bar_sync_n(kJacBarEmpty + j, kJacWetThreads);
             int lb, nb;
             const Inst& I = src.get_at(v, nvirt, lb, nb);
             const DevMesh m = I.m;
@@ -512,26 +505,26 @@ __global__ void __launch_bounds__(kJacWetThreads, MINB) k_jac_elem_wet(const __g
                 wet_pre_velocity(S.in, p);
             }
             __syncwarp();
-            bar_arrive(kBarFull + j, kJacWetThreads);
+            bar_arrive_n(kJacBarFull + j, kJacWetThreads);
         }
         return;
     }
     for (int i = 0, v = blockIdx.x; v < nvirt; i++, v += stride) {
         const int j = i & 1;
-        bar_sync(kBarFull + j, kJacWetThreads);
+        bar_sync_n(kJacBarFull + j, kJacWetThreads);
         int lb, nb;
         const Inst& I = src.get_at(v, nvirt, lb, nb);
         const int e0 = lb * kJacElems;
         const int nel = min(kJacElems, I.m.T - e0);
         if (sm.eid[j][lane] >= 0) jac_column<false>(I.m, I.P, sm.se[j][lane], &sm.pre[j][lane], item, sm.out + lane * 81);
         __syncwarp();
-        bar_sync(kBarCols, kJacThreads);
+        bar_sync_n(kJacBarCols, kJacThreads);
         double* dst = I.jslots + (size_t)e0 * 81;
         for (int k = threadIdx.x; k < nel * 81; k += kJacThreads)
             if (sm.eid[j][k / 81] >= 0) dst[k] = sm.out[k];
         __syncwarp();
-        bar_sync(kBarCols, kJacThreads);   // `out` and buffer j are free again
-        if (v + 2 * stride < nvirt) bar_arrive(kBarEmpty + j, kJacWetThreads);
+        bar_sync_n(kJacBarCols, kJacThreads);   // `out` and buffer j are free again
+        if (v + 2 * stride < nvirt) bar_arrive_n(kJacBarEmpty + j, kJacWetThreads);
     }
 }
 

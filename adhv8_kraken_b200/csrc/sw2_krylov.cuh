@@ -23,12 +23,14 @@
 
 namespace sw2 {
 
-constexpr int kKrylovThreads = 256;
+// 8 row warps (SpMV rows, vector passes, partials) and one copy warp that fills the tile ring
+constexpr int kKrylovRowThreads = 256;
+constexpr int kKrylovThreads = kKrylovRowThreads + 32;
 constexpr long long kBarrierSpinLimit = 1ll << 28;   // bounded wait (~seconds of polls), then error
 constexpr long long kMbarSpinLimit = 1ll << 20;      // polls of one tile copy's mbarrier, then error
 constexpr int kStall = 40;                           // iterations without a new best residual
 constexpr int kRowLanes = 8;                         // lanes per node row in the SpMV sweeps
-constexpr int kTileRows = kKrylovThreads / kRowLanes;   // node rows per CTA tile (32)
+constexpr int kTileRows = kKrylovRowThreads / kRowLanes;   // node rows per CTA tile (32)
 constexpr int kMaxStages = 3;                        // deepest shared-memory tile ring of the staged sweeps
 constexpr int kVirtualPerSM = 3;                     // virtual CTAs per SM of a large instance (fixed:
                                                      // it sets the reduction order, so no tuning knob may)
@@ -98,7 +100,16 @@ __device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks) {
     return *(volatile int*)&ctl->err == 0;
 }
 
-constexpr int kKrylovWarps = kKrylovThreads / 32;
+constexpr int kKrylovWarps = kKrylovRowThreads / 32;   // warps that hold partials
+// named barriers of the Krylov CTA (0 is __syncthreads'): the row warps alone, and per ring
+// stage "read by every row warp" (row warps arrive, the copy warp waits)
+constexpr int kBarRows = 1, kBarEmpty = 2;
+__device__ __forceinline__ void bar_sync_n(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bar_arrive_n(int id, int count) {
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
 
 // fixed-order warp tree (xor shuffles): every lane ends with the same value
 __device__ __forceinline__ double warp_combine(double a, bool is_max) {
@@ -111,20 +122,24 @@ __device__ __forceinline__ double warp_combine(double a, bool is_max) {
 }
 
 // deterministic all-reduce of up to 4 per-block partials: every block combines the partials
-// of all blocks in the same fixed order (sum or max per slot); red = shared [4][kKrylovWarps]
+// of all blocks in the same fixed order (sum or max per slot); red = shared [4][kKrylovWarps].
+// The row warps read the partials; every thread of the CTA (the copy warp too, which needs
+// the loop decisions) ends with the result.  Called by the whole CTA.
 template <int NV>
 __device__ __forceinline__ void grid_allreduce(const double* part, int nparts, const int* is_max, double* out,
                                                double* red) {
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (threadIdx.x < kKrylovRowThreads) {
 #pragma unroll
-    for (int q = 0; q < NV; q++) {
-        double a = 0.0;
-        for (int k = threadIdx.x; k < nparts; k += blockDim.x) {
-            const double p = __ldcg(part + (size_t)k * 4 + q);
-            a = is_max[q] ? fmax(a, p) : a + p;
+        for (int q = 0; q < NV; q++) {
+            double a = 0.0;
+            for (int k = threadIdx.x; k < nparts; k += kKrylovRowThreads) {
+                const double p = __ldcg(part + (size_t)k * 4 + q);
+                a = is_max[q] ? fmax(a, p) : a + p;
+            }
+            a = warp_combine(a, is_max[q]);
+            if (lane == 0) red[q * kKrylovWarps + warp] = a;
         }
-        a = warp_combine(a, is_max[q]);
-        if (lane == 0) red[q * kKrylovWarps + warp] = a;
     }
     __syncthreads();
 #pragma unroll
@@ -137,7 +152,8 @@ __device__ __forceinline__ void grid_allreduce(const double* part, int nparts, c
     __syncthreads();
 }
 
-// block partials: thread values combined in a fixed order, written by thread 0 to slot `slot`
+// block partials: the row threads' values combined in a fixed order, written by thread 0 to
+// slot `slot`.  Called by the row warps only (the copy warp may be ahead in the tile sequence).
 template <int NV>
 __device__ __forceinline__ void block_partial(double* vals, const int* is_max, double* part, int slot, double* red) {
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -146,7 +162,7 @@ __device__ __forceinline__ void block_partial(double* vals, const int* is_max, d
         const double a = warp_combine(vals[q], is_max[q]);
         if (lane == 0) red[q * kKrylovWarps + warp] = a;
     }
-    __syncthreads();
+    bar_sync_n(kBarRows, kKrylovRowThreads);
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int q = 0; q < NV; q++) {
@@ -157,7 +173,7 @@ __device__ __forceinline__ void block_partial(double* vals, const int* is_max, d
             part[(size_t)slot * 4 + q] = a;
         }
     }
-    __syncthreads();
+    bar_sync_n(kBarRows, kKrylovRowThreads);
 }
 
 template <typename T>
@@ -431,8 +447,9 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     VT* __restrict__ ubest = KI.vec[7];
     const int V = K.V;
     const int VG = K.vgrid;
-    const int pstride = np * blockDim.x;                  // reduction-free loops: physical CTAs
-    const int pt0 = pl * blockDim.x + threadIdx.x;
+    const bool rows = threadIdx.x < kKrylovRowThreads;   // row warp (else: the copy warp)
+    const int pstride = np * kKrylovRowThreads;           // reduction-free loops: physical CTAs
+    const int pt0 = pl * kKrylovRowThreads + threadIdx.x;
     const int lane8 = threadIdx.x % kRowLanes;
     const int li = threadIdx.x / kRowLanes;   // row of the tile this lane group works on
     const int ntiles = (V + kTileRows - 1) / kTileRows;   // >= VG: every virtual CTA has a tile
@@ -449,8 +466,8 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         if (threadIdx.x == 0) {
             for (int s = 0; s < NST; s++) mbar_init(&bar[s], 1);
             mbar_init_fence();
-            pol = policy_evict_first();
         }
+        if (threadIdx.x == kKrylovRowThreads) pol = policy_evict_first();
         __syncthreads();
     }
 
@@ -458,35 +475,42 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     // m = v, v + VG, ... < ntiles.  y = sum_j B_ij (xa_j - alpha xb_j) over the off-diagonal
     // blocks of each row; lane 0 of each row group calls epi(i, y, ev) with ev[v][c] =
     // component c of epilogue vector v at row i (NV vectors: v0, v1, v2), from which the
-    // epilogue forms the diagonal term; fin(v) closes virtual CTA v (its partial).  The
-    // producer cursor (pv, pm) runs NST - 1 items ahead along the same sequence.
+    // epilogue forms the diagonal term; fin(v) closes virtual CTA v (its partial).
+    // STAGED: the copy warp walks the same tile sequence up to NST tiles ahead, filling ring
+    // stage (item % NST) once every row warp has released it (named barrier kBarEmpty + stage);
+    // the row warps wait on the stage's mbarrier, so each warp proceeds at its own pace.
+    // Called by the whole CTA.
     auto sweep = [&](auto nvc, const VT* xa, const VT* xb, VT alpha, const VT* v0, const VT* v1, const VT* v2,
                      auto&& epi, auto&& fin) {
         constexpr int NV = decltype(nvc)::value;
         const VT* vecs[3] = {v0, v1, v2};
-        int pv = pl, pm = pl;
-        auto produce = [&](unsigned item) {
-            if (pv >= VG) return;
-            issue_tile<MT, VT>(pm, V, K.rowptr, K.col, A, NV, vecs, stage(item), L, &bar[item % NST], pol);
-            pm += VG;
-            if (pm >= ntiles) {
-                pv += np;
-                pm = pv;
+        int nitems = 0;   // tiles of this CTA in this sweep
+        for (int v = pl; v < VG; v += np) nitems += (ntiles - v + VG - 1) / VG;
+        if (!rows) {
+            if (STAGED) {
+                const bool issuer = threadIdx.x == kKrylovRowThreads;
+                if (issuer) fence_proxy_async_global();
+                int j = 0;
+                for (int v = pl; v < VG; v += np)
+                    for (int m = v; m < ntiles; m += VG, j++) {
+                        const unsigned item = tc + j;
+                        if (j >= NST) bar_sync_n(kBarEmpty + (int)(item % NST), kKrylovThreads);
+                        if (issuer)
+                            issue_tile<MT, VT>(m, V, K.rowptr, K.col, A, NV, vecs, stage(item), L, &bar[item % NST], pol);
+                        __syncwarp();
+                    }
             }
-        };
-        if (STAGED && threadIdx.x == 0) {
-            fence_proxy_async_global();
-            for (int d = 0; d < NST - 1; d++) produce(tc + d);
+            tc += nitems;
+            return;
         }
+        int j = 0;
         for (int v = pl; v < VG; v += np) {
-            for (int m = v; m < ntiles; m += VG) {
+            for (int m = v; m < ntiles; m += VG, j++) {
                 const int i = m * kTileRows + li;
                 const bool act = i < V;
                 VT y[3];
                 VT ev[NV][3];
                 if (STAGED) {
-                    // into the stage of item tc - 1, released by the __syncthreads that ended it
-                    if (threadIdx.x == 0) produce(tc + NST - 1);
                     // a wait that runs out flags the error once; this thread then stops waiting,
                     // the sweep finishes on stale data and the next barrier returns
                     if (!wait_failed && !mbar_wait(&bar[tc % NST], (tc / NST) & 1u)) {
@@ -524,7 +548,9 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                 }
                 if (act && lane8 == 0) epi(i, y, ev);
                 if (STAGED) {
-                    __syncthreads();
+                    // this warp is done with the stage; the copy warp refills it for item + NST
+                    __syncwarp();
+                    if (j + NST < nitems) bar_arrive_n(kBarEmpty + (int)(tc % NST), kKrylovThreads);
                     tc++;
                 }
             }
@@ -533,7 +559,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     };
 
     // b <- M^-1 b'
-    for (int i = pt0; i < V; i += pstride) {
+    for (int i = pt0; rows && i < V; i += pstride) {
         const double* d = Dinv + (size_t)i * 9;
         const double b0 = K.bs[3 * i], b1 = K.bs[3 * i + 1], b2 = K.bs[3 * i + 2];
 #pragma unroll
@@ -693,11 +719,11 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                     reinterpret_cast<V2*>(r)[k2] = rn;
                     reinterpret_cast<V2*>(p)[k2] = pn;
                 };
-                for (int v = pl; v < VG; v += np) {
+                for (int v = pl; rows && v < VG; v += np) {
                     // element pairs (16-byte accesses), virtual CTA v's share; each element is
                     // updated on its own, the pairing only widens the loads
                     const int n2 = (3 * V) / 2;
-                    for (int k2 = v * blockDim.x + threadIdx.x; k2 < n2; k2 += VG * blockDim.x) upd2(k2);
+                    for (int k2 = v * kKrylovRowThreads + threadIdx.x; k2 < n2; k2 += VG * kKrylovRowThreads) upd2(k2);
                     if ((3 * V) % 2 && v == 0 && threadIdx.x == 0) upd(3 * V - 1);
                     block_partial<1>(mx, mm, pbuf(), v, red);
                     mx[0] = 0.0;
@@ -717,7 +743,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         // x = S u; state += x; sol = -x.  Without convergence the best iterate is u itself when
         // the last iteration set it (not saved yet), else ubest.
         const VT* ux = (conv || pending) ? uu : ubest;
-        for (int i = pt0; i < V; i += pstride) {
+        for (int i = pt0; rows && i < V; i += pstride) {
             const double x0 = (double)ldv(ux + 3 * i) * K.S[3 * i];
             const double x1 = (double)ldv(ux + 3 * i + 1) * K.S[3 * i + 1];
             const double x2 = (double)ldv(ux + 3 * i + 2) * K.S[3 * i + 2];
