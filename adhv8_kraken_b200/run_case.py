@@ -1,6 +1,7 @@
 """Runs the seeded basin workload for a few time steps and prints per-step statistics.
 
     python -m adhv8_kraken_b200.run_case --points 500000 --steps 2 [--precision fp64|mixed]
+                                         [--variant JAC_MINB,STAGES]
 
 One JSON line per step (Newton and Krylov iterations, device time per phase).  This is the
 command the kernel profiles are taken on: it runs the same code path as ``bench.py`` without
@@ -19,6 +20,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--variant", default=None,
+                    help="launch variant 'jac_minb,stages' (e.g. 1,3); default: the library's own")
     a = ap.parse_args(argv)
     from . import capi, meshgen
     from .sw2 import SW2GPU
@@ -27,6 +30,8 @@ def main(argv=None):
     model = meshgen.bumpy_basin(a.points, seed=a.seed, size=size, nsteps=a.steps, dt=5.0, name="basin")
     prec = capi.SW2GPU_FP64 if a.precision == "fp64" else capi.SW2GPU_MIXED
     g = SW2GPU(model, precision=prec)
+    if a.variant:
+        g.set_variant(*(int(x) for x in a.variant.split(",")))
     print(json.dumps({"triangles": model.nelems2d, "nodes": model.nnodes, "nnzb": g.nnzb}))
     for _ in range(a.steps):
         st = g.step()
