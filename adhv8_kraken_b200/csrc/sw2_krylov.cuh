@@ -225,6 +225,10 @@ struct KrylovArgs {
     double* part;             // [2][vgrid][4] partials (ping-pong: a slot is rewritten only two reductions later)
     KrylovCtl* ctl;
     int vgrid;                // virtual CTAs: the partial structure, fixed per instance
+    int fuse_update;          // 1: an iteration's update is applied by the next iteration's first
+                              // sweep (one grid barrier and one vector pass fewer per iteration,
+                              // more vectors live: for launches whose vectors stay in L2); a batch
+                              // launch decides for all its instances (KrylovTab::fuse)
 };
 
 // one instance of a Krylov launch
@@ -232,8 +236,14 @@ struct KrylovInst {
     KrylovArgs K;
     const void* A;            // folded off-diagonal blocks, MT
     const double* Dinv;       // FP64 block-Jacobi inverses (b = M^-1 b' only)
-    double* vec[8];           // b, u, r, q, p, Ap, As, best u
+    double* vec[12];          // b, u, r, q, p, Ap, As, best u, and the second copies of u, r, p, Ap
 };
+constexpr int kKrylovVectors = 12;
+// The fused update keeps all 12 vectors live within one sweep and gathers four of them; it pays
+// while the vectors of every instance of a launch stay in L2 together (126 MB on B200), i.e.
+// up to ~170k nodes in total.
+constexpr long long kFuseUpdateMaxBytes = 48ll << 20;
+inline int krylov_fuse_update(long long nodes) { return kKrylovVectors * 24ll * nodes <= kFuseUpdateMaxBytes ? 1 : 0; }
 
 // Stage layout of the staged sweeps: byte offsets inside one stage of the tile's column
 // indices, row pointers and epilogue vectors (the blocks start at 0), and the stage stride.
@@ -256,12 +266,14 @@ struct KrylovOne {
         rt = rtol_dev ? __ldcg(rtol_dev) : rtol;
         return Q;
     }
+    __device__ __forceinline__ bool fuse_update(const KrylovInst& KI) const { return KI.K.fuse_update != 0; }
 };
 struct KrylovTab {
     const KrylovInst* tab;
     LaunchMap mp;
     double rtol[kMaxBatch];
     StageLayout lay;
+    int fuse;                 // fused update for every instance of the launch (their vectors together)
     __device__ __forceinline__ const KrylovInst& get(int& pl, int& np, double& rt) const {
         int nb;
         const int b = blockIdx.x;
@@ -277,11 +289,13 @@ struct KrylovTab {
         rt = rtol[lo];
         return tab[mp.ids[lo]];
     }
+    __device__ __forceinline__ bool fuse_update(const KrylovInst&) const { return fuse != 0; }
 };
 
 // bytes of one epilogue vector's slice for a full tile (3 components per row)
 template <typename VT>
 __host__ __device__ constexpr unsigned tile_vec_bytes() { return kTileRows * 3 * sizeof(VT); }
+constexpr int kMaxEpilogue = 6;   // epilogue vectors a sweep stages per tile
 
 // ---- tile staging: one bulk copy per tile, completion on an mbarrier -------------------------
 // Tile m = node rows [m kTileRows, (m+1) kTileRows); its blocks and column indices are contiguous.
@@ -371,17 +385,16 @@ struct IntC {
 };
 
 // Off-diagonal row sum y = sum_j B_ij x_j of the folded operator (B_ij = D_i^-1 A'_ij, blocks
-// kb..ke-1) for node row i, with x_j = xa_j - alpha * xb_j when xb != null; the caller adds the
-// identity diagonal block's x_i.  Eight lanes share a row and each lane takes whole 3x3 blocks
+// kb..ke-1) for node row i, with x_j formed by gat(j, x) from the vectors at node j; the caller
+// adds the identity diagonal block's x_i.  Eight lanes share a row and each lane takes whole 3x3 blocks
 // (lane l: the row's blocks l, l+8, ...); the column index and the three x components are loaded
 // once per block.  blk(k) / cix(k) give block k's values and column index (from the staged tile
 // in shared memory, or from global memory).  The three sums are combined with xor shuffles in a
 // fixed order, so staged and direct sweeps give bitwise identical results.  Products and sums
 // are formed in the matrix type MT (FP32 accumulation on the mixed path).  The result is valid
 // on lane 0 of the group; `active` false contributes zeros so the whole warp can shuffle.
-template <typename MT, typename VT, class BLK, class CIX>
-__device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke, BLK blk, CIX cix, const VT* xa,
-                                          const VT* xb, VT alpha, VT y[3]) {
+template <typename MT, typename VT, class BLK, class CIX, class GAT>
+__device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke, BLK blk, CIX cix, GAT gat, VT y[3]) {
     MT a0 = 0, a1 = 0, a2 = 0;
     if (active) {
         for (int k = kb + lane8; k < ke; k += kRowLanes) {
@@ -390,13 +403,9 @@ __device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke
 #pragma unroll
             for (int q = 0; q < 9; q++) m[q] = bk[q];
             const int j = cix(k);
-            VT x0 = ldv(xa + 3 * j), x1 = ldv(xa + 3 * j + 1), x2 = ldv(xa + 3 * j + 2);
-            if (xb) {
-                x0 = fmadd(-alpha, ldv(xb + 3 * j), x0);
-                x1 = fmadd(-alpha, ldv(xb + 3 * j + 1), x1);
-                x2 = fmadd(-alpha, ldv(xb + 3 * j + 2), x2);
-            }
-            const MT c0 = (MT)x0, c1 = (MT)x1, c2 = (MT)x2;
+            VT x[3];
+            gat(j, x);
+            const MT c0 = (MT)x[0], c1 = (MT)x[1], c2 = (MT)x[2];
             a0 = fmadd(m[2], c2, fmadd(m[1], c1, fmadd(m[0], c0, a0)));
             a1 = fmadd(m[5], c2, fmadd(m[4], c1, fmadd(m[3], c0, a1)));
             a2 = fmadd(m[8], c2, fmadd(m[7], c1, fmadd(m[6], c0, a2)));
@@ -438,13 +447,15 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     const MT* __restrict__ A = (const MT*)KI.A;
     const double* __restrict__ Dinv = KI.Dinv;
     VT* __restrict__ b = KI.vec[0];
-    VT* __restrict__ uu = KI.vec[1];
-    VT* __restrict__ r = KI.vec[2];
     VT* __restrict__ q = KI.vec[3];
-    VT* __restrict__ p = KI.vec[4];
-    VT* __restrict__ Ap = KI.vec[5];
     VT* __restrict__ As = KI.vec[6];
     VT* __restrict__ ubest = KI.vec[7];
+    // u, r, p, Ap in two copies: the sweep that applies an iteration's update reads the old
+    // copy (its gathers at neighbour rows too) and writes the new one
+    VT* const U2[2] = {KI.vec[1], KI.vec[8]};
+    VT* const R2[2] = {KI.vec[2], KI.vec[9]};
+    VT* const P2[2] = {KI.vec[4], KI.vec[10]};
+    VT* const AP2[2] = {KI.vec[5], KI.vec[11]};
     const int V = K.V;
     const int VG = K.vgrid;
     const bool rows = threadIdx.x < kKrylovRowThreads;   // row warp (else: the copy warp)
@@ -472,18 +483,17 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     }
 
     // One SpMV sweep: this CTA runs virtual CTAs v = pl, pl + np, ... < VG, each over tiles
-    // m = v, v + VG, ... < ntiles.  y = sum_j B_ij (xa_j - alpha xb_j) over the off-diagonal
-    // blocks of each row; lane 0 of each row group calls epi(i, y, ev) with ev[v][c] =
-    // component c of epilogue vector v at row i (NV vectors: v0, v1, v2), from which the
-    // epilogue forms the diagonal term; fin(v) closes virtual CTA v (its partial).
+    // m = v, v + VG, ... < ntiles.  y = sum_j B_ij x_j over the off-diagonal blocks of each row,
+    // x_j = gat(j) from the vectors at node j; lane 0 of each row group calls epi(i, y, ev) with
+    // ev(v, c) = component c of epilogue vector v at row i (NV vectors; read from the staged tile
+    // or from global memory), from which the epilogue forms the diagonal term; fin(v) closes
+    // virtual CTA v (its partial).
     // STAGED: the copy warp walks the same tile sequence up to NST tiles ahead, filling ring
     // stage (item % NST) once every row warp has released it (named barrier kBarEmpty + stage);
     // the row warps wait on the stage's mbarrier, so each warp proceeds at its own pace.
     // Called by the whole CTA.
-    auto sweep = [&](auto nvc, const VT* xa, const VT* xb, VT alpha, const VT* v0, const VT* v1, const VT* v2,
-                     auto&& epi, auto&& fin) {
+    auto sweep = [&](auto nvc, const VT* const* vecs, auto&& gat, auto&& epi, auto&& fin) {
         constexpr int NV = decltype(nvc)::value;
-        const VT* vecs[3] = {v0, v1, v2};
         int nitems = 0;   // tiles of this CTA in this sweep
         for (int v = pl; v < VG; v += np) nitems += (ntiles - v + VG - 1) / VG;
         if (!rows) {
@@ -509,7 +519,6 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                 const int i = m * kTileRows + li;
                 const bool act = i < V;
                 VT y[3];
-                VT ev[NV][3];
                 if (STAGED) {
                     // a wait that runs out flags the error once; this thread then stops waiting,
                     // the sweep finishes on stale data and the next barrier returns
@@ -526,27 +535,16 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                     const int kb = act ? sR[li] : 0, ke = act ? sR[li + 1] : 0;
                     row_apply<MT, VT>(
                         act, lane8, kb, ke, [&](int k) { return sA + (size_t)(k - k0) * 9; },
-                        [&](int k) { return sC[k - k0]; }, xa, xb, alpha, y);
-                    if (act && lane8 == 0) {
-#pragma unroll
-                        for (int w = 0; w < NV; w++)
-#pragma unroll
-                            for (int c = 0; c < 3; c++)
-                                ev[w][c] = sV[w * (tile_vec_bytes<VT>() / sizeof(VT)) + 3 * li + c];
-                    }
+                        [&](int k) { return sC[k - k0]; }, gat, y);
+                    if (act && lane8 == 0)
+                        epi(i, y, [&](int w, int c) { return sV[w * (tile_vec_bytes<VT>() / sizeof(VT)) + 3 * li + c]; });
                 } else {
-                    if (act && lane8 == 0) {   // issued ahead of the row's gathers
-#pragma unroll
-                        for (int w = 0; w < NV; w++)
-#pragma unroll
-                            for (int c = 0; c < 3; c++) ev[w][c] = ldv(vecs[w] + 3 * i + c);
-                    }
                     const int kb = act ? __ldg(K.rowptr + i) : 0, ke = act ? __ldg(K.rowptr + i + 1) : 0;
                     row_apply<MT, VT>(
                         act, lane8, kb, ke, [&](int k) { return A + (size_t)k * 9; },
-                        [&](int k) { return __ldg(K.col + k); }, xa, xb, alpha, y);
+                        [&](int k) { return __ldg(K.col + k); }, gat, y);
+                    if (act && lane8 == 0) epi(i, y, [&](int w, int c) { return ldv(vecs[w] + 3 * i + c); });
                 }
-                if (act && lane8 == 0) epi(i, y, ev);
                 if (STAGED) {
                     // this warp is done with the stage; the copy warp refills it for item + NST
                     __syncwarp();
@@ -558,6 +556,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         }
     };
 
+    int cur = 0;   // the copy of u, r, p, Ap that holds the current iterate
     // b <- M^-1 b'
     for (int i = pt0; rows && i < V; i += pstride) {
         const double* d = Dinv + (size_t)i * 9;
@@ -566,7 +565,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         for (int c = 0; c < 3; c++) {
             const VT y = (VT)(d[3 * c] * b0 + d[3 * c + 1] * b1 + d[3 * c + 2] * b2);
             b[3 * i + c] = y;
-            uu[3 * i + c] = y;
+            U2[0][3 * i + c] = y;
         }
     }
     if (!grid_sync(ctl, np)) return;
@@ -574,13 +573,23 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     {
         double vals[4] = {0, 0, 0, 0};
         const int ism[4] = {MAX, MAX, SUM, SUM};
+        const VT* ev2[2] = {b, U2[0]};
+        const VT* x0 = U2[0];
+        VT* const r = R2[0];
+        VT* const p = P2[0];
+        VT* const Ap = AP2[0];
         sweep(
-            IntC<2>{}, uu, (const VT*)nullptr, (VT)0, b, uu, nullptr,
-            [&](int i, const VT* y, const VT(*ev)[3]) {
+            IntC<2>{}, ev2,
+            [&](int j, VT (&x)[3]) {
+                x[0] = ldv(x0 + 3 * j);
+                x[1] = ldv(x0 + 3 * j + 1);
+                x[2] = ldv(x0 + 3 * j + 2);
+            },
+            [&](int i, const VT* y, auto&& ev) {
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
-                    const VT bb = ev[0][c];
-                    const VT rr = bb - (ev[1][c] + y[c]);
+                    const VT bb = ev(0, c);
+                    const VT rr = bb - (ev(1, c) + y[c]);
                     r[3 * i + c] = rr;
                     q[3 * i + c] = rr;
                     p[3 * i + c] = rr;
@@ -600,39 +609,118 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         nred++;
         double rnorm = rd[0];
         const double bnorm = rd[1];
-        double rho = rd[2], rhop = 1.0, alpha = 1.0, omega = 1.0;
+        double rho = rd[2], rhop = 1.0, alpha = 1.0, omega = 1.0, beta = 0.0;
         int it = 0;
         const double tol = K.atol + bnorm * rtol;
         // best iterate so far: past its attainable accuracy BiCGSTAB's residual drifts back up,
         // so on stagnation (no new best for kStall iterations) or at max_lin_it the best one is
         // used.  It is saved lazily: when an iteration sets a new best (`pending`), the next
-        // update pass, which reads u anyway, writes that u to ubest before overwriting it.
+        // update, which reads u anyway, writes that u to ubest.
         double best = rnorm;
         int best_it = 0;
         bool pending = true;
-        while (rnorm > tol && it < K.maxit && it - best_it < kStall) {
-            it++;
-            // (d)-(e): Ap = M^-1 A p, gamma = q . Ap
+        // An iteration's update (u += alpha p + omega s, r = s - omega As, p = beta (p - omega Ap)
+        // + r) is either its own vector pass with a grid barrier (fuse_update 0) or applied by the
+        // first sweep of the next iteration (fuse_update 1): that sweep's epilogue updates its own
+        // rows into the other copy, and its gathers form the new p of the neighbour rows from the
+        // old copies, with the same arithmetic, so the bits are those of the separate pass.  The
+        // stopping test of the updated residual then follows that sweep; when it stops the solve,
+        // the product A p that sweep formed is not used.
+        const bool fuse = src.fuse_update(KI);
+        bool upd = false;
+        while (upd || (rnorm > tol && it < K.maxit && it - best_it < kStall)) {
+            // [update of iteration it] and Ap = M^-1 A p, gamma = q . Ap
             {
                 double g[4] = {0, 0, 0, 0};
-                const int gm[4] = {SUM, SUM, SUM, SUM};
-                sweep(
-                    IntC<2>{}, p, (const VT*)nullptr, (VT)0, q, p, nullptr,
-                    [&](int i, const VT* y, const VT(*ev)[3]) {
+                const int gm[4] = {SUM, MAX, SUM, SUM};
+                if (!upd) {
+                    const VT* const p = P2[cur];
+                    VT* const Ap = AP2[cur];
+                    const VT* ev2[2] = {q, p};
+                    sweep(
+                        IntC<2>{}, ev2,
+                        [&](int j, VT (&x)[3]) {
+                            x[0] = ldv(p + 3 * j);
+                            x[1] = ldv(p + 3 * j + 1);
+                            x[2] = ldv(p + 3 * j + 2);
+                        },
+                        [&](int i, const VT* y, auto&& ev) {
 #pragma unroll
-                        for (int c = 0; c < 3; c++) {
-                            const VT apc = ev[1][c] + y[c];
-                            Ap[3 * i + c] = apc;
-                            g[0] += (double)ev[0][c] * (double)apc;
-                        }
-                    },
-                    [&](int v) {
-                        block_partial<1>(g, gm, pbuf(), v, red);
-                        g[0] = 0.0;
-                    });
+                            for (int c = 0; c < 3; c++) {
+                                const VT apc = ev(1, c) + y[c];
+                                Ap[3 * i + c] = apc;
+                                g[0] += (double)ev(0, c) * (double)apc;
+                            }
+                        },
+                        [&](int v) {
+                            block_partial<1>(g, gm, pbuf(), v, red);
+                            g[0] = 0.0;
+                        });
+                } else {
+                    const VT al = (VT)alpha, om = (VT)omega, be = (VT)beta;
+                    const VT* const uo = U2[cur];
+                    const VT* const ro = R2[cur];
+                    const VT* const po = P2[cur];
+                    const VT* const apo = AP2[cur];
+                    VT* const un = U2[cur ^ 1];
+                    VT* const rn = R2[cur ^ 1];
+                    VT* const pn = P2[cur ^ 1];
+                    VT* const apn = AP2[cur ^ 1];
+                    const bool save = pending;
+                    const VT* ev6[6] = {q, uo, po, apo, As, ro};
+                    sweep(
+                        IntC<6>{}, ev6,
+                        [&](int j, VT (&x)[3]) {   // the new p at node j
+#pragma unroll
+                            for (int c = 0; c < 3; c++) {
+                                const VT apk = ldv(apo + 3 * j + c);
+                                const VT s = fmadd(-al, apk, ldv(ro + 3 * j + c));
+                                const VT rk = fmadd(-om, ldv(As + 3 * j + c), s);
+                                x[c] = fmadd(fmadd(-om, apk, ldv(po + 3 * j + c)), be, rk);
+                            }
+                        },
+                        [&](int i, const VT* y, auto&& ev) {
+#pragma unroll
+                            for (int c = 0; c < 3; c++) {
+                                const int k = 3 * i + c;
+                                const VT apk = ev(3, c), pk = ev(2, c);
+                                const VT s = fmadd(-al, apk, ev(5, c));
+                                VT uk = ev(1, c);
+                                if (save) ubest[k] = uk;
+                                uk = fmadd(al, pk, uk);
+                                uk = fmadd(om, s, uk);
+                                un[k] = uk;
+                                const VT rk = fmadd(-om, ev(4, c), s);
+                                rn[k] = rk;
+                                const VT pnk = fmadd(fmadd(-om, apk, pk), be, rk);
+                                pn[k] = pnk;
+                                g[1] = fmax(g[1], fabs((double)rk));
+                                const VT apc = pnk + y[c];
+                                apn[k] = apc;
+                                g[0] += (double)ev(0, c) * (double)apc;
+                            }
+                        },
+                        [&](int v) {
+                            block_partial<2>(g, gm, pbuf(), v, red);
+                            g[0] = g[1] = 0.0;
+                        });
+                }
                 if (!grid_sync(ctl, np)) return;
-                grid_allreduce<1>(pbuf(), VG, gm, g, red);
+                if (!upd) {
+                    grid_allreduce<1>(pbuf(), VG, gm, g, red);
+                } else {
+                    grid_allreduce<2>(pbuf(), VG, gm, g, red);
+                    cur ^= 1;
+                    rnorm = g[1];
+                    pending = rnorm < best;   // identical decision in every CTA of the instance
+                    if (pending) {
+                        best = rnorm;
+                        best_it = it;
+                    }
+                    if (!(rnorm > tol && it < K.maxit && it - best_it < kStall)) break;
+                }
                 nred++;
+                it++;
                 alpha = rho / g[0];
             }
             // (f)-(g): As = M^-1 A (r - alpha Ap); omega, next rho
@@ -640,17 +728,24 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                 double w[4] = {0, 0, 0, 0};
                 const int wm[4] = {SUM, SUM, SUM, SUM};
                 const VT al = (VT)alpha;
+                const VT* const r = R2[cur];
+                const VT* const Ap = AP2[cur];
+                const VT* ev3[3] = {r, Ap, q};
                 sweep(
-                    IntC<3>{}, r, Ap, al, r, Ap, q,
-                    [&](int i, const VT* y, const VT(*ev)[3]) {
+                    IntC<3>{}, ev3,
+                    [&](int j, VT (&x)[3]) {   // the s the epilogue forms
+#pragma unroll
+                        for (int c = 0; c < 3; c++) x[c] = fmadd(-al, ldv(Ap + 3 * j + c), ldv(r + 3 * j + c));
+                    },
+                    [&](int i, const VT* y, auto&& ev) {
 #pragma unroll
                         for (int c = 0; c < 3; c++) {
-                            const VT s = fmadd(-al, ev[1][c], ev[0][c]);   // the s the gathers form
+                            const VT s = fmadd(-al, ev(1, c), ev(0, c));   // the s the gathers form
                             const VT asc = s + y[c];
                             As[3 * i + c] = asc;
                             w[0] += (double)asc * (double)s;
                             w[1] += (double)asc * (double)asc;
-                            w[2] += (double)asc * (double)ev[2][c];
+                            w[2] += (double)asc * (double)ev(2, c);
                         }
                     },
                     [&](int v) {
@@ -663,15 +758,20 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                 omega = w[0] / w[1];
                 rhop = rho;
                 rho = -1.0 * omega * w[2];
+                beta = (rho * alpha) / (rhop * omega);
+                upd = fuse;
             }
-            // (h)-(i) and the next search direction (c): u += alpha p + omega s; r = s - omega As;
-            // p = beta (p - omega Ap) + r with beta = (rho alpha) / (rhop omega)
+            if (fuse) continue;
+            // (h)-(i) and the next search direction (c) as a pass of its own, in place
             {
                 double mx[4] = {0, 0, 0, 0};
                 const int mm[4] = {MAX, MAX, MAX, MAX};
-                const double beta = (rho * alpha) / (rhop * omega);
                 const VT al = (VT)alpha, om = (VT)omega, be = (VT)beta;
-                auto upd = [&](int k) {
+                VT* const uu = U2[cur];
+                VT* const r = R2[cur];
+                VT* const p = P2[cur];
+                const VT* const Ap = AP2[cur];
+                auto upd1 = [&](int k) {
                     const VT apk = ldv(Ap + k), pk = ldv(p + k);
                     const VT s = fmadd(-al, apk, ldv(r + k));
                     VT uk = ldv(uu + k);
@@ -685,7 +785,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                     mx[0] = fmax(mx[0], fabs((double)rk));
                 };
                 // two elements per thread with 16-byte accesses (the vectors start on 256-byte
-                // boundaries); the arithmetic is that of upd, element by element
+                // boundaries); the arithmetic is that of upd1, element by element
                 auto upd2 = [&](int k2) {
                     using V2 = typename std::conditional<sizeof(VT) == 8, double2, float2>::type;
                     const V2 a2 = __ldcg(reinterpret_cast<const V2*>(Ap) + k2);
@@ -724,7 +824,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                     // updated on its own, the pairing only widens the loads
                     const int n2 = (3 * V) / 2;
                     for (int k2 = v * kKrylovRowThreads + threadIdx.x; k2 < n2; k2 += VG * kKrylovRowThreads) upd2(k2);
-                    if ((3 * V) % 2 && v == 0 && threadIdx.x == 0) upd(3 * V - 1);
+                    if ((3 * V) % 2 && v == 0 && threadIdx.x == 0) upd1(3 * V - 1);
                     block_partial<1>(mx, mm, pbuf(), v, red);
                     mx[0] = 0.0;
                 }
@@ -742,7 +842,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         const bool conv = rnorm <= tol;
         // x = S u; state += x; sol = -x.  Without convergence the best iterate is u itself when
         // the last iteration set it (not saved yet), else ubest.
-        const VT* ux = (conv || pending) ? uu : ubest;
+        const VT* ux = (conv || pending) ? U2[cur] : ubest;
         for (int i = pt0; rows && i < V; i += pstride) {
             const double x0 = (double)ldv(ux + 3 * i) * K.S[3 * i];
             const double x1 = (double)ldv(ux + 3 * i + 1) * K.S[3 * i + 1];

@@ -118,7 +118,7 @@ struct sw2gpu_ctx {
     DBuf<int> orowptr, ocol;
     DBuf<double> aoff64, dinv64;
     DBuf<float> aoff32;
-    DBuf<double> kv64[8];
+    DBuf<double> kv64[kKrylovVectors];
     DBuf<double> part;
     DBuf<Norms> npart;
     DBuf<unsigned> ncounter;
@@ -238,6 +238,7 @@ struct Runner {
     int stages = 0;               // Krylov tile-ring depth in use (0: sweeps from global memory)
     int jac_minb = 2;             // wet-Jacobian variant in use
     int jac_ctas[2] = {0, 0};     // persistent wet-Jacobian grid per variant (co-resident CTAs)
+    bool jac_ready = false;       // jac_ctas set (kernel attributes applied)
     unsigned c_off = 0, r_off = 0, v_off = 0, stage_bytes = 0;
     size_t smem = 0;
     int capacity = 0;             // co-resident Krylov CTAs
@@ -407,9 +408,13 @@ int runner_set(Runner& R, const std::vector<sw2gpu_ctx*>& ctx) {
     }
     int want = big ? big->tune_stages : 3;
     R.jac_minb = big ? big->tune_jac_minb : 2;
+    auto fitting_variant = [&R] {   // a wet-Jacobian variant that does not fit yields to the other
+        if (R.jac_ready && !R.jac_ctas[R.jac_minb - 1] && R.jac_ctas[2 - R.jac_minb]) R.jac_minb = 3 - R.jac_minb;
+    };
+    fitting_variant();
     const unsigned c_off = a_cap, r_off = c_off + c_cap;
     const unsigned v_off = r_off + ((unsigned)(kTileRows + 1) * 4u + 15u) / 16u * 16u;
-    const unsigned stage = (v_off + 3u * tile_vec_bytes<double>() + 127u) & ~127u;
+    const unsigned stage = (v_off + (unsigned)kMaxEpilogue * tile_vec_bytes<double>() + 127u) & ~127u;
     if (want > 0 && (size_t)want * stage > kMaxStagedSmem) want = (size_t)2 * stage <= kMaxStagedSmem ? 2 : 0;
     if (R.capacity > 0 && want == R.stages &&
         (!want || (a_cap <= R.c_off && c_cap <= R.r_off - R.c_off)))
@@ -439,7 +444,8 @@ int runner_set(Runner& R, const std::vector<sw2gpu_ctx*>& ctx) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tab, ktab, kKrylovThreads, R.smem));
     per_sm = std::min(per_sm, per_sm_tab);
     R.capacity = sms * std::max(1, std::min(per_sm, 4));
-    if (!R.jac_ctas[0]) {
+    if (!R.jac_ready) {
+        R.jac_ready = true;
         // wet-Jacobian kernels: double-buffered records above the 48 KB static limit, and a
         // persistent grid of the CTAs that fit at once
         const void* wet[2][2] = {{(const void*)k_jac_elem_wet<SrcOne, 1>, (const void*)k_jac_elem_wet<SrcPar, 1>},
@@ -452,9 +458,10 @@ int runner_set(Runner& R, const std::vector<sw2gpu_ctx*>& ctx) {
                 CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wet[v][k], kJacWetThreads, kJacWetSmem));
                 fit = std::min(fit, n);
             }
-            R.jac_ctas[v] = sms * std::max(1, fit);
+            R.jac_ctas[v] = sms * fit;   // 0: the variant does not fit on this device
         }
     }
+    fitting_variant();
     return 0;
 }
 
@@ -501,9 +508,10 @@ int runner_tables(Runner& R, int apply_inc) {
         A.part = c->part.p;
         A.ctl = R.ctl.p + k;
         A.vgrid = c->krylov_grid;
+        A.fuse_update = krylov_fuse_update(c->V);   // alone; a batch launch decides for its group
         Q.A = I.aoff;
         Q.Dinv = c->dinv64.p;
-        for (int v = 0; v < 8; v++) Q.vec[v] = c->kv64[v].p;
+        for (int v = 0; v < kKrylovVectors; v++) Q.vec[v] = c->kv64[v].p;
     }
     // the descriptors travel as kernel parameters; only batch Krylov launches read a table
     if (K > 1) {
@@ -616,6 +624,8 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
                 <<<std::min(nb_, R.jac_ctas[MB - 1]), th_, kJacWetSmem, R.stream>>>(src, nb_);
         });
     };
+    if (!R.jac_ctas[R.jac_minb - 1])
+        return fail(SW2GPU_E_CUDA, "wet-Jacobian variant %d does not fit on this device", R.jac_minb);
     int rc = R.jac_minb == 1 ? wet(std::integral_constant<int, 1>{}) : wet(std::integral_constant<int, 2>{});
     if (rc) return rc;
     // a captured launch covers the largest list (the kernel reads the list's length itself)
@@ -700,6 +710,9 @@ int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<doub
             }
             t.mp.boff[grp.size()] = off;
             t.lay = lay;
+            long long nodes = 0;
+            for (int k : grp) nodes += C(k)->V;
+            t.fuse = krylov_fuse_update(nodes);
             void* args[] = {(void*)&t};
             void* kern = R.mixed ? krylov_kernel<float, KrylovTab>(R.stages) : krylov_kernel<double, KrylovTab>(R.stages);
             CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kKrylovThreads), args, R.smem, R.stream));
@@ -1476,6 +1489,7 @@ int sw2gpu_autotune(sw2gpu_ctx* c, int32_t* jac_minb, int32_t* stages) {
     int best_j = c->tune_jac_minb;
     float tb = 1e30f;
     for (int m : {1, 2}) {
+        if (!R.jac_ctas[m - 1]) continue;   // does not fit on this device
         R.jac_minb = m;
         float t = 1e30f;
         if ((rc = timed([&] { return launch_jacobian(R, one); }, t))) break;

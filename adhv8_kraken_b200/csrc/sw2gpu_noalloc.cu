@@ -35,7 +35,7 @@ constexpr int kMaxGrid = (kMaxNodes + kKrylovThreads - 1) / kKrylovThreads;   //
 constexpr size_t kAlign = 32;                                                 // doubles = 256 bytes
 constexpr size_t al(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 // layout (in doubles): control word, partials, S, b', Dinv, folded off-diagonal blocks, their
-// row pointers and column indices (int32, two per double), 8 Krylov vectors
+// row pointers and column indices (int32, two per double), the Krylov vectors
 constexpr size_t kOffCtl = 0;
 constexpr size_t kOffPart = kOffCtl + al((sizeof(KrylovCtl) + 7) / 8);
 constexpr size_t kOffS = kOffPart + al(2ull * kMaxGrid * 4);
@@ -45,7 +45,7 @@ constexpr size_t kOffA = kOffDinv + al(9ull * kMaxNodes);
 constexpr size_t kOffRp = kOffA + al(9ull * kMaxBlocks);
 constexpr size_t kOffCol = kOffRp + al((kMaxNodes + 2) / 2);
 constexpr size_t kOffVec = kOffCol + al((kMaxBlocks + 1) / 2);
-constexpr size_t kScratchDoubles = kOffVec + 8 * al(3ull * kMaxNodes);
+constexpr size_t kScratchDoubles = kOffVec + kKrylovVectors * al(3ull * kMaxNodes);
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
@@ -171,8 +171,8 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     double* A = sc + kOffA;
     int* orp = reinterpret_cast<int*>(sc + kOffRp);
     int* ocol = reinterpret_cast<int*>(sc + kOffCol);
-    double* v[8];
-    for (int k = 0; k < 8; k++) v[k] = sc + kOffVec + k * al(3ull * kMaxNodes);
+    double* v[kKrylovVectors];
+    for (int k = 0; k < kKrylovVectors; k++) v[k] = sc + kOffVec + k * al(3ull * kMaxNodes);
     // the control words (barrier counter and generation, error and result fields) must
     // start at zero; everything else is written before it is read
     if (cudaMemsetAsync(ctl, 0, sizeof(KrylovCtl), st) != cudaSuccess)
@@ -203,9 +203,10 @@ extern "C" int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int
     K.part = part;
     K.ctl = ctl;
     K.vgrid = grid;
+    K.fuse_update = krylov_fuse_update(nnodes);
     one.Q.A = A;
     one.Q.Dinv = dinv;
-    for (int k = 0; k < 8; k++) one.Q.vec[k] = v[k];
+    for (int k = 0; k < kKrylovVectors; k++) one.Q.vec[k] = v[k];
     one.rtol = rtol;
     one.rtol_dev = nullptr;
     one.lay = StageLayout{0, 0, 0, 0};

@@ -169,7 +169,7 @@ int sw2gpu_linear_solve(sw2gpu_ctx *ctx, const double *val, const double *rhs, d
  * -> x[3*nnodes], all DEVICE pointers owned by the caller) with the same Jacobi scaling and
  * block-Jacobi BiCGSTAB as sw2gpu_linear_solve; the stopping test is
  * ||r||inf <= atol + rtol ||M^-1 S rhs||inf.  Its only work memory is one file-scope device
- * array of about 14.6 MB that every GPU loading the library keeps until exit, so systems
+ * array of about 16.7 MB that every GPU loading the library keeps until exit, so systems
  * above SW2GPU_NOALLOC_MAX_NODES rows or SW2GPU_NOALLOC_MAX_BLOCKS blocks are rejected with
  * SW2GPU_E_ARG.  The first call on a device looks up that array's device address (make it
  * before any stream capture).  All calls share the array: calls that overlap on the GPU
