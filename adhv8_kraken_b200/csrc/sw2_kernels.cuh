@@ -632,34 +632,48 @@ __global__ void k_jac_edge(const __grid_constant__ Src src) {
     }
 }
 
-// BCSR values: thread (block k, entry q) sums entry q of every contributing element
-// block in reference order (fe_global_matrix_assemble_sw2 :166-224).
+// BCSR values: thread k sums the nine entries of every element block contributing to BCSR
+// block k, in reference order (fe_global_matrix_assemble_sw2 :166-224).  Four contributions
+// (36 values) are loaded before they are added, so each warp keeps ~9 KB of loads in flight
+// behind its one dependent index load; the sums go out through shared memory as contiguous
+// 9-double records.
+constexpr int kGatherBlocks = 128;
 template <class Src>
-__global__ void k_jac_gather(const __grid_constant__ Src src) {
+__global__ void __launch_bounds__(kGatherBlocks) k_jac_gather(const __grid_constant__ Src src) {
+    __shared__ double out[kGatherBlocks * 9];
     int lb, nb;
     const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
     const double* __restrict__ jslots = I.jslots;
     double* __restrict__ val = I.val;
-    const long long t = (long long)lb * blockDim.x + threadIdx.x;
-    if (t >= (long long)m.nnzb * 9) return;
-    const int k = (int)(t / 9), q = (int)(t % 9);
-    const int c0 = m.blk_ptr[k], c1 = m.blk_ptr[k + 1];
-    // up to eight contributions' slot indices, then their values, are in flight together; the
-    // sum runs in contribution (reference) order
-    double acc = 0.0;
-    for (int c = c0; c < c1; c += 8) {
-        int src[8];
-        double v[8];
+    const int k0 = lb * kGatherBlocks;
+    const int k = k0 + threadIdx.x;
+    if (k < m.nnzb) {
+        double acc[9];
 #pragma unroll
-        for (int u = 0; u < 8; u++) src[u] = (c + u < c1) ? m.blk_src[c + u] : -1;
+        for (int q = 0; q < 9; q++) acc[q] = 0.0;
+        const int c0 = m.blk_ptr[k], c1 = m.blk_ptr[k + 1];
+        for (int c = c0; c < c1; c += 4) {
+            int sl[4];
+            double v[4][9];
 #pragma unroll
-        for (int u = 0; u < 8; u++) v[u] = src[u] >= 0 ? jslots[(size_t)src[u] * 9 + q] : 0.0;
+            for (int u = 0; u < 4; u++) sl[u] = (c + u < c1) ? __ldg(m.blk_src + c + u) : -1;
 #pragma unroll
-        for (int u = 0; u < 8; u++)
-            if (c + u < c1) acc += v[u];
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int q = 0; q < 9; q++) v[u][q] = sl[u] >= 0 ? __ldg(jslots + (size_t)sl[u] * 9 + q) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (c + u < c1)
+#pragma unroll
+                    for (int q = 0; q < 9; q++) acc[q] += v[u][q];
+        }
+#pragma unroll
+        for (int q = 0; q < 9; q++) out[threadIdx.x * 9 + q] = acc[q];
     }
-    val[t] = acc;
+    __syncthreads();
+    const int nk = min(kGatherBlocks, m.nnzb - k0);
+    for (int i = threadIdx.x; i < nk * 9; i += kGatherBlocks) val[(size_t)k0 * 9 + i] = out[i];
 }
 
 // Tiny-diagonal fix of fe_sw2_load (:218-236), the Jacobi scale vector of spv_jacobi and the
@@ -691,6 +705,7 @@ __global__ void k_rowscale(const __grid_constant__ Src src, int fix_only) {
     if (fabs(d[8]) < kNotQuiteSmall) d[8] = kNotQuiteSmall;
     if (fix_only) return;
     double mx[3] = {0.0, 0.0, 0.0};
+#pragma unroll 4
     for (int k = m.rowptr[n]; k < m.rowptr[n + 1]; k++) {
         const double* a = val + (size_t)k * 9;
 #pragma unroll

@@ -634,7 +634,8 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
                          SW2_GO(k_jac_elem_general<std::decay_t<decltype(src)>>))))
         return rc;
     if ((rc = launch_map(R, sub, 128, [&](int k) { return nblk(6LL * C(k)->E, 128); }, SW2_GO(k_jac_edge<std::decay_t<decltype(src)>>)))) return rc;
-    return launch_map(R, sub, 256, [&](int k) { return nblk(9LL * C(k)->nnzb, 256); }, SW2_GO(k_jac_gather<std::decay_t<decltype(src)>>));
+    return launch_map(R, sub, kGatherBlocks, [&](int k) { return nblk(C(k)->nnzb, kGatherBlocks); },
+                      SW2_GO(k_jac_gather<std::decay_t<decltype(src)>>));
 }
 
 // Krylov CTAs per instance: shares of the co-resident capacity by expected work (blocks x
