@@ -185,8 +185,12 @@ __global__ void k_classify(const __grid_constant__ Src src) {
     classify_elem(t, s.wd[t] == 0 && wet_depths(h, ho, hoo), ewet, glist, gcount);
 }
 
+// The element's record lives in shared memory (44 KB per CTA of 128 threads; 43 doubles per
+// record, an odd stride in 8-byte words: no bank conflicts), which leaves the registers to the
+// residual's arithmetic: three CTAs per SM instead of two.
+static_assert(sizeof(ElemIn) % 8 == 0 && (sizeof(ElemIn) / 8) % 2 == 1, "odd record stride");
 template <class Src>
-__global__ void k_resid_elem(const __grid_constant__ Src src) {
+__global__ void __launch_bounds__(128, 3) k_resid_elem(const __grid_constant__ Src src) {
     int lb, nb;
     const Inst& I = src.get(lb, nb);
     const DevMesh m = I.m;
@@ -200,8 +204,9 @@ __global__ void k_resid_elem(const __grid_constant__ Src src) {
     int* gcount = I.gcount;
     const int t = lb * blockDim.x + threadIdx.x;
     const int nslot = 3 * m.T + 2 * m.E;
+    __shared__ ElemIn rec[128];
     if (t < m.T) {
-        ElemIn in;
+        ElemIn& in = rec[threadIdx.x];
         int n[3], df[3];
         load_elem(m, s, t, 1, in, n, df);
         const int wd = s.wd[t];

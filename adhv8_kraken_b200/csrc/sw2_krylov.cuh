@@ -58,8 +58,8 @@ __device__ __forceinline__ int map_block(const LaunchMap& mp, int& lb, int& nb) 
 }
 
 struct KrylovCtl {
-    unsigned count;       // barrier arrival counter
-    unsigned gen;         // barrier generation
+    unsigned count;       // barrier arrivals since the launch (zeroed before it)
+    unsigned pad0;
     int err;              // 1 = a barrier or tile-copy wait ran out
     int iterations;
     int converged;        // 1 = stopping test met, 0 = hit max_lin_it
@@ -67,31 +67,26 @@ struct KrylovCtl {
     double rnorm, bnorm;
 };
 
-// Grid barrier with a bounded spin.  Returns false (and sets ctl->err) if any block
-// gave up; the caller then returns, so the kernel always terminates.
-__device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks) {
+// Grid barrier with a bounded spin.  Arrivals only ever add to one counter, so the b-th
+// barrier of a launch is passed once the counter reaches b * nblocks (`epoch`, per CTA): the
+// last arrival releases everyone without a second atomic.  Returns false (and sets ctl->err)
+// if any block gave up; the caller then returns, so the kernel always terminates.
+__device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks, unsigned& epoch) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = &ctl->gen;
-        const unsigned g = *vgen;
+        epoch += nblocks;
         __threadfence();
-        const unsigned arrived = atomicAdd(&ctl->count, 1u) + 1u;
-        if (arrived == nblocks) {
-            ctl->count = 0u;
-            __threadfence();
-            atomicAdd(&ctl->gen, 1u);
-        } else {
-            // tight bounded poll of the generation word (acquire loads, no sleep: a wake-up
-            // later than the release would be paid at every barrier)
-            long long spins = 0;
-            for (;;) {
-                unsigned cur;
-                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&ctl->gen) : "memory");
-                if (cur != g) break;
-                if (++spins > kBarrierSpinLimit || *(volatile int*)&ctl->err) {
-                    atomicExch(&ctl->err, 1);
-                    break;
-                }
+        atomicAdd(&ctl->count, 1u);
+        // tight bounded poll (acquire loads, no sleep: a wake-up later than the last arrival
+        // would be paid at every barrier)
+        long long spins = 0;
+        for (;;) {
+            unsigned cur;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&ctl->count) : "memory");
+            if ((int)(cur - epoch) >= 0) break;
+            if (++spins > kBarrierSpinLimit || *(volatile int*)&ctl->err) {
+                atomicExch(&ctl->err, 1);
+                break;
             }
         }
         __threadfence();
@@ -467,6 +462,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     const int SUM = 0, MAX = 1;
     KrylovCtl* ctl = K.ctl;
     int nred = 0;      // reductions so far; selects the partial buffer
+    unsigned epoch = 0;   // barrier arrivals this CTA waits for (grid_sync)
     unsigned tc = 0;   // tiles consumed by this CTA: stage tc % NST, mbarrier parity (tc / NST) & 1
     bool wait_failed = false;
     unsigned long long pol = 0;
@@ -568,7 +564,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
             U2[0][3 * i + c] = y;
         }
     }
-    if (!grid_sync(ctl, np)) return;
+    if (!grid_sync(ctl, np, epoch)) return;
     // r = b - M^-1 A u, q = r, p = r; norms and rho
     {
         double vals[4] = {0, 0, 0, 0};
@@ -603,7 +599,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                 block_partial<4>(vals, ism, pbuf(), v, red);
                 vals[0] = vals[1] = vals[2] = vals[3] = 0.0;
             });
-        if (!grid_sync(ctl, np)) return;
+        if (!grid_sync(ctl, np, epoch)) return;
         double rd[4];
         grid_allreduce<4>(pbuf(), VG, ism, rd, red);
         nred++;
@@ -705,7 +701,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                             g[0] = g[1] = 0.0;
                         });
                 }
-                if (!grid_sync(ctl, np)) return;
+                if (!grid_sync(ctl, np, epoch)) return;
                 if (!upd) {
                     grid_allreduce<1>(pbuf(), VG, gm, g, red);
                 } else {
@@ -752,7 +748,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                         block_partial<3>(w, wm, pbuf(), v, red);
                         w[0] = w[1] = w[2] = 0.0;
                     });
-                if (!grid_sync(ctl, np)) return;
+                if (!grid_sync(ctl, np, epoch)) return;
                 grid_allreduce<3>(pbuf(), VG, wm, w, red);
                 nred++;
                 omega = w[0] / w[1];
@@ -828,7 +824,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                     block_partial<1>(mx, mm, pbuf(), v, red);
                     mx[0] = 0.0;
                 }
-                if (!grid_sync(ctl, np)) return;
+                if (!grid_sync(ctl, np, epoch)) return;
                 grid_allreduce<1>(pbuf(), VG, mm, mx, red);
                 nred++;
                 rnorm = mx[0];
