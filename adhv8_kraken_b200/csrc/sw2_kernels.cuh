@@ -382,13 +382,14 @@ __device__ __forceinline__ void stage_elem(const DevMesh& m, const State& s, int
     S.mat = m.emat[e];
 }
 
-// One column (item = 3 b + var) of one element's 9x9 matrix into o[81]: R(x + eps e_j) and
-// R(x - eps e_j), the central difference, and the Dirichlet zeroing of the element matrix.
+// One column (item = 3 b + var) of one element's 9x9 matrix into o[81] (or, when g is given,
+// into the element's record g[81] in global memory, o holding only R(x + eps e_j)): R(x + eps e_j)
+// and R(x - eps e_j), the central difference, and the Dirichlet zeroing of the element matrix.
 // GENERAL = false: fully wet physics, with the parts the column leaves unperturbed read from
 // `pre`; GENERAL = true: full wet/dry physics.
 template <bool GENERAL>
 __device__ __forceinline__ void jac_column(const DevMesh& m, const PhysParams& P, const StagedElem& S,
-                                           const WetPre* pre, int item, double* o) {
+                                           const WetPre* pre, int item, double* o, double* g = nullptr) {
     const int b = item / 3, var = item % 3;  // var: 0 = u, 1 = v, 2 = h
     // only the current iterate (9 values) is private; everything else is read from the
     // staged element in shared memory
@@ -460,7 +461,8 @@ __device__ __forceinline__ void jac_column(const DevMesh& m, const PhysParams& P
                                               (aP && var == 2 && row == 2));
                 if (one) val = 1.0;
                 else if (zero) val = 0.0;
-                slot = val;
+                if (g) g[(3 * a + b) * 9 + 3 * row + var] = val;
+                else slot = val;
             }
         }
     }
@@ -468,19 +470,21 @@ __device__ __forceinline__ void jac_column(const DevMesh& m, const PhysParams& P
 
 // Fully wet elements: a persistent CTA of 9 column warps and one staging warp walks the
 // launch's 32-element groups (virtual blocks v = blockIdx.x, + gridDim.x, ...).  The staging
-// warp loads group i into buffer i & 1 and forms its shared parts (WetPre) while the column
-// warps evaluate group i - 1, so no column warp waits on element loads; buffers are handed
-// over with named barriers (FULL: staged, EMPTY: read).  Elements not eligible for the wet
+// warp loads group i into buffer i % kJacBufs and forms its shared parts (WetPre) while the
+// column warps evaluate earlier groups, so no column warp waits on element loads; buffers are
+// handed over with named barriers (FULL: staged, EMPTY: read by every column warp), and a column
+// warp may run ahead of the others by up to kJacBufs - 1 groups.  Elements not eligible for the wet
 // physics are skipped; the general launch, which runs after this one on the same stream,
 // writes their records.
 constexpr int kJacWetThreads = kJacThreads + 32;
-// named barriers of the wet-Jacobian CTA (0 is __syncthreads')
-constexpr int kJacBarFull = 1, kJacBarEmpty = 3, kJacBarCols = 5;
+constexpr int kJacBufs = 2;
+// named barriers of the wet-Jacobian CTA (0 is __syncthreads'), one FULL and one EMPTY per buffer
+constexpr int kJacBarFull = 1, kJacBarEmpty = 1 + kJacBufs;
 struct JacWetSmem {
-    StagedElem se[2][kJacElems];
-    WetPre pre[2][kJacElems];
-    double out[kJacElems * 81];
-    int eid[2][kJacElems];
+    StagedElem se[kJacBufs][kJacElems];
+    WetPre pre[kJacBufs][kJacElems];
+    double out[kJacElems * 81];   // per column thread: its nine R(x + eps e_j) values
+    int eid[kJacBufs][kJacElems];
 };
 constexpr size_t kJacWetSmem = sizeof(JacWetSmem);
 
@@ -495,8 +499,8 @@ __global__ void __launch_bounds__(kJacWetThreads, MINB) k_jac_elem_wet(const __g
     const int stride = gridDim.x;
     if (item == 9) {
         for (int i = 0, v = blockIdx.x; v < nvirt; i++, v += stride) {
-            const int j = i & 1;
-            if (i >= 2) bar_sync_n(kJacBarEmpty + j, kJacWetThreads);
+            const int j = i % kJacBufs;
+            if (i >= kJacBufs) bar_sync_n(kJacBarEmpty + j, kJacWetThreads);
             int lb, nb;
             const Inst& I = src.get_at(v, nvirt, lb, nb);
             const DevMesh m = I.m;
@@ -518,21 +522,18 @@ __global__ void __launch_bounds__(kJacWetThreads, MINB) k_jac_elem_wet(const __g
         return;
     }
     for (int i = 0, v = blockIdx.x; v < nvirt; i++, v += stride) {
-        const int j = i & 1;
+        const int j = i % kJacBufs;
         bar_sync_n(kJacBarFull + j, kJacWetThreads);
         int lb, nb;
         const Inst& I = src.get_at(v, nvirt, lb, nb);
-        const int e0 = lb * kJacElems;
-        const int nel = min(kJacElems, I.m.T - e0);
-        if (sm.eid[j][lane] >= 0) jac_column<false>(I.m, I.P, sm.se[j][lane], &sm.pre[j][lane], item, sm.out + lane * 81);
+        // each column thread stores its nine finished entries itself (the nine columns of an
+        // element meet in L2), so a column warp never waits for the others
+        const int e = sm.eid[j][lane];
+        if (e >= 0)
+            jac_column<false>(I.m, I.P, sm.se[j][lane], &sm.pre[j][lane], item, sm.out + lane * 81,
+                              I.jslots + (size_t)e * 81);
         __syncwarp();
-        bar_sync_n(kJacBarCols, kJacThreads);
-        double* dst = I.jslots + (size_t)e0 * 81;
-        for (int k = threadIdx.x; k < nel * 81; k += kJacThreads)
-            if (sm.eid[j][k / 81] >= 0) dst[k] = sm.out[k];
-        __syncwarp();
-        bar_sync_n(kJacBarCols, kJacThreads);   // `out` and buffer j are free again
-        if (v + 2 * stride < nvirt) bar_arrive_n(kJacBarEmpty + j, kJacWetThreads);
+        if (v + kJacBufs * stride < nvirt) bar_arrive_n(kJacBarEmpty + j, kJacWetThreads);
     }
 }
 
