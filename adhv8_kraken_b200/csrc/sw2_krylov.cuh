@@ -89,7 +89,8 @@ __device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks, unsi
                 break;
             }
         }
-        __threadfence();
+        // no trailing fence: the acquire load orders this thread's later accesses, and the
+        // __syncthreads below orders the rest of the CTA's after it
     }
     __syncthreads();
     return *(volatile int*)&ctl->err == 0;
