@@ -190,8 +190,16 @@ class SW2GPU:
         h, u, v = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, u, v))
         _check(lib().sw2gpu_set_state(self.h, level, _dp(h), _dp(u), _dp(v)))
 
-    def get_state(self, level=0):
-        h, u, v = (np.zeros(self.V) for _ in range(3))
+    def get_state(self, level=0, out=None):
+        """(h, u, v) of a time level; into `out` (three contiguous float64 arrays of V values,
+        e.g. views of pinned host buffers) when given, else into new arrays."""
+        if out is None:
+            h, u, v = (np.zeros(self.V) for _ in range(3))
+        else:
+            h, u, v = out
+            for a in (h, u, v):
+                if a.dtype != np.float64 or a.shape != (self.V,) or not a.flags.c_contiguous:
+                    raise ValueError("get_state: out arrays must be contiguous float64 of length V")
         _check(lib().sw2gpu_get_state(self.h, level, _dp(h), _dp(u), _dp(v)))
         return h, u, v
 
