@@ -423,9 +423,9 @@ __device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke
 // iteration stagnates).  Per instance, A holds the folded off-diagonal blocks D_i^-1 A'_ij
 // (rowptr / col of K) and Dinv the FP64 inverses (used once, for b = M^-1 b').  STAGED: the
 // SpMV sweeps read each tile's blocks, column indices, row pointers and epilogue vectors from
-// a STAGES-deep shared-memory ring filled by bulk copies (one thread issues, completion on
-// an mbarrier) STAGES - 1 tiles ahead of the rows being computed, so a row's only global
-// loads are its x gathers; the streamed matrix data carry an L2 evict-first hint, which keeps
+// a STAGES-deep shared-memory ring filled by bulk copies (the copy warp issues them up to
+// STAGES tiles ahead of the row warps, completion on an mbarrier per stage), so a row's only
+// global loads are its x gathers; the streamed matrix data carry an L2 evict-first hint, which keeps
 // the Krylov vectors in L2.  The dynamic shared memory is STAGES * L.stage_bytes.  STAGES = 0:
 // the lanes load everything from global memory.  Every variant computes the same bits.
 template <typename MT, typename VT, int STAGES, class KS>
