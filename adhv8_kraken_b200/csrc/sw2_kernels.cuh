@@ -361,8 +361,8 @@ __global__ void __launch_bounds__(kGatherThreads) k_resid_gather(const __grid_co
 // FD Jacobian of the 2D elements (fe_sw2_load :85-142, perturb_sw2_head / perturb_sw2_vel).
 // 32 elements x 9 perturbation columns (node b, variable u/v/h) at a time: warp w evaluates
 // column w for the 32 elements (lane = element), so the pressure-term branch is warp-uniform.
-// Element data are staged in shared memory once; the 9x9 element matrices are staged in
-// shared memory and written out as contiguous 81-double records (slot 9e + 3a + b).
+// Element data are staged in shared memory once; each element's 9x9 matrix is an 81-double
+// record (slot 9e + 3a + b) in global memory.
 constexpr int kJacElems = 32;
 constexpr int kJacThreads = kJacElems * 9;
 
