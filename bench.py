@@ -27,6 +27,7 @@ import json
 import math
 import os
 import statistics
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -356,12 +357,19 @@ def cpu_reference_sample(points: int = 10000, steps: int = 4, procs: int = 1, ti
         runs.append((m, d, subprocess.Popen([EXE, "m"], cwd=d, env=env, stdout=subprocess.DEVNULL,
                                             stderr=subprocess.DEVNULL)))
     tri_steps, secs = 0.0, []
-    for m, d, p in runs:
-        p.wait(timeout=timeout)
-        out = parse(read_dump(os.path.join(d, "dump.bin")))
-        s = sum(st["seconds"] for st in out["steps"])
-        tri_steps += m.nelems2d * len(out["steps"])
-        secs.append(s)
+    try:
+        for m, d, p in runs:
+            p.wait(timeout=timeout)
+            out = parse(read_dump(os.path.join(d, "dump.bin")))
+            s = sum(st["seconds"] for st in out["steps"])
+            tri_steps += m.nelems2d * len(out["steps"])
+            secs.append(s)
+    finally:
+        for _, d, p in runs:   # the runs' input decks and dumps are scratch
+            if p.poll() is None:
+                p.kill()
+                p.wait()
+            shutil.rmtree(d, ignore_errors=True)
     elapsed = max(secs)
     return {"value": tri_steps / elapsed, "tri_steps": tri_steps, "seconds": elapsed,
             "triangles": runs[0][0].nelems2d, "steps": steps, "procs": procs}

@@ -8,6 +8,7 @@ are parsed back into numpy arrays.
 from __future__ import annotations
 
 import os
+import shutil
 import subprocess
 import tempfile
 import time
@@ -65,14 +66,18 @@ def run_reference(model, nsteps=None, loads: int = 0, workdir: str = None, timeo
     if not os.path.exists(EXE):
         raise FileNotFoundError("oracle/_ref/adh_dump is not built (python oracle/ref/build_ref.py)")
     tmp = workdir or tempfile.mkdtemp(prefix="adhref_")
-    base = model.write_adh(tmp, "m", nsteps=nsteps)
-    env = dict(os.environ, ADH_DUMP=os.path.join(tmp, "dump.bin"), ADH_DUMP_LOADS=str(loads))
-    t0 = time.perf_counter()
-    r = subprocess.run([EXE, "m"], cwd=tmp, env=env, capture_output=True, text=True, timeout=timeout)
-    wall = time.perf_counter() - t0
-    if r.returncode != 0:
-        raise RuntimeError(f"reference run failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-2000:]}")
-    out = parse(read_dump(os.path.join(tmp, "dump.bin")))
+    try:
+        model.write_adh(tmp, "m", nsteps=nsteps)
+        env = dict(os.environ, ADH_DUMP=os.path.join(tmp, "dump.bin"), ADH_DUMP_LOADS=str(loads))
+        t0 = time.perf_counter()
+        r = subprocess.run([EXE, "m"], cwd=tmp, env=env, capture_output=True, text=True, timeout=timeout)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError(f"reference run failed ({r.returncode}):\n{r.stdout[-3000:]}\n{r.stderr[-2000:]}")
+        out = parse(read_dump(os.path.join(tmp, "dump.bin")))
+    finally:
+        if workdir is None:   # a scratch directory of our own
+            shutil.rmtree(tmp, ignore_errors=True)
     out["wall"] = wall
     out["stdout"] = r.stdout
     return out
