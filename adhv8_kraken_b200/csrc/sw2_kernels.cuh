@@ -69,7 +69,7 @@ struct __align__(16) Inst {
 
 // Where a launch finds its instances.  SrcOne: a single instance, its descriptor a kernel
 // parameter (fields read from the constant bank, the physics constants as direct operands);
-// SrcTab: a batch, descriptors in a device table and a LaunchMap of blocks to instances.
+// SrcPar (below): a group of instances, descriptors and block ranges as kernel parameters.
 struct SrcOne {
     Inst I;
     __device__ __forceinline__ const Inst& get(int& lb, int& nb) const {
@@ -83,11 +83,6 @@ struct SrcOne {
         nb = nvirt;
         return I;
     }
-};
-struct SrcTab {
-    const Inst* tab;
-    LaunchMap mp;
-    __device__ __forceinline__ const Inst& get(int& lb, int& nb) const { return tab[map_block(mp, lb, nb)]; }
 };
 // SrcPar: a group of up to kParInst instances whose descriptors are themselves kernel
 // parameters (~22 KB; fields come from the constant cache like SrcOne's instead of a global

@@ -541,28 +541,28 @@ int make_map(LaunchMap& mp, const std::vector<int>& subset, F blocks) {
 
 // one launch over the subset: instance k gets blocks(k) blocks of `threads` threads, and
 // go(src, blocks, threads) launches the kernel with its instance source -- the descriptor
-// itself when one instance is mapped, else the device table and the map
+// itself when one instance is mapped, else groups of descriptors with their block ranges
 template <class F, class G>
 int launch_map(Runner& R, const std::vector<int>& subset, int threads, F blocks, G go) {
-    static thread_local SrcTab t;   // ~2 KB map: not on every caller's stack
-    static thread_local SrcPar par; // ~22 KB
-    const int nb = make_map(t.mp, subset, blocks);
+    static thread_local LaunchMap mp;   // ~2 KB: not on every caller's stack
+    static thread_local SrcPar par;     // ~22 KB
+    const int nb = make_map(mp, subset, blocks);
     if (nb == 0) return 0;
-    if (t.mp.n == 1) {
+    if (mp.n == 1) {
         SrcOne one;
-        one.I = R.tab_h[t.mp.ids[0]];
+        one.I = R.tab_h[mp.ids[0]];
         go(one, nb, threads);
         R.launches++;
     } else {
         // groups of kParInst instances, descriptors as kernel parameters
-        for (int j0 = 0; j0 < t.mp.n; j0 += kParInst) {
-            const int j1 = std::min(t.mp.n, j0 + kParInst);
+        for (int j0 = 0; j0 < mp.n; j0 += kParInst) {
+            const int j1 = std::min(mp.n, j0 + kParInst);
             par.n = j1 - j0;
             for (int j = j0; j < j1; j++) {
-                par.boff[j - j0] = t.mp.boff[j] - t.mp.boff[j0];
-                par.I[j - j0] = R.tab_h[t.mp.ids[j]];
+                par.boff[j - j0] = mp.boff[j] - mp.boff[j0];
+                par.I[j - j0] = R.tab_h[mp.ids[j]];
             }
-            par.boff[j1 - j0] = t.mp.boff[j1] - t.mp.boff[j0];
+            par.boff[j1 - j0] = mp.boff[j1] - mp.boff[j0];
             go(par, par.boff[j1 - j0], threads);
             R.launches++;
         }
@@ -666,8 +666,7 @@ std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub) {
 
 // scaling, preconditioner folding and the persistent BiCGSTAB of the subset, each instance
 // with its own relative tolerance eta[k]
-int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<double>& eta, int fix_only_unused = 0) {
-    (void)fix_only_unused;
+int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<double>& eta) {
     auto C = [&](int k) { return R.ctx[k]; };
     CK(cudaMemsetAsync(R.singular.p, 0, sizeof(int) * R.ctx.size(), R.stream));
     int rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, SW2_GO(k_rowscale<std::decay_t<decltype(src)>>, 0));
