@@ -123,10 +123,10 @@ class ClockSampler:
                 "reasons": sorted(set().union(*[r[2] for r in self.rows])), "samples": len(self.rows)}
 
 
-def config2_model(points: int, nsteps: int):
+def basin_model(points: int, nsteps: int):
     from adhv8_kraken_b200 import meshgen
     size = 20000.0 * math.sqrt(points / 5e5)
-    return meshgen.bumpy_basin(points, seed=2024, size=size, nsteps=nsteps, dt=5.0, name="config2")
+    return meshgen.bumpy_basin(points, seed=2024, size=size, nsteps=nsteps, dt=5.0, name="basin")
 
 
 def max_over_ranks(x: float, world: int, device="cpu") -> float:
@@ -169,7 +169,7 @@ def run_small(stream, steps: int = 20, warmup: int = 3):
     from adhv8_kraken_b200 import meshgen
     from adhv8_kraken_b200.sw2 import SW2GPU
     m = meshgen.channel(nsteps=warmup + steps)
-    out = {"workload": f"config 1 channel: {m.nelems2d} triangles, dt {m.dt} s, {steps} steps after {warmup}"}
+    out = {"workload": f"channel: {m.nelems2d} triangles, dt {m.dt} s, {steps} steps after {warmup}"}
     for name, graphs in (("direct", False), ("graphs", True)):
         g = SW2GPU(m, stream=stream.cuda_stream)
         g.set_graphs(graphs)
@@ -408,7 +408,7 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.Stream(device=dev)
-    model = config2_model(args.points, args.warmup + args.steps + 8)
+    model = basin_model(args.points, args.warmup + args.steps + 8)
     T, V = model.nelems2d, model.nnodes
 
     def barrier():
