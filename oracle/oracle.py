@@ -53,6 +53,10 @@ def lib():
         L.orc_pattern.argtypes = [C.c_void_p, c_int32_p, c_int32_p]
         L.orc_get_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
         L.orc_set_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
+        L.orc_grid_mass.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.orc_grid_mass.restype = C.c_double
+        L.orc_mass_flux.argtypes = [C.c_void_p, C.c_double, C.c_double, c_double_p]
+        L.orc_mass_flux.restype = C.c_double
         _lib = L
     return _lib
 
@@ -148,6 +152,19 @@ class Oracle:
         out = np.zeros(9)
         lib().orc_body_resid(self.h, ie, eps, pnode, pvar, psign, _dp(out))
         return out.reshape(3, 3)
+
+    def grid_mass(self, level=0, density=None):
+        """Water mass of a time level (tl_find_grid_mass_elem2d)."""
+        rho = self.model.params.density if density is None else density
+        return lib().orc_grid_mass(self.h, level, rho)
+
+    def mass_flux(self, dt, series_now=None, density=None):
+        """Mass entering through sources and boundary edges over a step of dt at the current
+        level (the per-step term tl_find_grid_mass_error_elem2d accumulates); series_now: value
+        of every series at the evaluation time (water sources only)."""
+        rho = self.model.params.density if density is None else density
+        s = np.zeros(max(len(self.model.series), 1)) if series_now is None else np.ascontiguousarray(series_now, float)
+        return lib().orc_mass_flux(self.h, rho, dt, _dp(s))
 
     def step(self, dt=None, t=None):
         """One time step with the series averaged over [t, t + dt]; returns the stats dict."""

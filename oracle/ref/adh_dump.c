@@ -13,7 +13,12 @@
  *            wd_flag arrays;
  *   "load"   for the first ADH_DUMP_LOADS calls of fe_sw2_load: the state the
  *            Jacobian was built at (three time levels), the residual vector,
- *            the 3x3 diagonal blocks and every off-diagonal SPARSE_VECT row.
+ *            the 3x3 diagonal blocks and every off-diagonal SPARSE_VECT row;
+ *   "mass"   when ADH_DUMP_MASS is set, after every accepted step (right after its
+ *            "step" records): the reference's mass diagnostics of src/tools/tl_grid_mass.c
+ *            -- the initial grid mass (tl_find_grid_mass_elem2d before the first step),
+ *            the current grid mass, tl_find_grid_mass_error_elem2d and its accumulated
+ *            boundary / source mass flux.
  *
  * Record layout: char tag[8]; int32 kind (0 = f64, 1 = i32); int64 count; data.
  */
@@ -22,12 +27,22 @@
 
 int __real_fe_main(SSUPER_MODEL *sm);
 void __real_fe_sw2_load(SSUPER_MODEL *sm, int imod);
+/* the reference's mass diagnostics (src/tools/tl_grid_mass.c:20, :102); their prototypes are
+ * commented out in its headers (src/include/fnctn.h:176-178) */
+double tl_find_grid_mass_elem2d(double density, STR_VALUE *str, SSERIES *series_head, double *depth, SGRID *grid,
+                                SFLAGS flags);
+double tl_find_grid_mass_error_elem2d(double density, double *depth, SVECT2D *vel, SGRID *grid, SFLAGS flags,
+                                      double initial_grid_mass, SSERIES *series_head, STR_VALUE *str, double dt,
+                                      double *total_time_mass_flux_T);
 
 static FILE *dump_fp = NULL;
 static int dump_loads_left = -1;
 static int attempts = 0;
 static int it_mark = 0;
 static double solve_seconds = 0.0;   /* fe_main wall time since the last accepted step */
+static int dump_mass = 0;            /* ADH_DUMP_MASS set */
+static int mass_ready = 0;
+static double mass0 = 0.0, mass_flux_total = 0.0;
 
 static double now_seconds(void) {
     struct timespec ts;
@@ -42,6 +57,7 @@ static void dump_open(void) {
     dump_fp = fopen(path, "wb");
     const char *nl = getenv("ADH_DUMP_LOADS");
     dump_loads_left = nl ? atoi(nl) : 0;
+    dump_mass = getenv("ADH_DUMP_MASS") != NULL;
 }
 
 static void put_f64(const char *tag, const double *v, long n) {
@@ -81,6 +97,12 @@ static void put_state(const char *th, const char *tu, const char *tv, double *h,
 int __wrap_fe_main(SSUPER_MODEL *sm) {
     int r;
     dump_open();
+    if (dump_mass && !mass_ready && dump_fp != NULL) {   /* the initial state, before any shift */
+        SMODEL *mod = &(sm->submodel[0]);
+        mass0 = tl_find_grid_mass_elem2d(mod->density, mod->str_values, mod->series_head, mod->sw->d2->head,
+                                         mod->grid, mod->flag);
+        mass_ready = 1;
+    }
     double t0 = now_seconds();
     r = __real_fe_main(sm);
     solve_seconds += now_seconds() - t0;
@@ -100,6 +122,17 @@ int __wrap_fe_main(SSUPER_MODEL *sm) {
         put_i32("stepi", ihdr, 3);
         put_state("h", "u", "v", mod->sw->d2->head, mod->sw->d2->vel, n);
         put_i32("wd", mod->grid->wd_flag, mod->grid->nelems2d);
+        if (dump_mass) {
+            double m[4];
+            m[0] = mass0;
+            m[1] = tl_find_grid_mass_elem2d(mod->density, mod->str_values, mod->series_head, mod->sw->d2->head,
+                                            mod->grid, mod->flag);
+            m[2] = tl_find_grid_mass_error_elem2d(mod->density, mod->sw->d2->head, mod->sw->d2->vel, mod->grid,
+                                                  mod->flag, mass0, mod->series_head, mod->str_values, mod->dt,
+                                                  &mass_flux_total);
+            m[3] = mass_flux_total;
+            put_f64("mass", m, 4);
+        }
         fflush(dump_fp);
         attempts = 0;
         solve_seconds = 0.0;

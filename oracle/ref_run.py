@@ -48,6 +48,11 @@ def parse(recs) -> Dict[str, list]:
                               newton_its=int(hi[0]), attempts=int(hi[1]),
                               h=recs[i + 2][1], u=recs[i + 3][1], v=recs[i + 4][1], wd=recs[i + 5][1]))
             i += 6
+            if i < len(recs) and recs[i][0] == "mass":   # initial, current, error, accumulated flux
+                m = recs[i][1]
+                steps[-1].update(mass0=float(m[0]), mass=float(m[1]), mass_error=float(m[2]),
+                                 mass_flux_total=float(m[3]))
+                i += 1
         elif tag == "load":
             d = dict(t=arr[0], dt=arr[1])
             j = i + 1
@@ -61,14 +66,18 @@ def parse(recs) -> Dict[str, list]:
     return dict(steps=steps, loads=loads)
 
 
-def run_reference(model, nsteps=None, loads: int = 0, workdir: str = None, timeout: float = 3600.0):
-    """Run the reference on ``model``; returns parsed records and the wall time (s)."""
+def run_reference(model, nsteps=None, loads: int = 0, workdir: str = None, timeout: float = 3600.0,
+                  mass: bool = False):
+    """Run the reference on ``model``; returns parsed records and the wall time (s).  mass: also
+    record the reference's grid mass diagnostics after every step."""
     if not os.path.exists(EXE):
         raise FileNotFoundError("oracle/_ref/adh_dump is not built (python oracle/ref/build_ref.py)")
     tmp = workdir or tempfile.mkdtemp(prefix="adhref_")
     try:
         model.write_adh(tmp, "m", nsteps=nsteps)
         env = dict(os.environ, ADH_DUMP=os.path.join(tmp, "dump.bin"), ADH_DUMP_LOADS=str(loads))
+        if mass:
+            env["ADH_DUMP_MASS"] = "1"
         t0 = time.perf_counter()
         r = subprocess.run([EXE, "m"], cwd=tmp, env=env, capture_output=True, text=True, timeout=timeout)
         wall = time.perf_counter() - t0

@@ -1290,3 +1290,123 @@ int orc_step(orc_ctx *C, double dt, const double *series, sw2gpu_stats *st) {
     }
     return rc;
 }
+
+/* ------------------------------------------------------------------------------ */
+/* grid mass diagnostics (src/tools/tl_grid_mass.c) */
+
+/* fe_3m2d_dry_wet_factornew (tl_grid_mass.c:289-346): the wrapper's corner clip with "dry"
+ * meaning h < 0 (not <= 0); also returns the number of dry vertices (0 or 3 when the clipped
+ * corner is negligible) */
+static double mass_wet_factor(const v2 *x, const double *h, double edjac, int *num_dry) {
+    int i, total = 0, pass = 0, only;
+    v2 nx[3];
+    for (i = 0; i < 3; i++) {
+        int dry = h[i] < 0.0;
+        total += dry;
+        pass += dry << i;
+    }
+    if (total == 3) { *num_dry = 3; return 0.0; }
+    if (total == 0) { *num_dry = 0; return 1.0; }
+    if (total != 1) pass = 7 - pass;
+    only = pass / 2;
+    for (i = 0; i < 3; i++) {
+        if (i != only) {
+            double xsi = h[i] / (h[i] - h[only]);
+            nx[i].x = x[i].x + xsi * (x[only].x - x[i].x);
+            nx[i].y = x[i].y + xsi * (x[only].y - x[i].y);
+        } else {
+            nx[i] = x[i];
+        }
+    }
+    double djac = ((nx[1].x - nx[0].x) * (nx[2].y - nx[0].y) - (nx[1].y - nx[0].y) * (nx[2].x - nx[0].x)) / 2.0;
+    if (djac / edjac < ORC_SMALL) {
+        int odd = total % 2;
+        *num_dry = odd == 1 ? 0 : 3;
+        return (double) odd;
+    }
+    double factor = (double) ((total >> 1) - (total % 2));
+    *num_dry = total;
+    factor *= djac / edjac;
+    return factor + ((factor < 0) ? 1.0 : 0.0);
+}
+
+static double tri_f(double djac, double c, const double *f) {   /* integrate_triangle_f, elem2d :60 */
+    return c * djac * (f[0] + f[1] + f[2]) / 3.0;
+}
+
+/* tl_find_grid_mass_elem2d (tl_grid_mass.c:20-97): water mass of time level `level`; a
+ * partially dry triangle adds its wet part and, with one dry vertex, the negative depth of the
+ * dry corner counted as positive mass */
+double orc_grid_mass(const orc_ctx *C, int level, double density) {
+    const double *depth = C->h[level];
+    double mass = 0.0;
+    int e, i;
+    for (e = 0; e < C->T; e++) {
+        double eh[3], hneg[3] = {0.0, 0.0, 0.0}, f1, f2;
+        v2 x[3];
+        int num_dry;
+        for (i = 0; i < 3; i++) {
+            const int n = C->tri[3 * e + i];
+            eh[i] = depth[n];
+            x[i].x = C->x[n];
+            x[i].y = C->y[n];
+        }
+        const double factor = mass_wet_factor(x, eh, C->djac[e], &num_dry);
+        switch (num_dry) {
+            case 1:
+                for (i = 0; i < 3; i++)
+                    if (eh[i] < 0.0) hneg[i] = eh[i];
+                f1 = 1.0;
+                f2 = -1.0 * (1.0 - factor);
+                break;
+            case 2:
+                for (i = 0; i < 3; i++)
+                    if (eh[i] < 0.0) { hneg[i] = eh[i]; eh[i] = 0.0; }
+                f1 = factor;
+                f2 = 0.0;
+                break;
+            default:
+                f1 = factor;
+                f2 = 0.0;
+                break;
+        }
+        mass += tri_f(C->djac[e], f1, eh) + tri_f(C->djac[e], f2, hneg);
+    }
+    return mass * density;
+}
+
+/* The mass flux of one step for tl_find_grid_mass_error_elem2d (tl_grid_mass.c:102-159), at
+ * the current level: water sources over BCT_WATER_SOURCE elements (the series value
+ * `series_now[isigma]`, the wet/dry factor of fe_sw2_wet_dry_factor) and the implicit flow through
+ * the boundary edges, -integrate_line_h_f(djac, density dt, v.n, h) per edge with the djac of
+ * the first edge for every edge (grid->elem1d->djac, :141-142, kept).  The caller accumulates
+ * these and forms |mass - accumulated flux - initial mass|. */
+double orc_mass_flux(const orc_ctx *C, double density, double dt, const double *series_now) {
+    double body = 0.0, edge = 0.0;
+    int e, i;
+    for (e = 0; e < C->T; e++) {
+        const int s = C->tri_mat[e];
+        if (C->str_bc[s] != SW2GPU_BCT_WATER_SOURCE) continue;
+        double eh[3];
+        v2 x[3];
+        for (i = 0; i < 3; i++) {
+            const int n = C->tri[3 * e + i];
+            eh[i] = C->h[0][n];
+            x[i].x = C->x[n];
+            x[i].y = C->y[n];
+        }
+        const double factor = wd_factor(x, eh, C->djac[e]);
+        body += series_now[C->str_isigma[s]] * C->djac[e] * dt * density * factor;
+    }
+    for (e = 0; e < C->E; e++) {
+        double vn[2], eh[2];
+        for (i = 0; i < 2; i++) {
+            const int n = C->edges[2 * e + i];
+            eh[i] = C->h[0][n];
+            vn[i] = C->u[0][n] * C->enrml[2 * e] + C->v[0][n] * C->enrml[2 * e + 1];
+        }
+        const double t1 = C->edjac[0] * ONE_6 * (density * dt);    /* integrate_line_h_f, elem1d :18 */
+        edge -= t1 * ((2 * vn[0] + vn[1]) * eh[0] + (vn[0] + 2 * vn[1]) * eh[1]);
+    }
+    return body + edge;
+}

@@ -14,6 +14,10 @@ Fixtures (numpy ``.npz``):
 * ``basin_ref.npz`` -- a seeded Delaunay basin with dry bump tops (wet/dry fronts),
   8 steps: Newton iterations, state and wd flags after every step, and the first
   fe_sw2_load state / residual / Jacobian.
+* ``mass_ref.npz`` -- the reference's grid mass diagnostics (src/tools/tl_grid_mass.c) after
+  every step of 6 channel steps and of the 8 basin steps: initial and current mass, mass error
+  and accumulated mass flux, with the channel's state after every step (the basin's states are
+  in ``basin_ref.npz``).
 
 Each fixture stores a fingerprint of the generated model so a generator change is
 detected instead of silently comparing different problems.
@@ -117,8 +121,28 @@ def basin():
     np.savez_compressed(os.path.join(HERE, "basin_ref.npz"), **out)
 
 
+def mass():
+    out = {}
+    for name, m, n in (("channel", meshgen.channel(nsteps=6), 6), ("basin", basin_model(), 8)):
+        ref = run_reference(m, nsteps=n, mass=True)
+        out[f"{name}_fingerprint"] = np.array(fingerprint(m))
+        out[f"{name}_dt"] = np.array([s["dt"] for s in ref["steps"]])
+        for key in ("mass0", "mass", "mass_error", "mass_flux_total"):
+            out[f"{name}_{key}"] = np.array([s[key] for s in ref["steps"]])
+        if name == "channel":
+            for k, s in enumerate(ref["steps"], 1):
+                out[f"channel_step{k}_h"], out[f"channel_step{k}_u"], out[f"channel_step{k}_v"] = s["h"], s["u"], s["v"]
+    np.savez_compressed(os.path.join(HERE, "mass_ref.npz"), **out)
+
+
 if __name__ == "__main__":
-    channel()
-    basin()
-    for f in ("channel_ref.npz", "basin_ref.npz"):
+    import sys as _sys
+    which = _sys.argv[1:] or ["channel", "basin", "mass"]
+    if "channel" in which:
+        channel()
+    if "basin" in which:
+        basin()
+    if "mass" in which:
+        mass()
+    for f in ("channel_ref.npz", "basin_ref.npz", "mass_ref.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -70,3 +70,27 @@ def test_oracle_lake_at_rest_stays_at_rest():
     wet = h > 0.05
     assert np.abs(u[wet]).max() < 1e-6 and np.abs(v[wet]).max() < 1e-6
     assert np.abs((h + m.z - 2.0)[wet]).max() < 1e-7
+
+
+@pytest.mark.parametrize("case", ["channel", "basin"])
+def test_oracle_grid_mass_matches_reference(case, mass_ref, basin_ref):
+    """tl_find_grid_mass_elem2d and the per-step mass flux of tl_find_grid_mass_error_elem2d,
+    restated, against the reference's own values after every step (wet/dry clipped mass with
+    the negative-depth correction; boundary flux with the reference's edge length quirk)."""
+    from adhv8_kraken_b200 import meshgen
+    m = meshgen.channel(nsteps=6) if case == "channel" else basin_model()
+    assert str(mass_ref[f"{case}_fingerprint"]) == fingerprint(m)
+    o = Oracle(m)
+    mass0 = o.grid_mass(0)
+    assert relerr(mass0, mass_ref[f"{case}_mass0"][0]) <= 1e-14
+    acc = 0.0
+    for k, dt in enumerate(mass_ref[f"{case}_dt"], 1):
+        src = mass_ref if case == "channel" else basin_ref
+        pre = "channel_step" if case == "channel" else "step"
+        o.set_state(0, src[f"{pre}{k}_h"], src[f"{pre}{k}_u"], src[f"{pre}{k}_v"])
+        mass = o.grid_mass(0)
+        acc += o.mass_flux(dt)
+        err = abs(mass - acc - mass0)
+        assert relerr(mass, mass_ref[f"{case}_mass"][k - 1]) <= 1e-14, k
+        assert abs(acc - mass_ref[f"{case}_mass_flux_total"][k - 1]) <= 1e-13 * mass0, k
+        assert abs(err - mass_ref[f"{case}_mass_error"][k - 1]) <= 1e-13 * mass0, k
