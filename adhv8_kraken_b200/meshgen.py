@@ -83,6 +83,22 @@ def channel(nx: int = 100, ny: int = 20, length: float = 1000.0, width: float = 
                     v0=np.zeros(V), dt=dt, nsteps=nsteps, name=name)
 
 
+def channel_ovh(nsteps: int = 6, u_in: float = 0.5, **kw) -> SW2Model:
+    """The channel with its inflow given as NB OVH instead of NB VEL: water elevation 1 m above
+    the datum (the west bed) and velocity (u_in, 0) on the west edge; NB OTW tailwater east."""
+    from .model import BCT_OVH_NEU
+    m = channel(nsteps=nsteps, **kw)
+    t_end = (nsteps + 10) * m.dt
+    ns = len(m.series)
+    m.series = list(m.series) + [Series(np.array([0.0, t_end]), np.array([u_in, u_in])),
+                                 Series(np.array([0.0, t_end]), np.array([0.0, 0.0])),
+                                 Series(np.array([0.0, t_end]), np.array([1.0, 1.0]))]
+    m.strings = list(m.strings)
+    m.strings[1] = StringSpec("edge", bc_flag=BCT_OVH_NEU, ivx=ns, ivy=ns + 1, isigma=ns + 2)
+    m.name = "channel_ovh"
+    return m
+
+
 def bumpy_basin(npoints: int, seed: int, size: float = 20000.0, slope: float = 5e-4,
                 nbumps: int = 40, wse0: float = 2.0, n_median: float = 0.03, n_sigma: float = 0.3,
                 nbins: int = 32, q_start: float = 1.0, q_peak: float = 5.0, ramp_steps: int = 30,

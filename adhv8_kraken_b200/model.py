@@ -37,6 +37,7 @@ BCT_VEL_NEU = 10            # define.h:384  (NB VEL, unit discharge)
 BCT_WATER_SOURCE = 12       # define.h:386
 BCT_VEL_PRS_DIR = 16        # define.h:403
 BCT_OUTFLOW = 4             # define.h:378
+BCT_OVH_NEU = 18            # define.h:406  (NB OVH, tailwater elevation + velocities)
 BCT_DIS_NEU = 24            # define.h:412
 DBL_EPSILON = np.finfo(np.float64).eps
 FLT_EPSILON = float(np.finfo(np.float32).eps)
@@ -238,6 +239,8 @@ class SW2Model:
                         w(f"NB VEL {s_id + 1} {s.isigma + 1}\n")
                     elif s.bc_flag == BCT_PRS_NEU:
                         w(f"NB OTW {s_id + 1} {s.isigma + 1}\n")
+                    elif s.bc_flag == BCT_OVH_NEU:   # read_bc_NB.c:94-103: vx, vy, elevation series
+                        w(f"NB OVH {s_id + 1} {s.ivx + 1} {s.ivy + 1} {s.isigma + 1}\n")
                     else:
                         raise ValueError(f"unsupported edge bc flag {s.bc_flag}")
             for (a, b), s_id in zip(self.edges, self.edge_string):

@@ -46,6 +46,7 @@ extern "C" {
 #define SW2GPU_BCT_VEL_NEU    10   /* NB VEL: prescribed normal unit discharge */
 #define SW2GPU_BCT_WATER_SOURCE 12
 #define SW2GPU_BCT_VEL_PRS_DIR 16
+#define SW2GPU_BCT_OVH_NEU    18   /* NB OVH: tailwater elevation + velocities (sw2gpu_create rejects it for now) */
 
 /* precision modes */
 #define SW2GPU_FP64          0   /* everything FP64 */

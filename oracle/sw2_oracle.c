@@ -580,6 +580,32 @@ static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof
 /* ------------------------------------------------------------------------------ */
 /* fe_sw2_boundary_resid (edges) */
 
+/* fe_sw2_1d_implicit_flow (:637-): flow through the edge with the current velocity (outflow
+ * components only in the momentum fluxes) */
+static void implicit_flow(double djac, double dt, v2 n, const double *hh, const v2 *vel, dof3 *er) {
+    int i;
+    double u[2] = {vel[0].x, vel[1].x}, v[2] = {vel[0].y, vel[1].y};
+    double ur[2] = {u[0], u[1]}, vr[2] = {v[0], v[1]}, rc[2] = {0, 0}, rx[2] = {0, 0}, ry[2] = {0, 0};
+    for (i = 0; i < 2; i++) if (vel[i].x * n.x + vel[i].y * n.y < ORC_SMALL) { ur[i] = 0.; vr[i] = 0.; }
+    line_phi_h_v_dot_n(djac, 1., hh, vel, n, rc);
+    line_phi_f_g_h(djac, n.x, ur[0], ur[1], u[0], u[1], hh[0], hh[1], rx);
+    line_phi_f_g_h(djac, n.y, vr[0], vr[1], v[0], v[1], hh[0], hh[1], ry);
+    line_phi_f_g_h(djac, n.y, ur[0], ur[1], v[0], v[1], hh[0], hh[1], rx);
+    line_phi_f_g_h(djac, n.x, vr[0], vr[1], u[0], u[1], hh[0], hh[1], ry);
+    for (i = 0; i < 2; i++) { er[i].c += dt * rc[i]; er[i].x += dt * rx[i]; er[i].y += dt * ry[i]; }
+}
+/* fe_sw2_1d_pressure twice (:773-): the outside water column dep minus the inside one hh */
+static void boundary_pressure(double djac, double dt, double gr, v2 n, const double *dep, const double *hh, dof3 *er) {
+    int i;
+    double r[2] = {0, 0}, t1 = dt * 0.5 * gr;
+    line_phi_h_h(djac, 1., dep[0], dep[1], r);
+    for (i = 0; i < 2; i++) { er[i].x += t1 * n.x * r[i]; er[i].y += t1 * n.y * r[i]; }
+    r[0] = r[1] = 0;
+    t1 = dt * 0.5 * (-gr);
+    line_phi_h_h(djac, 1., hh[0], hh[1], r);
+    for (i = 0; i < 2; i++) { er[i].x += t1 * n.x * r[i]; er[i].y += t1 * n.y * r[i]; }
+}
+
 static void boundary_resid(const orc_ctx *C, int ie, const double *hh, const v2 *vel, int pvar, dof3 *er) {
     const sw2gpu_params *P = &C->p;
     int s = C->edge_string[ie], flag = C->str_bc[s], i;
@@ -614,24 +640,27 @@ static void boundary_resid(const orc_ctx *C, int ie, const double *hh, const v2 
             dep[1] = tail - z0;                                /* both from node 0 (:375-376) */
             if (dep[0] < ORC_SMALL || dep[1] < ORC_SMALL || hh[0] < ORC_SMALL || hh[1] < ORC_SMALL) return;
         }
-        /* implicit flow :637- */
-        double ur[2] = {u[0], u[1]}, vr[2] = {v[0], v[1]}, rc[2] = {0, 0}, rx[2] = {0, 0}, ry[2] = {0, 0};
-        for (i = 0; i < 2; i++) if (vel[i].x * n.x + vel[i].y * n.y < ORC_SMALL) { ur[i] = 0.; vr[i] = 0.; }
-        line_phi_h_v_dot_n(djac, 1., hh, vel, n, rc);
-        line_phi_f_g_h(djac, n.x, ur[0], ur[1], u[0], u[1], hh[0], hh[1], rx);
-        line_phi_f_g_h(djac, n.y, vr[0], vr[1], v[0], v[1], hh[0], hh[1], ry);
-        line_phi_f_g_h(djac, n.y, ur[0], ur[1], v[0], v[1], hh[0], hh[1], rx);
-        line_phi_f_g_h(djac, n.x, vr[0], vr[1], u[0], u[1], hh[0], hh[1], ry);
-        for (i = 0; i < 2; i++) { er[i].c += dt * rc[i]; er[i].x += dt * rx[i]; er[i].y += dt * ry[i]; }
-        if (flag == SW2GPU_BCT_PRS_NEU && pressure) {           /* fe_sw2_1d_pressure x2 */
-            double r[2] = {0, 0}, t1 = dt * 0.5 * gr;
-            line_phi_h_h(djac, 1., dep[0], dep[1], r);
-            for (i = 0; i < 2; i++) { er[i].x += t1 * n.x * r[i]; er[i].y += t1 * n.y * r[i]; }
-            r[0] = r[1] = 0;
-            t1 = dt * 0.5 * (-gr);
-            line_phi_h_h(djac, 1., hh[0], hh[1], r);
-            for (i = 0; i < 2; i++) { er[i].x += t1 * n.x * r[i]; er[i].y += t1 * n.y * r[i]; }
+        implicit_flow(djac, dt, n, hh, vel, er);
+        if (flag == SW2GPU_BCT_PRS_NEU && pressure) boundary_pressure(djac, dt, gr, n, dep, hh, er);
+    } else if (flag == SW2GPU_BCT_OVH_NEU) {                    /* elevation + velocities :398-440 */
+        const int na = C->edges[2 * ie], nb = C->edges[2 * ie + 1];
+        const double tail = C->series[C->str_isigma[s]];
+        double dep[2] = {tail - C->z[na], tail - C->z[nb]};   /* each node's own bed here */
+        if (dep[0] < ORC_SMALL || dep[1] < ORC_SMALL)           /* the reference stops the run (tl_error) */
+            fprintf(stderr, "oracle: NB OVH tailwater elevation below the bed on edge %d\n", ie);
+        v2 uv = {C->series[C->str_ivx[s]], C->series[C->str_ivy[s]]};
+        if (uv.x * n.x + uv.y * n.y < -ORC_SMALL) {             /* inflow: fe_sw2_1d_hvel :882-897 */
+            double rc[2] = {0, 0};
+            line_phi_h_v_dot_n(djac, 1., hh, vel, n, rc);
+            for (i = 0; i < 2; i++) {
+                er[i].c += dt * rc[i];
+                er[i].x += dt * rc[i] * uv.x;
+                er[i].y += dt * rc[i] * uv.y;
+            }
+        } else {
+            implicit_flow(djac, dt, n, hh, vel, er);
         }
+        if (pressure) boundary_pressure(djac, dt, gr, n, dep, hh, er);
     }
     for (i = 0; i < 2; i++) {                                  /* Dirichlet :483-498 */
         int ns = C->node_string[C->edges[2 * ie + i]];
@@ -780,7 +809,7 @@ orc_ctx *orc_create(const sw2gpu_mesh *m, const sw2gpu_params *p, int nblock) {
         C->edjac[i] = sqrt((C->x[a] - C->x[b]) * (C->x[a] - C->x[b]) + (C->y[a] - C->y[b]) * (C->y[a] - C->y[b]));
         C->enrml[2 * i] = nx; C->enrml[2 * i + 1] = ny;
         int f = C->str_bc[C->edge_string[i]];
-        if (f != SW2GPU_BCT_VEL_NEU && f != SW2GPU_BCT_PRS_NEU && f != SW2GPU_BCT_OUTFLOW) {
+        if (f != SW2GPU_BCT_VEL_NEU && f != SW2GPU_BCT_PRS_NEU && f != SW2GPU_BCT_OUTFLOW && f != SW2GPU_BCT_OVH_NEU) {
             fprintf(stderr, "oracle: unsupported edge bc flag %d\n", f); free(C); return NULL;
         }
     }

@@ -94,3 +94,25 @@ def test_oracle_grid_mass_matches_reference(case, mass_ref, basin_ref):
         assert relerr(mass, mass_ref[f"{case}_mass"][k - 1]) <= 1e-14, k
         assert abs(acc - mass_ref[f"{case}_mass_flux_total"][k - 1]) <= 1e-13 * mass0, k
         assert abs(err - mass_ref[f"{case}_mass_error"][k - 1]) <= 1e-13 * mass0, k
+
+
+def test_oracle_ovh_boundary_matches_reference(ovh_ref):
+    """NB OVH inflow (elevation + velocity, fe_sw2_boundary_resid.c:398-440 with
+    fe_sw2_1d_hvel): residual and FD Jacobian at the first load, then 6 steps."""
+    from adhv8_kraken_b200 import meshgen
+    m = meshgen.channel_ovh(nsteps=6)
+    assert str(ovh_ref["fingerprint"]) == fingerprint(m)
+    o = Oracle(m)
+    set_load_state(o, m, ovh_ref)
+    o.resid()
+    val, r = o.load()
+    assert relerr(r, ovh_ref["load0_resid"]) <= 1e-13
+    assert relerr(val, ovh_ref["load0_val"]) <= 1e-7
+    o = Oracle(m)
+    for k in range(6):
+        st = o.step(dt=ovh_ref["dt"][k], t=ovh_ref["t"][k])
+        assert st["status"] == 0 and st["newton_its"] == ovh_ref["newton_its"][k]
+        got = fields(*o.get_state(0))
+        exp = fields(ovh_ref[f"step{k+1}_h"], ovh_ref[f"step{k+1}_u"], ovh_ref[f"step{k+1}_v"])
+        for f, e in field_errors(got, exp).items():
+            assert e <= 1e-10, (k, f, e)
