@@ -99,6 +99,16 @@ def channel_ovh(nsteps: int = 6, u_in: float = 0.5, **kw) -> SW2Model:
     return m
 
 
+def channel_outflow(nsteps: int = 6, **kw) -> SW2Model:
+    """The channel with a free outflow edge (NB OF: implicit flow, no tailwater) east."""
+    from .model import BCT_OUTFLOW
+    m = channel(nsteps=nsteps, **kw)
+    m.strings = list(m.strings)
+    m.strings[2] = StringSpec("edge", bc_flag=BCT_OUTFLOW)
+    m.name = "channel_outflow"
+    return m
+
+
 def bumpy_basin(npoints: int, seed: int, size: float = 20000.0, slope: float = 5e-4,
                 nbumps: int = 40, wse0: float = 2.0, n_median: float = 0.03, n_sigma: float = 0.3,
                 nbins: int = 32, q_start: float = 1.0, q_peak: float = 5.0, ramp_steps: int = 30,

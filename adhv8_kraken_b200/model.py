@@ -241,6 +241,8 @@ class SW2Model:
                         w(f"NB OTW {s_id + 1} {s.isigma + 1}\n")
                     elif s.bc_flag == BCT_OVH_NEU:   # read_bc_NB.c:94-103: vx, vy, elevation series
                         w(f"NB OVH {s_id + 1} {s.ivx + 1} {s.ivy + 1} {s.isigma + 1}\n")
+                    elif s.bc_flag == BCT_OUTFLOW:   # read_bc_NB.c:21-27
+                        w(f"NB OF {s_id + 1}\n")
                     else:
                         raise ValueError(f"unsupported edge bc flag {s.bc_flag}")
             for (a, b), s_id in zip(self.edges, self.edge_string):

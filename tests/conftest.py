@@ -25,11 +25,6 @@ def basin_ref():
 
 
 @pytest.fixture(scope="session")
-def ovh_ref():
-    return dict(np.load(os.path.join(GOLDEN, "ovh_ref.npz")))
-
-
-@pytest.fixture(scope="session")
 def mass_ref():
     return dict(np.load(os.path.join(GOLDEN, "mass_ref.npz")))
 

@@ -17,6 +17,8 @@ Fixtures (numpy ``.npz``):
 * ``ovh_ref.npz`` -- the channel with its inflow given as NB OVH (elevation + velocity),
   6 steps: Newton iterations, state after every step, and the first fe_sw2_load state /
   residual / Jacobian.
+* ``outflow_ref.npz`` -- the channel with a free outflow edge (NB OF) east, 6 steps, recorded
+  like ``ovh_ref.npz``.
 * ``mass_ref.npz`` -- the reference's grid mass diagnostics (src/tools/tl_grid_mass.c) after
   every step of 6 channel steps and of the 8 basin steps: initial and current mass, mass error
   and accumulated mass flux, with the channel's state after every step (the basin's states are
@@ -124,8 +126,8 @@ def basin():
     np.savez_compressed(os.path.join(HERE, "basin_ref.npz"), **out)
 
 
-def ovh():
-    m = meshgen.channel_ovh(nsteps=6)
+def ovh(m=None, fname="ovh_ref.npz"):
+    m = meshgen.channel_ovh(nsteps=6) if m is None else m
     ref = run_reference(m, nsteps=6, loads=1)
     out = {"fingerprint": np.array(fingerprint(m)),
            "newton_its": np.array([s["newton_its"] for s in ref["steps"]], np.int32),
@@ -133,7 +135,7 @@ def ovh():
     for k, s in enumerate(ref["steps"], 1):
         out[f"step{k}_h"], out[f"step{k}_u"], out[f"step{k}_v"] = s["h"], s["u"], s["v"]
     out.update(load_record(m, ref["loads"][0], "load0"))
-    np.savez_compressed(os.path.join(HERE, "ovh_ref.npz"), **out)
+    np.savez_compressed(os.path.join(HERE, fname), **out)
 
 
 def mass():
@@ -152,14 +154,16 @@ def mass():
 
 if __name__ == "__main__":
     import sys as _sys
-    which = _sys.argv[1:] or ["channel", "basin", "ovh", "mass"]
+    which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "mass"]
     if "channel" in which:
         channel()
     if "basin" in which:
         basin()
     if "ovh" in which:
         ovh()
+    if "outflow" in which:
+        ovh(meshgen.channel_outflow(nsteps=6), "outflow_ref.npz")
     if "mass" in which:
         mass()
-    for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "mass_ref.npz"):
+    for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "mass_ref.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))
