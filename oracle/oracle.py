@@ -53,6 +53,7 @@ def lib():
         L.orc_pattern.argtypes = [C.c_void_p, c_int32_p, c_int32_p]
         L.orc_get_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
         L.orc_set_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
+        L.orc_geometry.argtypes = [C.c_void_p, C.c_int, c_double_p]
         L.orc_grid_mass.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.orc_grid_mass.restype = C.c_double
         L.orc_mass_flux.argtypes = [C.c_void_p, C.c_double, C.c_double, c_double_p]
@@ -152,6 +153,12 @@ class Oracle:
         out = np.zeros(9)
         lib().orc_body_resid(self.h, ie, eps, pnode, pvar, psign, _dp(out))
         return out.reshape(3, 3)
+
+    def geometry(self, ie):
+        """(djac, [gx0, gy0, gx1, gy1, gx2, gy2]) of element ie."""
+        out = np.zeros(7)
+        lib().orc_geometry(self.h, ie, _dp(out))
+        return out[0], out[1:]
 
     def grid_mass(self, level=0, density=None):
         """Water mass of a time level (tl_find_grid_mass_elem2d)."""

@@ -875,6 +875,13 @@ void orc_wdflag(orc_ctx *C) {
 }
 
 /* single element residual (unit tests): out[9] = node-major (c, x, y) */
+/* element ie's area and P1 shape gradients: out = djac, gx0, gy0, gx1, gy1, gx2, gy2 */
+void orc_geometry(const orc_ctx *C, int ie, double *out) {
+    int i;
+    out[0] = C->djac[ie];
+    for (i = 0; i < 6; i++) out[1 + i] = C->grad[6 * ie + i];
+}
+
 void orc_body_resid(orc_ctx *C, int ie, double eps, int pnode, int pvar, int psign, double *out) {
     elem_in E; dof3 er[3]; int i;
     gather_elem(C, ie, &E);

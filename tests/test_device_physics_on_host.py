@@ -1,0 +1,148 @@
+"""The device element physics (adhv8_kraken_b200/csrc/sw2_physics.cuh, the code every residual and
+Jacobian kernel runs) compiled as host C++ and checked element by element against the oracle:
+fully wet and wet/dry elements, unperturbed and with the Jacobian's +-eps perturbations, on a basin
+with wet/dry fronts and every optional term switched on (temporal alpha, eddy viscosity, Coriolis).
+Runs on CPU, so a change to the physics is checked on every CPU run; the GPU parity tests check
+the same code as compiled for sm_100a."""
+import ctypes as C
+import dataclasses
+import math
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from adhv8_kraken_b200 import capi, meshgen
+from adhv8_kraken_b200.model import Material
+from oracle.oracle import Oracle
+from oracle.oracle import lib as oracle_lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, "adhv8_kraken_b200", "csrc")
+
+SHIM = r"""
+#include <algorithm>
+#include <cmath>
+using std::fabs; using std::fmax; using std::log; using std::pow; using std::sqrt;
+#define __device__
+#define __host__
+#define __forceinline__ inline
+#define __noinline__
+#include "sw2_physics.cuh"
+using namespace sw2;
+
+// xyz: x[3], y[3], z[3]; lv: h, u, v at the current, old and older levels (3 values each);
+// geo: djac, gx0, gy0, gx1, gy1, gx2, gy2; phys: g, dll, dul, alpha, tau_pg, dt;
+// mat: ks, ev_st, ev_tr, eev_coef, cor_speed, water_src
+extern "C" void host_elem_resid(const double* xyz, const double* lv, const double* geo, int wd, int pvar, int pnode,
+                                double dx, const double* phys, const double* mat, int eev_mode, int has_source,
+                                double* out) {
+    ElemIn in;
+    for (int i = 0; i < 3; i++) {
+        in.x[i] = xyz[i]; in.y[i] = xyz[3 + i]; in.z[i] = xyz[6 + i];
+        in.h[i] = lv[i]; in.u[i] = lv[3 + i]; in.v[i] = lv[6 + i];
+        in.ho[i] = lv[9 + i]; in.uo[i] = lv[12 + i]; in.vo[i] = lv[15 + i];
+        in.hoo[i] = lv[18 + i]; in.uoo[i] = lv[21 + i]; in.voo[i] = lv[24 + i];
+        in.gx[i] = geo[1 + 2 * i]; in.gy[i] = geo[2 + 2 * i];
+    }
+    in.djac = geo[0];
+    double hc[3], uc[3], vc[3];
+    for (int i = 0; i < 3; i++) { hc[i] = in.h[i]; uc[i] = in.u[i]; vc[i] = in.v[i]; }
+    if (pvar == kPertH) hc[pnode] += dx;
+    else if (pvar == kPertU) uc[pnode] += dx;
+    else if (pvar == kPertV) vc[pnode] += dx;
+    const PhysParams P{phys[0], phys[1], phys[2], phys[3], phys[4], phys[5]};
+    MatParams M{};
+    M.ks = mat[0]; M.ev_st = mat[1]; M.ev_tr = mat[2]; M.eev_coef = mat[3]; M.cor_speed = mat[4];
+    M.water_src = mat[5]; M.eev_mode = eev_mode; M.has_source = has_source;
+    const int df[3] = {0, 0, 0};
+    double er[3][3];
+    sw2_elem_resid(in, hc, uc, vc, wd, pvar, P, M, df, er);
+    for (int i = 0; i < 3; i++)
+        for (int q = 0; q < 3; q++) out[3 * i + q] = er[i][q];
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def host_physics():
+    if shutil.which("g++") is None or not os.path.isdir("/usr/local/cuda/include"):
+        pytest.skip("no host C++ compiler or CUDA headers")
+    work = os.path.join(ROOT, "_build", "host_physics")   # git-ignored scratch inside the tree
+    os.makedirs(work, exist_ok=True)
+    src, lib = os.path.join(work, "shim.cpp"), os.path.join(work, "libhostphys.so")
+    with open(src, "w") as fh:
+        fh.write(SHIM)
+    r = subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I", CSRC, "-I", "/usr/local/cuda/include",
+                        "-o", lib, src], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    L = C.CDLL(lib)
+    yield L
+    shutil.rmtree(work, ignore_errors=True)
+    try:
+        os.rmdir(os.path.dirname(work))
+    except OSError:
+        pass
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _fd_eps(x):   # NUM_DIFF_EPSILON (src/include/macro.h:669-673)
+    p = 1.4901161193847656e-08
+    e = abs(x) * (1.0 + p) - abs(x)
+    return p if e < p else e
+
+
+def test_device_physics_matches_oracle_on_host(host_physics):
+    base = meshgen.bumpy_basin(900, seed=5, size=2500.0, nsteps=4, dt=5.0, nbins=3, name="physics")
+    m = dataclasses.replace(
+        base, params=dataclasses.replace(base.params, tau_temporal=0.5),
+        materials=[Material(evs=(6.0, 2.0, 1.0), coriolis=30.0)] + [Material(eev_coef=0.4, eev_mode=k) for k in (1, 2)])
+    o = Oracle(m)
+    for _ in range(2):   # distinct time levels and moving wet/dry fronts
+        assert o.step()["status"] == 0
+    o.set_dt(m.dt, m.series_values(o.t, o.t + m.dt))
+    o.wdflag()
+    wd = o.get_wd()
+    arrays = capi.MeshArrays(m)
+    prm = capi.make_params(m)
+    levels = [o.get_state(k) for k in range(3)]
+    phys = np.array([prm.gravity, prm.drying_lower_limit, prm.drying_upper_limit, prm.tau_temporal, prm.tau_pg, m.dt])
+    ks = np.ctypeslib.as_array(arrays.mesh.str_rough_height, shape=(len(m.strings),))
+    rng = np.random.Generator(np.random.PCG64(3))
+    h0 = levels[0][0]
+    tri = m.tri
+    fringe = np.nonzero((wd != 0) | (h0[tri] <= 0.0).any(axis=1))[0]
+    picks = np.concatenate([fringe[:150], rng.choice(m.nelems2d, 150, replace=False)])
+    assert fringe.size > 0
+    worst = 0.0
+    for ie in picks:
+        nodes = tri[ie]
+        xyz = np.concatenate([m.x[nodes], m.y[nodes], m.z[nodes]])
+        lv = np.concatenate([levels[k][j][nodes] for k in range(3) for j in range(3)])
+        djac, g6 = o.geometry(int(ie))
+        geo = np.concatenate([[djac], g6])
+        k = int(m.tri_mat[ie])
+        mt = m.materials[k]
+        xx, yy = mt.evs[0] + prm.viscosity, mt.evs[1] + prm.viscosity
+        mat = np.array([ks[k], abs(xx - yy), min(xx, yy), mt.eev_coef,
+                        math.sin(math.pi / 180.0 * mt.coriolis) * 2.0 * 7.2722e-5, 0.0])
+        cases = [(-1, 0, 0.0, 0)]
+        for pvar, arr in ((1, levels[0][1]), (2, levels[0][2]), (5, levels[0][0])):
+            b = int(rng.integers(0, 3))
+            eps = _fd_eps(arr[nodes[b]])
+            cases += [(pvar, b, eps, 1), (pvar, b, -eps, -1)]
+        for pvar, b, dx, sign in cases:
+            dev, ref = np.zeros(9), np.zeros(9)
+            host_physics.host_elem_resid(_dp(xyz), _dp(lv), _dp(geo), int(wd[ie]), pvar, b, C.c_double(dx), _dp(phys),
+                                         _dp(mat), mt.eev_mode, 0, _dp(dev))
+            oracle_lib().orc_body_resid(o.h, int(ie), abs(dx), b, pvar, sign, _dp(ref))
+            scale = max(np.abs(ref).max(), 1e-300)
+            err = float(np.abs(dev - ref).max() / scale)
+            worst = max(worst, err)
+            assert err <= 1e-12, (int(ie), pvar, b, sign, err, dev, ref)
+    assert worst <= 1e-12
