@@ -54,6 +54,7 @@ def lib():
         L.orc_get_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
         L.orc_set_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
         L.orc_geometry.argtypes = [C.c_void_p, C.c_int, c_double_p]
+        L.orc_edge_resid.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, c_double_p, c_double_p]
         L.orc_grid_mass.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.orc_grid_mass.restype = C.c_double
         L.orc_mass_flux.argtypes = [C.c_void_p, C.c_double, C.c_double, c_double_p]

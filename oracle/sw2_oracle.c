@@ -875,6 +875,30 @@ void orc_wdflag(orc_ctx *C) {
 }
 
 /* single element residual (unit tests): out[9] = node-major (c, x, y) */
+/* boundary edge ie's residual (out[3 i + {c, x, y}] for its two nodes) at the current level,
+ * with the perturbation psign * eps of variable pvar at its node pnode; also its length and
+ * outward normal (geo = djac, nx, ny) */
+void orc_edge_resid(orc_ctx *C, int ie, double eps, int pnode, int pvar, int psign, double *out, double *geo) {
+    double hh[2];
+    v2 vel[2];
+    dof3 er[2];
+    int i;
+    for (i = 0; i < 2; i++) {
+        int n = C->edges[2 * ie + i];
+        hh[i] = C->h[0][n];
+        vel[i].x = C->u[0][n];
+        vel[i].y = C->v[0][n];
+    }
+    if (pvar == P_H) hh[pnode] += psign * eps;
+    else if (pvar == P_U) vel[pnode].x += psign * eps;
+    else if (pvar == P_V) vel[pnode].y += psign * eps;
+    boundary_resid(C, ie, hh, vel, pvar, er);
+    for (i = 0; i < 2; i++) { out[3 * i] = er[i].c; out[3 * i + 1] = er[i].x; out[3 * i + 2] = er[i].y; }
+    geo[0] = C->edjac[ie];
+    geo[1] = C->enrml[2 * ie];
+    geo[2] = C->enrml[2 * ie + 1];
+}
+
 /* element ie's area and P1 shape gradients: out = djac, gx0, gy0, gx1, gy1, gx2, gy2 */
 void orc_geometry(const orc_ctx *C, int ie, double *out) {
     int i;

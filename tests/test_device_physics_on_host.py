@@ -1,7 +1,8 @@
 """The device element physics (adhv8_kraken_b200/csrc/sw2_physics.cuh, the code every residual and
 Jacobian kernel runs) compiled as host C++ and checked element by element against the oracle:
 fully wet and wet/dry elements, unperturbed and with the Jacobian's +-eps perturbations, on a basin
-with wet/dry fronts and every optional term switched on (temporal alpha, eddy viscosity, Coriolis).
+with wet/dry fronts and every optional term switched on (temporal alpha, eddy viscosity, Coriolis);
+and the boundary-edge residual (NB VEL inflow, NB OTW tailwater, NB OF free outflow) edge by edge.
 Runs on CPU, so a change to the physics is checked on every CPU run; the GPU parity tests check
 the same code as compiled for sm_100a."""
 import ctypes as C
@@ -61,6 +62,24 @@ extern "C" void host_elem_resid(const double* xyz, const double* lv, const doubl
     double er[3][3];
     sw2_elem_resid(in, hc, uc, vc, wd, pvar, P, M, df, er);
     for (int i = 0; i < 3; i++)
+        for (int q = 0; q < 3; q++) out[3 * i + q] = er[i][q];
+}
+
+// huv: h, u, v at the edge's two nodes (2 values each); geo: djac, nx, ny; value: the string's
+// series value (unit discharge or tailwater elevation)
+extern "C" void host_edge_resid(const double* huv, const double* geo, double z0, int kind, double value, int pvar,
+                                int pnode, double dx, const double* phys, double* out) {
+    EdgeIn in;
+    for (int i = 0; i < 2; i++) { in.h[i] = huv[i]; in.u[i] = huv[2 + i]; in.v[i] = huv[4 + i]; }
+    if (pvar == kPertH) in.h[pnode] += dx;
+    else if (pvar == kPertU) in.u[pnode] += dx;
+    else if (pvar == kPertV) in.v[pnode] += dx;
+    in.djac = geo[0]; in.nx = geo[1]; in.ny = geo[2]; in.z0 = z0;
+    const PhysParams P{phys[0], phys[1], phys[2], phys[3], phys[4], phys[5]};
+    const int df[2] = {0, 0};
+    double er[2][3];
+    sw2_edge_resid(in, kind, value, pvar, P, df, er);
+    for (int i = 0; i < 2; i++)
         for (int q = 0; q < 3; q++) out[3 * i + q] = er[i][q];
 }
 """
@@ -145,4 +164,37 @@ def test_device_physics_matches_oracle_on_host(host_physics):
             err = float(np.abs(dev - ref).max() / scale)
             worst = max(worst, err)
             assert err <= 1e-12, (int(ie), pvar, b, sign, err, dev, ref)
+    assert worst <= 1e-12
+
+
+@pytest.mark.parametrize("case", ["tailwater", "outflow"])
+def test_device_edge_physics_matches_oracle_on_host(host_physics, case):
+    from adhv8_kraken_b200.model import BCT_OUTFLOW, BCT_PRS_NEU, BCT_VEL_NEU
+    m = meshgen.channel(nsteps=4) if case == "tailwater" else meshgen.channel_outflow(nsteps=4)
+    o = Oracle(m)
+    assert o.step()["status"] == 0
+    series = m.series_values(o.t, o.t + m.dt)
+    o.set_dt(m.dt, series)
+    prm = capi.make_params(m)
+    phys = np.array([prm.gravity, prm.drying_lower_limit, prm.drying_upper_limit, prm.tau_temporal, prm.tau_pg, m.dt])
+    h, u, v = o.get_state(0)
+    kinds = {BCT_VEL_NEU: 1, BCT_PRS_NEU: 2, BCT_OUTFLOW: 3}
+    worst = 0.0
+    for ie, (a, b) in enumerate(m.edges):
+        st = m.strings[int(m.edge_string[ie])]
+        value = float(series[st.isigma]) if st.isigma >= 0 else 0.0
+        huv = np.array([h[a], h[b], u[a], u[b], v[a], v[b]])
+        cases = [(-1, 0, 0.0, 0)]
+        for pvar, arr in ((1, u), (2, v), (5, h)):
+            for nd in (0, 1):
+                eps = _fd_eps(arr[(a, b)[nd]])
+                cases += [(pvar, nd, eps, 1), (pvar, nd, -eps, -1)]
+        for pvar, nd, dx, sign in cases:
+            dev, ref, geo = np.zeros(6), np.zeros(6), np.zeros(3)
+            oracle_lib().orc_edge_resid(o.h, ie, abs(dx), nd, pvar, sign, _dp(ref), _dp(geo))
+            host_physics.host_edge_resid(_dp(huv), _dp(geo), C.c_double(m.z[a]), kinds[st.bc_flag], C.c_double(value),
+                                         pvar, nd, C.c_double(dx), _dp(phys), _dp(dev))
+            err = float(np.abs(dev - ref).max() / max(np.abs(ref).max(), 1e-300))
+            worst = max(worst, err)
+            assert err <= 1e-12, (ie, pvar, nd, sign, err, dev, ref)
     assert worst <= 1e-12
