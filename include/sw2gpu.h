@@ -181,8 +181,10 @@ int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int32_t *row_p
                               const double *val, const double *rhs, double *x, double rtol, double atol,
                               int32_t max_it, void *stream, int32_t *iterations);
 
-/* Batched ensemble: many independent contexts stepped by one persistent launch per
- * phase over a concatenated BCSR with per-instance offsets. */
+/* Batched ensemble: many independent contexts stepped together, each Newton phase one
+ * launch over all of them (element kernels: per group of up to 30 instances; the Krylov
+ * solve: one cooperative launch, each instance on its own range of CTAs); every context
+ * keeps its own data and gets bitwise the results it gets alone. */
 typedef struct sw2gpu_batch sw2gpu_batch;
 int sw2gpu_batch_create(sw2gpu_ctx **ctxs, int32_t n, void *stream, sw2gpu_batch **out);
 int sw2gpu_batch_step(sw2gpu_batch *b, const double *dt, const double *const *series, sw2gpu_stats *stats);
