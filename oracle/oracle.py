@@ -54,6 +54,7 @@ def lib():
         L.orc_get_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
         L.orc_set_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
         L.orc_geometry.argtypes = [C.c_void_p, C.c_int, c_double_p]
+        L.orc_get_dacont.argtypes = [C.c_void_p, c_double_p]
         L.orc_edge_resid.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, c_double_p, c_double_p]
         L.orc_grid_mass.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.orc_grid_mass.restype = C.c_double
@@ -154,6 +155,13 @@ class Oracle:
         out = np.zeros(9)
         lib().orc_body_resid(self.h, ie, eps, pnode, pvar, psign, _dp(out))
         return out.reshape(3, 3)
+
+    def dacont(self):
+        """elem_rhs_dacont_extra_terms as [3, T] (continuity parts of shock capturing and SUPG of
+        each element's last residual evaluation, the reference's side output for transport)."""
+        out = np.zeros(3 * self.T)
+        lib().orc_get_dacont(self.h, _dp(out))
+        return out.reshape(3, self.T)
 
     def geometry(self, ie):
         """(djac, [gx0, gy0, gx1, gy1, gx2, gy2]) of element ie."""

@@ -18,7 +18,9 @@
  *            "step" records): the reference's mass diagnostics of src/tools/tl_grid_mass.c
  *            -- the initial grid mass (tl_find_grid_mass_elem2d before the first step),
  *            the current grid mass, tl_find_grid_mass_error_elem2d and its accumulated
- *            boundary / source mass flux.
+ *            boundary / source mass flux;
+ *   "dacont" when ADH_DUMP_DACONT is set, after every accepted step (after "mass"): the
+ *            side output sw->d2->elem_rhs_dacont_extra_terms[3][nelems2d], vertex-major.
  *
  * Record layout: char tag[8]; int32 kind (0 = f64, 1 = i32); int64 count; data.
  */
@@ -41,6 +43,7 @@ static int attempts = 0;
 static int it_mark = 0;
 static double solve_seconds = 0.0;   /* fe_main wall time since the last accepted step */
 static int dump_mass = 0;            /* ADH_DUMP_MASS set */
+static int dump_dacont = 0;          /* ADH_DUMP_DACONT set */
 static int mass_ready = 0;
 static double mass0 = 0.0, mass_flux_total = 0.0;
 
@@ -58,6 +61,7 @@ static void dump_open(void) {
     const char *nl = getenv("ADH_DUMP_LOADS");
     dump_loads_left = nl ? atoi(nl) : 0;
     dump_mass = getenv("ADH_DUMP_MASS") != NULL;
+    dump_dacont = getenv("ADH_DUMP_DACONT") != NULL;
 }
 
 static void put_f64(const char *tag, const double *v, long n) {
@@ -132,6 +136,14 @@ int __wrap_fe_main(SSUPER_MODEL *sm) {
                                                   &mass_flux_total);
             m[3] = mass_flux_total;
             put_f64("mass", m, 4);
+        }
+        if (dump_dacont) {
+            int T = mod->grid->nelems2d, i, e;
+            double *d = (double *) malloc(sizeof(double) * 3 * (size_t) (T ? T : 1));
+            for (i = 0; i < 3; i++)
+                for (e = 0; e < T; e++) d[(size_t) i * T + e] = mod->sw->d2->elem_rhs_dacont_extra_terms[i][e];
+            put_f64("dacont", d, 3L * T);
+            free(d);
         }
         fflush(dump_fp);
         attempts = 0;

@@ -53,6 +53,9 @@ def parse(recs) -> Dict[str, list]:
                 steps[-1].update(mass0=float(m[0]), mass=float(m[1]), mass_error=float(m[2]),
                                  mass_flux_total=float(m[3]))
                 i += 1
+            if i < len(recs) and recs[i][0] == "dacont":   # elem_rhs_dacont_extra_terms [3][T]
+                steps[-1]["dacont"] = recs[i][1].reshape(3, -1)
+                i += 1
         elif tag == "load":
             d = dict(t=arr[0], dt=arr[1])
             j = i + 1
@@ -67,9 +70,10 @@ def parse(recs) -> Dict[str, list]:
 
 
 def run_reference(model, nsteps=None, loads: int = 0, workdir: str = None, timeout: float = 3600.0,
-                  mass: bool = False):
+                  mass: bool = False, dacont: bool = False):
     """Run the reference on ``model``; returns parsed records and the wall time (s).  mass: also
-    record the reference's grid mass diagnostics after every step."""
+    record the reference's grid mass diagnostics after every step; dacont: its transport side
+    output elem_rhs_dacont_extra_terms."""
     if not os.path.exists(EXE):
         raise FileNotFoundError("oracle/_ref/adh_dump is not built (python oracle/ref/build_ref.py)")
     tmp = workdir or tempfile.mkdtemp(prefix="adhref_")
@@ -78,6 +82,8 @@ def run_reference(model, nsteps=None, loads: int = 0, workdir: str = None, timeo
         env = dict(os.environ, ADH_DUMP=os.path.join(tmp, "dump.bin"), ADH_DUMP_LOADS=str(loads))
         if mass:
             env["ADH_DUMP_MASS"] = "1"
+        if dacont:
+            env["ADH_DUMP_DACONT"] = "1"
         t0 = time.perf_counter()
         r = subprocess.run([EXE, "m"], cwd=tmp, env=env, capture_output=True, text=True, timeout=timeout)
         wall = time.perf_counter() - t0

@@ -65,6 +65,7 @@ typedef struct orc_ctx {
     /* state: level 0 current, 1 old, 2 older */
     double *h[3], *u[3], *v[3];
     int *wd;
+    double *dacont;            /* [3T] elem_rhs_dacont_extra_terms of the last body_resid call per element */
     double dt;
     double *series;
     /* BCSR pattern (sorted columns, diagonal included) */
@@ -441,6 +442,10 @@ static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof
 
     for (i = 0; i < 3; i++) { er[i].c = 0; er[i].x = 0; er[i].y = 0; }
     dof3 rhs[3];
+    /* the continuity parts of shock capturing and SUPG are kept for transport, as the reference's
+     * side output elem_rhs_dacont_extra_terms (:353-355, :400, :1214), by every call */
+    double *dac = C->dacont + 3 * ie;
+    for (i = 0; i < 3; i++) dac[i] = 0.;
 
     /* shock capturing :357-400 */
     if (wd == 1 || wd == 2) {
@@ -456,7 +461,10 @@ static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof
             rhs[i].x = cu * dt * djac * nx * (un.x * g[i].x + un.y * g[i].y);
             rhs[i].y = cv * dt * djac * ny * (vn.x * g[i].x + vn.y * g[i].y);
         }
-        for (i = 0; i < 3; i++) { er[i].c += rhs[i].c; er[i].x += rhs[i].x; er[i].y += rhs[i].y; }
+        for (i = 0; i < 3; i++) {
+            dac[i] += rhs[i].c;
+            er[i].c += rhs[i].c; er[i].x += rhs[i].x; er[i].y += rhs[i].y;
+        }
     }
 
     /* advection :434-457 */
@@ -560,6 +568,7 @@ static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof
             double rc = g[i].x * (tau * vwd.x * c_eq + tau * h_wd * x_eq) + g[i].y * (tau * vwd.y * c_eq + tau * h_wd * y_eq);
             double rx = g[i].x * (tau * gf * h_wd * c_eq + tau * vwd.x * h_wd * x_eq) + g[i].y * (tau * vwd.y * h_wd * x_eq);
             double ry = g[i].y * (tau * gf * h_wd * c_eq + tau * vwd.y * h_wd * y_eq) + g[i].x * (tau * vwd.x * h_wd * y_eq);
+            dac[i] += rc;
             er[i].c += rc; er[i].x += rx; er[i].y += ry;
         }
     }
@@ -780,6 +789,7 @@ orc_ctx *orc_create(const sw2gpu_mesh *m, const sw2gpu_params *p, int nblock) {
         C->v[k] = (double *) calloc(C->V, sizeof(double));
     }
     C->wd = (int *) calloc(C->T ? C->T : 1, sizeof(int));
+    C->dacont = (double *) calloc(3 * (size_t) (C->T ? C->T : 1), sizeof(double));
     C->resid = (double *) calloc(3 * C->V, sizeof(double));
     C->sol = (double *) calloc(3 * C->V, sizeof(double));
     C->include = (int *) calloc(C->V, sizeof(int));
@@ -826,7 +836,7 @@ void orc_destroy(orc_ctx *C) {
     free(C->str_ivx); free(C->str_ivy); free(C->str_iu0); free(C->str_rough); free(C->mat_eev_mode);
     free(C->mat_ev); free(C->mat_eev_coef); free(C->mat_cor); free(C->series);
     for (k = 0; k < 3; k++) { free(C->h[k]); free(C->u[k]); free(C->v[k]); }
-    free(C->wd); free(C->resid); free(C->sol); free(C->include); free(C->djac); free(C->grad);
+    free(C->wd); free(C->dacont); free(C->resid); free(C->sol); free(C->include); free(C->djac); free(C->grad);
     free(C->edjac); free(C->enrml); free(C->rowptr); free(C->col); free(C->blk_of_pair); free(C->eblk_of_pair);
     free(C->val); free(C->perm); free(C->iperm);
     free(C);
@@ -854,6 +864,12 @@ void orc_set_dt(orc_ctx *C, double dt, const double *series) {
     if (C->NS > 0 && series) memcpy(C->series, series, sizeof(double) * C->NS);
 }
 void orc_get_wd(const orc_ctx *C, int *wd) { memcpy(wd, C->wd, sizeof(int) * C->T); }
+/* elem_rhs_dacont_extra_terms, vertex-major like the reference's [3][T] array: out[i T + e] */
+void orc_get_dacont(const orc_ctx *C, double *out) {
+    int e, i;
+    for (i = 0; i < 3; i++)
+        for (e = 0; e < C->T; e++) out[(size_t) i * C->T + e] = C->dacont[3 * e + i];
+}
 void orc_set_wd(orc_ctx *C, const int *wd) { memcpy(C->wd, wd, sizeof(int) * C->T); }
 
 /* fe_sw2_wdflag (src/fe/sw2/fe_sw2_wdflag.c:24-75) */

@@ -19,6 +19,9 @@ Fixtures (numpy ``.npz``):
   residual / Jacobian.
 * ``outflow_ref.npz`` -- the channel with a free outflow edge (NB OF) east, 6 steps, recorded
   like ``ovh_ref.npz``.
+* ``dacont_ref.npz`` -- the reference's transport side output elem_rhs_dacont_extra_terms
+  (continuity parts of shock capturing and SUPG per element vertex) after steps 1, 4 and 8 of
+  the basin run.
 * ``mass_ref.npz`` -- the reference's grid mass diagnostics (src/tools/tl_grid_mass.c) after
   every step of 6 channel steps and of the 8 basin steps: initial and current mass, mass error
   and accumulated mass flux, with the channel's state after every step (the basin's states are
@@ -138,6 +141,15 @@ def ovh(m=None, fname="ovh_ref.npz"):
     np.savez_compressed(os.path.join(HERE, fname), **out)
 
 
+def dacont():
+    m = basin_model()
+    ref = run_reference(m, nsteps=8, dacont=True)
+    out = {"fingerprint": np.array(fingerprint(m))}
+    for k in (1, 4, 8):
+        out[f"step{k}_dacont"] = ref["steps"][k - 1]["dacont"]
+    np.savez_compressed(os.path.join(HERE, "dacont_ref.npz"), **out)
+
+
 def mass():
     out = {}
     for name, m, n in (("channel", meshgen.channel(nsteps=6), 6), ("basin", basin_model(), 8)):
@@ -154,7 +166,7 @@ def mass():
 
 if __name__ == "__main__":
     import sys as _sys
-    which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "mass"]
+    which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "dacont", "mass"]
     if "channel" in which:
         channel()
     if "basin" in which:
@@ -163,7 +175,9 @@ if __name__ == "__main__":
         ovh()
     if "outflow" in which:
         ovh(meshgen.channel_outflow(nsteps=6), "outflow_ref.npz")
+    if "dacont" in which:
+        dacont()
     if "mass" in which:
         mass()
-    for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "mass_ref.npz"):
+    for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "dacont_ref.npz", "mass_ref.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))

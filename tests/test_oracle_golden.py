@@ -121,3 +121,19 @@ def test_oracle_boundary_variants_match_reference(case):
         exp = fields(ovh_ref[f"step{k+1}_h"], ovh_ref[f"step{k+1}_u"], ovh_ref[f"step{k+1}_v"])
         for f, e in field_errors(got, exp).items():
             assert e <= 1e-10, (k, f, e)
+
+
+def test_oracle_transport_side_output_matches_reference(basin_ref):
+    """elem_rhs_dacont_extra_terms (fe_sw2_body_resid.c:353-355, :400, :1214: the continuity
+    parts of shock capturing and SUPG kept per element vertex for transport) after steps of the
+    wet/dry basin, against the reference's own array."""
+    import os
+    from conftest import GOLDEN
+    ref = dict(np.load(os.path.join(GOLDEN, "dacont_ref.npz")))
+    m = basin_model()
+    assert str(ref["fingerprint"]) == fingerprint(m)
+    o = Oracle(m)
+    for k in range(8):
+        assert o.step(dt=basin_ref["dt"][k], t=basin_ref["t"][k])["status"] == 0
+        if k + 1 in (1, 4, 8):
+            assert relerr(o.dacont(), ref[f"step{k+1}_dacont"]) <= 1e-10, k
