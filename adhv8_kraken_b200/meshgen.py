@@ -18,6 +18,7 @@ GPU and the block solver of the reference CPU path both see local data.
 """
 from __future__ import annotations
 
+import dataclasses
 import math
 
 import numpy as np
@@ -81,6 +82,18 @@ def channel(nx: int = 100, ny: int = 20, length: float = 1000.0, width: float = 
                     materials=[Material(evs=(0.0, 0.0, 0.0))], series=series,
                     params=Params(tol_nonlin=tol_nonlin), h0=np.full(V, h0), u0=np.zeros(V),
                     v0=np.zeros(V), dt=dt, nsteps=nsteps, name=name)
+
+
+def basin_all_terms(nsteps: int = 6) -> SW2Model:
+    """A small wet/dry basin with every optional body term on: temporal weight alpha = 0.5
+    (OP TEM), and per material EVS eddy viscosity with Coriolis, EEV modes 1 and 2, and EEV
+    mode 3 with Coriolis."""
+    from .model import Material
+    m = bumpy_basin(700, seed=11, size=2000.0, nsteps=nsteps, dt=5.0, nbins=4, name="terms")
+    m.params = dataclasses.replace(m.params, tau_temporal=0.5)
+    m.materials = [Material(evs=(6.0, 2.0, 1.0), coriolis=30.0), Material(eev_coef=0.4, eev_mode=1),
+                   Material(eev_coef=0.4, eev_mode=2), Material(eev_coef=0.4, eev_mode=3, coriolis=-20.0)]
+    return m
 
 
 def channel_ovh(nsteps: int = 6, u_in: float = 0.5, **kw) -> SW2Model:

@@ -19,6 +19,8 @@ Fixtures (numpy ``.npz``):
   residual / Jacobian.
 * ``outflow_ref.npz`` -- the channel with a free outflow edge (NB OF) east, 6 steps, recorded
   like ``ovh_ref.npz``.
+* ``terms_ref.npz`` -- a wet/dry basin with every optional body term on (temporal alpha, EVS
+  and EEV modes 1-3 eddy viscosity, Coriolis), 6 steps, recorded like ``ovh_ref.npz``.
 * ``dacont_ref.npz`` -- the reference's transport side output elem_rhs_dacont_extra_terms
   (continuity parts of shock capturing and SUPG per element vertex) after steps 1, 4 and 8 of
   the basin run.
@@ -166,7 +168,7 @@ def mass():
 
 if __name__ == "__main__":
     import sys as _sys
-    which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "dacont", "mass"]
+    which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "terms", "dacont", "mass"]
     if "channel" in which:
         channel()
     if "basin" in which:
@@ -175,9 +177,12 @@ if __name__ == "__main__":
         ovh()
     if "outflow" in which:
         ovh(meshgen.channel_outflow(nsteps=6), "outflow_ref.npz")
+    if "terms" in which:
+        ovh(meshgen.basin_all_terms(nsteps=6), "terms_ref.npz")
     if "dacont" in which:
         dacont()
     if "mass" in which:
         mass()
-    for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "dacont_ref.npz", "mass_ref.npz"):
+    for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "terms_ref.npz", "dacont_ref.npz",
+              "mass_ref.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))

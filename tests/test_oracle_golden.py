@@ -96,16 +96,18 @@ def test_oracle_grid_mass_matches_reference(case, mass_ref, basin_ref):
         assert abs(err - mass_ref[f"{case}_mass_error"][k - 1]) <= 1e-13 * mass0, k
 
 
-@pytest.mark.parametrize("case", ["ovh", "outflow"])
+@pytest.mark.parametrize("case", ["ovh", "outflow", "terms"])
 def test_oracle_boundary_variants_match_reference(case):
-    """NB OVH inflow (elevation + velocity, fe_sw2_boundary_resid.c:398-440 with fe_sw2_1d_hvel)
-    and a free NB OF outflow edge (:227-240, fe_sw2_1d_implicit_flow): residual and FD Jacobian
-    at the first load, then 6 steps."""
+    """NB OVH inflow (elevation + velocity, fe_sw2_boundary_resid.c:398-440 with fe_sw2_1d_hvel),
+    a free NB OF outflow edge (:227-240, fe_sw2_1d_implicit_flow) and a wet/dry basin with every
+    optional body term (temporal alpha, EVS / EEV 1-3 eddy viscosity, Coriolis): residual and FD
+    Jacobian at the first load, then 6 steps."""
     import os
     from adhv8_kraken_b200 import meshgen
     from conftest import GOLDEN
     ovh_ref = dict(np.load(os.path.join(GOLDEN, f"{case}_ref.npz")))
-    m = meshgen.channel_ovh(nsteps=6) if case == "ovh" else meshgen.channel_outflow(nsteps=6)
+    m = {"ovh": meshgen.channel_ovh, "outflow": meshgen.channel_outflow,
+         "terms": meshgen.basin_all_terms}[case](nsteps=6)
     assert str(ovh_ref["fingerprint"]) == fingerprint(m)
     o = Oracle(m)
     set_load_state(o, m, ovh_ref)
