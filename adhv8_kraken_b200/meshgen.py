@@ -96,6 +96,18 @@ def basin_all_terms(nsteps: int = 6) -> SW2Model:
     return m
 
 
+def basin_rain(nsteps: int = 6, rate: float = 2e-4) -> SW2Model:
+    """The small wet/dry basin with a water source (NB SOURCE, `rate` m/s of rain) on its first
+    material string."""
+    from .model import BCT_WATER_SOURCE
+    m = bumpy_basin(700, seed=11, size=2000.0, nsteps=nsteps, dt=5.0, nbins=3, name="rain")
+    t_end = (nsteps + 10) * m.dt
+    m.series = list(m.series) + [Series(np.array([0.0, t_end]), np.array([rate, rate]))]
+    m.strings = list(m.strings)
+    m.strings[0] = dataclasses.replace(m.strings[0], bc_flag=BCT_WATER_SOURCE, isigma=len(m.series) - 1)
+    return m
+
+
 def channel_ovh(nsteps: int = 6, u_in: float = 0.5, **kw) -> SW2Model:
     """The channel with its inflow given as NB OVH instead of NB VEL: water elevation 1 m above
     the datum (the west bed) and velocity (u_in, 0) on the west edge; NB OTW tailwater east."""

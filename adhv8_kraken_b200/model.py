@@ -234,6 +234,8 @@ class SW2Model:
             w(f"SERIES AWRITE {nser + 2} 1 0 0 0 0\n{_f(self.t0)} {_f(tf)} {_f(self.dt)} 0\n")
             w(f"TC T0 {_f(self.t0)} 0\nTC TF {_f(tf)} 0\n")
             for s_id, s in enumerate(self.strings):
+                if s.kind == "mat" and s.bc_flag == BCT_WATER_SOURCE:   # read_bc_NB.c:83-88
+                    w(f"NB SOURCE {s_id + 1} {s.isigma + 1}\n")
                 if s.kind == "edge":
                     if s.bc_flag == BCT_VEL_NEU:
                         w(f"NB VEL {s_id + 1} {s.isigma + 1}\n")

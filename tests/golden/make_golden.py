@@ -21,6 +21,8 @@ Fixtures (numpy ``.npz``):
   like ``ovh_ref.npz``.
 * ``terms_ref.npz`` -- a wet/dry basin with every optional body term on (temporal alpha, EVS
   and EEV modes 1-3 eddy viscosity, Coriolis), 6 steps, recorded like ``ovh_ref.npz``.
+* ``rain_ref.npz`` -- the basin with a water source (NB SOURCE) on one material string, 6 steps,
+  recorded like ``ovh_ref.npz`` plus the grid mass diagnostics after every step.
 * ``dacont_ref.npz`` -- the reference's transport side output elem_rhs_dacont_extra_terms
   (continuity parts of shock capturing and SUPG per element vertex) after steps 1, 4 and 8 of
   the basin run.
@@ -131,15 +133,18 @@ def basin():
     np.savez_compressed(os.path.join(HERE, "basin_ref.npz"), **out)
 
 
-def ovh(m=None, fname="ovh_ref.npz"):
+def ovh(m=None, fname="ovh_ref.npz", mass=False):
     m = meshgen.channel_ovh(nsteps=6) if m is None else m
-    ref = run_reference(m, nsteps=6, loads=1)
+    ref = run_reference(m, nsteps=6, loads=1, mass=mass)
     out = {"fingerprint": np.array(fingerprint(m)),
            "newton_its": np.array([s["newton_its"] for s in ref["steps"]], np.int32),
            "t": np.array([s["t"] for s in ref["steps"]]), "dt": np.array([s["dt"] for s in ref["steps"]])}
     for k, s in enumerate(ref["steps"], 1):
         out[f"step{k}_h"], out[f"step{k}_u"], out[f"step{k}_v"] = s["h"], s["u"], s["v"]
     out.update(load_record(m, ref["loads"][0], "load0"))
+    if mass:
+        for key in ("mass0", "mass", "mass_error", "mass_flux_total"):
+            out[key] = np.array([s[key] for s in ref["steps"]])
     np.savez_compressed(os.path.join(HERE, fname), **out)
 
 
@@ -168,7 +173,7 @@ def mass():
 
 if __name__ == "__main__":
     import sys as _sys
-    which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "terms", "dacont", "mass"]
+    which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "terms", "rain", "dacont", "mass"]
     if "channel" in which:
         channel()
     if "basin" in which:
@@ -179,10 +184,12 @@ if __name__ == "__main__":
         ovh(meshgen.channel_outflow(nsteps=6), "outflow_ref.npz")
     if "terms" in which:
         ovh(meshgen.basin_all_terms(nsteps=6), "terms_ref.npz")
+    if "rain" in which:
+        ovh(meshgen.basin_rain(nsteps=6), "rain_ref.npz", mass=True)
     if "dacont" in which:
         dacont()
     if "mass" in which:
         mass()
-    for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "terms_ref.npz", "dacont_ref.npz",
-              "mass_ref.npz"):
+    for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "terms_ref.npz", "rain_ref.npz",
+              "dacont_ref.npz", "mass_ref.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from adhv8_kraken_b200 import capi, meshgen
-from adhv8_kraken_b200.model import Material
+from adhv8_kraken_b200.model import BCT_WATER_SOURCE, Material
 from oracle.oracle import Oracle
 from oracle.oracle import lib as oracle_lib
 
@@ -116,15 +116,20 @@ def _fd_eps(x):   # NUM_DIFF_EPSILON (src/include/macro.h:669-673)
     return p if e < p else e
 
 
-def test_device_physics_matches_oracle_on_host(host_physics):
-    base = meshgen.bumpy_basin(900, seed=5, size=2500.0, nsteps=4, dt=5.0, nbins=3, name="physics")
-    m = dataclasses.replace(
-        base, params=dataclasses.replace(base.params, tau_temporal=0.5),
-        materials=[Material(evs=(6.0, 2.0, 1.0), coriolis=30.0)] + [Material(eev_coef=0.4, eev_mode=k) for k in (1, 2)])
+@pytest.mark.parametrize("case", ["all_terms", "rain"])
+def test_device_physics_matches_oracle_on_host(host_physics, case):
+    if case == "rain":
+        m = meshgen.basin_rain(nsteps=4)
+    else:
+        base = meshgen.bumpy_basin(900, seed=5, size=2500.0, nsteps=4, dt=5.0, nbins=3, name="physics")
+        m = dataclasses.replace(
+            base, params=dataclasses.replace(base.params, tau_temporal=0.5),
+            materials=[Material(evs=(6.0, 2.0, 1.0), coriolis=30.0)] + [Material(eev_coef=0.4, eev_mode=k) for k in (1, 2)])
     o = Oracle(m)
     for _ in range(2):   # distinct time levels and moving wet/dry fronts
         assert o.step()["status"] == 0
-    o.set_dt(m.dt, m.series_values(o.t, o.t + m.dt))
+    series = m.series_values(o.t, o.t + m.dt)
+    o.set_dt(m.dt, series)
     o.wdflag()
     wd = o.get_wd()
     arrays = capi.MeshArrays(m)
@@ -148,8 +153,11 @@ def test_device_physics_matches_oracle_on_host(host_physics):
         k = int(m.tri_mat[ie])
         mt = m.materials[k]
         xx, yy = mt.evs[0] + prm.viscosity, mt.evs[1] + prm.viscosity
+        st = m.strings[k]   # material k's string
+        source = st.bc_flag == BCT_WATER_SOURCE
         mat = np.array([ks[k], abs(xx - yy), min(xx, yy), mt.eev_coef,
-                        math.sin(math.pi / 180.0 * mt.coriolis) * 2.0 * 7.2722e-5, 0.0])
+                        math.sin(math.pi / 180.0 * mt.coriolis) * 2.0 * 7.2722e-5,
+                        float(series[st.isigma]) if source else 0.0])
         cases = [(-1, 0, 0.0, 0)]
         for pvar, arr in ((1, levels[0][1]), (2, levels[0][2]), (5, levels[0][0])):
             b = int(rng.integers(0, 3))
@@ -158,7 +166,7 @@ def test_device_physics_matches_oracle_on_host(host_physics):
         for pvar, b, dx, sign in cases:
             dev, ref = np.zeros(9), np.zeros(9)
             host_physics.host_elem_resid(_dp(xyz), _dp(lv), _dp(geo), int(wd[ie]), pvar, b, C.c_double(dx), _dp(phys),
-                                         _dp(mat), mt.eev_mode, 0, _dp(dev))
+                                         _dp(mat), mt.eev_mode, int(source), _dp(dev))
             oracle_lib().orc_body_resid(o.h, int(ie), abs(dx), b, pvar, sign, _dp(ref))
             scale = max(np.abs(ref).max(), 1e-300)
             err = float(np.abs(dev - ref).max() / scale)

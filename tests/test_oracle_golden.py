@@ -96,18 +96,19 @@ def test_oracle_grid_mass_matches_reference(case, mass_ref, basin_ref):
         assert abs(err - mass_ref[f"{case}_mass_error"][k - 1]) <= 1e-13 * mass0, k
 
 
-@pytest.mark.parametrize("case", ["ovh", "outflow", "terms"])
+@pytest.mark.parametrize("case", ["ovh", "outflow", "terms", "rain"])
 def test_oracle_boundary_variants_match_reference(case):
     """NB OVH inflow (elevation + velocity, fe_sw2_boundary_resid.c:398-440 with fe_sw2_1d_hvel),
-    a free NB OF outflow edge (:227-240, fe_sw2_1d_implicit_flow) and a wet/dry basin with every
-    optional body term (temporal alpha, EVS / EEV 1-3 eddy viscosity, Coriolis): residual and FD
-    Jacobian at the first load, then 6 steps."""
+    a free NB OF outflow edge (:227-240, fe_sw2_1d_implicit_flow), a wet/dry basin with every
+    optional body term (temporal alpha, EVS / EEV 1-3 eddy viscosity, Coriolis) and one with a
+    water source (NB SOURCE, fe_sw2_body_resid.c:728-754): residual and FD Jacobian at the first
+    load, then 6 steps (for the source, also the grid mass and the accumulated mass flux)."""
     import os
     from adhv8_kraken_b200 import meshgen
     from conftest import GOLDEN
     ovh_ref = dict(np.load(os.path.join(GOLDEN, f"{case}_ref.npz")))
     m = {"ovh": meshgen.channel_ovh, "outflow": meshgen.channel_outflow,
-         "terms": meshgen.basin_all_terms}[case](nsteps=6)
+         "terms": meshgen.basin_all_terms, "rain": meshgen.basin_rain}[case](nsteps=6)
     assert str(ovh_ref["fingerprint"]) == fingerprint(m)
     o = Oracle(m)
     set_load_state(o, m, ovh_ref)
@@ -116,13 +117,19 @@ def test_oracle_boundary_variants_match_reference(case):
     assert relerr(r, ovh_ref["load0_resid"]) <= 1e-13
     assert relerr(val, ovh_ref["load0_val"]) <= 1e-7
     o = Oracle(m)
+    mass0, acc = o.grid_mass(0), 0.0
     for k in range(6):
-        st = o.step(dt=ovh_ref["dt"][k], t=ovh_ref["t"][k])
+        t, dt = ovh_ref["t"][k], ovh_ref["dt"][k]
+        st = o.step(dt=dt, t=t)
         assert st["status"] == 0 and st["newton_its"] == ovh_ref["newton_its"][k]
         got = fields(*o.get_state(0))
         exp = fields(ovh_ref[f"step{k+1}_h"], ovh_ref[f"step{k+1}_u"], ovh_ref[f"step{k+1}_v"])
         for f, e in field_errors(got, exp).items():
             assert e <= 1e-10, (k, f, e)
+        if "mass" in ovh_ref:   # sources count in the mass flux at the step's series values
+            acc += o.mass_flux(dt, m.series_values(t, t + dt))
+            assert relerr(o.grid_mass(0), ovh_ref["mass"][k]) <= 1e-12, k
+            assert abs(acc - ovh_ref["mass_flux_total"][k]) <= 1e-12 * mass0, k
 
 
 def test_oracle_transport_side_output_matches_reference(basin_ref):
