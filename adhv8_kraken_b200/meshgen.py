@@ -108,6 +108,28 @@ def basin_rain(nsteps: int = 6, rate: float = 2e-4) -> SW2Model:
     return m
 
 
+def channel_obstacle(nsteps: int = 6, with_depth: bool = False) -> SW2Model:
+    """The channel with a short line of interior nodes across mid-channel held at zero velocity
+    (DB OVL), or at zero velocity and 1 m depth (DB OVH, `with_depth`): a small obstacle in the
+    flow.  The reference itself ends with a segmentation fault on the DB OVL form (its edge
+    elements generated for DB OVL assume the string lies on the domain boundary)."""
+    from .model import BCT_VEL_DIR, BCT_VEL_PRS_DIR
+    m = channel(nsteps=nsteps)
+    t_end = (nsteps + 10) * m.dt
+    ns = len(m.series)
+    m.series = list(m.series) + [Series(np.array([0.0, t_end]), np.array([0.0, 0.0])),
+                                 Series(np.array([0.0, t_end]), np.array([0.0, 0.0])),
+                                 Series(np.array([0.0, t_end]), np.array([1.0, 1.0]))]
+    m.strings = list(m.strings) + [StringSpec("node", bc_flag=BCT_VEL_PRS_DIR if with_depth else BCT_VEL_DIR,
+                                              ivx=ns, ivy=ns + 1, iu0=ns + 2)]
+    pick = (np.abs(m.x - 500.0) < 1.0) & (m.y > 60.0) & (m.y < 140.0)   # a short line across mid-channel
+    ns_arr = m.node_string.copy()
+    ns_arr[pick] = len(m.strings) - 1
+    m.node_string = ns_arr
+    m.name = "channel_obstacle"
+    return m
+
+
 def channel_ovh(nsteps: int = 6, u_in: float = 0.5, **kw) -> SW2Model:
     """The channel with its inflow given as NB OVH instead of NB VEL: water elevation 1 m above
     the datum (the west bed) and velocity (u_in, 0) on the west edge; NB OTW tailwater east."""

@@ -236,6 +236,12 @@ class SW2Model:
             for s_id, s in enumerate(self.strings):
                 if s.kind == "mat" and s.bc_flag == BCT_WATER_SOURCE:   # read_bc_NB.c:83-88
                     w(f"NB SOURCE {s_id + 1} {s.isigma + 1}\n")
+                # DB OVL: the reference then adds edge elements of its own along the string
+                # (BCT_DB_VEL, src/tools/create_dbovl_elem1d.c) that this model does not carry
+                if s.kind == "node" and s.bc_flag == BCT_VEL_DIR:        # read_bc_DB.c:41-48
+                    w(f"DB OVL {s_id + 1} {s.ivx + 1} {s.ivy + 1}\n")
+                elif s.kind == "node" and s.bc_flag == BCT_VEL_PRS_DIR:  # read_bc_DB.c:49-58
+                    w(f"DB OVH {s_id + 1} {s.ivx + 1} {s.ivy + 1} {s.iu0 + 1}\n")
                 if s.kind == "edge":
                     if s.bc_flag == BCT_VEL_NEU:
                         w(f"NB VEL {s_id + 1} {s.isigma + 1}\n")

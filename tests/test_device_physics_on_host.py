@@ -1,8 +1,9 @@
 """The device element physics (adhv8_kraken_b200/csrc/sw2_physics.cuh, the code every residual and
 Jacobian kernel runs) compiled as host C++ and checked element by element against the oracle:
 fully wet and wet/dry elements, unperturbed and with the Jacobian's +-eps perturbations, on a basin
-with wet/dry fronts and every optional term switched on (temporal alpha, eddy viscosity, Coriolis);
-and the boundary-edge residual (NB VEL inflow, NB OTW tailwater, NB OF free outflow) edge by edge.
+with wet/dry fronts and every optional term switched on (temporal alpha, eddy viscosity, Coriolis),
+on one with a water source, and on elements holding Dirichlet nodes (DB OVH); and the boundary-edge
+residual (NB VEL inflow, NB OTW tailwater, NB OF free outflow) edge by edge.
 Runs on CPU, so a change to the physics is checked on every CPU run; the GPU parity tests check
 the same code as compiled for sm_100a."""
 import ctypes as C
@@ -16,7 +17,7 @@ import numpy as np
 import pytest
 
 from adhv8_kraken_b200 import capi, meshgen
-from adhv8_kraken_b200.model import BCT_WATER_SOURCE, Material
+from adhv8_kraken_b200.model import BCT_PRS_DIR, BCT_VEL_DIR, BCT_VEL_PRS_DIR, BCT_WATER_SOURCE, Material
 from oracle.oracle import Oracle
 from oracle.oracle import lib as oracle_lib
 
@@ -36,10 +37,10 @@ using namespace sw2;
 
 // xyz: x[3], y[3], z[3]; lv: h, u, v at the current, old and older levels (3 values each);
 // geo: djac, gx0, gy0, gx1, gy1, gx2, gy2; phys: g, dll, dul, alpha, tau_pg, dt;
-// mat: ks, ev_st, ev_tr, eev_coef, cor_speed, water_src
+// mat: ks, ev_st, ev_tr, eev_coef, cor_speed, water_src; dflag: the vertices' Dirichlet flags
 extern "C" void host_elem_resid(const double* xyz, const double* lv, const double* geo, int wd, int pvar, int pnode,
                                 double dx, const double* phys, const double* mat, int eev_mode, int has_source,
-                                double* out) {
+                                const int* dflag, double* out) {
     ElemIn in;
     for (int i = 0; i < 3; i++) {
         in.x[i] = xyz[i]; in.y[i] = xyz[3 + i]; in.z[i] = xyz[6 + i];
@@ -58,9 +59,8 @@ extern "C" void host_elem_resid(const double* xyz, const double* lv, const doubl
     MatParams M{};
     M.ks = mat[0]; M.ev_st = mat[1]; M.ev_tr = mat[2]; M.eev_coef = mat[3]; M.cor_speed = mat[4];
     M.water_src = mat[5]; M.eev_mode = eev_mode; M.has_source = has_source;
-    const int df[3] = {0, 0, 0};
     double er[3][3];
-    sw2_elem_resid(in, hc, uc, vc, wd, pvar, P, M, df, er);
+    sw2_elem_resid(in, hc, uc, vc, wd, pvar, P, M, dflag, er);
     for (int i = 0; i < 3; i++)
         for (int q = 0; q < 3; q++) out[3 * i + q] = er[i][q];
 }
@@ -116,10 +116,19 @@ def _fd_eps(x):   # NUM_DIFF_EPSILON (src/include/macro.h:669-673)
     return p if e < p else e
 
 
-@pytest.mark.parametrize("case", ["all_terms", "rain"])
+def _dirichlet_flags(m):
+    """Per node: the device's Dirichlet flag (bit0 PRS_DIR, bit1 VEL_DIR, bit2 VEL_PRS_DIR)."""
+    code = {BCT_PRS_DIR: 1, BCT_VEL_DIR: 2, BCT_VEL_PRS_DIR: 4}
+    per_string = np.array([code.get(s.bc_flag, 0) if s.kind == "node" else 0 for s in m.strings] + [0], np.int32)
+    return per_string[np.where(m.node_string >= 0, m.node_string, len(m.strings))]
+
+
+@pytest.mark.parametrize("case", ["all_terms", "rain", "obstacle"])
 def test_device_physics_matches_oracle_on_host(host_physics, case):
     if case == "rain":
         m = meshgen.basin_rain(nsteps=4)
+    elif case == "obstacle":
+        m = meshgen.channel_obstacle(nsteps=4, with_depth=True)
     else:
         base = meshgen.bumpy_basin(900, seed=5, size=2500.0, nsteps=4, dt=5.0, nbins=3, name="physics")
         m = dataclasses.replace(
@@ -140,7 +149,11 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
     rng = np.random.Generator(np.random.PCG64(3))
     h0 = levels[0][0]
     tri = m.tri
-    fringe = np.nonzero((wd != 0) | (h0[tri] <= 0.0).any(axis=1))[0]
+    dflag = _dirichlet_flags(m)
+    if case == "obstacle":   # every element holding a Dirichlet node
+        fringe = np.nonzero((dflag[tri] != 0).any(axis=1))[0]
+    else:                    # wet/dry fronts
+        fringe = np.nonzero((wd != 0) | (h0[tri] <= 0.0).any(axis=1))[0]
     picks = np.concatenate([fringe[:150], rng.choice(m.nelems2d, 150, replace=False)])
     assert fringe.size > 0
     worst = 0.0
@@ -158,6 +171,7 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
         mat = np.array([ks[k], abs(xx - yy), min(xx, yy), mt.eev_coef,
                         math.sin(math.pi / 180.0 * mt.coriolis) * 2.0 * 7.2722e-5,
                         float(series[st.isigma]) if source else 0.0])
+        df = np.ascontiguousarray(dflag[nodes], np.int32)
         cases = [(-1, 0, 0.0, 0)]
         for pvar, arr in ((1, levels[0][1]), (2, levels[0][2]), (5, levels[0][0])):
             b = int(rng.integers(0, 3))
@@ -166,7 +180,8 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
         for pvar, b, dx, sign in cases:
             dev, ref = np.zeros(9), np.zeros(9)
             host_physics.host_elem_resid(_dp(xyz), _dp(lv), _dp(geo), int(wd[ie]), pvar, b, C.c_double(dx), _dp(phys),
-                                         _dp(mat), mt.eev_mode, int(source), _dp(dev))
+                                         _dp(mat), mt.eev_mode, int(source),
+                                         df.ctypes.data_as(C.POINTER(C.c_int)), _dp(dev))
             oracle_lib().orc_body_resid(o.h, int(ie), abs(dx), b, pvar, sign, _dp(ref))
             scale = max(np.abs(ref).max(), 1e-300)
             err = float(np.abs(dev - ref).max() / scale)

@@ -107,3 +107,29 @@ def test_reruns_are_bitwise_identical():
             assert g.step()["status"] == 0
         outs.append(np.concatenate(g.get_state(0)))
     assert np.array_equal(outs[0], outs[1])
+
+
+VARIANTS = {"outflow": meshgen.channel_outflow, "terms": meshgen.basin_all_terms, "rain": meshgen.basin_rain,
+            "obstacle": lambda nsteps: meshgen.channel_obstacle(nsteps=nsteps, with_depth=True)}
+
+
+@pytest.mark.parametrize("case", sorted(VARIANTS))
+def test_boundary_and_term_variants_match_reference(case):
+    """The reference fixtures of a free outflow edge (NB OF), a wet/dry basin with every optional
+    body term (temporal alpha, EVS / EEV 1-3 eddy viscosity, Coriolis), a water source (NB SOURCE)
+    and interior nodes held by a DB OVH string: residual and Jacobian at the first load, then 6
+    steps, each state within 1e-10 and Newton iterations within +-1."""
+    import os
+    from conftest import GOLDEN
+    from golden.make_golden import fingerprint
+    ref = dict(np.load(os.path.join(GOLDEN, f"{case}_ref.npz")))
+    model = VARIANTS[case](nsteps=6)
+    assert str(ref["fingerprint"]) == fingerprint(model)
+    g = SW2GPU(model)
+    set_load_state(g, model, ref)
+    g.resid()
+    rp, col, val, r = g.load()
+    assert np.array_equal(rp, ref["load0_rowptr"]) and np.array_equal(col, ref["load0_col"])
+    assert relerr(r, ref["load0_resid"]) <= 1e-12
+    assert relerr(val, ref["load0_val"]) <= 1e-7
+    _run_against(model, ref, 6, range(1, 7))
