@@ -23,6 +23,7 @@ struct DevMesh {
     const double *bdjac, *bnx, *bny;
     const MatParams *mats;
     const double *str_value;          // [nstrings] step value of each edge string's series
+    const double *str_uv;             // [2 nstrings] NB OVH strings: step values of the vx, vy series
     const int *slot_ptr, *slot_idx;   // node -> residual slots in reference order
     const int *blk_ptr, *blk_src;     // BCSR block -> element-block slots in reference order
     const int *rowptr, *col, *blk_row, *dpos;
@@ -233,8 +234,12 @@ __global__ void __launch_bounds__(128, 3) k_resid_elem(const __grid_constant__ S
         in.ny = m.bny[j];
         in.djac = m.bdjac[j];
         in.z0 = m.z[b[0]];
+        in.z1 = m.z[b[1]];
+        const int kind = m.bkind[j], sid = m.bstr[j];
+        in.bvx = kind == 4 ? m.str_uv[2 * sid] : 0.0;
+        in.bvy = kind == 4 ? m.str_uv[2 * sid + 1] : 0.0;
         double er[2][3];
-        sw2_edge_resid(in, m.bkind[j], m.str_value[m.bstr[j]], kPertNone, P, df, er);
+        sw2_edge_resid(in, kind, m.str_value[sid], kPertNone, P, df, er);
 #pragma unroll
         for (int i = 0; i < 2; i++) {
             const bool dry = s.ho[b[i]] <= 0.;
@@ -586,8 +591,11 @@ __global__ void k_jac_edge(const __grid_constant__ Src src) {
     in.ny = m.bny[j];
     in.djac = m.bdjac[j];
     in.z0 = m.z[nd[0]];
-    const int kind = m.bkind[j];
-    const double value = m.str_value[m.bstr[j]];
+    in.z1 = m.z[nd[1]];
+    const int kind = m.bkind[j], sid = m.bstr[j];
+    in.bvx = kind == 4 ? m.str_uv[2 * sid] : 0.0;
+    in.bvy = kind == 4 ? m.str_uv[2 * sid + 1] : 0.0;
+    const double value = m.str_value[sid];
     double cur = 0.0;
 #pragma unroll
     for (int i = 0; i < 2; i++)

@@ -784,11 +784,13 @@ __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, const double* h
 
 // ---------------------------------------------------------------------------------
 // boundary edge residual (fe_sw2_boundary_resid, src/fe/sw2/fe_sw2_boundary_resid.c:72-510)
-// kind: 1 = BCT_VEL_NEU (value = series q), 2 = BCT_PRS_NEU (value = tailwater elevation),
-//       3 = BCT_OUTFLOW.  Returns er[node][eq] (eq 0 = c, 1 = x, 2 = y).
+// kind: 1 = BCT_VEL_NEU, 2 = BCT_PRS_NEU, 3 = BCT_OUTFLOW, 4 = BCT_OVH_NEU.
+// Returns er[node][eq] (eq 0 = c, 1 = x, 2 = y).
 struct EdgeIn {
     double h[2], u[2], v[2];
-    double nx, ny, djac, z0;
+    double nx, ny, djac;
+    double z0, z1;              // bed elevations of the edge's two nodes
+    double bvx, bvy;            // NB OVH: the string's velocity series values (unused by other kinds)
 };
 
 __device__ __forceinline__ void line_phi_f_g_h(double djac, double c, double f1, double f2, double g1, double g2,
@@ -798,6 +800,9 @@ __device__ __forceinline__ void line_phi_f_g_h(double djac, double c, double f1,
     i1 += t1 * (((3 * f1 + 2 * f2) * g1 + (2 * f1 + 3 * f2) * g2) * h1 + ((2 * f1 + 3 * f2) * g1 + 3 * (f1 + 4 * f2) * g2) * h2);
 }
 
+// One boundary edge's residual.  kind 1: NB VEL explicit flow, `value` the unit discharge; 2: NB OTW tailwater, `value` the
+// water elevation; 3: NB OF free outflow; 4: NB OVH, `value` the water elevation and
+// (in.bvx, in.bvy) the prescribed velocity.
 __device__ __forceinline__ void sw2_edge_resid(const EdgeIn& in, int kind, double value, int pvar, const PhysParams& P,
                                                const int* dflag, double (&er)[2][3]) {
     const bool pressure = !(pvar == kPertU || pvar == kPertV);
@@ -806,6 +811,43 @@ __device__ __forceinline__ void sw2_edge_resid(const EdgeIn& in, int kind, doubl
     if (h_avg < kSmall) h_avg = kSmall;
 #pragma unroll
     for (int i = 0; i < 2; i++) er[i][0] = er[i][1] = er[i][2] = 0.0;
+    const double h0 = in.h[0], h1 = in.h[1];
+    // depth-weighted normal flux h v.n tested with the edge's linear functions (fe_sw2_1d_*)
+    auto normal_flux = [&](double& rc0, double& rc1) {
+        const double t1 = djac * kOne12;
+        rc0 = t1 * (nx * ((3 * h0 + h1) * in.u[0] + (h0 + h1) * in.u[1]) + ny * ((3 * h0 + h1) * in.v[0] + (h0 + h1) * in.v[1]));
+        rc1 = t1 * (nx * ((h0 + h1) * in.u[0] + (h0 + 3 * h1) * in.u[1]) + ny * ((h0 + h1) * in.v[0] + (h0 + 3 * h1) * in.v[1]));
+    };
+    // fe_sw2_1d_implicit_flow (:637-): flow with the current velocity, outflow components only
+    // in the momentum fluxes
+    auto implicit_flow = [&]() {
+        double ur0 = in.u[0], ur1 = in.u[1], vr0 = in.v[0], vr1 = in.v[1];
+        if (in.u[0] * nx + in.v[0] * ny < kSmall) { ur0 = 0.; vr0 = 0.; }
+        if (in.u[1] * nx + in.v[1] * ny < kSmall) { ur1 = 0.; vr1 = 0.; }
+        double rc0, rc1;
+        normal_flux(rc0, rc1);
+        double rx0 = 0, rx1 = 0, ry0 = 0, ry1 = 0;
+        line_phi_f_g_h(djac, nx, ur0, ur1, in.u[0], in.u[1], h0, h1, rx0, rx1);
+        line_phi_f_g_h(djac, ny, vr0, vr1, in.v[0], in.v[1], h0, h1, ry0, ry1);
+        line_phi_f_g_h(djac, ny, ur0, ur1, in.v[0], in.v[1], h0, h1, rx0, rx1);
+        line_phi_f_g_h(djac, nx, vr0, vr1, in.u[0], in.u[1], h0, h1, ry0, ry1);
+        er[0][0] += dt * rc0; er[1][0] += dt * rc1;
+        er[0][1] += dt * rx0; er[1][1] += dt * rx1;
+        er[0][2] += dt * ry0; er[1][2] += dt * ry1;
+    };
+    // fe_sw2_1d_pressure twice (:773-): the outside water column (d0, d1) minus the inside one
+    auto boundary_pressure = [&](double d0, double d1) {
+        double tt = djac * kOne12;
+        double p0 = tt * (3 * d0 * d0 + 2 * d0 * d1 + d1 * d1), p1 = tt * (d0 * d0 + 2 * d0 * d1 + 3 * d1 * d1);
+        double c1 = dt * 0.5 * g;
+        er[0][1] += c1 * nx * p0; er[1][1] += c1 * nx * p1;
+        er[0][2] += c1 * ny * p0; er[1][2] += c1 * ny * p1;
+        p0 = tt * (3 * h0 * h0 + 2 * h0 * h1 + h1 * h1);
+        p1 = tt * (h0 * h0 + 2 * h0 * h1 + 3 * h1 * h1);
+        c1 = dt * 0.5 * (-g);
+        er[0][1] += c1 * nx * p0; er[1][1] += c1 * nx * p1;
+        er[0][2] += c1 * ny * p0; er[1][2] += c1 * ny * p1;
+    };
     if (kind == 1) {                       // explicit flow (:562-604)
         const double flux = -1.0 * value;
         const double rc = 0.5 * djac;
@@ -824,40 +866,29 @@ __device__ __forceinline__ void sw2_edge_resid(const EdgeIn& in, int kind, doubl
         er[0][0] += t1 * rc; er[1][0] += t1 * rc;
         er[0][1] += t1 * rx0; er[1][1] += t1 * rx1;
         er[0][2] += t1 * ry0; er[1][2] += t1 * ry1;
-    } else if (kind == 2 || kind == 3) {
+    } else if (kind == 2 || kind == 3) {   // tailwater (:360-397) and free outflow (:227-240)
         double d0 = 0.0, d1 = 0.0;
         if (kind == 2) {
             d0 = value - in.z0;
             d1 = value - in.z0;             // both depths from node 0 (:375-376)
-            if (d0 < kSmall || d1 < kSmall || in.h[0] < kSmall || in.h[1] < kSmall) return;
+            if (d0 < kSmall || d1 < kSmall || h0 < kSmall || h1 < kSmall) return;
         }
-        double ur0 = in.u[0], ur1 = in.u[1], vr0 = in.v[0], vr1 = in.v[1];
-        if (in.u[0] * nx + in.v[0] * ny < kSmall) { ur0 = 0.; vr0 = 0.; }
-        if (in.u[1] * nx + in.v[1] * ny < kSmall) { ur1 = 0.; vr1 = 0.; }
-        const double h0 = in.h[0], h1 = in.h[1];
-        const double t1 = djac * kOne12;
-        double rc0 = t1 * (nx * ((3 * h0 + h1) * in.u[0] + (h0 + h1) * in.u[1]) + ny * ((3 * h0 + h1) * in.v[0] + (h0 + h1) * in.v[1]));
-        double rc1 = t1 * (nx * ((h0 + h1) * in.u[0] + (h0 + 3 * h1) * in.u[1]) + ny * ((h0 + h1) * in.v[0] + (h0 + 3 * h1) * in.v[1]));
-        double rx0 = 0, rx1 = 0, ry0 = 0, ry1 = 0;
-        line_phi_f_g_h(djac, nx, ur0, ur1, in.u[0], in.u[1], h0, h1, rx0, rx1);
-        line_phi_f_g_h(djac, ny, vr0, vr1, in.v[0], in.v[1], h0, h1, ry0, ry1);
-        line_phi_f_g_h(djac, ny, ur0, ur1, in.v[0], in.v[1], h0, h1, rx0, rx1);
-        line_phi_f_g_h(djac, nx, vr0, vr1, in.u[0], in.u[1], h0, h1, ry0, ry1);
-        er[0][0] += dt * rc0; er[1][0] += dt * rc1;
-        er[0][1] += dt * rx0; er[1][1] += dt * rx1;
-        er[0][2] += dt * ry0; er[1][2] += dt * ry1;
-        if (kind == 2 && pressure) {
-            double tt = djac * kOne12;
-            double p0 = tt * (3 * d0 * d0 + 2 * d0 * d1 + d1 * d1), p1 = tt * (d0 * d0 + 2 * d0 * d1 + 3 * d1 * d1);
-            double c1 = dt * 0.5 * g;
-            er[0][1] += c1 * nx * p0; er[1][1] += c1 * nx * p1;
-            er[0][2] += c1 * ny * p0; er[1][2] += c1 * ny * p1;
-            p0 = tt * (3 * h0 * h0 + 2 * h0 * h1 + h1 * h1);
-            p1 = tt * (h0 * h0 + 2 * h0 * h1 + 3 * h1 * h1);
-            c1 = dt * 0.5 * (-g);
-            er[0][1] += c1 * nx * p0; er[1][1] += c1 * nx * p1;
-            er[0][2] += c1 * ny * p0; er[1][2] += c1 * ny * p1;
+        implicit_flow();
+        if (kind == 2 && pressure) boundary_pressure(d0, d1);
+    } else if (kind == 4) {                // elevation and velocity (:398-440)
+        // each node's own bed here; an elevation below the bed stops the reference's run
+        // (tl_error), the residual is evaluated as written
+        const double d0 = value - in.z0, d1 = value - in.z1;
+        if (in.bvx * nx + in.bvy * ny < -kSmall) {   // inflow: fe_sw2_1d_hvel (:882-897)
+            double rc0, rc1;
+            normal_flux(rc0, rc1);
+            er[0][0] += dt * rc0; er[1][0] += dt * rc1;
+            er[0][1] += dt * rc0 * in.bvx; er[1][1] += dt * rc1 * in.bvx;
+            er[0][2] += dt * rc0 * in.bvy; er[1][2] += dt * rc1 * in.bvy;
+        } else {
+            implicit_flow();
         }
+        if (pressure) boundary_pressure(d0, d1);
     }
 #pragma unroll
     for (int i = 0; i < 2; i++) {

@@ -98,7 +98,8 @@ struct sw2gpu_ctx {
     DBuf<int> en0, en1, en2, emat, bn0, bn1, bkind, bstr;
     DBuf<unsigned char> efirst, dflag, mark;
     DBuf<MatParams> mats;
-    DBuf<double> str_value;
+    DBuf<double> str_value, str_uv;
+    bool has_ovh = false;       // some edge string is NB OVH (its velocity series go up every step)
     DBuf<int> slot_ptr, slot_idx, blk_ptr, blk_src, rowptr, col, blk_row, dpos;
     DBuf<int> dir_node_d, dir_mask_d;
     DBuf<double> dir_h, dir_u, dir_v;
@@ -314,9 +315,11 @@ int zalloc(DBuf<T>& b, size_t n, cudaStream_t st) {
 inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 
 // per-step tables: string values (edge series), material water sources, Dirichlet values
-// Staging layout (doubles): S string values | M MatParams | 3 x ndir Dirichlet values.
+// Staging layout (doubles): S string values | M MatParams | 3 x ndir Dirichlet values |
+// 2 x S NB OVH velocities.
 size_t stage_doubles(const sw2gpu_ctx* c) {
-    return (size_t)std::max(c->S, 1) + (sizeof(MatParams) * std::max(c->M, 1) + 7) / 8 + 3 * c->dir_node.size() + 1;
+    return (size_t)std::max(c->S, 1) + (sizeof(MatParams) * std::max(c->M, 1) + 7) / 8 + 3 * c->dir_node.size() +
+           2 * (size_t)std::max(c->S, 1) + 1;
 }
 
 // per-step tables through the context's pinned staging buffer (no host sync; the buffer is
@@ -359,6 +362,16 @@ int upload_step_tables(sw2gpu_ctx* c, const double* series, cudaStream_t st) {
         CK(cudaMemcpyAsync(c->dir_h.p, h, sizeof(double) * nd, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(c->dir_u.p, u, sizeof(double) * nd, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(c->dir_v.p, v, sizeof(double) * nd, cudaMemcpyHostToDevice, st));
+    }
+    if (c->has_ovh) {
+        double* uv = dv + 3 * nd;
+        auto get = [&](int k) { return (k >= 0 && k < c->NS && series) ? series[k] : 0.0; };
+        for (int s = 0; s < c->S; s++) {
+            const bool ovh = c->str_bc[s] == SW2GPU_BCT_OVH_NEU;
+            uv[2 * s] = ovh ? get(c->str_ivx[s]) : 0.0;
+            uv[2 * s + 1] = ovh ? get(c->str_ivy[s]) : 0.0;
+        }
+        CK(cudaMemcpyAsync(c->str_uv.p, uv, sizeof(double) * 2 * c->S, cudaMemcpyHostToDevice, st));
     }
     CK(cudaEventRecord(c->stage_ev, st));
     c->stage_pending = true;
@@ -1124,7 +1137,9 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
         bn1[j] = b;
         bstr[j] = s;
         const int f = c->str_bc[s];
-        bkind[j] = f == SW2GPU_BCT_VEL_NEU ? 1 : f == SW2GPU_BCT_PRS_NEU ? 2 : f == SW2GPU_BCT_OUTFLOW ? 3 : 0;
+        bkind[j] = f == SW2GPU_BCT_VEL_NEU ? 1 : f == SW2GPU_BCT_PRS_NEU ? 2 : f == SW2GPU_BCT_OUTFLOW ? 3
+                 : f == SW2GPU_BCT_OVH_NEU ? 4 : 0;
+        if (bkind[j] == 4) c->has_ovh = true;
         if (!bkind[j]) return fail(SW2GPU_E_ARG, "edge %d: boundary condition %d not supported", j, f);
     }
     // Dirichlet flags per node
@@ -1249,6 +1264,7 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     rc |= up(c->bdjac, bdj, st); rc |= up(c->bnx, bnx, st); rc |= up(c->bny, bny, st);
     rc |= up(c->mats, c->mats_h, st);
     rc |= zalloc(c->str_value, std::max(c->S, 1), st);
+    rc |= zalloc(c->str_uv, 2 * std::max(c->S, 1), st);
     rc |= up(c->slot_ptr, slot_ptr, st); rc |= up(c->slot_idx, slot_idx, st);
     rc |= up(c->blk_ptr, blk_ptr, st); rc |= up(c->blk_src, blk_src, st);
     rc |= up(c->rowptr, rp, st); rc |= up(c->col, col, st); rc |= up(c->blk_row, blk_row, st); rc |= up(c->dpos, dpos, st);
@@ -1321,7 +1337,7 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     d.efirst = c->efirst.p; d.dflag = c->dflag.p;
     d.bn0 = c->bn0.p; d.bn1 = c->bn1.p; d.bkind = c->bkind.p; d.bstr = c->bstr.p;
     d.bdjac = c->bdjac.p; d.bnx = c->bnx.p; d.bny = c->bny.p;
-    d.mats = c->mats.p; d.str_value = c->str_value.p;
+    d.mats = c->mats.p; d.str_value = c->str_value.p; d.str_uv = c->str_uv.p;
     d.slot_ptr = c->slot_ptr.p; d.slot_idx = c->slot_idx.p; d.blk_ptr = c->blk_ptr.p; d.blk_src = c->blk_src.p;
     d.rowptr = c->rowptr.p; d.col = c->col.p; d.blk_row = c->blk_row.p; d.dpos = c->dpos.p;
     for (int i = 0; i < 3; i++) d.qflag[i] = (i < V) ? dflag[i] : 0;

@@ -46,7 +46,7 @@ extern "C" {
 #define SW2GPU_BCT_VEL_NEU    10   /* NB VEL: prescribed normal unit discharge */
 #define SW2GPU_BCT_WATER_SOURCE 12
 #define SW2GPU_BCT_VEL_PRS_DIR 16
-#define SW2GPU_BCT_OVH_NEU    18   /* NB OVH: tailwater elevation + velocities (sw2gpu_create rejects it for now) */
+#define SW2GPU_BCT_OVH_NEU    18   /* NB OVH: water elevation (str_isigma) + velocity (str_ivx, str_ivy) series */
 
 /* precision modes */
 #define SW2GPU_FP64          0   /* everything FP64 */
@@ -69,7 +69,7 @@ typedef struct sw2gpu_mesh {
     const int32_t *elem1d_parent;      /* [nelems1d] adjacent 2D element */
     const int32_t *str_bc_flag;        /* [nstrings] ol_flow.bc_flag */
     const int32_t *str_isigma;         /* [nstrings] series id or -1 */
-    const int32_t *str_ivx, *str_ivy, *str_iu0;   /* [nstrings] Dirichlet series ids or -1 */
+    const int32_t *str_ivx, *str_ivy, *str_iu0;   /* [nstrings] Dirichlet (and NB OVH velocity) series ids or -1 */
     const double  *str_rough_height;   /* [nstrings] fterms.eqrheight (UNSET_FLT = no drag) */
     const int32_t *mat_eev_mode;       /* [nmats] 0: user eddy viscosity (EVS); 1..3: EEV mode */
     const double  *mat_ev;             /* [3*nmats] EVS xx, yy, xy */

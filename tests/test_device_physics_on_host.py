@@ -3,7 +3,8 @@ Jacobian kernel runs) compiled as host C++ and checked element by element agains
 fully wet and wet/dry elements, unperturbed and with the Jacobian's +-eps perturbations, on a basin
 with wet/dry fronts and every optional term switched on (temporal alpha, eddy viscosity, Coriolis),
 on one with a water source, and on elements holding Dirichlet nodes (DB OVH); and the boundary-edge
-residual (NB VEL inflow, NB OTW tailwater, NB OF free outflow) edge by edge.
+residual (NB VEL inflow, NB OTW tailwater, NB OF free outflow, NB OVH elevation + velocity) edge by
+edge.
 Runs on CPU, so a change to the physics is checked on every CPU run; the GPU parity tests check
 the same code as compiled for sm_100a."""
 import ctypes as C
@@ -65,20 +66,21 @@ extern "C" void host_elem_resid(const double* xyz, const double* lv, const doubl
         for (int q = 0; q < 3; q++) out[3 * i + q] = er[i][q];
 }
 
-// huv: h, u, v at the edge's two nodes (2 values each); geo: djac, nx, ny; value: the string's
-// series value (unit discharge or tailwater elevation)
-extern "C" void host_edge_resid(const double* huv, const double* geo, double z0, int kind, double value, int pvar,
-                                int pnode, double dx, const double* phys, double* out) {
+// huv: h, u, v at the edge's two nodes (2 values each); geo: djac, nx, ny; zb: the nodes' beds;
+// value: the string's series value (unit discharge or water elevation); bv: NB OVH velocity
+extern "C" void host_edge_resid(const double* huv, const double* geo, const double* zb, int kind, double value,
+                                const double* bv, int pvar, int pnode, double dx, const double* phys,
+                                const int* dflag, double* out) {
     EdgeIn in;
     for (int i = 0; i < 2; i++) { in.h[i] = huv[i]; in.u[i] = huv[2 + i]; in.v[i] = huv[4 + i]; }
     if (pvar == kPertH) in.h[pnode] += dx;
     else if (pvar == kPertU) in.u[pnode] += dx;
     else if (pvar == kPertV) in.v[pnode] += dx;
-    in.djac = geo[0]; in.nx = geo[1]; in.ny = geo[2]; in.z0 = z0;
+    in.djac = geo[0]; in.nx = geo[1]; in.ny = geo[2]; in.z0 = zb[0]; in.z1 = zb[1];
+    in.bvx = bv[0]; in.bvy = bv[1];
     const PhysParams P{phys[0], phys[1], phys[2], phys[3], phys[4], phys[5]};
-    const int df[2] = {0, 0};
     double er[2][3];
-    sw2_edge_resid(in, kind, value, pvar, P, df, er);
+    sw2_edge_resid(in, kind, value, pvar, P, dflag, er);
     for (int i = 0; i < 2; i++)
         for (int q = 0; q < 3; q++) out[3 * i + q] = er[i][q];
 }
@@ -190,10 +192,10 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
     assert worst <= 1e-12
 
 
-@pytest.mark.parametrize("case", ["tailwater", "outflow"])
+@pytest.mark.parametrize("case", ["tailwater", "outflow", "ovh"])
 def test_device_edge_physics_matches_oracle_on_host(host_physics, case):
-    from adhv8_kraken_b200.model import BCT_OUTFLOW, BCT_PRS_NEU, BCT_VEL_NEU
-    m = meshgen.channel(nsteps=4) if case == "tailwater" else meshgen.channel_outflow(nsteps=4)
+    from adhv8_kraken_b200.model import BCT_OUTFLOW, BCT_OVH_NEU, BCT_PRS_NEU, BCT_VEL_NEU
+    m = {"tailwater": meshgen.channel, "outflow": meshgen.channel_outflow, "ovh": meshgen.channel_ovh}[case](nsteps=4)
     o = Oracle(m)
     assert o.step()["status"] == 0
     series = m.series_values(o.t, o.t + m.dt)
@@ -201,11 +203,17 @@ def test_device_edge_physics_matches_oracle_on_host(host_physics, case):
     prm = capi.make_params(m)
     phys = np.array([prm.gravity, prm.drying_lower_limit, prm.drying_upper_limit, prm.tau_temporal, prm.tau_pg, m.dt])
     h, u, v = o.get_state(0)
-    kinds = {BCT_VEL_NEU: 1, BCT_PRS_NEU: 2, BCT_OUTFLOW: 3}
+    kinds = {BCT_VEL_NEU: 1, BCT_PRS_NEU: 2, BCT_OUTFLOW: 3, BCT_OVH_NEU: 4}
+    dflag = _dirichlet_flags(m)
     worst = 0.0
+    seen = set()
     for ie, (a, b) in enumerate(m.edges):
         st = m.strings[int(m.edge_string[ie])]
+        seen.add(st.bc_flag)
         value = float(series[st.isigma]) if st.isigma >= 0 else 0.0
+        bv = np.array([float(series[st.ivx]), float(series[st.ivy])]) if st.bc_flag == BCT_OVH_NEU else np.zeros(2)
+        zb = np.array([m.z[a], m.z[b]])
+        df = np.ascontiguousarray(dflag[[a, b]], np.int32)
         huv = np.array([h[a], h[b], u[a], u[b], v[a], v[b]])
         cases = [(-1, 0, 0.0, 0)]
         for pvar, arr in ((1, u), (2, v), (5, h)):
@@ -215,9 +223,11 @@ def test_device_edge_physics_matches_oracle_on_host(host_physics, case):
         for pvar, nd, dx, sign in cases:
             dev, ref, geo = np.zeros(6), np.zeros(6), np.zeros(3)
             oracle_lib().orc_edge_resid(o.h, ie, abs(dx), nd, pvar, sign, _dp(ref), _dp(geo))
-            host_physics.host_edge_resid(_dp(huv), _dp(geo), C.c_double(m.z[a]), kinds[st.bc_flag], C.c_double(value),
-                                         pvar, nd, C.c_double(dx), _dp(phys), _dp(dev))
+            host_physics.host_edge_resid(_dp(huv), _dp(geo), _dp(zb), kinds[st.bc_flag], C.c_double(value), _dp(bv),
+                                         pvar, nd, C.c_double(dx), _dp(phys), df.ctypes.data_as(C.POINTER(C.c_int)),
+                                         _dp(dev))
             err = float(np.abs(dev - ref).max() / max(np.abs(ref).max(), 1e-300))
             worst = max(worst, err)
             assert err <= 1e-12, (ie, pvar, nd, sign, err, dev, ref)
     assert worst <= 1e-12
+    assert {"tailwater": BCT_PRS_NEU, "outflow": BCT_OUTFLOW, "ovh": BCT_OVH_NEU}[case] in seen
