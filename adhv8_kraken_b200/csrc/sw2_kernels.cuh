@@ -7,6 +7,7 @@
 // summation order of fe_sw2_resid / fe_global_matrix_assemble_sw2.
 #pragma once
 #include "sw2_krylov.cuh"   // inv3, fold_block
+#include "sw2_mass.cuh"      // mass-balance terms
 #include "sw2_physics.cuh"
 
 namespace sw2 {
@@ -852,6 +853,95 @@ __global__ void k_dirichlet(const __grid_constant__ Src src) {
         I.s.v[k] = I.dir_v[t];
     }
     if (f & 1) I.s.h[k] = I.dir_h[t];
+}
+
+// ---------------------------------------------------------------------------------
+// Mass-balance diagnostics (src/tools/tl_grid_mass.c): per-block partial sums of the terms of
+// sw2_mass.cuh over a fixed grid, then one block adds the partials in block order, so a result
+// is the same on every run and every GPU.
+constexpr int kMassBlocks = 296;    // fixed, so the summation order is the same on every GPU
+constexpr int kMassThreads = 256;
+
+// fixed-order block sum of one value per thread (tree over the warp, then over the warps)
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    __syncthreads();
+    return s;   // valid in thread 0
+}
+
+// Partial sums per block: part[b] = grid mass of depth h (density 1); with FLUX, instead
+// part[2b] = source mass and part[2b+1] = boundary outflow of the step at state (h, u, v).
+template <bool FLUX>
+__global__ void __launch_bounds__(kMassThreads) k_mass_partial(const __grid_constant__ DevMesh m, const double* h,
+                                                               const double* u, const double* v, double dt,
+                                                               double density, double* part) {
+    __shared__ double red[kMassThreads / 32];
+    const int stride = kMassBlocks * kMassThreads;
+    double a = 0.0, b = 0.0;
+    for (int e = blockIdx.x * kMassThreads + threadIdx.x; e < m.T; e += stride) {
+        const int n[3] = {m.en0[e], m.en1[e], m.en2[e]};
+        double x[3], y[3], d[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            x[i] = m.x[n[i]];
+            y[i] = m.y[n[i]];
+            d[i] = h[n[i]];
+        }
+        if (!FLUX) {
+            a += elem_mass(x, y, d, m.djac[e]);
+        } else {
+            const MatParams& M = m.mats[m.emat[e]];
+            if (M.has_source) a += elem_source_mass(x, y, d, m.djac[e], M.water_src, dt, density);
+        }
+    }
+    if (FLUX && m.E > 0) {
+        const double djac0 = m.bdjac[0];
+        for (int j = blockIdx.x * kMassThreads + threadIdx.x; j < m.E; j += stride) {
+            const int n0 = m.bn0[j], n1 = m.bn1[j];
+            const double nx = m.bnx[j], ny = m.bny[j];
+            const double vn0 = u[n0] * nx + v[n0] * ny, vn1 = u[n1] * nx + v[n1] * ny;
+            b += edge_outflow_term(djac0, density, dt, h[n0], h[n1], vn0, vn1);
+        }
+    }
+    a = block_sum(a, red);
+    if (FLUX) b = block_sum(b, red);
+    if (threadIdx.x == 0) {
+        if (FLUX) {
+            part[2 * blockIdx.x] = a;
+            part[2 * blockIdx.x + 1] = b;
+        } else {
+            part[blockIdx.x] = a;
+        }
+    }
+}
+
+// The partials in block order: out[0] = density x grid mass, or (FLUX) out[0] = sources minus
+// boundary outflow of the step, the term tl_find_grid_mass_error_elem2d accumulates.
+template <bool FLUX>
+__global__ void __launch_bounds__(kMassThreads) k_mass_final(const double* part, double density, double* out) {
+    __shared__ double red[kMassThreads / 32];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < kMassBlocks; i += kMassThreads) {
+        if (FLUX) {
+            a += part[2 * i];
+            b += part[2 * i + 1];
+        } else {
+            a += part[i];
+        }
+    }
+    a = block_sum(a, red);
+    if (FLUX) b = block_sum(b, red);
+    if (threadIdx.x == 0) out[0] = FLUX ? a - b : a * density;
 }
 
 }  // namespace sw2

@@ -99,6 +99,7 @@ struct sw2gpu_ctx {
     DBuf<unsigned char> efirst, dflag, mark;
     DBuf<MatParams> mats;
     DBuf<double> str_value, str_uv;
+    DBuf<double> mass_part;     // mass-balance partials (2 per block) and the result
     bool has_ovh = false;       // some edge string is NB OVH (its velocity series go up every step)
     DBuf<int> slot_ptr, slot_idx, blk_ptr, blk_src, rowptr, col, blk_row, dpos;
     DBuf<int> dir_node_d, dir_mask_d;
@@ -1265,6 +1266,7 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     rc |= up(c->mats, c->mats_h, st);
     rc |= zalloc(c->str_value, std::max(c->S, 1), st);
     rc |= zalloc(c->str_uv, 2 * std::max(c->S, 1), st);
+    rc |= zalloc(c->mass_part, 2 * kMassBlocks + 1, st);
     rc |= up(c->slot_ptr, slot_ptr, st); rc |= up(c->slot_idx, slot_idx, st);
     rc |= up(c->blk_ptr, blk_ptr, st); rc |= up(c->blk_src, blk_src, st);
     rc |= up(c->rowptr, rp, st); rc |= up(c->col, col, st); rc |= up(c->blk_row, blk_row, st); rc |= up(c->dpos, dpos, st);
@@ -1387,6 +1389,39 @@ int sw2gpu_set_wd_flag(sw2gpu_ctx* c, const int32_t* wd) {
     if (c->T) CK(cudaMemcpyAsync(c->wd.p, wd, sizeof(int) * c->T, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return SW2GPU_OK;
+}
+
+// Mass-balance diagnostics (src/tools/tl_grid_mass.c): one fixed-grid partial pass and one
+// block adding the partials in order
+static int mass_reduce(sw2gpu_ctx* c, bool flux, const double* h, double density, double* out) {
+    double* part = c->mass_part.p;
+    double* res = part + 2 * kMassBlocks;
+    if (flux) {
+        k_mass_partial<true><<<kMassBlocks, kMassThreads, 0, c->stream>>>(c->dm, h, c->U(0), c->Vv(0), c->dt, density,
+                                                                          part);
+        CK(cudaGetLastError());
+        k_mass_final<true><<<1, kMassThreads, 0, c->stream>>>(part, density, res);
+    } else {
+        k_mass_partial<false><<<kMassBlocks, kMassThreads, 0, c->stream>>>(c->dm, h, nullptr, nullptr, 0.0, density,
+                                                                           part);
+        CK(cudaGetLastError());
+        k_mass_final<false><<<1, kMassThreads, 0, c->stream>>>(part, density, res);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_grid_mass(sw2gpu_ctx* c, int level, double density, double* mass) {
+    if (!c || !mass || level < 0 || level > 2) return fail(SW2GPU_E_ARG, "bad context, level or output");
+    return mass_reduce(c, false, c->H(level), density, mass);
+}
+
+int sw2gpu_mass_flux(sw2gpu_ctx* c, double density, double* flux) {
+    if (!c || !flux) return fail(SW2GPU_E_ARG, "bad context or output");
+    if (!(c->dt > 0.0)) return fail(SW2GPU_E_ARG, "no step taken yet (dt unset)");
+    return mass_reduce(c, true, c->H(0), density, flux);
 }
 
 int sw2gpu_set_dt(sw2gpu_ctx* c, double dt, const double* series) {

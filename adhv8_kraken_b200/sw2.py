@@ -30,8 +30,9 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_resid", "sw2gpu_load", "sw2gpu_linear_solve", "sw2gpu_batch_create", "sw2gpu_batch_step",
            "sw2gpu_batch_destroy", "sw2gpu_bcsr_solve_noalloc", "sw2gpu_engine_create", "sw2gpu_engine_add",
            "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_last_tick", "sw2gpu_engine_destroy",
-           "sw2gpu_device_bytes", "sw2gpu_autotune", "sw2gpu_set_graphs", "sw2gpu_set_variant", "sw2gpu_get_variant", "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait",
-           "sw2gpu_server_status", "sw2gpu_server_destroy"]
+           "sw2gpu_device_bytes", "sw2gpu_autotune", "sw2gpu_set_graphs", "sw2gpu_set_variant", "sw2gpu_get_variant",
+           "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
+           "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux"]
 
 
 class SW2Error(RuntimeError):
@@ -55,6 +56,8 @@ def lib():
         L.sw2gpu_get_state.argtypes = [vp, C.c_int, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_get_wd_flag.argtypes = [vp, c_int32_p]
         L.sw2gpu_set_wd_flag.argtypes = [vp, c_int32_p]
+        L.sw2gpu_grid_mass.argtypes = [vp, C.c_int, C.c_double, c_double_p]
+        L.sw2gpu_mass_flux.argtypes = [vp, C.c_double, c_double_p]
         L.sw2gpu_step.argtypes = [vp, C.c_double, c_double_p, vp]
         L.sw2gpu_set_dt.argtypes = [vp, C.c_double, c_double_p]
         L.sw2gpu_resid.argtypes = [vp, c_double_p]
@@ -211,6 +214,21 @@ class SW2GPU:
     def set_wd(self, wd):
         wd = np.ascontiguousarray(wd, dtype=np.int32)
         _check(lib().sw2gpu_set_wd_flag(self.h, _ip(wd)))
+
+    def grid_mass(self, level=0, density=None):
+        """Water mass of a time level (tl_find_grid_mass_elem2d), reduced on the device."""
+        rho = self.model.params.density if density is None else density
+        out = C.c_double()
+        _check(lib().sw2gpu_grid_mass(self.h, level, rho, C.byref(out)))
+        return out.value
+
+    def mass_flux(self, density=None):
+        """Mass that entered the grid during the last step (sources minus boundary outflow, the
+        per-step term tl_find_grid_mass_error_elem2d accumulates), reduced on the device."""
+        rho = self.model.params.density if density is None else density
+        out = C.c_double()
+        _check(lib().sw2gpu_mass_flux(self.h, rho, C.byref(out)))
+        return out.value
 
     def set_dt(self, dt, series):
         s = np.ascontiguousarray(series, dtype=np.float64)

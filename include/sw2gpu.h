@@ -141,6 +141,18 @@ int sw2gpu_get_wd_flag(sw2gpu_ctx *ctx, int32_t *wd_flag);
 /* Overrides the element wet/dry flags (normally set by the step's fe_sw2_init). */
 int sw2gpu_set_wd_flag(sw2gpu_ctx *ctx, const int32_t *wd_flag);
 
+/* Mass-balance diagnostics (src/tools/tl_grid_mass.c), on the device.
+ * sw2gpu_grid_mass: water mass of time level `level` times `density`
+ * (tl_find_grid_mass_elem2d, :20-97; partially dry triangles by the h < 0 corner clip of
+ * fe_3m2d_dry_wet_factornew, :289-346).
+ * sw2gpu_mass_flux: the mass that entered the grid during the last step at the current level,
+ * water sources minus boundary outflow (the per-step term tl_find_grid_mass_error_elem2d,
+ * :102-159, adds to its running total; the caller keeps that total and forms
+ * |mass - total - initial mass|).  Uses the last step's dt and series values.
+ * Both add their terms in a fixed order: the same bits on every run and every GPU. */
+int sw2gpu_grid_mass(sw2gpu_ctx *ctx, int level, double density, double *mass);
+int sw2gpu_mass_flux(sw2gpu_ctx *ctx, double density, double *flux);
+
 /* One implicit time step: time-level shift (fe_sw2, src/fe/sw2/fe_sw2.c:43-50) then the
  * damped Newton loop (fe_newton).  `series` holds the step-averaged value of every BC
  * series over [t, t+dt] (sseries_setall_ts_valuesAVG).  On SW2GPU_E_NEWTON the current

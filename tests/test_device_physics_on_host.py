@@ -34,6 +34,7 @@ using std::fabs; using std::fmax; using std::log; using std::pow; using std::sqr
 #define __forceinline__ inline
 #define __noinline__
 #include "sw2_physics.cuh"
+#include "sw2_mass.cuh"
 using namespace sw2;
 
 // xyz: x[3], y[3], z[3]; lv: h, u, v at the current, old and older levels (3 values each);
@@ -83,6 +84,42 @@ extern "C" void host_edge_resid(const double* huv, const double* geo, const doub
     sw2_edge_resid(in, kind, value, pvar, P, dflag, er);
     for (int i = 0; i < 2; i++)
         for (int q = 0; q < 3; q++) out[3 * i + q] = er[i][q];
+}
+
+// grid mass and one step's mass flux from the per-element / per-edge terms of sw2_mass.cuh,
+// added in element order (the device adds the same terms in a fixed tree order)
+static void corners(const int* tri, const double* x, const double* y, const double* h, int e, double* ex, double* ey,
+                    double* eh) {
+    for (int i = 0; i < 3; i++) { const int n = tri[3 * e + i]; ex[i] = x[n]; ey[i] = y[n]; eh[i] = h[n]; }
+}
+
+extern "C" double host_grid_mass(int T, const int* tri, const double* x, const double* y, const double* h,
+                                 const double* djac, double density) {
+    double mass = 0.0, ex[3], ey[3], eh[3];
+    for (int e = 0; e < T; e++) {
+        corners(tri, x, y, h, e, ex, ey, eh);
+        mass += elem_mass(ex, ey, eh, djac[e]);
+    }
+    return mass * density;
+}
+
+// rate[e]: the element's source rate, or NaN for an element without a source;
+// edges: node pairs with their outward normals nrm (nx, ny per edge)
+extern "C" double host_mass_flux(int T, const int* tri, const double* x, const double* y, const double* h,
+                                 const double* u, const double* v, const double* djac, const double* rate, int E,
+                                 const int* edges, const double* nrm, double djac0, double density, double dt) {
+    double body = 0.0, edge = 0.0, ex[3], ey[3], eh[3];
+    for (int e = 0; e < T; e++) {
+        if (rate[e] != rate[e]) continue;
+        corners(tri, x, y, h, e, ex, ey, eh);
+        body += elem_source_mass(ex, ey, eh, djac[e], rate[e], dt, density);
+    }
+    for (int j = 0; j < E; j++) {
+        const int a = edges[2 * j], b = edges[2 * j + 1];
+        const double nx = nrm[2 * j], ny = nrm[2 * j + 1];
+        edge -= edge_outflow_term(djac0, density, dt, h[a], h[b], u[a] * nx + v[a] * ny, u[b] * nx + v[b] * ny);
+    }
+    return body + edge;
 }
 """
 
@@ -231,3 +268,50 @@ def test_device_edge_physics_matches_oracle_on_host(host_physics, case):
             assert err <= 1e-12, (ie, pvar, nd, sign, err, dev, ref)
     assert worst <= 1e-12
     assert {"tailwater": BCT_PRS_NEU, "outflow": BCT_OUTFLOW, "ovh": BCT_OVH_NEU}[case] in seen
+
+
+@pytest.mark.parametrize("case", ["basin", "rain", "channel"])
+def test_device_mass_terms_match_oracle_on_host(host_physics, case):
+    """Grid mass (tl_find_grid_mass_elem2d, with its h < 0 corner clip and dry corners counted
+    as positive mass) and one step's mass flux (water sources, boundary outflow) from the
+    device's per-element terms, added in element order: bit-identical to the oracle after every
+    step of a wet/dry basin, a basin with rain and the channel with its inflow and tailwater
+    edges."""
+    from helpers import basin_model
+    m = {"basin": basin_model, "rain": lambda: meshgen.basin_rain(nsteps=6), "channel": lambda: meshgen.channel(nsteps=6)}[case]()
+    o = Oracle(m)
+    tri = np.ascontiguousarray(m.tri, np.int32)
+    djac = np.array([o.geometry(e)[0] for e in range(m.nelems2d)])
+    edges = np.ascontiguousarray(m.edges, np.int32).reshape(-1, 2)
+    nrm, elen = np.zeros((len(edges), 2)), np.zeros(len(edges))
+    for j in range(len(edges)):   # the oracle's edge geometry: length and outward normal
+        geo = np.zeros(3)
+        oracle_lib().orc_edge_resid(o.h, j, 1e-8, 0, -1, 0, _dp(np.zeros(6)), _dp(geo))
+        elen[j], nrm[j] = geo[0], geo[1:]
+    djac0 = float(elen[0]) if len(edges) else 0.0
+    assert (case != "channel") or len(edges) > 0
+    rho = m.params.density
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+    host_physics.host_grid_mass.restype = C.c_double
+    host_physics.host_mass_flux.restype = C.c_double
+    saw_negative = False
+    for k in range(6):
+        t, dt = o.t, m.dt
+        assert o.step()["status"] == 0
+        series = m.series_values(t, t + dt)
+        h, u, v = (np.ascontiguousarray(a) for a in o.get_state(0))
+        saw_negative |= bool((h < 0).any())
+        got = host_physics.host_grid_mass(m.nelems2d, ip(tri), _dp(m.x), _dp(m.y), _dp(h), _dp(djac), C.c_double(rho))
+        assert got == o.grid_mass(0), (k, got, o.grid_mass(0))
+        rate = np.full(m.nelems2d, np.nan)
+        for e in range(m.nelems2d):
+            st = m.strings[int(m.tri_mat[e])]
+            if st.bc_flag == BCT_WATER_SOURCE:
+                rate[e] = series[st.isigma]
+        assert (case != "rain") or np.isfinite(rate).any()
+        flux = host_physics.host_mass_flux(m.nelems2d, ip(tri), _dp(m.x), _dp(m.y), _dp(h), _dp(u), _dp(v), _dp(djac),
+                                           _dp(rate), len(edges), ip(edges), _dp(nrm), C.c_double(djac0),
+                                           C.c_double(rho), C.c_double(dt))
+        assert flux == o.mass_flux(dt, series), (k, flux, o.mass_flux(dt, series))
+    if case == "basin":
+        assert saw_negative   # the dry-corner branches ran

@@ -135,3 +135,38 @@ def test_boundary_and_term_variants_match_reference(case):
     assert relerr(r, ref["load0_resid"]) <= 1e-12
     assert relerr(val, ref["load0_val"]) <= 1e-7
     _run_against(model, ref, 6, range(1, 7))
+
+
+@pytest.mark.parametrize("case", ["channel", "basin", "rain"])
+def test_mass_balance_on_device_matches_reference(case, mass_ref, basin_ref):
+    """The device's grid mass (tl_find_grid_mass_elem2d) and per-step mass flux (sources minus
+    boundary outflow, tl_find_grid_mass_error_elem2d) at the reference's own state after every
+    step, against the reference's values: the channel (inflow and tailwater edges), the wet/dry
+    basin (dry corners) and the basin with rain.  The device adds its terms in a fixed tree
+    order, the reference in element order: 1e-12 relative to the initial mass."""
+    import os
+    from conftest import GOLDEN
+    from golden.make_golden import fingerprint
+    if case == "rain":
+        model, ref = meshgen.basin_rain(nsteps=6), dict(np.load(os.path.join(GOLDEN, "rain_ref.npz")))
+        assert str(ref["fingerprint"]) == fingerprint(model)
+        dts, masses, totals, pre, src = ref["dt"], ref["mass"], ref["mass_flux_total"], "step", ref
+        ref_mass0 = ref["mass0"][0]
+    else:
+        model = meshgen.channel(nsteps=6) if case == "channel" else basin_model()
+        assert str(mass_ref[f"{case}_fingerprint"]) == fingerprint(model)
+        dts, masses, totals = (mass_ref[f"{case}_{k}"] for k in ("dt", "mass", "mass_flux_total"))
+        pre, src = ("channel_step", mass_ref) if case == "channel" else ("step", basin_ref)
+        ref_mass0 = mass_ref[f"{case}_mass0"][0]
+    g = SW2GPU(model)
+    mass0 = g.grid_mass(0)
+    assert relerr(mass0, ref_mass0) <= 1e-12
+    t, acc = model.t0, 0.0
+    for k, dt in enumerate(dts, 1):
+        g.set_state(0, src[f"{pre}{k}_h"], src[f"{pre}{k}_u"], src[f"{pre}{k}_v"])
+        g.set_dt(dt, model.series_values(t, t + dt))
+        t += dt
+        acc += g.mass_flux()
+        assert relerr(g.grid_mass(0), masses[k - 1]) <= 1e-12, k
+        assert abs(acc - totals[k - 1]) <= 1e-12 * mass0, k
+    assert g.grid_mass(0) == g.grid_mass(0)   # fixed-order reduction: the same bits every call
