@@ -67,6 +67,7 @@ struct __align__(16) Inst {
     int ndir;                   // Dirichlet nodes and their step values
     const int *dir_node, *dir_mask;
     const double *dir_h, *dir_u, *dir_v;
+    double* dacont;             // [3][T] elem_rhs_dacont_extra_terms of the last residual, or null
 };
 
 // Where a launch finds its instances.  SrcOne: a single instance, its descriptor a kernel
@@ -186,7 +187,9 @@ __global__ void k_classify(const __grid_constant__ Src src) {
 // record, an odd stride in 8-byte words: no bank conflicts), which leaves the registers to the
 // residual's arithmetic: three CTAs per SM instead of two.
 static_assert(sizeof(ElemIn) % 8 == 0 && (sizeof(ElemIn) / 8) % 2 == 1, "odd record stride");
-template <class Src>
+// DAC: also write the transport side output (instances whose `dacont` is set), vertex-major
+// like the reference's elem_rhs_dacont_extra_terms[3][nelems2d]
+template <class Src, bool DAC = false>
 __global__ void __launch_bounds__(128, 3) k_resid_elem(const __grid_constant__ Src src) {
     int lb, nb;
     const Inst& I = src.get(lb, nb);
@@ -208,8 +211,12 @@ __global__ void __launch_bounds__(128, 3) k_resid_elem(const __grid_constant__ S
         load_elem(m, s, t, 1, in, n, df);
         const int wd = s.wd[t];
         classify_elem(t, wd == 0 && wet_depths(in.h, in.ho, in.hoo), ewet, glist, gcount);
-        double er[3][3];
-        sw2_elem_resid(in, in.h, in.u, in.v, wd, kPertNone, P, m.mats[m.emat[t]], df, er);
+        double er[3][3], dac[3];
+        sw2_elem_resid(in, in.h, in.u, in.v, wd, kPertNone, P, m.mats[m.emat[t]], df, er, DAC ? dac : nullptr);
+        if (DAC && I.dacont) {
+#pragma unroll
+            for (int i = 0; i < 3; i++) I.dacont[(size_t)i * m.T + t] = dac[i];
+        }
 #pragma unroll
         for (int i = 0; i < 3; i++) {
             const bool dry = in.ho[i] <= 0.;

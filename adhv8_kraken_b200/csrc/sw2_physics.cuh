@@ -329,11 +329,13 @@ __device__ __forceinline__ void wet_pre_velocity(const ElemIn& in, WetPre& p) {
 //   pvar:     kPertNone / kPertU / kPertV / kPertH (u, v perturbations drop the pressure terms)
 //   dflag[3]: Dirichlet flags of the element's nodes (bit0 PRS_DIR, bit1 VEL_DIR, bit2 VEL_PRS_DIR)
 //   PRE:      (fully wet only) the parts named by `fix` are read from `pre` (see WetPre)
+//   dac[3]:   when given, receives the continuity parts of shock capturing and SUPG per vertex, the
+//             side output elem_rhs_dacont_extra_terms that transport reads (:353-355, :400, :1214)
 template <bool WET, bool PRE = false>
 __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* hc, const double* uc, const double* vc,
                                                 int wd_flag, int pvar, const PhysParams& P, const MatParams& M,
                                                 const int* dflag, double (&er)[3][3], const WetPre* pre = nullptr,
-                                                unsigned fix = 0u) {
+                                                unsigned fix = 0u, double* dac = nullptr) {
     static_assert(WET || !PRE, "precomputed parts exist for fully wet elements only");
     const double djac = in.djac, dt = P.dt, g = P.g, dll = P.dll, dul = P.dul;
     const double* gx = in.gx;
@@ -425,6 +427,7 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
 
 #pragma unroll
     for (int i = 0; i < 3; i++) er[i][0] = er[i][1] = er[i][2] = 0.0;
+    if (dac) dac[0] = dac[1] = dac[2] = 0.0;
 
     // shock capturing, partially/fully dry elements (:357-400)
     if (!WET && (wd_flag == 1 || wd_flag == 2)) {
@@ -435,7 +438,9 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
         const double nx = unx * gux + uny * guy, ny = vnx * gvx + vny * gvy;
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            er[i][0] += dt * 0.5 * g * djac * ((dll * gwx) * gx[i] + (dll * gwy) * gy[i]);
+            const double rc = dt * 0.5 * g * djac * ((dll * gwx) * gx[i] + (dll * gwy) * gy[i]);
+            er[i][0] += rc;
+            if (dac) dac[i] += rc;
             er[i][1] += cu * dt * djac * nx * (unx * gx[i] + uny * gy[i]);
             er[i][2] += cv * dt * djac * ny * (vnx * gx[i] + vny * gy[i]);
         }
@@ -747,7 +752,9 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
         const double tu = tau * u_wd, tv = tau * v_wd, th = tau * h_wd;
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            er[i][0] += gx[i] * (tu * c_eq + th * x_eq) + gy[i] * (tv * c_eq + th * y_eq);
+            const double rc = gx[i] * (tu * c_eq + th * x_eq) + gy[i] * (tv * c_eq + th * y_eq);
+            er[i][0] += rc;
+            if (dac) dac[i] += rc;
             er[i][1] += gx[i] * (tau * gf * h_wd * c_eq + tu * h_wd * x_eq) + gy[i] * (tv * h_wd * x_eq);
             er[i][2] += gy[i] * (tau * gf * h_wd * c_eq + tv * h_wd * y_eq) + gx[i] * (tu * h_wd * y_eq);
         }
@@ -771,13 +778,24 @@ __device__ __noinline__ void elem_resid_general(const ElemIn& in, const double* 
     elem_resid_impl<false>(in, hc, uc, vc, wd_flag, pvar, P, M, dflag, er);
 }
 
+// the same with the transport side output; a function of its own, so the kernels that never
+// ask for that output keep their code
+__device__ __noinline__ void elem_resid_general_dac(const ElemIn& in, const double* hc, const double* uc,
+                                                    const double* vc, int wd_flag, int pvar, const PhysParams& P,
+                                                    const MatParams& M, const int* dflag, double (&er)[3][3],
+                                                    double* dac) {
+    elem_resid_impl<false>(in, hc, uc, vc, wd_flag, pvar, P, M, dflag, er, nullptr, 0u, dac);
+}
+
 __device__ __forceinline__ void sw2_elem_resid(const ElemIn& in, const double* hc, const double* uc, const double* vc,
                                                int wd_flag, int pvar, const PhysParams& P, const MatParams& M,
-                                               const int* dflag, double (&er)[3][3]) {
+                                               const int* dflag, double (&er)[3][3], double* dac = nullptr) {
     const bool wet = wd_flag == 0 && hc[0] > 0.0 && hc[1] > 0.0 && hc[2] > 0.0 && in.ho[0] > 0.0 &&
                      in.ho[1] > 0.0 && in.ho[2] > 0.0 && in.hoo[0] > 0.0 && in.hoo[1] > 0.0 && in.hoo[2] > 0.0;
     if (wet)
-        elem_resid_impl<true>(in, hc, uc, vc, wd_flag, pvar, P, M, dflag, er);
+        elem_resid_impl<true>(in, hc, uc, vc, wd_flag, pvar, P, M, dflag, er, nullptr, 0u, dac);
+    else if (dac)
+        elem_resid_general_dac(in, hc, uc, vc, wd_flag, pvar, P, M, dflag, er, dac);
     else
         elem_resid_general(in, hc, uc, vc, wd_flag, pvar, P, M, dflag, er);
 }

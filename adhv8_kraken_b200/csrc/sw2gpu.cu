@@ -100,6 +100,8 @@ struct sw2gpu_ctx {
     DBuf<MatParams> mats;
     DBuf<double> str_value, str_uv;
     DBuf<double> mass_part;     // mass-balance partials (2 per block) and the result
+    DBuf<double> dacont;        // [3][T] transport side output, allocated when first enabled
+    bool dacont_on = false;
     bool has_ovh = false;       // some edge string is NB OVH (its velocity series go up every step)
     DBuf<int> slot_ptr, slot_idx, blk_ptr, blk_src, rowptr, col, blk_row, dpos;
     DBuf<int> dir_node_d, dir_mask_d;
@@ -507,6 +509,7 @@ int runner_tables(Runner& R, int apply_inc) {
         I.ndir = (int)c->dir_node.size();
         I.dir_node = c->dir_node_d.p; I.dir_mask = c->dir_mask_d.p;
         I.dir_h = c->dir_h.p; I.dir_u = c->dir_u.p; I.dir_v = c->dir_v.p;
+        I.dacont = c->dacont_on ? c->dacont.p : nullptr;
         KrylovInst& Q = R.ktab_h[k];
         KrylovArgs& A = Q.K;
         A.V = c->V;
@@ -601,7 +604,14 @@ int launch_init(Runner& R, const std::vector<int>& sub) {     // fe_sw2_init
 // residual at the current state: element slots, reference-order gather, norms (async)
 int launch_resid(Runner& R, const std::vector<int>& sub) {
     Phase ph(&R, kPhResid);
-    int rc = launch_map(R, sub, 128, [&](int k) { return nblk(R.ctx[k]->T + R.ctx[k]->E, 128); }, SW2_GO(k_resid_elem<std::decay_t<decltype(src)>>));
+    bool dac = false;   // some instance keeps the transport side output
+    for (int k : sub) dac |= R.ctx[k]->dacont_on;
+    auto blocks = [&](int k) { return nblk(R.ctx[k]->T + R.ctx[k]->E, 128); };
+    int rc = dac ? launch_map(R, sub, 128, blocks,
+                              [&](const auto& src, int nb_, int th_) {
+                                  k_resid_elem<std::decay_t<decltype(src)>, true><<<nb_, th_, 0, R.stream>>>(src);
+                              })
+                 : launch_map(R, sub, 128, blocks, SW2_GO(k_resid_elem<std::decay_t<decltype(src)>>));
     if (rc) return rc;
     return launch_map(R, sub, kGatherThreads, [&](int k) { return nblk(R.ctx[k]->V, kGatherThreads); },
                       SW2_GO(k_resid_gather<std::decay_t<decltype(src)>>));
@@ -1422,6 +1432,28 @@ int sw2gpu_mass_flux(sw2gpu_ctx* c, double density, double* flux) {
     if (!c || !flux) return fail(SW2GPU_E_ARG, "bad context or output");
     if (!(c->dt > 0.0)) return fail(SW2GPU_E_ARG, "no step taken yet (dt unset)");
     return mass_reduce(c, true, c->H(0), density, flux);
+}
+
+int sw2gpu_set_dacont(sw2gpu_ctx* c, int32_t enable) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    if (enable && !c->dacont.p) {
+        g_alloc_bytes = &c->bytes;
+        const int rc = zalloc(c->dacont, 3 * (size_t)c->T, c->stream);
+        g_alloc_bytes = nullptr;
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    c->dacont_on = enable != 0;
+    c->drop_graphs();   // the residual launches change
+    return SW2GPU_OK;
+}
+
+int sw2gpu_get_dacont(sw2gpu_ctx* c, double* out) {
+    if (!c || !out) return fail(SW2GPU_E_ARG, "null argument");
+    if (!c->dacont_on) return fail(SW2GPU_E_ARG, "transport side output not enabled (sw2gpu_set_dacont)");
+    if (c->T) CK(cudaMemcpyAsync(out, c->dacont.p, sizeof(double) * 3 * c->T, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
 }
 
 int sw2gpu_set_dt(sw2gpu_ctx* c, double dt, const double* series) {

@@ -32,7 +32,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_last_tick", "sw2gpu_engine_destroy",
            "sw2gpu_device_bytes", "sw2gpu_autotune", "sw2gpu_set_graphs", "sw2gpu_set_variant", "sw2gpu_get_variant",
            "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
-           "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux"]
+           "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont"]
 
 
 class SW2Error(RuntimeError):
@@ -58,6 +58,8 @@ def lib():
         L.sw2gpu_set_wd_flag.argtypes = [vp, c_int32_p]
         L.sw2gpu_grid_mass.argtypes = [vp, C.c_int, C.c_double, c_double_p]
         L.sw2gpu_mass_flux.argtypes = [vp, C.c_double, c_double_p]
+        L.sw2gpu_set_dacont.argtypes = [vp, C.c_int32]
+        L.sw2gpu_get_dacont.argtypes = [vp, c_double_p]
         L.sw2gpu_step.argtypes = [vp, C.c_double, c_double_p, vp]
         L.sw2gpu_set_dt.argtypes = [vp, C.c_double, c_double_p]
         L.sw2gpu_resid.argtypes = [vp, c_double_p]
@@ -229,6 +231,16 @@ class SW2GPU:
         out = C.c_double()
         _check(lib().sw2gpu_mass_flux(self.h, rho, C.byref(out)))
         return out.value
+
+    def set_dacont(self, enable: bool = True):
+        """Keep the transport side output elem_rhs_dacont_extra_terms of every residual evaluation."""
+        _check(lib().sw2gpu_set_dacont(self.h, 1 if enable else 0))
+
+    def dacont(self):
+        """elem_rhs_dacont_extra_terms of the last residual evaluation, vertex-major [3 * T]."""
+        out = np.zeros(3 * self.T)
+        _check(lib().sw2gpu_get_dacont(self.h, _dp(out)))
+        return out
 
     def set_dt(self, dt, series):
         s = np.ascontiguousarray(series, dtype=np.float64)

@@ -153,6 +153,15 @@ int sw2gpu_set_wd_flag(sw2gpu_ctx *ctx, const int32_t *wd_flag);
 int sw2gpu_grid_mass(sw2gpu_ctx *ctx, int level, double density, double *mass);
 int sw2gpu_mass_flux(sw2gpu_ctx *ctx, double density, double *flux);
 
+/* Transport side output elem_rhs_dacont_extra_terms (src/fe/sw2/fe_sw2_body_resid.c:353-355,
+ * :400, :1214): the continuity parts of shock capturing and SUPG per element vertex from the
+ * last residual evaluation, which the reference keeps for its transport solve.  Off by default
+ * (the residual kernel then skips it); sw2gpu_set_dacont(ctx, 1) allocates 24 B per element.
+ * sw2gpu_get_dacont copies it vertex-major like the reference's [3][nelems2d] array:
+ * out[i * nelems2d + e]; SW2GPU_E_ARG while it is off. */
+int sw2gpu_set_dacont(sw2gpu_ctx *ctx, int32_t enable);
+int sw2gpu_get_dacont(sw2gpu_ctx *ctx, double *out);
+
 /* One implicit time step: time-level shift (fe_sw2, src/fe/sw2/fe_sw2.c:43-50) then the
  * damped Newton loop (fe_newton).  `series` holds the step-averaged value of every BC
  * series over [t, t+dt] (sseries_setall_ts_valuesAVG).  On SW2GPU_E_NEWTON the current

@@ -39,10 +39,11 @@ using namespace sw2;
 
 // xyz: x[3], y[3], z[3]; lv: h, u, v at the current, old and older levels (3 values each);
 // geo: djac, gx0, gy0, gx1, gy1, gx2, gy2; phys: g, dll, dul, alpha, tau_pg, dt;
-// mat: ks, ev_st, ev_tr, eev_coef, cor_speed, water_src; dflag: the vertices' Dirichlet flags
+// mat: ks, ev_st, ev_tr, eev_coef, cor_speed, water_src; dflag: the vertices' Dirichlet flags;
+// dac: null, or the transport side output (continuity parts of shock capturing and SUPG)
 extern "C" void host_elem_resid(const double* xyz, const double* lv, const double* geo, int wd, int pvar, int pnode,
                                 double dx, const double* phys, const double* mat, int eev_mode, int has_source,
-                                const int* dflag, double* out) {
+                                const int* dflag, double* out, double* dac) {
     ElemIn in;
     for (int i = 0; i < 3; i++) {
         in.x[i] = xyz[i]; in.y[i] = xyz[3 + i]; in.z[i] = xyz[6 + i];
@@ -62,7 +63,7 @@ extern "C" void host_elem_resid(const double* xyz, const double* lv, const doubl
     M.ks = mat[0]; M.ev_st = mat[1]; M.ev_tr = mat[2]; M.eev_coef = mat[3]; M.cor_speed = mat[4];
     M.water_src = mat[5]; M.eev_mode = eev_mode; M.has_source = has_source;
     double er[3][3];
-    sw2_elem_resid(in, hc, uc, vc, wd, pvar, P, M, dflag, er);
+    sw2_elem_resid(in, hc, uc, vc, wd, pvar, P, M, dflag, er, dac);
     for (int i = 0; i < 3; i++)
         for (int q = 0; q < 3; q++) out[3 * i + q] = er[i][q];
 }
@@ -217,11 +218,13 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
             eps = _fd_eps(arr[nodes[b]])
             cases += [(pvar, b, eps, 1), (pvar, b, -eps, -1)]
         for pvar, b, dx, sign in cases:
-            dev, ref = np.zeros(9), np.zeros(9)
+            dev, ref, dac = np.zeros(9), np.zeros(9), np.zeros(3)
             host_physics.host_elem_resid(_dp(xyz), _dp(lv), _dp(geo), int(wd[ie]), pvar, b, C.c_double(dx), _dp(phys),
                                          _dp(mat), mt.eev_mode, int(source),
-                                         df.ctypes.data_as(C.POINTER(C.c_int)), _dp(dev))
+                                         df.ctypes.data_as(C.POINTER(C.c_int)), _dp(dev), _dp(dac))
             oracle_lib().orc_body_resid(o.h, int(ie), abs(dx), b, pvar, sign, _dp(ref))
+            # the transport side output of the same call (elem_rhs_dacont_extra_terms)
+            assert np.array_equal(dac, o.dacont()[:, ie]), (int(ie), pvar, dac, o.dacont()[:, ie])
             scale = max(np.abs(ref).max(), 1e-300)
             err = float(np.abs(dev - ref).max() / scale)
             worst = max(worst, err)
