@@ -1157,8 +1157,11 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     std::vector<unsigned char> dflag(V, 0);
     for (int n = 0; n < V; n++) {
         const int s = m->node_string[n];
-        if (s > SW2GPU_NORMAL && s < c->S) {
+        if (s >= c->S) return fail(SW2GPU_E_ARG, "node %d: bad string %d", n, s);
+        if (s > SW2GPU_NORMAL) {
             const int f = c->str_bc[s];
+            if (f == SW2GPU_BCT_LID_DFT || f == SW2GPU_BCT_LID_ELV || f == SW2GPU_BCT_LID_DEP)
+                return fail(SW2GPU_E_ARG, "node %d: lid boundary condition %d (string %d) not supported", n, f, s);
             dflag[n] = f == SW2GPU_BCT_PRS_DIR ? 1 : f == SW2GPU_BCT_VEL_DIR ? 2 : f == SW2GPU_BCT_VEL_PRS_DIR ? 4 : 0;
             if (dflag[n]) {
                 c->dir_node.push_back(n);

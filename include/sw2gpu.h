@@ -47,6 +47,11 @@ extern "C" {
 #define SW2GPU_BCT_WATER_SOURCE 12
 #define SW2GPU_BCT_VEL_PRS_DIR 16
 #define SW2GPU_BCT_OVH_NEU    18   /* NB OVH: water elevation (str_isigma) + velocity (str_ivx, str_ivy) series */
+/* lids on node strings (pressure under a lid in the body residual, fe_sw2_body_resid.c:154-177):
+ * not built; sw2gpu_create rejects them with SW2GPU_E_ARG rather than ignore them */
+#define SW2GPU_BCT_LID_DFT    20
+#define SW2GPU_BCT_LID_ELV    21
+#define SW2GPU_BCT_LID_DEP    22
 
 /* precision modes */
 #define SW2GPU_FP64          0   /* everything FP64 */

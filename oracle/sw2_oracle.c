@@ -793,6 +793,14 @@ orc_ctx *orc_create(const sw2gpu_mesh *m, const sw2gpu_params *p, int nblock) {
     C->resid = (double *) calloc(3 * C->V, sizeof(double));
     C->sol = (double *) calloc(3 * C->V, sizeof(double));
     C->include = (int *) calloc(C->V, sizeof(int));
+    for (i = 0; i < C->V; i++) {                       /* node strings: ids in range, no lids */
+        int s = C->node_string[i];
+        if (s >= C->S) { fprintf(stderr, "oracle: node %d has bad string %d\n", i, s); free(C); return NULL; }
+        if (s > SW2GPU_NORMAL && (C->str_bc[s] == SW2GPU_BCT_LID_DFT || C->str_bc[s] == SW2GPU_BCT_LID_ELV ||
+                                  C->str_bc[s] == SW2GPU_BCT_LID_DEP)) {
+            fprintf(stderr, "oracle: lid boundary condition on node %d not supported\n", i); free(C); return NULL;
+        }
+    }
     /* geometry (element_djac_nrml_gradPhi.c:193-273, elem1d_outward_nrml.c) */
     C->djac = (double *) malloc(sizeof(double) * (C->T ? C->T : 1));
     C->grad = (double *) malloc(sizeof(double) * 6 * (C->T ? C->T : 1));

@@ -99,3 +99,23 @@ def test_server_request_with_bad_mesh_fails_alone():
     st, _ = srv.wait(rid_good)
     assert st["status"] == 0 and st["steps"] == 2
     srv.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("what", ["lid", "bad_string"])
+def test_create_rejects_unsupported_node_strings(what):
+    """sw2gpu_create refuses a node string with a lid (BCT_LID_*, not built) or a string id out of
+    range with SW2GPU_E_ARG instead of solving without it."""
+    import dataclasses
+    m = meshgen.channel_obstacle(nsteps=2, with_depth=True)
+    if what == "lid":
+        strings = list(m.strings)
+        strings[-1] = dataclasses.replace(strings[-1], bc_flag=capi.SW2GPU_BCT_LID_DFT)
+        m = dataclasses.replace(m, strings=strings)
+    else:
+        ns = m.node_string.copy()
+        ns[ns >= 0] = len(m.strings)
+        m = dataclasses.replace(m, node_string=ns)
+    with pytest.raises(SW2Error) as err:
+        SW2GPU(m)
+    assert err.value.code == capi.SW2GPU_E_ARG

@@ -149,3 +149,22 @@ def test_oracle_transport_side_output_matches_reference(basin_ref):
         assert o.step(dt=basin_ref["dt"][k], t=basin_ref["t"][k])["status"] == 0
         if k + 1 in (1, 4, 8):
             assert relerr(o.dacont(), ref[f"step{k+1}_dacont"]) <= 1e-10, k
+
+
+@pytest.mark.parametrize("what", ["lid", "bad_string"])
+def test_oracle_rejects_unsupported_node_strings(what):
+    """A node string with a lid (BCT_LID_*, pressure under a lid in fe_sw2_body_resid.c:154-177,
+    not built) or a string id out of range is refused at creation, not ignored."""
+    import dataclasses
+    from adhv8_kraken_b200 import capi, meshgen
+    m = meshgen.channel_obstacle(nsteps=2, with_depth=True)
+    if what == "lid":
+        strings = list(m.strings)
+        strings[-1] = dataclasses.replace(strings[-1], bc_flag=capi.SW2GPU_BCT_LID_DFT)
+        m = dataclasses.replace(m, strings=strings)
+    else:
+        ns = m.node_string.copy()
+        ns[ns >= 0] = len(m.strings)
+        m = dataclasses.replace(m, node_string=ns)
+    with pytest.raises(ValueError):
+        Oracle(m)
