@@ -163,9 +163,11 @@ def _dirichlet_flags(m):
     return per_string[np.where(m.node_string >= 0, m.node_string, len(m.strings))]
 
 
-@pytest.mark.parametrize("case", ["all_terms", "rain", "obstacle"])
+@pytest.mark.parametrize("case", ["all_terms", "terms_fixture", "rain", "obstacle"])
 def test_device_physics_matches_oracle_on_host(host_physics, case):
-    if case == "rain":
+    if case == "terms_fixture":   # the all-terms reference fixture's model (EEV mode 3, southern Coriolis)
+        m = meshgen.basin_all_terms(nsteps=4)
+    elif case == "rain":
         m = meshgen.basin_rain(nsteps=4)
     elif case == "obstacle":
         m = meshgen.channel_obstacle(nsteps=4, with_depth=True)
