@@ -40,10 +40,13 @@ using namespace sw2;
 // xyz: x[3], y[3], z[3]; lv: h, u, v at the current, old and older levels (3 values each);
 // geo: djac, gx0, gy0, gx1, gy1, gx2, gy2; phys: g, dll, dul, alpha, tau_pg, dt;
 // mat: ks, ev_st, ev_tr, eev_coef, cor_speed, water_src; dflag: the vertices' Dirichlet flags;
-// dac: null, or the transport side output (continuity parts of shock capturing and SUPG)
+// dac: null, or the transport side output (continuity parts of shock capturing and SUPG);
+// pre: evaluate the way the wet Jacobian kernel does (fully wet elements, perturbed calls only):
+// the parts the perturbation leaves unchanged precomputed once per element (WetPre) from the
+// unperturbed iterate, as the kernel's staging warp forms them, and the column's `fix` mask
 extern "C" void host_elem_resid(const double* xyz, const double* lv, const double* geo, int wd, int pvar, int pnode,
                                 double dx, const double* phys, const double* mat, int eev_mode, int has_source,
-                                const int* dflag, double* out, double* dac) {
+                                int pre, const int* dflag, double* out, double* dac) {
     ElemIn in;
     for (int i = 0; i < 3; i++) {
         in.x[i] = xyz[i]; in.y[i] = xyz[3 + i]; in.z[i] = xyz[6 + i];
@@ -63,7 +66,18 @@ extern "C" void host_elem_resid(const double* xyz, const double* lv, const doubl
     M.ks = mat[0]; M.ev_st = mat[1]; M.ev_tr = mat[2]; M.eev_coef = mat[3]; M.cor_speed = mat[4];
     M.water_src = mat[5]; M.eev_mode = eev_mode; M.has_source = has_source;
     double er[3][3];
-    sw2_elem_resid(in, hc, uc, vc, wd, pvar, P, M, dflag, er, dac);
+    if (pre) {
+        WetPre wp;
+        wet_levels(in, P, wp.L);
+        wet_depth(in, in.h, P, M, wp.D);
+        wet_pre_velocity(in, wp);
+        const unsigned others = (7u & ~(1u << pnode)) << kFixNode;
+        const unsigned fix = pvar == kPertU ? (kFixH | kFixV | others)
+                           : pvar == kPertV ? (kFixH | kFixU | others) : (kFixU | kFixV | (7u << kFixNode));
+        elem_resid_impl<true, true>(in, hc, uc, vc, wd, pvar, P, M, dflag, er, &wp, fix);
+    } else {
+        sw2_elem_resid(in, hc, uc, vc, wd, pvar, P, M, dflag, er, dac);
+    }
     for (int i = 0; i < 3; i++)
         for (int q = 0; q < 3; q++) out[3 * i + q] = er[i][q];
 }
@@ -198,7 +212,7 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
         fringe = np.nonzero((wd != 0) | (h0[tri] <= 0.0).any(axis=1))[0]
     picks = np.concatenate([fringe[:150], rng.choice(m.nelems2d, 150, replace=False)])
     assert fringe.size > 0
-    worst = 0.0
+    worst, wet_columns = 0.0, 0
     for ie in picks:
         nodes = tri[ie]
         xyz = np.concatenate([m.x[nodes], m.y[nodes], m.z[nodes]])
@@ -214,6 +228,7 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
                         math.sin(math.pi / 180.0 * mt.coriolis) * 2.0 * 7.2722e-5,
                         float(series[st.isigma]) if source else 0.0])
         df = np.ascontiguousarray(dflag[nodes], np.int32)
+        fully_wet = wd[ie] == 0 and all((levels[k][0][nodes] > 0).all() for k in range(3))
         cases = [(-1, 0, 0.0, 0)]
         for pvar, arr in ((1, levels[0][1]), (2, levels[0][2]), (5, levels[0][0])):
             b = int(rng.integers(0, 3))
@@ -222,9 +237,16 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
         for pvar, b, dx, sign in cases:
             dev, ref, dac = np.zeros(9), np.zeros(9), np.zeros(3)
             host_physics.host_elem_resid(_dp(xyz), _dp(lv), _dp(geo), int(wd[ie]), pvar, b, C.c_double(dx), _dp(phys),
-                                         _dp(mat), mt.eev_mode, int(source),
+                                         _dp(mat), mt.eev_mode, int(source), 0,
                                          df.ctypes.data_as(C.POINTER(C.c_int)), _dp(dev), _dp(dac))
             oracle_lib().orc_body_resid(o.h, int(ie), abs(dx), b, pvar, sign, _dp(ref))
+            if fully_wet and pvar != -1:   # the wet Jacobian kernel's evaluation of the same column
+                pre = np.zeros(9)
+                host_physics.host_elem_resid(_dp(xyz), _dp(lv), _dp(geo), 0, pvar, b, C.c_double(dx), _dp(phys),
+                                             _dp(mat), mt.eev_mode, int(source), 1,
+                                             df.ctypes.data_as(C.POINTER(C.c_int)), _dp(pre), None)
+                assert np.array_equal(pre, ref), (int(ie), pvar, b, sign, pre, ref)
+                wet_columns += 1
             # the transport side output of the same call (elem_rhs_dacont_extra_terms)
             assert np.array_equal(dac, o.dacont()[:, ie]), (int(ie), pvar, dac, o.dacont()[:, ie])
             scale = max(np.abs(ref).max(), 1e-300)
@@ -232,6 +254,7 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
             worst = max(worst, err)
             assert err <= 1e-12, (int(ie), pvar, b, sign, err, dev, ref)
     assert worst <= 1e-12
+    assert wet_columns > 0   # the precomputed-parts path ran
 
 
 @pytest.mark.parametrize("case", ["tailwater", "outflow", "ovh"])
