@@ -27,6 +27,7 @@
 #include "../../include/sw2gpu.h"
 #include "sw2_kernels.cuh"
 #include "sw2_krylov.cuh"
+#include "sw2_series.h"
 
 using namespace sw2;
 
@@ -1683,32 +1684,6 @@ int sw2gpu_batch_destroy(sw2gpu_batch* b) {
 // continuous batching engine
 
 namespace {
-
-// piecewise-linear series and its average over a step (sseries_set_values_average,
-// src/structs/sseries.c:566-613): exact trapezoid integral over the breakpoints inside the
-// step, end segments extrapolated linearly
-struct PwlSeries {
-    std::vector<double> t, v;
-    double at(double tt) const {
-        const size_t n = t.size();
-        if (n == 1) return v[0];
-        long i = (long)(std::upper_bound(t.begin(), t.end(), tt) - t.begin()) - 1;
-        i = std::min(std::max(i, 0L), (long)n - 2);
-        const double w = (tt - t[i]) / (t[i + 1] - t[i]);
-        return v[i] + w * (v[i + 1] - v[i]);
-    }
-    double avg(double t1, double t2) const {
-        if (t2 <= t1) return at(t1);
-        double area = 0.0, a = t1;
-        for (double x : t) {
-            if (!(t1 < x && x < t2)) continue;
-            area += 0.5 * (at(a) + at(x)) * (x - a);
-            a = x;
-        }
-        area += 0.5 * (at(a) + at(t2)) * (t2 - a);
-        return area / (t2 - t1);
-    }
-};
 
 struct EngInst {
     sw2gpu_ctx* c = nullptr;
