@@ -21,9 +21,11 @@
  * (oracle/ref/build_ref.py) on the same inputs; see tests/golden/.
  *
  * Supported scope: triangles; EVS/EEV eddy viscosity; log-law drag from Manning n;
- * Coriolis; water source; NB VEL, NB OTW and OUTFLOW edges; PRS/VEL/VEL_PRS
- * Dirichlet node strings.  Lids, wind, waves, baroclinic terms, vorticity and
- * quadrilaterals are rejected at create time (the generated workloads use none).
+ * Coriolis; temporal alpha; water source; NB VEL, NB OTW, NB OF and NB OVH edges;
+ * PRS/VEL/VEL_PRS Dirichlet node strings; the grid mass diagnostics and the transport
+ * side output elem_rhs_dacont_extra_terms.  Lid node strings are rejected at create
+ * time; wind, waves, baroclinic terms, vorticity and quadrilaterals have no input
+ * fields here (the generated workloads use none).
  */
 #include <math.h>
 #include <float.h>
