@@ -108,6 +108,35 @@ def basin_rain(nsteps: int = 6, rate: float = 2e-4) -> SW2Model:
     return m
 
 
+def basin_combined(nsteps: int = 6, rate: float = 2e-4, u_in: float = 0.2) -> SW2Model:
+    """Every supported feature at once, for interactions: the all-terms wet/dry basin (temporal
+    alpha, EVS with Coriolis, EEV modes 1-3) with rain on its first material, an NB OVH inflow
+    west (water elevation 2 m, velocity (u_in, 0)), a free NB OF outflow east, and an interior
+    node with its element neighbours held at zero velocity and their mean initial depth (DB OVH)."""
+    from .model import BCT_OUTFLOW, BCT_OVH_NEU, BCT_VEL_PRS_DIR, BCT_WATER_SOURCE
+    m = basin_all_terms(nsteps=nsteps)
+    m.name = "combined"
+    t_end = (nsteps + 10) * m.dt
+    ns = len(m.series)
+    const = lambda val: Series(np.array([0.0, t_end]), np.array([val, val]))
+    # held nodes: the node nearest the basin centre and every node sharing an element with it
+    c = int(np.argmin(np.hypot(m.x - 1000.0, m.y - 1000.0)))
+    held = np.unique(m.tri[(m.tri == c).any(axis=1)].ravel())
+    m.series = list(m.series) + [const(rate), const(u_in), const(0.0), const(2.0),
+                                 const(float(np.mean(m.h0[held])))]
+    strings = list(m.strings)
+    nmat = len(m.materials)
+    strings[0] = dataclasses.replace(strings[0], bc_flag=BCT_WATER_SOURCE, isigma=ns)
+    strings[nmat] = StringSpec("edge", bc_flag=BCT_OVH_NEU, ivx=ns + 1, ivy=ns + 2, isigma=ns + 3)
+    strings[nmat + 1] = StringSpec("edge", bc_flag=BCT_OUTFLOW)
+    strings.append(StringSpec("node", bc_flag=BCT_VEL_PRS_DIR, ivx=ns + 2, ivy=ns + 2, iu0=ns + 4))
+    m.strings = strings
+    node_string = m.node_string.copy()
+    node_string[held] = len(strings) - 1
+    m.node_string = node_string
+    return m
+
+
 def channel_obstacle(nsteps: int = 6, with_depth: bool = False) -> SW2Model:
     """The channel with a short line of interior nodes across mid-channel held at zero velocity
     (DB OVL), or at zero velocity and 1 m depth (DB OVH, `with_depth`): a small obstacle in the

@@ -171,6 +171,23 @@ class SW2Model:
                 out[i] = 0.0 if n < 1e-8 else math.pow(8.25 * math.sqrt(g) * n / kn, 6.0)
         return out
 
+    def initial_state(self):
+        """The state every time level starts from: the hot start (h0, u0, v0) with the Dirichlet
+        node strings' values imposed.  Restates the reference's hot-start reader, which forces the
+        initial condition to meet the Dirichlet boundary conditions and then starts the old and
+        older levels from it (``src/structs/ssw.c:452-545``); the series are taken at ``t0``."""
+        h, u, v = (np.array(a, dtype=np.float64) for a in (self.h0, self.u0, self.v0))
+        for sid, st in enumerate(self.strings):
+            if st.kind != "node" or st.bc_flag not in (BCT_PRS_DIR, BCT_VEL_DIR, BCT_VEL_PRS_DIR):
+                continue
+            nodes = self.node_string == sid
+            if st.bc_flag in (BCT_VEL_DIR, BCT_VEL_PRS_DIR):
+                u[nodes] = self.series[st.ivx].value_at(self.t0)
+                v[nodes] = self.series[st.ivy].value_at(self.t0)
+            if st.bc_flag in (BCT_PRS_DIR, BCT_VEL_PRS_DIR):
+                h[nodes] = self.series[st.iu0].value_at(self.t0)
+        return h, u, v
+
     def series_values(self, t1: float, t2: float) -> np.ndarray:
         """Step-averaged value of every BC series over [t1, t2]."""
         return np.array([s.value_avg(t1, t2) for s in self.series], dtype=np.float64)

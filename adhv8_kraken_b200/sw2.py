@@ -159,8 +159,9 @@ class SW2GPU:
         _check(lib().sw2gpu_load(self.h, C.byref(n), None, None, None, None))
         self.nnzb = n.value
         self.t = model.t0
+        h0, u0, v0 = model.initial_state()
         for lvl in range(3):
-            self.set_state(lvl, model.h0, model.u0, model.v0)
+            self.set_state(lvl, h0, u0, v0)
 
     def autotune(self):
         """Times the launch variants on this mesh and keeps the fastest; (jac_minb, stages)."""
@@ -430,7 +431,7 @@ class SW2Server:
         arrays = MeshArrays(model) if arrays is None else arrays
         params = solver_params(model, self.precision)
         ns, lens, ts, vs = _series_arrays(model)
-        h0, u0, v0 = (np.ascontiguousarray(a, dtype=np.float64) for a in (model.h0, model.u0, model.v0))
+        h0, u0, v0 = (np.ascontiguousarray(a, dtype=np.float64) for a in model.initial_state())
         rid = C.c_int64()
         _check(lib().sw2gpu_server_submit(self.h, C.byref(arrays.mesh), C.byref(params), _dp(h0), _dp(u0), _dp(v0),
                                           model.t0, model.dt if dt is None else dt, nsteps, ns,

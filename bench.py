@@ -259,8 +259,9 @@ def run_ensemble(models, stream, steps: int):
 
     def reset(gs):
         for g in gs:
+            h0, u0, v0 = g.model.initial_state()
             for lvl in range(3):
-                g.set_state(lvl, g.model.h0, g.model.u0, g.model.v0)
+                g.set_state(lvl, h0, u0, v0)
             g.t = g.model.t0
 
     def timed(fn):

@@ -86,9 +86,9 @@ class Oracle:
         self.V, self.T = model.nnodes, model.nelems2d
         self.nnzb = L.orc_nnzb(self.h)
         self.t = model.t0
-        self.set_state(0, model.h0, model.u0, model.v0)
-        self.set_state(1, model.h0, model.u0, model.v0)
-        self.set_state(2, model.h0, model.u0, model.v0)
+        h0, u0, v0 = model.initial_state()
+        for level in range(3):
+            self.set_state(level, h0, u0, v0)
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -25,6 +25,9 @@ Fixtures (numpy ``.npz``):
   recorded like ``ovh_ref.npz`` plus the grid mass diagnostics after every step.
 * ``obstacle_ref.npz`` -- the channel with a line of interior nodes held at zero velocity and 1 m
   depth (DB OVH node string), 6 steps, recorded like ``ovh_ref.npz``.
+* ``combined_ref.npz`` -- every supported feature at once on the wet/dry basin (all optional body
+  terms, rain, NB OVH inflow, NB OF outflow, a DB OVH node group), 6 steps, recorded like
+  ``rain_ref.npz``.
 * ``dacont_ref.npz`` -- the reference's transport side output elem_rhs_dacont_extra_terms
   (continuity parts of shock capturing and SUPG per element vertex) after steps 1, 4 and 8 of
   the basin run.
@@ -175,7 +178,8 @@ def mass():
 
 if __name__ == "__main__":
     import sys as _sys
-    which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "terms", "rain", "obstacle", "dacont", "mass"]
+    which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "terms", "rain", "obstacle", "combined", "dacont",
+                              "mass"]
     if "channel" in which:
         channel()
     if "basin" in which:
@@ -190,10 +194,12 @@ if __name__ == "__main__":
         ovh(meshgen.basin_rain(nsteps=6), "rain_ref.npz", mass=True)
     if "obstacle" in which:
         ovh(meshgen.channel_obstacle(nsteps=6, with_depth=True), "obstacle_ref.npz")
+    if "combined" in which:
+        ovh(meshgen.basin_combined(nsteps=6), "combined_ref.npz", mass=True)
     if "dacont" in which:
         dacont()
     if "mass" in which:
         mass()
     for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "terms_ref.npz", "rain_ref.npz",
-              "obstacle_ref.npz", "dacont_ref.npz", "mass_ref.npz"):
+              "obstacle_ref.npz", "combined_ref.npz", "dacont_ref.npz", "mass_ref.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -177,9 +177,11 @@ def _dirichlet_flags(m):
     return per_string[np.where(m.node_string >= 0, m.node_string, len(m.strings))]
 
 
-@pytest.mark.parametrize("case", ["all_terms", "terms_fixture", "rain", "obstacle"])
+@pytest.mark.parametrize("case", ["all_terms", "terms_fixture", "rain", "obstacle", "combined"])
 def test_device_physics_matches_oracle_on_host(host_physics, case):
-    if case == "terms_fixture":   # the all-terms reference fixture's model (EEV mode 3, southern Coriolis)
+    if case == "combined":
+        m = meshgen.basin_combined(nsteps=4)
+    elif case == "terms_fixture":   # the all-terms reference fixture's model (EEV mode 3, southern Coriolis)
         m = meshgen.basin_all_terms(nsteps=4)
     elif case == "rain":
         m = meshgen.basin_rain(nsteps=4)
@@ -206,7 +208,7 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
     h0 = levels[0][0]
     tri = m.tri
     dflag = _dirichlet_flags(m)
-    if case == "obstacle":   # every element holding a Dirichlet node
+    if case in ("obstacle", "combined"):   # every element holding a Dirichlet node
         fringe = np.nonzero((dflag[tri] != 0).any(axis=1))[0]
     else:                    # wet/dry fronts
         fringe = np.nonzero((wd != 0) | (h0[tri] <= 0.0).any(axis=1))[0]

@@ -111,7 +111,8 @@ def test_reruns_are_bitwise_identical():
 
 VARIANTS = {"ovh": meshgen.channel_ovh, "outflow": meshgen.channel_outflow, "terms": meshgen.basin_all_terms,
             "rain": meshgen.basin_rain,
-            "obstacle": lambda nsteps: meshgen.channel_obstacle(nsteps=nsteps, with_depth=True)}
+            "obstacle": lambda nsteps: meshgen.channel_obstacle(nsteps=nsteps, with_depth=True),
+            "combined": meshgen.basin_combined}
 
 
 @pytest.mark.parametrize("case", sorted(VARIANTS))
@@ -119,8 +120,8 @@ def test_boundary_and_term_variants_match_reference(case):
     """The reference fixtures of an inflow given as water elevation and velocity (NB OVH), a free
     outflow edge (NB OF), a wet/dry basin with every optional body term (temporal alpha, EVS /
     EEV 1-3 eddy viscosity, Coriolis), a water source (NB SOURCE) and interior nodes held by a
-    DB OVH string: residual and Jacobian at the first load, then 6 steps, each state within 1e-10
-    and Newton iterations within +-1."""
+    DB OVH string, and all of them at once on the wet/dry basin: residual and Jacobian at the
+    first load, then 6 steps, each state within 1e-10 and Newton iterations within +-1."""
     import os
     from conftest import GOLDEN
     from golden.make_golden import fingerprint

@@ -96,13 +96,15 @@ def test_oracle_grid_mass_matches_reference(case, mass_ref, basin_ref):
         assert abs(err - mass_ref[f"{case}_mass_error"][k - 1]) <= 1e-13 * mass0, k
 
 
-@pytest.mark.parametrize("case", ["ovh", "outflow", "terms", "rain", "obstacle"])
+@pytest.mark.parametrize("case", ["ovh", "outflow", "terms", "rain", "obstacle", "combined"])
 def test_oracle_boundary_variants_match_reference(case):
     """NB OVH inflow (elevation + velocity, fe_sw2_boundary_resid.c:398-440 with fe_sw2_1d_hvel),
     a free NB OF outflow edge (:227-240, fe_sw2_1d_implicit_flow), a wet/dry basin with every
     optional body term (temporal alpha, EVS / EEV 1-3 eddy viscosity, Coriolis) and one with a
     water source (NB SOURCE, fe_sw2_body_resid.c:728-754), and interior nodes held by a DB OVH node
-    string (values set at fe_sw2_init.c:37-85, rows zeroed at fe_sw2_body_resid.c:1239-1256):
+    string (values set at fe_sw2_init.c:37-85, rows zeroed at fe_sw2_body_resid.c:1239-1256), and
+    all of them at once on the wet/dry basin (with the Dirichlet values imposed on the hot start
+    as the reference's reader does, ssw.c:452-545):
     residual and FD Jacobian at the first load, then 6 steps (for the source, also the grid mass
     and the accumulated mass flux)."""
     import os
@@ -111,7 +113,8 @@ def test_oracle_boundary_variants_match_reference(case):
     ovh_ref = dict(np.load(os.path.join(GOLDEN, f"{case}_ref.npz")))
     m = {"ovh": meshgen.channel_ovh, "outflow": meshgen.channel_outflow,
          "terms": meshgen.basin_all_terms, "rain": meshgen.basin_rain,
-         "obstacle": lambda nsteps: meshgen.channel_obstacle(nsteps=nsteps, with_depth=True)}[case](nsteps=6)
+         "obstacle": lambda nsteps: meshgen.channel_obstacle(nsteps=nsteps, with_depth=True),
+         "combined": meshgen.basin_combined}[case](nsteps=6)
     assert str(ovh_ref["fingerprint"]) == fingerprint(m)
     o = Oracle(m)
     set_load_state(o, m, ovh_ref)
