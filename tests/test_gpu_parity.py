@@ -138,18 +138,20 @@ def test_boundary_and_term_variants_match_reference(case):
     _run_against(model, ref, 6, range(1, 7))
 
 
-@pytest.mark.parametrize("case", ["channel", "basin", "rain"])
+@pytest.mark.parametrize("case", ["channel", "basin", "rain", "combined"])
 def test_mass_balance_on_device_matches_reference(case, mass_ref, basin_ref):
     """The device's grid mass (tl_find_grid_mass_elem2d) and per-step mass flux (sources minus
     boundary outflow, tl_find_grid_mass_error_elem2d) at the reference's own state after every
     step, against the reference's values: the channel (inflow and tailwater edges), the wet/dry
-    basin (dry corners) and the basin with rain.  The device adds its terms in a fixed tree
+    basin (dry corners), the basin with rain, and the all-features basin (rain, NB OVH and NB OF
+    edges, Dirichlet nodes).  The device adds its terms in a fixed tree
     order, the reference in element order: 1e-12 relative to the initial mass."""
     import os
     from conftest import GOLDEN
     from golden.make_golden import fingerprint
-    if case == "rain":
-        model, ref = meshgen.basin_rain(nsteps=6), dict(np.load(os.path.join(GOLDEN, "rain_ref.npz")))
+    if case in ("rain", "combined"):
+        model = (meshgen.basin_rain if case == "rain" else meshgen.basin_combined)(nsteps=6)
+        ref = dict(np.load(os.path.join(GOLDEN, f"{case}_ref.npz")))
         assert str(ref["fingerprint"]) == fingerprint(model)
         dts, masses, totals, pre, src = ref["dt"], ref["mass"], ref["mass_flux_total"], "step", ref
         ref_mass0 = ref["mass0"][0]
