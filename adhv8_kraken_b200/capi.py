@@ -144,7 +144,7 @@ class MeshArrays:
         me.mat_coriolis = p([mt.coriolis for mt in m.materials], "f")
 
 
-def make_params(m: SW2Model, precision: int = SW2GPU_FP64, precond: int = SW2GPU_PREC_ILU0,
+def make_params(m: SW2Model, precision: int = SW2GPU_FP64, precond: int = SW2GPU_PREC_BJACOBI,
                 lin_rtol: float = 1e-5, lin_atol: float = 1e-10) -> Params:
     p = m.params
     out = Params()

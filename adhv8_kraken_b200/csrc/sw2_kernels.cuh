@@ -863,6 +863,70 @@ __global__ void k_dirichlet(const __grid_constant__ Src src) {
 }
 
 // ---------------------------------------------------------------------------------
+// Adaption error indicator (ssw_2d_calculate_elem_error, src/structs/ssw_2d.c:424-500), one
+// thread per element: the steady continuity residual at the vertices of the current level
+// against the old one, ((h_i - ho_i) / dt + u_i dh/dx + v_i dh/dy + h_i (du/dx + dv/dy))^2,
+// summed over the vertices, square root, times the area.  raw[e] keeps that value (the nodal
+// average below adds it); err[e] = raw / refine_tol[material], 0.5 for wd_flag > 0 (partially
+// wet elements are neither refined nor relaxed).  Every operation in the reference's order.
+__global__ void k_elem_error(const __grid_constant__ DevMesh m, const double* __restrict__ h,
+                             const double* __restrict__ ho, const double* __restrict__ u,
+                             const double* __restrict__ v, const int* __restrict__ wd, double dt,
+                             const double* __restrict__ refine_tol, double* __restrict__ raw,
+                             double* __restrict__ err) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.T) return;
+    const int n[3] = {m.en0[e], m.en1[e], m.en2[e]};
+    const double gx[3] = {m.gx0[e], m.gx1[e], m.gx2[e]}, gy[3] = {m.gy0[e], m.gy1[e], m.gy2[e]};
+    double hh[3], hp[3], uu[3], vv[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        hh[i] = h[n[i]];
+        hp[i] = ho[n[i]];
+        uu[i] = u[n[i]];
+        vv[i] = v[n[i]];
+    }
+    double dhdx = 0., dhdy = 0., dudx = 0., dvdy = 0.;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        dhdx += gx[i] * hh[i];
+        dhdy += gy[i] * hh[i];
+        dudx += gx[i] * uu[i];
+        dvdy += gy[i] * vv[i];
+    }
+    double c[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        double t = (hh[i] - hp[i]) / dt;
+        t += uu[i] * dhdx;
+        t += vv[i] * dhdy;
+        t += hh[i] * (dudx + dvdy);
+        c[i] = t * t;
+    }
+    const double r = sqrt(c[0] + c[1] + c[2]) * m.djac[e];
+    raw[e] = r;
+    err[e] = wd[e] > 0 ? 0.5 : r / refine_tol[m.emat[e]];
+}
+
+// its nodal average (:471-496): the raw values of a node's elements summed in element order
+// (the node's residual slots below 3T, which list its elements ascending) over their count
+__global__ void k_node_error(const __grid_constant__ DevMesh m, const double* __restrict__ raw,
+                             double* __restrict__ out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m.V) return;
+    double s = 0.;
+    int cnt = 0;
+    for (int k = m.slot_ptr[n]; k < m.slot_ptr[n + 1]; k++) {
+        const int q = m.slot_idx[k];
+        if (q < 3 * m.T) {
+            s += raw[q / 3];
+            cnt++;
+        }
+    }
+    out[n] = s / (double)cnt;
+}
+
+// ---------------------------------------------------------------------------------
 // Mass-balance diagnostics (src/tools/tl_grid_mass.c): per-block partial sums of the terms of
 // sw2_mass.cuh over a fixed grid, then one block adds the partials in block order, so a result
 // is the same on every run and every GPU.

@@ -28,6 +28,8 @@ constexpr int kKrylovRowThreads = 256;
 constexpr int kKrylovThreads = kKrylovRowThreads + 32;
 constexpr long long kBarrierSpinLimit = 1ll << 28;   // bounded wait (~seconds of polls), then error
 constexpr long long kMbarSpinLimit = 1ll << 20;      // polls of one tile copy's mbarrier, then error
+// a launch may bound its waits more tightly (KrylovArgs::spin_limit / copy_limit, 0 = these
+// defaults): failure-detection tests make a wait run out that way, without a fault
 constexpr int kStall = 40;                           // iterations without a new best residual
 constexpr int kRowLanes = 8;                         // lanes per node row in the SpMV sweeps
 constexpr int kTileRows = kKrylovRowThreads / kRowLanes;   // node rows per CTA tile (32)
@@ -71,7 +73,7 @@ struct KrylovCtl {
 // barrier of a launch is passed once the counter reaches b * nblocks (`epoch`, per CTA): the
 // last arrival releases everyone without a second atomic.  Returns false (and sets ctl->err)
 // if any block gave up; the caller then returns, so the kernel always terminates.
-__device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks, unsigned& epoch) {
+__device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks, unsigned& epoch, long long limit) {
     __syncthreads();
     if (threadIdx.x == 0) {
         epoch += nblocks;
@@ -84,7 +86,7 @@ __device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks, unsi
             unsigned cur;
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(&ctl->count) : "memory");
             if ((int)(cur - epoch) >= 0) break;
-            if (++spins > kBarrierSpinLimit || *(volatile int*)&ctl->err) {
+            if (++spins > limit || *(volatile int*)&ctl->err) {
                 atomicExch(&ctl->err, 1);
                 break;
             }
@@ -225,6 +227,8 @@ struct KrylovArgs {
                               // sweep (one grid barrier and one vector pass fewer per iteration,
                               // more vectors live: for launches whose vectors stay in L2); a batch
                               // launch decides for all its instances (KrylovTab::fuse)
+    long long spin_limit;     // polls of a grid-barrier wait before it gives up (0: kBarrierSpinLimit)
+    long long copy_limit;     // polls of a tile-copy wait before it gives up (0: kMbarSpinLimit)
 };
 
 // one instance of a Krylov launch
@@ -329,10 +333,26 @@ __device__ __forceinline__ unsigned long long policy_evict_first() {
 // orders this thread's view of global data written through the generic proxy (other CTAs'
 // stores before the last grid barrier) before its following bulk copies (async proxy)
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
-// bounded wait for the completion of the phase with the given parity
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+// bounded wait (at most `limit` polls) for the completion of the phase with the given parity.
+// A try_wait poll may itself suspend the thread for a hardware time window, long enough for a
+// tile copy to land; a limit below kShortWait polls with the non-blocking test_wait instead, so
+// that a short limit really bounds the wait (failure-detection tests).
+constexpr long long kShortWait = 64;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long limit) {
     const unsigned a = smem_addr(bar);
-    for (long long k = 0; k < kMbarSpinLimit; k++) {
+    if (limit < kShortWait) {
+        for (long long k = 0; k < limit; k++) {
+            unsigned done;
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                : "=r"(done)
+                : "r"(a), "r"(parity)
+                : "memory");
+            if (done) return true;
+        }
+        return false;
+    }
+    for (long long k = 0; k < limit; k++) {
         unsigned done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -469,6 +489,22 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     unsigned long long pol = 0;
     auto pbuf = [&]() { return K.part + (size_t)(nred & 1) * VG * 4; };
     auto stage = [&](unsigned c) { return stage_mem + (c % NST) * L.stage_bytes; };
+    const long long bar_limit = K.spin_limit > 0 ? K.spin_limit : kBarrierSpinLimit;
+    const long long copy_limit = K.copy_limit > 0 ? K.copy_limit : kMbarSpinLimit;
+    // Before a CTA leaves on an error, the bulk copies it issued must have landed in its shared
+    // memory: thread 0 waits (bounded by the default limit) for the last item of every ring
+    // stage.  The copy warp issues exactly the items the row warps consume, so tc counts both.
+    auto drain = [&]() {
+        if (STAGED && threadIdx.x == 0)
+            for (unsigned it = tc > (unsigned)NST ? tc - NST : 0u; it < tc; it++)
+                mbar_wait(&bar[it % NST], (it / NST) & 1u, kMbarSpinLimit);
+    };
+    // grid barrier; false (after draining the tile ring) when some CTA gave up: return at once
+    auto gsync = [&]() -> bool {
+        if (grid_sync(ctl, np, epoch, bar_limit)) return true;
+        drain();
+        return false;
+    };
 
     if (STAGED) {
         if (threadIdx.x == 0) {
@@ -502,6 +538,10 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                     for (int m = v; m < ntiles; m += VG, j++) {
                         const unsigned item = tc + j;
                         if (j >= NST) bar_sync_n(kBarEmpty + (int)(item % NST), kKrylovThreads);
+                        // the stage's previous copy has landed before it is refilled (the row warps
+                        // waited for it, unless their wait ran out): one copy per stage in flight
+                        if (issuer && item >= (unsigned)NST)
+                            mbar_wait(&bar[item % NST], ((item - NST) / NST) & 1u, kMbarSpinLimit);
                         if (issuer)
                             issue_tile<MT, VT>(m, V, K.rowptr, K.col, A, NV, vecs, stage(item), L, &bar[item % NST], pol);
                         __syncwarp();
@@ -517,23 +557,26 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                 const bool act = i < V;
                 VT y[3];
                 if (STAGED) {
-                    // a wait that runs out flags the error once; this thread then stops waiting,
-                    // the sweep finishes on stale data and the next barrier returns
-                    if (!wait_failed && !mbar_wait(&bar[tc % NST], (tc / NST) & 1u)) {
+                    // a wait that runs out flags the error once; this thread then stops waiting
+                    // and treats the rest of the sweep's rows as absent (a stage that may not have
+                    // landed is never read, so no index comes from stale shared memory), and the
+                    // next barrier returns
+                    if (!wait_failed && !mbar_wait(&bar[tc % NST], (tc / NST) & 1u, copy_limit)) {
                         wait_failed = true;
                         atomicExch(&ctl->err, 1);
                     }
+                    const bool use = act && !wait_failed;
                     const unsigned char* st = stage(tc);
                     const int* sR = (const int*)(st + L.r_off);
-                    const int k0 = sR[0];
+                    const int k0 = wait_failed ? 0 : sR[0];
                     const MT* sA = (const MT*)(st + ((unsigned long long)(A + (size_t)k0 * 9) & 15ull));
                     const int* sC = (const int*)(st + L.c_off + ((unsigned long long)(K.col + k0) & 15ull));
                     const VT* sV = (const VT*)(st + L.v_off);
-                    const int kb = act ? sR[li] : 0, ke = act ? sR[li + 1] : 0;
+                    const int kb = use ? sR[li] : 0, ke = use ? sR[li + 1] : 0;
                     row_apply<MT, VT>(
-                        act, lane8, kb, ke, [&](int k) { return sA + (size_t)(k - k0) * 9; },
+                        use, lane8, kb, ke, [&](int k) { return sA + (size_t)(k - k0) * 9; },
                         [&](int k) { return sC[k - k0]; }, gat, y);
-                    if (act && lane8 == 0)
+                    if (use && lane8 == 0)
                         epi(i, y, [&](int w, int c) { return sV[w * (tile_vec_bytes<VT>() / sizeof(VT)) + 3 * li + c]; });
                 } else {
                     const int kb = act ? __ldg(K.rowptr + i) : 0, ke = act ? __ldg(K.rowptr + i + 1) : 0;
@@ -565,7 +608,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
             U2[0][3 * i + c] = y;
         }
     }
-    if (!grid_sync(ctl, np, epoch)) return;
+    if (!gsync()) return;
     // r = b - M^-1 A u, q = r, p = r; norms and rho
     {
         double vals[4] = {0, 0, 0, 0};
@@ -600,7 +643,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                 block_partial<4>(vals, ism, pbuf(), v, red);
                 vals[0] = vals[1] = vals[2] = vals[3] = 0.0;
             });
-        if (!grid_sync(ctl, np, epoch)) return;
+        if (!gsync()) return;
         double rd[4];
         grid_allreduce<4>(pbuf(), VG, ism, rd, red);
         nred++;
@@ -702,7 +745,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                             g[0] = g[1] = 0.0;
                         });
                 }
-                if (!grid_sync(ctl, np, epoch)) return;
+                if (!gsync()) return;
                 if (!upd) {
                     grid_allreduce<1>(pbuf(), VG, gm, g, red);
                 } else {
@@ -749,7 +792,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                         block_partial<3>(w, wm, pbuf(), v, red);
                         w[0] = w[1] = w[2] = 0.0;
                     });
-                if (!grid_sync(ctl, np, epoch)) return;
+                if (!gsync()) return;
                 grid_allreduce<3>(pbuf(), VG, wm, w, red);
                 nred++;
                 omega = w[0] / w[1];
@@ -825,7 +868,7 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                     block_partial<1>(mx, mm, pbuf(), v, red);
                     mx[0] = 0.0;
                 }
-                if (!grid_sync(ctl, np, epoch)) return;
+                if (!gsync()) return;
                 grid_allreduce<1>(pbuf(), VG, mm, mx, red);
                 nred++;
                 rnorm = mx[0];

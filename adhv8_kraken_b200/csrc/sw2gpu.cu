@@ -102,6 +102,7 @@ struct sw2gpu_ctx {
     DBuf<double> str_value, str_uv;
     DBuf<double> mass_part;     // mass-balance partials (2 per block) and the result
     DBuf<double> dacont;        // [3][T] transport side output, allocated when first enabled
+    DBuf<double> errind;        // adaption error indicator: raw [T], scaled [T], nodal [V], tolerances [M]
     bool dacont_on = false;
     bool has_ovh = false;       // some edge string is NB OVH (its velocity series go up every step)
     DBuf<int> slot_ptr, slot_idx, blk_ptr, blk_src, rowptr, col, blk_row, dpos;
@@ -138,6 +139,9 @@ struct sw2gpu_ctx {
     // autotuned launch variants (sw2gpu_autotune): they change speed, never results
     int tune_jac_minb = 2;          // wet-Jacobian CTAs per SM the register budget is cut for
     int tune_stages = 3;            // Krylov tile-ring depth (0: sweeps from global memory)
+    // polls of a Krylov grid-barrier / tile-copy wait before it gives up (0: the library's
+    // defaults); sw2gpu_set_wait_limits
+    long long wait_barrier = 0, wait_copy = 0;
     DevMesh dm{};
     std::unique_ptr<Runner> self;   // runs this instance alone
     // CUDA graphs of a step's launch sequences (sw2gpu_set_graphs), one set per arrangement of
@@ -527,6 +531,8 @@ int runner_tables(Runner& R, int apply_inc) {
         A.ctl = R.ctl.p + k;
         A.vgrid = c->krylov_grid;
         A.fuse_update = krylov_fuse_update(c->V);   // alone; a batch launch decides for its group
+        A.spin_limit = c->wait_barrier;
+        A.copy_limit = c->wait_copy;
         Q.A = I.aoff;
         Q.Dinv = c->dinv64.p;
         for (int v = 0; v < kKrylovVectors; v++) Q.vec[v] = c->kv64[v].p;
@@ -899,6 +905,13 @@ void phase_times(Runner& R, double ph[3]) {
     }
 }
 
+// after a Krylov wait ran out: the instances back at their old level, the error text kept
+void reset_after_timeout(Runner& R, const std::vector<int>& sub) {
+    const std::string msg = g_err;
+    if (launch_init(R, sub) == 0) cudaStreamSynchronize(R.stream);
+    g_err = msg;
+}
+
 // One time step of every instance (fe_sw2 level shift + fe_newton), the instances in
 // lockstep: each Newton phase is one launch over the instances still iterating, and each
 // instance follows exactly the decisions it takes alone.
@@ -925,7 +938,12 @@ int runner_step(Runner& R, const double* dt, const double* const* series, sw2gpu
         for (int k = 0; k < K; k++)
             if (!ns[k].done) act.push_back(k);
         if (act.empty()) break;
-        if ((rc = newton_iteration(R, act, ns))) return rc;
+        if ((rc = newton_iteration(R, act, ns))) {
+            // a device wait that ran out ends the step like a failed one: every instance is
+            // back at its old level (fe_sw2_init) and the caller may step again
+            if (rc == SW2GPU_E_TIMEOUT) reset_after_timeout(R, all);
+            return rc;
+        }
     }
     std::vector<int> failed;
     for (int k = 0; k < K; k++) {
@@ -1043,7 +1061,10 @@ int graph_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* sta
         ns[0].old_l2 = ns[0].l2;
         CK(cudaGraphLaunch(G.newton, R.stream));
         R.launches += G.kernels_newton;
-        if ((rc = newton_finish(R, one, ns))) return rc;
+        if ((rc = newton_finish(R, one, ns))) {
+            if (rc == SW2GPU_E_TIMEOUT) reset_after_timeout(R, one);
+            return rc;
+        }
     }
     status[0] = newton_status(ns[0], c->p);
     if (status[0] != SW2GPU_OK && (rc = launch_init(R, one))) return rc;   // reset to the old level
@@ -1080,6 +1101,8 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     *out = nullptr;
     if (m->nnodes <= 0 || m->nelems2d < 0 || m->nelems1d < 0) return fail(SW2GPU_E_ARG, "bad mesh sizes");
     if (prm->precision != SW2GPU_FP64 && prm->precision != SW2GPU_MIXED) return fail(SW2GPU_E_ARG, "bad precision");
+    if (prm->precond != SW2GPU_PREC_BJACOBI)
+        return fail(SW2GPU_E_ARG, "preconditioner %d not built (SW2GPU_PREC_BJACOBI only)", prm->precond);
     int dev = 0;
     CK(cudaGetDevice(&dev));
     auto* c = new sw2gpu_ctx();
@@ -1391,6 +1414,15 @@ int sw2gpu_get_state(sw2gpu_ctx* c, int level, double* h, double* u, double* v) 
     return SW2GPU_OK;
 }
 
+int sw2gpu_snapshot(sw2gpu_ctx* c, int level, double* d_h, double* d_u, double* d_v) {
+    if (!c || level < 0 || level > 2) return fail(SW2GPU_E_ARG, "bad context or level");
+    const size_t nb = sizeof(double) * c->V;
+    if (d_h) CK(cudaMemcpyAsync(d_h, c->H(level), nb, cudaMemcpyDeviceToDevice, c->stream));
+    if (d_u) CK(cudaMemcpyAsync(d_u, c->U(level), nb, cudaMemcpyDeviceToDevice, c->stream));
+    if (d_v) CK(cudaMemcpyAsync(d_v, c->Vv(level), nb, cudaMemcpyDeviceToDevice, c->stream));
+    return SW2GPU_OK;
+}
+
 int sw2gpu_get_wd_flag(sw2gpu_ctx* c, int32_t* wd) {
     if (!c || !wd) return fail(SW2GPU_E_ARG, "null argument");
     if (c->T) CK(cudaMemcpyAsync(wd, c->wd.p, sizeof(int) * c->T, cudaMemcpyDeviceToHost, c->stream));
@@ -1436,6 +1468,34 @@ int sw2gpu_mass_flux(sw2gpu_ctx* c, double density, double* flux) {
     if (!c || !flux) return fail(SW2GPU_E_ARG, "bad context or output");
     if (!(c->dt > 0.0)) return fail(SW2GPU_E_ARG, "no step taken yet (dt unset)");
     return mass_reduce(c, true, c->H(0), density, flux);
+}
+
+int sw2gpu_elem_error(sw2gpu_ctx* c, const double* refine_tol, double* elem_error, double* node_error) {
+    if (!c || !refine_tol || !elem_error) return fail(SW2GPU_E_ARG, "null argument");
+    if (!(c->dt > 0.0)) return fail(SW2GPU_E_ARG, "no step taken yet (dt unset)");
+    const int T = c->T, V = c->V, M = std::max(c->M, 1);
+    if (!c->errind.p) {
+        g_alloc_bytes = &c->bytes;
+        const int rc = zalloc(c->errind, 2 * (size_t)T + V + M, c->stream);
+        g_alloc_bytes = nullptr;
+        if (rc) return rc;
+    }
+    double* raw = c->errind.p;
+    double* err = raw + T;
+    double* nod = err + T;
+    double* tol = nod + V;
+    if (c->M) CK(cudaMemcpyAsync(tol, refine_tol, sizeof(double) * c->M, cudaMemcpyHostToDevice, c->stream));
+    if (T) {
+        k_elem_error<<<nblk(T, 256), 256, 0, c->stream>>>(c->dm, c->H(0), c->H(1), c->U(0), c->Vv(0), c->wd.p, c->dt,
+                                                          tol, raw, err);
+        CK(cudaGetLastError());
+    }
+    k_node_error<<<nblk(V, 256), 256, 0, c->stream>>>(c->dm, raw, nod);
+    CK(cudaGetLastError());
+    if (T) CK(cudaMemcpyAsync(elem_error, err, sizeof(double) * T, cudaMemcpyDeviceToHost, c->stream));
+    if (node_error) CK(cudaMemcpyAsync(node_error, nod, sizeof(double) * V, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
 }
 
 int sw2gpu_set_dacont(sw2gpu_ctx* c, int32_t enable) {
@@ -1606,6 +1666,14 @@ int sw2gpu_autotune(sw2gpu_ctx* c, int32_t* jac_minb, int32_t* stages) {
     if (rc) return rc;
     if (jac_minb) *jac_minb = R.jac_minb;
     if (stages) *stages = R.stages;
+    return SW2GPU_OK;
+}
+
+int sw2gpu_set_wait_limits(sw2gpu_ctx* c, int64_t barrier_polls, int64_t copy_polls) {
+    if (!c || barrier_polls < 0 || copy_polls < 0) return fail(SW2GPU_E_ARG, "bad context or wait limit");
+    c->wait_barrier = barrier_polls;
+    c->wait_copy = copy_polls;
+    c->drop_graphs();   // the limits travel in the Krylov launch's parameters
     return SW2GPU_OK;
 }
 

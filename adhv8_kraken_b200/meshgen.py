@@ -259,12 +259,11 @@ def bumpy_basin(npoints: int, seed: int, size: float = 20000.0, slope: float = 5
     bin_n = np.sqrt(edges_b[:-1] * edges_b[1:])
     # boundary edges (west: inflow, east: tailwater), oriented as in the mesh
     tol = 1e-9 * size
-    ekey = {}
-    for (a, b, c) in tri:
-        for p, q in ((a, b), (b, c), (c, a)):
-            k = (min(p, q), max(p, q))
-            ekey[k] = ekey.get(k, 0) + 1
-    bedges = [k for k, cnt in ekey.items() if cnt == 1]
+    # edges used by one triangle only, as (min, max) node pairs
+    pairs = np.concatenate([tri[:, [0, 1]], tri[:, [1, 2]], tri[:, [2, 0]]])
+    pairs.sort(axis=1)
+    uniq, cnt = np.unique(pairs, axis=0, return_counts=True)
+    bedges = [(int(a), int(b)) for a, b in uniq[cnt == 1]]
     west = sorted([k for k in bedges if x[k[0]] < tol and x[k[1]] < tol], key=lambda k: y[k[0]] + y[k[1]])
     east = sorted([k for k in bedges if x[k[0]] > size - tol and x[k[1]] > size - tol],
                   key=lambda k: y[k[0]] + y[k[1]])

@@ -32,7 +32,8 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_last_tick", "sw2gpu_engine_destroy",
            "sw2gpu_device_bytes", "sw2gpu_autotune", "sw2gpu_set_graphs", "sw2gpu_set_variant", "sw2gpu_get_variant",
            "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
-           "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont"]
+           "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont",
+           "sw2gpu_set_wait_limits", "sw2gpu_snapshot", "sw2gpu_elem_error"]
 
 
 class SW2Error(RuntimeError):
@@ -81,6 +82,9 @@ def lib():
         L.sw2gpu_device_bytes.argtypes = [vp]
         L.sw2gpu_autotune.argtypes = [vp, c_int32_p, c_int32_p]
         L.sw2gpu_set_graphs.argtypes = [vp, C.c_int32]
+        L.sw2gpu_set_wait_limits.argtypes = [vp, C.c_int64, C.c_int64]
+        L.sw2gpu_snapshot.argtypes = [vp, C.c_int, vp, vp, vp]
+        L.sw2gpu_elem_error.argtypes = [vp, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_set_variant.argtypes = [vp, C.c_int32, C.c_int32]
         L.sw2gpu_get_variant.argtypes = [vp, c_int32_p, c_int32_p]
         L.sw2gpu_device_bytes.restype = C.c_int64
@@ -173,6 +177,10 @@ class SW2GPU:
         """Replay each step's launch sequences from CUDA graphs (small meshes)."""
         _check(lib().sw2gpu_set_graphs(self.h, 1 if enable else 0))
 
+    def set_wait_limits(self, barrier_polls: int = 0, copy_polls: int = 0):
+        """Bounds of the Krylov kernel's device waits in polls (0: the library's defaults)."""
+        _check(lib().sw2gpu_set_wait_limits(self.h, barrier_polls, copy_polls))
+
     def set_variant(self, jac_minb: int, stages: int):
         _check(lib().sw2gpu_set_variant(self.h, jac_minb, stages))
 
@@ -209,6 +217,11 @@ class SW2GPU:
         _check(lib().sw2gpu_get_state(self.h, level, _dp(h), _dp(u), _dp(v)))
         return h, u, v
 
+    def snapshot(self, level, d_h, d_u, d_v):
+        """Copies a time level into three device buffers (addresses of V doubles each, e.g.
+        torch tensors' data_ptr()), ordered on the context's stream, without waiting."""
+        _check(lib().sw2gpu_snapshot(self.h, level, C.c_void_p(d_h), C.c_void_p(d_u), C.c_void_p(d_v)))
+
     def get_wd(self):
         wd = np.zeros(self.T, np.int32)
         _check(lib().sw2gpu_get_wd_flag(self.h, _ip(wd)))
@@ -224,6 +237,14 @@ class SW2GPU:
         out = C.c_double()
         _check(lib().sw2gpu_grid_mass(self.h, level, rho, C.byref(out)))
         return out.value
+
+    def elem_error(self, refine_tol):
+        """Adaption error indicator of the last step (ssw_2d_calculate_elem_error), computed on the
+        device: (elem_error [T], node_error [V]); refine_tol per material."""
+        tol = np.ascontiguousarray(refine_tol, dtype=np.float64)
+        ee, ne = np.zeros(self.T), np.zeros(self.V)
+        _check(lib().sw2gpu_elem_error(self.h, _dp(tol), _dp(ee), _dp(ne)))
+        return ee, ne
 
     def mass_flux(self, density=None):
         """Mass that entered the grid during the last step (sources minus boundary outflow, the

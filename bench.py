@@ -322,22 +322,101 @@ def run_ensemble(models, stream, steps: int):
     gm = [SW2GPU(m, precision=capi.SW2GPU_MIXED, stream=stream.cuda_stream) for m in models]
     warm(gm, capi.SW2GPU_MIXED)
     ms, (done, fails, ticks, ph) = timed(lambda: engine(gm, capi.SW2GPU_MIXED))
-    eh = eq = 0.0
+    # error of every instance's final state against its batched FP64 run (h, uh, vh)
+    per_inst = []
     for g, ref in zip(gm, b64_state):
-        h, u, v = g.get_state(0)
-        eh = max(eh, float(np.abs(h - ref[0]).max() / max(np.abs(ref[0]).max(), 1e-300)))
-        dq = np.hypot(h * u - ref[0] * ref[1], h * v - ref[0] * ref[2])
-        eq = max(eq, float(dq.max() / max(np.hypot(ref[0] * ref[1], ref[0] * ref[2]).max(), 1e-300)))
+        per_inst.append(_rel_errs(*g.get_state(0), *ref))
+    worst = max(range(len(per_inst)), key=lambda k: max(per_inst[k].values()))
     out["batched_mixed"] = {"value": float(done / (ms * 1e-3)), "ms": ms, "failed_steps": int(fails), "ticks": ticks,
-                            "phase_ms": ph, "max_rel_err_vs_fp64": {"h": eh, "q": eq}}
+                            "phase_ms": ph,
+                            "max_rel_err_vs_fp64": {f: max(e[f] for e in per_inst) for f in ("h", "uh", "vh")},
+                            "rel_err_vs_fp64_per_instance": {f: [float("%.2e" % e[f]) for e in per_inst]
+                                                             for f in ("h", "uh", "vh")}}
     for g in gm:
         g.close()
+    # the worst instance traced step by step: it runs alone (an instance computes in the engine
+    # exactly what it computes alone) in FP64 and mixed, and its error after every step
+    m = models[worst]
+    trace = {}
+    for name, prec in (("fp64", capi.SW2GPU_FP64), ("mixed", capi.SW2GPU_MIXED)):
+        g = SW2GPU(m, precision=prec, stream=stream.cuda_stream)
+        states = []
+        run(g, steps, callback=lambda k, st, g=g, states=states: states.append(g.get_state(0)))
+        g.close()
+        trace[name] = states
+    out["batched_mixed"]["worst_instance"] = {
+        "index": worst, "triangles": int(m.nelems2d), "dt": float(m.dt),
+        "rel_err_vs_fp64_per_step": [{f: float("%.3e" % v) for f, v in _rel_errs(*a, *b).items()}
+                                     for a, b in zip(trace["mixed"], trace["fp64"])]}
     out["workload"] = (f"batched ensemble: {len(models)} seeded basins, triangles log-uniform 5k-200k "
                        f"(total {int(tri.sum())}), own bathymetry, Manning median U[0.015,0.05], inflow peak "
                        f"U[1,8] m^2/s, dt U[2,10] s; {steps} steps per instance")
     out["instances"] = len(models)
     out["triangles"] = int(tri.sum())
     out["steps"] = steps
+    return out
+
+
+def _rel_errs(hm, um, vm, h64, u64, v64):
+    """max |x - x_fp64| / max |x_fp64| for h, uh and vh (numpy or torch arrays)."""
+    out = {}
+    for name, a, b in (("h", hm, h64), ("uh", hm * um, h64 * u64), ("vh", hm * vm, h64 * v64)):
+        d = abs(a - b).max()
+        r = abs(b).max()
+        out[name] = float(d) / max(float(r), 1e-300)
+    return out
+
+
+def run_config3(stream, points: int, steps: int):
+    """Config 3: the mixed path at ~4M triangles (the 1M basin's generator at 2M points, the
+    domain scaled to keep the element size), `steps` steps of 5 s, against the plain FP64 path on
+    the same mesh step by step: the max relative h / uh / vh error per step.  The CPU reference
+    cannot run this size (about a day for 50 steps on one core), so the FP64 GPU path -- pinned
+    to the reference within 1e-10 per step on the same generator at 20k triangles -- is the FP64
+    reference here.  Each leg snapshots its state into device memory after every step
+    (sw2gpu_snapshot, 48 MB per step at 2M nodes, inside the timed region)."""
+    import torch
+    from adhv8_kraken_b200 import capi
+    from adhv8_kraken_b200.sw2 import SW2GPU
+    m = basin_model(points, steps + 8)
+    T, V = m.nelems2d, m.nnodes
+    dev = torch.device("cuda", torch.cuda.current_device())
+    snaps, out = {}, {}
+    for name, prec in (("fp64", capi.SW2GPU_FP64), ("mixed", capi.SW2GPU_MIXED)):
+        g = SW2GPU(m, precision=prec, stream=stream.cuda_stream)
+        variant = g.autotune()
+        buf = torch.empty((steps, 3, V), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stats = []
+        e0.record(stream)
+        for k in range(steps):
+            stats.append(g.step())
+            g.snapshot(0, buf[k, 0].data_ptr(), buf[k, 1].data_ptr(), buf[k, 2].data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        g.close()
+        assert all(st["status"] == 0 for st in stats), [st["status"] for st in stats]
+        snaps[name] = buf
+        out[name] = {"value": T * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                     "newton_its_per_step": sum(st["newton_its"] for st in stats) / steps,
+                     "krylov_its_per_step": sum(st["linear_its"] for st in stats) / steps,
+                     "variant": {"jac_minb": variant[0], "krylov_stages": variant[1]}}
+    a, b = snaps["mixed"], snaps["fp64"]
+    per = {"h": [], "uh": [], "vh": []}
+    for k in range(steps):
+        e = _rel_errs(a[k, 0], a[k, 1], a[k, 2], b[k, 0], b[k, 1], b[k, 2])
+        for f in per:
+            per[f].append(float("%.3e" % e[f]))
+    del snaps, a, b
+    torch.cuda.empty_cache()
+    out["max_rel_err_vs_fp64_per_step"] = per
+    out["max_rel_err_vs_fp64"] = {f: max(v) for f, v in per.items()}
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["workload"] = (f"mixed precision at scale: the 1M basin's generator at {points} points, {T} triangles, "
+                       f"{V} nodes, {steps} steps of 5 s from the hot start, FP64 and mixed on the same mesh")
+    out["triangles"], out["nodes"], out["steps"] = T, V, steps
     return out
 
 
@@ -541,6 +620,7 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
     if ens_models:
         batched = run_ensemble(ens_models, stream, args.ens_steps)
     small = run_small(stream) if world == 1 else None
+    config3 = run_config3(stream, args.c3_points, args.c3_steps) if (world == 1 and args.c3_points > 0) else None
     serving = None
     if serve:
         serving = run_serving(serve[0], serve[1], args.serve_rate)
@@ -574,6 +654,7 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
         "e2e": e2e,
         "mixed": mixed,
         "small": small,
+        "config3": config3,
         "batched": batched,
         "serving": serving,
         "cpu_baseline": cpu,
@@ -591,15 +672,32 @@ def main():
     ap.add_argument("--ref-points", type=int, default=10000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ens", type=int, default=256, help="batched-ensemble instances (0: skip the leg)")
-    ap.add_argument("--ens-steps", type=int, default=10, help="time steps per ensemble instance")
+    ap.add_argument("--ens-steps", type=int, default=50, help="time steps per ensemble instance")
+    ap.add_argument("--c3-points", type=int, default=2000000,
+                    help="config-3 mixed-precision leg: basin points (~2x triangles; 0: skip the leg)")
+    ap.add_argument("--c3-steps", type=int, default=50, help="config-3 time steps")
     ap.add_argument("--serve", type=int, default=24, help="serving-loop requests (0: skip the leg)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-horizon-scale", type=float, default=0.1,
                     help="horizons U{10..500} steps times this factor (1.0: the full horizons)")
     args = ap.parse_args()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # one process per GPU: launch the ranks (torchrun on this node, rendezvous on 127.0.0.1)
+        # and let their rank 0 print the line
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        sys.stderr.write(f"bench.py: --gpus {args.gpus} but WORLD_SIZE is {world}: run one rank per GPU "
+                         f"(torchrun --nproc-per-node {args.gpus}) or drop --gpus\n")
+        sys.exit(2)
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         return

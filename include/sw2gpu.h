@@ -59,7 +59,7 @@ extern "C" {
 
 /* preconditioners of the device Krylov solve */
 #define SW2GPU_PREC_BJACOBI  0   /* 3x3 block Jacobi */
-#define SW2GPU_PREC_ILU0     1   /* block ILU(0) on the BCSR pattern, colour-ordered */
+#define SW2GPU_PREC_ILU0     1   /* block ILU(0): not built; sw2gpu_create rejects it with SW2GPU_E_ARG */
 
 /* Mesh and model data (what fe_sw2_* read from SGRID / SMODEL).  Host pointers;
  * the library copies what it needs at create time. */
@@ -115,9 +115,9 @@ typedef struct sw2gpu_ctx sw2gpu_ctx;
 int         sw2gpu_abi_version(void);
 const char *sw2gpu_last_error(void);
 
-/* Builds the device mesh, element colouring and BCSR pattern (sw2gpu_prepare in the
- * reference-side adapter; call again after every mesh adaption).  `stream` is a
- * cudaStream_t (NULL = a stream owned by the context). */
+/* Builds the device mesh, the BCSR pattern and the reference-order gather lists of the
+ * atomic-free assembly (sw2gpu_prepare in the reference-side adapter; call again after every
+ * mesh adaption).  `stream` is a cudaStream_t (NULL = a stream owned by the context). */
 int sw2gpu_create(const sw2gpu_mesh *mesh, const sw2gpu_params *params, void *stream, sw2gpu_ctx **out);
 int sw2gpu_destroy(sw2gpu_ctx *ctx);
 /* Launch variants (no counterpart in the reference).  Two knobs change the speed of a step,
@@ -137,12 +137,30 @@ int sw2gpu_get_variant(const sw2gpu_ctx *ctx, int32_t *jac_minb, int32_t *stages
 int sw2gpu_set_graphs(sw2gpu_ctx *ctx, int32_t enable);
 /* device memory the context holds (bytes); no counterpart in the reference */
 int64_t sw2gpu_device_bytes(const sw2gpu_ctx *ctx);
+/* Bounds of the device waits (no counterpart in the reference, whose solver runs on one CPU
+ * thread): the Krylov kernel's grid barriers and its tile-copy waits give up after this many
+ * polls, set SW2GPU_E_TIMEOUT and return; the step then resets the current level to the old
+ * one, like a failed step, and the context stays usable.  0 = the library's defaults (2^28 and
+ * 2^20 polls, seconds and milliseconds).  Failure-detection tests set a few polls to make a
+ * wait run out without any fault. */
+int sw2gpu_set_wait_limits(sw2gpu_ctx *ctx, int64_t barrier_polls, int64_t copy_polls);
 
 /* State of time level `level` (0 = current t+dt iterate, 1 = old, 2 = older);
- * SW2 state is (head, vel.x, vel.y) as in src/structs/ssw_2d.h:13-18. */
+ * SW2 state is (head, vel.x, vel.y) as in src/structs/ssw_2d.h:13-18.  The library takes the
+ * levels as given: a caller starting from a hot start passes levels with the Dirichlet node
+ * values (DB OVH / OVL strings) already imposed on all three, as the reference's reader does
+ * (src/structs/ssw.c:452-545); a raw hot start whose held depth differs from it gives results
+ * that differ from the reference from the first Jacobian on. */
 int sw2gpu_set_state(sw2gpu_ctx *ctx, int level, const double *h, const double *u, const double *v);
 int sw2gpu_get_state(sw2gpu_ctx *ctx, int level, double *h, double *u, double *v);
 int sw2gpu_get_wd_flag(sw2gpu_ctx *ctx, int32_t *wd_flag);
+/* On-device output snapshot (for callers that keep their output on the GPU instead of writing
+ * it through the host each step, as the reference's smodel_print_ts does,
+ * src/structs/smodel.c:697): copies time level `level` into caller-owned DEVICE buffers of
+ * nnodes doubles each (NULL skips a field).  The copies are ordered on the context's stream and
+ * the call does not wait for them: they are complete once that stream has reached them (any
+ * later blocking call of the library, or the caller's own synchronization of the stream). */
+int sw2gpu_snapshot(sw2gpu_ctx *ctx, int level, double *d_h, double *d_u, double *d_v);
 /* Overrides the element wet/dry flags (normally set by the step's fe_sw2_init). */
 int sw2gpu_set_wd_flag(sw2gpu_ctx *ctx, const int32_t *wd_flag);
 
@@ -156,6 +174,15 @@ int sw2gpu_set_wd_flag(sw2gpu_ctx *ctx, const int32_t *wd_flag);
  * |mass - total - initial mass|).  Uses the last step's dt and series values.
  * Both add their terms in a fixed order: the same bits on every run and every GPU. */
 int sw2gpu_grid_mass(sw2gpu_ctx *ctx, int level, double density, double *mass);
+/* Adaption error indicator of the last step, on the device (ssw_2d_calculate_elem_error,
+ * src/structs/ssw_2d.c:424-500, which fe_main calls after every accepted SW2 step and
+ * adpt_main / error_main read, src/grid/error_main.c:2): per element the square root of the
+ * summed squared steady continuity residuals at its vertices (current level against the old one,
+ * the last step's dt) times its area, divided by refine_tol[material] (the reference's
+ * refine_tolerance, MP SRT; one value per material id of the mesh), and 0.5 for elements with
+ * wd_flag > 0.  elem_error[nelems2d]; node_error[nnodes] (may be NULL) the unscaled element
+ * values averaged over each node's elements, the reference's sw->error. */
+int sw2gpu_elem_error(sw2gpu_ctx *ctx, const double *refine_tol, double *elem_error, double *node_error);
 int sw2gpu_mass_flux(sw2gpu_ctx *ctx, double density, double *flux);
 
 /* Transport side output elem_rhs_dacont_extra_terms (src/fe/sw2/fe_sw2_body_resid.c:353-355,
@@ -198,7 +225,9 @@ int sw2gpu_linear_solve(sw2gpu_ctx *ctx, const double *val, const double *rhs, d
  * ||r||inf <= atol + rtol ||M^-1 S rhs||inf.  Its only work memory is one file-scope device
  * array of about 16.7 MB that every GPU loading the library keeps until exit, so systems
  * above SW2GPU_NOALLOC_MAX_NODES rows or SW2GPU_NOALLOC_MAX_BLOCKS blocks are rejected with
- * SW2GPU_E_ARG.  The first call on a device looks up that array's device address (make it
+ * SW2GPU_E_ARG.  The block structure is checked before the array is written: row_ptr[0] = 0,
+ * row_ptr[nnodes] = nnzb, ordered row ranges, column indices in [0, nnodes) and exactly one
+ * diagonal block per row, else SW2GPU_E_ARG.  The first call on a device looks up that array's device address (make it
  * before any stream capture).  All calls share the array: calls that overlap on the GPU
  * race and corrupt each other.  Returns SW2GPU_E_LINEAR if max_it is reached. */
 #define SW2GPU_NOALLOC_MAX_NODES  16384

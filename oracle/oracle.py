@@ -56,6 +56,7 @@ def lib():
         L.orc_geometry.argtypes = [C.c_void_p, C.c_int, c_double_p]
         L.orc_get_dacont.argtypes = [C.c_void_p, c_double_p]
         L.orc_edge_resid.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, c_double_p, c_double_p]
+        L.orc_elem_error.argtypes = [C.c_void_p, c_double_p, c_double_p, c_double_p]
         L.orc_grid_mass.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.orc_grid_mass.restype = C.c_double
         L.orc_mass_flux.argtypes = [C.c_void_p, C.c_double, C.c_double, c_double_p]
@@ -168,6 +169,14 @@ class Oracle:
         out = np.zeros(7)
         lib().orc_geometry(self.h, ie, _dp(out))
         return out[0], out[1:]
+
+    def elem_error(self, refine_tol):
+        """Adaption error indicator (ssw_2d_calculate_elem_error) of the current and old levels
+        and the last dt: (elem_error [T], node_error [V]); refine_tol per material."""
+        tol = np.ascontiguousarray(refine_tol, dtype=np.float64)
+        ee, ne = np.zeros(self.T), np.zeros(self.V)
+        lib().orc_elem_error(self.h, _dp(tol), _dp(ee), _dp(ne))
+        return ee, ne
 
     def grid_mass(self, level=0, density=None):
         """Water mass of a time level (tl_find_grid_mass_elem2d)."""

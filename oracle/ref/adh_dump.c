@@ -20,7 +20,11 @@
  *            the current grid mass, tl_find_grid_mass_error_elem2d and its accumulated
  *            boundary / source mass flux;
  *   "dacont" when ADH_DUMP_DACONT is set, after every accepted step (after "mass"): the
- *            side output sw->d2->elem_rhs_dacont_extra_terms[3][nelems2d], vertex-major.
+ *            side output sw->d2->elem_rhs_dacont_extra_terms[3][nelems2d], vertex-major;
+ *   "elemerr", "nodeerr" when ADH_DUMP_ERROR is set, after every accepted step (after
+ *            "dacont"): the adaption error indicator fe_main computed for the step
+ *            (ssw_2d_calculate_elem_error, src/structs/ssw_2d.c:424-500), grid->elem_error
+ *            per element and its nodal average sw->error.
  *
  * Record layout: char tag[8]; int32 kind (0 = f64, 1 = i32); int64 count; data.
  */
@@ -44,6 +48,7 @@ static int it_mark = 0;
 static double solve_seconds = 0.0;   /* fe_main wall time since the last accepted step */
 static int dump_mass = 0;            /* ADH_DUMP_MASS set */
 static int dump_dacont = 0;          /* ADH_DUMP_DACONT set */
+static int dump_error = 0;           /* ADH_DUMP_ERROR set */
 static int mass_ready = 0;
 static double mass0 = 0.0, mass_flux_total = 0.0;
 
@@ -62,6 +67,7 @@ static void dump_open(void) {
     dump_loads_left = nl ? atoi(nl) : 0;
     dump_mass = getenv("ADH_DUMP_MASS") != NULL;
     dump_dacont = getenv("ADH_DUMP_DACONT") != NULL;
+    dump_error = getenv("ADH_DUMP_ERROR") != NULL;
 }
 
 static void put_f64(const char *tag, const double *v, long n) {
@@ -144,6 +150,10 @@ int __wrap_fe_main(SSUPER_MODEL *sm) {
                 for (e = 0; e < T; e++) d[(size_t) i * T + e] = mod->sw->d2->elem_rhs_dacont_extra_terms[i][e];
             put_f64("dacont", d, 3L * T);
             free(d);
+        }
+        if (dump_error) {
+            put_f64("elemerr", mod->grid->elem_error, mod->grid->nelems2d);
+            put_f64("nodeerr", mod->sw->d2->error, n);
         }
         fflush(dump_fp);
         attempts = 0;

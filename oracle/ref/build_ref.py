@@ -22,9 +22,20 @@ of the reference tree and its build system is not used; the recipe is:
    groundwater, sediment coupling or ADCIRC winds are left out.
 3. The objects are linked with the observation harness ``adh_dump.c`` and
    ``--wrap=fe_main --wrap=fe_sw2_load`` into ``oracle/_ref/adh_dump``.
+4. The same objects, the same harness and the drop-in binding of the B200 library
+   (``adhv8_kraken_b200/adapter/fe_sw2_solve_gpu.c``, compiled against the reference's own
+   headers) are linked with ``--wrap=fe_sw2_solve --wrap=ssw_2d_calculate_elem_error`` against
+   ``libsw2gpu.so`` into
+   ``oracle/_ref/adh_gpu``: the reference's own executable and time loop with its SW2 solve
+   replaced by the GPU step.  Only where the library is built.
+5. The reference's SW2 QA decks that run on triangles (``qa/sw2/<case>/tri``: mesh, boundary
+   cards, hot start and the stored ``error.out.last``) are staged into ``oracle/_ref/qa`` so
+   that the drop-in can run them where the reference tree is absent.
 
-Usage: ``python oracle/ref/build_ref.py [REFERENCE_SRC]`` (default
-``/root/reference/src``).  Re-running only rebuilds missing objects.
+Usage: ``python oracle/ref/build_ref.py [REFERENCE_SRC]``.  The reference's ``src`` directory
+is the argument, else the environment variable ``ADH_REFERENCE_SRC``, else a checkout of the
+reference beside this repository (``../reference/src`` from the repository root).  Re-running
+only rebuilds missing objects.
 """
 from __future__ import annotations
 
@@ -93,7 +104,8 @@ def _sources(src: str):
     return sorted(set(srcs))
 
 
-REFERENCE_SRC = "/root/reference/src"
+REFERENCE_SRC = os.environ.get("ADH_REFERENCE_SRC") or os.path.normpath(
+    os.path.join(HERE, "..", "..", "..", "reference", "src"))
 
 
 def sources_present(src: str = REFERENCE_SRC) -> bool:
@@ -130,7 +142,44 @@ def build(src: str = REFERENCE_SRC, jobs: int = os.cpu_count() or 4) -> str:
     subprocess.run(["gcc", "-c"] + flags + [harness, "-o", hobj], check=True, capture_output=True)
     subprocess.run(["gcc", "-fcommon", "-o", exe] + objs + [hobj, stub, "-lm",
                     "-Wl,--wrap=fe_main", "-Wl,--wrap=fe_sw2_load"], check=True)
+    stage_qa(src)
+    lib = os.path.join(REPO, "adhv8_kraken_b200", "libsw2gpu.so")
+    if os.path.exists(lib):
+        build_gpu_harness(flags, objs, hobj, stub, lib)
     return exe
+
+
+REPO = os.path.normpath(os.path.join(HERE, "..", ".."))
+GPU_EXE = os.path.join(OUT, "adh_gpu")
+QA_CASES = ["wet_dry", "angle_nb", "angle_source", "angle_dam", "angle_coriolis"]
+
+
+def build_gpu_harness(flags, objs, hobj, stub, lib) -> str:
+    """The reference executable with fe_sw2_solve bound to the B200 library (step 4)."""
+    adapter = os.path.join(REPO, "adhv8_kraken_b200", "adapter", "fe_sw2_solve_gpu.c")
+    aobj = os.path.join(OUT, "obj", "fe_sw2_solve_gpu.o")
+    subprocess.run(["gcc", "-c"] + flags + [f"-I{os.path.join(REPO, 'include')}", adapter, "-o", aobj], check=True)
+    libdir = os.path.dirname(lib)
+    rpath = "$ORIGIN/" + os.path.relpath(libdir, OUT)
+    subprocess.run(["gcc", "-fcommon", "-o", GPU_EXE] + objs + [hobj, aobj, stub, f"-L{libdir}", "-lsw2gpu", "-lm",
+                    f"-Wl,-rpath,{rpath}", "-Wl,--wrap=fe_main", "-Wl,--wrap=fe_sw2_load",
+                    "-Wl,--wrap=fe_sw2_solve", "-Wl,--wrap=ssw_2d_calculate_elem_error"], check=True)
+    return GPU_EXE
+
+
+def stage_qa(src: str) -> str:
+    """Copies the SW2 QA decks on triangles into oracle/_ref/qa/<case> (step 5)."""
+    import shutil
+    qa = os.path.normpath(os.path.join(src, "..", "qa", "sw2"))
+    dst = os.path.join(OUT, "qa")
+    for case in QA_CASES:
+        d = os.path.join(dst, case)
+        if os.path.isdir(os.path.join(qa, case, "tri")) and not os.path.isdir(d):
+            shutil.copytree(os.path.join(qa, case, "tri"), d)
+            os.chmod(d, 0o755)
+            for f in os.listdir(d):
+                os.chmod(os.path.join(d, f), 0o644)
+    return dst
 
 
 if __name__ == "__main__":

@@ -56,6 +56,10 @@ def parse(recs) -> Dict[str, list]:
             if i < len(recs) and recs[i][0] == "dacont":   # elem_rhs_dacont_extra_terms [3][T]
                 steps[-1]["dacont"] = recs[i][1].reshape(3, -1)
                 i += 1
+            if i + 1 < len(recs) and recs[i][0] == "elemerr":   # adaption error indicator
+                steps[-1]["elem_error"] = recs[i][1]
+                steps[-1]["node_error"] = recs[i + 1][1]
+                i += 2
         elif tag == "load":
             d = dict(t=arr[0], dt=arr[1])
             j = i + 1
@@ -70,10 +74,11 @@ def parse(recs) -> Dict[str, list]:
 
 
 def run_reference(model, nsteps=None, loads: int = 0, workdir: str = None, timeout: float = 3600.0,
-                  mass: bool = False, dacont: bool = False):
+                  mass: bool = False, dacont: bool = False, error: bool = False):
     """Run the reference on ``model``; returns parsed records and the wall time (s).  mass: also
     record the reference's grid mass diagnostics after every step; dacont: its transport side
-    output elem_rhs_dacont_extra_terms."""
+    output elem_rhs_dacont_extra_terms; error: its adaption error indicator (elem_error per
+    element and its nodal average)."""
     if not os.path.exists(EXE):
         raise FileNotFoundError("oracle/_ref/adh_dump is not built (python oracle/ref/build_ref.py)")
     tmp = workdir or tempfile.mkdtemp(prefix="adhref_")
@@ -84,6 +89,8 @@ def run_reference(model, nsteps=None, loads: int = 0, workdir: str = None, timeo
             env["ADH_DUMP_MASS"] = "1"
         if dacont:
             env["ADH_DUMP_DACONT"] = "1"
+        if error:
+            env["ADH_DUMP_ERROR"] = "1"
         t0 = time.perf_counter()
         r = subprocess.run([EXE, "m"], cwd=tmp, env=env, capture_output=True, text=True, timeout=timeout)
         wall = time.perf_counter() - t0

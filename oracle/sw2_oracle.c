@@ -1496,3 +1496,48 @@ double orc_mass_flux(const orc_ctx *C, double density, double dt, const double *
     }
     return body + edge;
 }
+
+/* ------------------------------------------------------------------------------ */
+/* Adaption error indicator (ssw_2d_calculate_elem_error, src/structs/ssw_2d.c:424-500):
+ * per element the steady continuity residual at the vertices, ((h_i - h_old_i) / dt +
+ * u_i dh/dx + v_i dh/dy + h_i (du/dx + dv/dy))^2, summed over the three vertices, square root,
+ * times the area; elem_error = that / refine_tol[material] (0.5 for an element with wd_flag > 0);
+ * node_error = the unscaled element values averaged over each node's elements (:471-496).  The
+ * state is level 0 (the step's result) and level 1 (its old level), dt the step's. */
+void orc_elem_error(const orc_ctx *C, const double *refine_tol, double *elem_error, double *node_error) {
+    int e, i;
+    int *cnt = (int *) calloc((size_t) C->V, sizeof(int));
+    for (i = 0; i < C->V; i++) node_error[i] = 0.;
+    for (e = 0; e < C->T; e++) {
+        const int *n = C->tri + 3 * e;
+        const double *g = C->grad + 6 * e;
+        double hh[3], ho[3], uu[3], vv[3], c[3];
+        double dhdx = 0., dhdy = 0., dudx = 0., dvdy = 0.;
+        for (i = 0; i < 3; i++) {
+            hh[i] = C->h[0][n[i]]; ho[i] = C->h[1][n[i]]; uu[i] = C->u[0][n[i]]; vv[i] = C->v[0][n[i]];
+        }
+        for (i = 0; i < 3; i++) {
+            dhdx += g[2 * i] * hh[i];
+            dhdy += g[2 * i + 1] * hh[i];
+            dudx += g[2 * i] * uu[i];
+            dvdy += g[2 * i + 1] * vv[i];
+        }
+        for (i = 0; i < 3; i++) {
+            c[i] = (hh[i] - ho[i]) / C->dt;
+            c[i] += uu[i] * dhdx;
+            c[i] += vv[i] * dhdy;
+            c[i] += hh[i] * (dudx + dvdy);
+            c[i] = c[i] * c[i];
+        }
+        double err = sqrt(c[0] + c[1] + c[2]) * C->djac[e];
+        for (i = 0; i < 3; i++) {
+            node_error[n[i]] += err;
+            cnt[n[i]] += 1;
+        }
+        err /= refine_tol[C->tri_mat[e]];
+        elem_error[e] = err;
+        if (C->wd[e] > 0) elem_error[e] = 0.5;
+    }
+    for (i = 0; i < C->V; i++) node_error[i] /= (double) cnt[i];
+    free(cnt);
+}

@@ -31,6 +31,13 @@ Fixtures (numpy ``.npz``):
 * ``dacont_ref.npz`` -- the reference's transport side output elem_rhs_dacont_extra_terms
   (continuity parts of shock capturing and SUPG per element vertex) after steps 1, 4 and 8 of
   the basin run.
+* ``scale_ref.npz`` -- the generator of the 1M-triangle benchmark basin (seed 2024, 32 Manning
+  bins, 40 bumps with dry tops, inflow ramp 1 -> 5 m^2/s over 30 steps, dt 5 s) at 10k points
+  (~20k triangles, the domain scaled to keep the element size), 10 steps: Newton iterations,
+  state and wd flags after every step.
+* ``errind_ref.npz`` -- the reference's adaption error indicator (ssw_2d_calculate_elem_error,
+  src/structs/ssw_2d.c:424-500: grid->elem_error and its nodal average) after steps 1, 4 and 8
+  of the basin run, whose states are in ``basin_ref.npz``.
 * ``mass_ref.npz`` -- the reference's grid mass diagnostics (src/tools/tl_grid_mass.c) after
   every step of 6 channel steps and of the 8 basin steps: initial and current mass, mass error
   and accumulated mass flux, with the channel's state after every step (the basin's states are
@@ -153,6 +160,40 @@ def ovh(m=None, fname="ovh_ref.npz", mass=False):
     np.savez_compressed(os.path.join(HERE, fname), **out)
 
 
+def scale_model(nsteps=10):
+    """The benchmark basin's generator at 10k points (bench.py scales the domain with the
+    square root of the point count, so the element size is that of the 1M-triangle mesh)."""
+    import math
+    points = 10000
+    return meshgen.bumpy_basin(points, seed=2024, size=20000.0 * math.sqrt(points / 5e5), nsteps=nsteps, dt=5.0,
+                               name="scale")
+
+
+def scale():
+    m = scale_model()
+    ref = run_reference(m, nsteps=10)
+    out = {"fingerprint": np.array(fingerprint(m)),
+           "newton_its": np.array([s["newton_its"] for s in ref["steps"]], np.int32),
+           "attempts": np.array([s["attempts"] for s in ref["steps"]], np.int32),
+           "t": np.array([s["t"] for s in ref["steps"]]), "dt": np.array([s["dt"] for s in ref["steps"]]),
+           "op_blk": np.array(m.params.nblock, np.int32)}
+    for k, s in enumerate(ref["steps"], 1):
+        out[f"step{k}_h"], out[f"step{k}_u"], out[f"step{k}_v"] = s["h"], s["u"], s["v"]
+        out[f"step{k}_wd"] = s["wd"].astype(np.int8)
+    np.savez_compressed(os.path.join(HERE, "scale_ref.npz"), **out)
+
+
+def errind():
+    m = basin_model()
+    ref = run_reference(m, nsteps=8, error=True)
+    out = {"fingerprint": np.array(fingerprint(m))}
+    for k in (1, 4, 8):
+        out[f"step{k}_elem_error"] = ref["steps"][k - 1]["elem_error"]
+        out[f"step{k}_node_error"] = ref["steps"][k - 1]["node_error"]
+        out[f"step{k}_h"] = ref["steps"][k - 1]["h"]
+    np.savez_compressed(os.path.join(HERE, "errind_ref.npz"), **out)
+
+
 def dacont():
     m = basin_model()
     ref = run_reference(m, nsteps=8, dacont=True)
@@ -179,7 +220,7 @@ def mass():
 if __name__ == "__main__":
     import sys as _sys
     which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "terms", "rain", "obstacle", "combined", "dacont",
-                              "mass"]
+                              "mass", "scale", "errind"]
     if "channel" in which:
         channel()
     if "basin" in which:
@@ -200,6 +241,12 @@ if __name__ == "__main__":
         dacont()
     if "mass" in which:
         mass()
+    if "scale" in which:
+        scale()
+    if "errind" in which:
+        errind()
     for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "terms_ref.npz", "rain_ref.npz",
-              "obstacle_ref.npz", "combined_ref.npz", "dacont_ref.npz", "mass_ref.npz"):
-        print(f, os.path.getsize(os.path.join(HERE, f)))
+              "obstacle_ref.npz", "combined_ref.npz", "dacont_ref.npz", "mass_ref.npz", "scale_ref.npz",
+              "errind_ref.npz"):
+        if os.path.exists(os.path.join(HERE, f)):
+            print(f, os.path.getsize(os.path.join(HERE, f)))

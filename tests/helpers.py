@@ -12,6 +12,15 @@ def basin_model():
     return meshgen.bumpy_basin(700, seed=11, size=2000.0, nsteps=8, dt=5.0, nbins=3, name="basin")
 
 
+def scale_model(nsteps=10):
+    """The 1M-triangle benchmark basin's generator at 10k points (~20k triangles, the domain
+    scaled like bench.py does, so the element size is the benchmark's)."""
+    import math
+    points = 10000
+    return meshgen.bumpy_basin(points, seed=2024, size=20000.0 * math.sqrt(points / 5e5), nsteps=nsteps, dt=5.0,
+                               name="scale")
+
+
 def set_load_state(solver, model, ref, prefix="load0"):
     """Puts a solver (oracle or GPU) in the state the reference built its Jacobian at."""
     solver.set_state(0, ref[f"{prefix}_h"], ref[f"{prefix}_u"], ref[f"{prefix}_v"])

@@ -119,3 +119,36 @@ def test_create_rejects_unsupported_node_strings(what):
     with pytest.raises(SW2Error) as err:
         SW2GPU(m)
     assert err.value.code == capi.SW2GPU_E_ARG
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("stages,barrier_polls,copy_polls", [(0, 1, 0), (3, 0, 1)])
+def test_device_wait_that_runs_out_ends_the_step_with_timeout(stages, barrier_polls, copy_polls):
+    """A Krylov grid-barrier wait (direct sweeps) or tile-copy wait (staged sweeps) bounded to
+    one poll runs out: no fault, no hang -- the kernel flags the error and returns, the step
+    reports SW2GPU_E_TIMEOUT with the current level reset to the old one, and once the limits
+    are back at their defaults the same context steps on exactly as a context that never
+    timed out."""
+    m = _basin(n=10000, seed=23, nsteps=4)   # ~20k triangles: hundreds of Krylov CTAs
+    g = SW2GPU(m)
+    ref = SW2GPU(m)
+    for s in (g, ref):
+        s.set_variant(1, stages)
+    g.set_wait_limits(barrier_polls, copy_polls)
+    with pytest.raises(SW2Error) as ei:
+        g.step()
+    assert ei.value.code == capi.SW2GPU_E_TIMEOUT
+    h, u, v = g.get_state(0)
+    h1, u1, v1 = g.get_state(1)
+    assert np.array_equal(h, h1) and np.array_equal(u, u1) and np.array_equal(v, v1)
+    # the same levels in both contexts, then one step each
+    for lvl in range(3):
+        g.set_state(lvl, *ref.get_state(lvl))
+    g.set_wait_limits(0, 0)
+    a, b = g.step(), ref.step()
+    assert a["status"] == 0 and b["status"] == 0
+    for x, y in zip(g.get_state(0), ref.get_state(0)):
+        assert np.array_equal(x, y)
+    g.close()
+    ref.close()
+

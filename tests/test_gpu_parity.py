@@ -8,7 +8,7 @@ import pytest
 from adhv8_kraken_b200 import capi, meshgen
 from adhv8_kraken_b200.sw2 import SW2Error, SW2GPU, run
 from conftest import relerr
-from helpers import basin_model, channel_model, field_errors, fields, set_load_state
+from helpers import basin_model, channel_model, field_errors, fields, scale_model, set_load_state
 from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -96,6 +96,37 @@ def test_basin_run_matches_reference(basin_ref):
 
 def test_mixed_precision_channel_within_1e8(channel_ref):
     _run_against(channel_model(), channel_ref, 20, (1, 5, 10, 20), precision=capi.SW2GPU_MIXED, tol=1e-8)
+
+
+@pytest.fixture(scope="module")
+def scale_ref():
+    import os
+    from conftest import GOLDEN
+    return dict(np.load(os.path.join(GOLDEN, "scale_ref.npz")))
+
+
+def _scale_model_checked(ref):
+    from golden.make_golden import fingerprint
+    m = scale_model()
+    assert str(ref["fingerprint"]) == fingerprint(m)   # the generator still makes the recorded problem
+    return m
+
+
+def test_bench_generator_basin_fp64_matches_reference_every_step(scale_ref):
+    """The benchmark's own generator (seed 2024, 32 Manning bins, 40 bumps with dry tops, inflow
+    ramp) at ~20k triangles against the reference over 10 steps: plain FP64 within 1e-10 per
+    step in depth and unit discharge, Newton iterations within +-1, identical wet/dry flags."""
+    m = _scale_model_checked(scale_ref)
+    worst = _run_against(m, scale_ref, 10, range(1, 11), wd=True)
+    assert worst <= 1e-10
+
+
+def test_bench_generator_basin_mixed_matches_reference_every_step(scale_ref):
+    """The mixed path (FP32 Jacobian storage, SpMV and preconditioner inside the FP64 Newton
+    loop) on the same problem, against the reference's states (not against the GPU's own FP64
+    run): within 1e-8 per step, Newton iterations within +-1."""
+    m = _scale_model_checked(scale_ref)
+    _run_against(m, scale_ref, 10, range(1, 11), precision=capi.SW2GPU_MIXED, tol=1e-8)
 
 
 def test_reruns_are_bitwise_identical():
@@ -197,3 +228,30 @@ def test_transport_side_output_matches_reference(basin_ref):
         if k + 1 in (1, 4, 8):
             got = g.dacont().reshape(3, model.nelems2d)
             assert relerr(got, ref[f"step{k+1}_dacont"]) <= 1e-7, k
+
+
+@pytest.mark.parametrize("k", [1, 4, 8])
+def test_device_error_indicator_matches_oracle_and_reference(basin_ref, k):
+    """The adaption error indicator computed on the device from the reference's states after basin
+    steps 1, 4 and 8: bit-identical to the oracle, and within 1e-14 of the reference's own
+    grid->elem_error and nodal error (shape-gradient round-off, as for the residual)."""
+    import os
+    from conftest import GOLDEN
+    from oracle.oracle import Oracle
+    ref = dict(np.load(os.path.join(GOLDEN, "errind_ref.npz")))
+    m = basin_model()
+    h0, u0, v0 = m.initial_state()
+    prev = (h0, u0, v0) if k == 1 else tuple(basin_ref[f"step{k-1}_{f}"] for f in "huv")
+    cur = tuple(basin_ref[f"step{k}_{f}"] for f in "huv")
+    tol = np.full(len(m.materials), 100.0)
+    out = []
+    for s in (SW2GPU(m), Oracle(m)):
+        s.set_state(0, *cur)
+        s.set_state(1, *prev)
+        s.set_dt(m.dt, m.series_values(0.0, m.dt))
+        s.set_wd(basin_ref[f"step{k}_wd"])
+        out.append(s.elem_error(tol))
+    (eg, ng), (eo, no) = out
+    assert np.array_equal(eg, eo) and np.array_equal(ng, no)
+    assert relerr(eg, ref[f"step{k}_elem_error"]) <= 1e-14
+    assert relerr(ng, ref[f"step{k}_node_error"]) <= 1e-14

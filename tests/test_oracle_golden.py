@@ -1,10 +1,12 @@
 """The CPU oracle against fixtures produced by the reference executable itself."""
+import os
+
 import numpy as np
 import pytest
 
 from golden.make_golden import fingerprint
 from helpers import basin_model, channel_model, field_errors, fields, set_load_state
-from conftest import relerr
+from conftest import GOLDEN, relerr
 from oracle.oracle import Oracle
 
 
@@ -171,3 +173,30 @@ def test_oracle_rejects_unsupported_node_strings(what):
         m = dataclasses.replace(m, node_string=ns)
     with pytest.raises(ValueError):
         Oracle(m)
+
+
+def _errind_states(basin_ref, k):
+    m = basin_model()
+    h0, u0, v0 = m.initial_state()
+    prev = (h0, u0, v0) if k == 1 else tuple(basin_ref[f"step{k-1}_{f}"] for f in "huv")
+    cur = tuple(basin_ref[f"step{k}_{f}"] for f in "huv")
+    return m, cur, prev, basin_ref[f"step{k}_wd"]
+
+
+@pytest.mark.parametrize("k", [1, 4, 8])
+def test_oracle_error_indicator_matches_reference(basin_ref, k):
+    """The adaption error indicator (ssw_2d_calculate_elem_error) of the oracle against the
+    reference's own grid->elem_error and nodal error after basin steps 1, 4 and 8, from the
+    reference's states: within 1e-14 relative (a few ulps: on this Delaunay mesh the shape
+    gradients differ from the reference's by round-off, as the residual pin shows)."""
+    ref = dict(np.load(os.path.join(GOLDEN, "errind_ref.npz")))
+    m, cur, prev, wd = _errind_states(basin_ref, k)
+    o = Oracle(m)
+    o.set_state(0, *cur)
+    o.set_state(1, *prev)
+    o.set_dt(m.dt, m.series_values(0.0, m.dt))
+    o.set_wd(wd)
+    ee, ne = o.elem_error(np.full(len(m.materials), 100.0))   # MP SRT 100 in every generated deck
+    assert relerr(ee, ref[f"step{k}_elem_error"]) <= 1e-14
+    assert relerr(ne, ref[f"step{k}_node_error"]) <= 1e-14
+    assert np.array_equal(ee == 0.5, ref[f"step{k}_elem_error"] == 0.5)   # the wet/dry elements held

@@ -53,3 +53,14 @@ def test_single_rank_needs_no_group():
     import bench
     assert bench.max_over_ranks(3.5, 1) == 3.5
     assert bench.replica_throughput(1, 998582, 10, 219.4) == 998582 * 10 / 0.2194
+
+
+def test_bench_refuses_a_world_size_other_than_gpus():
+    """`--gpus N` under a launcher with another world size would time the wrong number of
+    replicas: bench.py refuses before any GPU work."""
+    import subprocess
+    env = dict(os.environ, WORLD_SIZE="3", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--steps", "1"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 2
+    assert "WORLD_SIZE is 3" in r.stderr
