@@ -26,8 +26,8 @@ namespace sw2 {
 // 8 row warps (SpMV rows, vector passes, partials) and one copy warp that fills the tile ring
 constexpr int kKrylovRowThreads = 256;
 constexpr int kKrylovThreads = kKrylovRowThreads + 32;
-constexpr long long kBarrierSpinLimit = 1ll << 28;   // bounded wait (~seconds of polls), then error
-constexpr long long kMbarSpinLimit = 1ll << 20;      // polls of one tile copy's mbarrier, then error
+constexpr long long kBarrierSpinLimit = 1ll << 23;   // polls (a few seconds: each is an L2 round trip), then error
+constexpr long long kMbarSpinLimit = 1ll << 20;      // polls (about a second) of one tile mbarrier, then error
 // a launch may bound its waits more tightly (KrylovArgs::spin_limit / copy_limit, 0 = these
 // defaults): failure-detection tests make a wait run out that way, without a fault
 constexpr int kStall = 40;                           // iterations without a new best residual
@@ -99,9 +99,8 @@ __device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks, unsi
 }
 
 constexpr int kKrylovWarps = kKrylovRowThreads / 32;   // warps that hold partials
-// named barriers of the Krylov CTA (0 is __syncthreads'): the row warps alone, and per ring
-// stage "read by every row warp" (row warps arrive, the copy warp waits)
-constexpr int kBarRows = 1, kBarEmpty = 2;
+// named barrier of the Krylov CTA's row warps alone (0 is __syncthreads')
+constexpr int kBarRows = 1;
 __device__ __forceinline__ void bar_sync_n(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
@@ -307,6 +306,9 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned coun
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
 __device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
@@ -338,6 +340,7 @@ __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence
 // tile copy to land; a limit below kShortWait polls with the non-blocking test_wait instead, so
 // that a short limit really bounds the wait (failure-detection tests).
 constexpr long long kShortWait = 64;
+constexpr unsigned kWaitHintNs = 1000;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long limit) {
     const unsigned a = smem_addr(bar);
     if (limit < kShortWait) {
@@ -354,10 +357,12 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
     }
     for (long long k = 0; k < limit; k++) {
         unsigned done;
+        // the suspend-time hint (ns) caps how long one poll may park the thread, so `limit` polls
+        // bound the wait to about limit microseconds; a completed phase wakes the thread at once
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done)
-            : "r"(a), "r"(parity)
+            : "r"(a), "r"(parity), "r"(kWaitHintNs)
             : "memory");
         if (done) return true;
     }
@@ -453,7 +458,8 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     __shared__ double red[4 * kKrylovWarps];
     constexpr bool STAGED = STAGES > 0;
     constexpr int NST = STAGES > 0 ? STAGES : 1;
-    __shared__ unsigned long long bar[NST];
+    __shared__ unsigned long long bar[NST];     // per ring stage: its tile copy has landed ("full")
+    __shared__ unsigned long long ebar[NST];    // per ring stage: every row warp is done with it ("empty")
     extern __shared__ __align__(128) unsigned char stage_mem[];
     int pl, np;   // this CTA's index among the instance's np CTAs
     double rtol;
@@ -485,6 +491,8 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     int nred = 0;      // reductions so far; selects the partial buffer
     unsigned epoch = 0;   // barrier arrivals this CTA waits for (grid_sync)
     unsigned tc = 0;   // tiles consumed by this CTA: stage tc % NST, mbarrier parity (tc / NST) & 1
+    unsigned issued = 0;   // tile copies issued (the copy warp's issuing lane)
+    bool copy_stop = false;   // the issuing lane gave up a wait: no more copies
     bool wait_failed = false;
     unsigned long long pol = 0;
     auto pbuf = [&]() { return K.part + (size_t)(nred & 1) * VG * 4; };
@@ -492,11 +500,11 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     const long long bar_limit = K.spin_limit > 0 ? K.spin_limit : kBarrierSpinLimit;
     const long long copy_limit = K.copy_limit > 0 ? K.copy_limit : kMbarSpinLimit;
     // Before a CTA leaves on an error, the bulk copies it issued must have landed in its shared
-    // memory: thread 0 waits (bounded by the default limit) for the last item of every ring
-    // stage.  The copy warp issues exactly the items the row warps consume, so tc counts both.
+    // memory: the issuing lane waits (bounded by the default limit) for its last copy into every
+    // ring stage.
     auto drain = [&]() {
-        if (STAGED && threadIdx.x == 0)
-            for (unsigned it = tc > (unsigned)NST ? tc - NST : 0u; it < tc; it++)
+        if (STAGED && threadIdx.x == kKrylovRowThreads)
+            for (unsigned it = issued > (unsigned)NST ? issued - NST : 0u; it < issued; it++)
                 mbar_wait(&bar[it % NST], (it / NST) & 1u, kMbarSpinLimit);
     };
     // grid barrier; false (after draining the tile ring) when some CTA gave up: return at once
@@ -508,7 +516,10 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
 
     if (STAGED) {
         if (threadIdx.x == 0) {
-            for (int s = 0; s < NST; s++) mbar_init(&bar[s], 1);
+            for (int s = 0; s < NST; s++) {
+                mbar_init(&bar[s], 1);
+                mbar_init(&ebar[s], kKrylovWarps);
+            }
             mbar_init_fence();
         }
         if (threadIdx.x == kKrylovRowThreads) pol = policy_evict_first();
@@ -521,9 +532,14 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     // ev(v, c) = component c of epilogue vector v at row i (NV vectors; read from the staged tile
     // or from global memory), from which the epilogue forms the diagonal term; fin(v) closes
     // virtual CTA v (its partial).
-    // STAGED: the copy warp walks the same tile sequence up to NST tiles ahead, filling ring
-    // stage (item % NST) once every row warp has released it (named barrier kBarEmpty + stage);
-    // the row warps wait on the stage's mbarrier, so each warp proceeds at its own pace.
+    // STAGED: the copy warp's issuing lane walks the same tile sequence up to NST tiles ahead,
+    // filling ring stage (item % NST) once every row warp has released the stage's previous item
+    // (its "empty" mbarrier: one arrival per row warp and item) and that item's copy has landed;
+    // the row warps wait on the stage's "full" mbarrier, so each warp proceeds at its own pace.
+    // Every wait is bounded: a row warp whose wait runs out flags the error and stops reading the
+    // ring for the rest of the sweep (still waiting for and releasing every item, so the issuing
+    // lane never waits on a release that cannot come); an issuing lane whose wait runs out flags
+    // the error and issues nothing more; the next grid barrier then ends the kernel.
     // Called by the whole CTA.
     auto sweep = [&](auto nvc, const VT* const* vecs, auto&& gat, auto&& epi, auto&& fin) {
         constexpr int NV = decltype(nvc)::value;
@@ -531,39 +547,58 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         for (int v = pl; v < VG; v += np) nitems += (ntiles - v + VG - 1) / VG;
         if (!rows) {
             if (STAGED) {
+                // the whole warp walks the items (it stays converged for the CTA barriers that
+                // follow); its first lane waits and issues, the stop decision is broadcast
                 const bool issuer = threadIdx.x == kKrylovRowThreads;
                 if (issuer) fence_proxy_async_global();
-                int j = 0;
                 for (int v = pl; v < VG; v += np)
-                    for (int m = v; m < ntiles; m += VG, j++) {
-                        const unsigned item = tc + j;
-                        if (j >= NST) bar_sync_n(kBarEmpty + (int)(item % NST), kKrylovThreads);
-                        // the stage's previous copy has landed before it is refilled (the row warps
-                        // waited for it, unless their wait ran out): one copy per stage in flight
-                        if (issuer && item >= (unsigned)NST)
-                            mbar_wait(&bar[item % NST], ((item - NST) / NST) & 1u, kMbarSpinLimit);
-                        if (issuer)
-                            issue_tile<MT, VT>(m, V, K.rowptr, K.col, A, NV, vecs, stage(item), L, &bar[item % NST], pol);
+                    for (int m = v; m < ntiles; m += VG) {
+                        if (!copy_stop) {
+                            bool stop = false;
+                            if (issuer) {
+                                const unsigned item = issued;
+                                if (item >= (unsigned)NST) {
+                                    // the stage's previous item: released by every row warp, and
+                                    // its copy landed (the row warps waited for it)
+                                    const unsigned par = ((item - NST) / NST) & 1u;
+                                    stop = !mbar_wait(&ebar[item % NST], par, kMbarSpinLimit) ||
+                                           !mbar_wait(&bar[item % NST], par, kMbarSpinLimit);
+                                }
+                                if (stop) atomicExch(&ctl->err, 1);
+                                else issue_tile<MT, VT>(m, V, K.rowptr, K.col, A, NV, vecs, stage(item), L,
+                                                        &bar[item % NST], pol);
+                            }
+                            copy_stop = __shfl_sync(0xffffffffu, stop, 0);
+                            if (!copy_stop) issued++;
+                        }
                         __syncwarp();
                     }
             }
             tc += nitems;
             return;
         }
-        int j = 0;
         for (int v = pl; v < VG; v += np) {
-            for (int m = v; m < ntiles; m += VG, j++) {
+            for (int m = v; m < ntiles; m += VG) {
                 const int i = m * kTileRows + li;
                 const bool act = i < V;
                 VT y[3];
                 if (STAGED) {
-                    // a wait that runs out flags the error once; this thread then stops waiting
-                    // and treats the rest of the sweep's rows as absent (a stage that may not have
-                    // landed is never read, so no index comes from stale shared memory), and the
-                    // next barrier returns
-                    if (!wait_failed && !mbar_wait(&bar[tc % NST], (tc / NST) & 1u, copy_limit)) {
-                        wait_failed = true;
-                        atomicExch(&ctl->err, 1);
+                    // a wait that runs out flags the error once; the warp then treats the rest of
+                    // the sweep's rows as absent (a stage that may not have landed is never read,
+                    // so no index comes from stale shared memory) and the next barrier returns.
+                    // It still waits (with the default bound) for every tile before releasing
+                    // it, so it never runs ahead of the copies: the ring stays in step and every
+                    // copy has landed before the kernel returns.
+                    {
+                        const unsigned par = (tc / NST) & 1u;
+                        const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar[tc % NST], par,
+                                                                          wait_failed ? kMbarSpinLimit : copy_limit));
+                        if (!ok && !wait_failed) {
+                            wait_failed = true;
+                            if ((threadIdx.x & 31) == 0) atomicExch(&ctl->err, 1);
+                            __syncwarp();
+                            (void)mbar_wait(&bar[tc % NST], par, kMbarSpinLimit);
+                        }
                     }
                     const bool use = act && !wait_failed;
                     const unsigned char* st = stage(tc);
@@ -586,9 +621,9 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                     if (act && lane8 == 0) epi(i, y, [&](int w, int c) { return ldv(vecs[w] + 3 * i + c); });
                 }
                 if (STAGED) {
-                    // this warp is done with the stage; the copy warp refills it for item + NST
+                    // this warp is done with the stage: one arrival per warp releases it
                     __syncwarp();
-                    if (j + NST < nitems) bar_arrive_n(kBarEmpty + (int)(tc % NST), kKrylovThreads);
+                    if ((threadIdx.x & 31) == 0) mbar_arrive(&ebar[tc % NST]);
                     tc++;
                 }
             }

@@ -100,7 +100,13 @@ struct sw2gpu_ctx {
     DBuf<unsigned char> efirst, dflag, mark;
     DBuf<MatParams> mats;
     DBuf<double> str_value, str_uv;
-    DBuf<double> mass_part;     // mass-balance partials (2 per block) and the result
+    DBuf<double> mass_part;     // mass-balance partials (2 per block) and three results
+    // mass balance of every accepted step, reduced inside the step (sw2gpu_set_mass_tracking)
+    bool mass_on = false;
+    double mass_density = 0.0;
+    double* mass_h = nullptr;   // pinned: grid mass and flux of the last accepted step
+    bool mass_valid = false;
+    double step_mass = 0.0, step_flux = 0.0;
     DBuf<double> dacont;        // [3][T] transport side output, allocated when first enabled
     DBuf<double> errind;        // adaption error indicator: raw [T], scaled [T], nodal [V], tolerances [M]
     bool dacont_on = false;
@@ -280,6 +286,7 @@ sw2gpu_ctx::~sw2gpu_ctx() {
         cudaEventDestroy(stage_ev);
     }
     if (stage_h) cudaFreeHost(stage_h);
+    if (mass_h) cudaFreeHost(mass_h);
     self.reset();
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -905,6 +912,22 @@ void phase_times(Runner& R, double ph[3]) {
     }
 }
 
+// the grid mass and the mass flux of instance c's accepted step, reduced on its stream `st`
+// into the context's pinned mirror (the values are read after the step's final sync)
+int enqueue_step_mass(sw2gpu_ctx* c, cudaStream_t st) {
+    double* part = c->mass_part.p;
+    double* res = part + 2 * kMassBlocks + 1;   // [0] grid mass, [1] flux
+    k_mass_partial<false><<<kMassBlocks, kMassThreads, 0, st>>>(c->dm, c->H(0), nullptr, nullptr, 0.0, c->mass_density,
+                                                                part);
+    k_mass_final<false><<<1, kMassThreads, 0, st>>>(part, c->mass_density, res);
+    k_mass_partial<true><<<kMassBlocks, kMassThreads, 0, st>>>(c->dm, c->H(0), c->U(0), c->Vv(0), c->dt,
+                                                               c->mass_density, part);
+    k_mass_final<true><<<1, kMassThreads, 0, st>>>(part, c->mass_density, res + 1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->mass_h, res, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
 // after a Krylov wait ran out: the instances back at their old level, the error text kept
 void reset_after_timeout(Runner& R, const std::vector<int>& sub) {
     const std::string msg = g_err;
@@ -951,8 +974,25 @@ int runner_step(Runner& R, const double* dt, const double* const* series, sw2gpu
         if (status[k] != SW2GPU_OK) failed.push_back(k);
     }
     if (!failed.empty() && (rc = launch_init(R, failed))) return rc;   // reset to the old level
+    // mass balance of the accepted steps, in the same stream order (no extra host round trip)
+    for (int k = 0; k < K; k++) {
+        sw2gpu_ctx* c = R.ctx[k];
+        c->mass_valid = false;
+        if (c->mass_on && status[k] == SW2GPU_OK) {
+            if ((rc = enqueue_step_mass(c, R.stream))) return rc;
+            R.launches += 4;
+        }
+    }
     CK(cudaEventRecord(R.ev1, R.stream));
     CK(cudaEventSynchronize(R.ev1));
+    for (int k = 0; k < K; k++) {
+        sw2gpu_ctx* c = R.ctx[k];
+        if (c->mass_on && status[k] == SW2GPU_OK) {
+            c->step_mass = c->mass_h[0];
+            c->step_flux = c->mass_h[1];
+            c->mass_valid = true;
+        }
+    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, R.ev0, R.ev1);
     double ph[3];
@@ -1068,8 +1108,19 @@ int graph_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* sta
     }
     status[0] = newton_status(ns[0], c->p);
     if (status[0] != SW2GPU_OK && (rc = launch_init(R, one))) return rc;   // reset to the old level
+    c->mass_valid = false;
+    const bool mass = c->mass_on && status[0] == SW2GPU_OK;
+    if (mass) {
+        if ((rc = enqueue_step_mass(c, R.stream))) return rc;
+        R.launches += 4;
+    }
     CK(cudaEventRecord(R.ev1, R.stream));
     CK(cudaEventSynchronize(R.ev1));
+    if (mass) {
+        c->step_mass = c->mass_h[0];
+        c->step_flux = c->mass_h[1];
+        c->mass_valid = true;
+    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, R.ev0, R.ev1);
     if (stats) {
@@ -1303,7 +1354,7 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     rc |= up(c->mats, c->mats_h, st);
     rc |= zalloc(c->str_value, std::max(c->S, 1), st);
     rc |= zalloc(c->str_uv, 2 * std::max(c->S, 1), st);
-    rc |= zalloc(c->mass_part, 2 * kMassBlocks + 1, st);
+    rc |= zalloc(c->mass_part, 2 * kMassBlocks + 3, st);
     rc |= up(c->slot_ptr, slot_ptr, st); rc |= up(c->slot_idx, slot_idx, st);
     rc |= up(c->blk_ptr, blk_ptr, st); rc |= up(c->blk_src, blk_src, st);
     rc |= up(c->rowptr, rp, st); rc |= up(c->col, col, st); rc |= up(c->blk_row, blk_row, st); rc |= up(c->dpos, dpos, st);
@@ -1495,6 +1546,23 @@ int sw2gpu_elem_error(sw2gpu_ctx* c, const double* refine_tol, double* elem_erro
     if (T) CK(cudaMemcpyAsync(elem_error, err, sizeof(double) * T, cudaMemcpyDeviceToHost, c->stream));
     if (node_error) CK(cudaMemcpyAsync(node_error, nod, sizeof(double) * V, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_set_mass_tracking(sw2gpu_ctx* c, int32_t enable, double density) {
+    if (!c || (enable && !(density > 0.0))) return fail(SW2GPU_E_ARG, "bad context or density");
+    if (enable && !c->mass_h) CK(cudaMallocHost(&c->mass_h, 2 * sizeof(double)));
+    c->mass_on = enable != 0;
+    c->mass_density = density;
+    c->mass_valid = false;
+    return SW2GPU_OK;
+}
+
+int sw2gpu_step_mass(sw2gpu_ctx* c, double* mass, double* flux) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    if (!c->mass_valid) return fail(SW2GPU_E_ARG, "no accepted step with mass tracking on since it was enabled");
+    if (mass) *mass = c->step_mass;
+    if (flux) *flux = c->step_flux;
     return SW2GPU_OK;
 }
 

@@ -159,6 +159,20 @@ def channel_obstacle(nsteps: int = 6, with_depth: bool = False) -> SW2Model:
     return m
 
 
+def channel_spike(nsteps: int = 12, peak: float = 20.0, max_nonlin_it: int = 5) -> SW2Model:
+    """The rectangular channel with a one-step inflow spike (0.5 -> `peak` -> 0.5 m^2/s over
+    [40, 50] s) and at most `max_nonlin_it` Newton iterations: the step that meets the spike
+    fails, is retried with dt / 4 (twice), and the time loop then recovers the nominal dt by
+    doubling it after every accepted step (the reference's tc_end, src/tools/tc_end.c:55-66);
+    the run ends with the time loop's shortened last steps."""
+    m = channel(nsteps=nsteps, name="spike")
+    t_end = (nsteps + 10) * m.dt
+    m.series = [Series(np.array([0.0, 40.0, 45.0, 50.0, t_end]), np.array([0.5, 0.5, peak, 0.5, 0.5])),
+                m.series[1]]
+    m.params = dataclasses.replace(m.params, max_nonlin_it=max_nonlin_it)
+    return m
+
+
 def channel_ovh(nsteps: int = 6, u_in: float = 0.5, **kw) -> SW2Model:
     """The channel with its inflow given as NB OVH instead of NB VEL: water elevation 1 m above
     the datum (the west bed) and velocity (u_in, 0) on the west edge; NB OTW tailwater east."""

@@ -33,7 +33,8 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_device_bytes", "sw2gpu_autotune", "sw2gpu_set_graphs", "sw2gpu_set_variant", "sw2gpu_get_variant",
            "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
            "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont",
-           "sw2gpu_set_wait_limits", "sw2gpu_snapshot", "sw2gpu_elem_error"]
+           "sw2gpu_set_wait_limits", "sw2gpu_snapshot", "sw2gpu_elem_error", "sw2gpu_set_mass_tracking",
+           "sw2gpu_step_mass"]
 
 
 class SW2Error(RuntimeError):
@@ -85,6 +86,8 @@ def lib():
         L.sw2gpu_set_wait_limits.argtypes = [vp, C.c_int64, C.c_int64]
         L.sw2gpu_snapshot.argtypes = [vp, C.c_int, vp, vp, vp]
         L.sw2gpu_elem_error.argtypes = [vp, c_double_p, c_double_p, c_double_p]
+        L.sw2gpu_set_mass_tracking.argtypes = [vp, C.c_int32, C.c_double]
+        L.sw2gpu_step_mass.argtypes = [vp, c_double_p, c_double_p]
         L.sw2gpu_set_variant.argtypes = [vp, C.c_int32, C.c_int32]
         L.sw2gpu_get_variant.argtypes = [vp, c_int32_p, c_int32_p]
         L.sw2gpu_device_bytes.restype = C.c_int64
@@ -253,6 +256,17 @@ class SW2GPU:
         out = C.c_double()
         _check(lib().sw2gpu_mass_flux(self.h, rho, C.byref(out)))
         return out.value
+
+    def set_mass_tracking(self, enable: bool = True, density=None):
+        """Reduce the grid mass and the mass flux inside every accepted step (step_mass())."""
+        rho = self.model.params.density if density is None else density
+        _check(lib().sw2gpu_set_mass_tracking(self.h, 1 if enable else 0, rho))
+
+    def step_mass(self):
+        """(grid mass, mass flux) of the last accepted step, reduced inside that step."""
+        m, f = C.c_double(), C.c_double()
+        _check(lib().sw2gpu_step_mass(self.h, C.byref(m), C.byref(f)))
+        return m.value, f.value
 
     def set_dacont(self, enable: bool = True):
         """Keep the transport side output elem_rhs_dacont_extra_terms of every residual evaluation."""

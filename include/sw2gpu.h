@@ -140,9 +140,9 @@ int64_t sw2gpu_device_bytes(const sw2gpu_ctx *ctx);
 /* Bounds of the device waits (no counterpart in the reference, whose solver runs on one CPU
  * thread): the Krylov kernel's grid barriers and its tile-copy waits give up after this many
  * polls, set SW2GPU_E_TIMEOUT and return; the step then resets the current level to the old
- * one, like a failed step, and the context stays usable.  0 = the library's defaults (2^28 and
- * 2^20 polls, seconds and milliseconds).  Failure-detection tests set a few polls to make a
- * wait run out without any fault. */
+ * one, like a failed step, and the context stays usable.  0 = the library's defaults (2^23 and
+ * 2^20 polls, a few seconds and about a second).  Failure-detection tests set a few polls to
+ * make a wait run out without any fault. */
 int sw2gpu_set_wait_limits(sw2gpu_ctx *ctx, int64_t barrier_polls, int64_t copy_polls);
 
 /* State of time level `level` (0 = current t+dt iterate, 1 = old, 2 = older);
@@ -184,6 +184,15 @@ int sw2gpu_grid_mass(sw2gpu_ctx *ctx, int level, double density, double *mass);
  * values averaged over each node's elements, the reference's sw->error. */
 int sw2gpu_elem_error(sw2gpu_ctx *ctx, const double *refine_tol, double *elem_error, double *node_error);
 int sw2gpu_mass_flux(sw2gpu_ctx *ctx, double density, double *flux);
+/* The same two diagnostics for every accepted step, reduced inside sw2gpu_step (and a batch
+ * step) on the step's stream after its Newton loop, with no launch or host round trip of their
+ * own -- for callers that report mass every step, as the reference's SOUT MERROR does
+ * (tl_find_grid_mass_error_elem2d after every step).  sw2gpu_step_mass returns the grid mass of
+ * the new level and the step's flux, bitwise the values sw2gpu_grid_mass(ctx, 0, density) and
+ * sw2gpu_mass_flux(ctx, density) give right after that step; SW2GPU_E_ARG if the last step was
+ * not accepted or tracking is off.  Not part of the continuous-batching engine's ticks. */
+int sw2gpu_set_mass_tracking(sw2gpu_ctx *ctx, int32_t enable, double density);
+int sw2gpu_step_mass(sw2gpu_ctx *ctx, double *mass, double *flux);
 
 /* Transport side output elem_rhs_dacont_extra_terms (src/fe/sw2/fe_sw2_body_resid.c:353-355,
  * :400, :1214): the continuity parts of shock capturing and SUPG per element vertex from the

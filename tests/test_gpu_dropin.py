@@ -51,25 +51,47 @@ def _ntl(bc_path):
     return 1e-8
 
 
-def _run(exe, case):
-    """Runs exe on a scratch copy of the deck; returns (per-step records, error.out lines)."""
+def _run(exe, case, model=None):
+    """Runs exe on a scratch copy of a staged QA deck (or on `model` written as a deck); returns
+    (per-step records, error.out lines or None, error.out.last lines or None, IP NTL)."""
     from oracle.ref_run import parse, read_dump
     work = tempfile.mkdtemp(prefix=f"dropin_{case}_")
     try:
         run = os.path.join(work, case)
-        shutil.copytree(os.path.join(QA, case), run)
-        (deck,) = [f[:-3] for f in os.listdir(run) if f.endswith(".bc")]
+        if model is None:
+            shutil.copytree(os.path.join(QA, case), run)
+            (deck,) = [f[:-3] for f in os.listdir(run) if f.endswith(".bc")]
+        else:
+            deck = "m"
+            model.write_adh(run, deck)
         env = dict(os.environ, ADH_DUMP=os.path.join(run, "dump.bin"), ADH_DUMP_LOADS="0")
         r = subprocess.run([exe, deck], cwd=run, env=env, capture_output=True, text=True, timeout=900)
         assert r.returncode == 0, (exe, r.stdout[-3000:], r.stderr[-2000:])
         steps = parse(read_dump(os.path.join(run, "dump.bin")))["steps"]
-        with open(os.path.join(run, "error.out")) as fh:
-            report = [ln for ln in fh.read().splitlines() if ln.strip()]
-        with open(os.path.join(run, "error.out.last")) as fh:
-            stored = [ln for ln in fh.read().splitlines() if ln.strip()]
+        report = stored = None
+        if model is None:
+            with open(os.path.join(run, "error.out")) as fh:
+                report = [ln for ln in fh.read().splitlines() if ln.strip()]
+            with open(os.path.join(run, "error.out.last")) as fh:
+                stored = [ln for ln in fh.read().splitlines() if ln.strip()]
         return steps, report, stored, _ntl(os.path.join(run, deck + ".bc"))
     finally:
         shutil.rmtree(work, ignore_errors=True)
+
+
+def _compare_trajectories(case, gpu_steps, ref_steps, tol):
+    """Accepted steps one for one: the same model times, dt and attempts (dt retries), Newton
+    iterations within +-1 per attempt, the state within tol."""
+    assert len(gpu_steps) == len(ref_steps), (len(gpu_steps), len(ref_steps))
+    worst = {"h": 0.0, "q": 0.0}
+    for k, (g, r) in enumerate(zip(gpu_steps, ref_steps)):
+        assert g["t"] == r["t"] and g["dt"] == r["dt"], (k, g["t"], r["t"], g["dt"], r["dt"])
+        assert g["attempts"] == r["attempts"], k
+        assert abs(g["newton_its"] - r["newton_its"]) <= max(1, r["attempts"]), (k, g["newton_its"], r["newton_its"])
+        for f, e in field_errors(fields(g["h"], g["u"], g["v"]), fields(r["h"], r["u"], r["v"])).items():
+            worst[f] = max(worst[f], e)
+            assert e <= tol, (case, k, f, e, tol)
+    return worst
 
 
 def _split(line):
@@ -98,15 +120,7 @@ def test_reference_time_loop_with_the_gpu_step_matches_the_reference(case):
     ref_steps, ref_report, stored, ntl = _run(CPU_EXE, case)
     gpu_steps, gpu_report, _, _ = _run(GPU_EXE, case)
     tol = 1e-10 if ntl <= 1e-8 else 100.0 * ntl
-    assert len(gpu_steps) == len(ref_steps)
-    worst = {"h": 0.0, "q": 0.0}
-    for k, (g, r) in enumerate(zip(gpu_steps, ref_steps)):
-        assert g["t"] == r["t"] and g["dt"] == r["dt"], (k, g["t"], r["t"], g["dt"], r["dt"])
-        assert g["attempts"] == r["attempts"], k
-        assert abs(g["newton_its"] - r["newton_its"]) <= max(1, r["attempts"]), (k, g["newton_its"], r["newton_its"])
-        for f, e in field_errors(fields(g["h"], g["u"], g["v"]), fields(r["h"], r["u"], r["v"])).items():
-            worst[f] = max(worst[f], e)
-            assert e <= tol, (case, k, f, e, tol)
+    worst = _compare_trajectories(case, gpu_steps, ref_steps, tol)
     print(f"{case}: {len(gpu_steps)} steps, worst per-step error h {worst['h']:.2e} q {worst['q']:.2e} (bound {tol:g})")
     assert len(gpu_report) == len(stored)
     for g, e in zip(gpu_report, stored):
@@ -114,3 +128,25 @@ def test_reference_time_loop_with_the_gpu_step_matches_the_reference(case):
         ew, en = _split(e)
         assert gw == ew, (g, e)
         assert np.allclose(gn, en, rtol=1e-4, atol=1e-6), (g, e)
+
+
+@pytest.mark.gpu
+def test_retry_path_through_the_reference_time_loop_matches_the_reference():
+    """Retry-path parity: the channel with a one-step inflow spike and at most 5 Newton iterations
+    (meshgen.channel_spike).  In the reference the step that meets the spike fails twice and is
+    retried with dt / 4 each time (tc_scale, src/fe/fe_newton.c:854-892), a later step fails once,
+    and after every accepted step the time loop doubles dt back toward the nominal 10 s
+    (tc_end, src/tools/tc_end.c:55-66), re-shifting the time levels on every attempt
+    (src/fe/fe_main.c:353).  Through the drop-in the GPU step must take the same path: the
+    same accepted steps, dt and attempts, and the state within 1e-10 every step."""
+    if not os.path.exists(GPU_EXE):
+        pytest.fail("oracle/_ref/adh_gpu is missing (python oracle/ref/build_ref.py)")
+    from adhv8_kraken_b200 import meshgen
+    m = meshgen.channel_spike()
+    ref_steps, _, _, _ = _run(CPU_EXE, "spike", m)
+    gpu_steps, _, _, _ = _run(GPU_EXE, "spike", m)
+    assert sum(s["attempts"] for s in ref_steps) > len(ref_steps)   # the case does fail and retry
+    worst = _compare_trajectories("spike", gpu_steps, ref_steps, 1e-10)
+    print(f"spike: {len(gpu_steps)} steps, {sum(s['attempts'] for s in gpu_steps)} attempts, worst per-step "
+          f"error h {worst['h']:.2e} q {worst['q']:.2e}")
+

@@ -255,3 +255,19 @@ def test_device_error_indicator_matches_oracle_and_reference(basin_ref, k):
     assert np.array_equal(eg, eo) and np.array_equal(ng, no)
     assert relerr(eg, ref[f"step{k}_elem_error"]) <= 1e-14
     assert relerr(ng, ref[f"step{k}_node_error"]) <= 1e-14
+
+
+def test_mass_reduced_inside_the_step_equals_the_on_demand_diagnostics():
+    """With mass tracking on, every accepted step reduces the grid mass and the step's mass flux
+    inside the step; the values are bitwise those of sw2gpu_grid_mass / sw2gpu_mass_flux called
+    right after the step (the reference's SOUT MERROR path), on the rain basin with a source."""
+    m = meshgen.basin_rain(nsteps=4)
+    g = SW2GPU(m)
+    g.set_mass_tracking(True)
+    with pytest.raises(SW2Error):
+        g.step_mass()                 # no accepted step yet
+    for _ in range(4):
+        assert g.step()["status"] == 0
+        mass, flux = g.step_mass()
+        assert mass == g.grid_mass(0) and flux == g.mass_flux()
+    g.close()
