@@ -42,6 +42,9 @@ typedef struct {
     double *h, *u, *v;      /* staging of one time level */
     double *series;         /* step-averaged value of every series, by id */
     int *mat_of;            /* [nstring] material of the elements on each material string, or -1 */
+    int32_t *wind_flag;     /* [nstring] MP WND STR of that material (wind runs only) */
+    double *wind_att;       /* [nstring] MP WND ATT of that material */
+    double *wsx, *wsy;      /* [nnodes] nodal wind values of the coming step */
     int state_on_device;    /* the host's current and old levels are the device's (last step accepted) */
 } GPU_SW2;
 
@@ -79,6 +82,7 @@ static int series_count(SSERIES *head) {
 static void gpu_release(void) {
     if (gpu.ctx) sw2gpu_destroy(gpu.ctx);
     free(gpu.h); free(gpu.u); free(gpu.v); free(gpu.series); free(gpu.mat_of);
+    free(gpu.wind_flag); free(gpu.wind_att); free(gpu.wsx); free(gpu.wsy);
     memset(&gpu, 0, sizeof gpu);
 }
 
@@ -90,10 +94,11 @@ static void gpu_prepare(SSUPER_MODEL *sm, SMODEL *mod) {
     const int V = g->nnodes, T = g->nelems2d, S = mod->nstring;
     int i, k, E = 0;
     gpu_release();
-    /* body terms the library does not compute (fe_sw2_body_resid.c:674-719 surface stresses,
-     * :869-970 baroclinic terms): refuse the model rather than solve without them */
-    if (mod->flag.WIND == ON || mod->flag.WAVE == ON)
-        tl_error("B200 SW2 step: wind and wave surface stresses are not supported\n");
+    /* body terms the library does not compute (fe_sw2_body_resid.c:674-719 wave stresses and
+     * the wind library's forms, :869-970 baroclinic terms): refuse the model rather than solve
+     * without them */
+    if (mod->flag.WAVE == ON || mod->flag.WIND_LIBRARY == ON)
+        tl_error("B200 SW2 step: wave stresses and the wind library are not supported\n");
     if (mod->flag.BAROCLINIC != OFF)
         tl_error("B200 SW2 step: baroclinic terms are not supported\n");
     for (i = 0; i < g->nelems1d; i++) {
@@ -186,6 +191,16 @@ static void gpu_prepare(SSUPER_MODEL *sm, SMODEL *mod) {
     if (mod->ntransport > 0 && sw2gpu_set_dacont(gpu.ctx, 1) != SW2GPU_OK) gpu_fail("sw2gpu_set_dacont");
     gpu.nnodes = V; gpu.nelems2d = T; gpu.nelems1d = g->nelems1d;
     gpu.h = malloc(V * sizeof(double)); gpu.u = malloc(V * sizeof(double)); gpu.v = malloc(V * sizeof(double));
+    if (mod->flag.WIND == ON) {   /* the material wind forms, indexed like the library's material table */
+        gpu.wind_flag = malloc((S + 1) * sizeof(int32_t));
+        gpu.wind_att = malloc((S + 1) * sizeof(double));
+        gpu.wsx = malloc(V * sizeof(double));
+        gpu.wsy = malloc(V * sizeof(double));
+        for (k = 0; k < S; k++) {
+            gpu.wind_flag[k] = gpu.mat_of[k] >= 0 ? mod->mat[gpu.mat_of[k]].sw->wind_flag : 0;
+            gpu.wind_att[k] = gpu.mat_of[k] >= 0 ? mod->mat[gpu.mat_of[k]].sw->windatt : 1.0;
+        }
+    }
     gpu.series = malloc((gpu.nseries + 1) * sizeof(double));
 }
 
@@ -217,6 +232,11 @@ int fe_sw2_solve_gpu(SSUPER_MODEL *sm, int isubModel) {
     for (i = 0; i < gpu.nseries; i++) gpu.series[i] = 0.0;
     for (s = mod->series_head; s != NULL; s = s->next)
         if (s->id >= 0 && s->id < gpu.nseries && s->ivalue != NULL) gpu.series[s->id] = s->ivalue[0];
+    if (gpu.wsx) {   /* the nodal winds meteor_update set for this step (fe_sw2_body_resid.c:679-686) */
+        for (i = 0; i < gpu.nnodes; i++) { gpu.wsx[i] = sw->winds[i].stress.x; gpu.wsy[i] = sw->winds[i].stress.y; }
+        if (sw2gpu_set_wind(gpu.ctx, gpu.wind_flag, gpu.wind_att, gpu.wsx, gpu.wsy) != SW2GPU_OK)
+            gpu_fail("sw2gpu_set_wind");
+    }
     sw2gpu_stats st;
     gpu.state_on_device = 0;
     const int rc = sw2gpu_step(gpu.ctx, sm->dt, gpu.series, &st);

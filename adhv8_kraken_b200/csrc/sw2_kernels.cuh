@@ -28,6 +28,7 @@ struct DevMesh {
     const int *slot_ptr, *slot_idx;   // node -> residual slots in reference order
     const int *blk_ptr, *blk_src;     // BCSR block -> element-block slots in reference order
     const int *rowptr, *col, *blk_row, *dpos;
+    const double *wsx, *wsy;          // [T] element wind surface stress (sw2gpu_set_wind), or null
     int qflag[3];                     // flags of global nodes 0..2 (fe_sw2_load.c:103 indexes by local id)
 };
 
@@ -142,6 +143,8 @@ __device__ __forceinline__ void load_elem(const DevMesh& m, const State& s, int 
         df[i] = m.dflag[k];
     }
     in.djac = m.djac[e];
+    in.wsx = m.wsx ? m.wsx[e] : 0.0;
+    in.wsy = m.wsy ? m.wsy[e] : 0.0;
     in.gx[0] = m.gx0[e]; in.gy[0] = m.gy0[e];
     in.gx[1] = m.gx1[e]; in.gy[1] = m.gy1[e];
     in.gx[2] = m.gx2[e]; in.gy[2] = m.gy2[e];
@@ -860,6 +863,55 @@ __global__ void k_dirichlet(const __grid_constant__ Src src) {
         I.s.v[k] = I.dir_v[t];
     }
     if (f & 1) I.s.h[k] = I.dir_h[t];
+}
+
+// ---------------------------------------------------------------------------------
+// Wind surface stress per element (swind_elem2d_get_local_stress, src/structs/smeteor.c:241-306):
+// the nodal wind values (what meteor_update puts in winds[node].stress) turned into a shear by
+// the element material's flag -- 0: the value itself, 1: Wu's drag law (winds_proc_wu,
+// src/meteor/winds_proc_wu.c:5-26, pow(x, 2.0) written as x * x, the same correctly rounded
+// value) -- summed over the vertices in order and scaled by windatt^2 / (3 density) (`fac`,
+// formed on the host with the reference's pow).
+__device__ __forceinline__ void wind_wu(double g, double xs, double ys, double& sx, double& sy) {
+    double wmag = sqrt(xs * xs + ys * ys + 1e-10), x = xs, y = ys;
+    if (g > 10.) {
+        wmag *= 0.3048;
+        x *= 0.3048;
+        y *= 0.3048;
+    }
+    const double cd = (0.8 + 0.065 * wmag) * .001;
+    if (g > 10.) {
+        sx = 1.225 * cd * x * wmag * 0.020885;
+        sy = 1.225 * cd * y * wmag * 0.020885;
+    } else {
+        sx = 1.225 * cd * x * wmag;
+        sy = 1.225 * cd * y * wmag;
+    }
+}
+__global__ void k_elem_wind(const __grid_constant__ DevMesh m, double g, double density, const int* __restrict__ flag,
+                            const double* __restrict__ fac, const double* __restrict__ nsx,
+                            const double* __restrict__ nsy, double* __restrict__ wsx, double* __restrict__ wsy) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.T) return;
+    const int mt = m.emat[e];
+    const int n[3] = {m.en0[e], m.en1[e], m.en2[e]};
+    double wx = 0., wy = 0.;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        double sx = 0., sy = 0.;
+        if (density > 0.0) {
+            if (flag[mt] == 0) {
+                sx = nsx[n[i]];
+                sy = nsy[n[i]];
+            } else {
+                wind_wu(g, nsx[n[i]], nsy[n[i]], sx, sy);
+            }
+        }
+        wx += sx;
+        wy += sy;
+    }
+    wsx[e] = wx * fac[mt];
+    wsy[e] = wy * fac[mt];
 }
 
 // ---------------------------------------------------------------------------------

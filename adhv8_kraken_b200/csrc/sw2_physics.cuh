@@ -49,6 +49,7 @@ struct ElemIn {
     double ho[3], uo[3], vo[3];     // old time level
     double hoo[3], uoo[3], voo[3];  // older time level
     double djac, gx[3], gy[3];
+    double wsx, wsy;                // wind surface stress of the element (0: none)
 };
 
 // a[k] for a runtime k in 0..2 as selects, so register arrays stay in registers
@@ -598,6 +599,17 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
         };
         phifg(-t1, hc, vc, 1);
         phifg(+t1, hc, uc, 2);
+    }
+
+    // wind surface stress, fully wet elements only (:674-719; no wave stress).  A zero stress
+    // would subtract +0.0 from every entry, which changes no bits, so it is skipped.
+    if (wd_flag == 0 && (in.wsx != 0.0 || in.wsy != 0.0)) {
+        const double tx = in.wsx * djac * kOne3, ty = in.wsy * djac * kOne3;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            er[i][1] -= dt * tx;
+            er[i][2] -= dt * ty;
+        }
     }
 
     // rainfall / water source (:728-754)

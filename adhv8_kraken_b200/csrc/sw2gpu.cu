@@ -109,6 +109,9 @@ struct sw2gpu_ctx {
     double step_mass = 0.0, step_flux = 0.0;
     DBuf<double> dacont;        // [3][T] transport side output, allocated when first enabled
     DBuf<double> errind;        // adaption error indicator: raw [T], scaled [T], nodal [V], tolerances [M]
+    DBuf<double> wind;          // wind: element stress x [T], y [T], nodal values x [V], y [V], factors [M]
+    DBuf<int> wind_flag;        // [M] wind stress flag per material
+    bool wind_on = false;
     bool dacont_on = false;
     bool has_ovh = false;       // some edge string is NB OVH (its velocity series go up every step)
     DBuf<int> slot_ptr, slot_idx, blk_ptr, blk_src, rowptr, col, blk_row, dpos;
@@ -1519,6 +1522,54 @@ int sw2gpu_mass_flux(sw2gpu_ctx* c, double density, double* flux) {
     if (!c || !flux) return fail(SW2GPU_E_ARG, "bad context or output");
     if (!(c->dt > 0.0)) return fail(SW2GPU_E_ARG, "no step taken yet (dt unset)");
     return mass_reduce(c, true, c->H(0), density, flux);
+}
+
+int sw2gpu_set_wind(sw2gpu_ctx* c, const int32_t* mat_flag, const double* mat_windatt, const double* stress_x,
+                    const double* stress_y) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    if (!stress_x || !stress_y) {   // off
+        c->wind_on = false;
+        c->dm.wsx = c->dm.wsy = nullptr;
+        c->drop_graphs();
+        return SW2GPU_OK;
+    }
+    if (!mat_flag || !mat_windatt) return fail(SW2GPU_E_ARG, "null material wind tables");
+    const int T = c->T, V = c->V, M = std::max(c->M, 1);
+    std::vector<double> fac(M, 0.0);
+    std::vector<int> flag(M, 0);
+    for (int k = 0; k < c->M; k++) {
+        if (mat_flag[k] != 0 && mat_flag[k] != 1)
+            return fail(SW2GPU_E_ARG, "material %d: wind stress flag %d not supported (0 or 1)", k, mat_flag[k]);
+        flag[k] = mat_flag[k];
+        fac[k] = std::pow(mat_windatt[k], 2.0) / (3 * c->p.density);   // smeteor.c:302-303
+    }
+    if (!c->wind.p) {
+        g_alloc_bytes = &c->bytes;
+        int rc = zalloc(c->wind, 2 * (size_t)T + 2 * (size_t)V + M, c->stream);
+        if (!rc) rc = zalloc(c->wind_flag, M, c->stream);
+        g_alloc_bytes = nullptr;
+        if (rc) return rc;
+    }
+    double* wsx = c->wind.p;
+    double* wsy = wsx + T;
+    double* nsx = wsy + T;
+    double* nsy = nsx + V;
+    double* fd = nsy + V;
+    CK(cudaMemcpyAsync(nsx, stress_x, sizeof(double) * V, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(nsy, stress_y, sizeof(double) * V, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(fd, fac.data(), sizeof(double) * M, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->wind_flag.p, flag.data(), sizeof(int) * M, cudaMemcpyHostToDevice, c->stream));
+    if (T) {
+        k_elem_wind<<<nblk(T, 256), 256, 0, c->stream>>>(c->dm, c->p.gravity, c->p.density, c->wind_flag.p, fd, nsx, nsy,
+                                                         wsx, wsy);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(c->stream));   // the host tables above are released on return
+    if (!c->wind_on) c->drop_graphs();      // the descriptors baked into captured steps change
+    c->wind_on = true;
+    c->dm.wsx = wsx;
+    c->dm.wsy = wsy;
+    return SW2GPU_OK;
 }
 
 int sw2gpu_elem_error(sw2gpu_ctx* c, const double* refine_tol, double* elem_error, double* node_error) {

@@ -34,7 +34,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
            "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont",
            "sw2gpu_set_wait_limits", "sw2gpu_snapshot", "sw2gpu_elem_error", "sw2gpu_set_mass_tracking",
-           "sw2gpu_step_mass"]
+           "sw2gpu_step_mass", "sw2gpu_set_wind"]
 
 
 class SW2Error(RuntimeError):
@@ -87,6 +87,7 @@ def lib():
         L.sw2gpu_snapshot.argtypes = [vp, C.c_int, vp, vp, vp]
         L.sw2gpu_elem_error.argtypes = [vp, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_set_mass_tracking.argtypes = [vp, C.c_int32, C.c_double]
+        L.sw2gpu_set_wind.argtypes = [vp, c_int32_p, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_step_mass.argtypes = [vp, c_double_p, c_double_p]
         L.sw2gpu_set_variant.argtypes = [vp, C.c_int32, C.c_int32]
         L.sw2gpu_get_variant.argtypes = [vp, c_int32_p, c_int32_p]
@@ -256,6 +257,17 @@ class SW2GPU:
         out = C.c_double()
         _check(lib().sw2gpu_mass_flux(self.h, rho, C.byref(out)))
         return out.value
+
+    def set_wind(self, mat_flag=None, mat_windatt=None, stress_x=None, stress_y=None):
+        """Wind surface stress: nodal wind values and per-material flag / attenuation; None: off."""
+        if stress_x is None:
+            _check(lib().sw2gpu_set_wind(self.h, None, None, None, None))
+            return
+        f = np.ascontiguousarray(mat_flag, dtype=np.int32)
+        a = np.ascontiguousarray(mat_windatt, dtype=np.float64)
+        sx = np.ascontiguousarray(stress_x, dtype=np.float64)
+        sy = np.ascontiguousarray(stress_y, dtype=np.float64)
+        _check(lib().sw2gpu_set_wind(self.h, _ip(f), _dp(a), _dp(sx), _dp(sy)))
 
     def set_mass_tracking(self, enable: bool = True, density=None):
         """Reduce the grid mass and the mass flux inside every accepted step (step_mass())."""

@@ -469,7 +469,7 @@ def cpu_reference_sample(points: int = 10000, steps: int = 4, procs: int = 1, ti
             shutil.rmtree(d, ignore_errors=True)
     elapsed = max(secs)
     return {"value": tri_steps / elapsed, "tri_steps": tri_steps, "seconds": elapsed,
-            "triangles": runs[0][0].nelems2d, "steps": steps, "procs": procs}
+            "triangles": runs[0][0].nelems2d, "steps": steps, "procs": procs, "op_blk": runs[0][0].params.nblock}
 
 
 def run_reference_arm(args, rank, world):
@@ -487,9 +487,11 @@ def run_reference_arm(args, rank, world):
         "data": "synthetic", "impl": "reference",
         "config": {"workload": f"reference AdH executable (serial C, profile-LU block-Jacobi BiCGSTAB) on "
                                f"{procs} concurrent seeded basins of {res['triangles']} triangles, "
-                               f"{res['steps']} steps each (bounded sample of the 1M-triangle workload)"},
+                               f"{res['steps']} steps each (bounded sample of the 1M-triangle workload)",
+                   "op_blk": res["op_blk"]},
         "cpu_baseline": {"value": res["value"], "unit": "triangle-steps/s", "cores": procs, "kind": "reference",
-                         "sample": f"{procs} x {res['triangles']} triangles x {res['steps']} steps"},
+                         "sample": f"{procs} x {res['triangles']} triangles x {res['steps']} steps, OP BLK {res['op_blk']}",
+                         "op_blk": res["op_blk"]},
         "e2e": {"value": res["value"], "unit": "triangle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -650,7 +652,8 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
         if cpu_res:
             cpu = {"value": cpu_res["value"], "unit": "triangle-steps/s", "cores": 1, "kind": "reference",
                    "sample": f"reference AdH executable, one seeded basin of {cpu_res['triangles']} triangles "
-                             f"from the same generator, 3 steps, time loop only ({cpu_res['seconds']:.1f} s)"}
+                             f"from the same generator, 3 steps, OP BLK {cpu_res['op_blk']}, time loop only "
+                             f"({cpu_res['seconds']:.1f} s)", "op_blk": cpu_res["op_blk"]}
     line = {
         "metric": METRIC, "value": value, "unit": "triangle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",

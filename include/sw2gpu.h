@@ -164,6 +164,17 @@ int sw2gpu_snapshot(sw2gpu_ctx *ctx, int level, double *d_h, double *d_u, double
 /* Overrides the element wet/dry flags (normally set by the step's fe_sw2_init). */
 int sw2gpu_set_wd_flag(sw2gpu_ctx *ctx, const int32_t *wd_flag);
 
+/* Wind surface stress (fe_sw2_body_resid.c:674-719 with swind_elem2d_get_local_stress,
+ * src/structs/smeteor.c:241-306): stress_x / stress_y [nnodes] are the nodal wind values the
+ * reference's meteor_update puts in winds[node].stress for the coming step; mat_flag[nmats] the
+ * material's wind stress form (MP WND STR: 0 = the values are the stress, 1 = Wu's drag law of a
+ * wind speed; the depth-dependent form 2 is not built and is rejected with SW2GPU_E_ARG) and
+ * mat_windatt[nmats] its attenuation (MP WND ATT).  The element stress, the vertex average
+ * scaled by windatt^2 / (3 density), enters the momentum residual of fully wet elements.  Kept
+ * until the next call; stress_x = NULL turns the term off (the default). */
+int sw2gpu_set_wind(sw2gpu_ctx *ctx, const int32_t *mat_flag, const double *mat_windatt, const double *stress_x,
+                    const double *stress_y);
+
 /* Mass-balance diagnostics (src/tools/tl_grid_mass.c), on the device.
  * sw2gpu_grid_mass: water mass of time level `level` times `density`
  * (tl_find_grid_mass_elem2d, :20-97; partially dry triangles by the h < 0 corner clip of

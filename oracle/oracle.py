@@ -57,6 +57,8 @@ def lib():
         L.orc_get_dacont.argtypes = [C.c_void_p, c_double_p]
         L.orc_edge_resid.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, c_double_p, c_double_p]
         L.orc_elem_error.argtypes = [C.c_void_p, c_double_p, c_double_p, c_double_p]
+        L.orc_set_wind.argtypes = [C.c_void_p, c_int32_p, c_double_p, c_double_p, c_double_p]
+        L.orc_set_wind.restype = C.c_int
         L.orc_grid_mass.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.orc_grid_mass.restype = C.c_double
         L.orc_mass_flux.argtypes = [C.c_void_p, C.c_double, C.c_double, c_double_p]
@@ -169,6 +171,18 @@ class Oracle:
         out = np.zeros(7)
         lib().orc_geometry(self.h, ie, _dp(out))
         return out[0], out[1:]
+
+    def set_wind(self, mat_flag=None, mat_windatt=None, stress_x=None, stress_y=None):
+        """Wind surface stress from nodal wind values (None: off)."""
+        if stress_x is None:
+            lib().orc_set_wind(self.h, None, None, None, None)
+            return
+        f = np.ascontiguousarray(mat_flag, dtype=np.int32)
+        a = np.ascontiguousarray(mat_windatt, dtype=np.float64)
+        sx = np.ascontiguousarray(stress_x, dtype=np.float64)
+        sy = np.ascontiguousarray(stress_y, dtype=np.float64)
+        if lib().orc_set_wind(self.h, f.ctypes.data_as(c_int32_p), _dp(a), _dp(sx), _dp(sy)):
+            raise ValueError("wind stress flag not supported")
 
     def elem_error(self, refine_tol):
         """Adaption error indicator (ssw_2d_calculate_elem_error) of the current and old levels

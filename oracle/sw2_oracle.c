@@ -70,6 +70,7 @@ typedef struct orc_ctx {
     double *dacont;            /* [3T] elem_rhs_dacont_extra_terms of the last body_resid call per element */
     double dt;
     double *series;
+    double *wsx, *wsy;         /* [T] element wind stress (orc_set_wind), or NULL: no wind */
     /* BCSR pattern (sorted columns, diagonal included) */
     int *rowptr, *col, nnzb;
     int *blk_of_pair;          /* [9*T] value block of (i, j) pair of each element */
@@ -520,6 +521,14 @@ static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof
         for (i = 0; i < 3; i++) { er[i].x += rx[i]; er[i].y += ry[i]; }
     }
 
+    /* wind surface stress, fully wet elements only :674-719 (no wave stress: 0) */
+    if (wd == 0 && C->wsx) {
+        double rx[3] = {0, 0, 0}, ry[3] = {0, 0, 0};
+        tri_phi(djac, C->wsx[ie] + 0.0, rx);
+        tri_phi(djac, C->wsy[ie] + 0.0, ry);
+        for (i = 0; i < 3; i++) { er[i].x -= dt * rx[i]; er[i].y -= dt * ry[i]; }
+    }
+
     /* rainfall :728-754 */
     double water_source = 0.;
     if (C->str_bc[str] == SW2GPU_BCT_WATER_SOURCE) {
@@ -844,7 +853,7 @@ void orc_destroy(orc_ctx *C) {
     free(C->x); free(C->y); free(C->z); free(C->node_string); free(C->tri); free(C->tri_mat);
     free(C->edges); free(C->edge_string); free(C->edge_parent); free(C->str_bc); free(C->str_isigma);
     free(C->str_ivx); free(C->str_ivy); free(C->str_iu0); free(C->str_rough); free(C->mat_eev_mode);
-    free(C->mat_ev); free(C->mat_eev_coef); free(C->mat_cor); free(C->series);
+    free(C->mat_ev); free(C->mat_eev_coef); free(C->mat_cor); free(C->series); free(C->wsx); free(C->wsy);
     for (k = 0; k < 3; k++) { free(C->h[k]); free(C->u[k]); free(C->v[k]); }
     free(C->wd); free(C->dacont); free(C->resid); free(C->sol); free(C->include); free(C->djac); free(C->grad);
     free(C->edjac); free(C->enrml); free(C->rowptr); free(C->col); free(C->blk_of_pair); free(C->eblk_of_pair);
@@ -1540,4 +1549,48 @@ void orc_elem_error(const orc_ctx *C, const double *refine_tol, double *elem_err
     }
     for (i = 0; i < C->V; i++) node_error[i] /= (double) cnt[i];
     free(cnt);
+}
+
+/* ------------------------------------------------------------------------------ */
+/* Wind (meteor_update, swind_elem2d_get_local_stress, src/structs/smeteor.c:241-300;
+ * winds_proc_wu, src/meteor/winds_proc_wu.c:5-26): the nodal wind values stress_x/y (what
+ * meteor_update puts in winds[node].stress) turned into a shear per the element's material
+ * flag (0: the value itself, 1: Wu's drag law; the depth-dependent form 2 is not restated),
+ * summed over the three vertices and scaled by windatt^2 / (3 density).  NULL stresses turn the
+ * term off. */
+static void wind_wu(double gravity, double xs, double ys, double *sx, double *sy) {
+    double wmag = sqrt(pow(xs, 2.0) + pow(ys, 2.0) + 1e-10), x = xs, y = ys, cd;
+    if (gravity > 10.) { wmag *= 0.3048; x *= 0.3048; y *= 0.3048; }
+    cd = (0.8 + 0.065 * wmag) * .001;
+    if (gravity > 10.) { *sx = 1.225 * cd * x * wmag * 0.020885; *sy = 1.225 * cd * y * wmag * 0.020885; }
+    else { *sx = 1.225 * cd * x * wmag; *sy = 1.225 * cd * y * wmag; }
+}
+int orc_set_wind(orc_ctx *C, const int *mat_flag, const double *mat_windatt, const double *stress_x,
+                 const double *stress_y) {
+    int e, i;
+    free(C->wsx); free(C->wsy);
+    C->wsx = C->wsy = NULL;
+    if (!stress_x || !stress_y) return 0;
+    C->wsx = (double *) calloc((size_t) (C->T ? C->T : 1), sizeof(double));
+    C->wsy = (double *) calloc((size_t) (C->T ? C->T : 1), sizeof(double));
+    const double rho = C->p.density;
+    for (e = 0; e < C->T; e++) {
+        const int m = C->tri_mat[e];
+        if (mat_flag[m] < 0 || mat_flag[m] > 1) return 1;
+        double wx = 0., wy = 0.;
+        for (i = 0; i < 3; i++) {
+            const int n = C->tri[3 * e + i];
+            double sx = 0., sy = 0.;
+            if (rho > 0.0) {
+                if (mat_flag[m] == 0) { sx = stress_x[n]; sy = stress_y[n]; }
+                else wind_wu(C->p.gravity, stress_x[n], stress_y[n], &sx, &sy);
+            }
+            wx += sx;
+            wy += sy;
+        }
+        const double f = pow(mat_windatt[m], 2.0) / (3 * rho);
+        C->wsx[e] = wx * f;
+        C->wsy[e] = wy * f;
+    }
+    return 0;
 }

@@ -41,13 +41,16 @@ using namespace sw2;
 // geo: djac, gx0, gy0, gx1, gy1, gx2, gy2; phys: g, dll, dul, alpha, tau_pg, dt;
 // mat: ks, ev_st, ev_tr, eev_coef, cor_speed, water_src; dflag: the vertices' Dirichlet flags;
 // dac: null, or the transport side output (continuity parts of shock capturing and SUPG);
+// ws: null, or the element's wind surface stress (x, y);
 // pre: evaluate the way the wet Jacobian kernel does (fully wet elements, perturbed calls only):
 // the parts the perturbation leaves unchanged precomputed once per element (WetPre) from the
 // unperturbed iterate, as the kernel's staging warp forms them, and the column's `fix` mask
 extern "C" void host_elem_resid(const double* xyz, const double* lv, const double* geo, int wd, int pvar, int pnode,
                                 double dx, const double* phys, const double* mat, int eev_mode, int has_source,
-                                int pre, const int* dflag, double* out, double* dac) {
+                                int pre, const int* dflag, double* out, double* dac, const double* ws) {
     ElemIn in;
+    in.wsx = ws ? ws[0] : 0.0;   // the element's wind surface stress
+    in.wsy = ws ? ws[1] : 0.0;
     for (int i = 0; i < 3; i++) {
         in.x[i] = xyz[i]; in.y[i] = xyz[3 + i]; in.z[i] = xyz[6 + i];
         in.h[i] = lv[i]; in.u[i] = lv[3 + i]; in.v[i] = lv[6 + i];
@@ -177,8 +180,29 @@ def _dirichlet_flags(m):
     return per_string[np.where(m.node_string >= 0, m.node_string, len(m.strings))]
 
 
-@pytest.mark.parametrize("case", ["all_terms", "terms_fixture", "rain", "obstacle", "combined"])
+def _element_wind(m, flags, att, sx, sy, density):
+    """Element wind stress as swind_elem2d_get_local_stress forms it (vertex sum in order, then
+    windatt^2 / (3 density)); flag 1 is Wu's drag law (winds_proc_wu) of the nodal value."""
+    def wu(g, xs, ys):
+        wmag = math.sqrt(math.pow(xs, 2.0) + math.pow(ys, 2.0) + 1e-10)
+        cd = (0.8 + 0.065 * wmag) * .001
+        return 1.225 * cd * xs * wmag, 1.225 * cd * ys * wmag
+    out = np.zeros((m.nelems2d, 2))
+    for e, nodes in enumerate(m.tri):
+        k = int(m.tri_mat[e])
+        wx = wy = 0.0
+        for n in nodes:
+            a, b = (sx[n], sy[n]) if flags[k] == 0 else wu(m.params.gravity, sx[n], sy[n])
+            wx += a
+            wy += b
+        f = math.pow(att[k], 2.0) / (3 * density)
+        out[e] = (wx * f, wy * f)
+    return out
+
+
+@pytest.mark.parametrize("case", ["all_terms", "terms_fixture", "rain", "obstacle", "combined", "wind"])
 def test_device_physics_matches_oracle_on_host(host_physics, case):
+    wind = None
     if case == "combined":
         m = meshgen.basin_combined(nsteps=4)
     elif case == "terms_fixture":   # the all-terms reference fixture's model (EEV mode 3, southern Coriolis)
@@ -187,12 +211,22 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
         m = meshgen.basin_rain(nsteps=4)
     elif case == "obstacle":
         m = meshgen.channel_obstacle(nsteps=4, with_depth=True)
+    elif case == "wind":   # wind surface stress on fully wet elements, both stress forms
+        m = meshgen.bumpy_basin(900, seed=5, size=2500.0, nsteps=4, dt=5.0, nbins=3, name="wind")
     else:
         base = meshgen.bumpy_basin(900, seed=5, size=2500.0, nsteps=4, dt=5.0, nbins=3, name="physics")
         m = dataclasses.replace(
             base, params=dataclasses.replace(base.params, tau_temporal=0.5),
             materials=[Material(evs=(6.0, 2.0, 1.0), coriolis=30.0)] + [Material(eev_coef=0.4, eev_mode=k) for k in (1, 2)])
     o = Oracle(m)
+    if case == "wind":
+        wrng = np.random.Generator(np.random.PCG64(17))
+        flags = np.array([0, 1, 0], np.int32)
+        att = np.array([1.0, 0.8, 0.5])
+        sx = wrng.normal(0.0, 0.3, m.nnodes)
+        sy = wrng.normal(0.0, 0.3, m.nnodes)
+        o.set_wind(flags, att, sx, sy)
+        wind = _element_wind(m, flags, att, sx, sy, m.params.density)
     for _ in range(2):   # distinct time levels and moving wet/dry fronts
         assert o.step()["status"] == 0
     series = m.series_values(o.t, o.t + m.dt)
@@ -236,17 +270,20 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
             b = int(rng.integers(0, 3))
             eps = _fd_eps(arr[nodes[b]])
             cases += [(pvar, b, eps, 1), (pvar, b, -eps, -1)]
+        ws = None if wind is None else np.ascontiguousarray(wind[ie])
         for pvar, b, dx, sign in cases:
             dev, ref, dac = np.zeros(9), np.zeros(9), np.zeros(3)
             host_physics.host_elem_resid(_dp(xyz), _dp(lv), _dp(geo), int(wd[ie]), pvar, b, C.c_double(dx), _dp(phys),
                                          _dp(mat), mt.eev_mode, int(source), 0,
-                                         df.ctypes.data_as(C.POINTER(C.c_int)), _dp(dev), _dp(dac))
+                                         df.ctypes.data_as(C.POINTER(C.c_int)), _dp(dev), _dp(dac),
+                                         None if ws is None else _dp(ws))
             oracle_lib().orc_body_resid(o.h, int(ie), abs(dx), b, pvar, sign, _dp(ref))
             if fully_wet and pvar != -1:   # the wet Jacobian kernel's evaluation of the same column
                 pre = np.zeros(9)
                 host_physics.host_elem_resid(_dp(xyz), _dp(lv), _dp(geo), 0, pvar, b, C.c_double(dx), _dp(phys),
                                              _dp(mat), mt.eev_mode, int(source), 1,
-                                             df.ctypes.data_as(C.POINTER(C.c_int)), _dp(pre), None)
+                                             df.ctypes.data_as(C.POINTER(C.c_int)), _dp(pre), None,
+                                             None if ws is None else _dp(ws))
                 assert np.array_equal(pre, ref), (int(ie), pvar, b, sign, pre, ref)
                 wet_columns += 1
             # the transport side output of the same call (elem_rhs_dacont_extra_terms)

@@ -37,8 +37,8 @@ REF = os.path.join(ROOT, "oracle", "_ref")
 GPU_EXE = os.path.join(REF, "adh_gpu")
 CPU_EXE = os.path.join(REF, "adh_dump")
 QA = os.path.join(REF, "qa")
-# decks whose physics the library covers (wind stress, used by wet_dry, is not built)
-CASES = ["angle_nb", "angle_source", "angle_dam", "angle_coriolis"]
+# the reference's SW2 QA decks on triangles (wet_dry runs with a wind series, MP WND STR 0)
+CASES = ["wet_dry", "angle_nb", "angle_source", "angle_dam", "angle_coriolis"]
 NUM = re.compile(r"[-+]?\d+\.\d*(?:[eE][-+]?\d+)?|[-+]?\d+[eE][-+]?\d+")
 
 

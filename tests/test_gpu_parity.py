@@ -271,3 +271,26 @@ def test_mass_reduced_inside_the_step_equals_the_on_demand_diagnostics():
         mass, flux = g.step_mass()
         assert mass == g.grid_mass(0) and flux == g.mass_flux()
     g.close()
+
+
+def test_wind_stress_residual_and_steps_match_oracle():
+    """Wind surface stress (both stress forms, per-material attenuation) on the wet/dry basin:
+    the device residual and three steps against the oracle with the same nodal winds."""
+    m = basin_model()
+    rng = np.random.Generator(np.random.PCG64(29))
+    nm = len(m.materials)
+    flags = np.array([k % 2 for k in range(nm)], np.int32)
+    att = np.linspace(1.0, 0.6, nm)
+    sx, sy = rng.normal(0.0, 0.2, m.nnodes), rng.normal(0.0, 0.2, m.nnodes)
+    g, o = SW2GPU(m), Oracle(m)
+    for s in (g, o):
+        s.set_wind(flags, att, sx, sy)
+        s.set_dt(m.dt, m.series_values(0.0, m.dt))
+    o.wdflag()
+    g.set_wd(o.get_wd())
+    assert relerr(g.resid(), o.resid()) <= 1e-12
+    for _ in range(3):
+        a, b = g.step(), o.step()
+        assert a["status"] == 0 and b["status"] == 0 and abs(a["newton_its"] - b["newton_its"]) <= 1
+        errs = field_errors(fields(*g.get_state(0)), fields(*o.get_state(0)))
+        assert max(errs.values()) <= 1e-10, errs
