@@ -6,7 +6,8 @@ Mirrors the reference's SW2 plug-in interface:
   time step, returning YES/NO semantics through an exception-free status code;
 * :meth:`SW2GPU.resid`  -- ``fe_sw2_resid``;  :meth:`SW2GPU.load` -- ``fe_sw2_load``;
 * :func:`run`           -- the dt-retry loop of ``adh_run_func_``/``fe_main``
-  (src/main/adh_func.c:535-549): a failed step is retried with dt * 0.25 (tc_scale).
+  (src/main/adh_func.c:535-549): a failed step is retried with dt * 0.25 (tc_scale), and dt
+  doubles back toward the nominal one after every accepted step (tc_end).
 
 There is no CPU fallback: if the CUDA library or a GPU is missing, construction fails.
 """
@@ -506,12 +507,13 @@ class SW2Server:
 
 
 def run(solver: SW2GPU, nsteps: int, dt: float = None, max_retries: int = 8, callback=None):
-    """Time loop with the reference's failure contract: a step that returns NO is
-    retried from the old state with dt * 0.25 (src/tools/tc_scale.c:3-17)."""
+    """Time loop with the reference's step-size rule: a step that returns NO is retried from
+    the old state with dt * 0.25 (tc_scale, src/tools/tc_scale.c:3-17), and after every accepted
+    step dt doubles again, up to the nominal dt (tc_end, src/tools/tc_end.c:55-66)."""
     dt = solver.model.dt if dt is None else dt
     out = []
+    d = dt
     for k in range(nsteps):
-        d = dt
         for _ in range(max_retries + 1):
             st = solver.step(dt=d)
             if st["status"] == 0:
@@ -523,4 +525,5 @@ def run(solver: SW2GPU, nsteps: int, dt: float = None, max_retries: int = 8, cal
         out.append(st)
         if callback:
             callback(k, st)
+        d = min(2.0 * d, dt)
     return out

@@ -121,8 +121,9 @@ const char *sw2gpu_last_error(void);
 int sw2gpu_create(const sw2gpu_mesh *mesh, const sw2gpu_params *params, void *stream, sw2gpu_ctx **out);
 int sw2gpu_destroy(sw2gpu_ctx *ctx);
 /* Launch variants (no counterpart in the reference).  Two knobs change the speed of a step,
- * never its results: the register budget of the wet-Jacobian kernel (jac_minb: 1 or 2
- * resident CTAs per SM) and the depth of the Krylov kernel's shared-memory tile ring (stages:
+ * never its results: the wet-Jacobian kernel (jac_minb: 1 or 2 = the register budget for 1 or 2
+ * resident CTAs per SM, 3 = seven warps per SM with both perturbed evaluations of a column in
+ * flight per thread) and the depth of the Krylov kernel's shared-memory tile ring (stages:
  * 0 = sweeps read global memory, 2 or 3).  sw2gpu_autotune times every variant on the
  * context's own mesh and current state (which it leaves as it found it) and keeps the
  * fastest; a batch uses the variants of its instance with the most blocks. */
@@ -269,9 +270,9 @@ int sw2gpu_batch_destroy(sw2gpu_batch *b);
  * Instances of uneven size join and leave an engine between ticks.  A tick starts a time
  * step for every instance between steps (step-averaged series, level shift, fe_sw2_init,
  * residual) and runs one Newton iteration for every instance inside a step, each phase as
- * one launch over all of them.  A failed step is retried with dt / 4, as the reference's
- * time loop does, and the step after a successful retry starts again from the base dt; an
- * instance computes exactly what sw2gpu_step computes for it alone.
+ * one launch over all of them.  A failed step is retried with dt / 4 and dt doubles again
+ * after every accepted step, up to the base dt, as the reference's time loop does (tc_scale,
+ * tc_end); an instance computes exactly what sw2gpu_step computes for it alone.
  * The engine does not own the contexts; an instance that finished leaves the engine and is
  * reported by the tick. */
 typedef struct sw2gpu_engine sw2gpu_engine;

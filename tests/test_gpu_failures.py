@@ -122,7 +122,7 @@ def test_create_rejects_unsupported_node_strings(what):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("stages,barrier_polls,copy_polls", [(0, 1, 0), (3, 0, 1)])
+@pytest.mark.parametrize("stages,barrier_polls,copy_polls", [(0, 1, 0), (3, 1, 0), (3, 0, 1)])
 def test_device_wait_that_runs_out_ends_the_step_with_timeout(stages, barrier_polls, copy_polls):
     """A Krylov grid-barrier wait (direct sweeps) or tile-copy wait (staged sweeps) bounded to
     one poll runs out: no fault, no hang -- the kernel flags the error and returns, the step
