@@ -548,135 +548,6 @@ __global__ void __launch_bounds__(kJacWetThreads, MINB) k_jac_elem_wet(const __g
     }
 }
 
-// The same columns with both perturbed evaluations in flight: R(x + eps e_j) and R(x - eps e_j)
-// are two independent residual bodies in one straight-line block, which the scheduler
-// interleaves; the entries are (R+ - R-) / (2 eps) formed exactly as jac_column forms them (the
-// same bits), with its Dirichlet zeroing, written to the element's record g[81].
-__device__ __forceinline__ void jac_column_pair(const DevMesh& m, const PhysParams& P, const StagedElem& S,
-                                                const WetPre* pre, int item, double* g) {
-    const int b = item / 3, var = item % 3;
-    const MatParams M = m.mats[S.mat];
-    double hp[3], up[3], vp[3], hm[3], um[3], vm[3];
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-        hp[i] = hm[i] = S.in.h[i];
-        up[i] = um[i] = S.in.u[i];
-        vp[i] = vm[i] = S.in.v[i];
-    }
-    double cur = 0.0;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-        if (i == b) cur = (var == 0) ? up[i] : (var == 1) ? vp[i] : hp[i];
-    const double eps = fd_eps(cur);
-    const int pv = (var == 0) ? kPertU : (var == 1) ? kPertV : kPertH;
-    const unsigned fix = (var == 0)   ? (kFixH | kFixV | ((7u & ~(1u << b)) << kFixNode))
-                         : (var == 1) ? (kFixH | kFixU | ((7u & ~(1u << b)) << kFixNode))
-                                      : (kFixU | kFixV | (7u << kFixNode));
-    unsigned Dm = 0, Pm = 0;
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-        const int f = m.qflag[i];
-        if (S.in.ho[i] <= 0.) Dm |= 1u << i;
-        if (f & 1) Pm |= 1u << i;
-        if (f & 2) Dm |= 1u << i;
-        if (f & 4) { Dm |= 1u << i; Pm |= 1u << i; }
-    }
-    const double ie2 = 1.0 / (2.0 * eps);
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-        if (i == b) {
-            if (var == 0) { up[i] = cur + eps; um[i] = cur - eps; }
-            else if (var == 1) { vp[i] = cur + eps; vm[i] = cur - eps; }
-            else { hp[i] = cur + eps; hm[i] = cur - eps; }
-        }
-    }
-    double rp[3][3], rm[3][3];
-    elem_resid_impl<true, true>(S.in, hp, up, vp, S.wd, pv, P, M, S.df, rp, pre, fix);
-    elem_resid_impl<true, true>(S.in, hm, um, vm, S.wd, pv, P, M, S.df, rm, pre, fix);
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-#pragma unroll
-        for (int eq = 0; eq < 3; eq++) {
-            const int row = (eq == 0) ? 2 : eq - 1;
-            double val = (rp[a][eq] - rm[a][eq]) * ie2;
-            const bool aD = (Dm >> a) & 1u, bD = (Dm >> b) & 1u, aP = (Pm >> a) & 1u, bP = (Pm >> b) & 1u;
-            const bool zero = (aD && row < 2) || (bD && var < 2) || (aP && row == 2) || (bP && var == 2);
-            const bool one = (a == b) && ((aD && ((var == 0 && row == 0) || (var == 1 && row == 1))) ||
-                                          (aP && var == 2 && row == 2));
-            if (one) val = 1.0;
-            else if (zero) val = 0.0;
-            g[(3 * a + b) * 9 + 3 * row + var] = val;
-        }
-    }
-}
-
-// Fully wet elements, the variant with two evaluations in flight per thread: a persistent CTA of
-// six column warps and one staging warp walks groups of 64 elements; column thread t takes
-// element t % 64 and vertex t / 64 and evaluates that vertex's three columns (u, v, h) one after
-// the other with jac_column_pair.  Seven warps per SM leave each thread up to 255 registers
-// (two warps per scheduler), room for the two residual bodies side by side.  Buffers are handed
-// over as in k_jac_elem_wet (FULL / EMPTY named barriers, two buffers).  Same bits.
-constexpr int kJacIlpElems = 64;
-constexpr int kJacIlpThreads = kJacIlpElems * 3 + 32;
-struct JacIlpSmem {
-    StagedElem se[kJacBufs][kJacIlpElems];
-    WetPre pre[kJacBufs][kJacIlpElems];
-    int eid[kJacBufs][kJacIlpElems];
-};
-constexpr size_t kJacIlpSmem = sizeof(JacIlpSmem);
-
-template <class Src>
-__global__ void __launch_bounds__(kJacIlpThreads, 1) k_jac_elem_wet_ilp(const __grid_constant__ Src src, int nvirt) {
-    extern __shared__ __align__(16) unsigned char jac_smem[];
-    JacIlpSmem& sm = *reinterpret_cast<JacIlpSmem*>(jac_smem);
-    const int stride = gridDim.x;
-    if (threadIdx.x >= kJacIlpElems * 3) {   // the staging warp: two elements per lane
-        const int lane = threadIdx.x - kJacIlpElems * 3;
-        for (int i = 0, v = blockIdx.x; v < nvirt; i++, v += stride) {
-            const int j = i % kJacBufs;
-            if (i >= kJacBufs) bar_sync_n(kJacBarEmpty + j, kJacIlpThreads);
-            int lb, nb;
-            const Inst& I = src.get_at(v, nvirt, lb, nb);
-            const DevMesh m = I.m;
-            const int e0 = lb * kJacIlpElems;
-#pragma unroll 1
-            for (int h = 0; h < 2; h++) {
-                const int q = lane + 32 * h;
-                int e = -1;
-                if (e0 + q < m.T && I.ewet[e0 + q]) e = e0 + q;
-                sm.eid[j][q] = e;
-                if (e >= 0) {
-                    StagedElem& S = sm.se[j][q];
-                    stage_elem(m, I.s, e, S);
-                    WetPre& p = sm.pre[j][q];
-                    wet_levels(S.in, I.P, p.L);
-                    wet_depth(S.in, S.in.h, I.P, m.mats[S.mat], p.D);
-                    wet_pre_velocity(S.in, p);
-                }
-            }
-            __syncwarp();
-            bar_arrive_n(kJacBarFull + j, kJacIlpThreads);
-        }
-        return;
-    }
-    const int q = threadIdx.x % kJacIlpElems;   // element of the group
-    const int b = threadIdx.x / kJacIlpElems;   // its vertex
-    for (int i = 0, v = blockIdx.x; v < nvirt; i++, v += stride) {
-        const int j = i % kJacBufs;
-        bar_sync_n(kJacBarFull + j, kJacIlpThreads);
-        int lb, nb;
-        const Inst& I = src.get_at(v, nvirt, lb, nb);
-        const int e = sm.eid[j][q];
-        if (e >= 0) {
-#pragma unroll 1
-            for (int var = 0; var < 3; var++)
-                jac_column_pair(I.m, I.P, sm.se[j][q], &sm.pre[j][q], 3 * b + var, I.jslots + (size_t)e * 81);
-        }
-        __syncwarp();
-        if (v + kJacBufs * stride < nvirt) bar_arrive_n(kJacBarEmpty + j, kJacIlpThreads);
-    }
-}
-
 // Elements of the general list (some vertex dry at some level, or a wet/dry-flagged
 // element), full wet/dry physics; the list length is the one the last residual evaluation
 // recorded.  One CTA per 32 listed elements.

@@ -254,9 +254,8 @@ struct Runner {
     Norms* norms_h = nullptr;     // pinned mirrors, one entry per instance
     KrylovCtl* ctl_h = nullptr;
     int stages = 0;               // Krylov tile-ring depth in use (0: sweeps from global memory)
-    int jac_minb = 2;             // wet-Jacobian variant in use (1, 2: register budget for 1 or 2
-                                  // CTAs per SM; 3: two evaluations in flight per thread)
-    int jac_ctas[3] = {0, 0, 0};  // persistent wet-Jacobian grid per variant (co-resident CTAs)
+    int jac_minb = 2;             // wet-Jacobian variant in use (register budget for 1 or 2 CTAs per SM)
+    int jac_ctas[2] = {0, 0};     // persistent wet-Jacobian grid per variant (co-resident CTAs)
     bool jac_ready = false;       // jac_ctas set (kernel attributes applied)
     unsigned c_off = 0, r_off = 0, v_off = 0, stage_bytes = 0;
     size_t smem = 0;
@@ -440,13 +439,8 @@ int runner_set(Runner& R, const std::vector<sw2gpu_ctx*>& ctx) {
     }
     int want = big ? big->tune_stages : 3;
     R.jac_minb = big ? big->tune_jac_minb : 2;
-    auto fitting_variant = [&R] {   // a wet-Jacobian variant that does not fit yields to one that does
-        if (!R.jac_ready || R.jac_ctas[R.jac_minb - 1]) return;
-        for (int v = 1; v <= 3; v++)
-            if (R.jac_ctas[v - 1]) {
-                R.jac_minb = v;
-                return;
-            }
+    auto fitting_variant = [&R] {   // a wet-Jacobian variant that does not fit yields to the other
+        if (R.jac_ready && !R.jac_ctas[R.jac_minb - 1] && R.jac_ctas[2 - R.jac_minb]) R.jac_minb = 3 - R.jac_minb;
     };
     fitting_variant();
     const unsigned c_off = a_cap, r_off = c_off + c_cap;
@@ -496,17 +490,6 @@ int runner_set(Runner& R, const std::vector<sw2gpu_ctx*>& ctx) {
                 fit = std::min(fit, n);
             }
             R.jac_ctas[v] = sms * fit;   // 0: the variant does not fit on this device
-        }
-        {
-            const void* ilp[2] = {(const void*)k_jac_elem_wet_ilp<SrcOne>, (const void*)k_jac_elem_wet_ilp<SrcPar>};
-            int fit = 1 << 30;
-            for (int k = 0; k < 2; k++) {
-                int n = 0;
-                CK(cudaFuncSetAttribute(ilp[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacIlpSmem));
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ilp[k], kJacIlpThreads, kJacIlpSmem));
-                fit = std::min(fit, n);
-            }
-            R.jac_ctas[2] = sms * fit;
         }
     }
     fitting_variant();
@@ -684,16 +667,7 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
     };
     if (!R.jac_ctas[R.jac_minb - 1])
         return fail(SW2GPU_E_CUDA, "wet-Jacobian variant %d does not fit on this device", R.jac_minb);
-    int rc = 0;
-    if (R.jac_minb == 3) {
-        rc = launch_map(R, sub, kJacIlpThreads, [&](int k) { return nblk(C(k)->T, kJacIlpElems); },
-                        [&](const auto& src, int nb_, int th_) {
-                            k_jac_elem_wet_ilp<std::decay_t<decltype(src)>>
-                                <<<std::min(nb_, R.jac_ctas[2]), th_, kJacIlpSmem, R.stream>>>(src, nb_);
-                        });
-    } else {
-        rc = R.jac_minb == 1 ? wet(std::integral_constant<int, 1>{}) : wet(std::integral_constant<int, 2>{});
-    }
+    int rc = R.jac_minb == 1 ? wet(std::integral_constant<int, 1>{}) : wet(std::integral_constant<int, 2>{});
     if (rc) return rc;
     // a captured launch covers the largest list (the kernel reads the list's length itself)
     if ((rc = launch_map(R, sub, kJacThreads,
@@ -1727,8 +1701,8 @@ int sw2gpu_linear_solve(sw2gpu_ctx* c, const double* val, const double* rhs, dou
 }
 
 int sw2gpu_set_variant(sw2gpu_ctx* c, int32_t jac_minb, int32_t stages) {
-    if (!c || jac_minb < 1 || jac_minb > 3 || (stages != 0 && stages != 2 && stages != 3))
-        return fail(SW2GPU_E_ARG, "variant: jac_minb 1|2|3, stages 0|2|3");
+    if (!c || (jac_minb != 1 && jac_minb != 2) || (stages != 0 && stages != 2 && stages != 3))
+        return fail(SW2GPU_E_ARG, "variant: jac_minb 1|2, stages 0|2|3");
     c->tune_jac_minb = jac_minb;
     c->tune_stages = stages;
     c->drop_graphs();
@@ -1780,7 +1754,7 @@ int sw2gpu_autotune(sw2gpu_ctx* c, int32_t* jac_minb, int32_t* stages) {
     };
     int best_j = c->tune_jac_minb;
     float tb = 1e30f;
-    for (int m : {1, 2, 3}) {
+    for (int m : {1, 2}) {
         if (!R.jac_ctas[m - 1]) continue;   // does not fit on this device
         R.jac_minb = m;
         float t = 1e30f;

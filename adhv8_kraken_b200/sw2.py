@@ -118,11 +118,14 @@ def _ip(a):
 
 
 # Krylov stopping floors.  The reference preconditions with an exact LU of the whole system,
-# so its linear solves are exact to round-off; the plain FP64 path reaches toward that
-# (relative floor 1e-10, about where block-Jacobi BiCGSTAB on these systems stops improving;
-# the library tightens each Newton iteration's test against tol_nonlin).  The mixed path's
-# FP32 inner solves stop at 1e-6 (at most 100 iterations) and the FP64 Newton loop refines.
-DEFAULT_TOL = {capi.SW2GPU_FP64: (1e-10, 1e-30), capi.SW2GPU_MIXED: (1e-6, 1e-30)}
+# so its linear solves are exact to round-off; the plain FP64 path solves each Newton
+# iteration to a relative 1e-8 at least (the library tightens the test against tol_nonlin
+# as the residual falls), which keeps every reference fixture within 1e-10 per step with the
+# same Newton iterations (measured: the bench generator's basin at 1e-8 is 6.7e-11 from the
+# reference, at 1e-10 3.5e-11, at 1e-6 3.7e-10) at 17 % fewer Krylov iterations than 1e-10.
+# The mixed path's FP32 inner solves stop at 1e-6 (at most 100 iterations) and the FP64 Newton
+# loop refines.
+DEFAULT_TOL = {capi.SW2GPU_FP64: (1e-8, 1e-30), capi.SW2GPU_MIXED: (1e-6, 1e-30)}
 
 
 def solver_params(model, precision=capi.SW2GPU_FP64, precond=capi.SW2GPU_PREC_BJACOBI, lin_rtol=None,

@@ -121,9 +121,8 @@ const char *sw2gpu_last_error(void);
 int sw2gpu_create(const sw2gpu_mesh *mesh, const sw2gpu_params *params, void *stream, sw2gpu_ctx **out);
 int sw2gpu_destroy(sw2gpu_ctx *ctx);
 /* Launch variants (no counterpart in the reference).  Two knobs change the speed of a step,
- * never its results: the wet-Jacobian kernel (jac_minb: 1 or 2 = the register budget for 1 or 2
- * resident CTAs per SM, 3 = seven warps per SM with both perturbed evaluations of a column in
- * flight per thread) and the depth of the Krylov kernel's shared-memory tile ring (stages:
+ * never its results: the register budget of the wet-Jacobian kernel (jac_minb: 1 or 2
+ * resident CTAs per SM) and the depth of the Krylov kernel's shared-memory tile ring (stages:
  * 0 = sweeps read global memory, 2 or 3).  sw2gpu_autotune times every variant on the
  * context's own mesh and current state (which it leaves as it found it) and keeps the
  * fastest; a batch uses the variants of its instance with the most blocks. */

@@ -1,7 +1,6 @@
-"""Launch variants and the autotuner: the wet-Jacobian kernel variant (register budget, or two
-evaluations in flight per thread) and the depth of the Krylov tile ring change speed only --
-every variant steps to the same bits, and autotuning (which runs the step's kernels on the
-current state) leaves the state untouched."""
+"""Launch variants and the autotuner: the register budget of the wet-Jacobian kernel and the
+depth of the Krylov tile ring change speed only -- every variant steps to the same bits, and
+autotuning (which runs the step's kernels on the current state) leaves the state untouched."""
 import itertools
 
 import numpy as np
@@ -24,7 +23,7 @@ def _states(g):
 def test_variants_give_identical_steps(precision):
     m = _model()
     ref = None
-    for jac, stages in itertools.product((1, 2, 3), (0, 2, 3)):
+    for jac, stages in itertools.product((1, 2), (0, 2, 3)):
         g = SW2GPU(m, precision=precision)
         g.set_variant(jac, stages)
         assert g.variant() == (jac, stages)
@@ -54,7 +53,7 @@ def test_autotune_keeps_state_and_results(warm_steps):
         run(g, warm_steps)
     before = _states(g)
     jac, stages = g.autotune()
-    assert jac in (1, 2, 3) and stages in (0, 2, 3) and g.variant() == (jac, stages)
+    assert jac in (1, 2) and stages in (0, 2, 3) and g.variant() == (jac, stages)
     for a, b in zip(_states(g), before):
         assert np.array_equal(a, b)
     run(g, 3)
