@@ -72,8 +72,12 @@ struct KrylovCtl {
 // Grid barrier with a bounded spin.  Arrivals only ever add to one counter, so the b-th
 // barrier of a launch is passed once the counter reaches b * nblocks (`epoch`, per CTA): the
 // last arrival releases everyone without a second atomic.  Returns false (and sets ctl->err)
-// if any block gave up; the caller then returns, so the kernel always terminates.
+// if any block gave up; the caller then returns, so the kernel always terminates.  The error
+// word is read once, by thread 0, and the decision reaches the whole CTA through shared
+// memory: another CTA may set the word at any moment, and threads reading it one by one could
+// disagree, some returning while the rest of the CTA waits for them at its next barrier.
 __device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks, unsigned& epoch, long long limit) {
+    __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         epoch += nblocks;
@@ -93,9 +97,10 @@ __device__ __forceinline__ bool grid_sync(KrylovCtl* ctl, unsigned nblocks, unsi
         }
         // no trailing fence: the acquire load orders this thread's later accesses, and the
         // __syncthreads below orders the rest of the CTA's after it
+        s_ok = *(volatile int*)&ctl->err == 0;
     }
     __syncthreads();
-    return *(volatile int*)&ctl->err == 0;
+    return s_ok != 0;
 }
 
 constexpr int kKrylovWarps = kKrylovRowThreads / 32;   // warps that hold partials
