@@ -179,11 +179,21 @@ static void gpu_prepare(SSUPER_MODEL *sm, SMODEL *mod) {
     p.max_lin_it = sm->solver_info.max_lin_it > kMinLinIt ? sm->solver_info.max_lin_it : kMinLinIt;
     p.max_linesearch_cuts = sm->solver_info.max_nonlin_linesearch_cuts;
     p.precision = SW2GPU_FP64;
-    p.precond = SW2GPU_PREC_BJACOBI;
     /* the device Krylov solve's own floor (the library's default): each Newton iteration is
      * solved to a relative 1e-8 at least, tightened against tol_nonlin as the residual falls */
     p.lin_rtol = 1e-8; p.lin_atol = 1e-30;
-    const int rc = sw2gpu_create(&me, &p, NULL, &gpu.ctx);
+    /* OP BLK 1 with OP PRE 1 (the reference's default) preconditions with an exact LU of the
+     * whole system, so its BiCGSTAB converges at any time-step length: the device takes the same
+     * exact solve (a banded LU) whenever the band fits, else block-Jacobi BiCGSTAB */
+    int rc = SW2GPU_E_ARG;
+    if (mod->nblock == 1 && mod->solver_info.prec_value == 1) {
+        p.precond = SW2GPU_PREC_BAND;
+        rc = sw2gpu_create(&me, &p, NULL, &gpu.ctx);
+    }
+    if (rc != SW2GPU_OK) {
+        p.precond = SW2GPU_PREC_BJACOBI;
+        rc = sw2gpu_create(&me, &p, NULL, &gpu.ctx);
+    }
     free(x); free(y); free(z); free(nstr); free(tri); free(emat); free(edg); free(estr); free(epar);
     free(bc); free(isg); free(ivx); free(ivy); free(iu0); free(mode); free(ks); free(ev);
     free(coef); free(cor);

@@ -759,8 +759,11 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
         const double xf = g * bedx * dt * factor, yf = g * bedy * dt * factor;
         const double xc = -v_wd * cs, yc = u_wd * cs;
         const double c_eq = dhdt + adv[0] + factor * water_source * djac * dt;
-        const double x_eq = dudt + adv[1] + (xp + xf / hden) * djac + xc * djac * factor * dt;
-        const double y_eq = dvdt + adv[2] + (yp + yf / hden) * djac + yc * djac * factor * dt;
+        // the surface stress of a fully wet element enters the strong momentum equations
+        // (:1049-1050); subtracting 0 / hden leaves the no-wind terms bit for bit
+        const double tsx = wd_flag == 0 ? in.wsx : 0.0, tsy = wd_flag == 0 ? in.wsy : 0.0;
+        const double x_eq = dudt + adv[1] + (xp + xf / hden) * djac + (xc - tsx / hden) * djac * factor * dt;
+        const double y_eq = dvdt + adv[2] + (yp + yf / hden) * djac + (yc - tsy / hden) * djac * factor * dt;
         const double tu = tau * u_wd, tv = tau * v_wd, th = tau * h_wd;
 #pragma unroll
         for (int i = 0; i < 3; i++) {

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/sw2gpu.h"
+#include "sw2_band.cuh"
 #include "sw2_kernels.cuh"
 #include "sw2_krylov.cuh"
 #include "sw2_series.h"
@@ -109,6 +110,12 @@ struct sw2gpu_ctx {
     double step_mass = 0.0, step_flux = 0.0;
     DBuf<double> dacont;        // [3][T] transport side output, allocated when first enabled
     DBuf<double> errind;        // adaption error indicator: raw [T], scaled [T], nodal [V], tolerances [M]
+    // exact banded LU solve (SW2GPU_PREC_BAND): reverse Cuthill-McKee position of every node, the
+    // band of the scaled system [3V][2 bw + 1] and its right-hand side / solution [3V]
+    bool band = false;
+    int band_bw = 0;
+    DBuf<int> band_perm;
+    DBuf<double> band_mem, band_y;
     DBuf<double> wind;          // wind: element stress x [T], y [T], nodal values x [V], y [V], factors [M]
     DBuf<int> wind_flag;        // [M] wind stress flag per material
     bool wind_on = false;
@@ -220,6 +227,44 @@ void stage_caps(const std::vector<int>& rp, int V, size_t esz, unsigned& a_cap, 
     a_cap = (unsigned)am;
     c_cap = (unsigned)cm;
 }
+
+// Reverse Cuthill-McKee order of the nodes for the banded LU: breadth-first from a node of least
+// degree in every connected part, each node's unvisited neighbours taken by increasing degree, the
+// whole sequence reversed.  perm[i] = new position of node i; returns the half-bandwidth in nodes.
+int rcm_order(const std::vector<int>& rp, const std::vector<int>& col, int V, std::vector<int>& perm) {
+    std::vector<int> deg(V), start(V), order;
+    order.reserve(V);
+    for (int i = 0; i < V; i++) {
+        deg[i] = rp[i + 1] - rp[i];
+        start[i] = i;
+    }
+    std::stable_sort(start.begin(), start.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+    std::vector<char> seen(V, 0);
+    size_t head = 0;
+    for (int s0 : start) {
+        if (seen[s0]) continue;
+        seen[s0] = 1;
+        order.push_back(s0);
+        while (head < order.size()) {
+            const int a = order[head++];
+            const size_t n0 = order.size();
+            for (int k = rp[a]; k < rp[a + 1]; k++)
+                if (!seen[col[k]]) {
+                    seen[col[k]] = 1;
+                    order.push_back(col[k]);
+                }
+            std::stable_sort(order.begin() + n0, order.end(), [&](int a2, int b2) { return deg[a2] < deg[b2]; });
+        }
+    }
+    perm.assign(V, 0);
+    for (int i = 0; i < V; i++) perm[order[V - 1 - i]] = i;
+    int bw = 0;
+    for (int i = 0; i < V; i++)
+        for (int k = rp[i]; k < rp[i + 1]; k++) bw = std::max(bw, std::abs(perm[i] - perm[col[k]]));
+    return bw;
+}
+// largest band the direct solve accepts (bytes of the band of the scaled system)
+constexpr size_t kBandMaxBytes = size_t(2) << 30;
 
 // Krylov kernel with a tile ring of `stages` stages (0: sweeps read global memory)
 template <typename MT, class KS>
@@ -707,10 +752,41 @@ std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub) {
 
 // scaling, preconditioner folding and the persistent BiCGSTAB of the subset, each instance
 // with its own relative tolerance eta[k]
-int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<double>& eta) {
+// The exact banded LU solve of instance k (SW2GPU_PREC_BAND), after k_rowscale: the scaled system
+// into the band, its factors, the two triangular solves and the increment, on the runner's stream.
+int launch_band(Runner& R, int k) {
+    sw2gpu_ctx* c = R.ctx[k];
+    BandArgs B;
+    B.V = c->V;
+    B.n = 3 * c->V;
+    B.bw = c->band_bw;
+    B.width = 2 * c->band_bw + 1;
+    B.perm = c->band_perm.p;
+    B.rowptr = c->rowptr.p;
+    B.col = c->col.p;
+    B.val = c->val.p;
+    B.S = c->S_.p;
+    B.bs = c->bs.p;
+    B.band = c->band_mem.p;
+    B.y = c->band_y.p;
+    CK(cudaMemsetAsync(B.band, 0, sizeof(double) * (size_t)B.n * B.width, R.stream));
+    k_band_fill<<<nblk(c->nnzb, 256), 256, 0, R.stream>>>(B, c->blk_row.p, c->nnzb);
+    k_band_rhs<<<nblk(c->V, 256), 256, 0, R.stream>>>(B);
+    k_band_factor<<<1, kBandThreads, 0, R.stream>>>(B);
+    k_band_solve<<<1, kBandThreads, 0, R.stream>>>(B);
+    k_band_apply<<<nblk(c->V, 256), 256, 0, R.stream>>>(B, c->H(0), c->U(0), c->Vv(0), c->sol.p,
+                                                          R.ktab_h[k].K.apply_inc, R.ctl.p + k);
+    CK(cudaGetLastError());
+    R.launches += 5;
+    return 0;
+}
+
+int launch_linear(Runner& R, const std::vector<int>& all, const std::vector<double>& eta) {
     auto C = [&](int k) { return R.ctx[k]; };
+    std::vector<int> sub, band;   // Krylov instances, direct banded solves
+    for (int k : all) (C(k)->band ? band : sub).push_back(k);
     CK(cudaMemsetAsync(R.singular.p, 0, sizeof(int) * R.ctx.size(), R.stream));
-    int rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->V, 256); }, SW2_GO(k_rowscale<std::decay_t<decltype(src)>>, 0));
+    int rc = launch_map(R, all, 256, [&](int k) { return nblk(C(k)->V, 256); }, SW2_GO(k_rowscale<std::decay_t<decltype(src)>>, 0));
     if (rc) return rc;
     if (R.mixed)
         rc = launch_map(R, sub, 256, [&](int k) { return nblk(C(k)->nnzb, 256); }, SW2_GO_T(k_fold_offdiag, float));
@@ -719,6 +795,8 @@ int launch_linear(Runner& R, const std::vector<int>& sub, const std::vector<doub
     if (rc) return rc;
     CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * R.ctx.size(), R.stream));
     Phase ph(&R, kPhKrylov);
+    for (int k : band)
+        if ((rc = launch_band(R, k))) return rc;
     // instances that cannot all be co-resident go in successive launches
     size_t j0 = 0;
     while (j0 < sub.size()) {
@@ -1155,8 +1233,10 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     *out = nullptr;
     if (m->nnodes <= 0 || m->nelems2d < 0 || m->nelems1d < 0) return fail(SW2GPU_E_ARG, "bad mesh sizes");
     if (prm->precision != SW2GPU_FP64 && prm->precision != SW2GPU_MIXED) return fail(SW2GPU_E_ARG, "bad precision");
-    if (prm->precond != SW2GPU_PREC_BJACOBI)
-        return fail(SW2GPU_E_ARG, "preconditioner %d not built (SW2GPU_PREC_BJACOBI only)", prm->precond);
+    if (prm->precond != SW2GPU_PREC_BJACOBI && prm->precond != SW2GPU_PREC_BAND)
+        return fail(SW2GPU_E_ARG, "preconditioner %d not built (SW2GPU_PREC_BJACOBI or SW2GPU_PREC_BAND)", prm->precond);
+    if (prm->precond == SW2GPU_PREC_BAND && prm->precision != SW2GPU_FP64)
+        return fail(SW2GPU_E_ARG, "the banded LU solve is FP64 only");
     int dev = 0;
     CK(cudaGetDevice(&dev));
     auto* c = new sw2gpu_ctx();
@@ -1394,6 +1474,19 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
         }
         rc |= up(c->orowptr, orp, st);
         rc |= up(c->ocol, ocol, st);
+    }
+    if (prm->precond == SW2GPU_PREC_BAND) {
+        std::vector<int> perm;
+        const int bwn = rcm_order(rp, col, V, perm);
+        c->band = true;
+        c->band_bw = 3 * bwn + 2;
+        const size_t nb = (size_t)3 * V * (2 * (size_t)c->band_bw + 1) * sizeof(double);
+        if (nb > kBandMaxBytes)
+            return fail(SW2GPU_E_ARG, "the band of this system (%zu MB, half-width %d) exceeds the direct solve's %zu MB",
+                        nb >> 20, c->band_bw, kBandMaxBytes >> 20);
+        rc |= up(c->band_perm, perm, st);
+        rc |= zalloc(c->band_mem, 3ull * V * (2ull * c->band_bw + 1), st);
+        rc |= zalloc(c->band_y, 3ull * V, st);
     }
     for (auto& b : c->kv64) rc |= zalloc(b, 3ull * V, st);
     rc |= zalloc(c->ncounter, 1, st);

@@ -57,9 +57,17 @@ extern "C" {
 #define SW2GPU_FP64          0   /* everything FP64 */
 #define SW2GPU_MIXED         1   /* FP32 Jacobian storage, SpMV and preconditioner; FP64 Newton */
 
-/* preconditioners of the device Krylov solve */
-#define SW2GPU_PREC_BJACOBI  0   /* 3x3 block Jacobi */
+/* linear solve of every Newton iteration */
+#define SW2GPU_PREC_BJACOBI  0   /* BiCGSTAB preconditioned with 3x3 block Jacobi */
 #define SW2GPU_PREC_ILU0     1   /* block ILU(0): not built; sw2gpu_create rejects it with SW2GPU_E_ARG */
+#define SW2GPU_PREC_BAND     2   /* exact LU of the Jacobi-scaled system in a band (nodes in reverse
+                                  * Cuthill-McKee order, no pivoting), the direct solve the reference's
+                                  * OP BLK 1 profile LU gives (solv_blk_set_profile,
+                                  * src/solver/solv_blk_profile.c:5-79).  FP64 only; sw2gpu_create
+                                  * rejects it with SW2GPU_E_ARG when the band would exceed 2 GiB.
+                                  * Work n bw^2 per factorisation (n = 3 nnodes, bw the half-width in
+                                  * unknowns): for the small and medium meshes of test decks, whose
+                                  * time steps are too long for block Jacobi to converge */
 
 /* Mesh and model data (what fe_sw2_* read from SGRID / SMODEL).  Host pointers;
  * the library copies what it needs at create time. */

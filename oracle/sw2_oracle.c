@@ -573,8 +573,11 @@ static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof
         double xf = gr * bed.x * dt * factor, yf = gr * bed.y * dt * factor;
         double xc = -vwd.y * cspeed, yc = vwd.x * cspeed;
         double c_eq = dhdt + adv[0].c + factor * water_source * djac * dt;
-        double x_eq = dudt + adv[0].x + (xp + xf / hden) * djac + (xc - 0.0 / hden) * djac * factor * dt;
-        double y_eq = dvdt + adv[0].y + (yp + yf / hden) * djac + (yc - 0.0 / hden) * djac * factor * dt;
+        /* the surface stress enters the strong momentum equations too (:1049-1050); it is zero
+         * off fully wet elements (:674-675) */
+        double tsx = (wd == 0 && C->wsx) ? C->wsx[ie] : 0.0, tsy = (wd == 0 && C->wsy) ? C->wsy[ie] : 0.0;
+        double x_eq = dudt + adv[0].x + (xp + xf / hden) * djac + (xc - tsx / hden) * djac * factor * dt;
+        double y_eq = dvdt + adv[0].y + (yp + yf / hden) * djac + (yc - tsy / hden) * djac * factor * dt;
         for (i = 0; i < 3; i++) {
             double rc = g[i].x * (tau * vwd.x * c_eq + tau * h_wd * x_eq) + g[i].y * (tau * vwd.y * c_eq + tau * h_wd * y_eq);
             double rx = g[i].x * (tau * gf * h_wd * c_eq + tau * vwd.x * h_wd * x_eq) + g[i].y * (tau * vwd.y * h_wd * x_eq);

@@ -68,6 +68,33 @@ def test_linear_solve_matches_direct_solve(channel_ref):
     assert relerr(x, spla.spsolve(A, b)) <= 1e-7
 
 
+def test_band_linear_solve_is_the_exact_solve(channel_ref):
+    """SW2GPU_PREC_BAND factors the scaled system exactly: its solution is the direct solve's to
+    round-off (the reference's OP BLK 1 profile LU gives the same), one reported iteration."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    model = channel_model()
+    g = SW2GPU(model, precond=capi.SW2GPU_PREC_BAND)
+    V = model.nnodes
+    A = sp.bsr_matrix((channel_ref["load0_val"], channel_ref["load0_col"], channel_ref["load0_rowptr"]),
+                      shape=(3 * V, 3 * V)).tocsc()
+    b = channel_ref["load0_resid"]
+    x, its, rc = g.linear_solve(channel_ref["load0_val"], b)
+    assert rc == 0 and its == 1
+    assert relerr(x, spla.spsolve(A, b)) <= 1e-10
+
+
+def test_band_solve_rejects_mixed_precision():
+    with pytest.raises(SW2Error):
+        SW2GPU(channel_model(), precision=capi.SW2GPU_MIXED, precond=capi.SW2GPU_PREC_BAND)
+
+
+def test_band_runs_match_reference(channel_ref, basin_ref):
+    """Whole time steps with the exact banded solve follow the reference like the Krylov path."""
+    _run_against(channel_model(), channel_ref, 20, (1, 5, 10, 20), precond=capi.SW2GPU_PREC_BAND)
+    _run_against(basin_model(), basin_ref, 8, range(1, 9), wd=True, precond=capi.SW2GPU_PREC_BAND)
+
+
 def _run_against(model, ref, nsteps, check_every, precision=capi.SW2GPU_FP64, tol=1e-10, wd=False, **kw):
     g = SW2GPU(model, precision=precision, **kw)
     worst = 0.0
