@@ -45,6 +45,7 @@ typedef struct {
     int32_t *wind_flag;     /* [nstring] MP WND STR of that material (wind runs only) */
     double *wind_att;       /* [nstring] MP WND ATT of that material */
     double *wsx, *wsy;      /* [nnodes] nodal wind values of the coming step */
+    double *rxx, *rxy, *ryy;  /* [nnodes] nodal wave radiation stresses (wave runs only) */
     int state_on_device;    /* the host's current and old levels are the device's (last step accepted) */
 } GPU_SW2;
 
@@ -85,6 +86,7 @@ static void gpu_release(void) {
     if (gpu.ctx) sw2gpu_destroy(gpu.ctx);
     free(gpu.h); free(gpu.u); free(gpu.v); free(gpu.series); free(gpu.mat_of);
     free(gpu.wind_flag); free(gpu.wind_att); free(gpu.wsx); free(gpu.wsy);
+    free(gpu.rxx); free(gpu.rxy); free(gpu.ryy);
     memset(&gpu, 0, sizeof gpu);
 }
 
@@ -96,11 +98,13 @@ static void gpu_prepare(SSUPER_MODEL *sm, SMODEL *mod) {
     const int V = g->nnodes, T = g->nelems2d, S = mod->nstring;
     int i, k, E = 0;
     gpu_release();
-    /* body terms the library does not compute (fe_sw2_body_resid.c:674-719 wave stresses and
-     * the wind library's forms, :869-970 baroclinic terms): refuse the model rather than solve
-     * without them */
-    if (mod->flag.WAVE == ON || mod->flag.WIND_LIBRARY == ON)
-        tl_error("B200 SW2 step: wave stresses and the wind library are not supported\n");
+    /* body terms the library does not compute (the wind library's forms and the CSTORM-coupled
+     * wave stress of fe_sw2_body_resid.c:679-690, :869-970 baroclinic terms): refuse the model
+     * rather than solve without them */
+    if (mod->flag.WIND_LIBRARY == ON)
+        tl_error("B200 SW2 step: the wind library is not supported\n");
+    if (mod->flag.WAVE == ON && mod->flag.CSTORM_WSID != OFF && mod->flag.CSTORM_WSID != 7)
+        tl_error("B200 SW2 step: CSTORM-coupled wave stresses are not supported\n");
     if (mod->flag.BAROCLINIC != OFF)
         tl_error("B200 SW2 step: baroclinic terms are not supported\n");
     for (i = 0; i < g->nelems1d; i++) {
@@ -215,6 +219,11 @@ static void gpu_prepare(SSUPER_MODEL *sm, SMODEL *mod) {
             gpu.wind_att[k] = gpu.mat_of[k] >= 0 ? mod->mat[gpu.mat_of[k]].sw->windatt : 1.0;
         }
     }
+    if (mod->flag.WAVE == ON) {
+        gpu.rxx = malloc(V * sizeof(double));
+        gpu.rxy = malloc(V * sizeof(double));
+        gpu.ryy = malloc(V * sizeof(double));
+    }
     gpu.series = malloc((gpu.nseries + 1) * sizeof(double));
 }
 
@@ -251,6 +260,12 @@ int fe_sw2_solve_gpu(SSUPER_MODEL *sm, int isubModel) {
         if (sw2gpu_set_wind(gpu.ctx, gpu.wind_flag, gpu.wind_att, gpu.wsx, gpu.wsy) != SW2GPU_OK)
             gpu_fail("sw2gpu_set_wind");
     }
+    if (gpu.rxx) {   /* the nodal radiation stresses (hot file or wave series, fe_sw2_body_resid.c:689-690) */
+        for (i = 0; i < gpu.nnodes; i++) {
+            gpu.rxx[i] = sw->waves[i].rads.xx; gpu.rxy[i] = sw->waves[i].rads.xy; gpu.ryy[i] = sw->waves[i].rads.yy;
+        }
+        if (sw2gpu_set_waves(gpu.ctx, gpu.rxx, gpu.rxy, gpu.ryy) != SW2GPU_OK) gpu_fail("sw2gpu_set_waves");
+    }
     sw2gpu_stats st;
     gpu.state_on_device = 0;
     const int rc = sw2gpu_step(gpu.ctx, sm->dt, gpu.series, &st);
@@ -262,6 +277,14 @@ int fe_sw2_solve_gpu(SSUPER_MODEL *sm, int isubModel) {
         if (sw2gpu_get_state(gpu.ctx, 0, gpu.h, gpu.u, gpu.v) != SW2GPU_OK) gpu_fail("sw2gpu_get_state");
         for (i = 0; i < gpu.nnodes; i++) { sw->head[i] = gpu.h[i]; sw->vel[i].x = gpu.u[i]; sw->vel[i].y = gpu.v[i]; }
         if (sw2gpu_get_wd_flag(gpu.ctx, g->wd_flag) != SW2GPU_OK) gpu_fail("sw2gpu_get_wd_flag");
+        if (gpu.rxx) {   /* the nodal wave stresses the host residual leaves behind for output: every
+                          * fully wet SW2 element, in element order, stores its stress at its nodes
+                          * (fe_sw2_resid.c:74-80, fe_sw2_body_resid.c:689-690, smeteor.c:333-337) */
+            int e;
+            for (e = 0; e < gpu.nelems2d; e++)
+                if (g->wd_flag[e] == 0 && mod->str_values[g->elem2d[e].string].phys_flag == SW2_FLAG)
+                    swave_elem2d_get_local_stress(2, mod->flag.CSTORM_WSID, sw->waves, g->elem2d[e], g->elem2d[e].nodes);
+        }
         if (mod->ntransport > 0) {   /* [3][nelems2d], read by the transport solve */
             double *dac = malloc(3 * (size_t) gpu.nelems2d * sizeof(double));
             int k;

@@ -914,6 +914,36 @@ __global__ void k_elem_wind(const __grid_constant__ DevMesh m, double g, double 
     wsy[e] = wy * fac[mt];
 }
 
+// Wave radiation stress of every element from the nodal radiation stresses Sxx, Sxy, Syy
+// (swave_elem2d_get_local_stress, src/structs/smeteor.c:312-327, the CSTORM_WSID OFF branch):
+// -sum_i (dphi_i/dx Sxx_i + dphi_i/dy Sxy_i) and -sum_i (dphi_i/dx Sxy_i + dphi_i/dy Syy_i), in
+// vertex order; one thread per element, out = [x T][y T].
+__global__ void k_elem_wave(const __grid_constant__ DevMesh m, const double* __restrict__ rxx,
+                            const double* __restrict__ rxy, const double* __restrict__ ryy, double* __restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.T) return;
+    const int n[3] = {m.en0[e], m.en1[e], m.en2[e]};
+    const double gx[3] = {m.gx0[e], m.gx1[e], m.gx2[e]}, gy[3] = {m.gy0[e], m.gy1[e], m.gy2[e]};
+    double sx = 0., sy = 0.;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        sx -= (gx[i] * rxx[n[i]] + gy[i] * rxy[n[i]]);
+        sy -= (gx[i] * rxy[n[i]] + gy[i] * ryy[n[i]]);
+    }
+    out[e] = sx;
+    out[m.T + e] = sy;
+}
+
+// The element surface stress the residual reads (total_stress, fe_sw2_body_resid.c:674-694):
+// wind + waves, either one 0 when it is off; arrays [x T][y T].
+__global__ void k_surface_stress(int T, const double* __restrict__ wind, const double* __restrict__ wave,
+                                 double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 2 * T) return;
+    const double w = wind ? wind[k] : 0.0, r = wave ? wave[k] : 0.0;
+    out[k] = w + r;
+}
+
 // ---------------------------------------------------------------------------------
 // Adaption error indicator (ssw_2d_calculate_elem_error, src/structs/ssw_2d.c:424-500), one
 // thread per element: the steady continuity residual at the vertices of the current level

@@ -119,6 +119,9 @@ struct sw2gpu_ctx {
     DBuf<double> wind;          // wind: element stress x [T], y [T], nodal values x [V], y [V], factors [M]
     DBuf<int> wind_flag;        // [M] wind stress flag per material
     bool wind_on = false;
+    DBuf<double> wave;          // waves: element stress x [T], y [T], nodal Sxx, Sxy, Syy [3][V]
+    bool wave_on = false;
+    DBuf<double> stress;        // element surface stress, wind + waves: x [T], y [T]
     bool dacont_on = false;
     bool has_ovh = false;       // some edge string is NB OVH (its velocity series go up every step)
     DBuf<int> slot_ptr, slot_idx, blk_ptr, blk_src, rowptr, col, blk_row, dpos;
@@ -1617,14 +1620,39 @@ int sw2gpu_mass_flux(sw2gpu_ctx* c, double density, double* flux) {
     return mass_reduce(c, true, c->H(0), density, flux);
 }
 
+// The element surface stress (wind + waves) the residual kernels read, after either part changed;
+// captured step graphs hold the mesh descriptor, so they are dropped when the stress turns on or off.
+int update_surface_stress(sw2gpu_ctx* c) {
+    const bool on = c->wind_on || c->wave_on, was = c->dm.wsx != nullptr;
+    const int T = c->T;
+    if (on) {
+        if (!c->stress.p) {
+            g_alloc_bytes = &c->bytes;
+            const int rc = zalloc(c->stress, 2 * (size_t)T, c->stream);
+            g_alloc_bytes = nullptr;
+            if (rc) return rc;
+        }
+        if (T) {
+            k_surface_stress<<<nblk(2 * T, 256), 256, 0, c->stream>>>(T, c->wind_on ? c->wind.p : nullptr,
+                                                                     c->wave_on ? c->wave.p : nullptr, c->stress.p);
+            CK(cudaGetLastError());
+        }
+        c->dm.wsx = c->stress.p;
+        c->dm.wsy = c->stress.p + T;
+    } else {
+        c->dm.wsx = c->dm.wsy = nullptr;
+    }
+    if (on != was) c->drop_graphs();
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
 int sw2gpu_set_wind(sw2gpu_ctx* c, const int32_t* mat_flag, const double* mat_windatt, const double* stress_x,
                     const double* stress_y) {
     if (!c) return fail(SW2GPU_E_ARG, "null context");
     if (!stress_x || !stress_y) {   // off
         c->wind_on = false;
-        c->dm.wsx = c->dm.wsy = nullptr;
-        c->drop_graphs();
-        return SW2GPU_OK;
+        return update_surface_stress(c);
     }
     if (!mat_flag || !mat_windatt) return fail(SW2GPU_E_ARG, "null material wind tables");
     const int T = c->T, V = c->V, M = std::max(c->M, 1);
@@ -1657,12 +1685,33 @@ int sw2gpu_set_wind(sw2gpu_ctx* c, const int32_t* mat_flag, const double* mat_wi
                                                          wsx, wsy);
         CK(cudaGetLastError());
     }
-    CK(cudaStreamSynchronize(c->stream));   // the host tables above are released on return
-    if (!c->wind_on) c->drop_graphs();      // the descriptors baked into captured steps change
     c->wind_on = true;
-    c->dm.wsx = wsx;
-    c->dm.wsy = wsy;
-    return SW2GPU_OK;
+    return update_surface_stress(c);   // synchronizes: the host tables above are released on return
+}
+
+int sw2gpu_set_waves(sw2gpu_ctx* c, const double* rads_xx, const double* rads_xy, const double* rads_yy) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    if (!rads_xx || !rads_xy || !rads_yy) {   // off
+        c->wave_on = false;
+        return update_surface_stress(c);
+    }
+    const int T = c->T, V = c->V;
+    if (!c->wave.p) {
+        g_alloc_bytes = &c->bytes;
+        const int rc = zalloc(c->wave, 2 * (size_t)T + 3 * (size_t)V, c->stream);
+        g_alloc_bytes = nullptr;
+        if (rc) return rc;
+    }
+    double* rads = c->wave.p + 2 * (size_t)T;
+    CK(cudaMemcpyAsync(rads, rads_xx, sizeof(double) * V, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(rads + V, rads_xy, sizeof(double) * V, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(rads + 2 * (size_t)V, rads_yy, sizeof(double) * V, cudaMemcpyHostToDevice, c->stream));
+    if (T) {
+        k_elem_wave<<<nblk(T, 256), 256, 0, c->stream>>>(c->dm, rads, rads + V, rads + 2 * (size_t)V, c->wave.p);
+        CK(cudaGetLastError());
+    }
+    c->wave_on = true;
+    return update_surface_stress(c);
 }
 
 int sw2gpu_elem_error(sw2gpu_ctx* c, const double* refine_tol, double* elem_error, double* node_error) {

@@ -35,7 +35,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
            "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont",
            "sw2gpu_set_wait_limits", "sw2gpu_snapshot", "sw2gpu_elem_error", "sw2gpu_set_mass_tracking",
-           "sw2gpu_step_mass", "sw2gpu_set_wind"]
+           "sw2gpu_step_mass", "sw2gpu_set_wind", "sw2gpu_set_waves"]
 
 
 class SW2Error(RuntimeError):
@@ -89,6 +89,7 @@ def lib():
         L.sw2gpu_elem_error.argtypes = [vp, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_set_mass_tracking.argtypes = [vp, C.c_int32, C.c_double]
         L.sw2gpu_set_wind.argtypes = [vp, c_int32_p, c_double_p, c_double_p, c_double_p]
+        L.sw2gpu_set_waves.argtypes = [vp, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_step_mass.argtypes = [vp, c_double_p, c_double_p]
         L.sw2gpu_set_variant.argtypes = [vp, C.c_int32, C.c_int32]
         L.sw2gpu_get_variant.argtypes = [vp, c_int32_p, c_int32_p]
@@ -272,6 +273,14 @@ class SW2GPU:
         sx = np.ascontiguousarray(stress_x, dtype=np.float64)
         sy = np.ascontiguousarray(stress_y, dtype=np.float64)
         _check(lib().sw2gpu_set_wind(self.h, _ip(f), _dp(a), _dp(sx), _dp(sy)))
+
+    def set_waves(self, rads_xx=None, rads_xy=None, rads_yy=None):
+        """Wave radiation stress from nodal radiation stresses Sxx, Sxy, Syy; None: off."""
+        if rads_xx is None:
+            _check(lib().sw2gpu_set_waves(self.h, None, None, None))
+            return
+        a, b, c = (np.ascontiguousarray(r, dtype=np.float64) for r in (rads_xx, rads_xy, rads_yy))
+        _check(lib().sw2gpu_set_waves(self.h, _dp(a), _dp(b), _dp(c)))
 
     def set_mass_tracking(self, enable: bool = True, density=None):
         """Reduce the grid mass and the mass flux inside every accepted step (step_mass())."""

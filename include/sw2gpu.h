@@ -178,10 +178,18 @@ int sw2gpu_set_wd_flag(sw2gpu_ctx *ctx, const int32_t *wd_flag);
  * material's wind stress form (MP WND STR: 0 = the values are the stress, 1 = Wu's drag law of a
  * wind speed; the depth-dependent form 2 is not built and is rejected with SW2GPU_E_ARG) and
  * mat_windatt[nmats] its attenuation (MP WND ATT).  The element stress, the vertex average
- * scaled by windatt^2 / (3 density), enters the momentum residual of fully wet elements.  Kept
- * until the next call; stress_x = NULL turns the term off (the default). */
+ * scaled by windatt^2 / (3 density), enters the momentum residual of fully wet elements and
+ * their SUPG strong momentum equations (:1049-1050).  Kept until the next call; stress_x = NULL
+ * turns the term off (the default). */
 int sw2gpu_set_wind(sw2gpu_ctx *ctx, const int32_t *mat_flag, const double *mat_windatt, const double *stress_x,
                     const double *stress_y);
+/* Wave radiation stress (the same term, fe_sw2_body_resid.c:689-694, with
+ * swave_elem2d_get_local_stress, src/structs/smeteor.c:312-327): rads_xx / rads_xy / rads_yy
+ * [nnodes] are the nodal radiation stresses waves[node].rads the reference reads from the hot
+ * file (WAVE_STRESS) or a wave station series.  The element stress is -sum_i grad(phi_i) . S_i and
+ * adds to the wind stress.  The CSTORM coupled form (nodal stresses averaged) is not built.  Kept
+ * until the next call; rads_xx = NULL turns the term off (the default). */
+int sw2gpu_set_waves(sw2gpu_ctx *ctx, const double *rads_xx, const double *rads_xy, const double *rads_yy);
 
 /* Mass-balance diagnostics (src/tools/tl_grid_mass.c), on the device.
  * sw2gpu_grid_mass: water mass of time level `level` times `density`

@@ -59,6 +59,8 @@ def lib():
         L.orc_elem_error.argtypes = [C.c_void_p, c_double_p, c_double_p, c_double_p]
         L.orc_set_wind.argtypes = [C.c_void_p, c_int32_p, c_double_p, c_double_p, c_double_p]
         L.orc_set_wind.restype = C.c_int
+        L.orc_set_waves.argtypes = [C.c_void_p, c_double_p, c_double_p, c_double_p]
+        L.orc_set_waves.restype = None
         L.orc_grid_mass.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.orc_grid_mass.restype = C.c_double
         L.orc_mass_flux.argtypes = [C.c_void_p, C.c_double, C.c_double, c_double_p]
@@ -183,6 +185,14 @@ class Oracle:
         sy = np.ascontiguousarray(stress_y, dtype=np.float64)
         if lib().orc_set_wind(self.h, f.ctypes.data_as(c_int32_p), _dp(a), _dp(sx), _dp(sy)):
             raise ValueError("wind stress flag not supported")
+
+    def set_waves(self, rads_xx=None, rads_xy=None, rads_yy=None):
+        """Wave radiation stress from nodal radiation stresses Sxx, Sxy, Syy (None: off)."""
+        if rads_xx is None:
+            lib().orc_set_waves(self.h, None, None, None)
+            return
+        a, b, c = (np.ascontiguousarray(r, dtype=np.float64) for r in (rads_xx, rads_xy, rads_yy))
+        lib().orc_set_waves(self.h, _dp(a), _dp(b), _dp(c))
 
     def elem_error(self, refine_tol):
         """Adaption error indicator (ssw_2d_calculate_elem_error) of the current and old levels

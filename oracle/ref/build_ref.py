@@ -151,7 +151,7 @@ def build(src: str = REFERENCE_SRC, jobs: int = os.cpu_count() or 4) -> str:
 
 REPO = os.path.normpath(os.path.join(HERE, "..", ".."))
 GPU_EXE = os.path.join(OUT, "adh_gpu")
-QA_CASES = ["wet_dry", "angle_nb", "angle_source", "angle_dam", "angle_coriolis"]
+QA_CASES = ["wet_dry", "angle_nb", "angle_source", "angle_dam", "angle_coriolis", "angle_wind", "angle_wave"]
 
 
 def build_gpu_harness(flags, objs, hobj, stub, lib) -> str:

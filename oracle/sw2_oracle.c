@@ -71,6 +71,7 @@ typedef struct orc_ctx {
     double dt;
     double *series;
     double *wsx, *wsy;         /* [T] element wind stress (orc_set_wind), or NULL: no wind */
+    double *wvx, *wvy;         /* [T] element wave radiation stress (orc_set_waves), or NULL: none */
     /* BCSR pattern (sorted columns, diagonal included) */
     int *rowptr, *col, nnzb;
     int *blk_of_pair;          /* [9*T] value block of (i, j) pair of each element */
@@ -383,6 +384,14 @@ static void temporal(const v2 *X, double djac, double dll, const double *h, cons
     }
 }
 
+/* total_stress of an element (fe_sw2_body_resid.c:674-694): wind plus wave stress, each 0 when
+ * it is off (both start as 0 and are summed in that order) */
+static double surface_stress(const orc_ctx *C, int ie, int y) {
+    const double w = C->wsx ? (y ? C->wsy[ie] : C->wsx[ie]) : 0.0;
+    const double r = C->wvx ? (y ? C->wvy[ie] : C->wvx[ie]) : 0.0;
+    return w + r;
+}
+
 static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof3 *er) {
     const sw2gpu_params *P = &C->p;
     const v2 *g = (const v2 *) (C->grad + 6 * ie);
@@ -522,10 +531,10 @@ static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof
     }
 
     /* wind surface stress, fully wet elements only :674-719 (no wave stress: 0) */
-    if (wd == 0 && C->wsx) {
+    if (wd == 0 && (C->wsx || C->wvx)) {
         double rx[3] = {0, 0, 0}, ry[3] = {0, 0, 0};
-        tri_phi(djac, C->wsx[ie] + 0.0, rx);
-        tri_phi(djac, C->wsy[ie] + 0.0, ry);
+        tri_phi(djac, surface_stress(C, ie, 0), rx);
+        tri_phi(djac, surface_stress(C, ie, 1), ry);
         for (i = 0; i < 3; i++) { er[i].x -= dt * rx[i]; er[i].y -= dt * ry[i]; }
     }
 
@@ -575,7 +584,7 @@ static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof
         double c_eq = dhdt + adv[0].c + factor * water_source * djac * dt;
         /* the surface stress enters the strong momentum equations too (:1049-1050); it is zero
          * off fully wet elements (:674-675) */
-        double tsx = (wd == 0 && C->wsx) ? C->wsx[ie] : 0.0, tsy = (wd == 0 && C->wsy) ? C->wsy[ie] : 0.0;
+        double tsx = wd == 0 ? surface_stress(C, ie, 0) : 0.0, tsy = wd == 0 ? surface_stress(C, ie, 1) : 0.0;
         double x_eq = dudt + adv[0].x + (xp + xf / hden) * djac + (xc - tsx / hden) * djac * factor * dt;
         double y_eq = dvdt + adv[0].y + (yp + yf / hden) * djac + (yc - tsy / hden) * djac * factor * dt;
         for (i = 0; i < 3; i++) {
@@ -857,6 +866,7 @@ void orc_destroy(orc_ctx *C) {
     free(C->edges); free(C->edge_string); free(C->edge_parent); free(C->str_bc); free(C->str_isigma);
     free(C->str_ivx); free(C->str_ivy); free(C->str_iu0); free(C->str_rough); free(C->mat_eev_mode);
     free(C->mat_ev); free(C->mat_eev_coef); free(C->mat_cor); free(C->series); free(C->wsx); free(C->wsy);
+    free(C->wvx); free(C->wvy);
     for (k = 0; k < 3; k++) { free(C->h[k]); free(C->u[k]); free(C->v[k]); }
     free(C->wd); free(C->dacont); free(C->resid); free(C->sol); free(C->include); free(C->djac); free(C->grad);
     free(C->edjac); free(C->enrml); free(C->rowptr); free(C->col); free(C->blk_of_pair); free(C->eblk_of_pair);
@@ -1596,4 +1606,28 @@ int orc_set_wind(orc_ctx *C, const int *mat_flag, const double *mat_windatt, con
         C->wsy[e] = wy * f;
     }
     return 0;
+}
+
+/* Wave radiation stress from nodal radiation stresses (swave_elem2d_get_local_stress,
+ * src/structs/smeteor.c:312-327, the CSTORM_WSID OFF branch): per element
+ * -sum_i (dphi_i/dx Sxx_i + dphi_i/dy Sxy_i), -sum_i (dphi_i/dx Sxy_i + dphi_i/dy Syy_i), in vertex
+ * order.  NULL arrays: off. */
+void orc_set_waves(orc_ctx *C, const double *rxx, const double *rxy, const double *ryy) {
+    int e, i;
+    free(C->wvx); free(C->wvy);
+    C->wvx = C->wvy = NULL;
+    if (!rxx || !rxy || !ryy) return;
+    C->wvx = (double *) calloc((size_t) (C->T ? C->T : 1), sizeof(double));
+    C->wvy = (double *) calloc((size_t) (C->T ? C->T : 1), sizeof(double));
+    for (e = 0; e < C->T; e++) {
+        double sx = 0., sy = 0.;
+        for (i = 0; i < 3; i++) {
+            const int n = C->tri[3 * e + i];
+            const double gx = C->grad[6 * e + 2 * i], gy = C->grad[6 * e + 2 * i + 1];
+            sx -= (gx * rxx[n] + gy * rxy[n]);
+            sy -= (gx * rxy[n] + gy * ryy[n]);
+        }
+        C->wvx[e] = sx;
+        C->wvy[e] = sy;
+    }
 }

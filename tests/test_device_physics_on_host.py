@@ -200,7 +200,22 @@ def _element_wind(m, flags, att, sx, sy, density):
     return out
 
 
-@pytest.mark.parametrize("case", ["all_terms", "terms_fixture", "rain", "obstacle", "combined", "wind"])
+def _element_wave(o, m, rxx, rxy, ryy):
+    """Element wave radiation stress as swave_elem2d_get_local_stress forms it (CSTORM_WSID off):
+    -sum_i (dphi_i/dx Sxx_i + dphi_i/dy Sxy_i), -sum_i (dphi_i/dx Sxy_i + dphi_i/dy Syy_i)."""
+    out = np.zeros((m.nelems2d, 2))
+    for e, nodes in enumerate(m.tri):
+        _, g6 = o.geometry(e)
+        sx = sy = 0.0
+        for i, n in enumerate(nodes):
+            gx, gy = g6[2 * i], g6[2 * i + 1]
+            sx -= (gx * rxx[n] + gy * rxy[n])
+            sy -= (gx * rxy[n] + gy * ryy[n])
+        out[e] = (sx, sy)
+    return out
+
+
+@pytest.mark.parametrize("case", ["all_terms", "terms_fixture", "rain", "obstacle", "combined", "wind", "wave"])
 def test_device_physics_matches_oracle_on_host(host_physics, case):
     wind = None
     if case == "combined":
@@ -211,7 +226,7 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
         m = meshgen.basin_rain(nsteps=4)
     elif case == "obstacle":
         m = meshgen.channel_obstacle(nsteps=4, with_depth=True)
-    elif case == "wind":   # wind surface stress on fully wet elements, both stress forms
+    elif case in ("wind", "wave"):   # surface stress on fully wet elements: both wind forms; wind + waves
         m = meshgen.bumpy_basin(900, seed=5, size=2500.0, nsteps=4, dt=5.0, nbins=3, name="wind")
     else:
         base = meshgen.bumpy_basin(900, seed=5, size=2500.0, nsteps=4, dt=5.0, nbins=3, name="physics")
@@ -227,6 +242,16 @@ def test_device_physics_matches_oracle_on_host(host_physics, case):
         sy = wrng.normal(0.0, 0.3, m.nnodes)
         o.set_wind(flags, att, sx, sy)
         wind = _element_wind(m, flags, att, sx, sy, m.params.density)
+    if case == "wave":
+        wrng = np.random.Generator(np.random.PCG64(19))
+        flags = np.array([0, 0, 1], np.int32)
+        att = np.array([1.0, 0.9, 0.7])
+        sx = wrng.normal(0.0, 0.3, m.nnodes)
+        sy = wrng.normal(0.0, 0.3, m.nnodes)
+        rads = [wrng.normal(0.0, 0.05, m.nnodes) for _ in range(3)]
+        o.set_wind(flags, att, sx, sy)
+        o.set_waves(*rads)
+        wind = _element_wind(m, flags, att, sx, sy, m.params.density) + _element_wave(o, m, *rads)
     for _ in range(2):   # distinct time levels and moving wet/dry fronts
         assert o.step()["status"] == 0
     series = m.series_values(o.t, o.t + m.dt)

@@ -9,10 +9,10 @@ reference executable ``oracle/_ref/adh_dump``, both recording the state after ev
 step.  The GPU run must follow the reference step for step -- the same number of accepted
 steps and dt retries, Newton iterations within +-1, the state within the deck's tolerance
 below -- and its own error report (error.out, written by the reference's TEST module against
-the analytic solution) must read like the stored error.out.last.
+the analytic solution) must read like the reference run's and like the stored error.out.last.
 
-Tolerances.  The state is compared per step as everywhere in these tests (depth against
-max |h|, unit discharge as a vector field).  The plain FP64 GPU path matches the reference to
+Tolerances.  The state is compared per step (depth against max |h|, unit discharge as a vector
+field against the largest discharge of the reference run).  The plain FP64 GPU path matches the reference to
 1e-10 per step where Newton converges tightly; the QA decks set their own Newton tolerance
 (IP NTL up to 1e-4), and two solves that both stop below a loose tolerance can differ by what
 that tolerance allows (the reference's last Newton increment comes from an exact block LU, the
@@ -37,8 +37,9 @@ REF = os.path.join(ROOT, "oracle", "_ref")
 GPU_EXE = os.path.join(REF, "adh_gpu")
 CPU_EXE = os.path.join(REF, "adh_dump")
 QA = os.path.join(REF, "qa")
-# the reference's SW2 QA decks on triangles (wet_dry runs with a wind series, MP WND STR 0)
-CASES = ["wet_dry", "angle_nb", "angle_source", "angle_dam", "angle_coriolis"]
+# the reference's SW2 QA decks on triangles (wet_dry and angle_wind run with a wind series,
+# MP WND STR 0; angle_wave with the radiation stresses of its hot file)
+CASES = ["wet_dry", "angle_nb", "angle_source", "angle_dam", "angle_coriolis", "angle_wind", "angle_wave"]
 NUM = re.compile(r"[-+]?\d+\.\d*(?:[eE][-+]?\d+)?|[-+]?\d+[eE][-+]?\d+")
 
 
@@ -81,14 +82,21 @@ def _run(exe, case, model=None):
 
 def _compare_trajectories(case, gpu_steps, ref_steps, tol):
     """Accepted steps one for one: the same model times, dt and attempts (dt retries), Newton
-    iterations within +-1 per attempt, the state within tol."""
+    iterations within +-1 per attempt, the state within tol.  Depth is measured against the
+    step's max |h|; unit discharge against the largest discharge of the reference run (a deck
+    that settles to rest, like angle_wave, ends with a vanishing discharge field whose own
+    maximum would turn round-off into a large relative number)."""
     assert len(gpu_steps) == len(ref_steps), (len(gpu_steps), len(ref_steps))
+    qpeak = max(float(np.hypot(r["h"] * r["u"], r["h"] * r["v"]).max()) for r in ref_steps)
     worst = {"h": 0.0, "q": 0.0}
     for k, (g, r) in enumerate(zip(gpu_steps, ref_steps)):
         assert g["t"] == r["t"] and g["dt"] == r["dt"], (k, g["t"], r["t"], g["dt"], r["dt"])
         assert g["attempts"] == r["attempts"], k
         assert abs(g["newton_its"] - r["newton_its"]) <= max(1, r["attempts"]), (k, g["newton_its"], r["newton_its"])
-        for f, e in field_errors(fields(g["h"], g["u"], g["v"]), fields(r["h"], r["u"], r["v"])).items():
+        fg, fr = fields(g["h"], g["u"], g["v"]), fields(r["h"], r["u"], r["v"])
+        errs = {"h": field_errors(fg, fr)["h"],
+                "q": float(np.hypot(fg["uh"] - fr["uh"], fg["vh"] - fr["vh"]).max()) / max(qpeak, 1e-300)}
+        for f, e in errs.items():
             worst[f] = max(worst[f], e)
             assert e <= tol, (case, k, f, e, tol)
     return worst
@@ -122,8 +130,22 @@ def test_reference_time_loop_with_the_gpu_step_matches_the_reference(case):
     tol = 1e-10 if ntl <= 1e-8 else 100.0 * ntl
     worst = _compare_trajectories(case, gpu_steps, ref_steps, tol)
     print(f"{case}: {len(gpu_steps)} steps, worst per-step error h {worst['h']:.2e} q {worst['q']:.2e} (bound {tol:g})")
-    assert len(gpu_report) == len(stored)
-    for g, e in zip(gpu_report, stored):
+    _compare_reports(gpu_report, ref_report)
+    # the stored report too, wherever the reference built here reproduces it (all but angle_wind,
+    # whose stored transect error the reference's own run misses: 7.2e-6 FAIL against 3.5e-8 PASS)
+    if _reports_agree(ref_report, stored):
+        _compare_reports(gpu_report, stored)
+
+
+def _reports_agree(a, b):
+    return len(a) == len(b) and all(_split(x)[0] == _split(y)[0] and np.allclose(_split(x)[1], _split(y)[1],
+                                                                                rtol=1e-4, atol=1e-6)
+                                    for x, y in zip(a, b))
+
+
+def _compare_reports(got, exp):
+    assert len(got) == len(exp)
+    for g, e in zip(got, exp):
         gw, gn = _split(g)
         ew, en = _split(e)
         assert gw == ew, (g, e)

@@ -300,6 +300,37 @@ def test_mass_reduced_inside_the_step_equals_the_on_demand_diagnostics():
     g.close()
 
 
+def test_wind_and_wave_stress_residual_and_steps_match_oracle():
+    """Wave radiation stress (nodal Sxx, Sxy, Syy) on top of the wind stress on the wet/dry basin:
+    the device's element stresses, residual and three steps against the oracle; turning the
+    waves off again gives the wind-only residual back bit for bit."""
+    m = basin_model()
+    rng = np.random.Generator(np.random.PCG64(31))
+    nm = len(m.materials)
+    flags = np.zeros(nm, np.int32)
+    att = np.ones(nm)
+    sx, sy = rng.normal(0.0, 0.2, m.nnodes), rng.normal(0.0, 0.2, m.nnodes)
+    rads = [rng.normal(0.0, 0.05, m.nnodes) for _ in range(3)]
+    g, o = SW2GPU(m), Oracle(m)
+    for s in (g, o):
+        s.set_wind(flags, att, sx, sy)
+        s.set_dt(m.dt, m.series_values(0.0, m.dt))
+    o.wdflag()
+    g.set_wd(o.get_wd())
+    wind_only = g.resid()
+    for s in (g, o):
+        s.set_waves(*rads)
+    assert relerr(g.resid(), o.resid()) <= 1e-12
+    g.set_waves(None)
+    assert np.array_equal(g.resid(), wind_only)
+    g.set_waves(*rads)
+    for _ in range(3):
+        a, b = g.step(), o.step()
+        assert a["status"] == 0 and b["status"] == 0 and abs(a["newton_its"] - b["newton_its"]) <= 1
+        errs = field_errors(fields(*g.get_state(0)), fields(*o.get_state(0)))
+        assert max(errs.values()) <= 1e-10, errs
+
+
 def test_wind_stress_residual_and_steps_match_oracle():
     """Wind surface stress (both stress forms, per-material attenuation) on the wet/dry basin:
     the device residual and three steps against the oracle with the same nodal winds."""
