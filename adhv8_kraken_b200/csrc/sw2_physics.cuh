@@ -760,10 +760,12 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
         const double xc = -v_wd * cs, yc = u_wd * cs;
         const double c_eq = dhdt + adv[0] + factor * water_source * djac * dt;
         // the surface stress of a fully wet element enters the strong momentum equations
-        // (:1049-1050); subtracting 0 / hden leaves the no-wind terms bit for bit
+        // (:1049-1050).  Without one the reference subtracts 0 / hden, which changes no bits, so
+        // the division is skipped (it would cost an FP64 divide in every FD column evaluation).
         const double tsx = wd_flag == 0 ? in.wsx : 0.0, tsy = wd_flag == 0 ? in.wsy : 0.0;
-        const double x_eq = dudt + adv[1] + (xp + xf / hden) * djac + (xc - tsx / hden) * djac * factor * dt;
-        const double y_eq = dvdt + adv[2] + (yp + yf / hden) * djac + (yc - tsy / hden) * djac * factor * dt;
+        const double xs = tsx != 0.0 ? xc - tsx / hden : xc, ys = tsy != 0.0 ? yc - tsy / hden : yc;
+        const double x_eq = dudt + adv[1] + (xp + xf / hden) * djac + xs * djac * factor * dt;
+        const double y_eq = dvdt + adv[2] + (yp + yf / hden) * djac + ys * djac * factor * dt;
         const double tu = tau * u_wd, tv = tau * v_wd, th = tau * h_wd;
 #pragma unroll
         for (int i = 0; i < 3; i++) {
