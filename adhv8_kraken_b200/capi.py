@@ -27,6 +27,7 @@ SW2GPU_MIXED = 1
 SW2GPU_PREC_BJACOBI = 0
 SW2GPU_PREC_ILU0 = 1
 SW2GPU_PREC_BAND = 2
+SW2GPU_PREC_DILU = 3
 SW2GPU_BCT_LID_DFT = 20         # lids on node strings: refused by sw2gpu_create (not built)
 SW2GPU_BCT_LID_ELV = 21
 SW2GPU_BCT_LID_DEP = 22

@@ -15,6 +15,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <queue>
 #include <thread>
 #include <cstdarg>
 #include <cstdio>
@@ -26,6 +27,7 @@
 
 #include "../../include/sw2gpu.h"
 #include "sw2_band.cuh"
+#include "sw2_dilu.cuh"
 #include "sw2_kernels.cuh"
 #include "sw2_krylov.cuh"
 #include "sw2_series.h"
@@ -116,6 +118,18 @@ struct sw2gpu_ctx {
     int band_bw = 0;
     DBuf<int> band_perm;
     DBuf<double> band_mem, band_y;
+    // block D-ILU solve (SW2GPU_PREC_DILU): the coloured row order (colours padded to 32-row
+    // tiles), the off-diagonal blocks in an ELL layout per colour, the operator and the solve's
+    // own vectors
+    bool dilu = false;
+    int dl_ncol = 0, dl_rows = 0, dl_nlo = 0, dl_nup = 0, dl_cta = 0;
+    int dl_cstart[kMaxColours + 1] = {}, dl_cend[kMaxColours + 1] = {};
+    int dl_lbase[kMaxColours + 1] = {}, dl_ubase[kMaxColours + 1] = {}, dl_lkn[kMaxColours + 1] = {},
+        dl_ukn[kMaxColours + 1] = {};
+    DBuf<int> dl_lcol, dl_ucol, dl_lsrc, dl_usrc, dl_tslot, dl_old;
+    DBuf<double> dl_blk64, dl_Dti, dl_Dd, dl_part;
+    DBuf<float> dl_blk32;
+    DBuf<double> dl_vec[kDiluVectors];
     DBuf<double> wind;          // wind: element stress x [T], y [T], nodal values x [V], y [V], factors [M]
     DBuf<int> wind_flag;        // [M] wind stress flag per material
     bool wind_on = false;
@@ -294,6 +308,9 @@ struct Runner {
     DBuf<KrylovInst> ktab;
     std::vector<Inst> tab_h;       // descriptors (kernel parameters of every launch)
     KrylovInst* ktab_h = nullptr;  // pinned; uploaded to ktab for batch Krylov launches
+    DBuf<DiluArgs> dtab;           // D-ILU descriptors (setup kernels and batch solves)
+    DiluArgs* dtab_h = nullptr;    // pinned
+    bool any_dilu = false;
     cudaEvent_t tab_ev = nullptr;  // end of the last ktab upload
     bool tab_pending = false;
     DBuf<Norms> norms;
@@ -321,6 +338,7 @@ struct Runner {
             cudaEventDestroy(tab_ev);
         }
         if (ktab_h) cudaFreeHost(ktab_h);
+        if (dtab_h) cudaFreeHost(dtab_h);
         if (eta_h) cudaFreeHost(eta_h);
         for (auto e : pev) cudaEventDestroy(e);
         if (norms_h) cudaFreeHost(norms_h);
@@ -451,7 +469,7 @@ int runner_alloc(Runner& R, cudaStream_t stream, bool mixed, int cap) {
     R.stream = stream;
     R.mixed = mixed;
     R.cap = cap;
-    if (R.ktab.alloc(cap) || R.norms.alloc(cap) || R.ctl.alloc(cap) || R.singular.alloc(cap))
+    if (R.ktab.alloc(cap) || R.dtab.alloc(cap) || R.norms.alloc(cap) || R.ctl.alloc(cap) || R.singular.alloc(cap))
         return fail(SW2GPU_E_NOMEM, "batch tables");
     CK(cudaMemsetAsync(R.norms.p, 0, sizeof(Norms) * cap, stream));
     CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * cap, stream));
@@ -461,6 +479,7 @@ int runner_alloc(Runner& R, cudaStream_t stream, bool mixed, int cap) {
     CK(cudaMallocHost(&R.ctl_h, sizeof(KrylovCtl) * cap));
     R.tab_h.resize(cap);
     CK(cudaMallocHost(&R.ktab_h, sizeof(KrylovInst) * cap));
+    CK(cudaMallocHost(&R.dtab_h, sizeof(DiluArgs) * cap));
     CK(cudaEventCreateWithFlags(&R.tab_ev, cudaEventDisableTiming));
     CK(cudaEventCreate(&R.ev0));
     CK(cudaEventCreate(&R.ev1));
@@ -551,6 +570,53 @@ int runner_init(Runner& R, const std::vector<sw2gpu_ctx*>& ctx, cudaStream_t str
 }
 
 // device tables from the instances' current buffers and state levels
+// the D-ILU descriptor of instance k (its state pointers follow the rotating levels)
+void dilu_args(Runner& R, int k, int apply_inc) {
+    sw2gpu_ctx* c = R.ctx[k];
+    DiluArgs& D = R.dtab_h[k];
+    D.V = c->V;
+    D.N = c->dl_rows;
+    D.ncol = c->dl_ncol;
+    D.nlo = c->dl_nlo;
+    D.nup = c->dl_nup;
+    D.ncta = c->dl_cta;
+    for (int i = 0; i <= kMaxColours; i++) {
+        D.cstart[i] = c->dl_cstart[i];
+        D.cend[i] = c->dl_cend[i];
+        D.lbase[i] = c->dl_lbase[i];
+        D.ubase[i] = c->dl_ubase[i];
+        D.lkn[i] = c->dl_lkn[i];
+        D.ukn[i] = c->dl_ukn[i];
+    }
+    D.lcol = c->dl_lcol.p;
+    D.ucol = c->dl_ucol.p;
+    D.lsrc = c->dl_lsrc.p;
+    D.usrc = c->dl_usrc.p;
+    D.tslot = c->dl_tslot.p;
+    D.old = c->dl_old.p;
+    D.blk = R.mixed ? (void*)c->dl_blk32.p : (void*)c->dl_blk64.p;
+    D.Dti = c->dl_Dti.p;
+    D.Dd = c->dl_Dd.p;
+    D.blk_row = c->blk_row.p;
+    D.bcol = c->col.p;
+    D.dpos = c->dpos.p;
+    D.val = c->val.p;
+    D.S = c->S_.p;
+    D.bs = c->bs.p;
+    D.singular = R.singular.p + k;
+    D.atol = c->p.lin_atol;
+    D.maxit = c->p.max_lin_it;
+    D.h = c->H(0);
+    D.u = c->U(0);
+    D.v = c->Vv(0);
+    D.sol = c->sol.p;
+    D.apply_inc = apply_inc;
+    D.part = c->dl_part.p;
+    D.ctl = R.ctl.p + k;
+    D.spin_limit = c->wait_barrier;
+    for (int i = 0; i < kDiluVectors; i++) D.vec[i] = c->dl_vec[i].p;
+}
+
 int runner_tables(Runner& R, int apply_inc) {
     const int K = (int)R.ctx.size();
     if (R.tab_pending) {   // the pinned Krylov table is rewritten only after its last upload
@@ -594,10 +660,15 @@ int runner_tables(Runner& R, int apply_inc) {
         Q.A = I.aoff;
         Q.Dinv = c->dinv64.p;
         for (int v = 0; v < kKrylovVectors; v++) Q.vec[v] = c->kv64[v].p;
+        if (c->dilu) dilu_args(R, k, apply_inc);
     }
-    // the descriptors travel as kernel parameters; only batch Krylov launches read a table
-    if (K > 1) {
-        CK(cudaMemcpyAsync(R.ktab.p, R.ktab_h, sizeof(KrylovInst) * K, cudaMemcpyHostToDevice, R.stream));
+    R.any_dilu = false;
+    for (auto* c : R.ctx) R.any_dilu |= c->dilu;
+    // the descriptors travel as kernel parameters; batch Krylov launches and the D-ILU setup
+    // kernels read a table
+    if (K > 1) CK(cudaMemcpyAsync(R.ktab.p, R.ktab_h, sizeof(KrylovInst) * K, cudaMemcpyHostToDevice, R.stream));
+    if (R.any_dilu) CK(cudaMemcpyAsync(R.dtab.p, R.dtab_h, sizeof(DiluArgs) * K, cudaMemcpyHostToDevice, R.stream));
+    if (K > 1 || R.any_dilu) {
         CK(cudaEventRecord(R.tab_ev, R.stream));
         R.tab_pending = true;
     }
@@ -784,10 +855,90 @@ int launch_band(Runner& R, int k) {
     return 0;
 }
 
+// co-resident CTAs of the D-ILU solve kernel on this device (every instantiation)
+int dilu_capacity() {
+    static int cap = 0;
+    if (cap) return cap;
+    int dev = 0, sms = 0, fit = 1 << 30;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 0;
+    const void* ks[4] = {(const void*)k_dilu_bicgstab<double, DiluOne>, (const void*)k_dilu_bicgstab<double, DiluTab>,
+                         (const void*)k_dilu_bicgstab<float, DiluOne>, (const void*)k_dilu_bicgstab<float, DiluTab>};
+    for (const void* k : ks) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kDiluThreads, 0) != cudaSuccess) return 0;
+        fit = std::min(fit, n);
+    }
+    cap = sms * std::max(fit, 0);
+    return cap;
+}
+
+// The block D-ILU setup and solve of the instances `dl` (after k_rowscale): the scaled blocks
+// into the coloured order, the modified diagonal blocks colour by colour, then one cooperative
+// solve per group of instances whose CTAs fit on the device at once.
+int launch_dilu(Runner& R, const std::vector<int>& dl, const std::vector<double>& eta) {
+    if (dl.empty()) return 0;
+    auto C = [&](int k) { return R.ctx[k]; };
+    static thread_local DiluMap dmap;   // ~2 KB: not on every caller's stack
+    dmap.tab = R.dtab.p;
+    int nb = make_map(dmap.mp, dl, [&](int k) { return nblk(C(k)->dl_nlo + C(k)->dl_nup + C(k)->dl_rows, 256); });
+    if (nb) {
+        if (R.mixed) k_dilu_scatter<float><<<nb, 256, 0, R.stream>>>(dmap);
+        else k_dilu_scatter<double><<<nb, 256, 0, R.stream>>>(dmap);
+        R.launches++;
+    }
+    int maxc = 0;
+    for (int k : dl) maxc = std::max(maxc, C(k)->dl_ncol);
+    for (int c = 0; c < maxc; c++) {
+        nb = make_map(dmap.mp, dl, [&](int k) {
+            const sw2gpu_ctx* x = C(k);
+            return c < x->dl_ncol ? nblk(x->dl_cend[c] - x->dl_cstart[c], 256) : 0;
+        });
+        if (!nb) continue;
+        if (R.mixed) k_dilu_diag<float><<<nb, 256, 0, R.stream>>>(dmap, c);
+        else k_dilu_diag<double><<<nb, 256, 0, R.stream>>>(dmap, c);
+        R.launches++;
+    }
+    CK(cudaGetLastError());
+    const int cap = dilu_capacity();
+    if (cap <= 0) return fail(SW2GPU_E_CUDA, "the D-ILU solve kernel does not fit on this device");
+    size_t j0 = 0;
+    while (j0 < dl.size()) {
+        std::vector<int> grp;
+        int total = 0;
+        for (size_t j = j0; j < dl.size() && (int)grp.size() < kMaxBatch; j++) {
+            const int q = C(dl[j])->dl_cta;
+            if (!grp.empty() && total + q > cap) break;
+            grp.push_back(dl[j]);
+            total += q;
+        }
+        j0 += grp.size();
+        if (grp.size() == 1) {
+            DiluOne one;
+            one.K = R.dtab_h[grp[0]];
+            one.rtol = eta[grp[0]];
+            one.rtol_dev = R.capturing ? R.eta_dev.p : nullptr;
+            void* args[] = {(void*)&one};
+            void* kern = R.mixed ? (void*)k_dilu_bicgstab<float, DiluOne> : (void*)k_dilu_bicgstab<double, DiluOne>;
+            CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kDiluThreads), args, 0, R.stream));
+        } else {
+            static thread_local DiluTab t;   // ~4 KB
+            t.tab = R.dtab.p;
+            make_map(t.mp, grp, [&](int k) { return C(k)->dl_cta; });
+            for (size_t j = 0; j < grp.size(); j++) t.rtol[j] = eta[grp[j]];
+            void* args[] = {(void*)&t};
+            void* kern = R.mixed ? (void*)k_dilu_bicgstab<float, DiluTab> : (void*)k_dilu_bicgstab<double, DiluTab>;
+            CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kDiluThreads), args, 0, R.stream));
+        }
+        R.launches++;
+    }
+    return 0;
+}
+
 int launch_linear(Runner& R, const std::vector<int>& all, const std::vector<double>& eta) {
     auto C = [&](int k) { return R.ctx[k]; };
-    std::vector<int> sub, band;   // Krylov instances, direct banded solves
-    for (int k : all) (C(k)->band ? band : sub).push_back(k);
+    std::vector<int> sub, band, dl;   // block-Jacobi Krylov instances, direct banded solves, D-ILU solves
+    for (int k : all) (C(k)->band ? band : C(k)->dilu ? dl : sub).push_back(k);
     CK(cudaMemsetAsync(R.singular.p, 0, sizeof(int) * R.ctx.size(), R.stream));
     int rc = launch_map(R, all, 256, [&](int k) { return nblk(C(k)->V, 256); }, SW2_GO(k_rowscale<std::decay_t<decltype(src)>>, 0));
     if (rc) return rc;
@@ -800,6 +951,7 @@ int launch_linear(Runner& R, const std::vector<int>& all, const std::vector<doub
     Phase ph(&R, kPhKrylov);
     for (int k : band)
         if ((rc = launch_band(R, k))) return rc;
+    if ((rc = launch_dilu(R, dl, eta))) return rc;
     // instances that cannot all be co-resident go in successive launches
     size_t j0 = 0;
     while (j0 < sub.size()) {
@@ -1231,13 +1383,167 @@ extern "C" {
 int sw2gpu_abi_version(void) { return SW2GPU_ABI_VERSION; }
 const char* sw2gpu_last_error(void) { return g_err.c_str(); }
 
+// The D-ILU order and structure of a context (SW2GPU_PREC_DILU) from the BCSR pattern rp/col:
+// greedy colouring of the node graph (nodes in smallest-last order, each taking the lowest
+// colour none of its neighbours has), new rows colour by colour in natural order, each new
+// row's off-diagonal blocks sorted by new column (lower blocks first), the position of every
+// lower block's transpose, and the solve's CTAs: enough warps for the largest colour's 32-row
+// tiles, at most the co-resident grid.
+int build_dilu(sw2gpu_ctx* c, const std::vector<int>& rp, const std::vector<int>& col, cudaStream_t st) {
+    const int V = c->V;
+    // smallest-last order: repeatedly take out a node of least remaining degree (the lowest
+    // index among equals); colouring in the reverse of that order needs few colours on planar
+    // meshes (5 on the benchmark basins, where largest-first needs 6)
+    std::vector<int> order;
+    order.reserve(V);
+    {
+        std::vector<int> deg(V);
+        std::vector<char> gone(V, 0);
+        std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, std::greater<std::pair<int, int>>> pq;
+        for (int n = 0; n < V; n++) {
+            deg[n] = rp[n + 1] - rp[n] - 1;
+            pq.push({deg[n], n});
+        }
+        while (!pq.empty()) {
+            const auto top = pq.top();
+            pq.pop();
+            const int n = top.second;
+            if (gone[n] || top.first != deg[n]) continue;
+            gone[n] = 1;
+            order.push_back(n);
+            for (int k = rp[n]; k < rp[n + 1]; k++) {
+                const int j = col[k];
+                if (j != n && !gone[j]) pq.push({--deg[j], j});
+            }
+        }
+        std::reverse(order.begin(), order.end());
+    }
+    std::vector<int> colour(V, -1);
+    int ncol = 0;
+    for (int n : order) {
+        unsigned used = 0;
+        for (int k = rp[n]; k < rp[n + 1]; k++) {
+            const int j = col[k];
+            if (j != n && colour[j] >= 0) used |= 1u << colour[j];
+        }
+        int cc = 0;
+        while (cc < kMaxColours && ((used >> cc) & 1u)) cc++;
+        if (cc >= kMaxColours)
+            return fail(SW2GPU_E_ARG, "the node graph needs more than %d colours for the D-ILU order", kMaxColours);
+        colour[n] = cc;
+        ncol = std::max(ncol, cc + 1);
+    }
+    // new rows: colour q occupies pst[q] .. pst[q+1]-1, padded to whole 32-row tiles, its
+    // cnt[q] real rows first (natural order); padding rows have old = -1
+    std::vector<int> cnt(ncol, 0), pst(ncol + 1, 0);
+    for (int n = 0; n < V; n++) cnt[colour[n]]++;
+    for (int q = 0; q < ncol; q++) pst[q + 1] = pst[q] + (cnt[q] + 31) / 32 * 32;
+    const int N = pst[ncol], ntile = N / 32;
+    std::vector<int> old(N, -1), nw(V);
+    {
+        std::vector<int> f(pst.begin(), pst.end() - 1);
+        for (int n = 0; n < V; n++) {
+            const int q = f[colour[n]]++;
+            old[q] = n;
+            nw[n] = q;
+        }
+    }
+    // each real row's off-diagonal blocks (new column, natural block) sorted by new column;
+    // lower = lower colours, upper = higher colours
+    std::vector<int> lcnt(N, 0), ucnt(N, 0);
+    std::vector<std::pair<int, int>> row;
+    auto row_of = [&](int n) {
+        const int i = old[n];
+        row.clear();
+        for (int k = rp[i]; k < rp[i + 1]; k++)
+            if (col[k] != i) row.push_back({nw[col[k]], k});
+        std::sort(row.begin(), row.end());
+        return (int)(std::lower_bound(row.begin(), row.end(), std::make_pair(n, -1)) - row.begin());
+    };
+    for (int n = 0; n < N; n++)
+        if (old[n] >= 0) {
+            lcnt[n] = row_of(n);
+            ucnt[n] = (int)row.size() - lcnt[n];
+        }
+    // ELL layout per colour: colour q's rows take lkn[q] lower and ukn[q] upper slots each (its
+    // longest row's counts, at most kDiluMaxSlots); the k-th lower slot of row n is
+    // lbase[q] + k L_q + (n - pst[q]), L_q = pst[q+1] - pst[q] (upper: ubase, ukn)
+    std::vector<int> lkn(ncol, 0), ukn(ncol, 0), lbase(ncol + 1, 0), ubase(ncol + 1, 0);
+    for (int q = 0; q < ncol; q++) {
+        for (int n = pst[q]; n < pst[q + 1]; n++) {
+            lkn[q] = std::max(lkn[q], lcnt[n]);
+            ukn[q] = std::max(ukn[q], ucnt[n]);
+        }
+        if (lkn[q] > kDiluMaxSlots || ukn[q] > kDiluMaxSlots)
+            return fail(SW2GPU_E_ARG, "a node has more than %d neighbours of lower or higher colour (D-ILU order)",
+                        kDiluMaxSlots);
+        lbase[q + 1] = lbase[q] + lkn[q] * (pst[q + 1] - pst[q]);
+        ubase[q + 1] = ubase[q] + ukn[q] * (pst[q + 1] - pst[q]);
+    }
+    std::vector<int> colour_of(N);
+    for (int q = 0; q < ncol; q++)
+        for (int n = pst[q]; n < pst[q + 1]; n++) colour_of[n] = q;
+    auto lslot = [&](int n, int k) { const int q = colour_of[n]; return lbase[q] + k * (pst[q + 1] - pst[q]) + n - pst[q]; };
+    auto uslot = [&](int n, int k) { const int q = colour_of[n]; return ubase[q] + k * (pst[q + 1] - pst[q]) + n - pst[q]; };
+    const int nlo = lbase[ncol], nup = ubase[ncol];
+    std::vector<int> lcol(nlo, -1), lsrc(nlo, -1), ucol(nup, -1), usrc(nup, -1), tslot(nlo, -1);
+    for (int n = 0; n < N; n++) {
+        if (old[n] < 0) continue;
+        const int nl = row_of(n);
+        for (int k = 0; k < (int)row.size(); k++) {
+            const int s2 = k < nl ? lslot(n, k) : uslot(n, k - nl);
+            (k < nl ? lcol : ucol)[s2] = row[k].first;
+            (k < nl ? lsrc : usrc)[s2] = row[k].second;
+        }
+    }
+    // the transpose of every lower block (n, j): the slot of n among j's upper blocks
+    for (int n = 0; n < N; n++)
+        for (int k = 0; k < lcnt[n]; k++) {
+            const int s2 = lslot(n, k), jj = lcol[s2];
+            int found = -1;
+            for (int k2 = 0; k2 < ucnt[jj]; k2++)
+                if (ucol[uslot(jj, k2)] == n) found = uslot(jj, k2);
+            if (found < 0) return fail(SW2GPU_E_ARG, "the block pattern is not symmetric (D-ILU order)");
+            tslot[s2] = found;
+        }
+    int mt = 1;
+    for (int q = 0; q < ncol; q++) mt = std::max(mt, (pst[q + 1] - pst[q]) / 32);
+    const int cap = dilu_capacity();
+    if (cap <= 0) return fail(SW2GPU_E_CUDA, "the D-ILU solve kernel does not fit on this device");
+    c->dilu = true;
+    c->dl_ncol = ncol;
+    c->dl_rows = N;
+    c->dl_nlo = nlo;
+    c->dl_nup = nup;
+    c->dl_cta = std::max(1, std::min(cap, (mt + kDiluWarps - 1) / kDiluWarps));
+    for (int q = 0; q <= kMaxColours; q++) {
+        c->dl_cstart[q] = pst[std::min(q, ncol)];
+        c->dl_cend[q] = q < ncol ? pst[q] + cnt[q] : N;
+        c->dl_lbase[q] = q < ncol ? lbase[q] : nlo;
+        c->dl_ubase[q] = q < ncol ? ubase[q] : nup;
+        c->dl_lkn[q] = q < ncol ? lkn[q] : 0;
+        c->dl_ukn[q] = q < ncol ? ukn[q] : 0;
+    }
+    int rc = 0;
+    rc |= up(c->dl_lcol, lcol, st); rc |= up(c->dl_ucol, ucol, st);
+    rc |= up(c->dl_lsrc, lsrc, st); rc |= up(c->dl_usrc, usrc, st);
+    rc |= up(c->dl_tslot, tslot, st); rc |= up(c->dl_old, old, st);
+    const size_t nval = 9ull * std::max(nlo + nup, 1);
+    if (c->p.precision == SW2GPU_MIXED) rc |= zalloc(c->dl_blk32, nval, st);
+    else rc |= zalloc(c->dl_blk64, nval, st);
+    rc |= zalloc(c->dl_Dti, 9ull * N, st); rc |= zalloc(c->dl_Dd, 9ull * N, st);
+    rc |= zalloc(c->dl_part, 8ull * c->dl_cta, st);
+    for (auto& b : c->dl_vec) rc |= zalloc(b, 3ull * N, st);
+    return rc;
+}
+
 int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, sw2gpu_ctx** out) {
     if (!m || !prm || !out) return fail(SW2GPU_E_ARG, "null argument");
     *out = nullptr;
     if (m->nnodes <= 0 || m->nelems2d < 0 || m->nelems1d < 0) return fail(SW2GPU_E_ARG, "bad mesh sizes");
     if (prm->precision != SW2GPU_FP64 && prm->precision != SW2GPU_MIXED) return fail(SW2GPU_E_ARG, "bad precision");
-    if (prm->precond != SW2GPU_PREC_BJACOBI && prm->precond != SW2GPU_PREC_BAND)
-        return fail(SW2GPU_E_ARG, "preconditioner %d not built (SW2GPU_PREC_BJACOBI or SW2GPU_PREC_BAND)", prm->precond);
+    if (prm->precond != SW2GPU_PREC_BJACOBI && prm->precond != SW2GPU_PREC_BAND && prm->precond != SW2GPU_PREC_DILU)
+        return fail(SW2GPU_E_ARG, "preconditioner %d not built (SW2GPU_PREC_BJACOBI, _BAND or _DILU)", prm->precond);
     if (prm->precond == SW2GPU_PREC_BAND && prm->precision != SW2GPU_FP64)
         return fail(SW2GPU_E_ARG, "the banded LU solve is FP64 only");
     int dev = 0;
@@ -1460,9 +1766,10 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
     rc |= zalloc(c->val, 9ull * nnzb, st);
     rc |= zalloc(c->S_, 3ull * V, st); rc |= zalloc(c->bs, 3ull * V, st);
     rc |= zalloc(c->dinv64, 9ull * V, st);
-    if (prm->precision == SW2GPU_MIXED)
+    const bool bjacobi = prm->precond == SW2GPU_PREC_BJACOBI;   // the folded operator and its vectors
+    if (bjacobi && prm->precision == SW2GPU_MIXED)
         rc |= zalloc(c->aoff32, 9ull * (nnzb - V), st);
-    else
+    else if (bjacobi)
         rc |= zalloc(c->aoff64, 9ull * (nnzb - V), st);
     {
         // the pattern without its diagonal (one diagonal block per row, checked above)
@@ -1491,7 +1798,12 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
         rc |= zalloc(c->band_mem, 3ull * V * (2ull * c->band_bw + 1), st);
         rc |= zalloc(c->band_y, 3ull * V, st);
     }
-    for (auto& b : c->kv64) rc |= zalloc(b, 3ull * V, st);
+    if (prm->precond == SW2GPU_PREC_DILU && !rc) {
+        const int r2 = build_dilu(c, rp, col, st);
+        if (r2) return r2;
+    }
+    if (bjacobi)
+        for (auto& b : c->kv64) rc |= zalloc(b, 3ull * V, st);
     rc |= zalloc(c->ncounter, 1, st);
     const int gblocks = nblk(V, kGatherThreads);
     rc |= zalloc(c->npart, gblocks, st);

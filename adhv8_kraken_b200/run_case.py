@@ -1,7 +1,7 @@
 """Runs the seeded basin workload for a few time steps and prints per-step statistics.
 
     python -m adhv8_kraken_b200.run_case --points 500000 --steps 2 [--precision fp64|mixed]
-                                         [--variant JAC_MINB,STAGES]
+                                         [--variant JAC_MINB,STAGES] [--precond bjacobi|dilu] [--dt S]
 
 One JSON line per step (Newton and Krylov iterations, device time per phase).  This is the
 command the kernel profiles are taken on: it runs the same code path as ``bench.py`` without
@@ -20,6 +20,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precond", choices=["bjacobi", "dilu"], default="bjacobi")
+    ap.add_argument("--dt", type=float, default=5.0)
     ap.add_argument("--variant", default=None,
                     help="launch variant 'jac_minb,stages' (e.g. 1,3); default: the library's own")
     a = ap.parse_args(argv)
@@ -27,9 +29,10 @@ def main(argv=None):
     from .sw2 import SW2GPU
 
     size = 20000.0 * math.sqrt(a.points / 5e5)
-    model = meshgen.bumpy_basin(a.points, seed=a.seed, size=size, nsteps=a.steps, dt=5.0, name="basin")
+    model = meshgen.bumpy_basin(a.points, seed=a.seed, size=size, nsteps=a.steps, dt=a.dt, name="basin")
     prec = capi.SW2GPU_FP64 if a.precision == "fp64" else capi.SW2GPU_MIXED
-    g = SW2GPU(model, precision=prec)
+    pc = capi.SW2GPU_PREC_BJACOBI if a.precond == "bjacobi" else capi.SW2GPU_PREC_DILU
+    g = SW2GPU(model, precision=prec, precond=pc)
     if a.variant:
         g.set_variant(*(int(x) for x in a.variant.split(",")))
     print(json.dumps({"triangles": model.nelems2d, "nodes": model.nnodes, "nnzb": g.nnzb}))

@@ -68,6 +68,18 @@ extern "C" {
                                   * Work n bw^2 per factorisation (n = 3 nnodes, bw the half-width in
                                   * unknowns): for the small and medium meshes of test decks, whose
                                   * time steps are too long for block Jacobi to converge */
+#define SW2GPU_PREC_DILU     3   /* BiCGSTAB preconditioned with block D-ILU, the diagonal form of
+                                  * block ILU(0) (L and U are the matrix's own strict block parts,
+                                  * the diagonal blocks Dt_n = D_n - sum L_nk Dt_k^-1 U_kn), in a
+                                  * greedy multicolour node order, applied on the split system with
+                                  * Eisenstat's rearrangement (one SpMV's bytes per application).
+                                  * About 3x fewer iterations than block Jacobi on the benchmark
+                                  * basins, but each iteration waits at 4C - 1 grid barriers for C
+                                  * colours (19 for 5) against block Jacobi's 3, so on a B200 it is
+                                  * slower at every measured size (10k-1M triangles); block Jacobi
+                                  * stays the default.  FP64 or MIXED (FP32 blocks); create rejects
+                                  * a node graph that needs more than 16 colours, or a node with more
+                                  * than 16 neighbours of lower or of higher colour, with SW2GPU_E_ARG */
 
 /* Mesh and model data (what fe_sw2_* read from SGRID / SMODEL).  Host pointers;
  * the library copies what it needs at create time. */

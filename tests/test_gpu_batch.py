@@ -24,16 +24,19 @@ def _summary(stats):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", [capi.SW2GPU_FP64, capi.SW2GPU_MIXED])
-def test_batch_equals_alone(precision):
+@pytest.mark.parametrize("precision,precond", [(capi.SW2GPU_FP64, capi.SW2GPU_PREC_BJACOBI),
+                                               (capi.SW2GPU_MIXED, capi.SW2GPU_PREC_BJACOBI),
+                                               (capi.SW2GPU_FP64, capi.SW2GPU_PREC_DILU),
+                                               (capi.SW2GPU_MIXED, capi.SW2GPU_PREC_DILU)])
+def test_batch_equals_alone(precision, precond):
     models = uneven_models()
     alone = []
     for m in models:
-        g = SW2GPU(m, precision=precision)
+        g = SW2GPU(m, precision=precision, precond=precond)
         st = [g.step() for _ in range(NSTEPS)]
         alone.append((g.get_state(0), g.get_wd(), _summary(st)))
         g.close()
-    solvers = [SW2GPU(m, precision=precision) for m in models]
+    solvers = [SW2GPU(m, precision=precision, precond=precond) for m in models]
     batch = SW2Batch(solvers)
     steps = [batch.step() for _ in range(NSTEPS)]
     for k, g in enumerate(solvers):
