@@ -580,16 +580,17 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
     tot_ms, launches, bytes_per_launch = kernels[name]
     per_launch_ms = tot_ms / max(launches, 1)
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
-    # measured DRAM traffic of the Krylov kernel: bytes per BiCGSTAB iteration from one ncu
-    # capture of the same workload (profiles/traffic_basin_1M_tri.md), times this run's mean
-    # iterations per launch (traffic grows with the iterations)
+    # measured DRAM traffic of the Krylov kernel: bytes per BiCGSTAB iteration and node from one
+    # ncu capture of a smaller basin of the same generator (profiles/traffic_k_bicgstab_basin_
+    # 600k_tri.md), times this run's nodes and mean iterations per launch (the sweeps' and the
+    # vectors' bytes grow in proportion to both)
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic_basin_1M_tri.md")
-    if name == "k_bicgstab" and os.path.exists(tf) and T == 998582:
+    tf = os.path.join(ROOT, "profiles", "traffic_k_bicgstab_basin_600k_tri.md")
+    if name == "k_bicgstab" and os.path.exists(tf):
         with open(tf) as f:
             for ln in f:
-                if ln.startswith("k_bicgstab_bytes_per_iteration:"):
-                    traffic = float(ln.split(":")[1]) * (lin / max(newton, 1))
+                if ln.startswith("k_bicgstab_bytes_per_iteration_per_node:"):
+                    traffic = float(ln.split(":")[1]) * V * (lin / max(newton, 1))
     roofline = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": per_launch_ms,
