@@ -28,6 +28,7 @@
 #include "../../include/sw2gpu.h"
 #include "sw2_band.cuh"
 #include "sw2_dilu.cuh"
+#include "sw2_tables.h"
 #include "sw2_kernels.cuh"
 #include "sw2_krylov.cuh"
 #include "sw2_series.h"
@@ -96,7 +97,10 @@ struct sw2gpu_ctx {
     std::vector<int> str_bc, str_isigma, str_ivx, str_ivy, str_iu0;
     std::vector<MatParams> mats_h;
     std::vector<int> dir_node, dir_mask, dir_str;
-    std::vector<int> rowptr_h, col_h;
+    MeshTables tab;                    // pattern and gather lists (sw2_tables.h)
+    std::vector<int> tri_h, edg_h;     // connectivity the tables were made from (sw2gpu_remesh)
+    std::vector<int>& rowptr_h = tab.rp;
+    std::vector<int>& col_h = tab.col;
     // device mesh
     DBuf<double> x, y, z, djac, gx0, gy0, gx1, gy1, gx2, gy2, bdjac, bnx, bny;
     DBuf<int> en0, en1, en2, emat, bn0, bn1, bkind, bstr;
@@ -1537,7 +1541,14 @@ int build_dilu(sw2gpu_ctx* c, const std::vector<int>& rp, const std::vector<int>
     return rc;
 }
 
+// create with the mesh tables made by the caller (sw2gpu_remesh) or here (pre == nullptr)
+int create_impl(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, MeshTables* pre, sw2gpu_ctx** out);
+
 int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, sw2gpu_ctx** out) {
+    return create_impl(m, prm, stream, nullptr, out);
+}
+
+int create_impl(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, MeshTables* pre, sw2gpu_ctx** out) {
     if (!m || !prm || !out) return fail(SW2GPU_E_ARG, "null argument");
     *out = nullptr;
     if (m->nnodes <= 0 || m->nelems2d < 0 || m->nelems1d < 0) return fail(SW2GPU_E_ARG, "bad mesh sizes");
@@ -1660,76 +1671,27 @@ int sw2gpu_create(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, 
         mp.cor_speed = std::sin((kPi / 180.) * m->mat_coriolis[k]) * 2. * kEarthRotat;
         mp.has_source = (k < c->S && c->str_bc[k] == SW2GPU_BCT_WATER_SOURCE) ? 1 : 0;
     }
-    // BCSR pattern: sorted unique columns per node row (element pairs and edge pairs)
-    std::vector<int> deg(V + 1, 0);
-    for (int e = 0; e < T; e++) for (int i = 0; i < 3; i++) deg[tri[3 * e + i]] += 3;
-    for (int j = 0; j < E; j++) for (int i = 0; i < 2; i++) deg[edg[2 * j + i]] += 2;
-    std::vector<int> start(V + 1, 0);
-    for (int n = 0; n < V; n++) start[n + 1] = start[n] + deg[n];
-    std::vector<int> tmp(start[V]);
-    std::vector<int> fillc(V, 0);
-    for (int e = 0; e < T; e++)
-        for (int i = 0; i < 3; i++) {
-            const int a = tri[3 * e + i];
-            for (int k = 0; k < 3; k++) tmp[start[a] + fillc[a]++] = tri[3 * e + k];
-        }
-    for (int j = 0; j < E; j++)
-        for (int i = 0; i < 2; i++) {
-            const int a = edg[2 * j + i];
-            for (int k = 0; k < 2; k++) tmp[start[a] + fillc[a]++] = edg[2 * j + k];
-        }
-    std::vector<int>& rp = c->rowptr_h;
-    std::vector<int>& col = c->col_h;
-    rp.assign(V + 1, 0);
-    col.clear();
-    col.reserve(start[V] / 2);
-    for (int n = 0; n < V; n++) {
-        auto b = tmp.begin() + start[n], e2 = tmp.begin() + start[n + 1];
-        std::sort(b, e2);
-        auto last = std::unique(b, e2);
-        col.insert(col.end(), b, last);
-        rp[n + 1] = (int)col.size();
+    // BCSR pattern and reference-order gather lists (sw2_tables.h)
+    c->tri_h.assign(tri, tri + 3ull * T);
+    c->edg_h.assign(edg, edg + 2ull * E);
+    if (pre) {
+        c->tab = std::move(*pre);
+    } else {
+        const int tr = build_tables(V, T, E, tri, edg, c->tab);
+        if (tr > 0) return fail(SW2GPU_E_ARG, "node %d belongs to no element", tr - 1);
     }
+    if (c->tab.V != V || c->tab.T != T || c->tab.E != E) return fail(SW2GPU_E_ARG, "mesh tables of another mesh");
+    const std::vector<int>& rp = c->tab.rp;
+    const std::vector<int>& col = c->tab.col;
+    const std::vector<int>& blk_row = c->tab.blk_row;
+    const std::vector<int>& dpos = c->tab.dpos;
+    const std::vector<int>& blk_ptr = c->tab.blk_ptr;
+    const std::vector<int>& blk_src = c->tab.blk_src;
+    const std::vector<int>& slot_ptr = c->tab.slot_ptr;
+    const std::vector<int>& slot_idx = c->tab.slot_idx;
     const int nnzb = c->nnzb = (int)col.size();
-    std::vector<int> blk_row(nnzb), dpos(V, -1);
-    for (int n = 0; n < V; n++)
-        for (int k = rp[n]; k < rp[n + 1]; k++) {
-            blk_row[k] = n;
-            if (col[k] == n) dpos[n] = k;
-        }
-    for (int n = 0; n < V; n++)
-        if (dpos[n] < 0) return fail(SW2GPU_E_ARG, "node %d belongs to no element", n);
-    auto find_blk = [&](int i, int j) {
-        auto b = col.begin() + rp[i], e2 = col.begin() + rp[i + 1];
-        return (int)(std::lower_bound(b, e2, j) - col.begin());
-    };
-    // BCSR block <- element-block slots, in reference order (elements then edges)
     const size_t nsrc = 9ull * T + 4ull * E;
-    std::vector<int> src_blk(nsrc);
-    for (int e = 0; e < T; e++)
-        for (int a = 0; a < 3; a++)
-            for (int b = 0; b < 3; b++) src_blk[9ull * e + 3 * a + b] = find_blk(tri[3 * e + a], tri[3 * e + b]);
-    for (int j = 0; j < E; j++)
-        for (int a = 0; a < 2; a++)
-            for (int b = 0; b < 2; b++) src_blk[9ull * T + 4 * j + 2 * a + b] = find_blk(edg[2 * j + a], edg[2 * j + b]);
-    std::vector<int> blk_ptr(nnzb + 1, 0), blk_src(nsrc);
-    for (size_t q = 0; q < nsrc; q++) blk_ptr[src_blk[q] + 1]++;
-    for (int k = 0; k < nnzb; k++) blk_ptr[k + 1] += blk_ptr[k];
-    {
-        std::vector<int> f2(blk_ptr.begin(), blk_ptr.end() - 1);
-        for (size_t q = 0; q < nsrc; q++) blk_src[f2[src_blk[q]]++] = (int)q;   // q ascending = reference order
-    }
-    // node <- residual slots, reference order
     const size_t nslot = 3ull * T + 2ull * E;
-    std::vector<int> slot_ptr(V + 1, 0), slot_idx(nslot);
-    for (int e = 0; e < T; e++) for (int i = 0; i < 3; i++) slot_ptr[tri[3 * e + i] + 1]++;
-    for (int j = 0; j < E; j++) for (int i = 0; i < 2; i++) slot_ptr[edg[2 * j + i] + 1]++;
-    for (int n = 0; n < V; n++) slot_ptr[n + 1] += slot_ptr[n];
-    {
-        std::vector<int> f2(slot_ptr.begin(), slot_ptr.end() - 1);
-        for (int e = 0; e < T; e++) for (int i = 0; i < 3; i++) slot_idx[f2[tri[3 * e + i]]++] = 3 * e + i;
-        for (int j = 0; j < E; j++) for (int i = 0; i < 2; i++) slot_idx[f2[edg[2 * j + i]]++] = 3 * T + 2 * j + i;
-    }
     // upload
     std::vector<double> xv(m->x, m->x + V), yv(m->y, m->y + V), zv(m->z, m->z + V);
     std::vector<int> e0(T), e1(T), e2(T), em(m->elem2d_mat, m->elem2d_mat + T);
@@ -1853,6 +1815,56 @@ int sw2gpu_destroy(sw2gpu_ctx* c) {
     if (!c) return SW2GPU_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     delete c;
+    return SW2GPU_OK;
+}
+
+int sw2gpu_remesh(sw2gpu_ctx* old, const sw2gpu_mesh* m, sw2gpu_ctx** out) {
+    if (!old || !m || !out) return fail(SW2GPU_E_ARG, "null argument");
+    *out = nullptr;
+    const int V = m->nnodes, T = m->nelems2d, E = m->nelems1d;
+    if (V <= 0 || T < 0 || E < 0) return fail(SW2GPU_E_ARG, "bad mesh sizes");
+    for (size_t q = 0; q < 3ull * T; q++)
+        if (m->elem2d_nodes[q] < 0 || m->elem2d_nodes[q] >= V) return fail(SW2GPU_E_ARG, "element %zu: node out of range", q / 3);
+    for (size_t q = 0; q < 2ull * E; q++)
+        if (m->elem1d_nodes[q] < 0 || m->elem1d_nodes[q] >= V) return fail(SW2GPU_E_ARG, "edge %zu: node out of range", q / 2);
+    // the tables: only the pattern rows the adaption touched are rebuilt (from scratch when the
+    // mesh lost nodes)
+    MeshTables t;
+    int tr = update_tables(old->tab, old->tri_h.data(), old->edg_h.data(), V, T, E, m->elem2d_nodes, m->elem1d_nodes, t);
+    if (tr < 0) tr = build_tables(V, T, E, m->elem2d_nodes, m->elem1d_nodes, t);
+    if (tr > 0) return fail(SW2GPU_E_ARG, "node %d belongs to no element", tr - 1);
+    sw2gpu_params prm = old->p;
+    sw2gpu_ctx* c = nullptr;
+    int rc = create_impl(m, &prm, (void*)old->stream, &t, &c);
+    if (rc) return rc;
+    // the new context takes over the stream and the settings
+    c->own_stream = old->own_stream;
+    old->own_stream = false;
+    c->dt = old->dt;
+    c->wait_barrier = old->wait_barrier;
+    c->wait_copy = old->wait_copy;
+    c->tune_jac_minb = old->tune_jac_minb;
+    c->tune_stages = old->tune_stages;
+    if (!rc && old->dacont_on) rc = sw2gpu_set_dacont(c, 1);
+    if (!rc && old->mass_on) rc = sw2gpu_set_mass_tracking(c, 1, old->mass_density);
+    if (!rc && old->use_graphs) rc = sw2gpu_set_graphs(c, 1);
+    // the three time levels of the nodes both meshes have (node numbers are kept); new nodes start at 0
+    const size_t nb = sizeof(double) * std::min(V, old->V);
+    for (int l = 0; !rc && l < 3; l++) {
+        if (cudaMemcpyAsync(c->H(l), old->H(l), nb, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess ||
+            cudaMemcpyAsync(c->U(l), old->U(l), nb, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess ||
+            cudaMemcpyAsync(c->Vv(l), old->Vv(l), nb, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+            rc = fail(SW2GPU_E_CUDA, "copying the time levels: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = fail(SW2GPU_E_CUDA, "remesh: stream error");
+    if (rc) {   // the old context keeps its stream and stays usable
+        old->own_stream = c->own_stream;
+        c->own_stream = false;
+        delete c;
+        return rc;
+    }
+    sw2gpu_destroy(old);
+    *out = c;
     return SW2GPU_OK;
 }
 

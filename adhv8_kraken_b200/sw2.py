@@ -35,7 +35,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
            "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont",
            "sw2gpu_set_wait_limits", "sw2gpu_snapshot", "sw2gpu_elem_error", "sw2gpu_set_mass_tracking",
-           "sw2gpu_step_mass", "sw2gpu_set_wind", "sw2gpu_set_waves"]
+           "sw2gpu_step_mass", "sw2gpu_set_wind", "sw2gpu_set_waves", "sw2gpu_remesh"]
 
 
 class SW2Error(RuntimeError):
@@ -90,6 +90,7 @@ def lib():
         L.sw2gpu_set_mass_tracking.argtypes = [vp, C.c_int32, C.c_double]
         L.sw2gpu_set_wind.argtypes = [vp, c_int32_p, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_set_waves.argtypes = [vp, c_double_p, c_double_p, c_double_p]
+        L.sw2gpu_remesh.argtypes = [vp, vp, vp]
         L.sw2gpu_step_mass.argtypes = [vp, c_double_p, c_double_p]
         L.sw2gpu_set_variant.argtypes = [vp, C.c_int32, C.c_int32]
         L.sw2gpu_get_variant.argtypes = [vp, c_int32_p, c_int32_p]
@@ -175,6 +176,18 @@ class SW2GPU:
         h0, u0, v0 = model.initial_state()
         for lvl in range(3):
             self.set_state(lvl, h0, u0, v0)
+
+    def remesh(self, model):
+        """Moves this solver to `model`, an adaption of its mesh that keeps node and triangle
+        numbers (sw2gpu_remesh): the time levels of the kept nodes stay, new nodes start at 0."""
+        arrays = MeshArrays(model)
+        h = C.c_void_p()
+        _check(lib().sw2gpu_remesh(self.h, C.byref(arrays.mesh), C.byref(h)))
+        self.h, self.model, self.arrays = h, model, arrays
+        self.V, self.T = model.nnodes, model.nelems2d
+        n = C.c_int32()
+        _check(lib().sw2gpu_load(self.h, C.byref(n), None, None, None, None))
+        self.nnzb = n.value
 
     def autotune(self):
         """Times the launch variants on this mesh and keeps the fastest; (jac_minb, stages)."""

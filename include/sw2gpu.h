@@ -140,6 +140,19 @@ const char *sw2gpu_last_error(void);
  * mesh adaption).  `stream` is a cudaStream_t (NULL = a stream owned by the context). */
 int sw2gpu_create(const sw2gpu_mesh *mesh, const sw2gpu_params *params, void *stream, sw2gpu_ctx **out);
 int sw2gpu_destroy(sw2gpu_ctx *ctx);
+/* After a mesh adaption (adpt_main, src/grid/adpt_main.c:17): the context of the adapted mesh,
+ * made from `old`, which is released on success (*out replaces it; on failure `old` is kept and
+ * still usable).  The adaption must keep node and triangle numbers (nodes and triangles
+ * appended, some triangles' nodes changed, trailing triangles dropped, boundary edges changed),
+ * as refinement does: then only the pattern rows of nodes that a changed, new or removed
+ * element or edge touches are rebuilt and every other row is copied (a mesh with fewer nodes
+ * is rebuilt from scratch), the tables equal those sw2gpu_create would make, and so do all
+ * later results.  The new context keeps the stream, the parameters, dt, the launch variant, the
+ * wait limits and the transport-output, mass-tracking and graph settings, and the three time
+ * levels of the nodes both meshes have; new nodes start at 0 (set them with sw2gpu_set_state).
+ * Wind and wave stresses are per node: set them again.  A context inside a batch, engine or
+ * server is not remeshed. */
+int sw2gpu_remesh(sw2gpu_ctx *old, const sw2gpu_mesh *mesh, sw2gpu_ctx **out);
 /* Launch variants (no counterpart in the reference).  Two knobs change the speed of a step,
  * never its results: the register budget of the wet-Jacobian kernel (jac_minb: 1 or 2
  * resident CTAs per SM) and the depth of the Krylov kernel's shared-memory tile ring (stages:

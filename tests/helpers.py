@@ -45,3 +45,33 @@ def field_errors(got, exp):
     dq = np.hypot(got["uh"] - exp["uh"], got["vh"] - exp["vh"])
     qm = float(np.hypot(exp["uh"], exp["vh"]).max())
     return {"h": eh, "q": float(dq.max() / max(qm, 1e-300))}
+
+
+def centroid_refine(m, elems):
+    """The model `m` with each triangle of `elems` split at its centroid, as a refinement step of
+    an adaption would: the triangle keeps its number as (a, b, new node), the two other parts and
+    the new nodes are appended (node and triangle numbers kept).  The new node takes the mean
+    bed, coordinates and hot-start state of the triangle's vertices."""
+    import dataclasses
+    import numpy as np
+    x, y, z = list(m.x), list(m.y), list(m.z)
+    h0, u0, v0 = list(m.h0), list(m.u0), list(m.v0)
+    ns = list(m.node_string)
+    tri = m.tri.copy()
+    extra, extra_mat = [], []
+    for e in elems:
+        a, b, c = (int(q) for q in tri[e])
+        k = len(x)
+        for arr, src in ((x, m.x), (y, m.y), (z, m.z), (h0, m.h0), (u0, m.u0), (v0, m.v0)):
+            arr.append((src[a] + src[b] + src[c]) / 3.0)
+        ns.append(-1)
+        tri[e] = (a, b, k)
+        extra += [(b, c, k), (c, a, k)]
+        extra_mat += [m.tri_mat[e]] * 2
+    f = lambda a: np.asarray(a, dtype=np.float64)
+    return dataclasses.replace(
+        m, x=f(x), y=f(y), z=f(z), h0=f(h0), u0=f(u0), v0=f(v0),
+        node_string=np.asarray(ns, dtype=np.int32),
+        tri=np.concatenate([tri, np.asarray(extra, dtype=np.int32).reshape(-1, 3)]).astype(np.int32),
+        tri_mat=np.concatenate([m.tri_mat, np.asarray(extra_mat, dtype=np.int32)]).astype(np.int32),
+        name=m.name + "_refined")
