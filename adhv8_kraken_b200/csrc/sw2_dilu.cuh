@@ -115,6 +115,7 @@ struct DiluTab {
     const DiluArgs* tab;
     LaunchMap mp;
     double rtol[kMaxBatch];
+    const double* rtol_dev;         // when set, instance k's tolerance is read at rtol_dev[k] (graph replays)
     // the instance's descriptor is copied to shared memory once (called by the whole CTA)
     __device__ __forceinline__ const DiluArgs& get(int& pl, int& np, double& rt) const {
         __shared__ DiluArgs sk;
@@ -129,7 +130,7 @@ struct DiluTab {
         pl = b - mp.boff[lo];
         nb = mp.boff[lo + 1] - mp.boff[lo];
         np = nb;
-        rt = rtol[lo];
+        rt = rtol_dev ? __ldcg(rtol_dev + mp.ids[lo]) : rtol[lo];
         if (threadIdx.x == 0) sk = tab[mp.ids[lo]];
         __syncthreads();
         return sk;

@@ -278,6 +278,7 @@ struct KrylovTab {
     double rtol[kMaxBatch];
     StageLayout lay;
     int fuse;                 // fused update for every instance of the launch (their vectors together)
+    const double* rtol_dev;   // when set, instance k's tolerance is read at rtol_dev[k] (graph replays)
     __device__ __forceinline__ const KrylovInst& get(int& pl, int& np, double& rt) const {
         int nb;
         const int b = blockIdx.x;
@@ -290,7 +291,7 @@ struct KrylovTab {
         pl = b - mp.boff[lo];
         nb = mp.boff[lo + 1] - mp.boff[lo];
         np = nb;
-        rt = rtol[lo];
+        rt = rtol_dev ? __ldcg(rtol_dev + mp.ids[lo]) : rtol[lo];
         return tab[mp.ids[lo]];
     }
     __device__ __forceinline__ bool fuse_update(const KrylovInst&) const { return fuse != 0; }

@@ -305,8 +305,27 @@ void* krylov_kernel(int stages) {
 struct Runner {
     cudaStream_t stream = nullptr;
     bool capturing = false;       // launches are being captured into a CUDA graph
-    DBuf<double> eta_dev;         // Krylov tolerance of a graph-replayed Newton iteration
+    DBuf<double> eta_dev;         // Krylov tolerance of every instance in a graph-replayed Newton iteration
     double* eta_h = nullptr;      // its pinned host copy
+    // CUDA graphs of a batch step (sw2gpu_batch_set_graphs): the step start and a Newton
+    // iteration of all instances, per arrangement of the instances' time levels, dt and launch
+    // variant (they are baked into the captured launches); a few are kept
+    struct BatchGraph {
+        std::vector<int> lv;
+        std::vector<double> dt;
+        int jac_minb = -1, stages = -1;
+        cudaGraphExec_t start = nullptr, newton = nullptr;
+        int kernels_start = 0, kernels_newton = 0;
+    };
+    bool use_graphs = false;
+    std::vector<BatchGraph> bgraphs;
+    void drop_batch_graphs() {
+        for (auto& g : bgraphs) {
+            if (g.start) cudaGraphExecDestroy(g.start);
+            if (g.newton) cudaGraphExecDestroy(g.newton);
+        }
+        bgraphs.clear();
+    }
     std::vector<sw2gpu_ctx*> ctx;
     bool mixed = false;
     DBuf<KrylovInst> ktab;
@@ -341,6 +360,7 @@ struct Runner {
             cudaEventSynchronize(tab_ev);
             cudaEventDestroy(tab_ev);
         }
+        drop_batch_graphs();
         if (ktab_h) cudaFreeHost(ktab_h);
         if (dtab_h) cudaFreeHost(dtab_h);
         if (eta_h) cudaFreeHost(eta_h);
@@ -478,8 +498,8 @@ int runner_alloc(Runner& R, cudaStream_t stream, bool mixed, int cap) {
     CK(cudaMemsetAsync(R.norms.p, 0, sizeof(Norms) * cap, stream));
     CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * cap, stream));
     CK(cudaMallocHost(&R.norms_h, sizeof(Norms) * cap));
-    CK(cudaMallocHost(&R.eta_h, sizeof(double)));
-    if (R.eta_dev.alloc(1)) return fail(SW2GPU_E_NOMEM, "tolerance word");
+    CK(cudaMallocHost(&R.eta_h, sizeof(double) * cap));
+    if (R.eta_dev.alloc(cap)) return fail(SW2GPU_E_NOMEM, "tolerance words");
     CK(cudaMallocHost(&R.ctl_h, sizeof(KrylovCtl) * cap));
     R.tab_h.resize(cap);
     CK(cudaMallocHost(&R.ktab_h, sizeof(KrylovInst) * cap));
@@ -921,13 +941,14 @@ int launch_dilu(Runner& R, const std::vector<int>& dl, const std::vector<double>
             DiluOne one;
             one.K = R.dtab_h[grp[0]];
             one.rtol = eta[grp[0]];
-            one.rtol_dev = R.capturing ? R.eta_dev.p : nullptr;
+            one.rtol_dev = R.capturing ? R.eta_dev.p + grp[0] : nullptr;
             void* args[] = {(void*)&one};
             void* kern = R.mixed ? (void*)k_dilu_bicgstab<float, DiluOne> : (void*)k_dilu_bicgstab<double, DiluOne>;
             CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kDiluThreads), args, 0, R.stream));
         } else {
             static thread_local DiluTab t;   // ~4 KB
             t.tab = R.dtab.p;
+            t.rtol_dev = R.capturing ? R.eta_dev.p : nullptr;
             make_map(t.mp, grp, [&](int k) { return C(k)->dl_cta; });
             for (size_t j = 0; j < grp.size(); j++) t.rtol[j] = eta[grp[j]];
             void* args[] = {(void*)&t};
@@ -970,7 +991,7 @@ int launch_linear(Runner& R, const std::vector<int>& all, const std::vector<doub
             KrylovOne one;
             one.Q = R.ktab_h[grp[0]];
             one.rtol = eta[grp[0]];
-            one.rtol_dev = R.capturing ? R.eta_dev.p : nullptr;
+            one.rtol_dev = R.capturing ? R.eta_dev.p + grp[0] : nullptr;
             one.lay = lay;
             void* args[] = {(void*)&one};
             void* kern = R.mixed ? krylov_kernel<float, KrylovOne>(R.stages) : krylov_kernel<double, KrylovOne>(R.stages);
@@ -979,6 +1000,7 @@ int launch_linear(Runner& R, const std::vector<int>& all, const std::vector<doub
             static thread_local KrylovTab t;   // ~4 KB: not on the stack of every caller
             int off = 0;
             t.tab = R.ktab.p;
+            t.rtol_dev = R.capturing ? R.eta_dev.p : nullptr;
             t.mp.n = (int)grp.size();
             for (size_t j = 0; j < grp.size(); j++) {
                 t.mp.boff[j] = off;
@@ -1178,6 +1200,8 @@ void reset_after_timeout(Runner& R, const std::vector<int>& sub) {
 // One time step of every instance (fe_sw2 level shift + fe_newton), the instances in
 // lockstep: each Newton phase is one launch over the instances still iterating, and each
 // instance follows exactly the decisions it takes alone.
+int ensure_batch_graphs(Runner& R, const std::vector<int>& all, Runner::BatchGraph** out);
+
 int runner_step(Runner& R, const double* dt, const double* const* series, sw2gpu_stats* stats, int* status) {
     const int K = (int)R.ctx.size();
     for (int k = 0; k < K; k++)
@@ -1191,9 +1215,19 @@ int runner_step(Runner& R, const double* dt, const double* const* series, sw2gpu
     if ((rc = runner_tables(R, 1))) return rc;
     std::vector<int> all(K);
     for (int k = 0; k < K; k++) all[k] = k;
-    if ((rc = launch_init(R, all))) return rc;
-    if ((rc = launch_resid(R, all))) return rc;
-    if ((rc = read_results(R, all))) return rc;
+    // a batch replaying from CUDA graphs: the step start and every Newton iteration in which all
+    // instances iterate are graph launches; iterations of a subset launch directly
+    Runner::BatchGraph* G = nullptr;
+    if (R.use_graphs && K > 1 && (rc = ensure_batch_graphs(R, all, &G))) return rc;
+    if (G) {
+        CK(cudaGraphLaunch(G->start, R.stream));
+        R.launches += G->kernels_start;
+        if ((rc = finish_results(R, all))) return rc;
+    } else {
+        if ((rc = launch_init(R, all))) return rc;
+        if ((rc = launch_resid(R, all))) return rc;
+        if ((rc = read_results(R, all))) return rc;
+    }
     std::vector<NState> ns(K);
     for (int k = 0; k < K; k++) newton_begin(R, k, ns[k]);
     for (;;) {
@@ -1201,7 +1235,20 @@ int runner_step(Runner& R, const double* dt, const double* const* series, sw2gpu
         for (int k = 0; k < K; k++)
             if (!ns[k].done) act.push_back(k);
         if (act.empty()) break;
-        if ((rc = newton_iteration(R, act, ns))) {
+        if (G && (int)act.size() == K) {
+            const std::vector<double> eta = newton_eta(R, act, ns);
+            for (int k = 0; k < K; k++) {
+                R.eta_h[k] = eta[k];
+                ns[k].old_l2 = ns[k].l2;
+            }
+            CK(cudaMemcpyAsync(R.eta_dev.p, R.eta_h, sizeof(double) * K, cudaMemcpyHostToDevice, R.stream));
+            CK(cudaGraphLaunch(G->newton, R.stream));
+            R.launches += G->kernels_newton;
+            rc = newton_finish(R, act, ns);
+        } else {
+            rc = newton_iteration(R, act, ns);
+        }
+        if (rc) {
             // a device wait that ran out ends the step like a failed one: every instance is
             // back at its old level (fe_sw2_init) and the caller may step again
             if (rc == SW2GPU_E_TIMEOUT) reset_after_timeout(R, all);
@@ -1281,6 +1328,50 @@ int capture_graph(Runner& R, cudaGraphExec_t* out, int* kernels, F body) {
     const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (ei != cudaSuccess) return fail(SW2GPU_E_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ei));
+    return 0;
+}
+
+// the batch graphs of the instances' current level arrangement, dt and launch variant
+// (captured when new; the three most recent are kept)
+int ensure_batch_graphs(Runner& R, const std::vector<int>& all, Runner::BatchGraph** out) {
+    std::vector<int> lv;
+    std::vector<double> dts;
+    for (auto* c : R.ctx) {
+        lv.push_back(c->lv[0]);
+        dts.push_back(c->dt);
+    }
+    for (auto& g : R.bgraphs)
+        if (g.lv == lv && g.dt == dts && g.jac_minb == R.jac_minb && g.stages == R.stages) {
+            *out = &g;
+            return 0;
+        }
+    if (R.bgraphs.size() >= 3) {
+        if (R.bgraphs.front().start) cudaGraphExecDestroy(R.bgraphs.front().start);
+        if (R.bgraphs.front().newton) cudaGraphExecDestroy(R.bgraphs.front().newton);
+        R.bgraphs.erase(R.bgraphs.begin());
+    }
+    Runner::BatchGraph g;
+    g.lv = lv;
+    g.dt = dts;
+    g.jac_minb = R.jac_minb;
+    g.stages = R.stages;
+    int rc = capture_graph(R, &g.start, &g.kernels_start, [&] {
+        int r = launch_init(R, all);
+        if (!r) r = launch_resid(R, all);
+        if (!r) r = enqueue_results(R);
+        return r;
+    });
+    if (!rc) rc = capture_graph(R, &g.newton, &g.kernels_newton, [&] {
+        // every Krylov launch reads its instance's tolerance from eta_dev
+        return newton_launch(R, all, std::vector<double>(all.size(), 0.0));
+    });
+    if (rc) {
+        if (g.start) cudaGraphExecDestroy(g.start);
+        if (g.newton) cudaGraphExecDestroy(g.newton);
+        return rc;
+    }
+    R.bgraphs.push_back(g);
+    *out = &R.bgraphs.back();
     return 0;
 }
 
@@ -2318,6 +2409,13 @@ int sw2gpu_batch_step(sw2gpu_batch* b, const double* dt, const double* const* se
     if (rc) return rc;
     for (int k = 0; k < K; k++)
         if (status[k] != SW2GPU_OK) return fail(status[k], "instance %d: step failed", k);
+    return SW2GPU_OK;
+}
+
+int sw2gpu_batch_set_graphs(sw2gpu_batch* b, int32_t enable) {
+    if (!b) return fail(SW2GPU_E_ARG, "null batch");
+    b->run->use_graphs = enable != 0;
+    if (!enable) b->run->drop_batch_graphs();
     return SW2GPU_OK;
 }
 

@@ -35,7 +35,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
            "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont",
            "sw2gpu_set_wait_limits", "sw2gpu_snapshot", "sw2gpu_elem_error", "sw2gpu_set_mass_tracking",
-           "sw2gpu_step_mass", "sw2gpu_set_wind", "sw2gpu_set_waves", "sw2gpu_remesh"]
+           "sw2gpu_step_mass", "sw2gpu_set_wind", "sw2gpu_set_waves", "sw2gpu_remesh", "sw2gpu_batch_set_graphs"]
 
 
 class SW2Error(RuntimeError):
@@ -91,6 +91,7 @@ def lib():
         L.sw2gpu_set_wind.argtypes = [vp, c_int32_p, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_set_waves.argtypes = [vp, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_remesh.argtypes = [vp, vp, vp]
+        L.sw2gpu_batch_set_graphs.argtypes = [vp, C.c_int32]
         L.sw2gpu_step_mass.argtypes = [vp, c_double_p, c_double_p]
         L.sw2gpu_set_variant.argtypes = [vp, C.c_int32, C.c_int32]
         L.sw2gpu_get_variant.argtypes = [vp, c_int32_p, c_int32_p]
@@ -373,6 +374,10 @@ class SW2Batch:
         h = C.c_void_p()
         _check(lib().sw2gpu_batch_create(arr, n, C.c_void_p(stream) if stream else None, C.byref(h)))
         self.h = h
+
+    def set_graphs(self, enable: bool = True):
+        """Replay the step start and the all-instance Newton iterations from CUDA graphs."""
+        _check(lib().sw2gpu_batch_set_graphs(self.h, 1 if enable else 0))
 
     def close(self):
         if getattr(self, "h", None):

@@ -305,6 +305,12 @@ typedef struct sw2gpu_batch sw2gpu_batch;
 int sw2gpu_batch_create(sw2gpu_ctx **ctxs, int32_t n, void *stream, sw2gpu_batch **out);
 int sw2gpu_batch_step(sw2gpu_batch *b, const double *dt, const double *const *series, sw2gpu_stats *stats);
 int sw2gpu_batch_destroy(sw2gpu_batch *b);
+/* Replay the batch's step start and every Newton iteration in which all instances iterate from
+ * CUDA graphs, captured per arrangement of the instances' time levels, dt and launch variant
+ * (the three most recent kept); iterations of a subset launch directly.  Each instance's Krylov
+ * tolerance is read from device memory.  Bitwise the same as direct stepping; worth it for
+ * batches of small meshes, whose steps are launch-bound. */
+int sw2gpu_batch_set_graphs(sw2gpu_batch *b, int32_t enable);
 
 /* Continuous batching (no counterpart in the reference, whose time loop runs one model).
  * Instances of uneven size join and leave an engine between ticks.  A tick starts a time

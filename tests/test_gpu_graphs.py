@@ -34,3 +34,38 @@ def test_graph_steps_equal_direct(precision, which):
     assert np.array_equal(wg, wd)
     for a, b in zip(sg, sd):
         assert np.array_equal(a, b)
+
+
+def _run_batch(models, precision, precond, graphs, dts):
+    from adhv8_kraken_b200.sw2 import SW2Batch
+    solvers = [SW2GPU(m, precision=precision, precond=precond) for m in models]
+    b = SW2Batch(solvers)
+    if graphs:
+        b.set_graphs(True)
+    stats = [b.step([d] * len(models)) for d in dts]
+    out = [[np.concatenate(g.get_state(lvl)) for lvl in range(3)] + [g.get_wd()] for g in solvers]
+    summ = [[(s["status"], s["newton_its"], s["linear_its"]) for s in st] for st in stats]
+    b.close()
+    for g in solvers:
+        g.close()
+    return out, summ
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,precond", [(capi.SW2GPU_FP64, capi.SW2GPU_PREC_BJACOBI),
+                                               (capi.SW2GPU_MIXED, capi.SW2GPU_PREC_BJACOBI),
+                                               (capi.SW2GPU_FP64, capi.SW2GPU_PREC_DILU)])
+def test_batch_graph_steps_equal_direct(precision, precond):
+    """sw2gpu_batch_set_graphs: a batch of uneven meshes replayed from CUDA graphs (all-instance
+    Newton iterations as graph launches, each instance's Krylov tolerance from device memory)
+    gives bitwise the results of direct launches, across level arrangements and a dt change."""
+    models = [meshgen.channel(nsteps=5),
+              meshgen.bumpy_basin(700, seed=11, size=2000.0, nsteps=5, dt=5.0, nbins=3, name="g1"),
+              meshgen.bumpy_basin(400, seed=12, size=1500.0, nsteps=5, dt=5.0, nbins=3, name="g2")]
+    dts = [5.0, 5.0, 2.5, 5.0, 5.0]
+    od, sd = _run_batch(models, precision, precond, False, dts)
+    og, sg = _run_batch(models, precision, precond, True, dts)
+    assert sg == sd
+    for a, b in zip(og, od):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
