@@ -659,6 +659,10 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
     serving = None
     if serve:
         serving = run_serving(serve[0], serve[1], args.serve_rate)
+        if args.serve_rates:   # the same requests at each arrival rate of the sweep
+            serving["sweep"] = [run_serving(serve[0], serve[1], float(r)) for r in args.serve_rates.split(",")]
+            for leg in serving["sweep"]:
+                leg.pop("workload", None)
 
     if rank != 0:
         return
@@ -714,6 +718,8 @@ def main():
     ap.add_argument("--c3-steps", type=int, default=50, help="config-3 time steps")
     ap.add_argument("--serve", type=int, default=24, help="serving-loop requests (0: skip the leg)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-rates", default="",
+                    help="comma-separated arrival rates (req/s) of an extra serving sweep, e.g. 5,10,20,50,100,200")
     ap.add_argument("--serve-horizon-scale", type=float, default=0.1,
                     help="horizons U{10..500} steps times this factor (1.0: the full horizons)")
     args = ap.parse_args()
