@@ -249,41 +249,6 @@ void stage_caps(const std::vector<int>& rp, int V, size_t esz, unsigned& a_cap, 
     c_cap = (unsigned)cm;
 }
 
-// Reverse Cuthill-McKee order of the nodes for the banded LU: breadth-first from a node of least
-// degree in every connected part, each node's unvisited neighbours taken by increasing degree, the
-// whole sequence reversed.  perm[i] = new position of node i; returns the half-bandwidth in nodes.
-int rcm_order(const std::vector<int>& rp, const std::vector<int>& col, int V, std::vector<int>& perm) {
-    std::vector<int> deg(V), start(V), order;
-    order.reserve(V);
-    for (int i = 0; i < V; i++) {
-        deg[i] = rp[i + 1] - rp[i];
-        start[i] = i;
-    }
-    std::stable_sort(start.begin(), start.end(), [&](int a, int b) { return deg[a] < deg[b]; });
-    std::vector<char> seen(V, 0);
-    size_t head = 0;
-    for (int s0 : start) {
-        if (seen[s0]) continue;
-        seen[s0] = 1;
-        order.push_back(s0);
-        while (head < order.size()) {
-            const int a = order[head++];
-            const size_t n0 = order.size();
-            for (int k = rp[a]; k < rp[a + 1]; k++)
-                if (!seen[col[k]]) {
-                    seen[col[k]] = 1;
-                    order.push_back(col[k]);
-                }
-            std::stable_sort(order.begin() + n0, order.end(), [&](int a2, int b2) { return deg[a2] < deg[b2]; });
-        }
-    }
-    perm.assign(V, 0);
-    for (int i = 0; i < V; i++) perm[order[V - 1 - i]] = i;
-    int bw = 0;
-    for (int i = 0; i < V; i++)
-        for (int k = rp[i]; k < rp[i + 1]; k++) bw = std::max(bw, std::abs(perm[i] - perm[col[k]]));
-    return bw;
-}
 // largest band the direct solve accepts (bytes of the band of the scaled system)
 constexpr size_t kBandMaxBytes = size_t(2) << 30;
 
@@ -1486,48 +1451,9 @@ const char* sw2gpu_last_error(void) { return g_err.c_str(); }
 // tiles, at most the co-resident grid.
 int build_dilu(sw2gpu_ctx* c, const std::vector<int>& rp, const std::vector<int>& col, cudaStream_t st) {
     const int V = c->V;
-    // smallest-last order: repeatedly take out a node of least remaining degree (the lowest
-    // index among equals); colouring in the reverse of that order needs few colours on planar
-    // meshes (5 on the benchmark basins, where largest-first needs 6)
-    std::vector<int> order;
-    order.reserve(V);
-    {
-        std::vector<int> deg(V);
-        std::vector<char> gone(V, 0);
-        std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, std::greater<std::pair<int, int>>> pq;
-        for (int n = 0; n < V; n++) {
-            deg[n] = rp[n + 1] - rp[n] - 1;
-            pq.push({deg[n], n});
-        }
-        while (!pq.empty()) {
-            const auto top = pq.top();
-            pq.pop();
-            const int n = top.second;
-            if (gone[n] || top.first != deg[n]) continue;
-            gone[n] = 1;
-            order.push_back(n);
-            for (int k = rp[n]; k < rp[n + 1]; k++) {
-                const int j = col[k];
-                if (j != n && !gone[j]) pq.push({--deg[j], j});
-            }
-        }
-        std::reverse(order.begin(), order.end());
-    }
-    std::vector<int> colour(V, -1);
-    int ncol = 0;
-    for (int n : order) {
-        unsigned used = 0;
-        for (int k = rp[n]; k < rp[n + 1]; k++) {
-            const int j = col[k];
-            if (j != n && colour[j] >= 0) used |= 1u << colour[j];
-        }
-        int cc = 0;
-        while (cc < kMaxColours && ((used >> cc) & 1u)) cc++;
-        if (cc >= kMaxColours)
-            return fail(SW2GPU_E_ARG, "the node graph needs more than %d colours for the D-ILU order", kMaxColours);
-        colour[n] = cc;
-        ncol = std::max(ncol, cc + 1);
-    }
+    std::vector<int> colour;
+    const int ncol = smallest_last_colouring(rp, col, V, kMaxColours, colour);
+    if (ncol < 0) return fail(SW2GPU_E_ARG, "the node graph needs more than %d colours for the D-ILU order", kMaxColours);
     // new rows: colour q occupies pst[q] .. pst[q+1]-1, padded to whole 32-row tiles, its
     // cnt[q] real rows first (natural order); padding rows have old = -1
     std::vector<int> cnt(ncol, 0), pst(ncol + 1, 0);

@@ -1,9 +1,13 @@
-"""Mesh tables after an adaption (adhv8_kraken_b200/csrc/sw2_tables.h, compiled for the host):
+"""Mesh tables and node orders (adhv8_kraken_b200/csrc/sw2_tables.h, compiled for the host).
+
+After an adaption:
 the incremental update that sw2gpu_remesh uses -- rebuilding only the pattern rows of nodes a
 changed, new or removed element or edge touches -- gives exactly the tables of a build from
 scratch (BCSR pattern, per-block rows and diagonal positions, the reference-order element-slot
 gather lists and the node residual-slot lists), on refinements, edge flips, dropped trailing
-triangles and changed boundary edges; a mesh that lost nodes is reported for a full build."""
+triangles and changed boundary edges; a mesh that lost nodes is reported for a full build.  The
+node orders of the solvers: the block D-ILU colouring is proper, the banded solve's reverse
+Cuthill-McKee order a permutation with a narrow band."""
 import ctypes as C
 import os
 import shutil
@@ -32,6 +36,31 @@ extern "C" int tables_compare(int Vo, int To, int Eo, const int* tri_o, const in
         a.blk_src != b.blk_src || a.slot_ptr != b.slot_ptr || a.slot_idx != b.slot_idx)
         return 1;
     return 0;
+}
+// the D-ILU colouring: 0 when no block of the pattern joins two nodes of one colour
+extern "C" int colour_check(int V, int T, int E, const int* tri, const int* edg, int* ncol) {
+    sw2::MeshTables t;
+    if (sw2::build_tables(V, T, E, tri, edg, t)) return 10;
+    std::vector<int> colour;
+    *ncol = sw2::smallest_last_colouring(t.rp, t.col, V, 16, colour);
+    if (*ncol < 0) return 20;
+    for (int n = 0; n < V; n++)
+        for (int k = t.rp[n]; k < t.rp[n + 1]; k++)
+            if (t.col[k] != n && colour[t.col[k]] == colour[n]) return 1;
+    return 0;
+}
+// the banded solve's reverse Cuthill-McKee order: its half-bandwidth, -1 if perm is not a permutation
+extern "C" int rcm_check(int V, int T, int E, const int* tri, const int* edg) {
+    sw2::MeshTables t;
+    if (sw2::build_tables(V, T, E, tri, edg, t)) return -2;
+    std::vector<int> perm;
+    const int bw = sw2::rcm_order(t.rp, t.col, V, perm);
+    std::vector<char> seen(V, 0);
+    for (int p : perm) {
+        if (p < 0 || p >= V || seen[p]) return -1;
+        seen[p] = 1;
+    }
+    return bw;
 }
 '''
 
@@ -123,3 +152,37 @@ def test_mesh_that_lost_nodes_is_rebuilt_from_scratch(tables):
     m1 = channel_model()
     rc, _ = _compare(tables, m0, m1.tri, m1.edges, m1.nnodes)
     assert rc == 20
+
+
+def test_dilu_colouring_is_proper_and_needs_five_colours(tables):
+    """Smallest-last greedy colouring (block D-ILU order): no two neighbours share a colour; the
+    benchmark generator's basin needs 5 colours."""
+    import math
+    from adhv8_kraken_b200 import meshgen
+    for m in (channel_model(), basin_model(),
+              meshgen.bumpy_basin(10000, seed=2024, size=20000.0 * math.sqrt(10000 / 5e5), nsteps=1, dt=5.0, name="b")):
+        tri, e = np.ascontiguousarray(m.tri, np.int32), np.ascontiguousarray(m.edges, np.int32).reshape(-1, 2)
+        n = C.c_int(0)
+        assert tables.colour_check(m.nnodes, len(tri), len(e), _ip(tri), _ip(e), C.byref(n)) == 0
+        assert 3 <= n.value <= 6, (m.name, n.value)
+    assert n.value == 5
+
+
+def test_rcm_order_is_a_permutation_with_a_narrow_band(tables):
+    """Reverse Cuthill-McKee order of the banded exact solve: a permutation whose half-bandwidth
+    is within 10 % of scipy's reverse Cuthill-McKee on the same graph."""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import reverse_cuthill_mckee
+    for m in (channel_model(), basin_model()):
+        tri, e = np.ascontiguousarray(m.tri, np.int32), np.ascontiguousarray(m.edges, np.int32).reshape(-1, 2)
+        bw = tables.rcm_check(m.nnodes, len(tri), len(e), _ip(tri), _ip(e))
+        assert bw > 0
+        r = np.concatenate([tri[:, a] for a in range(3) for b in range(3)])
+        c = np.concatenate([tri[:, b] for a in range(3) for b in range(3)])
+        G = sp.csr_matrix((np.ones(len(r)), (r, c)), shape=(m.nnodes, m.nnodes))
+        order = reverse_cuthill_mckee(G, symmetric_mode=True)
+        pos = np.empty(m.nnodes, int)
+        pos[order] = np.arange(m.nnodes)
+        coo = G.tocoo()
+        ref = int(np.abs(pos[coo.row] - pos[coo.col]).max())
+        assert bw <= 1.1 * ref + 1, (m.name, bw, ref)
