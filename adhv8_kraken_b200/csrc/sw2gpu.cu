@@ -167,11 +167,14 @@ struct sw2gpu_ctx {
     DBuf<unsigned> ncounter;
     int krylov_grid = 0;            // virtual CTAs of the Krylov solve (its partial structure)
     // Krylov iterations expected of the next solve, and those seen at each Newton iteration
-    // of the last step (the first Newton iteration of a step needs the tightest solve): they
-    // weight the instance's CTA share in a batch
+    // of the last step (the first Newton iteration of a step needs the tightest solve) and of
+    // the step before (its_snap holds its_at as the current step began, its_prev as the last one
+    // began): they weight the instance's CTA share in a batch
     int pred_its = 20;
     size_t bytes = 0;               // device memory of the context
     int its_at[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int its_snap[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int its_prev[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     unsigned a_cap = 0, c_cap = 0;  // largest tile block / column-index ranges (staged sweeps)
     // autotuned launch variants (sw2gpu_autotune): they change speed, never results
     int tune_jac_minb = 2;          // wet-Jacobian CTAs per SM the register budget is cut for
@@ -791,24 +794,23 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
 // iterations of the instance's last solve), at least one, at most its virtual CTAs, so that
 // the instances of a launch finish together
 std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub) {
+    // A launch lasts as long as its instance with the most work per CTA, so the shares minimise
+    // that maximum: every instance starts with one CTA, and each further CTA goes to the instance
+    // whose predicted work per CTA is then the largest (ties to the lower index), up to its
+    // virtual grid.  (Proportional shares rounded down left instances that should have 1.7 CTAs
+    // with one.)  The shares set only the speed: the results of an instance depend on its
+    // virtual grid alone.
     auto work = [&](const sw2gpu_ctx* c) { return (double)c->nnzb * (double)std::max(c->pred_its, 1); };
-    double wsum = 0.0;
-    for (int k : sub) wsum += work(R.ctx[k]);
-    std::vector<int> P(sub.size());
-    long long tot = 0;
-    for (size_t j = 0; j < sub.size(); j++) {
+    const int n = (int)sub.size();
+    std::vector<int> P(n, 1);
+    std::priority_queue<std::pair<double, int>> pq;   // (work per CTA, -j)
+    for (int j = 0; j < n; j++)
+        if (R.ctx[sub[j]]->krylov_grid > 1) pq.push({work(R.ctx[sub[j]]), -j});
+    for (int left = R.capacity - n; left > 0 && !pq.empty(); left--) {
+        const int j = -pq.top().second;
+        pq.pop();
         const sw2gpu_ctx* c = R.ctx[sub[j]];
-        const int want = (int)std::floor(R.capacity * work(c) / std::max(wsum, 1.0));
-        P[j] = std::max(1, std::min(c->krylov_grid, want));
-        tot += P[j];
-    }
-    while (tot > R.capacity) {   // trim the largest shares
-        size_t jm = 0;
-        for (size_t j = 1; j < P.size(); j++)
-            if (P[j] > P[jm]) jm = j;
-        if (P[jm] <= 1) break;
-        P[jm]--;
-        tot--;
+        if (++P[j] < c->krylov_grid) pq.push({work(c) / P[j], -j});
     }
     return P;
 }
@@ -1030,7 +1032,11 @@ std::vector<double> newton_eta(Runner& R, const std::vector<int>& act, const std
         sw2gpu_ctx* c = R.ctx[k];
         const sw2gpu_params& p = c->p;
         eta[k] = std::min(1e-5, std::max(p.lin_rtol, kEtaNtl * p.tol_nonlin / std::max(ns[k].rmax, 1e-300)));
-        const int seen = c->its_at[std::min(ns[k].it, 7)];
+        // the larger count of the last two steps at this Newton iteration: a launch lasts as
+        // long as its most underestimated instance, and one atypical solve (a line-search cut,
+        // an extra iteration) would otherwise set the next prediction far too low
+        const int i = std::min(ns[k].it, 7);
+        const int seen = std::max(c->its_at[i], c->its_prev[i]);
         if (seen > 0) c->pred_its = seen;
     }
     return eta;
@@ -1124,6 +1130,10 @@ int newton_status(const NState& n, const sw2gpu_params& p) {
 int step_begin(Runner& R, int k, double dt, const double* series) {
     sw2gpu_ctx* c = R.ctx[k];
     c->dt = dt;
+    for (int i = 0; i < 8; i++) {
+        c->its_prev[i] = c->its_snap[i];
+        c->its_snap[i] = c->its_at[i];
+    }
     const int o2 = c->lv[2];
     c->lv[2] = c->lv[1];
     c->lv[1] = c->lv[0];
