@@ -312,3 +312,87 @@ def ensemble_member(seed: int, tri_lo: float = 5e3, tri_hi: float = 2e5, nsteps:
     size = 20000.0 * math.sqrt(T / 1.0e6)
     return bumpy_basin(int(T / 2), sub, size=size, n_median=n_med, q_peak=q_peak, dt=dt,
                        nsteps=nsteps, name=f"{name}{seed}")
+
+
+# ---------------------------------------------------------------------------------------------
+# constituent transport workloads (fe_transport after every flow step)
+
+def _const_series(m: SW2Model, value: float) -> int:
+    """Appends a constant series to the model; returns its id."""
+    t_end = m.t0 + (m.nsteps + 10) * m.dt
+    m.series = list(m.series) + [Series(np.array([m.t0, t_end]), np.array([value, value]))]
+    return len(m.series) - 1
+
+
+def channel_transport(nsteps: int = 6, nx: int = 100, ny: int = 20) -> SW2Model:
+    """The channel carrying a constituent (reference concentration 1): a Gaussian patch at
+    x = 300 m drifting east, the west column of nodes held at 2 (DB TRN node string) and
+    diffusion d_m = 0.5 m^2/s."""
+    from .model import Constituent
+    m = channel(nx=nx, ny=ny, nsteps=nsteps, name="trn_channel")
+    ser = _const_series(m, 2.0)
+    m.strings = list(m.strings) + [StringSpec("node")]
+    sid = len(m.strings) - 1
+    node_string = m.node_string.copy()
+    node_string[m.x == 0.0] = sid
+    m.node_string = node_string
+    m.constituents = [Constituent(ref_conc=1.0, diffusion=[0.5], node_bc={sid: ser},
+                                  c0=np.exp(-((m.x - 300.0) / 100.0) ** 2))]
+    return m
+
+
+def basin_transport(nsteps: int = 8, nbins: int = 3) -> SW2Model:
+    """The small wet/dry basin carrying two constituents through its fronts: the first
+    (reference concentration 2, diffusion 0.1 / 1 / 3 m^2/s by material) enters with the NB VEL
+    inflow at 3 (NB TRN, 1.5 in the reference's normalised units) and leaves through the NB OTW
+    tailwater, which also brings in 0.25 where it flows back; the second (reference 1, no
+    diffusion, no boundary condition) starts as a smooth field."""
+    from .model import Constituent
+    m = bumpy_basin(700, seed=11, size=2000.0, nsteps=nsteps, dt=5.0, nbins=nbins, name="trn_basin")
+    s_in, s_out = _const_series(m, 3.0), _const_series(m, 0.5)
+    e_in, e_out = nbins, nbins + 1
+    c0 = 0.5 + 0.4 * np.sin(m.x / 300.0) * np.cos(m.y / 250.0)
+    m.constituents = [Constituent(ref_conc=2.0, diffusion=[0.1, 1.0, 3.0][:nbins], edge_bc={e_in: s_in, e_out: s_out},
+                                  c0=c0),
+                      Constituent(ref_conc=1.0, c0=1.0 + 0.5 * np.cos(m.x / 400.0))]
+    return m
+
+
+def terms_transport(nsteps: int = 6) -> SW2Model:
+    """The all-terms basin (temporal alpha 0.5; EVS with Coriolis and EEV modes 1-3: transport
+    then takes its diffusion from the estimated eddy viscosity) with one constituent entering
+    at the inflow (NB TRN) and diffusion 2 m^2/s on the EVS material."""
+    from .model import Constituent
+    m = basin_all_terms(nsteps=nsteps)
+    m.name = "trn_terms"
+    s_in = _const_series(m, 1.0)
+    nmat = len(m.materials)
+    m.constituents = [Constituent(ref_conc=1.0, diffusion=[2.0, 0.0, 0.0, 0.0], edge_bc={nmat: s_in},
+                                  c0=0.2 + 0.1 * np.cos(m.y / 200.0))]
+    return m
+
+
+def outflow_transport(nsteps: int = 6) -> SW2Model:
+    """The channel with a free outflow (NB OF) east and a constituent entering with the NB VEL
+    inflow west at 0.8 (NB TRN), from a linear initial profile."""
+    from .model import Constituent
+    m = channel_outflow(nsteps=nsteps)
+    m.name = "trn_outflow"
+    s_in = _const_series(m, 0.8)
+    m.constituents = [Constituent(ref_conc=1.0, diffusion=[1.0], edge_bc={1: s_in}, c0=m.x / 1000.0)]
+    return m
+
+
+def salt_transport(nsteps: int = 6) -> SW2Model:
+    """Known answer of the reference's own angle_salt check (write_testcase_error_salt,
+    src/initio/test_cases.c:1506-1535: |c - 17.5| <= 1e-6 everywhere): the channel with a
+    constituent at 17.5 everywhere, entering at 17.5 through the inflow and the tailwater.  A
+    uniform concentration stays uniform only if the transport residual is consistent with the
+    flow's discrete continuity equation, which the side output elem_rhs_dacont_extra_terms
+    provides; it holds where the flow is wet everywhere."""
+    from .model import Constituent
+    m = channel(nsteps=nsteps, name="trn_salt")
+    s = _const_series(m, 17.5)
+    m.constituents = [Constituent(ref_conc=1.0, diffusion=[1.0], edge_bc={1: s, 2: s},
+                                  c0=np.full(m.nnodes, 17.5))]
+    return m

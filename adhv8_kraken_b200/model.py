@@ -22,7 +22,7 @@ from __future__ import annotations
 import dataclasses
 import math
 import os
-from typing import List, Optional, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -32,6 +32,8 @@ UNSET_INT = -3              # define.h:448
 UNSET_FLT = -9999999.9      # define.h:449
 BCT_PRS_DIR = 7             # define.h:381
 BCT_VEL_DIR = 8             # define.h:382
+BCT_DIR = 1                 # define.h:375  (DB TRN, a constituent's held concentration)
+BCT_NEU = 3                 # define.h:377  (NB TRN, a constituent's inflow concentration)
 BCT_PRS_NEU = 9             # define.h:383  (NB OTW, tailwater)
 BCT_VEL_NEU = 10            # define.h:384  (NB VEL, unit discharge)
 BCT_WATER_SOURCE = 12       # define.h:386
@@ -101,6 +103,24 @@ class StringSpec:
 
 
 @dataclasses.dataclass
+class Constituent:
+    """A general transported constituent (``CN CON``, src/initio/read_bc_CN.c:14-18), carried by
+    the 2D flow (fe_transport, src/fe/transport/fe_transport.c:31-113).
+
+    ``ref_conc`` is the reference concentration property[0]: boundary values are divided by it
+    (fe_transport_init.c:47, fe_2d_transport_boundary_resid.c:74) while the hot-start values are
+    taken as given (ssw.c, the ``ICON`` data set).  ``diffusion[m]`` is material m's ``MP DF``
+    coefficient d_m (0 when absent).  ``node_bc`` maps a node string to the series it holds the
+    concentration at (``DB TRN``, BCT_DIR); ``edge_bc`` an edge string to the series of the
+    concentration of the water that enters through it (``NB TRN``, BCT_NEU)."""
+    ref_conc: float = 1.0
+    diffusion: Sequence[float] = ()
+    node_bc: Dict[int, int] = dataclasses.field(default_factory=dict)
+    edge_bc: Dict[int, int] = dataclasses.field(default_factory=dict)
+    c0: Optional[np.ndarray] = None                  # initial concentration (None: 0)
+
+
+@dataclasses.dataclass
 class Params:
     """Model and solver parameters (defaults: src/structs/smodel_defaults.c:130-160)."""
     gravity: float = 9.8
@@ -139,6 +159,7 @@ class SW2Model:
     nsteps: int = 1
     t0: float = 0.0
     name: str = "sw2"
+    constituents: List[Constituent] = dataclasses.field(default_factory=list)
 
     # ------------------------------------------------------------------ sizes
     @property
@@ -188,6 +209,28 @@ class SW2Model:
                 h[nodes] = self.series[st.iu0].value_at(self.t0)
         return h, u, v
 
+    def transport_tables(self):
+        """The constituents as the transport interface takes them: reference concentrations
+        [ntrn], MP DF diffusion [ntrn, nmats], per string the constituent's bc flag (0, BCT_DIR
+        for DB TRN, BCT_NEU for NB TRN) and its series [ntrn, nstrings], and the initial
+        concentrations [ntrn, nnodes] (ICON, 0 when absent)."""
+        n, M, S, V = len(self.constituents), len(self.materials), len(self.strings), self.nnodes
+        refc = np.array([c.ref_conc for c in self.constituents], dtype=np.float64)
+        dm = np.zeros((n, M))
+        bc = np.zeros((n, S), np.int32)
+        ser = np.full((n, S), -1, np.int32)
+        c0 = np.zeros((n, V))
+        for k, con in enumerate(self.constituents):
+            for m in range(min(M, len(con.diffusion))):
+                dm[k, m] = con.diffusion[m]
+            for s_id, sr in con.node_bc.items():
+                bc[k, s_id], ser[k, s_id] = BCT_DIR, sr
+            for s_id, sr in con.edge_bc.items():
+                bc[k, s_id], ser[k, s_id] = BCT_NEU, sr
+            if con.c0 is not None:
+                c0[k] = con.c0
+        return refc, dm, bc, ser, c0
+
     def series_values(self, t1: float, t2: float) -> np.ndarray:
         """Step-averaged value of every BC series over [t1, t2]."""
         return np.array([s.value_avg(t1, t2) for s in self.series], dtype=np.float64)
@@ -218,7 +261,7 @@ class SW2Model:
         tf = self.t0 + nsteps * self.dt
         with open(base + ".bc", "w") as f:
             w = f.write
-            w("OP SW2\nOP TRN 0\n")
+            w(f"OP SW2\nOP TRN {len(self.constituents)}\n")
             w(f"OP BLK {p.nblock}\nOP PRE 1\nOP INC 40\n")
             w(f"OP TEM {_f(p.tau_temporal)}\nOP TPG {_f(p.tau_pg)}\n")
             w(f"IP NTL {_f(p.tol_nonlin)}\n")
@@ -235,6 +278,11 @@ class SW2Model:
                     w(f"MP EVS {m + 1} {_f(xx)} {_f(yy)} {_f(xy)}\n")
                 if mat.coriolis != 0.0:
                     w(f"MP COR {m + 1} {_f(mat.coriolis)}\n")
+            for k, con in enumerate(self.constituents):          # read_bc_CN.c:14-18, read_bc_MP.c:180-184
+                w(f"CN CON {k + 1} {_f(con.ref_conc)}\n")
+                for m in range(nmat):
+                    dm = con.diffusion[m] if m < len(con.diffusion) else 0.0
+                    w(f"MP DF {m + 1} {k + 1} {_f(dm)}\n")
             if p.drying_limit > 0:
                 w(f"MP DTL {_f(p.drying_limit)}\n")
             w(f"MP G {_f(p.gravity)}\nMP RHO {_f(p.density)}\nMP MU {_f(p.viscosity)}\nMP MUC {_f(p.manning_units)}\n")
@@ -270,6 +318,11 @@ class SW2Model:
                         w(f"NB OF {s_id + 1}\n")
                     else:
                         raise ValueError(f"unsupported edge bc flag {s.bc_flag}")
+            for k, con in enumerate(self.constituents):          # read_bc_DB.c:59-65, read_bc_NB.c:119-125
+                for s_id, ser in sorted(con.node_bc.items()):
+                    w(f"DB TRN {s_id + 1} {k + 1} {ser + 1}\n")
+                for s_id, ser in sorted(con.edge_bc.items()):
+                    w(f"NB TRN {s_id + 1} {k + 1} {ser + 1}\n")
             for (a, b), s_id in zip(self.edges, self.edge_string):
                 w(f"EGS {a + 1} {b + 1} {s_id + 1}\n")
             for i in np.nonzero(self.node_string >= 0)[0]:
@@ -287,6 +340,14 @@ class SW2Model:
             for a, b in zip(self.u0, self.v0):
                 f.write(f"{_f(float(a))} {_f(float(b))} 0.0\n")
             f.write("ENDDS\n")
+            for k, con in enumerate(self.constituents):          # ssw.c: NAME ICON <id>
+                if con.c0 is None:
+                    continue
+                f.write(f'DATASET\nOBJTYPE "mesh2d"\nBEGSCL\nND {self.nnodes}\nNC {T}\nNAME "icon" {k + 1}\n')
+                f.write(f"TIMEUNITS seconds\nTS 0 {_f(self.t0)}\n")
+                for v in con.c0:
+                    f.write(f"{_f(float(v))}\n")
+                f.write("ENDDS\n")
         return base
 
 

@@ -65,6 +65,20 @@ def lib():
         L.orc_grid_mass.restype = C.c_double
         L.orc_mass_flux.argtypes = [C.c_void_p, C.c_double, C.c_double, c_double_p]
         L.orc_mass_flux.restype = C.c_double
+        L.orc_trn_setup.argtypes = [C.c_void_p, C.c_int, c_double_p, c_double_p, c_int32_p, c_int32_p]
+        L.orc_trn_setup.restype = C.c_int
+        L.orc_trn_set_conc.argtypes = [C.c_void_p, C.c_int, C.c_int, c_double_p]
+        L.orc_trn_get_conc.argtypes = [C.c_void_p, C.c_int, C.c_int, c_double_p]
+        L.orc_set_dacont.argtypes = [C.c_void_p, c_double_p]
+        L.orc_trn_get_bcmask.argtypes = [C.c_void_p, c_int32_p]
+        L.orc_trn_init.argtypes = [C.c_void_p, C.c_int]
+        L.orc_trn_resid.argtypes = [C.c_void_p, C.c_int, c_double_p]
+        L.orc_trn_load.argtypes = [C.c_void_p, C.c_int]
+        L.orc_trn_get_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
+        L.orc_trn_step.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_trn_step.restype = C.c_int
+        for name in ("orc_trn_body_resid", "orc_trn_edge_resid"):
+            getattr(L, name).argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, c_double_p]
         _lib = L
     return _lib
 
@@ -94,6 +108,16 @@ class Oracle:
         h0, u0, v0 = model.initial_state()
         for level in range(3):
             self.set_state(level, h0, u0, v0)
+        self.ntrn = len(model.constituents)
+        if self.ntrn:
+            refc, dm, bc, ser, c0 = model.transport_tables()
+            self._trn = (refc, dm, bc, ser)     # kept alive: the C side copies them anyway
+            if L.orc_trn_setup(self.h, self.ntrn, _dp(refc), _dp(np.ascontiguousarray(dm)),
+                               _ip(np.ascontiguousarray(bc)), _ip(np.ascontiguousarray(ser))):
+                raise ValueError("oracle rejected the constituents")
+            for k in range(self.ntrn):          # the hot start's old and older levels (ssw.c)
+                for level in range(3):
+                    self.set_conc(k, level, c0[k])
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -225,3 +249,60 @@ class Oracle:
         if rc == 0:
             self.t = t + dt
         return st.as_dict()
+
+    # ------------------------------------------------------------------ transport
+    def set_conc(self, itrn, level, c):
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        lib().orc_trn_set_conc(C.c_void_p(self.h), itrn, level, _dp(c))
+
+    def get_conc(self, itrn, level=0):
+        c = np.zeros(self.V)
+        lib().orc_trn_get_conc(C.c_void_p(self.h), itrn, level, _dp(c))
+        return c
+
+    def set_dacont(self, dac):
+        """elem_rhs_dacont_extra_terms as [3, T] (vertex-major, as dacont() returns it)."""
+        d = np.ascontiguousarray(dac, dtype=np.float64).reshape(-1)
+        lib().orc_set_dacont(C.c_void_p(self.h), _dp(d))
+
+    def trn_init(self, itrn):
+        """fe_transport_init: the current concentration from the old one, dry nodes 0, Dirichlet
+        values; returns bc_mask."""
+        lib().orc_trn_init(C.c_void_p(self.h), itrn)
+        m = np.zeros(self.V, np.int32)
+        lib().orc_trn_get_bcmask(C.c_void_p(self.h), _ip(m))
+        return m
+
+    def trn_resid(self, itrn):
+        r = np.zeros(self.V)
+        lib().orc_trn_resid(C.c_void_p(self.h), itrn, _dp(r))
+        return r
+
+    def trn_load(self, itrn):
+        """Scalar FD Jacobian over the pattern (sorted columns) and the residual it goes with."""
+        lib().orc_trn_load(C.c_void_p(self.h), itrn)
+        val, r = np.zeros(self.nnzb), np.zeros(self.V)
+        lib().orc_trn_get_matrix(C.c_void_p(self.h), _dp(val), _dp(r))
+        return val, r
+
+    def transport_step(self):
+        """fe_transport after an accepted flow step: every constituent in order; returns the
+        stats dicts (stops at the first failure, as the reference does)."""
+        out = []
+        for k in range(self.ntrn):
+            st = Stats()
+            rc = lib().orc_trn_step(C.c_void_p(self.h), k, C.byref(st))
+            out.append(st.as_dict())
+            if rc:
+                break
+        return out
+
+    def trn_body_resid(self, itrn, ie, eps=0.0, pnode=-1, psign=1):
+        out = np.zeros(3)
+        lib().orc_trn_body_resid(C.c_void_p(self.h), itrn, ie, eps, pnode, psign, _dp(out))
+        return out
+
+    def trn_edge_resid(self, itrn, ie, eps=0.0, pnode=-1, psign=1):
+        out = np.zeros(2)
+        lib().orc_trn_edge_resid(C.c_void_p(self.h), itrn, ie, eps, pnode, psign, _dp(out))
+        return out

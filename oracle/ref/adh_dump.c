@@ -1,9 +1,9 @@
 /* Observation harness for the reference AdH executable (test infrastructure only).
  *
  * The reference's own objects are linked unmodified; the linker option
- * ``--wrap=fe_main --wrap=fe_sw2_load`` routes the calls made by the time loop
- * (src/main/adh_func.c:549) and by the Newton driver (src/fe/fe_newton.c:454)
- * through the two functions below, which call the originals and then append
+ * ``--wrap=fe_main --wrap=fe_sw2_load --wrap=fe_transport_load`` routes the calls made by the
+ * time loop (src/main/adh_func.c:549) and by the Newton driver (src/fe/fe_newton.c:454)
+ * through the functions below, which call the originals and then append
  * full-precision records to the binary file named by the environment variable
  * ADH_DUMP:
  *
@@ -25,6 +25,13 @@
  *            "dacont"): the adaption error indicator fe_main computed for the step
  *            (ssw_2d_calculate_elem_error, src/structs/ssw_2d.c:424-500), grid->elem_error
  *            per element and its nodal average sw->error.
+ *   "con"    after every accepted step of a model with constituents (after the records
+ *            above): each constituent's concentration array, constituent by constituent;
+ *   "tload"  for the first ADH_DUMP_TLOADS calls of fe_transport_load (the transport Newton's
+ *            Jacobian, src/fe/transport/fe_transport_load.c:41): the constituent, t_prev and
+ *            dt, the three concentration levels, the flow's three levels, wd_flag, the side
+ *            output elem_rhs_dacont_extra_terms, bc_mask, then the residual vector, the scalar
+ *            diagonal and every off-diagonal SPARSE_VECT row (one value per entry).
  *
  * Record layout: char tag[8]; int32 kind (0 = f64, 1 = i32); int64 count; data.
  */
@@ -33,6 +40,7 @@
 
 int __real_fe_main(SSUPER_MODEL *sm);
 void __real_fe_sw2_load(SSUPER_MODEL *sm, int imod);
+void __real_fe_transport_load(SSUPER_MODEL *sm, int imod);
 /* the reference's mass diagnostics (src/tools/tl_grid_mass.c:20, :102); their prototypes are
  * commented out in its headers (src/include/fnctn.h:176-178) */
 double tl_find_grid_mass_elem2d(double density, STR_VALUE *str, SSERIES *series_head, double *depth, SGRID *grid,
@@ -43,6 +51,7 @@ double tl_find_grid_mass_error_elem2d(double density, double *depth, SVECT2D *ve
 
 static FILE *dump_fp = NULL;
 static int dump_loads_left = -1;
+static int dump_tloads_left = -1;
 static int attempts = 0;
 static int it_mark = 0;
 static double solve_seconds = 0.0;   /* fe_main wall time since the last accepted step */
@@ -65,6 +74,8 @@ static void dump_open(void) {
     dump_fp = fopen(path, "wb");
     const char *nl = getenv("ADH_DUMP_LOADS");
     dump_loads_left = nl ? atoi(nl) : 0;
+    const char *nt = getenv("ADH_DUMP_TLOADS");
+    dump_tloads_left = nt ? atoi(nt) : 0;
     dump_mass = getenv("ADH_DUMP_MASS") != NULL;
     dump_dacont = getenv("ADH_DUMP_DACONT") != NULL;
     dump_error = getenv("ADH_DUMP_ERROR") != NULL;
@@ -155,6 +166,10 @@ int __wrap_fe_main(SSUPER_MODEL *sm) {
             put_f64("elemerr", mod->grid->elem_error, mod->grid->nelems2d);
             put_f64("nodeerr", mod->sw->d2->error, n);
         }
+        {
+            int k;
+            for (k = 0; k < mod->ntransport; k++) put_f64("con", mod->con[k].concentration, n);
+        }
         fflush(dump_fp);
         attempts = 0;
         solve_seconds = 0.0;
@@ -200,5 +215,56 @@ void __wrap_fe_sw2_load(SSUPER_MODEL *sm, int imod) {
         free(vals);
         fflush(dump_fp);
         dump_loads_left--;
+    }
+}
+
+void __wrap_fe_transport_load(SSUPER_MODEL *sm, int imod) {
+    dump_open();
+    if (dump_fp != NULL && dump_tloads_left > 0) {
+        SMODEL *mod = &(sm->submodel[imod]);
+        SCON *con = &(mod->con[mod->itrns]);
+        int n = mod->grid->nnodes, T = mod->grid->nelems2d, i, e;
+        double hdr[3];
+        hdr[0] = (double) mod->itrns;
+        hdr[1] = mod->t_prev;
+        hdr[2] = mod->dt;
+        put_f64("tload", hdr, 3);
+        put_f64("c", con->concentration, n);
+        put_f64("c1", con->old_concentration, n);
+        put_f64("c2", con->older_concentration, n);
+        put_state("h", "u", "v", mod->sw->d2->head, mod->sw->d2->vel, n);
+        put_state("h1", "u1", "v1", mod->sw->d2->old_head, mod->sw->d2->old_vel, n);
+        put_state("h2", "u2", "v2", mod->sw->d2->older_head, mod->sw->d2->older_vel, n);
+        put_i32("wd", mod->grid->wd_flag, T);
+        double *d = (double *) malloc(sizeof(double) * 3 * (size_t) (T ? T : 1));
+        for (i = 0; i < 3; i++)
+            for (e = 0; e < T; e++) d[(size_t) i * T + e] = mod->sw->d2->elem_rhs_dacont_extra_terms[i][e];
+        put_f64("dacont", d, 3L * T);
+        free(d);
+        put_i32("bcmask", mod->bc_mask, n);
+    }
+    __real_fe_transport_load(sm, imod);
+    if (dump_fp != NULL && dump_tloads_left > 0) {
+        SMODEL *mod = &(sm->submodel[imod]);
+        int n = mod->grid->nnodes, i, nnz = 0, k = 0;
+        put_f64("resid", sm->residual, n);
+        put_f64("diag", sm->diagonal, n);
+        int *rowsz = (int *) malloc(sizeof(int) * n);
+        for (i = 0; i < n; i++) { rowsz[i] = sm->matrix[i].size; nnz += rowsz[i]; }
+        int *cols = (int *) malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+        double *vals = (double *) malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+        for (i = 0; i < n; i++) {
+            memcpy(cols + k, sm->matrix[i].index, sizeof(int) * rowsz[i]);
+            memcpy(vals + k, sm->matrix[i].value, sizeof(double) * rowsz[i]);
+            k += rowsz[i];
+        }
+        put_i32("rowsz", rowsz, n);
+        put_i32("cols", cols, nnz);
+        put_f64("vals", vals, nnz);
+        free(rowsz);
+        free(cols);
+        free(vals);
+        fflush(dump_fp);
+        dump_tloads_left--;
     }
 }

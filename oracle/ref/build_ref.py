@@ -21,7 +21,7 @@ of the reference tree and its build system is not used; the recipe is:
    are compiled with ``gcc -O2 -fcommon``; units that only serve MPI, PETSc,
    groundwater, sediment coupling or ADCIRC winds are left out.
 3. The objects are linked with the observation harness ``adh_dump.c`` and
-   ``--wrap=fe_main --wrap=fe_sw2_load`` into ``oracle/_ref/adh_dump``.
+   ``--wrap=fe_main --wrap=fe_sw2_load --wrap=fe_transport_load`` into ``oracle/_ref/adh_dump``.
 4. The same objects, the same harness and the drop-in binding of the B200 library
    (``adhv8_kraken_b200/adapter/fe_sw2_solve_gpu.c``, compiled against the reference's own
    headers) are linked with ``--wrap=fe_sw2_solve --wrap=ssw_2d_calculate_elem_error`` against
@@ -141,7 +141,7 @@ def build(src: str = REFERENCE_SRC, jobs: int = os.cpu_count() or 4) -> str:
     hobj = os.path.join(objdir, "adh_dump.o")
     subprocess.run(["gcc", "-c"] + flags + [harness, "-o", hobj], check=True, capture_output=True)
     subprocess.run(["gcc", "-fcommon", "-o", exe] + objs + [hobj, stub, "-lm",
-                    "-Wl,--wrap=fe_main", "-Wl,--wrap=fe_sw2_load"], check=True)
+                    "-Wl,--wrap=fe_main", "-Wl,--wrap=fe_sw2_load", "-Wl,--wrap=fe_transport_load"], check=True)
     stage_qa(src)
     lib = os.path.join(REPO, "adhv8_kraken_b200", "libsw2gpu.so")
     if os.path.exists(lib):
@@ -163,6 +163,7 @@ def build_gpu_harness(flags, objs, hobj, stub, lib) -> str:
     rpath = "$ORIGIN/" + os.path.relpath(libdir, OUT)
     subprocess.run(["gcc", "-fcommon", "-o", GPU_EXE] + objs + [hobj, aobj, stub, f"-L{libdir}", "-lsw2gpu", "-lm",
                     f"-Wl,-rpath,{rpath}", "-Wl,--wrap=fe_main", "-Wl,--wrap=fe_sw2_load",
+                    "-Wl,--wrap=fe_transport_load",
                     "-Wl,--wrap=fe_sw2_solve", "-Wl,--wrap=ssw_2d_calculate_elem_error"], check=True)
     return GPU_EXE
 

@@ -38,7 +38,7 @@ def read_dump(path: str) -> List[tuple]:
 
 
 def parse(recs) -> Dict[str, list]:
-    steps, loads = [], []
+    steps, loads, tloads = [], [], []
     i = 0
     while i < len(recs):
         tag, arr = recs[i]
@@ -60,31 +60,48 @@ def parse(recs) -> Dict[str, list]:
                 steps[-1]["elem_error"] = recs[i][1]
                 steps[-1]["node_error"] = recs[i + 1][1]
                 i += 2
+            cons = []
+            while i < len(recs) and recs[i][0] == "con":        # constituent concentrations
+                cons.append(recs[i][1])
+                i += 1
+            if cons:
+                steps[-1]["con"] = cons
+        elif tag == "tload":                                     # transport Jacobian build
+            d = dict(itrn=int(arr[0]), t=arr[1], dt=arr[2])
+            j = i + 1
+            while j < len(recs) and recs[j][0] not in ("step", "load", "tload"):
+                d[recs[j][0]] = recs[j][1]
+                j += 1
+            tloads.append(d)
+            i = j
         elif tag == "load":
             d = dict(t=arr[0], dt=arr[1])
             j = i + 1
-            while j < len(recs) and recs[j][0] not in ("step", "load"):
+            while j < len(recs) and recs[j][0] not in ("step", "load", "tload"):
                 d[recs[j][0]] = recs[j][1]
                 j += 1
             loads.append(d)
             i = j
         else:
             i += 1
-    return dict(steps=steps, loads=loads)
+    return dict(steps=steps, loads=loads, tloads=tloads)
 
 
 def run_reference(model, nsteps=None, loads: int = 0, workdir: str = None, timeout: float = 3600.0,
-                  mass: bool = False, dacont: bool = False, error: bool = False):
+                  mass: bool = False, dacont: bool = False, error: bool = False, tloads: int = 0):
     """Run the reference on ``model``; returns parsed records and the wall time (s).  mass: also
     record the reference's grid mass diagnostics after every step; dacont: its transport side
     output elem_rhs_dacont_extra_terms; error: its adaption error indicator (elem_error per
-    element and its nodal average)."""
+    element and its nodal average); tloads: the inputs and results of the first `tloads`
+    transport Jacobian builds.  A model with constituents records their concentrations after
+    every step."""
     if not os.path.exists(EXE):
         raise FileNotFoundError("oracle/_ref/adh_dump is not built (python oracle/ref/build_ref.py)")
     tmp = workdir or tempfile.mkdtemp(prefix="adhref_")
     try:
         model.write_adh(tmp, "m", nsteps=nsteps)
-        env = dict(os.environ, ADH_DUMP=os.path.join(tmp, "dump.bin"), ADH_DUMP_LOADS=str(loads))
+        env = dict(os.environ, ADH_DUMP=os.path.join(tmp, "dump.bin"), ADH_DUMP_LOADS=str(loads),
+                   ADH_DUMP_TLOADS=str(tloads))
         if mass:
             env["ADH_DUMP_MASS"] = "1"
         if dacont:

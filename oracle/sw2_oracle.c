@@ -26,6 +26,11 @@
  * side output elem_rhs_dacont_extra_terms.  Lid node strings are rejected at create
  * time; wind, waves, baroclinic terms, vorticity and quadrilaterals have no input
  * fields here (the generated workloads use none).
+ *
+ * The 2D transport of general constituents carried by the flow (fe_transport,
+ * src/fe/transport/) is restated at the end of the file: fe_2d_transport_body_resid,
+ * fe_2d_transport_boundary_resid, fe_transport_resid / _load / _init / _inc and the
+ * transport branches of fe_newton.
  */
 #include <math.h>
 #include <float.h>
@@ -81,6 +86,14 @@ typedef struct orc_ctx {
     int bandwidth_nodes;
     int *perm, *iperm;         /* node order for the banded LU */
     int nblock;
+    /* constituent transport (orc_trn_setup) */
+    int ntrn;
+    double *trn_refc;          /* [ntrn] property[0] */
+    double *trn_dm;            /* [ntrn * M] MP DF d_m */
+    int *trn_bc, *trn_ser;     /* [ntrn * S] trans[itrn].bc_flag, its series (iu_0 / isigma) */
+    double *conc;              /* [ntrn][3][V] concentration levels */
+    int *bcmask;               /* [V] mod->bc_mask of the last fe_transport_init */
+    double *tval, *tres, *tsol;/* scalar Jacobian over the pattern [nnzb], residual, increment [V] */
 } orc_ctx;
 
 /* ------------------------------------------------------------------------------ */
@@ -193,7 +206,19 @@ static double roughness(const orc_ctx *C, int str, double depth) {   /* fe_sw2_g
 /* ------------------------------------------------------------------------------ */
 /* wet/dry wrapper (fe_sw2_wet_dry_wrapper.c:106-306) with the integrands as an enum */
 
-enum { WD_AVG, WD_CONT_TEMPORAL, WD_CONVECTION, WD_GLS_CONVECTION, WD_PRESSURE, WD_BODYFORCE, WD_BPRESSURE };
+enum { WD_AVG, WD_CONT_TEMPORAL, WD_CONVECTION, WD_GLS_CONVECTION, WD_PRESSURE, WD_BODYFORCE, WD_BPRESSURE,
+       WD_TRN_TEMPORAL, WD_TRN_CONVECTION };
+
+static void tri_gradphi_dot_f_g_v(const v2 *g, double djac, double c, const double *f, const double *gg,
+                                  const v2 *v, double *I) {          /* fe_elem2d_integrations.c:571-587 */
+    double b[3] = {0., 0., 0.};
+    tri_phi_f_g(djac, c, f, gg, b);
+    double ix = v[0].x * b[0] + v[1].x * b[1] + v[2].x * b[2];
+    double iy = v[0].y * b[0] + v[1].y * b[1] + v[2].y * b[2];
+    I[0] += ix * g[0].x + iy * g[0].y;
+    I[1] += ix * g[1].x + iy * g[1].y;
+    I[2] += ix * g[2].x + iy * g[2].y;
+}
 
 typedef struct {
     const v2 *x;          /* node coordinates */
@@ -251,6 +276,17 @@ static void wd_func(int kind, const v2 *x, const double *h, const v2 *g, const v
         double rx[3] = {0, 0, 0}, ry[3] = {0, 0, 0};
         tri_phi_h_df(djac, b, h, *v, rx, ry);
         for (i = 0; i < 3; i++) { rhs[i].x += rx[i]; rhs[i].y += ry[i]; }
+        break; }
+    case WD_TRN_TEMPORAL: {                   /* fe_2d_transport_wd_temporal_triangle
+                                                 (fe_2d_transport_wet_dry_integrations.c:86-99) */
+        double rc[3] = {0, 0, 0};
+        tri_phi_f_g(djac, a * b, h, fwd, rc);
+        for (i = 0; i < 3; i++) rhs[i].c += rc[i];
+        break; }
+    case WD_TRN_CONVECTION: {                 /* fe_2d_transport_wd_convection_triangle (:39-48) */
+        double rc[3] = {0, 0, 0};
+        tri_gradphi_dot_f_g_v(g, djac, a * b, h, fwd, vwd, rc);
+        for (i = 0; i < 3; i++) rhs[i].c += rc[i];
         break; }
     case WD_BPRESSURE: {                      /* fe_sw2_wd_boundaryPressure_triangle */
         int e;
@@ -347,6 +383,26 @@ static void wd_average(const v2 *x, const double *h, const v2 *vel, double djac,
     }
 }
 
+/* fe_sw2_get_EEVF (src/fe/sw2/fe_sw2_get_EEVF.c:33-60): estimated eddy viscosity of mode 1..3 */
+static void eevf(int mode, double coef, double gr, double dll, double h_fric, double rough, double area, v2 gu,
+                 v2 gv, double vmag, int wd, double *ev_st, double *ev_tr) {
+    double vmin = 0.1 * sqrt(gr * dll), evmin = 0., st, tr;
+    if (mode == 1) {
+        st = 0.0; tr = coef * 2.0 * h_fric * sqrt(rough) * vmag;
+        evmin = (coef / 0.5) * vmin * sqrt(area) / 40.; tr = MAXD(tr, evmin);
+    } else if (mode == 2) {
+        st = 1.3 * h_fric * sqrt(rough) * vmag;
+        tr = coef * 0.92 * h_fric * sqrt(rough) * vmag;
+        evmin = (coef / 0.5) * vmin * sqrt(area) / 40.; tr = MAXD(tr, evmin);
+    } else {
+        st = 0.;
+        tr = coef * coef * area * sqrt(gu.x * gu.x + gv.y * gv.y + 0.5 * (gu.y + gv.x) * (gu.y + gv.x));
+        evmin = (coef / 0.2) * vmin * sqrt(area) / 40.; tr = MAXD(tr, evmin);
+    }
+    if (wd == 1 || wd == 2) { st = 0.0; tr = MAXD(tr, 5. * evmin); }
+    *ev_st = st; *ev_tr = tr;
+}
+
 /* ------------------------------------------------------------------------------ */
 /* fe_sw2_body_resid (triangles) */
 
@@ -434,22 +490,9 @@ static void body_resid(const orc_ctx *C, int ie, const elem_in *E, int pvar, dof
         double xx = C->mat_ev[3 * imat] + P->viscosity, yy = C->mat_ev[3 * imat + 1] + P->viscosity;
         ev_st = fabs(xx - yy);
         ev_tr = MIND(xx, yy);
-    } else {                                                    /* fe_sw2_get_EEVF */
-        int mode = C->mat_eev_mode[imat];
-        double coef = C->mat_eev_coef[imat], vmin = 0.1 * sqrt(gr * dll), evmin = 0.;
-        if (mode == 1) {
-            ev_st = 0.0; ev_tr = coef * 2.0 * h_fric * sqrt(rough) * vmag;
-            evmin = (coef / 0.5) * vmin * sqrt(djac) / 40.; ev_tr = MAXD(ev_tr, evmin);
-        } else if (mode == 2) {
-            ev_st = 1.3 * h_fric * sqrt(rough) * vmag;
-            ev_tr = coef * 0.92 * h_fric * sqrt(rough) * vmag;
-            evmin = (coef / 0.5) * vmin * sqrt(djac) / 40.; ev_tr = MAXD(ev_tr, evmin);
-        } else {
-            ev_st = 0.;
-            ev_tr = coef * coef * djac * sqrt(gu.x * gu.x + gv.y * gv.y + 0.5 * (gu.y + gv.x) * (gu.y + gv.x));
-            evmin = (coef / 0.2) * vmin * sqrt(djac) / 40.; ev_tr = MAXD(ev_tr, evmin);
-        }
-        if (wd == 1 || wd == 2) { ev_st = 0.0; ev_tr = MAXD(ev_tr, 5. * evmin); }
+    } else {
+        eevf(C->mat_eev_mode[imat], C->mat_eev_coef[imat], gr, dll, h_fric, rough, djac, gu, gv, vmag, wd,
+             &ev_st, &ev_tr);
     }
 
     for (i = 0; i < 3; i++) { er[i].c = 0; er[i].x = 0; er[i].y = 0; }
@@ -871,6 +914,8 @@ void orc_destroy(orc_ctx *C) {
     free(C->wd); free(C->dacont); free(C->resid); free(C->sol); free(C->include); free(C->djac); free(C->grad);
     free(C->edjac); free(C->enrml); free(C->rowptr); free(C->col); free(C->blk_of_pair); free(C->eblk_of_pair);
     free(C->val); free(C->perm); free(C->iperm);
+    free(C->trn_refc); free(C->trn_dm); free(C->trn_bc); free(C->trn_ser); free(C->conc); free(C->bcmask);
+    free(C->tval); free(C->tres); free(C->tsol);
     free(C);
 }
 
@@ -1630,4 +1675,441 @@ void orc_set_waves(orc_ctx *C, const double *rxx, const double *rxy, const doubl
         C->wvx[e] = sx;
         C->wvy[e] = sy;
     }
+}
+
+/* ------------------------------------------------------------------------------ */
+/* 2D constituent transport (src/fe/transport/), after an accepted SW2 step.
+ * A general constituent (CN CON) moves with the water velocity: mfcf = 1 and vcf = 0
+ * (scon_init, src/structs/scon.c:38-50), so the constituent velocity (vel + vcf) * mfcf of
+ * fe_2d_transport_body_resid.c:183-187 is the water velocity.  Source/sink terms belong to
+ * sediment only (:469-487); salinity, temperature (baroclinic coupling) and the vorticity
+ * constituent are not restated. */
+
+#define ORC_BCT_DIR 1                  /* define.h:375 */
+#define ORC_BCT_NEU 3                  /* define.h:377 */
+#define ORC_BCT_CEQ 36                 /* define.h:388 */
+
+static double *TC(const orc_ctx *C, int t, int level) { return C->conc + ((size_t) 3 * t + level) * C->V; }
+
+int orc_trn_setup(orc_ctx *C, int ntrn, const double *refc, const double *dm, const int *bc, const int *ser) {
+    int k;
+    free(C->trn_refc); free(C->trn_dm); free(C->trn_bc); free(C->trn_ser); free(C->conc); free(C->bcmask);
+    free(C->tval); free(C->tres); free(C->tsol);
+    C->ntrn = ntrn;
+    C->trn_refc = (double *) dup(refc, sizeof(double) * ntrn);
+    C->trn_dm = (double *) dup(dm, sizeof(double) * ntrn * C->M);
+    C->trn_bc = (int *) dup(bc, sizeof(int) * ntrn * C->S);
+    C->trn_ser = (int *) dup(ser, sizeof(int) * ntrn * C->S);
+    C->conc = (double *) calloc((size_t) 3 * (ntrn ? ntrn : 1) * C->V, sizeof(double));
+    C->bcmask = (int *) calloc(C->V, sizeof(int));
+    C->tval = (double *) calloc(C->nnzb ? C->nnzb : 1, sizeof(double));
+    C->tres = (double *) calloc(C->V, sizeof(double));
+    C->tsol = (double *) calloc(C->V, sizeof(double));
+    for (k = 0; k < ntrn * C->S; k++) {
+        int f = C->trn_bc[k];
+        if (f != 0 && f != ORC_BCT_DIR && f != ORC_BCT_NEU) return -1;
+        if ((f == ORC_BCT_DIR || f == ORC_BCT_NEU) && (C->trn_ser[k] < 0 || C->trn_ser[k] >= C->NS)) return -1;
+    }
+    for (k = 0; k < ntrn; k++) if (!(C->trn_refc[k] != 0.0)) return -1;
+    for (k = 0; k < ntrn; k++) {
+        int e;
+        for (e = 0; e < C->E; e++) if (C->trn_bc[k * C->S + C->edge_string[e]] == ORC_BCT_DIR) return -1;
+    }
+    return 0;
+}
+void orc_trn_set_conc(orc_ctx *C, int t, int level, const double *c) { memcpy(TC(C, t, level), c, sizeof(double) * C->V); }
+void orc_trn_get_conc(const orc_ctx *C, int t, int level, double *c) { memcpy(c, TC(C, t, level), sizeof(double) * C->V); }
+void orc_set_dacont(orc_ctx *C, const double *in) {   /* vertex-major [3][T], as orc_get_dacont */
+    int i, e;
+    for (i = 0; i < 3; i++) for (e = 0; e < C->T; e++) C->dacont[3 * e + i] = in[(size_t) i * C->T + e];
+}
+void orc_trn_get_bcmask(const orc_ctx *C, int *mask) { memcpy(mask, C->bcmask, sizeof(int) * C->V); }
+
+static int trn_dirichlet(const orc_ctx *C, int t, int node) {
+    int s = C->node_string[node];
+    if (s <= SW2GPU_NORMAL) return 0;
+    return C->trn_bc[t * C->S + s] == ORC_BCT_DIR || C->trn_bc[t * C->S + s] == ORC_BCT_CEQ;
+}
+
+/* fe_2d_trns_temporal (fe_2d_transport_body_resid.c:692-726): one level's wrapped temporal term
+ * times dt_factor */
+static void trn_temporal(const v2 *X, double djac, const double *hh, const double *cc, double dtf, double *er) {
+    dof3 r[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    wd_args A = {X, hh, NULL, NULL, NULL, cc, djac, 1., 1.};
+    int i;
+    wd_wrapper(WD_TRN_TEMPORAL, r, &A, 1);
+    for (i = 0; i < 3; i++) er[i] += dtf * r[i].c;
+}
+
+/* fe_2d_transport_body_resid (src/fe/transport/fe_2d_transport_body_resid.c:50-676), triangles;
+ * pnode >= 0 perturbs the concentration of local node pnode by psign * eps (PERTURB_C) */
+static void trn_body_resid(const orc_ctx *C, int t, int ie, double eps, int pnode, int psign, double *er) {
+    const sw2gpu_params *P = &C->p;
+    const int *nd = C->tri + 3 * ie;
+    const double djac = C->djac[ie], dt = C->dt, alpha = P->tau_temporal, dll = P->drying_lower_limit;
+    const v2 *g = (const v2 *) (C->grad + 6 * ie);
+    const int imat = C->tri_mat[ie], wd = C->wd[ie];
+    const double *c0 = TC(C, t, 0), *c1 = TC(C, t, 1), *c2 = TC(C, t, 2);
+    double c[3], co[3], coo[3], h[3], ho[3], hoo[3], uc[3], vc[3];
+    v2 X[3], vcon[3];
+    int i;
+    for (i = 0; i < 3; i++) {
+        int n = nd[i];
+        X[i].x = C->x[n]; X[i].y = C->y[n];
+        c[i] = c0[n]; co[i] = c1[n]; coo[i] = c2[n];
+        h[i] = C->h[0][n]; ho[i] = C->h[1][n]; hoo[i] = C->h[2][n];
+        vcon[i].x = (C->u[0][n] + 0.0) * 1.0;               /* (vel + vcf) * mfcf (:183-187) */
+        vcon[i].y = (C->v[0][n] + 0.0) * 1.0;
+        uc[i] = vcon[i].x; vc[i] = vcon[i].y;
+    }
+    if (pnode >= 0) c[pnode] += psign * eps;                /* :171 */
+
+    /* elemental averages and gradients (:207-222) */
+    double c_avg = tri_f(1., 1., c), h_avg = tri_f(1., 1., h);
+    double u_avg = tri_f(1., 1., uc), v_avg = tri_f(1., 1., vc);
+    v2 gc = {0, 0}, gu = {0, 0}, gv = {0, 0};
+    for (i = 0; i < 3; i++) { gc.x += c[i] * g[i].x; gc.y += c[i] * g[i].y; }
+    for (i = 0; i < 3; i++) {
+        gu.x += vcon[i].x * g[i].x; gu.y += vcon[i].x * g[i].y;
+        gv.x += vcon[i].y * g[i].x; gv.y += vcon[i].y * g[i].y;
+    }
+    double vmag = sqrt(u_avg * u_avg + v_avg * v_avg);
+
+    /* wet/dry factors and averages (:242-256).  fe_sw2_wd_average's integrand averages the
+     * clipped depth whatever function it is given (fe_sw2_wet_dry_integrations.c:101-102), so
+     * the second call, made for the concentration, returns the wet-area depth average too. */
+    double factor = 1., h_wd = h_avg, c_wd = c_avg;
+    v2 vwd = {u_avg, v_avg};
+    if (wd != 0) {
+        v2 unused;
+        wd_average(X, h, vcon, djac, &h_wd, &vwd);
+        wd_average(X, h, NULL, djac, &c_wd, &unused);
+        factor = wd_factor(X, h, djac);
+    }
+
+    /* friction and diffusion coefficients (:258-290) */
+    double h_fric = MAXD(h_avg, ORC_SMALL);
+    double rough = roughness(C, imat, h_fric);
+    double dxx = 0.0, dyy = 0.0, dxy = C->trn_dm[t * C->M + imat];
+    if (C->mat_eev_mode[imat] != 0) {
+        double st, tr;
+        eevf(C->mat_eev_mode[imat], C->mat_eev_coef[imat], P->gravity, dll, h_fric, rough, djac, gu, gv, vmag, wd,
+             &st, &tr);
+        dxx = st; dxy = tr; dyy = st;
+    }
+    v2 vdir = {u_avg / MAXD(vmag, 1.E-8), v_avg / MAXD(vmag, 1.E-8)};   /* :293-295 */
+
+    for (i = 0; i < 3; i++) er[i] = 0.0;
+    /* temporal (:376-400) */
+    trn_temporal(X, djac, h, c, (1. + alpha / 2.), er);
+    trn_temporal(X, djac, ho, co, (-1.) * (1. + alpha), er);
+    trn_temporal(X, djac, hoo, coo, (alpha / 2.), er);
+    /* advection (:402-427) */
+    {
+        dof3 r[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        wd_args A = {X, h, g, NULL, vcon, c, djac, dt, -1.};
+        wd_wrapper(WD_TRN_CONVECTION, r, &A, 1);
+        for (i = 0; i < 3; i++) er[i] += r[i].c;
+    }
+    /* diffusion (:429-463), VT_2D_TENS2D_VECT2D_PROD_AI (macro.h:726-728) */
+    {
+        double factor_diff = MAXD(factor, .01);
+        double depth = MAXD(h_wd, ORC_SMALL);
+        double depth_diff = MAXD(depth, dll * .01);
+        v2 flux;
+        flux.x = dxx * vdir.x * (vdir.x * gc.x + vdir.y * gc.y) + dxy * gc.x;
+        flux.y = dyy * vdir.y * (vdir.x * gc.x + vdir.y * gc.y) + dxy * gc.y;
+        double r[3] = {0, 0, 0};
+        tri_gradphi_dot_vbar(g, dt * depth_diff * factor_diff, djac, flux, r);
+        for (i = 0; i < 3; i++) er[i] += r[i];
+    }
+    /* SUPG (:567-617): fe_get_supg_tau method 2 (fe_get_supg_tau.c:176-183) with the area
+     * element length sqrt(area) (:285-290); the strong residual is the advection term alone */
+    {
+        double fn = sqrt(u_avg * u_avg + v_avg * v_avg);
+        double le = sqrt(djac);
+        double tau = (le / (fn + 2. * ORC_NQS)) * P->tau_pg;
+        double conv = h_wd * (vwd.x * gc.x + vwd.y * gc.y);
+        double strong = 0. + conv + factor * (0. + 0.);
+        double r[3] = {0, 0, 0};
+        tri_gradphi_dot_vbar(g, tau * dt * strong, djac, vwd, r);
+        for (i = 0; i < 3; i++) er[i] += r[i];
+    }
+    /* the flow's extra continuity terms (:619-634) */
+    for (i = 0; i < 3; i++) er[i] += c_wd * C->dacont[3 * ie + i];
+    /* Dirichlet nodes (:641-660) */
+    for (i = 0; i < 3; i++) if (trn_dirichlet(C, t, nd[i])) er[i] = 0.0;
+}
+
+static void line_phi_f_g(double djac, double c, const double *f, const double *g, double *I) {  /* elem1d:101-105 */
+    double t1 = ONE_12 * djac * c;
+    I[0] += t1 * ((3 * f[0] + f[1]) * g[0] + (f[0] + f[1]) * g[1]);
+    I[1] += t1 * ((f[0] + f[1]) * g[0] + (f[0] + 3 * f[1]) * g[1]);
+}
+
+/* fe_2d_transport_boundary_resid (src/fe/transport/fe_2d_transport_boundary_resid.c:37-300) */
+static void trn_edge_resid(const orc_ctx *C, int t, int ie, double eps, int pnode, int psign, double *er) {
+    const int *nd = C->edges + 2 * ie;
+    const int str = C->edge_string[ie], hflag = C->str_bc[str];
+    const int cflag = C->trn_bc[t * C->S + str], cser = C->trn_ser[t * C->S + str];
+    const double c_inv = 1. / C->trn_refc[t], dt = C->dt, djac = C->edjac[ie];
+    const v2 n = {C->enrml[2 * ie], C->enrml[2 * ie + 1]};
+    double c[2], h[2], vn[2];
+    int i;
+    for (i = 0; i < 2; i++) {
+        int k = nd[i];
+        c[i] = TC(C, t, 0)[k];
+        h[i] = C->h[0][k];
+        vn[i] = C->u[0][k] * n.x + C->v[0][k] * n.y;
+    }
+    if (pnode >= 0) c[pnode] += psign * eps;
+    er[0] = er[1] = 0.0;
+    if (hflag == SW2GPU_BCT_VEL_NEU) {                                  /* :186-214 */
+        double flux = -1.0 * C->series[C->str_isigma[str]];
+        if (flux < -ORC_SMALL) {
+            /* con_bc_flag > NORMAL: only NB TRN (BCT_NEU) reaches here, setup refuses DB TRN on
+             * edge strings, whose isigma the reference would read unset */
+            if (cflag == ORC_BCT_NEU) line_phi(djac, C->series[cser] * c_inv * flux * dt, er);
+        } else {
+            line_phi_f(djac, flux * dt, c, er);
+        }
+    } else if (hflag == SW2GPU_BCT_OUTFLOW) {                           /* :216-231 */
+        line_phi_f_g_h(djac, dt, vn[0], vn[1], h[0], h[1], c[0], c[1], er);
+    } else if (hflag == SW2GPU_BCT_PRS_NEU) {                           /* :233-257 */
+        double hf = 0.5 * (vn[0] * h[0] + vn[1] * h[1]);
+        if (hf >= 0.) line_phi_f_g_h(djac, dt, vn[0], vn[1], h[0], h[1], c[0], c[1], er);
+        else if (cflag == ORC_BCT_NEU) line_phi_f_g(djac, C->series[cser] * c_inv * dt, h, vn, er);
+    }
+    for (i = 0; i < 2; i++) {                                           /* :281-296 */
+        if (h[i] < 0.0) er[i] = 0.0;
+        if (trn_dirichlet(C, t, nd[i])) er[i] = 0.0;
+    }
+}
+
+/* fe_transport_resid (src/fe/transport/fe_transport_resid.c:33-221): wet and partially wet
+ * triangles (wd_flag 0 or 1), then the boundary edges; Dirichlet rows stay 0; entries below
+ * SMALL are zeroed */
+void orc_trn_resid(orc_ctx *C, int t, double *R) {
+    int e, i;
+    memset(C->tres, 0, sizeof(double) * C->V);
+    for (e = 0; e < C->T; e++) {
+        if (C->wd[e] != 0 && C->wd[e] != 1) continue;
+        double er[3];
+        trn_body_resid(C, t, e, 0., -1, 1, er);
+        for (i = 0; i < 3; i++) { int n = C->tri[3 * e + i]; if (!C->bcmask[n]) C->tres[n] -= er[i]; }
+    }
+    for (e = 0; e < C->E; e++) {
+        double er[2];
+        trn_edge_resid(C, t, e, 0., -1, 1, er);
+        for (i = 0; i < 2; i++) { int n = C->edges[2 * e + i]; if (!C->bcmask[n]) C->tres[n] -= er[i]; }
+    }
+    for (i = 0; i < C->V; i++) if (fabs(C->tres[i]) < ORC_SMALL) C->tres[i] = 0.0;
+    if (R) memcpy(R, C->tres, sizeof(double) * C->V);
+}
+
+/* perturb_c's step (fe_transport_load.c:258-275): the node's concentration clamped to
+ * [1, property[0]], NUM_DIFF_EPSILON_GENERAL with the fraction 0.1 (macro.h:676-680) */
+static double trn_eps(double cn, double refc) {
+    double ce = cn, e;
+    if (ce < 1.0) ce = 1.0;
+    if (ce > refc) ce = refc;
+    e = fabs(ce) * (1. + 0.1);
+    e -= fabs(ce);
+    if (e < 0.1) e = 0.1;
+    return e;
+}
+
+/* fe_transport_load (src/fe/transport/fe_transport_load.c:41-225) with perturb_c (:227-340):
+ * central differences of every triangle (whatever its wd_flag) and edge, assembled by
+ * fe_global_matrix_assemble_scalar (fe_assemble_matrix.c:51-138: entries of magnitude SMALL
+ * or less are dropped), then diagonals below NOT_QUITE_SMALL raised to it
+ * (check_matrix_diagonal_for_nonexistant_entries, tl_matrix.c:59-67) */
+void orc_trn_load(orc_ctx *C, int t) {
+    int e, i, j, k;
+    const double *c = TC(C, t, 0), refc = C->trn_refc[t];
+    memset(C->tval, 0, sizeof(double) * (size_t) C->nnzb);
+    for (e = 0; e < C->T; e++) {
+        double M[9];
+        for (i = 0; i < 3; i++) {
+            double eps = trn_eps(c[C->tri[3 * e + i]], refc), rp[3], rm[3];
+            trn_body_resid(C, t, e, eps, i, +1, rp);
+            trn_body_resid(C, t, e, eps, i, -1, rm);
+            for (k = 0; k < 3; k++) M[i + 3 * k] = (rp[k] - rm[k]) / (2.0 * eps);   /* elem_matrix_deriv_1dof */
+        }
+        for (i = 0; i < 3; i++) for (j = 0; j < 3; j++) {
+            double v = M[3 * i + j];
+            if (fabs(v) > ORC_SMALL) C->tval[C->blk_of_pair[9 * e + 3 * i + j]] += v;
+        }
+    }
+    for (e = 0; e < C->E; e++) {
+        double M[4];
+        for (i = 0; i < 2; i++) {
+            double eps = trn_eps(c[C->edges[2 * e + i]], refc), rp[2], rm[2];
+            trn_edge_resid(C, t, e, eps, i, +1, rp);
+            trn_edge_resid(C, t, e, eps, i, -1, rm);
+            for (k = 0; k < 2; k++) M[i + 2 * k] = (rp[k] - rm[k]) / (2.0 * eps);
+        }
+        for (i = 0; i < 2; i++) for (j = 0; j < 2; j++) {
+            double v = M[2 * i + j];
+            if (fabs(v) > ORC_SMALL) C->tval[C->eblk_of_pair[4 * e + 2 * i + j]] += v;
+        }
+    }
+    for (i = 0; i < C->V; i++) {
+        double *d = C->tval + find_blk(C, i, i);
+        if (fabs(*d) < ORC_NQS) *d = ORC_NQS;
+    }
+}
+void orc_trn_get_matrix(const orc_ctx *C, double *val, double *resid) {
+    if (val) memcpy(val, C->tval, sizeof(double) * (size_t) C->nnzb);
+    if (resid) memcpy(resid, C->tres, sizeof(double) * C->V);
+}
+
+/* fe_transport_init (src/fe/transport/fe_transport_init.c:24-116) */
+void orc_trn_init(orc_ctx *C, int t) {
+    double *c = TC(C, t, 0);
+    const double *co = TC(C, t, 1), c_inv = 1. / C->trn_refc[t];
+    int i;
+    for (i = 0; i < C->V; i++) {
+        if (isnan(c[i]) || isinf(c[i])) c[i] = 0.0;
+        C->bcmask[i] = 0;
+        c[i] = co[i];
+        if (C->h[0][i] <= ORC_NQS) c[i] = 0.0;
+    }
+    for (i = 0; i < C->V; i++) {
+        int s = C->node_string[i];
+        if (s > SW2GPU_NORMAL && C->trn_bc[t * C->S + s] == ORC_BCT_DIR) {
+            C->bcmask[i] = 1;
+            c[i] = C->series[C->trn_ser[t * C->S + s]] * c_inv;
+        }
+    }
+}
+
+/* scalar banded LU of the spv_jacobi-scaled system in reverse Cuthill-McKee order: the exact
+ * solve the reference's profile LU preconditioner gives its BiCGSTAB (one iteration) */
+static int trn_linear_solve(orc_ctx *C, const double *rhs, double *x) {
+    int V = C->V, i, k, r, c, j;
+    double *S = (double *) malloc(sizeof(double) * V);
+    for (i = 0; i < V; i++) {                            /* spv_jacobi: row max */
+        double m = 0.0;
+        for (k = C->rowptr[i]; k < C->rowptr[i + 1]; k++) if (fabs(C->tval[k]) > m) m = fabs(C->tval[k]);
+        S[i] = (m < ORC_SMALL) ? 1.0 / sqrt(ORC_SMALL) : 1.0 / sqrt(m);
+    }
+    int w = 0;
+    for (i = 0; i < V; i++)
+        for (k = C->rowptr[i]; k < C->rowptr[i + 1]; k++) {
+            int d = abs(C->iperm[i] - C->iperm[C->col[k]]);
+            if (d > w) w = d;
+        }
+    int W = 2 * w + 1;
+    double *B = (double *) calloc((size_t) V * W, sizeof(double)), *y = (double *) malloc(sizeof(double) * V);
+    for (i = 0; i < V; i++) {
+        int pi = C->iperm[i];
+        for (k = C->rowptr[i]; k < C->rowptr[i + 1]; k++) {
+            int pj = C->iperm[C->col[k]];
+            B[(size_t) pi * W + (pj - pi + w)] = C->tval[k] * S[i] * S[C->col[k]];
+        }
+        y[pi] = rhs[i] * S[i];
+    }
+    for (r = 0; r < V; r++) {                            /* Doolittle, no pivoting */
+        double piv = B[(size_t) r * W + w];
+        if (piv == 0.0) piv = B[(size_t) r * W + w] = ORC_SMALL;
+        int rend = r + w < V - 1 ? r + w : V - 1;
+        for (j = r + 1; j <= rend; j++) {
+            double *Rj = B + (size_t) j * W, l = Rj[r - j + w] / piv;
+            if (l == 0.0) continue;
+            Rj[r - j + w] = l;
+            for (c = r + 1; c <= rend; c++) Rj[c - j + w] -= l * B[(size_t) r * W + (c - r + w)];
+        }
+    }
+    for (r = 0; r < V; r++) {
+        int c0 = r - w > 0 ? r - w : 0;
+        double acc = y[r];
+        for (c = c0; c < r; c++) acc -= B[(size_t) r * W + (c - r + w)] * y[c];
+        y[r] = acc;
+    }
+    for (r = V - 1; r >= 0; r--) {
+        int c1 = r + w < V - 1 ? r + w : V - 1;
+        double acc = y[r];
+        for (c = r + 1; c <= c1; c++) acc -= B[(size_t) r * W + (c - r + w)] * y[c];
+        y[r] = acc / B[(size_t) r * W + w];
+    }
+    for (i = 0; i < V; i++) x[i] = y[C->iperm[i]] * S[i];
+    free(S); free(B); free(y);
+    return 1;
+}
+
+static void trn_norms(orc_ctx *C, double *rmax, double *rl2, double *imax) {   /* get_residual_norms, nsys 1 */
+    int i;
+    double l2 = 0, mx = 0, im = 0;
+    for (i = 0; i < C->V; i++) {
+        int inc = MIND(C->h[0][i], C->h[1][i]) > 0;        /* include_node_in_residual (fe_newton.c:177-188) */
+        double r = C->tres[i], s = C->tsol[i];
+        if (fabs(s) > im && inc) im = fabs(s);
+        if (fabs(r) > mx && inc) mx = fabs(r);
+        l2 += r * r;
+    }
+    *rmax = mx; *rl2 = sqrt(l2 / C->V); *imax = im;
+}
+
+static void trn_inc(orc_ctx *C, int t) {                    /* fe_transport_inc.c:24-61 */
+    double *c = TC(C, t, 0);
+    int i;
+    for (i = 0; i < C->V; i++) c[i] += C->tsol[i];
+}
+
+/* fe_transport (fe_transport.c:58-74) for constituent t: level shift, then fe_newton with the
+ * transport functions, whose linear-problem test keeps iterating while the residual max norm
+ * exceeds tol_nonlin (fe_newton.c:817-823, :855-856).  Uses the flow's current levels, wd_flag,
+ * dt, series values and side output as the last SW2 step left them. */
+int orc_trn_step(orc_ctx *C, int t, sw2gpu_stats *st) {
+    const sw2gpu_params *P = &C->p;
+    int V = C->V, i, it = 0, lin_total = 0, cuts_total = 0, solv_ok = 1, isnan_flag = 0, keep;
+    double rmax, rl2, imax, old_l2;
+    memcpy(TC(C, t, 2), TC(C, t, 1), sizeof(double) * V);
+    memcpy(TC(C, t, 1), TC(C, t, 0), sizeof(double) * V);
+    memset(C->tsol, 0, sizeof(double) * V);
+    orc_trn_init(C, t);
+    orc_trn_resid(C, t, NULL);
+    trn_norms(C, &rmax, &rl2, &imax);
+    const int lin_test = P->tol_nonlin > ORC_SMALL;
+    do {
+        orc_trn_load(C, t);
+        lin_total += trn_linear_solve(C, C->tres, C->tsol);
+        trn_inc(C, t);
+        for (i = 0; i < V; i++) C->tsol[i] = -C->tsol[i];
+        old_l2 = rl2;
+        orc_trn_resid(C, t, NULL);
+        trn_norms(C, &rmax, &rl2, &imax);
+        if (isnan(rl2) || isinf(rl2)) { solv_ok = 0; isnan_flag = 1; }
+        int cuts = 0;
+        while (rmax > P->tol_nonlin && rl2 > old_l2 && cuts < P->max_linesearch_cuts) {
+            for (i = 0; i < V; i++) C->tsol[i] *= 0.5;
+            trn_inc(C, t);
+            orc_trn_resid(C, t, NULL);
+            trn_norms(C, &rmax, &rl2, &imax);
+            cuts++;
+        }
+        cuts_total += cuts;
+        it++;
+        keep = solv_ok && it < P->max_nonlin_it && rmax < 1.0E+20 && (lin_test && rmax > P->tol_nonlin);
+    } while (keep);
+    int rc = SW2GPU_OK;
+    if (!solv_ok || (lin_test && rmax > P->tol_nonlin) || rmax >= 1.0E+20) {
+        rc = isnan_flag ? SW2GPU_E_NAN : (!solv_ok ? SW2GPU_E_LINEAR : SW2GPU_E_NEWTON);
+        orc_trn_init(C, t);
+    }
+    if (st) {
+        memset(st, 0, sizeof(*st));
+        st->status = rc; st->newton_its = it; st->linear_its = lin_total; st->linesearch_cuts = cuts_total;
+        st->resid_max = rmax; st->resid_l2 = rl2; st->inc_max = imax;
+    }
+    return rc;
+}
+
+/* one element's transport residual, for checking the device physics element by element */
+void orc_trn_body_resid(orc_ctx *C, int t, int ie, double eps, int pnode, int psign, double *out) {
+    trn_body_resid(C, t, ie, eps, pnode, psign, out);
+}
+void orc_trn_edge_resid(orc_ctx *C, int t, int ie, double eps, int pnode, int psign, double *out) {
+    trn_edge_resid(C, t, ie, eps, pnode, psign, out);
 }

@@ -29,6 +29,11 @@ def mass_ref():
     return dict(np.load(os.path.join(GOLDEN, "mass_ref.npz")))
 
 
+@pytest.fixture(scope="session")
+def transport_ref():
+    return dict(np.load(os.path.join(GOLDEN, "transport_ref.npz")))
+
+
 def relerr(a, b):
     """max |a - b| / max |b| (the per-field error used throughout the tests)."""
     a, b = np.asarray(a), np.asarray(b)

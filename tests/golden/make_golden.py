@@ -38,6 +38,13 @@ Fixtures (numpy ``.npz``):
 * ``errind_ref.npz`` -- the reference's adaption error indicator (ssw_2d_calculate_elem_error,
   src/structs/ssw_2d.c:424-500: grid->elem_error and its nodal average) after steps 1, 4 and 8
   of the basin run, whose states are in ``basin_ref.npz``.
+* ``transport_ref.npz`` -- constituent transport after every flow step (fe_transport) on five
+  workloads of ``adhv8_kraken_b200.meshgen``: the channel with a held inflow concentration
+  (DB TRN) and diffusion, the wet/dry basin with two constituents (NB TRN at the inflow and the
+  tailwater, per-material diffusion), the all-terms basin (temporal alpha, EEV diffusion), the
+  free-outflow channel and the uniform-17.5 channel of the reference's angle_salt check:
+  concentrations after every step, and for the two basins the inputs and results of the first
+  two transport Jacobian builds.
 * ``mass_ref.npz`` -- the reference's grid mass diagnostics (src/tools/tl_grid_mass.c) after
   every step of 6 channel steps and of the 8 basin steps: initial and current mass, mass error
   and accumulated mass flux, with the channel's state after every step (the basin's states are
@@ -65,6 +72,10 @@ def fingerprint(m) -> str:
     h = hashlib.sha256()
     for a in (m.x, m.y, m.z, m.tri, m.tri_mat, m.edges, m.edge_string, m.h0, m.u0, m.v0):
         h.update(np.ascontiguousarray(a).tobytes())
+    if m.constituents:
+        for a in m.transport_tables():
+            h.update(np.ascontiguousarray(a).tobytes())
+        h.update(np.ascontiguousarray(m.node_string).tobytes())
     return h.hexdigest()
 
 
@@ -217,10 +228,55 @@ def mass():
     np.savez_compressed(os.path.join(HERE, "mass_ref.npz"), **out)
 
 
+TRANSPORT_CASES = {"channel": lambda: meshgen.channel_transport(nsteps=6),
+                   "basin": lambda: meshgen.basin_transport(nsteps=8),
+                   "terms": lambda: meshgen.terms_transport(nsteps=6),
+                   "outflow": lambda: meshgen.outflow_transport(nsteps=6),
+                   "salt": lambda: meshgen.salt_transport(nsteps=6)}
+
+
+def transport():
+    """Constituent transport after every flow step (fe_transport): each case's concentrations
+    after every step, and for the wet/dry basins the inputs and results of the first two
+    transport Jacobian builds (fe_transport_load): the three concentration and flow levels,
+    wd_flag, the flow's side output, bc_mask, the residual and the scalar Jacobian over the
+    sorted pattern."""
+    out = {}
+    for name, make in TRANSPORT_CASES.items():
+        m = make()
+        nl = 2 if name in ("basin", "terms") else 0
+        ref = run_reference(m, tloads=nl)
+        out[f"{name}_fingerprint"] = np.array(fingerprint(m))
+        out[f"{name}_t"] = np.array([s["t"] for s in ref["steps"]])
+        out[f"{name}_dt"] = np.array([s["dt"] for s in ref["steps"]])
+        out[f"{name}_attempts"] = np.array([s["attempts"] for s in ref["steps"]], np.int32)
+        out[f"{name}_con"] = np.stack([np.stack(s["con"]) for s in ref["steps"]])     # [step, ntrn, V]
+        rp, col = pattern(m)
+        for q, L in enumerate(ref["tloads"][:nl]):
+            p = f"{name}_tload{q}"
+            for key in ("c", "c1", "c2", "h", "u", "v", "h1", "u1", "v1", "h2", "u2", "v2", "resid", "dacont"):
+                out[f"{p}_{key}"] = L[key]
+            out[f"{p}_wd"] = L["wd"]
+            out[f"{p}_bcmask"] = (L["bcmask"] == 1).astype(np.int32)
+            out[f"{p}_meta"] = np.array([L["itrn"], L["t"], L["dt"]])
+            val = np.zeros(len(col))
+            k = 0
+            for i in range(m.nnodes):
+                lookup = {int(c): rp[i] + n for n, c in enumerate(col[rp[i]:rp[i + 1]])}
+                val[lookup[i]] = L["diag"][i]
+                for _ in range(L["rowsz"][i]):
+                    c = int(L["cols"][k])
+                    if c >= 0:
+                        val[lookup[c]] += L["vals"][k]
+                    k += 1
+            out[f"{p}_val"] = val
+    np.savez_compressed(os.path.join(HERE, "transport_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     import sys as _sys
     which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "terms", "rain", "obstacle", "combined", "dacont",
-                              "mass", "scale", "errind"]
+                              "mass", "scale", "errind", "transport"]
     if "channel" in which:
         channel()
     if "basin" in which:
@@ -245,8 +301,10 @@ if __name__ == "__main__":
         scale()
     if "errind" in which:
         errind()
+    if "transport" in which:
+        transport()
     for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "terms_ref.npz", "rain_ref.npz",
               "obstacle_ref.npz", "combined_ref.npz", "dacont_ref.npz", "mass_ref.npz", "scale_ref.npz",
-              "errind_ref.npz"):
+              "errind_ref.npz", "transport_ref.npz"):
         if os.path.exists(os.path.join(HERE, f)):
             print(f, os.path.getsize(os.path.join(HERE, f)))
