@@ -28,6 +28,8 @@ SW2GPU_PREC_BJACOBI = 0
 SW2GPU_PREC_ILU0 = 1
 SW2GPU_PREC_BAND = 2
 SW2GPU_PREC_DILU = 3
+SW2GPU_BCT_DIR = 1    # DB TRN
+SW2GPU_BCT_NEU = 3    # NB TRN
 SW2GPU_BCT_LID_DFT = 20         # lids on node strings: refused by sw2gpu_create (not built)
 SW2GPU_BCT_LID_ELV = 21
 SW2GPU_BCT_LID_DEP = 22
@@ -70,6 +72,14 @@ class Stats(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Transport(C.Structure):
+    """sw2gpu_transport: the constituents (include/sw2gpu.h)."""
+    _fields_ = [
+        ("ntransport", C.c_int32), ("ref_conc", C.POINTER(C.c_double)), ("diffusion", C.POINTER(C.c_double)),
+        ("str_bc_flag", C.POINTER(C.c_int32)), ("str_series", C.POINTER(C.c_int32)),
+    ]
 
 
 def _i32(a) -> np.ndarray:

@@ -221,6 +221,34 @@ __device__ __forceinline__ double drag_coef(double depth, double ks) {  // fr_be
     return 2. * (t * t);
 }
 
+// estimated eddy viscosity of mode 1..3 (fe_sw2_get_EEVF, src/fe/sw2/fe_sw2_get_EEVF.c:33-60):
+// streamwise and transverse coefficients from the friction depth, the drag coefficient, the
+// element area, the velocity gradients and the average speed
+__device__ __forceinline__ void eev_coefficients(int mode, double coef, double g, double dll, double h_fric,
+                                                 double rough, double area, double gux, double guy, double gvx,
+                                                 double gvy, double vmag, int wd_flag, double& ev_st, double& ev_tr) {
+    const double vmin = 0.1 * sqrt(g * dll);
+    double evmin;
+    if (mode == 1) {
+        ev_st = 0.0;
+        ev_tr = coef * 2.0 * h_fric * sqrt(rough) * vmag;
+        evmin = (coef / 0.5) * vmin * sqrt(area) / 40.;
+    } else if (mode == 2) {
+        ev_st = 1.3 * h_fric * sqrt(rough) * vmag;
+        ev_tr = coef * 0.92 * h_fric * sqrt(rough) * vmag;
+        evmin = (coef / 0.5) * vmin * sqrt(area) / 40.;
+    } else {
+        ev_st = 0.;
+        ev_tr = coef * coef * area * sqrt(gux * gux + gvy * gvy + 0.5 * (guy + gvx) * (guy + gvx));
+        evmin = (coef / 0.2) * vmin * sqrt(area) / 40.;
+    }
+    ev_tr = fmax(ev_tr, evmin);
+    if (wd_flag == 1 || wd_flag == 2) {
+        ev_st = 0.0;
+        ev_tr = fmax(ev_tr, 5. * evmin);
+    }
+}
+
 // ---------------------------------------------------------------------------------
 // Parts of the fully wet residual that depend on one part of the iterate only.  An FD
 // Jacobian column perturbs one variable at one vertex, so what depends only on the old
@@ -403,27 +431,8 @@ __device__ __forceinline__ void elem_resid_impl(const ElemIn& in, const double* 
         ev_st = M.ev_st;
         ev_tr = M.ev_tr;
     } else {
-        const double vmin = 0.1 * sqrt(g * dll);
-        double evmin;
-        const double coef = M.eev_coef;
-        if (M.eev_mode == 1) {
-            ev_st = 0.0;
-            ev_tr = coef * 2.0 * h_fric * sqrt(rough) * vmag;
-            evmin = (coef / 0.5) * vmin * sqrt(djac) / 40.;
-        } else if (M.eev_mode == 2) {
-            ev_st = 1.3 * h_fric * sqrt(rough) * vmag;
-            ev_tr = coef * 0.92 * h_fric * sqrt(rough) * vmag;
-            evmin = (coef / 0.5) * vmin * sqrt(djac) / 40.;
-        } else {
-            ev_st = 0.;
-            ev_tr = coef * coef * djac * sqrt(gux * gux + gvy * gvy + 0.5 * (guy + gvx) * (guy + gvx));
-            evmin = (coef / 0.2) * vmin * sqrt(djac) / 40.;
-        }
-        ev_tr = fmax(ev_tr, evmin);
-        if (wd_flag == 1 || wd_flag == 2) {
-            ev_st = 0.0;
-            ev_tr = fmax(ev_tr, 5. * evmin);
-        }
+        eev_coefficients(M.eev_mode, M.eev_coef, g, dll, h_fric, rough, djac, gux, guy, gvx, gvy, vmag, wd_flag,
+                         ev_st, ev_tr);
     }
 
 #pragma unroll

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -32,6 +33,7 @@
 #include "sw2_kernels.cuh"
 #include "sw2_krylov.cuh"
 #include "sw2_series.h"
+#include "trn_kernels.cuh"
 
 using namespace sw2;
 
@@ -99,6 +101,7 @@ struct sw2gpu_ctx {
     std::vector<int> dir_node, dir_mask, dir_str;
     MeshTables tab;                    // pattern and gather lists (sw2_tables.h)
     std::vector<int> tri_h, edg_h;     // connectivity the tables were made from (sw2gpu_remesh)
+    std::vector<int> node_str_h, edg_str_h;   // node and edge strings (transport boundary conditions)
     std::vector<int>& rowptr_h = tab.rp;
     std::vector<int>& col_h = tab.col;
     // device mesh
@@ -141,6 +144,26 @@ struct sw2gpu_ctx {
     bool wave_on = false;
     DBuf<double> stress;        // element surface stress, wind + waves: x [T], y [T]
     bool dacont_on = false;
+    // constituent transport (sw2gpu_set_transport): per constituent three levels rotated by index
+    // like the flow's, its string table and MP DF coefficients; work arrays shared by all
+    int ntrn = 0;
+    std::vector<double> trn_refc, trn_dm_h;     // [ntrn], [ntrn * M]
+    std::vector<int> trn_bc_h, trn_ser_h;       // [ntrn * S]
+    std::vector<std::array<int, 3>> trn_lv;     // level rotation per constituent
+    DBuf<double> tconc;                         // [ntrn][3][V]
+    DBuf<int> tbc, tnode_str;                   // [ntrn * S], [V]
+    DBuf<double> tdm, tsval;                    // [ntrn * M], [S]
+    DBuf<unsigned char> tmask;                  // [V] bc_mask
+    DBuf<double> trslot, tjslot, tR, tsol, taoff, tdinv, tkpart;
+    DBuf<double> tkv[kTrnKVectors];
+    DBuf<Norms> tnpart, tnorms;
+    DBuf<unsigned> tncount;
+    DBuf<KrylovCtl> tctl;
+    Norms* tnorms_h = nullptr;                  // pinned: residual norms of the last evaluation
+    KrylovCtl* tctl_h = nullptr;                // pinned: the last transport Krylov solve
+    double* tsval_h = nullptr;                  // pinned [S]
+    int trn_kgrid = 0;                          // CTAs of the transport Krylov solve
+    double* tlevel(int k, int l) { return tconc.p + ((size_t)3 * k + trn_lv[k][l]) * V; }
     bool has_ovh = false;       // some edge string is NB OVH (its velocity series go up every step)
     DBuf<int> slot_ptr, slot_idx, blk_ptr, blk_src, rowptr, col, blk_row, dpos;
     DBuf<int> dir_node_d, dir_mask_d;
@@ -348,6 +371,9 @@ sw2gpu_ctx::~sw2gpu_ctx() {
     }
     if (stage_h) cudaFreeHost(stage_h);
     if (mass_h) cudaFreeHost(mass_h);
+    if (tnorms_h) cudaFreeHost(tnorms_h);
+    if (tctl_h) cudaFreeHost(tctl_h);
+    if (tsval_h) cudaFreeHost(tsval_h);
     self.reset();
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -1701,6 +1727,8 @@ int create_impl(const sw2gpu_mesh* m, const sw2gpu_params* prm, void* stream, Me
     // BCSR pattern and reference-order gather lists (sw2_tables.h)
     c->tri_h.assign(tri, tri + 3ull * T);
     c->edg_h.assign(edg, edg + 2ull * E);
+    c->node_str_h.assign(m->node_string, m->node_string + V);
+    c->edg_str_h.assign(m->elem1d_string, m->elem1d_string + E);
     if (pre) {
         c->tab = std::move(*pre);
     } else {
@@ -1875,6 +1903,24 @@ int sw2gpu_remesh(sw2gpu_ctx* old, const sw2gpu_mesh* m, sw2gpu_ctx** out) {
     if (!rc && old->dacont_on) rc = sw2gpu_set_dacont(c, 1);
     if (!rc && old->mass_on) rc = sw2gpu_set_mass_tracking(c, 1, old->mass_density);
     if (!rc && old->use_graphs) rc = sw2gpu_set_graphs(c, 1);
+    if (!rc && old->ntrn) {
+        if (c->S != old->S || c->M != old->M) {
+            rc = fail(SW2GPU_E_ARG, "remesh: the constituents need the same strings and materials");
+        } else {
+            sw2gpu_transport spec{old->ntrn, old->trn_refc.data(), old->trn_dm_h.data(), old->trn_bc_h.data(),
+                                  old->trn_ser_h.data()};
+            rc = sw2gpu_set_transport(c, &spec);
+        }
+        // the concentration levels of the nodes both meshes have
+        for (int k = 0; !rc && k < old->ntrn; k++) {
+            c->trn_lv[k] = old->trn_lv[k];
+            for (int l = 0; !rc && l < 3; l++)
+                if (cudaMemcpyAsync(c->tconc.p + ((size_t)3 * k + l) * c->V, old->tconc.p + ((size_t)3 * k + l) * old->V,
+                                    sizeof(double) * std::min(V, old->V), cudaMemcpyDeviceToDevice,
+                                    c->stream) != cudaSuccess)
+                    rc = fail(SW2GPU_E_CUDA, "copying the concentrations: %s", cudaGetErrorString(cudaGetLastError()));
+        }
+    }
     // the three time levels of the nodes both meshes have (node numbers are kept); new nodes start at 0
     const size_t nb = sizeof(double) * std::min(V, old->V);
     for (int l = 0; !rc && l < 3; l++) {
@@ -2128,6 +2174,333 @@ int sw2gpu_get_dacont(sw2gpu_ctx* c, double* out) {
     if (!c || !out) return fail(SW2GPU_E_ARG, "null argument");
     if (!c->dacont_on) return fail(SW2GPU_E_ARG, "transport side output not enabled (sw2gpu_set_dacont)");
     if (c->T) CK(cudaMemcpyAsync(out, c->dacont.p, sizeof(double) * 3 * c->T, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// constituent transport (fe_transport, src/fe/transport/fe_transport.c:31-113)
+
+int sw2gpu_set_transport(sw2gpu_ctx* c, const sw2gpu_transport* t) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    if (!t || t->ntransport == 0) {
+        c->ntrn = 0;
+        return SW2GPU_OK;
+    }
+    const int n = t->ntransport, S = c->S, M = c->M, V = c->V, T = c->T, E = c->E;
+    if (n < 0 || !t->ref_conc || (M && !t->diffusion) || (S && (!t->str_bc_flag || !t->str_series)))
+        return fail(SW2GPU_E_ARG, "bad transport description");
+    for (int k = 0; k < n; k++) {
+        if (!(t->ref_conc[k] != 0.0) || !std::isfinite(t->ref_conc[k]))
+            return fail(SW2GPU_E_ARG, "constituent %d: reference concentration must be finite and nonzero", k);
+        for (int s = 0; s < S; s++) {
+            const int f = t->str_bc_flag[k * S + s], q = t->str_series[k * S + s];
+            if (f != 0 && f != SW2GPU_BCT_DIR && f != SW2GPU_BCT_NEU)
+                return fail(SW2GPU_E_ARG, "constituent %d, string %d: bc flag %d not supported", k, s, f);
+            if (f != 0 && (q < 0 || q >= c->NS))
+                return fail(SW2GPU_E_ARG, "constituent %d, string %d: series %d out of range", k, s, q);
+        }
+        for (int j = 0; j < E; j++)
+            if (t->str_bc_flag[k * S + c->edg_str_h[j]] == SW2GPU_BCT_DIR)
+                return fail(SW2GPU_E_ARG, "constituent %d: DB TRN on edge string %d", k, c->edg_str_h[j]);
+    }
+    c->trn_refc.assign(t->ref_conc, t->ref_conc + n);
+    c->trn_dm_h.assign((size_t)n * M, 0.0);
+    if (M) std::copy(t->diffusion, t->diffusion + (size_t)n * M, c->trn_dm_h.begin());
+    c->trn_bc_h.assign((size_t)n * S, 0);
+    c->trn_ser_h.assign((size_t)n * S, -1);
+    if (S) {
+        std::copy(t->str_bc_flag, t->str_bc_flag + (size_t)n * S, c->trn_bc_h.begin());
+        std::copy(t->str_series, t->str_series + (size_t)n * S, c->trn_ser_h.begin());
+    }
+    c->trn_lv.assign(n, std::array<int, 3>{0, 1, 2});
+    cudaStream_t st = c->stream;
+    g_alloc_bytes = &c->bytes;
+    int rc = 0;
+    if (c->ntrn != n || !c->tconc.p) rc |= zalloc(c->tconc, (size_t)3 * n * V, st);
+    rc |= up(c->tbc, c->trn_bc_h, st);
+    rc |= up(c->tdm, c->trn_dm_h, st);
+    if (!c->tnode_str.p) {
+        std::vector<int> ns(V, -1);
+        for (int i = 0; i < V; i++) ns[i] = c->node_str_h[i] > SW2GPU_NORMAL ? c->node_str_h[i] : -1;
+        rc |= up(c->tnode_str, ns, st);
+        rc |= zalloc(c->tsval, std::max(S, 1), st);
+        rc |= zalloc(c->tmask, V, st);
+        rc |= zalloc(c->trslot, 3ull * T + 2ull * E, st);
+        rc |= zalloc(c->tjslot, 9ull * T + 4ull * E, st);
+        rc |= zalloc(c->tR, V, st);
+        rc |= zalloc(c->tsol, V, st);
+        rc |= zalloc(c->taoff, (size_t)(c->nnzb - V), st);
+        rc |= zalloc(c->tdinv, V, st);
+        for (auto& b : c->tkv) rc |= zalloc(b, V, st);
+        rc |= zalloc(c->tnpart, nblk(V, kGatherThreads), st);
+        rc |= zalloc(c->tnorms, 1, st);
+        rc |= zalloc(c->tncount, 1, st);
+        rc |= zalloc(c->tctl, 1, st);
+        int dev = 0, sms = 0, per_sm = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trn_bicgstab, kTrnKThreads, 0));
+        // at most the co-resident CTAs (a cooperative launch), at least 512 rows each
+        c->trn_kgrid = std::max(1, std::min(sms * std::max(per_sm, 1), V / 512));
+        rc |= zalloc(c->tkpart, 9ull * c->trn_kgrid, st);
+        if (!c->tnorms_h) CK(cudaMallocHost(&c->tnorms_h, sizeof(Norms)));
+        if (!c->tctl_h) CK(cudaMallocHost(&c->tctl_h, sizeof(KrylovCtl)));
+        if (!c->tsval_h) CK(cudaMallocHost(&c->tsval_h, sizeof(double) * std::max(S, 1)));
+    }
+    g_alloc_bytes = nullptr;
+    if (rc) return rc;
+    c->ntrn = n;
+    if (!c->dacont_on && (rc = sw2gpu_set_dacont(c, 1))) return rc;   // the transport residual reads it
+    CK(cudaStreamSynchronize(st));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_set_conc(sw2gpu_ctx* c, int32_t itrn, int32_t level, const double* conc) {
+    if (!c || !conc || itrn < 0 || itrn >= c->ntrn || level < 0 || level > 2)
+        return fail(SW2GPU_E_ARG, "bad context, constituent or level");
+    CK(cudaMemcpyAsync(c->tlevel(itrn, level), conc, sizeof(double) * c->V, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_get_conc(sw2gpu_ctx* c, int32_t itrn, int32_t level, double* conc) {
+    if (!c || !conc || itrn < 0 || itrn >= c->ntrn || level < 0 || level > 2)
+        return fail(SW2GPU_E_ARG, "bad context, constituent or level");
+    CK(cudaMemcpyAsync(conc, c->tlevel(itrn, level), sizeof(double) * c->V, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+namespace {
+
+TrnArgs trn_args(sw2gpu_ctx* c, int k) {
+    TrnArgs A{};
+    A.m = c->dm;
+    A.h = c->H(0);
+    A.u = c->U(0);
+    A.v = c->Vv(0);
+    A.ho = c->H(1);
+    A.hoo = c->H(2);
+    A.wd = c->wd.p;
+    A.dac = c->dacont.p;
+    A.c = c->tlevel(k, 0);
+    A.co = c->tlevel(k, 1);
+    A.coo = c->tlevel(k, 2);
+    A.node_str = c->tnode_str.p;
+    A.tbc = c->tbc.p + (size_t)k * c->S;
+    A.tsval = c->tsval.p;
+    A.tdm = c->tdm.p + (size_t)k * c->M;
+    A.refc = c->trn_refc[k];
+    A.mask = c->tmask.p;
+    A.rslot = c->trslot.p;
+    A.jslot = c->tjslot.p;
+    A.R = c->tR.p;
+    A.sol = c->tsol.p;
+    A.aoff = c->taoff.p;
+    A.dinv = c->tdinv.p;
+    A.val = nullptr;
+    A.npart = c->tnpart.p;
+    A.norms = c->tnorms.p;
+    A.ncounter = c->tncount.p;
+    A.P = TrnParams{c->p.gravity, c->p.drying_lower_limit, c->p.tau_temporal, c->p.tau_pg, c->dt};
+    return A;
+}
+
+// step values of constituent k's string series over property[0] (DB TRN: fe_transport_init.c:93-100;
+// NB TRN: fe_2d_transport_boundary_resid.c:194, :240)
+int trn_upload_series(sw2gpu_ctx* c, int k, const double* series) {
+    const double c_inv = 1. / c->trn_refc[k];
+    for (int s = 0; s < c->S; s++) {
+        const int f = c->trn_bc_h[(size_t)k * c->S + s], q = c->trn_ser_h[(size_t)k * c->S + s];
+        c->tsval_h[s] = (f != 0 && q >= 0 && series) ? series[q] * c_inv : 0.0;
+    }
+    if (c->S) CK(cudaMemcpyAsync(c->tsval.p, c->tsval_h, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->stream));
+    return 0;
+}
+
+int trn_init(sw2gpu_ctx* c, const TrnArgs& A) {
+    k_trn_init<<<nblk(c->V, kTrnThreads), kTrnThreads, 0, c->stream>>>(A);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+// residual and its norms (fe_transport_resid + get_residual_norms); waits for them
+int trn_resid(sw2gpu_ctx* c, const TrnArgs& A, Norms& out, int& launches) {
+    k_trn_elem<false><<<nblk(c->T + c->E, kTrnThreads), kTrnThreads, 0, c->stream>>>(A);
+    k_trn_resid_gather<<<nblk(c->V, kGatherThreads), kGatherThreads, 0, c->stream>>>(A);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->tnorms_h, c->tnorms.p, sizeof(Norms), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out = *c->tnorms_h;
+    launches += 2;
+    return 0;
+}
+
+// FD Jacobian and the folded operator (fe_transport_load)
+int trn_load(sw2gpu_ctx* c, const TrnArgs& A, int& launches) {
+    k_trn_elem<true><<<nblk(c->T + c->E, kTrnThreads), kTrnThreads, 0, c->stream>>>(A);
+    k_trn_jac_gather<<<nblk(c->V, kTrnThreads), kTrnThreads, 0, c->stream>>>(A);
+    CK(cudaGetLastError());
+    launches += 2;
+    return 0;
+}
+
+// the Krylov solve of the folded system into tsol; its outcome lands in tctl_h at the next sync
+int trn_krylov(sw2gpu_ctx* c, int& launches) {
+    TrnKrylovArgs K{};
+    K.V = c->V;
+    K.orowptr = c->orowptr.p;
+    K.ocol = c->ocol.p;
+    K.aoff = c->taoff.p;
+    K.dinv = c->tdinv.p;
+    K.R = c->tR.p;
+    K.x = c->tsol.p;
+    for (int q = 0; q < kTrnKVectors; q++) K.vec[q] = c->tkv[q].p;
+    K.part = c->tkpart.p;
+    K.ctl = c->tctl.p;
+    K.rtol = c->p.lin_rtol;
+    K.atol = c->p.lin_atol;
+    K.max_it = c->p.max_lin_it;
+    K.spin_limit = c->wait_barrier;
+    CK(cudaMemsetAsync(c->tctl.p, 0, sizeof(KrylovCtl), c->stream));
+    void* args[] = {&K};
+    CK(cudaLaunchCooperativeKernel((void*)k_trn_bicgstab, dim3(c->trn_kgrid), dim3(kTrnKThreads), args, 0,
+                                   c->stream));
+    CK(cudaMemcpyAsync(c->tctl_h, c->tctl.p, sizeof(KrylovCtl), cudaMemcpyDeviceToHost, c->stream));
+    launches += 1;
+    return 0;
+}
+
+int trn_inc(sw2gpu_ctx* c, int k, int mode, int& launches) {
+    k_trn_inc<<<nblk(c->V, kTrnThreads), kTrnThreads, 0, c->stream>>>(c->tlevel(k, 0), c->tsol.p, c->V, mode);
+    CK(cudaGetLastError());
+    launches += 1;
+    return 0;
+}
+
+// fe_transport for constituent k (fe_transport.c:58-74): level shift, fe_transport_init, then
+// fe_newton with the transport functions, whose linear-problem test keeps iterating while the
+// residual max norm exceeds tol_nonlin (fe_newton.c:817-823, :855-856)
+int trn_step_one(sw2gpu_ctx* c, int k, const double* series, sw2gpu_stats* st) {
+    const sw2gpu_params& P = c->p;
+    auto& lv = c->trn_lv[k];
+    const int o2 = lv[2];
+    lv[2] = lv[1];
+    lv[1] = lv[0];
+    lv[0] = o2;
+    int rc, launches = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, c->stream));
+    if ((rc = trn_upload_series(c, k, series))) return rc;
+    const TrnArgs A = trn_args(c, k);
+    CK(cudaMemsetAsync(c->tsol.p, 0, sizeof(double) * c->V, c->stream));
+    if ((rc = trn_init(c, A))) return rc;
+    launches++;
+    Norms nr;
+    if ((rc = trn_resid(c, A, nr, launches))) return rc;
+    const bool lin_test = P.tol_nonlin > kSmall;
+    int it = 0, lin_total = 0, cuts_total = 0, status = SW2GPU_OK;
+    bool solv_ok = true, nan_flag = false, timeout = false;
+    double rl2 = sqrt(nr.l2sum / c->V);
+    for (;;) {
+        if ((rc = trn_load(c, A, launches))) return rc;
+        if ((rc = trn_krylov(c, launches))) return rc;
+        if ((rc = trn_inc(c, k, 0, launches))) return rc;
+        const double old_l2 = rl2;
+        if ((rc = trn_resid(c, A, nr, launches))) return rc;   // also brings the Krylov outcome
+        const KrylovCtl kc = *c->tctl_h;
+        if (kc.err) {
+            timeout = true;
+            break;
+        }
+        lin_total += kc.iterations;
+        if (!kc.converged) solv_ok = false;
+        rl2 = sqrt(nr.l2sum / c->V);
+        if (std::isnan(rl2) || std::isinf(rl2)) {
+            solv_ok = false;
+            nan_flag = true;
+        }
+        int cuts = 0;
+        while (nr.rmax > P.tol_nonlin && rl2 > old_l2 && cuts < P.max_linesearch_cuts) {
+            if ((rc = trn_inc(c, k, 1, launches))) return rc;
+            if ((rc = trn_resid(c, A, nr, launches))) return rc;
+            rl2 = sqrt(nr.l2sum / c->V);
+            cuts++;
+        }
+        cuts_total += cuts;
+        it++;
+        const bool keep = solv_ok && it < P.max_nonlin_it && nr.rmax < 1.0E+20 && (lin_test && nr.rmax > P.tol_nonlin);
+        if (!keep) break;
+    }
+    if (timeout) status = SW2GPU_E_TIMEOUT;
+    else if (!solv_ok || (lin_test && nr.rmax > P.tol_nonlin) || nr.rmax >= 1.0E+20)
+        status = nan_flag ? SW2GPU_E_NAN : (!solv_ok ? SW2GPU_E_LINEAR : SW2GPU_E_NEWTON);
+    if (status != SW2GPU_OK) {   // reset to the old level (fe_newton.c:883)
+        if ((rc = trn_init(c, A))) return rc;
+        launches++;
+    }
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) {
+        memset(st, 0, sizeof(*st));
+        st->status = status;
+        st->newton_its = it;
+        st->linear_its = lin_total;
+        st->linesearch_cuts = cuts_total;
+        st->resid_max = nr.rmax;
+        st->resid_l2 = rl2;
+        st->inc_max = nr.imax;
+        st->device_ms = ms;
+        st->kernel_launches = launches;
+    }
+    return status;
+}
+
+}  // namespace
+
+int sw2gpu_transport_step(sw2gpu_ctx* c, const double* series, sw2gpu_stats* stats) {
+    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    if (!c->ntrn) return fail(SW2GPU_E_ARG, "no constituents (sw2gpu_set_transport)");
+    if (!(c->dt > 0.0)) return fail(SW2GPU_E_ARG, "no flow step yet (dt unset)");
+    for (int k = 0; k < c->ntrn; k++) {
+        const int rc = trn_step_one(c, k, series, stats ? stats + k : nullptr);
+        if (rc) {
+            if (rc == SW2GPU_E_NEWTON || rc == SW2GPU_E_LINEAR || rc == SW2GPU_E_NAN || rc == SW2GPU_E_TIMEOUT)
+                return fail(rc, "transport of constituent %d did not converge (status %d)", k, rc);
+            return rc;
+        }
+    }
+    return SW2GPU_OK;
+}
+
+int sw2gpu_transport_init(sw2gpu_ctx* c, int32_t itrn, const double* series) {
+    if (!c || itrn < 0 || itrn >= c->ntrn) return fail(SW2GPU_E_ARG, "bad context or constituent");
+    int rc;
+    if ((rc = trn_upload_series(c, itrn, series))) return rc;
+    if ((rc = trn_init(c, trn_args(c, itrn)))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return SW2GPU_OK;
+}
+
+int sw2gpu_transport_load(sw2gpu_ctx* c, int32_t itrn, double* resid, double* val) {
+    if (!c || itrn < 0 || itrn >= c->ntrn) return fail(SW2GPU_E_ARG, "bad context or constituent");
+    DBuf<double> full;
+    if (val && full.alloc(c->nnzb)) return fail(SW2GPU_E_NOMEM, "cudaMalloc failed");
+    TrnArgs A = trn_args(c, itrn);
+    Norms nr;
+    int launches = 0, rc;
+    if ((rc = trn_resid(c, A, nr, launches))) return rc;
+    A.val = val ? full.p : nullptr;
+    if ((rc = trn_load(c, A, launches))) return rc;
+    if (resid) CK(cudaMemcpyAsync(resid, c->tR.p, sizeof(double) * c->V, cudaMemcpyDeviceToHost, c->stream));
+    if (val) CK(cudaMemcpyAsync(val, full.p, sizeof(double) * c->nnzb, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return SW2GPU_OK;
 }

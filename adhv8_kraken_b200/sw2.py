@@ -35,7 +35,9 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
            "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont",
            "sw2gpu_set_wait_limits", "sw2gpu_snapshot", "sw2gpu_elem_error", "sw2gpu_set_mass_tracking",
-           "sw2gpu_step_mass", "sw2gpu_set_wind", "sw2gpu_set_waves", "sw2gpu_remesh", "sw2gpu_batch_set_graphs"]
+           "sw2gpu_step_mass", "sw2gpu_set_wind", "sw2gpu_set_waves", "sw2gpu_remesh", "sw2gpu_batch_set_graphs",
+           "sw2gpu_set_transport", "sw2gpu_set_conc", "sw2gpu_get_conc", "sw2gpu_transport_step",
+           "sw2gpu_transport_init", "sw2gpu_transport_load"]
 
 
 class SW2Error(RuntimeError):
@@ -95,6 +97,12 @@ def lib():
         L.sw2gpu_step_mass.argtypes = [vp, c_double_p, c_double_p]
         L.sw2gpu_set_variant.argtypes = [vp, C.c_int32, C.c_int32]
         L.sw2gpu_get_variant.argtypes = [vp, c_int32_p, c_int32_p]
+        L.sw2gpu_set_transport.argtypes = [vp, vp]
+        L.sw2gpu_set_conc.argtypes = [vp, C.c_int32, C.c_int32, c_double_p]
+        L.sw2gpu_get_conc.argtypes = [vp, C.c_int32, C.c_int32, c_double_p]
+        L.sw2gpu_transport_step.argtypes = [vp, c_double_p, vp]
+        L.sw2gpu_transport_init.argtypes = [vp, C.c_int32, c_double_p]
+        L.sw2gpu_transport_load.argtypes = [vp, C.c_int32, c_double_p, c_double_p]
         L.sw2gpu_device_bytes.restype = C.c_int64
         L.sw2gpu_server_create.argtypes = [C.c_int32, C.c_double, C.c_int32, C.POINTER(vp)]
         L.sw2gpu_server_submit.argtypes = [vp, vp, vp, c_double_p, c_double_p, c_double_p, C.c_double, C.c_double,
@@ -174,9 +182,66 @@ class SW2GPU:
         _check(lib().sw2gpu_load(self.h, C.byref(n), None, None, None, None))
         self.nnzb = n.value
         self.t = model.t0
+        self._last = None          # (t, dt) of the last accepted step
         h0, u0, v0 = model.initial_state()
         for lvl in range(3):
             self.set_state(lvl, h0, u0, v0)
+        self.ntrn = 0
+        if model.constituents:
+            self.set_transport()
+
+    def set_transport(self, model=None):
+        """The model's constituents (sw2gpu_set_transport), every level at its initial
+        concentration (the hot start's ICON, whose old and older levels start from it)."""
+        model = self.model if model is None else model
+        refc, dm, bc, ser, c0 = model.transport_tables()
+        self._trn_arrays = [np.ascontiguousarray(a) for a in (refc, dm, bc, ser)]
+        a = self._trn_arrays
+        spec = capi.Transport(len(refc), _dp(a[0]), _dp(a[1]), a[2].ctypes.data_as(c_int32_p),
+                              a[3].ctypes.data_as(c_int32_p))
+        _check(lib().sw2gpu_set_transport(self.h, C.byref(spec)))
+        self.ntrn = len(refc)
+        for k in range(self.ntrn):
+            for lvl in range(3):
+                self.set_conc(k, lvl, c0[k])
+
+    def set_conc(self, itrn, level, conc):
+        c = np.ascontiguousarray(conc, dtype=np.float64)
+        _check(lib().sw2gpu_set_conc(self.h, itrn, level, _dp(c)))
+
+    def get_conc(self, itrn, level=0):
+        c = np.zeros(self.V)
+        _check(lib().sw2gpu_get_conc(self.h, itrn, level, _dp(c)))
+        return c
+
+    def transport_step(self, t=None, dt=None):
+        """fe_transport after the last accepted step (or over [t, t + dt]): every constituent;
+        a list of stats dicts, shorter than ntrn when a constituent failed (status != 0)."""
+        if t is None:
+            t, dt = self._last
+        s = self.model.series_values(t, t + dt)
+        st = (Stats * self.ntrn)()
+        rc = lib().sw2gpu_transport_step(self.h, _dp(s) if s.size else None, st)
+        if rc in (capi.SW2GPU_E_ARG, capi.SW2GPU_E_CUDA, capi.SW2GPU_E_NOMEM):
+            _check(rc)
+        out = []
+        for k in range(self.ntrn):
+            d = st[k].as_dict()
+            out.append(d)
+            if d["status"] != 0:
+                break
+        return out
+
+    def transport_init(self, itrn, t, dt):
+        """fe_transport_init of constituent itrn at the current levels (series over [t, t + dt])."""
+        s = self.model.series_values(t, t + dt)
+        _check(lib().sw2gpu_transport_init(self.h, itrn, _dp(s) if s.size else None))
+
+    def transport_load(self, itrn):
+        """Residual [V] and scalar FD Jacobian over the pattern [nnzb] at the current state."""
+        r, val = np.zeros(self.V), np.zeros(self.nnzb)
+        _check(lib().sw2gpu_transport_load(self.h, itrn, _dp(r), _dp(val)))
+        return val, r
 
     def remesh(self, model):
         """Moves this solver to `model`, an adaption of its mesh that keeps node and triangle
@@ -355,6 +420,7 @@ class SW2GPU:
             _check(rc)
         if rc == 0:
             self.t = t + dt
+            self._last = (t, dt)
         d = st.as_dict()
         d["status"] = rc
         return d
@@ -545,7 +611,15 @@ def run(solver: SW2GPU, nsteps: int, dt: float = None, max_retries: int = 8, cal
     d = dt
     for k in range(nsteps):
         for _ in range(max_retries + 1):
+            t = solver.t
             st = solver.step(dt=d)
+            if st["status"] == 0 and getattr(solver, "ntrn", 0):
+                # the constituents after the flow (fe_main.c:528-531); a failure fails the step
+                trn = solver.transport_step()
+                st["transport"] = trn
+                if len(trn) < solver.ntrn or trn[-1]["status"] != 0:
+                    st["status"] = trn[-1]["status"]
+                    solver.t = t
             if st["status"] == 0:
                 break
             d *= 0.25

@@ -255,6 +255,52 @@ int sw2gpu_step_mass(sw2gpu_ctx *ctx, double *mass, double *flux);
 int sw2gpu_set_dacont(sw2gpu_ctx *ctx, int32_t enable);
 int sw2gpu_get_dacont(sw2gpu_ctx *ctx, double *out);
 
+/* Constituent transport (fe_transport, src/fe/transport/fe_transport.c:31-113): general
+ * constituents (CN CON, src/initio/read_bc_CN.c:14-18) carried by the flow, solved after every
+ * accepted flow step on the flow's new, old and older levels, wd_flag and side output
+ * elem_rhs_dacont_extra_terms (switched on by sw2gpu_set_transport).  Per constituent and Newton
+ * iteration: the triangle and boundary-edge residuals (fe_2d_transport_body_resid.c:50-676,
+ * fe_2d_transport_boundary_resid.c:37-300: wrapped wet/dry temporal and advection terms,
+ * diffusion by MP DF or the estimated eddy viscosity, SUPG, the flow's extra continuity terms),
+ * the scalar FD Jacobian (fe_transport_load.c:41-340), a Jacobi-preconditioned BiCGSTAB on the
+ * device, and the reference's Newton rules for a linear problem (iterate while the residual max
+ * norm exceeds tol_nonlin).  Salinity and temperature (baroclinic coupling), the vorticity
+ * constituent, sediment and quadrilaterals are not built.
+ *   ref_conc[k]                  property[0]: boundary series values are divided by it
+ *   diffusion[k * nmats + m]     MP DF d_m of material m
+ *   str_bc_flag[k * nstrings + s] 0, SW2GPU_BCT_DIR (DB TRN: node string s holds the value of
+ *                                series str_series[..] / ref_conc) or SW2GPU_BCT_NEU (NB TRN: water
+ *                                entering through edge string s carries that value); DB TRN on an
+ *                                edge string is rejected with SW2GPU_E_ARG (the reference's
+ *                                boundary residual would read the string's unset NB TRN series)
+ * sw2gpu_set_transport copies the description (NULL or ntransport = 0 turns transport off) and
+ * starts every level at 0; sw2gpu_set_conc / sw2gpu_get_conc move a constituent's level
+ * (0 current, 1 old, 2 older) as stored, i.e. as the hot start's ICON data set gives it. */
+#define SW2GPU_BCT_DIR 1
+#define SW2GPU_BCT_NEU 3
+typedef struct sw2gpu_transport {
+    int32_t ntransport;
+    const double  *ref_conc;       /* [ntransport] */
+    const double  *diffusion;      /* [ntransport * nmats] */
+    const int32_t *str_bc_flag;    /* [ntransport * nstrings] */
+    const int32_t *str_series;     /* [ntransport * nstrings] series id or -1 */
+} sw2gpu_transport;
+int sw2gpu_set_transport(sw2gpu_ctx *ctx, const sw2gpu_transport *transport);
+int sw2gpu_set_conc(sw2gpu_ctx *ctx, int32_t itrn, int32_t level, const double *conc);
+int sw2gpu_get_conc(sw2gpu_ctx *ctx, int32_t itrn, int32_t level, double *conc);
+/* fe_transport after an accepted sw2gpu_step: every constituent in order (levels shifted, then
+ * its Newton solve); `series` are the step values the flow step used, stats[ntransport] (may be
+ * NULL).  Stops at the first constituent that fails with SW2GPU_E_NEWTON, _LINEAR, _NAN or
+ * _TIMEOUT, its current level reset to the old one (fe_transport_init); the reference then
+ * retries the whole time step with dt / 4, flow and transport shifting their levels again. */
+int sw2gpu_transport_step(sw2gpu_ctx *ctx, const double *series, sw2gpu_stats *stats);
+/* Hot-path pieces, for parity checks against the reference units: fe_transport_init of
+ * constituent itrn at the current levels (current level from the old one, dry nodes 0, DB TRN
+ * values); the residual resid[nnodes] (fe_transport_resid) and the scalar FD Jacobian
+ * val[nnzb] over the context's pattern (fe_transport_load) at the current state. */
+int sw2gpu_transport_init(sw2gpu_ctx *ctx, int32_t itrn, const double *series);
+int sw2gpu_transport_load(sw2gpu_ctx *ctx, int32_t itrn, double *resid, double *val);
+
 /* One implicit time step: time-level shift (fe_sw2, src/fe/sw2/fe_sw2.c:43-50) then the
  * damped Newton loop (fe_newton).  `series` holds the step-averaged value of every BC
  * series over [t, t+dt] (sseries_setall_ts_valuesAVG).  On SW2GPU_E_NEWTON the current

@@ -13,7 +13,8 @@ from adhv8_kraken_b200 import capi
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 STRUCTS = [("sw2gpu_mesh", capi.Mesh), ("sw2gpu_params", capi.Params), ("sw2gpu_stats", capi.Stats),
-           ("sw2gpu_run_stats", capi.RunStats), ("sw2gpu_request_stats", capi.RequestStats)]
+           ("sw2gpu_run_stats", capi.RunStats), ("sw2gpu_request_stats", capi.RequestStats),
+           ("sw2gpu_transport", capi.Transport)]
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compiler")
