@@ -281,6 +281,7 @@ __global__ void __launch_bounds__(kTrnThreads) k_trn_inc(double* __restrict__ c,
 // with the update) needs no barrier of its own because v = A'r + beta A'q is formed from r and q.
 // The barriers are bounded (grid_sync): a wait that runs out sets ctl->err and every CTA returns.
 constexpr int kTrnKThreads = 256;
+constexpr double kTrnKrylovRtol = 1e-12;   // relative stop of the transport Krylov solve (at most)
 constexpr int kTrnKVectors = 7;   // r, rhat, p, v, s, t, q
 
 struct TrnKrylovArgs {

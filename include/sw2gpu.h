@@ -263,8 +263,9 @@ int sw2gpu_get_dacont(sw2gpu_ctx *ctx, double *out);
  * fe_2d_transport_boundary_resid.c:37-300: wrapped wet/dry temporal and advection terms,
  * diffusion by MP DF or the estimated eddy viscosity, SUPG, the flow's extra continuity terms),
  * the scalar FD Jacobian (fe_transport_load.c:41-340), a Jacobi-preconditioned BiCGSTAB on the
- * device, and the reference's Newton rules for a linear problem (iterate while the residual max
- * norm exceeds tol_nonlin).  Salinity and temperature (baroclinic coupling), the vorticity
+ * device run to ||r||inf <= lin_atol + min(lin_rtol, 1e-12) ||b||inf (the reference solves each
+ * transport system exactly with its profile LU), and the reference's Newton rules for a linear
+ * problem (iterate while the residual max norm exceeds tol_nonlin).  Salinity and temperature (baroclinic coupling), the vorticity
  * constituent, sediment and quadrilaterals are not built.
  *   ref_conc[k]                  property[0]: boundary series values are divided by it
  *   diffusion[k * nmats + m]     MP DF d_m of material m

@@ -6,10 +6,11 @@ transport levels kept across a remesh, and a transport Krylov wait that runs out
 
 Tolerances: residual and Jacobian against the oracle 0 (the same operations in the same order);
 against the reference 1e-12 and 1e-10 (the reference's own round-off, and the flow's side output
-recomputed from the dumped state).  Time-stepped concentrations: 1e-8 of the field's maximum per
+recomputed from the dumped state).  Time-stepped concentrations: 1e-9 of the field's maximum per
 step -- the reference solves each transport system exactly and stops after one Newton iteration,
-the device runs Jacobi-preconditioned BiCGSTAB to 1e-8 and iterates until the residual max norm is
-below tol_nonlin, as the reference's Newton rule for a linear problem asks."""
+the device runs Jacobi-preconditioned BiCGSTAB to a relative 1e-12 and iterates until the residual
+max norm is below tol_nonlin, as the reference's Newton rule for a linear problem asks; what is
+left is the flow's own per-step difference (1e-13 to 1e-10) carried by the transport."""
 import numpy as np
 import pytest
 
@@ -93,7 +94,7 @@ def test_transport_runs_match_reference(name, transport_ref):
         for j in range(len(m.constituents)):
             e = relerr(g.get_conc(j), con[k, j])
             worst = max(worst, e)
-            assert e <= 1e-8, (name, k, j, e)
+            assert e <= 1e-9, (name, k, j, e)
     print(f"{name}: worst per-step relative concentration error against the reference {worst:.2e}")
 
 
@@ -116,7 +117,7 @@ def test_run_steps_flow_then_transport():
         assert o.step()["status"] == 0
         o.transport_step()
     for j in range(2):
-        assert relerr(g.get_conc(j), o.get_conc(j)) <= 1e-8
+        assert relerr(g.get_conc(j), o.get_conc(j)) <= 1e-9
 
 
 def test_remesh_keeps_the_concentrations():
