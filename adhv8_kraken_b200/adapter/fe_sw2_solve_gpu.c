@@ -31,6 +31,14 @@
  * with -Wl,--wrap=ssw_2d_calculate_elem_error: __wrap_ssw_2d_calculate_elem_error below takes
  * it from the state the device step just produced, and hands over to the host routine
  * whenever the device does not hold that state (before the first GPU step, after a failed one).
+ *
+ * The transport of general constituents (fe_transport, src/fe/transport/fe_transport.c:31-113,
+ * called by fe_main right after the flow, src/fe/fe_main.c:528-531) runs on the device too when
+ * the reference is linked with -Wl,--wrap=fe_transport: fe_transport_gpu below solves every
+ * constituent on the flow step the device just produced, with the host's concentration levels
+ * handed over and read back like the flow's.  Models the library does not transport (sediment,
+ * the vorticity constituent, transport-load edges, 3D grids, a flow state not on the device) go to
+ * the reference's own fe_transport, which reads the side output this binding copies back.
  */
 #include "global_header.h"
 #include "sw2gpu.h"
@@ -47,6 +55,9 @@ typedef struct {
     double *wsx, *wsy;      /* [nnodes] nodal wind values of the coming step */
     double *rxx, *rxy, *ryy;  /* [nnodes] nodal wave radiation stresses (wave runs only) */
     int state_on_device;    /* the host's current and old levels are the device's (last step accepted) */
+    int trn_ready;          /* the constituents are set up on the device (sw2gpu_set_transport) */
+    double *c;              /* staging of one concentration level */
+    sw2gpu_stats *tstats;   /* [ntransport] */
 } GPU_SW2;
 
 static GPU_SW2 gpu;
@@ -86,7 +97,7 @@ static void gpu_release(void) {
     if (gpu.ctx) sw2gpu_destroy(gpu.ctx);
     free(gpu.h); free(gpu.u); free(gpu.v); free(gpu.series); free(gpu.mat_of);
     free(gpu.wind_flag); free(gpu.wind_att); free(gpu.wsx); free(gpu.wsy);
-    free(gpu.rxx); free(gpu.rxy); free(gpu.ryy);
+    free(gpu.rxx); free(gpu.rxy); free(gpu.ryy); free(gpu.c); free(gpu.tstats);
     memset(&gpu, 0, sizeof gpu);
 }
 
@@ -332,6 +343,106 @@ void __wrap_ssw_2d_calculate_elem_error(SSW_2D *sw, SGRID *grid, SMAT *mat, doub
     if (sw2gpu_elem_error(gpu.ctx, tol, grid->elem_error, sw->error) != SW2GPU_OK) gpu_fail("sw2gpu_elem_error");
     free(tol);
 }
+
+/* ---- constituent transport ---- */
+
+int __real_fe_transport(SSUPER_MODEL *sm, int isubModel);
+
+static int transport_on_device(SMODEL *mod) {
+    int k, i;
+    if (!gpu.ctx || !gpu.state_on_device || mod->grid->ndim != 2 || mod->grid->nnodes != gpu.nnodes ||
+        mod->grid->nelems2d != gpu.nelems2d || mod->flag.VORTICITY == ON || mod->is_sediment_running ||
+        mod->nstring != gpu.nstring)
+        return 0;
+    for (k = 0; k < mod->ntransport; k++)
+        if (mod->con[k].type != CON) return 0;
+    for (i = 0; i < mod->grid->nelems1d; i++) {   /* a transport load edge (BCT_NEU_LOAD, :259-272) */
+        const int s = mod->grid->elem1d[i].string;
+        if (s >= 0 && s < mod->nstring && mod->str_values[s].ol_flow.bc_flag == BCT_NEU_LOAD) return 0;
+    }
+    return 1;
+}
+
+/* the constituents as the library takes them: property[0], MP DF per material string (the
+ * library's material table, gpu_prepare), and per string the DB TRN / NB TRN flag and series */
+static void transport_setup(SMODEL *mod) {
+    const int n = mod->ntransport, S = gpu.nstring;
+    int k, s;
+    double *refc = malloc((n + 1) * sizeof(double)), *dm = malloc(((size_t) n * S + 1) * sizeof(double));
+    int32_t *bc = malloc(((size_t) n * S + 1) * sizeof(int32_t)), *ser = malloc(((size_t) n * S + 1) * sizeof(int32_t));
+    for (k = 0; k < n; k++) {
+        refc[k] = mod->con[k].property[0];
+        for (s = 0; s < S; s++) {
+            const INPUT_DATA *in = &(mod->str_values[s].trans[k]);
+            dm[(size_t) k * S + s] = gpu.mat_of[s] >= 0 ? mod->mat[gpu.mat_of[s]].trn[k].d_m : 0.0;
+            bc[(size_t) k * S + s] = in->bc_flag == BCT_DIR ? SW2GPU_BCT_DIR : in->bc_flag == BCT_NEU ? SW2GPU_BCT_NEU : 0;
+            ser[(size_t) k * S + s] = in->bc_flag == BCT_DIR ? in->iu_0 : in->bc_flag == BCT_NEU ? in->isigma : -1;
+        }
+    }
+    sw2gpu_transport t = {n, refc, dm, bc, ser};
+    if (sw2gpu_set_transport(gpu.ctx, &t) != SW2GPU_OK) gpu_fail("sw2gpu_set_transport");
+    free(refc); free(dm); free(bc); free(ser);
+    gpu.c = realloc(gpu.c, (gpu.nnodes + 1) * sizeof(double));
+    gpu.tstats = realloc(gpu.tstats, (n + 1) * sizeof(sw2gpu_stats));
+    gpu.trn_ready = 1;
+}
+
+int fe_transport_gpu(SSUPER_MODEL *sm, int isubModel) {
+    SMODEL *mod = &(sm->submodel[isubModel]);
+    const int V = gpu.nnodes;
+    int k, i;
+    if (!transport_on_device(mod)) return __real_fe_transport(sm, isubModel);
+    if (!gpu.trn_ready) transport_setup(mod);
+    mod->nsys = 1; sm->nsys = 1;                       /* fe_transport.c:40-44 */
+    mod->nsys_sq = 1; sm->nsys_sq = 1;
+    sm->solver_info.refresh = YES;
+    sm->solver_info.LINEAR_PROBLEM = YES;
+    /* the device shifts each constituent's levels itself: the host's current level goes in as the
+     * device's current one and its old level as the device's old one */
+    for (k = 0; k < mod->ntransport; k++) {
+        if (sw2gpu_set_conc(gpu.ctx, k, 0, mod->con[k].concentration) != SW2GPU_OK ||
+            sw2gpu_set_conc(gpu.ctx, k, 1, mod->con[k].old_concentration) != SW2GPU_OK)
+            gpu_fail("sw2gpu_set_conc");
+    }
+    memset(gpu.tstats, 0, mod->ntransport * sizeof(sw2gpu_stats));
+    const int rc = sw2gpu_transport_step(gpu.ctx, gpu.series, gpu.tstats);
+    if (rc != SW2GPU_OK && rc != SW2GPU_E_NEWTON && rc != SW2GPU_E_LINEAR && rc != SW2GPU_E_NAN)
+        gpu_fail("sw2gpu_transport_step");
+    /* the constituents up to the first that failed were shifted and solved (or reset) on the
+     * device, those after it not at all, as fe_transport returns at the first failure: the host
+     * levels follow, older <- old, old <- current (fe_transport.c:60-61), then the new current */
+    int last = mod->ntransport - 1;
+    if (rc != SW2GPU_OK)
+        for (k = 0; k < mod->ntransport; k++)
+            if (gpu.tstats[k].status != SW2GPU_OK) { last = k; break; }
+    for (k = 0; k <= last; k++) {
+        sarray_copy_dbl(mod->con[k].older_concentration, mod->con[k].old_concentration, V);
+        sarray_copy_dbl(mod->con[k].old_concentration, mod->con[k].concentration, V);
+        if (sw2gpu_get_conc(gpu.ctx, k, 0, gpu.c) != SW2GPU_OK) gpu_fail("sw2gpu_get_conc");
+        for (i = 0; i < V; i++) mod->con[k].concentration[i] = gpu.c[i];
+        sm->solver_info.it_count_nonlin += gpu.tstats[k].newton_its;
+    }
+    sm->solver_info.PRN_NEWTON = OFF;
+    if (rc == SW2GPU_OK) {
+        /* the adaption error indicator of the constituents (fe_transport.c:83-88), host routine */
+        SVECT2D *vel2d = mod->flag.SW_FLOW == ON ? mod->sw->d2->vel : mod->ns->d2->vel;
+        scon_calculate_elem2d_error(mod->ntransport, mod->con, vel2d, mod->sw->d2->head, mod->grid, mod->mat, mod->dt);
+        return YES;
+    }
+    /* a failed constituent (fe_newton.c:854-892): its current level already reset by the device
+     * (fe_transport_init), dt * DT_REDUCE_FACTOR and every submodel told */
+    sm->solver_info.it_count_nonlin_failed += gpu.tstats[last].newton_its;
+    if (sm->solver_info.force_nonlin_it == YES) return YES;
+    tc_scale(&sm->dt);
+    for (i = 0; i < sm->nsubmodels; i++) {
+        sm->submodel[i].dt = sm->dt;
+        if (sm->submodel[i].proc_flag == 1) sm->submodel[i].flag.TIME_ADAPT_FAIL = YES;
+    }
+    return NO;
+}
+
+/* the linker's --wrap=fe_transport binding */
+int __wrap_fe_transport(SSUPER_MODEL *sm, int isubModel) { return fe_transport_gpu(sm, isubModel); }
 
 /* the linker's --wrap=fe_sw2_solve binding */
 int __wrap_fe_sw2_solve(SSUPER_MODEL *sm, int isubModel) { return fe_sw2_solve_gpu(sm, isubModel); }

@@ -2394,9 +2394,33 @@ int trn_step_one(sw2gpu_ctx* c, int k, const double* series, sw2gpu_stats* st) {
     lv[1] = lv[0];
     lv[0] = o2;
     int rc, launches = 0;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
+    // phase timers: event pairs around the Jacobian (0), Krylov (1) and residual (2) launches
+    std::vector<cudaEvent_t> evs;
+    std::vector<int> kinds;
+    auto ev = [&]() -> cudaEvent_t {   // pushed even when creation failed: pairs stay in step
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) e = nullptr;
+        evs.push_back(e);
+        return e;
+    };
+    auto phase_begin = [&](int kind) {
+        kinds.push_back(kind);
+        cudaEvent_t e = ev();
+        if (e) cudaEventRecord(e, c->stream);
+    };
+    auto phase_end = [&]() {
+        cudaEvent_t e = ev();
+        if (e) cudaEventRecord(e, c->stream);
+    };
+    struct Release {
+        std::vector<cudaEvent_t>& v;
+        ~Release() {
+            for (cudaEvent_t e : v)
+                if (e) cudaEventDestroy(e);
+        }
+    } release{evs};
+    cudaEvent_t e0 = ev(), e1 = nullptr;
+    if (!e0) return fail(SW2GPU_E_CUDA, "cudaEventCreate failed");
     CK(cudaEventRecord(e0, c->stream));
     if ((rc = trn_upload_series(c, k, series))) return rc;
     const TrnArgs A = trn_args(c, k);
@@ -2404,17 +2428,34 @@ int trn_step_one(sw2gpu_ctx* c, int k, const double* series, sw2gpu_stats* st) {
     if ((rc = trn_init(c, A))) return rc;
     launches++;
     Norms nr;
-    if ((rc = trn_resid(c, A, nr, launches))) return rc;
+    phase_begin(2);
+    auto resid = [&](Norms& out) {   // the residual phase ends before its host wait
+        k_trn_elem<false><<<nblk(c->T + c->E, kTrnThreads), kTrnThreads, 0, c->stream>>>(A);
+        k_trn_resid_gather<<<nblk(c->V, kGatherThreads), kGatherThreads, 0, c->stream>>>(A);
+        phase_end();
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(c->tnorms_h, c->tnorms.p, sizeof(Norms), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        out = *c->tnorms_h;
+        launches += 2;
+        return 0;
+    };
+    if ((rc = resid(nr))) return rc;
     const bool lin_test = P.tol_nonlin > kSmall;
     int it = 0, lin_total = 0, cuts_total = 0, status = SW2GPU_OK;
     bool solv_ok = true, nan_flag = false, timeout = false;
     double rl2 = sqrt(nr.l2sum / c->V);
     for (;;) {
+        phase_begin(0);
         if ((rc = trn_load(c, A, launches))) return rc;
+        phase_end();
+        phase_begin(1);
         if ((rc = trn_krylov(c, launches))) return rc;
+        phase_end();
         if ((rc = trn_inc(c, k, 0, launches))) return rc;
         const double old_l2 = rl2;
-        if ((rc = trn_resid(c, A, nr, launches))) return rc;   // also brings the Krylov outcome
+        phase_begin(2);
+        if ((rc = resid(nr))) return rc;   // also brings the Krylov outcome
         const KrylovCtl kc = *c->tctl_h;
         if (kc.err) {
             timeout = true;
@@ -2430,7 +2471,8 @@ int trn_step_one(sw2gpu_ctx* c, int k, const double* series, sw2gpu_stats* st) {
         int cuts = 0;
         while (nr.rmax > P.tol_nonlin && rl2 > old_l2 && cuts < P.max_linesearch_cuts) {
             if ((rc = trn_inc(c, k, 1, launches))) return rc;
-            if ((rc = trn_resid(c, A, nr, launches))) return rc;
+            phase_begin(2);
+            if ((rc = resid(nr))) return rc;
             rl2 = sqrt(nr.l2sum / c->V);
             cuts++;
         }
@@ -2446,12 +2488,19 @@ int trn_step_one(sw2gpu_ctx* c, int k, const double* series, sw2gpu_stats* st) {
         if ((rc = trn_init(c, A))) return rc;
         launches++;
     }
+    e1 = ev();
+    if (!e1) return fail(SW2GPU_E_CUDA, "cudaEventCreate failed");
     CK(cudaEventRecord(e1, c->stream));
     CK(cudaEventSynchronize(e1));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    double ph[3] = {0.0, 0.0, 0.0};
+    for (size_t q = 0; q < kinds.size(); q++) {   // pairs follow e0 in the event list
+        float t = 0.f;
+        if (2 + 2 * q < evs.size() && evs[1 + 2 * q] && evs[2 + 2 * q] &&
+            cudaEventElapsedTime(&t, evs[1 + 2 * q], evs[2 + 2 * q]) == cudaSuccess)
+            ph[kinds[q]] += t;
+    }
     if (st) {
         memset(st, 0, sizeof(*st));
         st->status = status;
@@ -2463,6 +2512,10 @@ int trn_step_one(sw2gpu_ctx* c, int k, const double* series, sw2gpu_stats* st) {
         st->inc_max = nr.imax;
         st->device_ms = ms;
         st->kernel_launches = launches;
+        st->jac_ms = ph[0];
+        st->krylov_ms = ph[1];
+        st->resid_ms = ph[2];
+        st->other_ms = ms - ph[0] - ph[1] - ph[2];
     }
     return status;
 }

@@ -317,7 +317,7 @@ def ensemble_member(seed: int, tri_lo: float = 5e3, tri_hi: float = 2e5, nsteps:
 # ---------------------------------------------------------------------------------------------
 # constituent transport workloads (fe_transport after every flow step)
 
-def _const_series(m: SW2Model, value: float) -> int:
+def const_series(m: SW2Model, value: float) -> int:
     """Appends a constant series to the model; returns its id."""
     t_end = m.t0 + (m.nsteps + 10) * m.dt
     m.series = list(m.series) + [Series(np.array([m.t0, t_end]), np.array([value, value]))]
@@ -330,7 +330,7 @@ def channel_transport(nsteps: int = 6, nx: int = 100, ny: int = 20) -> SW2Model:
     diffusion d_m = 0.5 m^2/s."""
     from .model import Constituent
     m = channel(nx=nx, ny=ny, nsteps=nsteps, name="trn_channel")
-    ser = _const_series(m, 2.0)
+    ser = const_series(m, 2.0)
     m.strings = list(m.strings) + [StringSpec("node")]
     sid = len(m.strings) - 1
     node_string = m.node_string.copy()
@@ -349,7 +349,7 @@ def basin_transport(nsteps: int = 8, nbins: int = 3) -> SW2Model:
     diffusion, no boundary condition) starts as a smooth field."""
     from .model import Constituent
     m = bumpy_basin(700, seed=11, size=2000.0, nsteps=nsteps, dt=5.0, nbins=nbins, name="trn_basin")
-    s_in, s_out = _const_series(m, 3.0), _const_series(m, 0.5)
+    s_in, s_out = const_series(m, 3.0), const_series(m, 0.5)
     e_in, e_out = nbins, nbins + 1
     c0 = 0.5 + 0.4 * np.sin(m.x / 300.0) * np.cos(m.y / 250.0)
     m.constituents = [Constituent(ref_conc=2.0, diffusion=[0.1, 1.0, 3.0][:nbins], edge_bc={e_in: s_in, e_out: s_out},
@@ -365,7 +365,7 @@ def terms_transport(nsteps: int = 6) -> SW2Model:
     from .model import Constituent
     m = basin_all_terms(nsteps=nsteps)
     m.name = "trn_terms"
-    s_in = _const_series(m, 1.0)
+    s_in = const_series(m, 1.0)
     nmat = len(m.materials)
     m.constituents = [Constituent(ref_conc=1.0, diffusion=[2.0, 0.0, 0.0, 0.0], edge_bc={nmat: s_in},
                                   c0=0.2 + 0.1 * np.cos(m.y / 200.0))]
@@ -378,7 +378,7 @@ def outflow_transport(nsteps: int = 6) -> SW2Model:
     from .model import Constituent
     m = channel_outflow(nsteps=nsteps)
     m.name = "trn_outflow"
-    s_in = _const_series(m, 0.8)
+    s_in = const_series(m, 0.8)
     m.constituents = [Constituent(ref_conc=1.0, diffusion=[1.0], edge_bc={1: s_in}, c0=m.x / 1000.0)]
     return m
 
@@ -392,7 +392,7 @@ def salt_transport(nsteps: int = 6) -> SW2Model:
     provides; it holds where the flow is wet everywhere."""
     from .model import Constituent
     m = channel(nsteps=nsteps, name="trn_salt")
-    s = _const_series(m, 17.5)
+    s = const_series(m, 17.5)
     m.constituents = [Constituent(ref_conc=1.0, diffusion=[1.0], edge_bc={1: s, 2: s},
                                   c0=np.full(m.nnodes, 17.5))]
     return m

@@ -16,6 +16,9 @@ ramping 1 -> 5 m^2/s over 30 steps, dt = 5 s.  Data are synthetic (no dataset ex
   advances its levels by rotating its buffers).
 * ``mixed``  -- the mixed-precision path on the same workload (FP32 Jacobian storage,
   SpMV and preconditioner inside the FP64 Newton loop) with its error against the FP64 run.
+* ``transport`` -- the same basin carrying one general constituent: the flow step then the
+  transport step (fe_transport) every step, the transport's phases and the roofline of its
+  Krylov kernel.
 * ``roofline`` -- the dominant kernel (largest device time in the timed region).
 * ``cpu_baseline`` -- the reference AdH executable built from its own sources
   (``oracle/_ref``), timed on this host's cores on a bounded sample.
@@ -513,6 +516,73 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def transport_model(points: int, nsteps: int):
+    """The benchmark basin carrying one general constituent: 0.3 everywhere at the start, entering
+    at 1.0 with the inflow (NB TRN), diffusion 0.5 m^2/s on every material (MP DF)."""
+    from adhv8_kraken_b200 import meshgen
+    from adhv8_kraken_b200.model import Constituent
+    m = basin_model(points, nsteps)
+    ser = meshgen.const_series(m, 1.0)
+    nmat = len(m.materials)
+    m.constituents = [Constituent(ref_conc=1.0, diffusion=[0.5] * nmat, edge_bc={nmat: ser},
+                                  c0=np.full(m.nnodes, 0.3))]
+    return m
+
+
+def run_transport(args, stream, variant, hbm, src):
+    """Flow and transport steps on the benchmark basin with one constituent: triangle-steps/s of
+    both, the transport's share and phases, and the roofline of the transport Krylov kernel
+    (k_trn_bicgstab).  Its algorithmic bytes per iteration: two sweeps over the off-diagonal
+    pattern (8 B value + 4 B column per entry, 4 B row pointer per row) and 19 vector streams of one
+    double per node (sweep 1: r, q, rhat in, p, v out; alpha step: r, v in, s out; sweep 2: s in,
+    t out; update: x, p, s, t, v, rhat in, x, r, q out)."""
+    import torch
+    from adhv8_kraken_b200 import capi
+    from adhv8_kraken_b200.sw2 import SW2GPU
+    m = transport_model(args.points, args.warmup + args.steps + 8)
+    T, V = m.nelems2d, m.nnodes
+    g = SW2GPU(m, precision=capi.SW2GPU_FP64, stream=stream.cuda_stream)
+    g.set_variant(*variant)
+    for _ in range(args.warmup):
+        assert g.step()["status"] == 0
+        assert g.transport_step()[0]["status"] == 0
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fl, tr = [], []
+    e0.record(stream)
+    for _ in range(args.steps):
+        fl.append(g.step())
+        tr.append(g.transport_step()[0])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    assert all(s["status"] == 0 for s in fl + tr)
+    c = g.get_conc(0)
+    nnzb = g.nnzb
+    g.close()
+    k = args.steps
+    kry = sum(t["krylov_ms"] for t in tr)
+    lin = sum(t["linear_its"] for t in tr)
+    iter_bytes = 2 * ((nnzb - V) * 12 + (V + 1) * 4) + 19 * 8 * V
+    achieved = iter_bytes * lin / (kry * 1e-3) / 1e9 if kry > 0 else None
+    return {"workload": f"the benchmark basin ({T} triangles) with one constituent (NB TRN inflow 1.0, "
+                        f"MP DF 0.5, 0.3 initially), flow then transport every step, dt 5 s",
+            "value": T * k / (ms * 1e-3), "unit": "triangle-steps/s", "ms_per_step": ms / k,
+            "flow_ms_per_step": sum(f["device_ms"] for f in fl) / k,
+            "transport_ms_per_step": sum(t["device_ms"] for t in tr) / k,
+            "transport_newton_its_per_step": sum(t["newton_its"] for t in tr) / k,
+            "transport_krylov_its_per_step": lin / k,
+            "transport_phase_ms_per_step": {"jacobian": sum(t["jac_ms"] for t in tr) / k, "krylov": kry / k,
+                                            "residual": sum(t["resid_ms"] for t in tr) / k,
+                                            "other": sum(t["other_ms"] for t in tr) / k},
+            "transport_launches_per_step": sum(t["kernel_launches"] for t in tr) / k,
+            "krylov_roofline": {"kernel": "k_trn_bicgstab", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                                "unit": "GB/s", "frac": achieved / hbm if achieved else None, "peak_source": src,
+                                "algorithmic_bytes_per_iteration": iter_bytes,
+                                "us_per_iteration": 1e3 * kry / max(lin, 1)},
+            "conc_range": [float(c.min()), float(c.max())]}
+
+
 def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
     import torch
     import torch.distributed as dist
@@ -651,6 +721,9 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
              "max_rel_err_vs_fp64": err, "newton_its": sum(s["newton_its"] for s in mstats),
              "linear_its": sum(s["linear_its"] for s in mstats)}
 
+    # ---- constituent transport on the same workload (fe_transport after every flow step)
+    transport = run_transport(args, stream, variant64, hbm, src) if world == 1 else None
+
     # ---- batched ensemble (plain FP64 alone vs batched FP64 vs batched mixed)
     batched = None
     if ens_models:
@@ -694,6 +767,7 @@ def run_ours(args, rank, world, local_rank, ens_models=None, serve=None):
         "roofline": roofline,
         "e2e": e2e,
         "mixed": mixed,
+        "transport": transport,
         "small": small,
         "config3": config3,
         "batched": batched,

@@ -24,10 +24,10 @@ of the reference tree and its build system is not used; the recipe is:
    ``--wrap=fe_main --wrap=fe_sw2_load --wrap=fe_transport_load`` into ``oracle/_ref/adh_dump``.
 4. The same objects, the same harness and the drop-in binding of the B200 library
    (``adhv8_kraken_b200/adapter/fe_sw2_solve_gpu.c``, compiled against the reference's own
-   headers) are linked with ``--wrap=fe_sw2_solve --wrap=ssw_2d_calculate_elem_error`` against
-   ``libsw2gpu.so`` into
-   ``oracle/_ref/adh_gpu``: the reference's own executable and time loop with its SW2 solve
-   replaced by the GPU step.  Only where the library is built.
+   headers) are linked with ``--wrap=fe_sw2_solve --wrap=ssw_2d_calculate_elem_error
+   --wrap=fe_transport`` against ``libsw2gpu.so`` into ``oracle/_ref/adh_gpu``: the reference's
+   own executable and time loop with its SW2 solve and its constituent transport replaced by the
+   GPU's.  Only where the library is built.
 5. The reference's SW2 QA decks that run on triangles (``qa/sw2/<case>/tri``: mesh, boundary
    cards, hot start and the stored ``error.out.last``) are staged into ``oracle/_ref/qa`` so
    that the drop-in can run them where the reference tree is absent.
@@ -164,7 +164,8 @@ def build_gpu_harness(flags, objs, hobj, stub, lib) -> str:
     subprocess.run(["gcc", "-fcommon", "-o", GPU_EXE] + objs + [hobj, aobj, stub, f"-L{libdir}", "-lsw2gpu", "-lm",
                     f"-Wl,-rpath,{rpath}", "-Wl,--wrap=fe_main", "-Wl,--wrap=fe_sw2_load",
                     "-Wl,--wrap=fe_transport_load",
-                    "-Wl,--wrap=fe_sw2_solve", "-Wl,--wrap=ssw_2d_calculate_elem_error"], check=True)
+                    "-Wl,--wrap=fe_sw2_solve", "-Wl,--wrap=ssw_2d_calculate_elem_error", "-Wl,--wrap=fe_transport"],
+                   check=True)
     return GPU_EXE
 
 

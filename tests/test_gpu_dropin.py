@@ -172,3 +172,23 @@ def test_retry_path_through_the_reference_time_loop_matches_the_reference():
     print(f"spike: {len(gpu_steps)} steps, {sum(s['attempts'] for s in gpu_steps)} attempts, worst per-step "
           f"error h {worst['h']:.2e} q {worst['q']:.2e}")
 
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["channel_transport", "basin_transport", "terms_transport"])
+def test_transport_dropin_follows_the_reference(case):
+    """The reference's time loop with its flow and its constituent transport on the device
+    (fe_transport bound by --wrap=fe_transport to the library's transport step): the same accepted
+    steps as the unmodified reference and every constituent's concentration within 1e-9 of the
+    field's maximum after every step (the flow's own per-step differences, carried)."""
+    from adhv8_kraken_b200 import meshgen
+    from conftest import relerr
+    m = getattr(meshgen, case)()
+    ref_steps, _, _, _ = _run(CPU_EXE, case, model=m)
+    gpu_steps, _, _, _ = _run(GPU_EXE, case, model=m)
+    assert len(gpu_steps) == len(ref_steps) == m.nsteps
+    for k, (a, b) in enumerate(zip(gpu_steps, ref_steps)):
+        assert a["attempts"] == b["attempts"] == 1
+        assert len(a["con"]) == len(b["con"]) == len(m.constituents)
+        for j in range(len(m.constituents)):
+            assert relerr(a["con"][j], b["con"][j]) <= 1e-9, (case, k, j)

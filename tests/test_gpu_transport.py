@@ -138,7 +138,7 @@ def test_remesh_keeps_the_concentrations():
 
 def _transport_basin(n=10000, seed=23, nsteps=4):
     m = meshgen.bumpy_basin(n, seed=seed, size=20000.0 * np.sqrt(n / 5e5), nsteps=nsteps, dt=5.0, name="trn_big")
-    ser = meshgen._const_series(m, 1.0)
+    ser = meshgen.const_series(m, 1.0)
     m.constituents = [Constituent(ref_conc=1.0, diffusion=[0.5] * len(m.materials), edge_bc={len(m.materials): ser},
                                   c0=np.full(m.nnodes, 0.3))]
     return m
