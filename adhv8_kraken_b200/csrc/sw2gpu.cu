@@ -2240,10 +2240,11 @@ int sw2gpu_set_transport(sw2gpu_ctx* c, const sw2gpu_transport* t) {
         int dev = 0, sms = 0, per_sm = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trn_bicgstab, kTrnKThreads, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trn_bicgstab<kTrnKThreads>, kTrnKThreads, 0));
         // at most the co-resident CTAs (a cooperative launch), at least 512 rows each
         c->trn_kgrid = std::max(1, std::min(sms * std::max(per_sm, 1), V / 512));
-        rc |= zalloc(c->tkpart, 9ull * c->trn_kgrid, st);
+        if (per_sm < 1) return fail(SW2GPU_E_CUDA, "the transport Krylov kernel does not fit on an SM");
+        rc |= zalloc(c->tkpart, 12ull * c->trn_kgrid, st);
         if (!c->tnorms_h) CK(cudaMallocHost(&c->tnorms_h, sizeof(Norms)));
         if (!c->tctl_h) CK(cudaMallocHost(&c->tctl_h, sizeof(KrylovCtl)));
         if (!c->tsval_h) CK(cudaMallocHost(&c->tsval_h, sizeof(double) * std::max(S, 1)));
@@ -2369,7 +2370,7 @@ int trn_krylov(sw2gpu_ctx* c, int& launches) {
     K.spin_limit = c->wait_barrier;
     CK(cudaMemsetAsync(c->tctl.p, 0, sizeof(KrylovCtl), c->stream));
     void* args[] = {&K};
-    CK(cudaLaunchCooperativeKernel((void*)k_trn_bicgstab, dim3(c->trn_kgrid), dim3(kTrnKThreads), args, 0,
+    CK(cudaLaunchCooperativeKernel((void*)k_trn_bicgstab<kTrnKThreads>, dim3(c->trn_kgrid), dim3(kTrnKThreads), args, 0,
                                    c->stream));
     CK(cudaMemcpyAsync(c->tctl_h, c->tctl.p, sizeof(KrylovCtl), cudaMemcpyDeviceToHost, c->stream));
     launches += 1;

@@ -277,12 +277,19 @@ __global__ void __launch_bounds__(kTrnThreads) k_trn_inc(double* __restrict__ c,
 // iterations.  CTA b owns a contiguous range of rows.  Every dot product and norm is reduced in
 // a fixed order: per-CTA partials (a fixed warp tree) to global slots, then after the grid
 // barrier every CTA sums the slots in CTA order with one warp, so all CTAs hold the same bits.
-// Four grid barriers per iteration: the next direction p = r + beta q (q = p - omega v, formed
-// with the update) needs no barrier of its own because v = A'r + beta A'q is formed from r and q.
+// Three grid barriers per iteration, one per reduction, and none for a product's input alone:
+//   sweep 1  p = r + beta q, Ar = A'r, v = Ar + beta A'q   (A'p without p complete; q = p - omega v)
+//            rhat.v                                         -- barrier
+//   sweep 2  s = r - alpha v, t = Ar - alpha A'v            (A's without s complete)
+//            t.s, t.t, rhat.s, rhat.t                       -- barrier
+//   update   x += alpha p + omega s, r = s - omega t, q = p - omega v, max |r|
+//            (rhat.r_new = rhat.s - omega rhat.t comes with the sweep-2 sums)  -- barrier
 // The barriers are bounded (grid_sync): a wait that runs out sets ctl->err and every CTA returns.
-constexpr int kTrnKThreads = 256;
+// one CTA of 1024 threads per SM (measured on the 1M-triangle basin: 43 us per iteration, against
+// 47-52 us for 256- and 512-thread CTAs at one to four per SM)
+constexpr int kTrnKThreads = 1024;
 constexpr double kTrnKrylovRtol = 1e-12;   // relative stop of the transport Krylov solve (at most)
-constexpr int kTrnKVectors = 7;   // r, rhat, p, v, s, t, q
+constexpr int kTrnKVectors = 8;   // r, rhat, p, v, s, t, q, Ar
 
 struct TrnKrylovArgs {
     int V;
@@ -303,11 +310,24 @@ __device__ __forceinline__ double trn_amult(const TrnKrylovArgs& K, const double
     for (int k = K.orowptr[i]; k < K.orowptr[i + 1]; k++) s += K.aoff[k] * y[K.ocol[k]];
     return s;
 }
+// A'y and A'z at row i in one pass over the row
+__device__ __forceinline__ void trn_amult2(const TrnKrylovArgs& K, const double* __restrict__ y,
+                                           const double* __restrict__ z, int i, double& ay, double& az) {
+    double a = y[i], b = z[i];
+    for (int k = K.orowptr[i]; k < K.orowptr[i + 1]; k++) {
+        const double w = K.aoff[k];
+        const int j = K.ocol[k];
+        a += w * y[j];
+        b += w * z[j];
+    }
+    ay = a;
+    az = b;
+}
 
-// fixed-order CTA reduction of up to three values into slot[0..2][blockIdx.x] (max for `ismax`)
-template <int NV>
+// fixed-order CTA reduction of up to four values into slot[q][blockIdx.x] (max for `ismax`)
+template <int THREADS, int NV>
 __device__ __forceinline__ void trn_cta_reduce(double (&a)[NV], const bool (&ismax)[NV], double* slot, int nb) {
-    __shared__ double red[kTrnKThreads / 32][3];
+    __shared__ double red[THREADS / 32][4];
 #pragma unroll
     for (int q = 0; q < NV; q++)
 #pragma unroll
@@ -324,7 +344,7 @@ __device__ __forceinline__ void trn_cta_reduce(double (&a)[NV], const bool (&ism
 #pragma unroll
         for (int q = 0; q < NV; q++) {
             double s = red[0][q];
-            for (int w = 1; w < kTrnKThreads / 32; w++) s = ismax[q] ? fmax(s, red[w][q]) : s + red[w][q];
+            for (int w = 1; w < THREADS / 32; w++) s = ismax[q] ? fmax(s, red[w][q]) : s + red[w][q];
             slot[(size_t)q * nb + blockIdx.x] = s;
         }
     }
@@ -333,7 +353,7 @@ __device__ __forceinline__ void trn_cta_reduce(double (&a)[NV], const bool (&ism
 // every CTA: the global values of the slots (lane-strided partial sums, then a fixed xor tree)
 template <int NV>
 __device__ __forceinline__ void trn_grid_values(const double* slot, const bool (&ismax)[NV], int nb, double (&g)[NV]) {
-    __shared__ double out[3];
+    __shared__ double out[4];
     if (threadIdx.x < 32) {
 #pragma unroll
         for (int q = 0; q < NV; q++) {
@@ -356,91 +376,105 @@ __device__ __forceinline__ void trn_grid_values(const double* slot, const bool (
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kTrnKThreads) k_trn_bicgstab(const __grid_constant__ TrnKrylovArgs K) {
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) k_trn_bicgstab(const __grid_constant__ TrnKrylovArgs K) {
     const int nb = gridDim.x;
     const int V = K.V;
     const int r0 = (int)((long long)V * blockIdx.x / nb), r1 = (int)((long long)V * (blockIdx.x + 1) / nb);
     double *r = K.vec[0], *rh = K.vec[1], *p = K.vec[2], *v = K.vec[3], *s = K.vec[4], *t = K.vec[5],
-           *q = K.vec[6];
+           *q = K.vec[6], *ar = K.vec[7];
     double* slotA = K.part;                    // rhat . v
-    double* slotB = K.part + 3 * (size_t)nb;   // t . s, t . t
-    double* slotC = K.part + 6 * (size_t)nb;   // rhat . r, max |r| (also the start's max |b'|)
+    double* slotB = K.part + 4 * (size_t)nb;   // t . s, t . t, rhat . s, rhat . t
+    double* slotC = K.part + 8 * (size_t)nb;   // max |r| (at the start: rhat . r, max |b'|)
     const long long lim = K.spin_limit > 0 ? K.spin_limit : kBarrierSpinLimit;
     unsigned epoch = 0;
     // start: r = b' = D^-1 R, rhat = r, x = 0, q = 0
-    double acc[2] = {0.0, 0.0};
-    const bool mC[2] = {false, true};
-    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-        const double b = K.dinv[i] * K.R[i];
-        r[i] = b;
-        rh[i] = b;
-        K.x[i] = 0.0;
-        q[i] = 0.0;
-        acc[0] += b * b;
-        acc[1] = fmax(acc[1], fabs(b));
+    {
+        double acc[2] = {0.0, 0.0};
+        const bool m0[2] = {false, true};
+        for (int i = r0 + threadIdx.x; i < r1; i += THREADS) {
+            const double b = K.dinv[i] * K.R[i];
+            r[i] = b;
+            rh[i] = b;
+            K.x[i] = 0.0;
+            q[i] = 0.0;
+            acc[0] += b * b;
+            acc[1] = fmax(acc[1], fabs(b));
+        }
+        trn_cta_reduce<THREADS, 2>(acc, m0, slotC, nb);
     }
-    trn_cta_reduce<2>(acc, mC, slotC, nb);
     if (!grid_sync(K.ctl, nb, epoch, lim)) return;
-    double g2[2];
-    trn_grid_values<2>(slotC, mC, nb, g2);
-    double rho = g2[0];
-    const double bnorm = g2[1];
-    double rnorm = bnorm, beta = 0.0, alpha = 0.0, omega = 0.0;
+    double rho, bnorm;
+    {
+        double g0[2];
+        const bool m0[2] = {false, true};
+        trn_grid_values<2>(slotC, m0, nb, g0);
+        rho = g0[0];
+        bnorm = g0[1];
+    }
+    double rnorm = bnorm, beta = 0.0;
     const double stop = K.atol + bnorm * K.rtol;
     int it = 0, conv = rnorm <= stop ? 1 : 0;
+    const bool mS1[1] = {false}, mS4[4] = {false, false, false, false}, mM1[1] = {true};
     while (!conv && it < K.max_it) {
-        // p = r + beta q; v = A'r + beta A'q; rhat . v
+        // sweep 1
         double a1[1] = {0.0};
-        const bool m1[1] = {false};
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-            const double ar = trn_amult(K, r, i);
-            const double vv = beta != 0.0 ? ar + beta * trn_amult(K, q, i) : ar;
+        for (int i = r0 + threadIdx.x; i < r1; i += THREADS) {
+            double av, aq = 0.0;
+            if (beta != 0.0) trn_amult2(K, r, q, i, av, aq);
+            else av = trn_amult(K, r, i);
+            const double vv = beta != 0.0 ? av + beta * aq : av;
             p[i] = r[i] + beta * q[i];
+            ar[i] = av;
             v[i] = vv;
             a1[0] += rh[i] * vv;
         }
-        trn_cta_reduce<1>(a1, m1, slotA, nb);
+        trn_cta_reduce<THREADS, 1>(a1, mS1, slotA, nb);
         if (!grid_sync(K.ctl, nb, epoch, lim)) return;
         double g1[1];
-        trn_grid_values<1>(slotA, m1, nb, g1);
+        trn_grid_values<1>(slotA, mS1, nb, g1);
         if (!(g1[0] != 0.0)) break;
-        alpha = rho / g1[0];
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) s[i] = r[i] - alpha * v[i];
-        if (!grid_sync(K.ctl, nb, epoch, lim)) return;
-        // t = A's; t . s, t . t
-        double a2[2] = {0.0, 0.0};
-        const bool m2[2] = {false, false};
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-            const double tt = trn_amult(K, s, i);
+        const double alpha = rho / g1[0];
+        // sweep 2
+        double a2[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = r0 + threadIdx.x; i < r1; i += THREADS) {
+            const double ss = r[i] - alpha * v[i];
+            const double tt = ar[i] - alpha * trn_amult(K, v, i);
+            s[i] = ss;
             t[i] = tt;
-            a2[0] += tt * s[i];
+            const double rr = rh[i];
+            a2[0] += tt * ss;
             a2[1] += tt * tt;
+            a2[2] += rr * ss;
+            a2[3] += rr * tt;
         }
-        trn_cta_reduce<2>(a2, m2, slotB, nb);
+        trn_cta_reduce<THREADS, 4>(a2, mS4, slotB, nb);
         if (!grid_sync(K.ctl, nb, epoch, lim)) return;
-        double gb[2];
-        trn_grid_values<2>(slotB, m2, nb, gb);
-        if (!(gb[1] > 0.0)) break;
-        omega = gb[0] / gb[1];
-        // x += alpha p + omega s; r = s - omega t; q = p - omega v; rhat . r, max |r|
-        double a3[2] = {0.0, 0.0};
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-            K.x[i] += alpha * p[i] + omega * s[i];
-            const double rr = s[i] - omega * t[i];
+        double g2[4];
+        trn_grid_values<4>(slotB, mS4, nb, g2);
+        if (!(g2[1] > 0.0)) break;
+        const double omega = g2[0] / g2[1];
+        const double rho_new = g2[2] - omega * g2[3];
+        // update
+        double a3[1] = {0.0};
+        for (int i = r0 + threadIdx.x; i < r1; i += THREADS) {
+            const double pi = p[i], si = s[i], ti = t[i];
+            K.x[i] += alpha * pi + omega * si;
+            const double rr = si - omega * ti;
             r[i] = rr;
-            q[i] = p[i] - omega * v[i];
-            a3[0] += rh[i] * rr;
-            a3[1] = fmax(a3[1], fabs(rr));
+            q[i] = pi - omega * v[i];
+            a3[0] = fmax(a3[0], fabs(rr));
         }
-        trn_cta_reduce<2>(a3, mC, slotC, nb);
+        trn_cta_reduce<THREADS, 1>(a3, mM1, slotC, nb);
         if (!grid_sync(K.ctl, nb, epoch, lim)) return;
-        trn_grid_values<2>(slotC, mC, nb, g2);
+        double g3[1];
+        trn_grid_values<1>(slotC, mM1, nb, g3);
         it++;
-        rnorm = g2[1];
+        rnorm = g3[0];
         conv = rnorm <= stop ? 1 : 0;
-        if (!(g2[0] != 0.0) || !(omega != 0.0)) break;
-        beta = (g2[0] / rho) * (alpha / omega);
-        rho = g2[0];
+        if (!(rho_new != 0.0) || !(omega != 0.0)) break;
+        beta = (rho_new / rho) * (alpha / omega);
+        rho = rho_new;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         K.ctl->iterations = it;

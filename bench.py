@@ -533,9 +533,9 @@ def run_transport(args, stream, variant, hbm, src):
     """Flow and transport steps on the benchmark basin with one constituent: triangle-steps/s of
     both, the transport's share and phases, and the roofline of the transport Krylov kernel
     (k_trn_bicgstab).  Its algorithmic bytes per iteration: two sweeps over the off-diagonal
-    pattern (8 B value + 4 B column per entry, 4 B row pointer per row) and 19 vector streams of one
-    double per node (sweep 1: r, q, rhat in, p, v out; alpha step: r, v in, s out; sweep 2: s in,
-    t out; update: x, p, s, t, v, rhat in, x, r, q out)."""
+    pattern (8 B value + 4 B column per entry, 4 B row pointer per row) and 20 vector streams of one
+    double per node (sweep 1: r, q, rhat in, p, Ar, v out; sweep 2: r, v, Ar, rhat in, s, t out;
+    update: x, p, s, t, v in, x, r, q out)."""
     import torch
     from adhv8_kraken_b200 import capi
     from adhv8_kraken_b200.sw2 import SW2GPU
@@ -563,7 +563,7 @@ def run_transport(args, stream, variant, hbm, src):
     k = args.steps
     kry = sum(t["krylov_ms"] for t in tr)
     lin = sum(t["linear_its"] for t in tr)
-    iter_bytes = 2 * ((nnzb - V) * 12 + (V + 1) * 4) + 19 * 8 * V
+    iter_bytes = 2 * ((nnzb - V) * 12 + (V + 1) * 4) + 20 * 8 * V
     achieved = iter_bytes * lin / (kry * 1e-3) / 1e9 if kry > 0 else None
     return {"workload": f"the benchmark basin ({T} triangles) with one constituent (NB TRN inflow 1.0, "
                         f"MP DF 0.5, 0.3 initially), flow then transport every step, dt 5 s",
