@@ -2,10 +2,14 @@
 
     python -m adhv8_kraken_b200.run_case --points 500000 --steps 2 [--precision fp64|mixed]
                                          [--variant JAC_MINB,STAGES] [--precond bjacobi|dilu] [--dt S]
+                                         [--constituents N]
 
-One JSON line per step (Newton and Krylov iterations, device time per phase).  This is the
-command the kernel profiles are taken on: it runs the same code path as ``bench.py`` without
-the timing legs around it, so a profiler sees only the steps asked for.
+One JSON line per step (Newton and Krylov iterations, device time per phase; with constituents,
+the transport step's too).  This is the command the kernel profiles are taken on: it runs the
+same code path as ``bench.py`` without the timing legs around it, so a profiler sees only the
+steps asked for.  ``--constituents N`` gives the basin N general constituents as ``bench.py``'s
+transport leg does (0.3 initially, entering at 1.0 with the inflow, MP DF 0.5) and runs the
+transport after every flow step.
 """
 from __future__ import annotations
 
@@ -24,12 +28,20 @@ def main(argv=None):
     ap.add_argument("--dt", type=float, default=5.0)
     ap.add_argument("--variant", default=None,
                     help="launch variant 'jac_minb,stages' (e.g. 1,3); default: the library's own")
+    ap.add_argument("--constituents", type=int, default=0)
     a = ap.parse_args(argv)
+    import numpy as np
     from . import capi, meshgen
+    from .model import Constituent
     from .sw2 import SW2GPU
 
     size = 20000.0 * math.sqrt(a.points / 5e5)
     model = meshgen.bumpy_basin(a.points, seed=a.seed, size=size, nsteps=a.steps, dt=a.dt, name="basin")
+    if a.constituents:
+        ser = meshgen.const_series(model, 1.0)
+        nmat = len(model.materials)
+        model.constituents = [Constituent(ref_conc=1.0, diffusion=[0.5] * nmat, edge_bc={nmat: ser},
+                                          c0=np.full(model.nnodes, 0.3)) for _ in range(a.constituents)]
     prec = capi.SW2GPU_FP64 if a.precision == "fp64" else capi.SW2GPU_MIXED
     pc = capi.SW2GPU_PREC_BJACOBI if a.precond == "bjacobi" else capi.SW2GPU_PREC_DILU
     g = SW2GPU(model, precision=prec, precond=pc)
@@ -42,6 +54,13 @@ def main(argv=None):
                                              "krylov_ms", "resid_ms", "other_ms")}))
         if st["status"] != 0:
             raise SystemExit(f"step failed with status {st['status']}")
+        if a.constituents:
+            for k, t in enumerate(g.transport_step()):
+                print(json.dumps({"constituent": k, **{q: t[q] for q in ("status", "newton_its", "linear_its",
+                                                                        "device_ms", "jac_ms", "krylov_ms",
+                                                                        "resid_ms", "other_ms")}}))
+                if t["status"] != 0:
+                    raise SystemExit(f"transport of constituent {k} failed with status {t['status']}")
     g.close()
 
 
