@@ -34,6 +34,7 @@
 #include "sw2_krylov.cuh"
 #include "sw2_series.h"
 #include "trn_kernels.cuh"
+#include "newton_ctl.cuh"
 
 using namespace sw2;
 
@@ -214,8 +215,17 @@ struct sw2gpu_ctx {
         int kernels_start = 0, kernels_newton = 0;
         double dt = -1.0;
         int jac_minb = -1, stages = -1;
+        // the whole step as one graph, its loops conditional nodes (graph mode 2): kernels of the
+        // step start, of one Newton iteration, of one line-search halving, of the final test, of
+        // the failure reset and of the tail (mass tracking)
+        cudaGraphExec_t loop = nullptr;
+        int k_start = 0, k_body = 0, k_ls = 0, k_final = 0, k_reset = 0, k_tail = 0;
+        bool loop_mass = false;
     };
     bool use_graphs = false;
+    bool loop_graphs = false;       // graph mode 2: the Newton loop's control on the device
+    DBuf<NewtonCtl> nctl;           // its state
+    NewtonCtl* nctl_h = nullptr;    // pinned: the state after the step
     StepGraph graphs[3];
     // pinned staging of the per-step tables; the event marks the end of their last upload
     double* stage_h = nullptr;
@@ -225,6 +235,7 @@ struct sw2gpu_ctx {
         for (auto& g : graphs) {
             if (g.start) cudaGraphExecDestroy(g.start);
             if (g.newton) cudaGraphExecDestroy(g.newton);
+            if (g.loop) cudaGraphExecDestroy(g.loop);
             g = StepGraph();
         }
     }
@@ -372,6 +383,7 @@ sw2gpu_ctx::~sw2gpu_ctx() {
     if (stage_h) cudaFreeHost(stage_h);
     if (mass_h) cudaFreeHost(mass_h);
     if (tnorms_h) cudaFreeHost(tnorms_h);
+    if (nctl_h) cudaFreeHost(nctl_h);
     if (tctl_h) cudaFreeHost(tctl_h);
     if (tsval_h) cudaFreeHost(tsval_h);
     self.reset();
@@ -1472,6 +1484,237 @@ int graph_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* sta
     return 0;
 }
 
+// ---------------------------------------------------------------------------------------------
+// graph mode 2: the whole step as one graph, the Newton loop and the line search as conditional
+// WHILE nodes whose conditions the control kernels of newton_ctl.cuh set, the failure reset as an
+// IF node; the host launches it and reads one status word
+
+// nodes of `g` with no outgoing edge
+int graph_sinks(cudaGraph_t g, std::vector<cudaGraphNode_t>& out) {
+    size_t nn = 0, ne = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (nn) CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+    CK(cudaGraphGetEdges(g, nullptr, nullptr, &ne));
+    std::vector<cudaGraphNode_t> from(ne), to(ne);
+    if (ne) CK(cudaGraphGetEdges(g, from.data(), to.data(), &ne));
+    out.clear();
+    for (cudaGraphNode_t n : nodes)
+        if (std::find(from.begin(), from.end(), n) == from.end()) out.push_back(n);
+    return 0;
+}
+
+// launches of `body` captured into `g` after `deps`; `sinks` receives the graph's new sinks
+template <class F>
+int capture_into(Runner& R, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, int* kernels,
+                 std::vector<cudaGraphNode_t>& sinks, F body) {
+    const int l0 = R.launches;
+    CK(cudaStreamBeginCaptureToGraph(R.stream, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                     cudaStreamCaptureModeThreadLocal));
+    R.capturing = true;
+    const int rc = body();
+    R.capturing = false;
+    cudaGraph_t same = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(R.stream, &same);
+    *kernels = R.launches - l0;
+    R.launches = l0;
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(SW2GPU_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    return graph_sinks(g, sinks);
+}
+
+int add_conditional(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, cudaGraphConditionalHandle h,
+                    cudaGraphConditionalNodeType type, cudaGraphNode_t* node, cudaGraph_t* body) {
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    CK(cudaGraphAddNode(node, g, deps.empty() ? nullptr : deps.data(), deps.size(), &np));
+    *body = np.conditional.phGraph_out[0];
+    return 0;
+}
+
+NewtonParams newton_params(const sw2gpu_ctx* c) {
+    NewtonParams P;
+    P.tol_nonlin = c->p.tol_nonlin;
+    P.inc_nonlin = c->p.inc_nonlin;
+    P.lin_rtol = c->p.lin_rtol;
+    P.eta_ntl = kEtaNtl;
+    P.accept_rel = kAcceptRel;
+    P.max_nonlin_it = c->p.max_nonlin_it;
+    P.max_ls_cuts = c->p.max_linesearch_cuts;
+    P.mixed = c->p.precision == SW2GPU_MIXED ? 1 : 0;
+    P.V = c->V;
+    return P;
+}
+
+int ensure_loop_graph(sw2gpu_ctx* c) {
+    Runner& R = *c->self;
+    sw2gpu_ctx::StepGraph& G = c->graphs[c->lv[0]];
+    if (G.loop && G.dt == c->dt && G.jac_minb == R.jac_minb && G.stages == R.stages && G.loop_mass == c->mass_on)
+        return 0;
+    if (G.loop) cudaGraphExecDestroy(G.loop);
+    G.loop = nullptr;
+    if (!c->nctl.p) {
+        g_alloc_bytes = &c->bytes;
+        const int r = zalloc(c->nctl, 1, R.stream);
+        g_alloc_bytes = nullptr;
+        if (r) return r;
+        CK(cudaMallocHost(&c->nctl_h, sizeof(NewtonCtl)));
+    }
+    const std::vector<int> one(1, 0);
+    const NewtonParams P = newton_params(c);
+    NewtonCtl* S = c->nctl.p;
+    const Norms* NM = R.norms.p;
+    const KrylovCtl* KC = R.ctl.p;
+    double* ETA = R.eta_dev.p;
+    cudaGraph_t T = nullptr;
+    CK(cudaGraphCreate(&T, 0));
+    struct Own {
+        cudaGraph_t g;
+        ~Own() { if (g) cudaGraphDestroy(g); }
+    } own{T};
+    cudaGraphConditionalHandle hN, hF, hL;
+    CK(cudaGraphConditionalHandleCreate(&hN, T, 0, cudaGraphCondAssignDefault));
+    CK(cudaGraphConditionalHandleCreate(&hF, T, 0, cudaGraphCondAssignDefault));
+    std::vector<cudaGraphNode_t> sinks, none;
+    int rc, kc = 0;
+    // step start: fe_sw2_init, the first residual, the control state
+    if ((rc = capture_into(R, T, none, &G.k_start, sinks, [&] {
+             int r = launch_init(R, one);
+             if (!r) r = launch_resid(R, one);
+             if (!r) {
+                 k_ctl_begin<<<1, 1, 0, R.stream>>>(S, P, NM, hN);
+                 R.launches++;
+             }
+             return r;
+         })))
+        return rc;
+    // the Newton loop
+    cudaGraphNode_t wn;
+    cudaGraph_t BN;
+    if ((rc = add_conditional(T, sinks, hN, cudaGraphCondTypeWhile, &wn, &BN))) return rc;
+    CK(cudaGraphConditionalHandleCreate(&hL, BN, 0, cudaGraphCondAssignDefault));
+    int k1 = 0, k2 = 0;
+    if ((rc = capture_into(R, BN, none, &k1, sinks, [&] {
+             k_ctl_eta<<<1, 1, 0, R.stream>>>(S, P, ETA);
+             R.launches++;
+             int r = launch_jacobian(R, one);
+             if (!r) r = launch_linear(R, one, std::vector<double>(1, c->p.lin_rtol));   // reads eta_dev
+             if (!r) r = launch_resid(R, one);
+             if (!r) {
+                 k_ctl_after<<<1, 1, 0, R.stream>>>(S, P, NM, KC, hL);
+                 R.launches++;
+             }
+             return r;
+         })))
+        return rc;
+    cudaGraphNode_t wl;
+    cudaGraph_t BL;
+    if ((rc = add_conditional(BN, sinks, hL, cudaGraphCondTypeWhile, &wl, &BL))) return rc;
+    std::vector<cudaGraphNode_t> lsinks;
+    if ((rc = capture_into(R, BL, none, &G.k_ls, lsinks, [&] {
+             int r = launch_half_inc(R, one);
+             if (!r) r = launch_resid(R, one);
+             if (!r) {
+                 k_ctl_ls<<<1, 1, 0, R.stream>>>(S, P, NM, hL);
+                 R.launches++;
+             }
+             return r;
+         })))
+        return rc;
+    if ((rc = capture_into(R, BN, std::vector<cudaGraphNode_t>{wl}, &k2, sinks, [&] {
+             k_ctl_end<<<1, 1, 0, R.stream>>>(S, P, hN);
+             R.launches++;
+             return 0;
+         })))
+        return rc;
+    G.k_body = k1 + k2;
+    // the status, the reset of a failed step, the tail
+    if ((rc = capture_into(R, T, std::vector<cudaGraphNode_t>{wn}, &G.k_final, sinks, [&] {
+             k_ctl_final<<<1, 1, 0, R.stream>>>(S, P, SW2GPU_E_NAN, SW2GPU_E_LINEAR, SW2GPU_E_NEWTON, SW2GPU_E_TIMEOUT,
+                                                hF);
+             R.launches++;
+             return 0;
+         })))
+        return rc;
+    cudaGraphNode_t fi;
+    cudaGraph_t BF;
+    if ((rc = add_conditional(T, sinks, hF, cudaGraphCondTypeIf, &fi, &BF))) return rc;
+    if ((rc = capture_into(R, BF, none, &G.k_reset, lsinks, [&] { return launch_init(R, one); }))) return rc;
+    if ((rc = capture_into(R, T, std::vector<cudaGraphNode_t>{fi}, &G.k_tail, sinks, [&] {
+             int r = 0;
+             if (c->mass_on) {   // reduced whatever the status; the host keeps it for an accepted step
+                 r = enqueue_step_mass(c, R.stream);
+                 R.launches += 4;
+             }
+             if (!r && cudaMemcpyAsync(c->nctl_h, S, sizeof(NewtonCtl), cudaMemcpyDeviceToHost, R.stream) != cudaSuccess)
+                 r = fail(SW2GPU_E_CUDA, "capturing the status copy failed");
+             if (!r) r = enqueue_results(R);
+             return r;
+         })))
+        return rc;
+    (void)kc;
+    const cudaError_t ei = cudaGraphInstantiate(&G.loop, T, 0);
+    if (ei != cudaSuccess) {
+        G.loop = nullptr;
+        return fail(SW2GPU_E_CUDA, "step graph instantiation failed: %s", cudaGetErrorString(ei));
+    }
+    G.dt = c->dt;
+    G.jac_minb = R.jac_minb;
+    G.stages = R.stages;
+    G.loop_mass = c->mass_on;
+    return 0;
+}
+
+// One time step of a single instance as one graph launch (graph mode 2): the Newton loop's
+// decisions are taken on the device; same kernels, same arithmetic as direct stepping.
+int loop_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* stats, int* status) {
+    Runner& R = *c->self;
+    R.launches = 0;
+    R.nphase = 0;
+    CK(cudaEventRecord(R.ev0, R.stream));
+    int rc = step_begin(R, 0, dt, series);
+    if (!rc) rc = runner_tables(R, 1);
+    if (!rc) rc = ensure_loop_graph(c);
+    if (rc) return rc;
+    const sw2gpu_ctx::StepGraph& G = c->graphs[c->lv[0]];
+    CK(cudaGraphLaunch(G.loop, R.stream));
+    CK(cudaEventRecord(R.ev1, R.stream));
+    CK(cudaEventSynchronize(R.ev1));
+    const NewtonCtl n = *c->nctl_h;
+    c->ngeneral = R.norms_h[0].ngeneral;
+    for (int i = 0; i < std::min(n.it, 8); i++) c->its_at[i] = n.its_at[i];
+    if (n.it > 0) c->pred_its = n.its_at[std::min(n.it - 1, 7)];
+    R.launches = G.k_start + n.it * G.k_body + (n.timeout ? G.k_body : 0) + n.cuts_total * G.k_ls + G.k_final +
+                 (n.status ? G.k_reset : 0) + G.k_tail;
+    status[0] = n.status;
+    c->mass_valid = false;
+    if (c->mass_on && n.status == SW2GPU_OK) {
+        c->step_mass = c->mass_h[0];
+        c->step_flux = c->mass_h[1];
+        c->mass_valid = true;
+    }
+    if (n.status == SW2GPU_E_TIMEOUT) return fail(SW2GPU_E_TIMEOUT, "Krylov barrier or tile-copy wait ran out");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, R.ev0, R.ev1);
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->status = n.status;
+        stats->newton_its = n.it;
+        stats->linear_its = n.lin;
+        stats->linesearch_cuts = n.cuts_total;
+        stats->resid_max = n.rmax;
+        stats->resid_l2 = n.l2;
+        stats->inc_max = n.imax;
+        stats->device_ms = ms;
+        stats->kernel_launches = R.launches;
+        stats->other_ms = ms;   // phases are not timed inside graphs
+    }
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1902,7 +2145,7 @@ int sw2gpu_remesh(sw2gpu_ctx* old, const sw2gpu_mesh* m, sw2gpu_ctx** out) {
     c->tune_stages = old->tune_stages;
     if (!rc && old->dacont_on) rc = sw2gpu_set_dacont(c, 1);
     if (!rc && old->mass_on) rc = sw2gpu_set_mass_tracking(c, 1, old->mass_density);
-    if (!rc && old->use_graphs) rc = sw2gpu_set_graphs(c, 1);
+    if (!rc && (old->use_graphs || old->loop_graphs)) rc = sw2gpu_set_graphs(c, old->loop_graphs ? 2 : 1);
     if (!rc && old->ntrn) {
         if (c->S != old->S || c->M != old->M) {
             rc = fail(SW2GPU_E_ARG, "remesh: the constituents need the same strings and materials");
@@ -2721,9 +2964,10 @@ int sw2gpu_set_wait_limits(sw2gpu_ctx* c, int64_t barrier_polls, int64_t copy_po
 }
 
 int sw2gpu_set_graphs(sw2gpu_ctx* c, int32_t enable) {
-    if (!c) return fail(SW2GPU_E_ARG, "null context");
+    if (!c || enable < 0 || enable > 2) return fail(SW2GPU_E_ARG, "bad context or graph mode");
     c->drop_graphs();
-    c->use_graphs = enable != 0;
+    c->use_graphs = enable == 1;
+    c->loop_graphs = enable == 2;
     return SW2GPU_OK;
 }
 
@@ -2731,7 +2975,9 @@ int sw2gpu_step(sw2gpu_ctx* c, double dt, const double* series, sw2gpu_stats* st
     if (!c || !(dt > 0.0)) return fail(SW2GPU_E_ARG, "bad context or dt");
     const double* ser[1] = {series};
     int status = 0;
-    int rc = c->use_graphs ? graph_step(c, dt, ser[0], stats, &status) : runner_step(*c->self, &dt, ser, stats, &status);
+    int rc = c->loop_graphs  ? loop_step(c, dt, ser[0], stats, &status)
+             : c->use_graphs ? graph_step(c, dt, ser[0], stats, &status)
+                             : runner_step(*c->self, &dt, ser, stats, &status);
     if (rc) return rc;
     if (status != SW2GPU_OK)
         fail(status, "step failed (Newton %d iterations, max residual %g)", stats ? stats->newton_its : -1,

@@ -261,9 +261,12 @@ class SW2GPU:
         _check(lib().sw2gpu_autotune(self.h, C.byref(j), C.byref(s)))
         return j.value, s.value
 
-    def set_graphs(self, enable: bool = True):
-        """Replay each step's launch sequences from CUDA graphs (small meshes)."""
-        _check(lib().sw2gpu_set_graphs(self.h, 1 if enable else 0))
+    def set_graphs(self, enable=True):
+        """Replay each step's launch sequences from CUDA graphs (small meshes): True or 1, one graph
+        per Newton iteration; 2, the whole step as one graph with the Newton loop's decisions on
+        the device; False or 0, direct launches."""
+        mode = 2 if enable == 2 else (1 if enable else 0)
+        _check(lib().sw2gpu_set_graphs(self.h, mode))
 
     def set_wait_limits(self, barrier_polls: int = 0, copy_polls: int = 0):
         """Bounds of the Krylov kernel's device waits in polls (0: the library's defaults)."""

@@ -167,13 +167,14 @@ def ensemble_models(n: int, nsteps: int, seed0: int = 7000, procs: int = 0):
 
 def run_small(stream, steps: int = 20, warmup: int = 3):
     """Config-1 channel (4,000 triangles), where launches and host round trips are a large
-    part of a step: direct launches vs the step replayed from CUDA graphs."""
+    part of a step: direct launches, the step's Newton iterations replayed from CUDA graphs, and
+    the whole step as one graph with the Newton loop's decisions on the device."""
     import torch
     from adhv8_kraken_b200 import meshgen
     from adhv8_kraken_b200.sw2 import SW2GPU
     m = meshgen.channel(nsteps=warmup + steps)
     out = {"workload": f"channel: {m.nelems2d} triangles, dt {m.dt} s, {steps} steps after {warmup}"}
-    for name, graphs in (("direct", False), ("graphs", True)):
+    for name, graphs in (("direct", False), ("graphs", True), ("step_graph", 2)):
         g = SW2GPU(m, stream=stream.cuda_stream)
         g.set_graphs(graphs)
         for _ in range(warmup):

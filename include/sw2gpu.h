@@ -163,10 +163,15 @@ int sw2gpu_autotune(sw2gpu_ctx *ctx, int32_t *jac_minb, int32_t *stages);
 int sw2gpu_set_variant(sw2gpu_ctx *ctx, int32_t jac_minb, int32_t stages);
 int sw2gpu_get_variant(const sw2gpu_ctx *ctx, int32_t *jac_minb, int32_t *stages);
 /* CUDA graphs for small meshes, where launches and host round trips are a large part of a
- * step (no counterpart in the reference): when enabled, sw2gpu_step replays the step start and
- * each Newton iteration as one graph launch each (captured at first use for each arrangement
- * of the rotating state levels, recaptured after a dt or variant change).  Same kernels and
- * results as direct launches; phase times are not reported in graph mode. */
+ * step (no counterpart in the reference).  enable = 1: sw2gpu_step replays the step start and
+ * each Newton iteration as one graph launch each, the host reading the norms after each
+ * iteration.  enable = 2: the whole step is one graph launch -- the Newton loop and the line
+ * search are conditional WHILE nodes whose conditions single-thread control kernels set on the
+ * device from the norms and the Krylov outcome (fe_newton's decisions, as direct stepping takes
+ * them on the host), the failure reset an IF node -- and the host reads one status word per
+ * step.  Graphs are captured at first use for each arrangement of the rotating state levels and
+ * recaptured after a dt, variant or mass-tracking change.  Same kernels and results as direct
+ * launches; phase times are not reported in graph mode.  0 = direct launches. */
 int sw2gpu_set_graphs(sw2gpu_ctx *ctx, int32_t enable);
 /* device memory the context holds (bytes); no counterpart in the reference */
 int64_t sw2gpu_device_bytes(const sw2gpu_ctx *ctx);
