@@ -2806,6 +2806,35 @@ int sw2gpu_transport_load(sw2gpu_ctx* c, int32_t itrn, double* resid, double* va
     return SW2GPU_OK;
 }
 
+int sw2gpu_transport_elem_error(sw2gpu_ctx* c, const double* refine_tol, double* elem_error, double* node_error) {
+    if (!c || !refine_tol || !elem_error) return fail(SW2GPU_E_ARG, "null argument");
+    if (!c->ntrn) return fail(SW2GPU_E_ARG, "no constituents (sw2gpu_set_transport)");
+    if (!(c->dt > 0.0)) return fail(SW2GPU_E_ARG, "no step yet (dt unset)");
+    for (int q = 0; q < c->ntrn * c->M; q++)
+        if (!(refine_tol[q] > 0.0)) return fail(SW2GPU_E_ARG, "refine tolerance %d must be positive", q);
+    const int T = c->T, V = c->V, M = c->M;
+    DBuf<double> elem, raw, tol, nodal;
+    if (elem.alloc(T) || raw.alloc(T) || tol.alloc(std::max(M, 1)) || nodal.alloc(V))
+        return fail(SW2GPU_E_NOMEM, "cudaMalloc failed");
+    cudaStream_t st = c->stream;
+    CK(cudaMemcpyAsync(elem.p, elem_error, sizeof(double) * T, cudaMemcpyHostToDevice, st));
+    for (int k = 0; k < c->ntrn; k++) {
+        CK(cudaMemcpyAsync(tol.p, refine_tol + (size_t)k * M, sizeof(double) * M, cudaMemcpyHostToDevice, st));
+        k_trn_elem_error<<<nblk(T, kTrnThreads), kTrnThreads, 0, st>>>(c->dm, c->H(0), c->U(0), c->Vv(0),
+                                                                        c->tlevel(k, 0), c->tlevel(k, 1), c->dt,
+                                                                        tol.p, raw.p, elem.p);
+        if (node_error) {   // the raw values averaged over each node's elements, in element order
+            k_node_error<<<nblk(V, 256), 256, 0, st>>>(c->dm, raw.p, nodal.p);
+            CK(cudaMemcpyAsync(node_error + (size_t)k * V, nodal.p, sizeof(double) * V, cudaMemcpyDeviceToHost, st));
+        }
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));   // tol is rewritten for the next constituent
+    }
+    CK(cudaMemcpyAsync(elem_error, elem.p, sizeof(double) * T, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return SW2GPU_OK;
+}
+
 int sw2gpu_set_dt(sw2gpu_ctx* c, double dt, const double* series) {
     if (!c || !(dt > 0.0)) return fail(SW2GPU_E_ARG, "bad context or dt");
     c->dt = dt;

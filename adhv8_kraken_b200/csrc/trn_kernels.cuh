@@ -271,6 +271,61 @@ __global__ void __launch_bounds__(kTrnThreads) k_trn_inc(double* __restrict__ c,
     sol[n] = mode == 0 ? -s : s;
 }
 
+// the constituents' adaption error indicator (scon_calculate_elem2d_error, src/structs/scon.c:
+// 282-361), one constituent per launch: per element the steady transport residual at each vertex
+// less its element mean, as a root sum of squares times the area (raw[e]), and elem[e] raised to
+// raw / refine_tol of the element's material where that is larger (max over the constituents and
+// whatever elem held before, the flow's indicator in fe_main's order, src/fe/fe_main.c:625-628)
+__global__ void __launch_bounds__(kTrnThreads) k_trn_elem_error(const __grid_constant__ DevMesh m,
+                                                                const double* __restrict__ h,
+                                                                const double* __restrict__ u,
+                                                                const double* __restrict__ v,
+                                                                const double* __restrict__ c,
+                                                                const double* __restrict__ co, double dt,
+                                                                const double* __restrict__ tol,
+                                                                double* __restrict__ raw,
+                                                                double* __restrict__ elem) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.T) return;
+    const int n[3] = {m.en0[e], m.en1[e], m.en2[e]};
+    const double gx[3] = {m.gx0[e], m.gx1[e], m.gx2[e]}, gy[3] = {m.gy0[e], m.gy1[e], m.gy2[e]};
+    double hh[3], uu[3], vv[3], cc[3], cp[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        hh[i] = h[n[i]];
+        uu[i] = u[n[i]];
+        vv[i] = v[n[i]];
+        cc[i] = c[n[i]];
+        cp[i] = co[n[i]];
+    }
+    double dudx = 0., dvdy = 0., dcdx = 0., dcdy = 0.;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        dudx += gx[i] * uu[i];
+        dvdy += gy[i] * vv[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        dcdx += gx[i] * cc[i];
+        dcdy += gy[i] * cc[i];
+    }
+    double coef[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+        coef[i] = hh[i] * (cc[i] - cp[i]) / dt + uu[i] * hh[i] * dcdx + hh[i] * cc[i] * dudx + hh[i] * vv[i] * dcdy +
+                  hh[i] * cc[i] * dvdy;
+    double err = (1. / 3.) * (coef[0] + coef[1] + coef[2]);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        coef[i] -= err;
+        coef[i] = coef[i] * coef[i];
+    }
+    err = sqrt(coef[0] + coef[1] + coef[2]) * m.djac[e];
+    raw[e] = err;
+    const double scaled = err / tol[m.emat[e]];
+    if (scaled > elem[e]) elem[e] = scaled;
+}
+
 // ---------------------------------------------------------------------------------
 // Persistent cooperative BiCGSTAB on the folded operator A' = D^-1 A (unit diagonal) with
 // b' = D^-1 R, from x = 0; stops when ||r||inf <= atol + rtol ||b'||inf or after max_it

@@ -118,6 +118,7 @@ class Constituent:
     node_bc: Dict[int, int] = dataclasses.field(default_factory=dict)
     edge_bc: Dict[int, int] = dataclasses.field(default_factory=dict)
     c0: Optional[np.ndarray] = None                  # initial concentration (None: 0)
+    refine_tol: float = 1.0                          # MP TRT, every material (adaption indicator)
 
 
 @dataclasses.dataclass
@@ -283,6 +284,7 @@ class SW2Model:
                 for m in range(nmat):
                     dm = con.diffusion[m] if m < len(con.diffusion) else 0.0
                     w(f"MP DF {m + 1} {k + 1} {_f(dm)}\n")
+                    w(f"MP TRT {m + 1} {k + 1} {_f(con.refine_tol)}\n")   # read_bc_MP.c:203-210
             if p.drying_limit > 0:
                 w(f"MP DTL {_f(p.drying_limit)}\n")
             w(f"MP G {_f(p.gravity)}\nMP RHO {_f(p.density)}\nMP MU {_f(p.viscosity)}\nMP MUC {_f(p.manning_units)}\n")

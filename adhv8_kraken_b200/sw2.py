@@ -37,7 +37,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_set_wait_limits", "sw2gpu_snapshot", "sw2gpu_elem_error", "sw2gpu_set_mass_tracking",
            "sw2gpu_step_mass", "sw2gpu_set_wind", "sw2gpu_set_waves", "sw2gpu_remesh", "sw2gpu_batch_set_graphs",
            "sw2gpu_set_transport", "sw2gpu_set_conc", "sw2gpu_get_conc", "sw2gpu_transport_step",
-           "sw2gpu_transport_init", "sw2gpu_transport_load"]
+           "sw2gpu_transport_init", "sw2gpu_transport_load", "sw2gpu_transport_elem_error"]
 
 
 class SW2Error(RuntimeError):
@@ -103,6 +103,7 @@ def lib():
         L.sw2gpu_transport_step.argtypes = [vp, c_double_p, vp]
         L.sw2gpu_transport_init.argtypes = [vp, C.c_int32, c_double_p]
         L.sw2gpu_transport_load.argtypes = [vp, C.c_int32, c_double_p, c_double_p]
+        L.sw2gpu_transport_elem_error.argtypes = [vp, c_double_p, c_double_p, c_double_p]
         L.sw2gpu_device_bytes.restype = C.c_int64
         L.sw2gpu_server_create.argtypes = [C.c_int32, C.c_double, C.c_int32, C.POINTER(vp)]
         L.sw2gpu_server_submit.argtypes = [vp, vp, vp, c_double_p, c_double_p, c_double_p, C.c_double, C.c_double,
@@ -242,6 +243,15 @@ class SW2GPU:
         r, val = np.zeros(self.V), np.zeros(self.nnzb)
         _check(lib().sw2gpu_transport_load(self.h, itrn, _dp(r), _dp(val)))
         return val, r
+
+    def transport_elem_error(self, refine_tol, elem_error):
+        """The constituents' adaption error indicator of the last step folded into elem_error (the
+        flow's, as fe_main calls them): (elem_error [T], node_error [ntrn, V])."""
+        tol = np.ascontiguousarray(refine_tol, dtype=np.float64)
+        ee = np.array(elem_error, dtype=np.float64)
+        ne = np.zeros(self.ntrn * self.V)
+        _check(lib().sw2gpu_transport_elem_error(self.h, _dp(tol), _dp(ee), _dp(ne)))
+        return ee, ne.reshape(self.ntrn, self.V)
 
     def remesh(self, model):
         """Moves this solver to `model`, an adaption of its mesh that keeps node and triangle

@@ -306,6 +306,15 @@ int sw2gpu_transport_step(sw2gpu_ctx *ctx, const double *series, sw2gpu_stats *s
  * val[nnzb] over the context's pattern (fe_transport_load) at the current state. */
 int sw2gpu_transport_init(sw2gpu_ctx *ctx, int32_t itrn, const double *series);
 int sw2gpu_transport_load(sw2gpu_ctx *ctx, int32_t itrn, double *resid, double *val);
+/* The constituents' adaption error indicator of the last step (scon_calculate_elem2d_error,
+ * src/structs/scon.c:282-361, which fe_main calls right after the flow's indicator,
+ * src/fe/fe_main.c:625-628): per element and constituent the steady transport residual at each
+ * vertex less its element mean, as a root sum of squares times the area.  elem_error[nelems2d]
+ * is in/out: each element keeps the largest of its value (pass the flow's, sw2gpu_elem_error)
+ * and every constituent's error over refine_tol[itrn * nmats + material] (MP TRT);
+ * node_error[ntransport * nnodes] (may be NULL) the constituents' element errors averaged over
+ * each node's elements, the reference's con[itrn].error. */
+int sw2gpu_transport_elem_error(sw2gpu_ctx *ctx, const double *refine_tol, double *elem_error, double *node_error);
 
 /* One implicit time step: time-level shift (fe_sw2, src/fe/sw2/fe_sw2.c:43-50) then the
  * damped Newton loop (fe_newton).  `series` holds the step-averaged value of every BC

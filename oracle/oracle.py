@@ -77,6 +77,7 @@ def lib():
         L.orc_trn_get_matrix.argtypes = [C.c_void_p, c_double_p, c_double_p]
         L.orc_trn_step.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.orc_trn_step.restype = C.c_int
+        L.orc_trn_elem_error.argtypes = [C.c_void_p, c_double_p, c_double_p, c_double_p]
         for name in ("orc_trn_body_resid", "orc_trn_edge_resid"):
             getattr(L, name).argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, c_double_p]
         _lib = L
@@ -306,3 +307,13 @@ class Oracle:
         out = np.zeros(2)
         lib().orc_trn_edge_resid(C.c_void_p(self.h), itrn, ie, eps, pnode, psign, _dp(out))
         return out
+
+    def trn_elem_error(self, refine_tol, elem_error):
+        """The constituents' adaption error indicator (scon_calculate_elem2d_error) folded into
+        elem_error (the flow's, as fe_main calls them): (elem_error [T], node_error [ntrn, V]);
+        refine_tol [ntrn, nmats] (MP TRT)."""
+        tol = np.ascontiguousarray(refine_tol, dtype=np.float64)
+        ee = np.array(elem_error, dtype=np.float64)
+        ne = np.zeros(self.ntrn * self.V)
+        lib().orc_trn_elem_error(self.h, _dp(tol), _dp(ee), _dp(ne))
+        return ee, ne.reshape(self.ntrn, self.V)

@@ -25,6 +25,9 @@
  *            "dacont"): the adaption error indicator fe_main computed for the step
  *            (ssw_2d_calculate_elem_error, src/structs/ssw_2d.c:424-500), grid->elem_error
  *            per element and its nodal average sw->error.
+ *   "conerr" with "elemerr", for every constituent: its nodal error indicator con[k].error
+ *            (scon_calculate_elem2d_error, src/structs/scon.c:282-361), whose element values
+ *            fe_main folds into grid->elem_error after the flow's (src/fe/fe_main.c:625-628);
  *   "con"    after every accepted step of a model with constituents (after the records
  *            above): each constituent's concentration array, constituent by constituent;
  *   "tload"  for the first ADH_DUMP_TLOADS calls of fe_transport_load (the transport Newton's
@@ -163,8 +166,10 @@ int __wrap_fe_main(SSUPER_MODEL *sm) {
             free(d);
         }
         if (dump_error) {
+            int k;
             put_f64("elemerr", mod->grid->elem_error, mod->grid->nelems2d);
             put_f64("nodeerr", mod->sw->d2->error, n);
+            for (k = 0; k < mod->ntransport; k++) put_f64("conerr", mod->con[k].error, n);
         }
         {
             int k;

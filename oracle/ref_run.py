@@ -60,6 +60,12 @@ def parse(recs) -> Dict[str, list]:
                 steps[-1]["elem_error"] = recs[i][1]
                 steps[-1]["node_error"] = recs[i + 1][1]
                 i += 2
+                cerr = []
+                while i < len(recs) and recs[i][0] == "conerr":   # the constituents' nodal indicator
+                    cerr.append(recs[i][1])
+                    i += 1
+                if cerr:
+                    steps[-1]["con_error"] = cerr
             cons = []
             while i < len(recs) and recs[i][0] == "con":        # constituent concentrations
                 cons.append(recs[i][1])

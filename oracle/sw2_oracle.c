@@ -2113,3 +2113,46 @@ void orc_trn_body_resid(orc_ctx *C, int t, int ie, double eps, int pnode, int ps
 void orc_trn_edge_resid(orc_ctx *C, int t, int ie, double eps, int pnode, int psign, double *out) {
     trn_edge_resid(C, t, ie, eps, pnode, psign, out);
 }
+
+/* scon_calculate_elem2d_error (src/structs/scon.c:282-361): the constituents' adaption error
+ * indicator at the current and old levels and the last dt.  Per element and constituent the
+ * steady transport residual h (c - c_old) / dt + u h dc/dx + h c du/dx + h v dc/dy + h c dv/dy at
+ * each vertex, less its element mean, as a root sum of squares times the area; elem_error[e]
+ * (in/out, e.g. the flow's indicator first, as fe_main calls them, src/fe/fe_main.c:625-628) keeps
+ * the largest of its value and every constituent's error over refine_tol[k * M + material];
+ * node_error[k * V + n] (may be NULL) the constituent's element errors averaged over n's elements */
+void orc_trn_elem_error(const orc_ctx *C, const double *refine_tol, double *elem_error, double *node_error) {
+    int V = C->V, e, i, k;
+    int *cnt = (int *) calloc(V, sizeof(int));
+    double *nerr = (double *) calloc((size_t) (C->ntrn ? C->ntrn : 1) * V, sizeof(double));
+    for (e = 0; e < C->T; e++) {
+        const int *nd = C->tri + 3 * e;
+        const v2 *g = (const v2 *) (C->grad + 6 * e);
+        double hh[3], uu[3], vv[3], dudx = 0., dvdy = 0.;
+        for (i = 0; i < 3; i++) { hh[i] = C->h[0][nd[i]]; uu[i] = C->u[0][nd[i]]; vv[i] = C->v[0][nd[i]]; }
+        for (i = 0; i < 3; i++) {
+            cnt[nd[i]] += 1;
+            dudx += g[i].x * uu[i];
+            dvdy += g[i].y * vv[i];
+        }
+        for (k = 0; k < C->ntrn; k++) {
+            const double *c = TC(C, k, 0), *co = TC(C, k, 1);
+            double cc[3], cp[3], dcdx = 0., dcdy = 0., coef[3], err;
+            for (i = 0; i < 3; i++) { cc[i] = c[nd[i]]; cp[i] = co[nd[i]]; }
+            for (i = 0; i < 3; i++) { dcdx += g[i].x * cc[i]; dcdy += g[i].y * cc[i]; }
+            for (i = 0; i < 3; i++)
+                coef[i] = hh[i] * (cc[i] - cp[i]) / C->dt + uu[i] * hh[i] * dcdx + hh[i] * cc[i] * dudx +
+                          hh[i] * vv[i] * dcdy + hh[i] * cc[i] * dvdy;
+            err = (1. / 3.) * (coef[0] + coef[1] + coef[2]);
+            for (i = 0; i < 3; i++) { coef[i] -= err; coef[i] = coef[i] * coef[i]; }
+            err = sqrt(coef[0] + coef[1] + coef[2]) * C->djac[e];
+            for (i = 0; i < 3; i++) nerr[(size_t) k * V + nd[i]] += err;
+            err /= refine_tol[k * C->M + C->tri_mat[e]];
+            if (err > elem_error[e]) elem_error[e] = err;
+        }
+    }
+    if (node_error)
+        for (k = 0; k < C->ntrn; k++)
+            for (i = 0; i < V; i++) node_error[(size_t) k * V + i] = nerr[(size_t) k * V + i] / cnt[i];
+    free(cnt); free(nerr);
+}

@@ -45,6 +45,9 @@ Fixtures (numpy ``.npz``):
   free-outflow channel and the uniform-17.5 channel of the reference's angle_salt check:
   concentrations after every step, and for the two basins the inputs and results of the first
   two transport Jacobian builds.
+* ``trnerr_ref.npz`` -- the adaption error indicator of the two-constituent basin (MP TRT 0.05 and
+  2.0) after each of 4 steps: grid->elem_error with the constituents' indicator folded in after
+  the flow's, and each constituent's nodal indicator con[k].error.
 * ``mass_ref.npz`` -- the reference's grid mass diagnostics (src/tools/tl_grid_mass.c) after
   every step of 6 channel steps and of the 8 basin steps: initial and current mass, mass error
   and accumulated mass flux, with the channel's state after every step (the basin's states are
@@ -273,10 +276,32 @@ def transport():
     np.savez_compressed(os.path.join(HERE, "transport_ref.npz"), **out)
 
 
+def trnerr_model():
+    """The two-constituent wet/dry basin with MP TRT 0.05 and 2.0: the constituents set most
+    elements' indicator, the flow the rest."""
+    m = meshgen.basin_transport(nsteps=4)
+    m.constituents[0].refine_tol = 0.05
+    m.constituents[1].refine_tol = 2.0
+    return m
+
+
+def trnerr():
+    """The adaption error indicator of a model with constituents after every step: grid->elem_error
+    (the flow's, then the constituents' folded in, src/fe/fe_main.c:625-628) and each constituent's
+    nodal con[k].error (scon_calculate_elem2d_error)."""
+    m = trnerr_model()
+    ref = run_reference(m, error=True)
+    out = {"fingerprint": np.array(fingerprint(m))}
+    for k, st in enumerate(ref["steps"], 1):
+        out[f"step{k}_elem_error"] = st["elem_error"]
+        out[f"step{k}_con_error"] = np.stack(st["con_error"])
+    np.savez_compressed(os.path.join(HERE, "trnerr_ref.npz"), **out)
+
+
 if __name__ == "__main__":
     import sys as _sys
     which = _sys.argv[1:] or ["channel", "basin", "ovh", "outflow", "terms", "rain", "obstacle", "combined", "dacont",
-                              "mass", "scale", "errind", "transport"]
+                              "mass", "scale", "errind", "transport", "trnerr"]
     if "channel" in which:
         channel()
     if "basin" in which:
@@ -303,8 +328,10 @@ if __name__ == "__main__":
         errind()
     if "transport" in which:
         transport()
+    if "trnerr" in which:
+        trnerr()
     for f in ("channel_ref.npz", "basin_ref.npz", "ovh_ref.npz", "outflow_ref.npz", "terms_ref.npz", "rain_ref.npz",
               "obstacle_ref.npz", "combined_ref.npz", "dacont_ref.npz", "mass_ref.npz", "scale_ref.npz",
-              "errind_ref.npz", "transport_ref.npz"):
+              "errind_ref.npz", "transport_ref.npz", "trnerr_ref.npz"):
         if os.path.exists(os.path.join(HERE, f)):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -166,3 +166,30 @@ def test_transport_wait_that_runs_out_ends_with_timeout():
         assert s.step()["status"] == 0
         assert s.transport_step()[0]["status"] == 0
     assert np.array_equal(g.get_conc(0), ref.get_conc(0))
+
+
+def test_transport_error_indicator_matches_oracle():
+    """sw2gpu_transport_elem_error against the oracle at the same state: the flow's indicator, then
+    the constituents' folded in, bit for bit (the same operations in the same order)."""
+    from golden.make_golden import trnerr_model
+    m = trnerr_model()
+    g, o = SW2GPU(m), Oracle(m)
+    for _ in range(2):
+        assert o.step()["status"] == 0
+        o.transport_step()
+    for s in (g,):
+        for lvl in range(3):
+            s.set_state(lvl, *o.get_state(lvl))
+            for j in range(2):
+                s.set_conc(j, lvl, o.get_conc(j, lvl))
+    g.set_dt(m.dt, m.series_values(0.0, m.dt))
+    srt = np.full(len(m.materials), 100.0)
+    trt = np.array([[c.refine_tol] * len(m.materials) for c in m.constituents])
+    eg, _ = g.elem_error(srt)
+    eo, _ = o.elem_error(srt)
+    assert np.array_equal(eg, eo)
+    eg2, cg = g.transport_elem_error(trt, eg)
+    eo2, co = o.trn_elem_error(trt, eo)
+    assert np.array_equal(eg2, eo2)
+    assert np.array_equal(cg, co)
+    assert (eg2 > eg).sum() > 0

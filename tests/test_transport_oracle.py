@@ -89,3 +89,28 @@ def test_oracle_rejects_held_concentration_on_an_edge_string():
     assert m.transport_tables()[2][0, 1] == BCT_DIR
     with pytest.raises(ValueError):
         Oracle(m)
+
+
+def test_oracle_transport_error_indicator_matches_reference():
+    """The adaption error indicator of a model with constituents: the flow's (ssw_2d_calculate_
+    elem_error), then the constituents' folded in (scon_calculate_elem2d_error), as fe_main calls
+    them (src/fe/fe_main.c:625-628); element values and each constituent's nodal values after every
+    step within 1e-9 of the reference's (the states' own differences)."""
+    import os
+    from conftest import GOLDEN
+    from golden.make_golden import trnerr_model
+    ref = dict(np.load(os.path.join(GOLDEN, "trnerr_ref.npz")))
+    m = trnerr_model()
+    assert str(ref["fingerprint"]) == fingerprint(m)
+    o = Oracle(m)
+    srt = np.full(len(m.materials), 100.0)                       # MP SRT of the deck writer
+    trt = np.array([[c.refine_tol] * len(m.materials) for c in m.constituents])
+    for k in range(1, 5):
+        assert o.step()["status"] == 0
+        assert all(s["status"] == 0 for s in o.transport_step())
+        ee, _ = o.elem_error(srt)
+        ee2, cerr = o.trn_elem_error(trt, ee)
+        assert (ee2 > ee).sum() > len(ee) // 2 and (ee2 == ee).sum() > 0   # both indicators decide some
+        assert relerr(ee2, ref[f"step{k}_elem_error"]) <= 1e-9
+        for j in range(2):
+            assert relerr(cerr[j], ref[f"step{k}_con_error"][j]) <= 1e-9
