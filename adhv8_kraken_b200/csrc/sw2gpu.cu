@@ -1579,7 +1579,7 @@ int ensure_loop_graph(sw2gpu_ctx* c) {
     CK(cudaGraphConditionalHandleCreate(&hN, T, 0, cudaGraphCondAssignDefault));
     CK(cudaGraphConditionalHandleCreate(&hF, T, 0, cudaGraphCondAssignDefault));
     std::vector<cudaGraphNode_t> sinks, none;
-    int rc, kc = 0;
+    int rc;
     // step start: fe_sw2_init, the first residual, the control state
     if ((rc = capture_into(R, T, none, &G.k_start, sinks, [&] {
              int r = launch_init(R, one);
@@ -1655,7 +1655,6 @@ int ensure_loop_graph(sw2gpu_ctx* c) {
              return r;
          })))
         return rc;
-    (void)kc;
     const cudaError_t ei = cudaGraphInstantiate(&G.loop, T, 0);
     if (ei != cudaSuccess) {
         G.loop = nullptr;
@@ -1738,7 +1737,7 @@ int build_dilu(sw2gpu_ctx* c, const std::vector<int>& rp, const std::vector<int>
     std::vector<int> cnt(ncol, 0), pst(ncol + 1, 0);
     for (int n = 0; n < V; n++) cnt[colour[n]]++;
     for (int q = 0; q < ncol; q++) pst[q + 1] = pst[q] + (cnt[q] + 31) / 32 * 32;
-    const int N = pst[ncol], ntile = N / 32;
+    const int N = pst[ncol];
     std::vector<int> old(N, -1), nw(V);
     {
         std::vector<int> f(pst.begin(), pst.end() - 1);
@@ -2671,7 +2670,7 @@ int trn_step_one(sw2gpu_ctx* c, int k, const double* series, sw2gpu_stats* st) {
     CK(cudaMemsetAsync(c->tsol.p, 0, sizeof(double) * c->V, c->stream));
     if ((rc = trn_init(c, A))) return rc;
     launches++;
-    Norms nr;
+    Norms nr{};
     phase_begin(2);
     auto resid = [&](Norms& out) {   // the residual phase ends before its host wait
         k_trn_elem<false><<<nblk(c->T + c->E, kTrnThreads), kTrnThreads, 0, c->stream>>>(A);
@@ -2795,7 +2794,7 @@ int sw2gpu_transport_load(sw2gpu_ctx* c, int32_t itrn, double* resid, double* va
     DBuf<double> full;
     if (val && full.alloc(c->nnzb)) return fail(SW2GPU_E_NOMEM, "cudaMalloc failed");
     TrnArgs A = trn_args(c, itrn);
-    Norms nr;
+    Norms nr{};
     int launches = 0, rc;
     if ((rc = trn_resid(c, A, nr, launches))) return rc;
     A.val = val ? full.p : nullptr;
