@@ -183,6 +183,7 @@ def test_transport_error_indicator_matches_oracle():
             for j in range(2):
                 s.set_conc(j, lvl, o.get_conc(j, lvl))
     g.set_dt(m.dt, m.series_values(0.0, m.dt))
+    g.set_wd(o.get_wd())                  # the flow's indicator marks elements with wd_flag > 0
     srt = np.full(len(m.materials), 100.0)
     trt = np.array([[c.refine_tol] * len(m.materials) for c in m.constituents])
     eg, _ = g.elem_error(srt)
