@@ -67,6 +67,15 @@ struct KrylovCtl {
     int converged;        // 1 = stopping test met, 0 = hit max_lin_it
     int pad;
     double rnorm, bnorm;
+    // A batch launch may pause an instance at the top of an iteration so that a later launch,
+    // with the CTAs of the instances that have finished, resumes it (KrylovTab::done_ctas).  The
+    // instance's first CTA sets pause_at (the iteration at whose top it stops) before the
+    // iteration's second grid barrier; every CTA reads it at the next loop top.  The loop's
+    // scalars are kept here; the vectors stay where they are.
+    int pause_at;         // 0: no pause requested
+    int paused;           // 1: the launch ended at a pause, the solve resumes in the next one
+    int s_it, s_best_it, s_pending, s_upd, s_cur, s_nred;
+    double s_rnorm, s_tol, s_rho, s_alpha, s_omega, s_beta, s_best;
 };
 
 // Grid barrier with a bounded spin.  Arrivals only ever add to one counter, so the b-th
@@ -271,6 +280,9 @@ struct KrylovOne {
         return Q;
     }
     __device__ __forceinline__ bool fuse_update(const KrylovInst& KI) const { return KI.K.fuse_update != 0; }
+    __device__ __forceinline__ unsigned* done_counter() const { return nullptr; }
+    __device__ __forceinline__ unsigned pause_threshold() const { return 0u; }
+    __device__ __forceinline__ bool resuming() const { return false; }
 };
 struct KrylovTab {
     const KrylovInst* tab;
@@ -279,6 +291,18 @@ struct KrylovTab {
     StageLayout lay;
     int fuse;                 // fused update for every instance of the launch (their vectors together)
     const double* rtol_dev;   // when set, instance k's tolerance is read at rtol_dev[k] (graph replays)
+    // Rebalancing (host-driven launches only): every CTA whose instance finished adds one to
+    // *done_ctas (zeroed before the launch); once it reaches pause_after, the instances still
+    // running pause at their next iteration top.  resume = 1: every instance of the launch
+    // continues a paused solve from the scalars in its KrylovCtl.  An instance's partial
+    // structure depends on its virtual grid alone, so its bits do not depend on where it paused
+    // nor on how many CTAs each launch gave it.
+    unsigned* done_ctas;      // nullptr: no pausing
+    unsigned pause_after;
+    int resume;
+    __device__ __forceinline__ unsigned* done_counter() const { return done_ctas; }
+    __device__ __forceinline__ unsigned pause_threshold() const { return pause_after; }
+    __device__ __forceinline__ bool resuming() const { return resume != 0; }
     __device__ __forceinline__ const KrylovInst& get(int& pl, int& np, double& rt) const {
         int nb;
         const int b = blockIdx.x;
@@ -296,6 +320,17 @@ struct KrylovTab {
     }
     __device__ __forceinline__ bool fuse_update(const KrylovInst&) const { return fuse != 0; }
 };
+
+// the control words of the instances a launch resumes: a fresh barrier, no pause pending (the
+// saved scalars stay)
+static __global__ void k_krylov_rearm(KrylovCtl* ctl, const __grid_constant__ LaunchMap mp) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= mp.n) return;
+    KrylovCtl* c = ctl + mp.ids[j];
+    c->count = 0;
+    c->pause_at = 0;
+    c->paused = 0;
+}
 
 // bytes of one epilogue vector's slice for a full tile (3 components per row)
 template <typename VT>
@@ -462,6 +497,7 @@ __device__ __forceinline__ void row_apply(bool active, int lane8, int kb, int ke
 template <typename MT, typename VT, int STAGES, class KS>
 __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_constant__ KS src) {
     __shared__ double red[4 * kKrylovWarps];
+    __shared__ int s_pause;                     // the instance's pause_at, read at a loop top
     constexpr bool STAGED = STAGES > 0;
     constexpr int NST = STAGES > 0 ? STAGES : 1;
     __shared__ unsigned long long bar[NST];     // per ring stage: its tile copy has landed ("full")
@@ -638,8 +674,9 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
     };
 
     int cur = 0;   // the copy of u, r, p, Ap that holds the current iterate
+    const bool resume = src.resuming();
     // b <- M^-1 b'
-    for (int i = pt0; rows && i < V; i += pstride) {
+    for (int i = pt0; !resume && rows && i < V; i += pstride) {
         const double* d = Dinv + (size_t)i * 9;
         const double b0 = K.bs[3 * i], b1 = K.bs[3 * i + 1], b2 = K.bs[3 * i + 2];
 #pragma unroll
@@ -649,9 +686,28 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
             U2[0][3 * i + c] = y;
         }
     }
-    if (!gsync()) return;
+    if (!resume && !gsync()) return;
     // r = b - M^-1 A u, q = r, p = r; norms and rho
     {
+        double rnorm, rho, rhop, alpha, omega, beta, tol, best;
+        int it, best_it;
+        bool pending, upd;
+        if (resume) {   // the scalars of the paused solve (written by the previous launch)
+            rnorm = ctl->s_rnorm;
+            tol = ctl->s_tol;
+            rho = ctl->s_rho;
+            rhop = 1.0;   // dead at a loop top (set from rho before its use)
+            alpha = ctl->s_alpha;
+            omega = ctl->s_omega;
+            beta = ctl->s_beta;
+            best = ctl->s_best;
+            it = ctl->s_it;
+            best_it = ctl->s_best_it;
+            pending = ctl->s_pending != 0;
+            upd = ctl->s_upd != 0;
+            cur = ctl->s_cur;
+            nred = ctl->s_nred;
+        } else {
         double vals[4] = {0, 0, 0, 0};
         const int ism[4] = {MAX, MAX, SUM, SUM};
         const VT* ev2[2] = {b, U2[0]};
@@ -688,18 +744,21 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         double rd[4];
         grid_allreduce<4>(pbuf(), VG, ism, rd, red);
         nred++;
-        double rnorm = rd[0];
+        rnorm = rd[0];
         const double bnorm = rd[1];
-        double rho = rd[2], rhop = 1.0, alpha = 1.0, omega = 1.0, beta = 0.0;
-        int it = 0;
-        const double tol = K.atol + bnorm * rtol;
+        if (pl == 0 && threadIdx.x == 0) ctl->bnorm = bnorm;   // read back with the outcome
+        rho = rd[2], rhop = 1.0, alpha = 1.0, omega = 1.0, beta = 0.0;
+        it = 0;
+        tol = K.atol + bnorm * rtol;
         // best iterate so far: past its attainable accuracy BiCGSTAB's residual drifts back up,
         // so on stagnation (no new best for kStall iterations) or at max_lin_it the best one is
         // used.  It is saved lazily: when an iteration sets a new best (`pending`), the next
         // update, which reads u anyway, writes that u to ubest.
-        double best = rnorm;
-        int best_it = 0;
-        bool pending = true;
+        best = rnorm;
+        best_it = 0;
+        pending = true;
+        upd = false;
+        }
         // An iteration's update (u += alpha p + omega s, r = s - omega As, p = beta (p - omega Ap)
         // + r) is either its own vector pass with a grid barrier (fuse_update 0) or applied by the
         // first sweep of the next iteration (fuse_update 1): that sweep's epilogue updates its own
@@ -708,8 +767,30 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
         // stopping test of the updated residual then follows that sweep; when it stops the solve,
         // the product A p that sweep formed is not used.
         const bool fuse = src.fuse_update(KI);
-        bool upd = false;
         while (upd || (rnorm > tol && it < K.maxit && it - best_it < kStall)) {
+            if (src.done_counter()) {   // a pause requested before the last iteration's second barrier
+                if (threadIdx.x == 0) s_pause = *(volatile int*)&ctl->pause_at;
+                __syncthreads();
+                if (s_pause != 0 && it >= s_pause) {
+                    if (pl == 0 && threadIdx.x == 0) {
+                        ctl->s_rnorm = rnorm;
+                        ctl->s_tol = tol;
+                        ctl->s_rho = rho;
+                        ctl->s_alpha = alpha;
+                        ctl->s_omega = omega;
+                        ctl->s_beta = beta;
+                        ctl->s_best = best;
+                        ctl->s_it = it;
+                        ctl->s_best_it = best_it;
+                        ctl->s_pending = pending ? 1 : 0;
+                        ctl->s_upd = upd ? 1 : 0;
+                        ctl->s_cur = cur;
+                        ctl->s_nred = nred;
+                        ctl->paused = 1;
+                    }
+                    return;
+                }
+            }
             // [update of iteration it] and Ap = M^-1 A p, gamma = q . Ap
             {
                 double g[4] = {0, 0, 0, 0};
@@ -833,6 +914,12 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
                         block_partial<3>(w, wm, pbuf(), v, red);
                         w[0] = w[1] = w[2] = 0.0;
                     });
+                // the pause request: after this iteration's first barrier (which every CTA
+                // reaches after its last loop-top read) and before its second one (which every
+                // CTA passes before its next loop-top read)
+                if (src.done_counter() && pl == 0 && threadIdx.x == 0 && *(volatile int*)&ctl->pause_at == 0 &&
+                    *(volatile unsigned*)src.done_counter() >= src.pause_threshold())
+                    *(volatile int*)&ctl->pause_at = it;
                 if (!gsync()) return;
                 grid_allreduce<3>(pbuf(), VG, wm, w, red);
                 nred++;
@@ -945,8 +1032,8 @@ __global__ void __launch_bounds__(kKrylovThreads, 3) k_bicgstab(const __grid_con
             ctl->iterations = it;
             ctl->converged = conv ? 1 : 0;
             ctl->rnorm = conv ? rnorm : best;
-            ctl->bnorm = bnorm;
         }
+        if (src.done_counter() && threadIdx.x == 0) atomicAdd(src.done_counter(), 1u);   // this CTA's instance is done
     }
 }
 

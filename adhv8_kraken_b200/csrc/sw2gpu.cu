@@ -350,6 +350,13 @@ struct Runner {
     unsigned c_off = 0, r_off = 0, v_off = 0, stage_bytes = 0;
     size_t smem = 0;
     int capacity = 0;             // co-resident Krylov CTAs
+    // Krylov rebalancing of host-driven batch launches: up to rb_rounds launches per solve; in
+    // every launch but the last, once rb_frac of its CTAs have finished their instances, the
+    // instances still running pause and the next launch shares all CTAs among them
+    int rb_rounds = 4;
+    double rb_frac = 0.5;
+    DBuf<unsigned> kdone;         // finished-CTA counter of each round
+    static constexpr int kMaxRounds = 8;
     int cap = 0;                  // instances the tables hold
     int launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -499,7 +506,8 @@ int runner_alloc(Runner& R, cudaStream_t stream, bool mixed, int cap) {
     R.stream = stream;
     R.mixed = mixed;
     R.cap = cap;
-    if (R.ktab.alloc(cap) || R.dtab.alloc(cap) || R.norms.alloc(cap) || R.ctl.alloc(cap) || R.singular.alloc(cap))
+    if (R.ktab.alloc(cap) || R.dtab.alloc(cap) || R.norms.alloc(cap) || R.ctl.alloc(cap) || R.singular.alloc(cap) ||
+        R.kdone.alloc(Runner::kMaxRounds))
         return fail(SW2GPU_E_NOMEM, "batch tables");
     CK(cudaMemsetAsync(R.norms.p, 0, sizeof(Norms) * cap, stream));
     CK(cudaMemsetAsync(R.ctl.p, 0, sizeof(KrylovCtl) * cap, stream));
@@ -831,24 +839,32 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
 // Krylov CTAs per instance: shares of the co-resident capacity by expected work (blocks x
 // iterations of the instance's last solve), at least one, at most its virtual CTAs, so that
 // the instances of a launch finish together
-std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub) {
+std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub, const std::vector<int>* done = nullptr) {
     // A launch lasts as long as its instance with the most work per CTA, so the shares minimise
     // that maximum: every instance starts with one CTA, and each further CTA goes to the instance
     // whose predicted work per CTA is then the largest (ties to the lower index), up to its
     // virtual grid.  (Proportional shares rounded down left instances that should have 1.7 CTAs
     // with one.)  The shares set only the speed: the results of an instance depend on its
     // virtual grid alone.
-    auto work = [&](const sw2gpu_ctx* c) { return (double)c->nnzb * (double)std::max(c->pred_its, 1); };
+    // A resumed solve (done[k] iterations behind it) is predicted to need the rest of its
+    // prediction, or half as many again as it has done once it is past the prediction.
     const int n = (int)sub.size();
+    std::vector<double> W(n);
+    for (int j = 0; j < n; j++) {
+        const sw2gpu_ctx* c = R.ctx[sub[j]];
+        const int pred = std::max(c->pred_its, 1);
+        const int d = done ? (*done)[sub[j]] : 0;
+        W[j] = (double)c->nnzb * (double)(d ? std::max(pred - d, (d + 1) / 2) : pred);
+    }
     std::vector<int> P(n, 1);
     std::priority_queue<std::pair<double, int>> pq;   // (work per CTA, -j)
     for (int j = 0; j < n; j++)
-        if (R.ctx[sub[j]]->krylov_grid > 1) pq.push({work(R.ctx[sub[j]]), -j});
+        if (R.ctx[sub[j]]->krylov_grid > 1) pq.push({W[j], -j});
     for (int left = R.capacity - n; left > 0 && !pq.empty(); left--) {
         const int j = -pq.top().second;
         pq.pop();
         const sw2gpu_ctx* c = R.ctx[sub[j]];
-        if (++P[j] < c->krylov_grid) pq.push({work(c) / P[j], -j});
+        if (++P[j] < c->krylov_grid) pq.push({W[j] / P[j], -j});
     }
     return P;
 }
@@ -984,15 +1000,13 @@ int launch_linear(Runner& R, const std::vector<int>& all, const std::vector<doub
     if ((rc = launch_dilu(R, dl, eta))) return rc;
     // instances that cannot all be co-resident go in successive launches
     size_t j0 = 0;
+    const StageLayout lay{R.c_off, R.r_off, R.v_off, R.stage_bytes};
     while (j0 < sub.size()) {
         std::vector<int> grp;
         for (size_t j = j0; j < sub.size() && (int)grp.size() < R.capacity; j++) grp.push_back(sub[j]);
         j0 += grp.size();
-        const std::vector<int> P = krylov_shares(R, grp);
-        const StageLayout lay{R.c_off, R.r_off, R.v_off, R.stage_bytes};
-        int total = 0;
-        for (int q : P) total += q;
         if (grp.size() == 1) {
+            const std::vector<int> P = krylov_shares(R, grp);
             KrylovOne one;
             one.Q = R.ktab_h[grp[0]];
             one.rtol = eta[grp[0]];
@@ -1000,8 +1014,19 @@ int launch_linear(Runner& R, const std::vector<int>& all, const std::vector<doub
             one.lay = lay;
             void* args[] = {(void*)&one};
             void* kern = R.mixed ? krylov_kernel<float, KrylovOne>(R.stages) : krylov_kernel<double, KrylovOne>(R.stages);
-            CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kKrylovThreads), args, R.smem, R.stream));
-        } else {
+            CK(cudaLaunchCooperativeKernel(kern, dim3(P[0]), dim3(kKrylovThreads), args, R.smem, R.stream));
+            R.launches++;
+            continue;
+        }
+        // rebalancing rounds (host-driven launches only: the host reads which instances paused)
+        const int rounds = R.capturing ? 1 : std::max(1, std::min(R.rb_rounds, (int)Runner::kMaxRounds));
+        if (rounds > 1) CK(cudaMemsetAsync(R.kdone.p, 0, sizeof(unsigned) * rounds, R.stream));
+        std::vector<int> done(R.ctx.size(), 0);   // iterations a paused solve has behind it
+        for (int round = 0; round < rounds; round++) {
+            const bool last = round + 1 == rounds;
+            const std::vector<int> P = krylov_shares(R, grp, round ? &done : nullptr);
+            int total = 0;
+            for (int q : P) total += q;
             static thread_local KrylovTab t;   // ~4 KB: not on the stack of every caller
             int off = 0;
             t.tab = R.ktab.p;
@@ -1018,11 +1043,29 @@ int launch_linear(Runner& R, const std::vector<int>& all, const std::vector<doub
             long long nodes = 0;
             for (int k : grp) nodes += C(k)->V;
             t.fuse = krylov_fuse_update(nodes);
+            t.done_ctas = last ? nullptr : R.kdone.p + round;
+            t.pause_after = (unsigned)std::ceil(R.rb_frac * total);
+            t.resume = round > 0 ? 1 : 0;
+            if (round > 0) {
+                k_krylov_rearm<<<nblk((int)grp.size(), 128), 128, 0, R.stream>>>(R.ctl.p, t.mp);
+                R.launches++;
+            }
             void* args[] = {(void*)&t};
             void* kern = R.mixed ? krylov_kernel<float, KrylovTab>(R.stages) : krylov_kernel<double, KrylovTab>(R.stages);
             CK(cudaLaunchCooperativeKernel(kern, dim3(total), dim3(kKrylovThreads), args, R.smem, R.stream));
+            R.launches++;
+            if (last) break;
+            CK(cudaMemcpyAsync(R.ctl_h, R.ctl.p, sizeof(KrylovCtl) * R.ctx.size(), cudaMemcpyDeviceToHost, R.stream));
+            CK(cudaStreamSynchronize(R.stream));
+            std::vector<int> next;
+            for (int k : grp)
+                if (R.ctl_h[k].paused && !R.ctl_h[k].err) {
+                    next.push_back(k);
+                    done[k] = R.ctl_h[k].s_it;
+                }
+            if (next.empty()) break;
+            grp.swap(next);
         }
-        R.launches++;
     }
     return 0;
 }
@@ -3163,6 +3206,14 @@ int32_t sw2gpu_engine_active(const sw2gpu_engine* e) { return e ? (int32_t)e->in
 int sw2gpu_engine_last_tick(const sw2gpu_engine* e, sw2gpu_stats* out) {
     if (!e || !out) return fail(SW2GPU_E_ARG, "null argument");
     *out = e->last;
+    return SW2GPU_OK;
+}
+
+int sw2gpu_engine_set_rebalance(sw2gpu_engine* e, int32_t rounds, double fraction) {
+    if (!e || rounds < 1 || rounds > Runner::kMaxRounds || !(fraction >= 0.0 && fraction <= 1.0))
+        return fail(SW2GPU_E_ARG, "rebalance: rounds in [1, %d], fraction in [0, 1]", Runner::kMaxRounds);
+    e->R->rb_rounds = rounds;
+    e->R->rb_frac = fraction;
     return SW2GPU_OK;
 }
 

@@ -56,7 +56,7 @@ constexpr size_t kScratchDoubles = kOffVec + kKrylovVectors * al(3ull * kMaxNode
 static_assert(kScratchDoubles * sizeof(double) > 16650000 && kScratchDoubles * sizeof(double) < 16750000,
               "the work array is documented as 16.7 MB");
 // the structure-check word sits in the control region, after the KrylovCtl record
-constexpr size_t kCheckByte = 64;
+constexpr size_t kCheckByte = 192;
 static_assert(sizeof(KrylovCtl) <= kCheckByte && kCheckByte + sizeof(int) <= kAlign * sizeof(double),
               "control region layout");
 constexpr int kBadRowRange = 1, kBadColumn = 2, kBadDiagonal = 4;   // bits of the check word

@@ -31,6 +31,7 @@ SYMBOLS = ["sw2gpu_abi_version", "sw2gpu_last_error", "sw2gpu_create", "sw2gpu_d
            "sw2gpu_resid", "sw2gpu_load", "sw2gpu_linear_solve", "sw2gpu_batch_create", "sw2gpu_batch_step",
            "sw2gpu_batch_destroy", "sw2gpu_bcsr_solve_noalloc", "sw2gpu_engine_create", "sw2gpu_engine_add",
            "sw2gpu_engine_tick", "sw2gpu_engine_active", "sw2gpu_engine_last_tick", "sw2gpu_engine_destroy",
+           "sw2gpu_engine_set_rebalance",
            "sw2gpu_device_bytes", "sw2gpu_autotune", "sw2gpu_set_graphs", "sw2gpu_set_variant", "sw2gpu_get_variant",
            "sw2gpu_server_create", "sw2gpu_server_submit", "sw2gpu_server_wait", "sw2gpu_server_status",
            "sw2gpu_server_destroy", "sw2gpu_grid_mass", "sw2gpu_mass_flux", "sw2gpu_set_dacont", "sw2gpu_get_dacont",
@@ -83,6 +84,7 @@ def lib():
         L.sw2gpu_engine_active.restype = C.c_int32
         L.sw2gpu_engine_destroy.argtypes = [vp]
         L.sw2gpu_engine_last_tick.argtypes = [vp, vp]
+        L.sw2gpu_engine_set_rebalance.argtypes = [vp, C.c_int32, C.c_double]
         L.sw2gpu_device_bytes.argtypes = [vp]
         L.sw2gpu_autotune.argtypes = [vp, c_int32_p, c_int32_p]
         L.sw2gpu_set_graphs.argtypes = [vp, C.c_int32]
@@ -541,6 +543,12 @@ class SW2Engine:
                 s.t = d["t"]
             done.append(d)
         return done
+
+    def set_rebalance(self, rounds: int, fraction: float = 0.5):
+        """Krylov rebalancing (sw2gpu_engine_set_rebalance): up to `rounds` launches per batched
+        solve; once `fraction` of a launch's CTAs have finished, the instances still iterating
+        pause and the next launch shares all CTAs among them.  rounds = 1: off."""
+        _check(lib().sw2gpu_engine_set_rebalance(self.h, int(rounds), float(fraction)))
 
     def last_tick(self):
         """Device time and phases of the last tick (see sw2gpu_engine_last_tick)."""

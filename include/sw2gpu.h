@@ -409,6 +409,13 @@ int32_t sw2gpu_engine_active(const sw2gpu_engine *e);
  * iteration count among them, in linesearch_cuts the instances that started a time step,
  * in wd_elems the instances in the engine */
 int sw2gpu_engine_last_tick(const sw2gpu_engine *e, sw2gpu_stats *out);
+/* Krylov rebalancing of the engine's launches (default 4 rounds, fraction 0.5): a batched
+ * Krylov launch lasts as long as its slowest instance, so in every launch but the last of
+ * `rounds`, once `fraction` of its CTAs have finished their instances, the instances still
+ * iterating pause at an iteration boundary and the next launch shares all CTAs among them.
+ * Results do not change (an instance's reductions depend only on its own partition, not on
+ * its CTAs); rounds = 1 turns it off.  rounds in [1, 8], fraction in [0, 1]. */
+int sw2gpu_engine_set_rebalance(sw2gpu_engine *e, int32_t rounds, double fraction);
 int sw2gpu_engine_destroy(sw2gpu_engine *e);
 
 /* Request server (no counterpart in the reference): a request loop in the library.  Each

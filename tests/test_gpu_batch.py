@@ -77,9 +77,13 @@ def _run_alone(solver, nsteps, max_retries=8):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", [capi.SW2GPU_FP64, capi.SW2GPU_MIXED])
-def test_engine_equals_alone(precision):
+@pytest.mark.parametrize("rebalance", [(1, 0.5), (4, 0.5), (8, 0.0)], ids=["off", "default", "every-iteration"])
+def test_engine_equals_alone(precision, rebalance):
     """Continuous batching: instances with different step counts join one engine (one of
-    them later, while the others are mid-run) and each ends bitwise where it ends alone."""
+    them later, while the others are mid-run) and each ends bitwise where it ends alone --
+    without Krylov rebalancing, with the default rounds, and with every solve paused after
+    each of its first seven iterations (fraction 0: the pause fires at once) and resumed in
+    the next launch with a different CTA share."""
     from adhv8_kraken_b200.sw2 import SW2Engine
     models = uneven_models()
     nsteps = [3, 2, 4, 1]
@@ -91,6 +95,7 @@ def test_engine_equals_alone(precision):
         g.close()
     solvers = [SW2GPU(m, precision=precision) for m in models]
     eng = SW2Engine(precision)
+    eng.set_rebalance(*rebalance)
     for g, n in list(zip(solvers, nsteps))[:3]:
         eng.add(g, n)
     done = eng.tick() + eng.tick()
