@@ -14,6 +14,10 @@
 // identical control decisions, and an instance's results are bitwise the same alone, in any
 // batch and on reruns.  s = r - alpha Ap is never stored: the second SpMV forms it on the
 // fly from r and Ap.
+// A batch launch may stop the instances still iterating at an iteration boundary once enough
+// CTAs have finished theirs (KrylovTab::done_ctas), keeping the loop scalars in each
+// instance's KrylovCtl; the next launch resumes them with all CTAs shared among them.  The
+// partial structure stays that of the instance's virtual grid, so the bits do not change.
 // On exit the kernel applies the Newton increment: x = S u, state += x (fe_sw2_inc),
 // sol = -x (fe_newton.c:561-585).
 #pragma once
