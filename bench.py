@@ -245,6 +245,11 @@ def run_serving(models, horizons, lam: float, seed: int = 1):
     return out
 
 
+# Krylov rebalancing of the engine legs (sw2gpu_engine_set_rebalance): up to 4 launches per
+# batched solve, the instances still iterating paused once half a launch's CTAs are done
+ENGINE_REBALANCE = (4, 0.5)
+
+
 def run_ensemble(models, stream, steps: int):
     """Config-4 legs on the same instances, every instance running `steps` time steps (a failed
     step is retried with dt / 4 and counts as wasted time; dt doubles back toward the nominal
@@ -297,6 +302,7 @@ def run_ensemble(models, stream, steps: int):
 
     def engine(gs, precision):
         eng = SW2Engine(precision, stream=stream.cuda_stream)
+        eng.set_rebalance(*ENGINE_REBALANCE)
         for g in gs:
             eng.add(g, steps)
         res, ph = [], {"jac_ms": 0.0, "krylov_ms": 0.0, "resid_ms": 0.0, "other_ms": 0.0}
@@ -324,7 +330,7 @@ def run_ensemble(models, stream, steps: int):
         eng.close()
         reset(gs)
 
-    out = {}
+    out = {"krylov_rebalance": {"rounds": ENGINE_REBALANCE[0], "fraction": ENGINE_REBALANCE[1]}}
     g64 = [SW2GPU(m, precision=capi.SW2GPU_FP64, stream=stream.cuda_stream) for m in models]
     warm(g64, capi.SW2GPU_FP64)
     ms, done = timed(lambda: alone(g64))
