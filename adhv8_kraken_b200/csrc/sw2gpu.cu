@@ -33,6 +33,7 @@
 #include "sw2_kernels.cuh"
 #include "sw2_krylov.cuh"
 #include "sw2_series.h"
+#include "sw2_shares.h"
 #include "trn_kernels.cuh"
 #include "newton_ctl.cuh"
 
@@ -840,33 +841,17 @@ int launch_jacobian(Runner& R, const std::vector<int>& sub) {
 // iterations of the instance's last solve), at least one, at most its virtual CTAs, so that
 // the instances of a launch finish together
 std::vector<int> krylov_shares(Runner& R, const std::vector<int>& sub, const std::vector<int>* done = nullptr) {
-    // A launch lasts as long as its instance with the most work per CTA, so the shares minimise
-    // that maximum: every instance starts with one CTA, and each further CTA goes to the instance
-    // whose predicted work per CTA is then the largest (ties to the lower index), up to its
-    // virtual grid.  (Proportional shares rounded down left instances that should have 1.7 CTAs
-    // with one.)  The shares set only the speed: the results of an instance depend on its
-    // virtual grid alone.
-    // A resumed solve (done[k] iterations behind it) is predicted to need the rest of its
-    // prediction, or half as many again as it has done once it is past the prediction.
+    // the min-max allocation of sw2_shares.h over the instances' predicted work (done[k]:
+    // iterations a resumed solve has behind it)
     const int n = (int)sub.size();
     std::vector<double> W(n);
+    std::vector<int> G(n);
     for (int j = 0; j < n; j++) {
         const sw2gpu_ctx* c = R.ctx[sub[j]];
-        const int pred = std::max(c->pred_its, 1);
-        const int d = done ? (*done)[sub[j]] : 0;
-        W[j] = (double)c->nnzb * (double)(d ? std::max(pred - d, (d + 1) / 2) : pred);
+        W[j] = krylov_work(c->nnzb, c->pred_its, done ? (*done)[sub[j]] : 0);
+        G[j] = c->krylov_grid;
     }
-    std::vector<int> P(n, 1);
-    std::priority_queue<std::pair<double, int>> pq;   // (work per CTA, -j)
-    for (int j = 0; j < n; j++)
-        if (R.ctx[sub[j]]->krylov_grid > 1) pq.push({W[j], -j});
-    for (int left = R.capacity - n; left > 0 && !pq.empty(); left--) {
-        const int j = -pq.top().second;
-        pq.pop();
-        const sw2gpu_ctx* c = R.ctx[sub[j]];
-        if (++P[j] < c->krylov_grid) pq.push({W[j] / P[j], -j});
-    }
-    return P;
+    return krylov_shares_minmax(W, G, R.capacity);
 }
 
 // scaling, preconditioner folding and the persistent BiCGSTAB of the subset, each instance
