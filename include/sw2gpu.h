@@ -361,7 +361,9 @@ int sw2gpu_bcsr_solve_noalloc(int32_t nnodes, int32_t nnzb, const int32_t *row_p
 /* Batched ensemble: many independent contexts stepped together, each Newton phase one
  * launch over all of them (element kernels: per group of up to 30 instances; the Krylov
  * solve: one cooperative launch, each instance on its own range of CTAs); every context
- * keeps its own data and gets bitwise the results it gets alone. */
+ * keeps its own data and gets bitwise the results it gets alone.  Steps launched directly
+ * spread a Krylov solve over up to 4 launches as the engine does by default (see
+ * sw2gpu_engine_set_rebalance); steps replayed from CUDA graphs keep one. */
 typedef struct sw2gpu_batch sw2gpu_batch;
 int sw2gpu_batch_create(sw2gpu_ctx **ctxs, int32_t n, void *stream, sw2gpu_batch **out);
 int sw2gpu_batch_step(sw2gpu_batch *b, const double *dt, const double *const *series, sw2gpu_stats *stats);
